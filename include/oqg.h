@@ -1,0 +1,201 @@
+/*
+ * oqg.h -- C ABI of the B200 implementation of OpenQG's per-timestep
+ * quasi-geostrophic core (module `core`, subroutine `step_qg`).
+ *
+ * Every entry point is `extern "C"`, takes plain pointers and sizes, and
+ * returns an int status (OQG_OK == 0).  No call aborts the process; the
+ * reference's `stop 1` paths (util/linalg.F90:124-136, qg/modes.F90:148-161)
+ * become nonzero status codes, and oqg_last_error() gives the message.
+ *
+ * Arrays crossing this boundary are FP64 in the reference's Fortran
+ * column-major layout: element (i, j, k) of an (nxp, nyp, nl) array is at
+ * offset i + nxp*(j + nyp*k), with 0-based i, j, k.  Host buffers are owned
+ * by the caller.  A handle owns one CUDA stream; a handle is not thread-safe,
+ * distinct handles are.
+ *
+ * Reference interface replaced (file:line within BreakawayLabs/openqg):
+ *   step_qg(tdt, ent, wekp, txis, txin, qg)        src/qg/core.F90:16-33
+ *   init_qg(go, bcco, delek, ah2, ah4, gp, rho,...) src/qg/qg.F90:60-103
+ *   init_pv / qcomp                                 src/qg/vorsubs.F90:17-56
+ *   init_constraint / init_mass_constr              src/qg/constraint.F90:80-165
+ *   suppress_comp_mode                              src/driver.F90:174-189
+ *   restart_qg / save_qg state (p, pm)              src/state.F90:29-112
+ *   solve_inhomog_eqn / generate_homog_soln         src/qg/inhomog.F90:146-168
+ *   ekman_from_tau                                  src/coupler/ekman.F90:53-83
+ *   qg_diagno (ekei, sfmin, sfmax, circ)            src/diagnostics/qg_monitor.F90:289-376
+ */
+#ifndef OQG_H
+#define OQG_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define OQG_MAX_NL 8
+
+/* status codes */
+#define OQG_OK           0
+#define OQG_EINVAL       1  /* bad argument or parameter set            */
+#define OQG_ECUDA        2  /* CUDA runtime error                        */
+#define OQG_ENAN         3  /* non-finite value found in the state       */
+#define OQG_ETIMEOUT     4  /* a bounded device wait ran out             */
+#define OQG_EUNSUPPORTED 5  /* size or mode this build does not handle   */
+#define OQG_ESETUP       6  /* init-time check failed (e.g. mode matrix
+                               product not the identity, singular LU)   */
+#define OQG_ENODEV       7  /* no CUDA device                            */
+
+/* precision modes */
+#define OQG_FP64   0  /* everything FP64, the reference's arithmetic            */
+#define OQG_MIXED  1  /* FP32 state, stencils, Jacobian and x-transforms; FP64
+                         vertical-mode projection, tridiagonal solves and
+                         constraint / area integrals                          */
+
+/*
+ * Parameters of one QG basin: the fields init_qg receives (qg.F90:60-70)
+ * plus the box geometry (glam/box.F90:11-41) and topography (topog.F90:20-21).
+ * Lengths in m, times in s, like the reference.
+ */
+typedef struct oqg_params {
+    int    nxp, nyp, nl;      /* p-grid points and layers (nxp = nxt+1)        */
+    int    cyclic;            /* 1: zonally periodic channel; 0: closed box    */
+    double dx, dy;            /* grid spacing                                   */
+    double fnot, beta;        /* f0 and beta of the beta-plane                  */
+    int    dz_sign;           /* -1 ocean, +1 atmosphere (basin.F90:36,129)     */
+    int    tau_sign;          /* +1 ocean, -1 atmosphere (basin.F90:62,158)     */
+    double h[OQG_MAX_NL];     /* layer thicknesses, nl used                     */
+    double gp[OQG_MAX_NL];    /* reduced gravities, nl-1 used                   */
+    double ah2[OQG_MAX_NL];   /* Laplacian viscosity per layer                  */
+    double ah4[OQG_MAX_NL];   /* biharmonic viscosity per layer                 */
+    double bcco;              /* mixed boundary coefficient (0 free slip,
+                                 large -> no slip)                              */
+    double delek;             /* bottom Ekman layer thickness                   */
+    double rho;               /* density used by the diagnostics                */
+    int    k_topo;            /* 1-based layer carrying topography and drag     */
+    int    precision;         /* OQG_FP64 or OQG_MIXED                          */
+    int    suppress_period;   /* average time levels when mod(nt-1,period)==0
+                                 (openqg.F90:485-487); 0 never                  */
+    const double *ddyn;       /* (nxp, nyp) dynamic topography; NULL = flat     */
+} oqg_params;
+
+typedef struct oqg_handle oqg_handle;
+
+/* Message of the last failure on this thread ("" if none). */
+const char *oqg_last_error(void);
+
+/* Library and device description (for logs): writes a NUL-terminated string. */
+int oqg_version(char *buf, int buflen);
+
+/* init_qg (qg.F90:60-103): vertical modes, Helmholtz tables and homogeneous
+ * solutions are computed, uploaded and kept on the current CUDA device.
+ * State starts at zero, forcing at zero, step counter nt = 0. */
+int oqg_create(const oqg_params *prm, oqg_handle **out);
+int oqg_destroy(oqg_handle *h);
+
+/* Restart semantics (openqg.F90:233-243, state.F90:29-44): takes p, pm
+ * (nxp,nyp,nl) and recomputes q, qm (init_pv), the channel momentum
+ * constraints (init_constraint) and the mass constraint (init_mass_constr). */
+int oqg_set_state(oqg_handle *h, const double *p, const double *pm);
+
+/* Full state: p, pm, q, qm (nxp,nyp,nl) and the constraint scalars
+ * dpi, dpip (nl-1) and cs, cn, csp, cnp (nl; ignored for a box). */
+int oqg_set_state_full(oqg_handle *h, const double *p, const double *pm,
+                       const double *q, const double *qm,
+                       const double *dpi, const double *dpip,
+                       const double *cs, const double *cn,
+                       const double *csp, const double *cnp);
+
+/* Copies the state out; any pointer may be NULL to skip that field. */
+int oqg_get_state(oqg_handle *h, double *p, double *pm, double *q, double *qm);
+int oqg_get_constraints(oqg_handle *h, double *dpi, double *dpip,
+                        double *cs, double *cn, double *csp, double *cnp);
+
+/* Copies layer k (0-based) of p out: the p(:,:,1) exchange of
+ * driver.F90:99-101. */
+int oqg_get_p_layer(oqg_handle *h, int k, double *out);
+
+/* Forcing of step_qg: wekp (nxp,nyp), ent (nxp,nyp,nl-1) or NULL for zero
+ * entrainment, and the channel wind-stress integrals txis, txin.  Stored on
+ * the device and reused by every step until set again. */
+int oqg_set_forcing(oqg_handle *h, const double *wekp, const double *ent,
+                    double txis, double txin);
+
+/* Runs nsteps calls of step_qg(tdt, ...) (core.F90:16-33).  Before step nt
+ * (1-based, counted by the handle) returns, suppress_comp_mode is applied when
+ * suppress_period > 0 and mod(nt-1, suppress_period) == 0, as the run loop
+ * does (openqg.F90:485-487, driver.F90:78-85).  Steps are queued on the
+ * handle's stream; the call returns after they are queued (see oqg_sync). */
+int oqg_step(oqg_handle *h, double tdt, int nsteps);
+
+/* Sets the step counter (number of steps already taken, nt-1 of the next). */
+int oqg_set_step_index(oqg_handle *h, long long steps_done);
+int oqg_get_step_index(oqg_handle *h, long long *steps_done);
+
+/* suppress_comp_mode (driver.F90:174-189) applied once, now. */
+int oqg_suppress(oqg_handle *h);
+
+/* Waits for the handle's stream; reports a deferred device error. */
+int oqg_sync(oqg_handle *h);
+
+/* Device validity scan of p and q (the role of valids, valsubs.F90:46-139):
+ * *bad = number of non-finite values found. */
+int oqg_check_finite(oqg_handle *h, long long *bad);
+
+/* Diagnostics of qg_diagno (qg_monitor.F90:289-376), each of length nl:
+ * layer kinetic energy ekei, stream-function extrema sfmin/sfmax (Sv) and the
+ * total circulation circ (Sv).  Any pointer may be NULL. */
+int oqg_diag(oqg_handle *h, double *ekei, double *sfmin, double *sfmax,
+             double *circ);
+
+/* solve_inhomog_eqn (inhomog.F90:156-168): (Del^2 - rdm2(m)) out = rhs with
+ * out = 0 on solid boundaries; m is the 1-based mode; rhs, out (nxp, nyp). */
+int oqg_solve_inhomog(oqg_handle *h, int m, const double *rhs, double *out);
+
+/* generate_homog_soln (inhomog.F90:146-154): out = L + rdm2(m)*solve(L). */
+int oqg_generate_homog_soln(oqg_handle *h, int m, const double *L, double *out);
+
+/* Vertical-mode tables of eigmod (modes.F90:46-219); amat, ctl2m, ctm2l are
+ * (nl, nl) column-major, rdm2 has nl entries.  Any pointer may be NULL. */
+int oqg_get_modes(oqg_handle *h, double *amat, double *rdm2,
+                  double *ctl2m, double *ctm2l);
+
+/* ekman_from_tau (ekman.F90:53-83) for a basin with these parameters:
+ * taux, tauy (nxp, nyp) kinematic stress -> wekp (nxp, nyp) Ekman velocity at
+ * p points and, for a channel, the boundary integrals txis, txin. */
+int oqg_ekman_from_tau(const oqg_params *prm, const double *taux,
+                       const double *tauy, double *wekp,
+                       double *txis, double *txin);
+
+/* Device pointers of the state, for zero-copy use by the PyTorch extension:
+ * p, pm, q, qm as (nl, nyp, pitch) arrays of the handle's storage type
+ * (FP64 or, in OQG_MIXED, FP32); *pitch is the row pitch in elements. */
+int oqg_device_state(oqg_handle *h, void **p, void **pm, void **q, void **qm,
+                     int *pitch, int *elem_bytes);
+
+/* CUDA stream of the handle (a cudaStream_t). */
+int oqg_stream(oqg_handle *h, void **stream);
+
+/* ---------------------------------------------------------------------
+ * Ensembles: many independent basins of uneven size stepped together by one
+ * launch per phase (captured in a CUDA graph).  Members keep the semantics of
+ * a single handle.
+ * ------------------------------------------------------------------- */
+typedef struct oqg_ensemble oqg_ensemble;
+
+int oqg_ensemble_create(const oqg_params *members, int nmembers,
+                        oqg_ensemble **out);
+int oqg_ensemble_destroy(oqg_ensemble *e);
+int oqg_ensemble_set_state(oqg_ensemble *e, int member,
+                           const double *p, const double *pm);
+int oqg_ensemble_get_state(oqg_ensemble *e, int member, double *p,
+                           double *pm, double *q, double *qm);
+int oqg_ensemble_set_forcing(oqg_ensemble *e, int member, const double *wekp,
+                             const double *ent, double txis, double txin);
+/* tdt[member] per member; nsteps for all. */
+int oqg_ensemble_step(oqg_ensemble *e, const double *tdt, int nsteps);
+int oqg_ensemble_sync(oqg_ensemble *e);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* OQG_H */
