@@ -1,0 +1,425 @@
+#!/usr/bin/env python
+"""Throughput of the QG core on B200: Mcell-layer-steps/s.
+
+Default workload (N=1): the ocean basin of the coupled configuration, a
+513 x 513 p-point, 3-layer double-gyre box at dx = 10 km in FP64, stepped
+with tdt = 2 dt = 3600 s.  One bench step is a batch of 10 model steps (the
+configuration's 10 ocean steps); Mcell-layer-steps/s counts
+nxp * nyp * nl * model steps / s / 1e6, summed over ranks.
+
+  value   device time of the batches (CUDA events on the handle's stream),
+          inputs resident in HBM, L2 flushed (a 256 MiB write) before every
+          timed batch;
+  e2e     the same work through the C ABI with host buffers: per model step
+          the coupler's exchange of driver.F90:99-107 -- forcing (wekp, ent)
+          uploaded from pinned host memory, one step, layer-1 pressure read
+          back -- timed by the host clock;
+  roofline  the dominant kernel (largest share of a step), timed alone by
+          oqg_profile_phases, against the measured HBM copy bandwidth;
+  cpu_baseline  the FP64 oracle (a restatement of the reference's Fortran,
+          one thread) on a bounded sample of the same basin.
+
+--impl reference times the CPU restatement of the reference (the oracle,
+all host threads) on the same workload; the Fortran reference itself does
+not build here (no Fortran compiler, FFTW, LAPACK or netCDF).
+
+Multi-GPU (torchrun): every rank steps its own basin (replicas, weak
+scaling); the time is the max over ranks.
+"""
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    # name: (builder kwargs, tdt, label)
+    "ocean513": (dict(kind="box", n=513, dx=10e3), 3600.0,
+                 "ocean double gyre 513x513x3 box, dx 10 km (coupled config ocean basin)"),
+    "ocean129": (dict(kind="box", n=129, dx=20e3), 3600.0,
+                 "ocean double gyre 129x129x3 box, dx 20 km"),
+    "atmos193x97": (dict(kind="channel", nxp=193, nyp=97, dx=80e3), 360.0,
+                    "atmosphere channel 193x97x3, dx 80 km (coupled config atmosphere)"),
+    "ocean1025": (dict(kind="box", n=1025, dx=10e3), 3600.0,
+                  "ocean double gyre 1025x1025x3 box, dx 10 km"),
+}
+
+
+def make_basin(name, precision):
+    from openqg_b200.params import atmos_channel, ocean_double_gyre
+    kw, tdt, label = WORKLOADS[name]
+    if kw["kind"] == "box":
+        b = ocean_double_gyre(kw["n"], dx=kw["dx"], precision=precision)
+    else:
+        b = atmos_channel(kw["nxp"], kw["nyp"], dx=kw["dx"], precision=precision)
+    return b, tdt, label
+
+
+def initial_inputs(b, seed, reference=False):
+    """Seeded initial pressure and the double-gyre Ekman pumping.  The
+    reference arm computes the pumping with the CPU restatement."""
+    if reference:
+        from oracle import ekman_from_tau
+    else:
+        from openqg_b200.core import ekman_from_tau
+    from openqg_b200.params import double_gyre_tau, initial_psi
+    p = b.fnot * initial_psi(b, seed=seed) * (30.0 if b.cyclic else 1.0)
+    taux, tauy = double_gyre_tau(b)
+    w, ts, tn = ekman_from_tau(b, taux, tauy)
+    return p, w, ts, tn
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def traffic_table():
+    """Bytes per launch from committed ncu summaries (profiles/traffic.txt)."""
+    out = {}
+    path = os.path.join(ROOT, "profiles", "traffic.txt")
+    if os.path.exists(path):
+        for line in open(path):
+            f = line.split()
+            if len(f) >= 4 and not line.startswith("#"):
+                out[(f[0], f[1], f[2])] = float(f[3])
+    return out
+
+
+class Clocks:
+    """nvidia-smi samples during the timed region."""
+
+    def __init__(self, uuid):
+        self.uuid = uuid
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        cmd = ["nvidia-smi", "--query-gpu=" + q, "--format=csv,noheader,nounits", "-lms", "200"]
+        if self.uuid:
+            cmd += ["-i", self.uuid]
+        try:
+            self.proc = subprocess.Popen(cmd, stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        try:
+            for line in open(self.path):
+                f = [x.strip() for x in line.split(",")]
+                if len(f) >= 9 and f[1].replace(".", "").isdigit():
+                    rows.append(f)
+        except Exception:
+            pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = [float(r[1]) for r in rows]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": float(rows[0][2]),
+                "reasons": reasons, "samples": len(rows)}
+
+
+def cpu_sample(b, p, w, ts, tn, tdt, seconds, threads):
+    """Oracle throughput (Mcell-layer-steps/s) over about `seconds` of work."""
+    import oracle
+    gomp = ctypes.CDLL("libgomp.so.1")
+    oracle.lib()
+    gomp.omp_set_num_threads(int(threads))
+    o = oracle.Oracle(b)
+    o.set_state(p, p)
+    o.set_forcing(w, None, ts, tn)
+    o.step(tdt, 1)                      # warm-up (FFT plans, first touch)
+    n, t0 = 0, time.perf_counter()
+    while True:
+        o.step(tdt, 1)
+        n += 1
+        el = time.perf_counter() - t0
+        if el >= seconds and n >= 2:
+            break
+    o.close()
+    cells = b.nxp * b.nyp * b.nl
+    return cells * n / el / 1e6, n, el
+
+
+def dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def run_reference(args):
+    ws, rank, _ = dist()
+    if rank != 0:
+        return 0
+    from openqg_b200.params import OQG_FP64
+    b, tdt, label = make_basin(args.workload, OQG_FP64)
+    p, w, ts, tn = initial_inputs(b, seed=1, reference=True)
+    import oracle
+    gomp = ctypes.CDLL("libgomp.so.1")
+    oracle.lib()
+    threads = os.cpu_count() or 1
+    gomp.omp_set_num_threads(threads)
+    o = oracle.Oracle(b)
+    o.set_state(p, p)
+    o.set_forcing(w, None, ts, tn)
+    msteps = args.ref_model_steps
+    for _ in range(args.warmup):
+        o.step(tdt, msteps)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        o.step(tdt, msteps)
+    el = time.perf_counter() - t0
+    cells = b.nxp * b.nyp * b.nl
+    value = cells * msteps * args.steps / el / 1e6
+    line = {
+        "impl": "reference", "metric": "Mcell-layer-steps/s", "value": value,
+        "unit": "Mcell-layer-steps/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": el * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": label, "nxp": b.nxp, "nyp": b.nyp, "nl": b.nl,
+                   "model_steps_per_step": msteps, "parallelism": "single process"},
+        "cpu_baseline": {"value": value, "unit": "Mcell-layer-steps/s", "cores": threads,
+                         "kind": "port",
+                         "sample": "%d x %d model steps of the %s basin (FP64 C++ restatement of the "
+                                   "Fortran step_qg, OpenMP on the leapfrog region only)"
+                                   % (args.steps, msteps, args.workload)},
+        "e2e": {"value": value, "unit": "Mcell-layer-steps/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def time_batches(g, tdt, msteps, steps, flush):
+    import torch
+    s = torch.cuda.ExternalStream(g.stream())
+    total = 0.0
+    for _ in range(steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        g.step(tdt, msteps)
+        e1.record(s)
+        e1.synchronize()
+        total += e0.elapsed_time(e1)
+    g.sync()
+    return total
+
+
+def run_ours(args):
+    import torch
+    ws, rank, local = dist()
+    torch.cuda.set_device(local)
+    pg = None
+    if ws > 1:
+        import datetime
+        import torch.distributed as td
+        td.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                              device_id=torch.device("cuda", local))
+        pg = td
+    from openqg_b200.core import QG, lib
+    from openqg_b200.params import OQG_FP64, OQG_MIXED
+    prec = OQG_MIXED if args.precision == "mixed" else OQG_FP64
+    b, tdt, label = make_basin(args.workload, prec)
+    p, w, ts, tn = initial_inputs(b, seed=1 + rank)
+    msteps = args.model_steps
+    cells = b.nxp * b.nyp * b.nl
+    g = QG(b)
+    g.set_state(p, p)
+    g.set_forcing(w, None, ts, tn)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")   # 256 MiB > L2
+    for _ in range(args.warmup):
+        g.step(tdt, msteps)
+    g.sync()
+    if g.check_finite() != 0:
+        raise RuntimeError("non-finite state after warm-up")
+
+    def barrier():
+        if pg:
+            pg.barrier()
+        torch.cuda.synchronize()
+
+    uuid = None
+    try:
+        uuid = "GPU-" + str(torch.cuda.get_device_properties(local).uuid)
+    except Exception:
+        pass
+    barrier()
+    with Clocks(uuid) as clk:
+        total_ms = time_batches(g, tdt, msteps, args.steps, flush)
+        barrier()
+    tmax = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+    if pg:
+        pg.all_reduce(tmax, op=pg.ReduceOp.MAX)
+    total_ms = float(tmax.item())
+    value = ws * cells * msteps * args.steps / (total_ms / 1e3) / 1e6
+
+    # variant: the same basin with FP32 bulk arithmetic
+    variants = {}
+    if args.variants and prec == OQG_FP64:
+        bm, _, _ = make_basin(args.workload, OQG_MIXED)
+        gm = QG(bm)
+        gm.set_state(p, p)
+        gm.set_forcing(w, None, ts, tn)
+        for _ in range(args.warmup):
+            gm.step(tdt, msteps)
+        barrier()
+        tm = time_batches(gm, tdt, msteps, args.steps, flush)
+        tmm = torch.tensor([tm], dtype=torch.float64, device="cuda")
+        if pg:
+            pg.all_reduce(tmm, op=pg.ReduceOp.MAX)
+        variants["mixed_fp32_bulk"] = ws * cells * msteps * args.steps / (float(tmm.item()) / 1e3) / 1e6
+        gm.close()
+
+    # e2e through the C ABI with pinned host buffers
+    L = lib()
+    wk_h = torch.empty(b.shape2, dtype=torch.float64, pin_memory=True)
+    wk_h.copy_(torch.from_numpy(w))
+    ent_h = torch.zeros((b.nl - 1,) + b.shape2, dtype=torch.float64, pin_memory=True)
+    p1_h = torch.empty(b.shape2, dtype=torch.float64, pin_memory=True)
+    dp = ctypes.POINTER(ctypes.c_double)
+    wk_p = ctypes.cast(wk_h.data_ptr(), dp)
+    ent_p = ctypes.cast(ent_h.data_ptr(), dp)
+    p1_p = ctypes.cast(p1_h.data_ptr(), dp)
+    e2e_steps = max(1, min(args.steps, 10))
+
+    def exchange_step():
+        for _ in range(msteps):
+            rc = L.oqg_set_forcing(g.h, wk_p, ent_p, ts, tn)
+            rc |= L.oqg_step(g.h, tdt, 1)
+            rc |= L.oqg_get_p_layer(g.h, 0, p1_p)
+            if rc:
+                raise RuntimeError(L.oqg_last_error().decode())
+
+    exchange_step()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        exchange_step()
+    g.sync()
+    e2e_s = time.perf_counter() - t0
+    te = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+    if pg:
+        pg.all_reduce(te, op=pg.ReduceOp.MAX)
+    e2e_s = float(te.item())
+    e2e_value = ws * cells * msteps * e2e_steps / e2e_s / 1e6
+    h2d = msteps * (b.nxp * b.nyp * 8) * b.nl        # wekp + (nl-1) ent layers
+    d2h = msteps * b.nxp * b.nyp * 8
+
+    # dominant kernel, timed alone, against the HBM roofline
+    g.set_forcing(w, None, ts, tn)
+    ms = g.profile_phases(tdt, 20)
+    names = ["k_vort", "k_xfwd", "k_ysolve", "k_xinv"]
+    dom = int(np.argmax(ms))
+    s = 8 if prec == OQG_FP64 else 4
+    # algorithmic bytes per cell-layer of each phase
+    alg = {
+        # reads p, q, pm, qm (+ wekp once per column of layers); writes q, modal rhs
+        "k_vort": 6 * s + s / b.nl,
+        # reads the modal rhs, writes its transform
+        "k_xfwd": 2 * s,
+        # reads and writes the spectral field (+ FP64 pivots, not counted)
+        "k_ysolve": 2 * s,
+        # reads the spectral field, p (old) and the homogeneous solutions, writes p
+        "k_xinv": 3 * s + s * (b.nl - 1) / b.nl,
+    }
+    peak, peak_kind = peaks()
+    dname = names[dom]
+    achieved = alg[dname] * cells / (ms[dom] / 1e3) / 1e9
+    step_alg = (6 * s + s / b.nl) * cells
+    tt = traffic_table().get((args.workload, args.precision, dname))
+    roof = {"bound": "hbm", "kernel": dname, "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "peak_kind": peak_kind,
+            "traffic": tt, "alg_bytes_per_launch": alg[dname] * cells,
+            "phase_ms": dict(zip(names, [float(x) for x in ms])),
+            "step_frac": step_alg / (sum(ms) / 1e3) / 1e9 / peak}
+
+    line = {
+        "metric": "Mcell-layer-steps/s", "value": value, "unit": "Mcell-layer-steps/s",
+        "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64" if prec == OQG_FP64 else "f32+f64",
+        "data": "synthetic",
+        "config": {"workload": label, "nxp": b.nxp, "nyp": b.nyp, "nl": b.nl,
+                   "model_steps_per_step": msteps, "tdt_s": tdt,
+                   "l2": "flushed (256 MiB write) before every timed step",
+                   "parallelism": "replicas" if ws > 1 else "single basin"},
+        "roofline": roof,
+        "e2e": {"value": e2e_value, "unit": "Mcell-layer-steps/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h, "timer": "host clock",
+                "pattern": "per model step: upload wekp+ent, step, read p(:,:,1)"},
+        "gpu_launches": args.steps * msteps * 4,
+        "clocks": clk.summary(),
+        "variants": variants,
+    }
+    if rank == 0 and ws == 1 and args.cpu_seconds > 0:
+        from openqg_b200.params import OQG_FP64 as F64
+        b64, _, _ = make_basin(args.workload, F64)
+        v, n, el = cpu_sample(b64, p, w, ts, tn, tdt, args.cpu_seconds, 1)
+        line["cpu_baseline"] = {"value": v, "unit": "Mcell-layer-steps/s", "cores": 1, "kind": "port",
+                                "sample": "%d model steps of the same basin in %.1f s (FP64 C++ restatement "
+                                          "of the Fortran step_qg, 1 thread)" % (n, el)}
+    g.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="ocean513", choices=sorted(WORKLOADS))
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--model-steps", type=int, default=10)
+    ap.add_argument("--ref-model-steps", type=int, default=2)
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--no-variants", dest="variants", action="store_false")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

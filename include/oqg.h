@@ -171,6 +171,13 @@ int oqg_ekman_from_tau(const oqg_params *prm, const double *taux,
 int oqg_device_state(oqg_handle *h, void **p, void **pm, void **q, void **qm,
                      int *pitch, int *elem_bytes);
 
+/* Runs nsteps steps as separate launches with CUDA events between the four
+ * kernels of each step, on the handle's stream, and returns the mean device
+ * time per launch (ms) of each phase: ms[0] vorticity step + modal RHS,
+ * ms[1] forward x-transform, ms[2] y-solve + scalar phase, ms[3] inverse
+ * x-transform + assembly.  For measurement; the state advances normally. */
+int oqg_profile_phases(oqg_handle *h, double tdt, int nsteps, double *ms);
+
 /* CUDA stream of the handle (a cudaStream_t). */
 int oqg_stream(oqg_handle *h, void **stream);
 

@@ -1,0 +1,269 @@
+"""Host-side mirror of OpenQG's QG-core interface over the C ABI (include/oqg.h).
+
+The names follow the reference so a caller reads the same program:
+
+    qg = init_qg(basin)                     # qg.F90:60-103   init_qg
+    qg.set_state(p, pm)                     # init_pv + init_constraint + init_mass_constr
+    step_qg(tdt, ent, wekp, txis, txin, qg) # core.F90:16-33  one step
+    suppress_comp_mode(qg)                  # driver.F90:174-189
+
+Arrays are numpy FP64 with shape (nl, nyp, nxp) in C order, which is the
+memory layout of the reference's Fortran (nxp, nyp, nl) arrays.  Every call
+runs on the GPU through liboqg.so; there is no CPU fallback, and a missing
+library or device raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Optional
+
+import numpy as np
+
+from .params import Basin, STATUS
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "liboqg.so")
+_dp = ctypes.POINTER(ctypes.c_double)
+_lib = None
+
+
+class OqgError(RuntimeError):
+    def __init__(self, code: int, where: str, msg: str):
+        super().__init__("%s failed: %s (%s)" % (where, STATUS.get(code, code), msg))
+        self.code = code
+
+
+def lib():
+    """Loads liboqg.so (built by openqg_b200.build); raises if it is absent."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError("liboqg.so is not built; run `python -m openqg_b200.build`")
+    L = ctypes.CDLL(LIB_PATH)
+    vp = ctypes.c_void_p
+    L.oqg_last_error.restype = ctypes.c_char_p
+    L.oqg_version.argtypes = [ctypes.c_char_p, ctypes.c_int]
+    L.oqg_create.argtypes = [vp, ctypes.POINTER(vp)]
+    L.oqg_destroy.argtypes = [vp]
+    L.oqg_set_state.argtypes = [vp, _dp, _dp]
+    L.oqg_set_state_full.argtypes = [vp] + [_dp] * 10
+    L.oqg_get_state.argtypes = [vp, _dp, _dp, _dp, _dp]
+    L.oqg_get_p_layer.argtypes = [vp, ctypes.c_int, _dp]
+    L.oqg_get_constraints.argtypes = [vp] + [_dp] * 6
+    L.oqg_set_forcing.argtypes = [vp, _dp, _dp, ctypes.c_double, ctypes.c_double]
+    L.oqg_step.argtypes = [vp, ctypes.c_double, ctypes.c_int]
+    L.oqg_set_step_index.argtypes = [vp, ctypes.c_longlong]
+    L.oqg_get_step_index.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
+    L.oqg_suppress.argtypes = [vp]
+    L.oqg_sync.argtypes = [vp]
+    L.oqg_check_finite.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
+    L.oqg_diag.argtypes = [vp, _dp, _dp, _dp, _dp]
+    L.oqg_solve_inhomog.argtypes = [vp, ctypes.c_int, _dp, _dp]
+    L.oqg_generate_homog_soln.argtypes = [vp, ctypes.c_int, _dp, _dp]
+    L.oqg_get_modes.argtypes = [vp, _dp, _dp, _dp, _dp]
+    L.oqg_ekman_from_tau.argtypes = [vp, _dp, _dp, _dp, _dp, _dp]
+    L.oqg_device_state.argtypes = [vp] + [ctypes.POINTER(vp)] * 4 + [ctypes.POINTER(ctypes.c_int)] * 2
+    L.oqg_stream.argtypes = [vp, ctypes.POINTER(vp)]
+    L.oqg_profile_phases.argtypes = [vp, ctypes.c_double, ctypes.c_int, _dp]
+    _lib = L
+    return L
+
+
+def _check(rc: int, where: str):
+    if rc != 0:
+        raise OqgError(rc, where, lib().oqg_last_error().decode())
+
+
+def _p(a: Optional[np.ndarray]):
+    if a is None:
+        return None
+    return a.ctypes.data_as(_dp)
+
+
+def _f64(a, shape=None):
+    if a is None:
+        return None
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    if shape is not None and a.size != int(np.prod(shape)):
+        raise ValueError("expected %s values, got %d" % (shape, a.size))
+    return a
+
+
+def version() -> str:
+    buf = ctypes.create_string_buffer(256)
+    lib().oqg_version(buf, 256)
+    return buf.value.decode()
+
+
+class QG:
+    """Device-resident qg_type (qg.F90:17-53) of one basin."""
+
+    def __init__(self, basin: Basin):
+        self.b = basin
+        self._prm = basin.to_c()
+        h = ctypes.c_void_p()
+        _check(lib().oqg_create(ctypes.byref(self._prm), ctypes.byref(h)), "oqg_create")
+        self.h = h
+
+    # lifetime -------------------------------------------------------------
+    def close(self):
+        if getattr(self, "h", None):
+            lib().oqg_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # state ----------------------------------------------------------------
+    def set_state(self, p, pm):
+        """Restart semantics: q, qm and constraints recomputed from p, pm."""
+        p = _f64(p, self.b.shape3)
+        pm = _f64(pm, self.b.shape3)
+        _check(lib().oqg_set_state(self.h, _p(p), _p(pm)), "oqg_set_state")
+
+    def set_state_full(self, p, pm, q, qm, dpi, dpip, cs=None, cn=None, csp=None, cnp=None):
+        arrs = [_f64(a) for a in (p, pm, q, qm, dpi, dpip, cs, cn, csp, cnp)]
+        _check(lib().oqg_set_state_full(self.h, *[_p(a) for a in arrs]), "oqg_set_state_full")
+
+    def get_state(self):
+        sh = self.b.shape3
+        p, pm, q, qm = (np.empty(sh) for _ in range(4))
+        _check(lib().oqg_get_state(self.h, _p(p), _p(pm), _p(q), _p(qm)), "oqg_get_state")
+        return p, pm, q, qm
+
+    @property
+    def p(self):
+        out = np.empty(self.b.shape3)
+        _check(lib().oqg_get_state(self.h, _p(out), None, None, None), "oqg_get_state")
+        return out
+
+    def p_layer(self, k: int = 0, out: Optional[np.ndarray] = None):
+        if out is None:
+            out = np.empty(self.b.shape2)
+        _check(lib().oqg_get_p_layer(self.h, k, _p(out)), "oqg_get_p_layer")
+        return out
+
+    def constraints(self):
+        nl = self.b.nl
+        dpi, dpip = np.empty(nl - 1), np.empty(nl - 1)
+        cs, cn, csp, cnp = (np.empty(nl) for _ in range(4))
+        _check(lib().oqg_get_constraints(self.h, _p(dpi), _p(dpip), _p(cs), _p(cn), _p(csp), _p(cnp)),
+               "oqg_get_constraints")
+        return dict(dpi=dpi, dpip=dpip, cs=cs, cn=cn, csp=csp, cnp=cnp)
+
+    # forcing and stepping ------------------------------------------------------
+    def set_forcing(self, wekp=None, ent=None, txis=0.0, txin=0.0):
+        w = _f64(wekp, self.b.shape2)
+        e = _f64(ent, (self.b.nl - 1,) + self.b.shape2)
+        _check(lib().oqg_set_forcing(self.h, _p(w), _p(e), float(txis), float(txin)), "oqg_set_forcing")
+
+    def step(self, tdt: float, nsteps: int = 1):
+        _check(lib().oqg_step(self.h, float(tdt), int(nsteps)), "oqg_step")
+
+    def set_step_index(self, steps_done: int):
+        _check(lib().oqg_set_step_index(self.h, int(steps_done)), "oqg_set_step_index")
+
+    def step_index(self) -> int:
+        v = ctypes.c_longlong()
+        _check(lib().oqg_get_step_index(self.h, ctypes.byref(v)), "oqg_get_step_index")
+        return v.value
+
+    def suppress(self):
+        _check(lib().oqg_suppress(self.h), "oqg_suppress")
+
+    def sync(self):
+        _check(lib().oqg_sync(self.h), "oqg_sync")
+
+    def check_finite(self) -> int:
+        v = ctypes.c_longlong()
+        rc = lib().oqg_check_finite(self.h, ctypes.byref(v))
+        if rc not in (0, 3):
+            _check(rc, "oqg_check_finite")
+        return v.value
+
+    def diag(self):
+        nl = self.b.nl
+        e, smin, smax, c = (np.empty(nl) for _ in range(4))
+        _check(lib().oqg_diag(self.h, _p(e), _p(smin), _p(smax), _p(c)), "oqg_diag")
+        return dict(ekei=e, sfmin=smin, sfmax=smax, circ=c)
+
+    # pieces of the path -----------------------------------------------------------
+    def solve_inhomog_eqn(self, m: int, rhs):
+        """solve_inhomog_eqn (inhomog.F90:156-168) for mode m (1-based)."""
+        rhs = _f64(rhs, self.b.shape2)
+        out = np.empty(self.b.shape2)
+        _check(lib().oqg_solve_inhomog(self.h, int(m), _p(rhs), _p(out)), "oqg_solve_inhomog")
+        return out
+
+    def generate_homog_soln(self, m: int, L):
+        L = _f64(L, self.b.shape2)
+        out = np.empty(self.b.shape2)
+        _check(lib().oqg_generate_homog_soln(self.h, int(m), _p(L), _p(out)), "oqg_generate_homog_soln")
+        return out
+
+    def modes(self):
+        nl = self.b.nl
+        amat, ctl2m, ctm2l = (np.empty(nl * nl) for _ in range(3))
+        rdm2 = np.empty(nl)
+        _check(lib().oqg_get_modes(self.h, _p(amat), _p(rdm2), _p(ctl2m), _p(ctm2l)), "oqg_get_modes")
+        f = lambda a: a.reshape(nl, nl).T.copy()
+        return dict(amat=f(amat), rdm2=rdm2, ctl2m=f(ctl2m), ctm2l=f(ctm2l))
+
+    def device_state(self):
+        """(p, pm, q, qm) device pointers, row pitch (elements), element bytes."""
+        ptr = [ctypes.c_void_p() for _ in range(4)]
+        pitch, eb = ctypes.c_int(), ctypes.c_int()
+        _check(lib().oqg_device_state(self.h, *[ctypes.byref(x) for x in ptr],
+                                      ctypes.byref(pitch), ctypes.byref(eb)), "oqg_device_state")
+        return [x.value for x in ptr], pitch.value, eb.value
+
+    def profile_phases(self, tdt: float, nsteps: int):
+        """Mean device ms per launch of the four phases of a step."""
+        ms = np.zeros(4)
+        _check(lib().oqg_profile_phases(self.h, float(tdt), int(nsteps), _p(ms)), "oqg_profile_phases")
+        return ms
+
+    def stream(self) -> int:
+        s = ctypes.c_void_p()
+        _check(lib().oqg_stream(self.h, ctypes.byref(s)), "oqg_stream")
+        return s.value or 0
+
+
+def init_qg(basin: Basin) -> QG:
+    """init_qg (qg.F90:60-103): modes, Helmholtz tables, homogeneous solutions."""
+    return QG(basin)
+
+
+def step_qg(tdt: float, ent, wekp, txis: float, txin: float, qg: QG):
+    """step_qg (core.F90:16-33): one QG step with the given forcing."""
+    qg.set_forcing(wekp, ent, txis, txin)
+    qg.step(tdt, 1)
+
+
+def suppress_comp_mode(qg: QG):
+    """suppress_comp_mode (driver.F90:174-189)."""
+    qg.suppress()
+
+
+def ekman_from_tau(basin: Basin, taux, tauy):
+    """ekman_from_tau (ekman.F90:53-83): (wekp, txis, txin) of a stress field."""
+    prm = basin.to_c()
+    taux = _f64(taux, basin.shape2)
+    tauy = _f64(tauy, basin.shape2)
+    w = np.empty(basin.shape2)
+    ts, tn = ctypes.c_double(0.0), ctypes.c_double(0.0)
+    _check(lib().oqg_ekman_from_tau(ctypes.byref(prm), _p(taux), _p(tauy), _p(w),
+                                    ctypes.cast(ctypes.byref(ts), _dp),
+                                    ctypes.cast(ctypes.byref(tn), _dp)), "oqg_ekman_from_tau")
+    return w, ts.value, tn.value

@@ -1,0 +1,929 @@
+// oqg_capi.cu -- the C ABI of include/oqg.h: handles, device memory, launches.
+//
+// A handle is one basin on one device with its own stream.  oqg_step queues
+// step_qg (qg/core.F90:16-33) as four kernels per step; pairs of steps are
+// captured once into a CUDA graph (the parity of the p/q buffers returns after
+// two steps) and replayed.
+#include "../../include/oqg.h"
+#include "oqg_dev.cuh"
+#include "oqg_kernels.cuh"
+#include "oqg_setup.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+using namespace oqg;
+
+static thread_local std::string g_err;
+
+static int fail(int code, const std::string &msg) {
+    g_err = msg;
+    return code;
+}
+
+#define CK(x)                                                                                  \
+    do {                                                                                       \
+        cudaError_t e_ = (x);                                                                  \
+        if (e_ != cudaSuccess) return fail(OQG_ECUDA, std::string(#x) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+static inline int rup(int v, int m) { return (v + m - 1) / m * m; }
+
+struct oqg_handle {
+    int dev = 0;
+    cudaStream_t st = nullptr;
+    oqg_params prm{};
+    bool mixed = false;
+    size_t esz = 8;
+    BasinDev hb{}, hb64{};
+    BasinDev *d_bas = nullptr, *d_bas64 = nullptr;
+    std::vector<void *> allocs;
+    Work *d_wv = nullptr, *d_wx = nullptr, *d_wy = nullptr, *d_wi = nullptr;
+    int nv = 0, nx = 0, nys = 0, ni = 0;
+    int E = 8, KB = 16;
+    size_t smem_v = 0, smem_x = 0, smem_x64 = 0, smem_y = 0, smem_i = 0, smem_i64 = 0;
+    double *stage[2] = {nullptr, nullptr};
+    unsigned long long *d_bad = nullptr;
+    double *d_diag = nullptr;
+    void *ent_buf = nullptr;
+    int par = 0;
+    cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+    double g_tdt[2] = {0.0, 0.0};
+    std::vector<double> modes_amat, modes_ctl2m, modes_ctm2l, modes_rdm2;
+};
+
+template <class X>
+static X *dalloc(oqg_handle *h, size_t count) {
+    void *p = nullptr;
+    if (cudaMalloc(&p, count * sizeof(X) + 16) != cudaSuccess) return nullptr;
+    cudaMemset(p, 0, count * sizeof(X) + 16);
+    h->allocs.push_back(p);
+    return (X *)p;
+}
+
+// ----------------------------------------------------------- launch helpers
+static const int XTHREADS = 256;
+
+template <class T, int NL, int E>
+static void launch_step_t(oqg_handle *h, int par, double tdt) {
+    const BasinDev &b = h->hb;
+    k_vort<T, NL><<<h->nv, VTHREADS, h->smem_v, h->st>>>(h->d_bas, h->d_wv, par, tdt);
+    k_xfwd<T, E><<<h->nx, XTHREADS, h->smem_x, h->st>>>(h->d_bas, h->d_wx, nullptr);
+    if (b.cyclic)
+        k_ysolve<T, true, NL><<<h->nys, 32 * h->KB, h->smem_y, h->st>>>(h->d_bas, h->d_wy, tdt, 1);
+    else
+        k_ysolve<T, false, NL><<<h->nys, 32 * h->KB, h->smem_y, h->st>>>(h->d_bas, h->d_wy, tdt, 1);
+    k_xinv<T, E, NL><<<h->ni, XTHREADS, h->smem_i, h->st>>>(h->d_bas, h->d_wi, par, nullptr);
+}
+
+// FP64 solve of the modal Helmholtz problems with the rhs buffer as input;
+// modal solutions into out ([nl][nyp][px] FP64).
+template <int NL, int E>
+static void launch_solve_t(oqg_handle *h, double *out) {
+    k_xfwd<double, E><<<h->nx, XTHREADS, h->smem_x64, h->st>>>(h->d_bas64, h->d_wx, nullptr);
+    if (h->hb.cyclic)
+        k_ysolve<double, true, NL><<<h->nys, 32 * h->KB, h->smem_y, h->st>>>(h->d_bas64, h->d_wy, 0.0, 0);
+    else
+        k_ysolve<double, false, NL><<<h->nys, 32 * h->KB, h->smem_y, h->st>>>(h->d_bas64, h->d_wy, 0.0, 0);
+    k_xinv<double, E, NL><<<h->ni, XTHREADS, h->smem_i64, h->st>>>(h->d_bas64, h->d_wi, 0, out);
+}
+
+template <class T, int NL, int E>
+static void set_attrs_t(oqg_handle *h) {
+    cudaFuncSetAttribute(k_vort<T, NL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->smem_v);
+    cudaFuncSetAttribute(k_xfwd<T, E>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->smem_x);
+    cudaFuncSetAttribute(k_ysolve<T, true, NL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->smem_y);
+    cudaFuncSetAttribute(k_ysolve<T, false, NL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->smem_y);
+    cudaFuncSetAttribute(k_xinv<T, E, NL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->smem_i);
+    cudaFuncSetAttribute(k_xfwd<double, E>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->smem_x64);
+    cudaFuncSetAttribute(k_ysolve<double, true, NL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->smem_y);
+    cudaFuncSetAttribute(k_ysolve<double, false, NL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->smem_y);
+    cudaFuncSetAttribute(k_xinv<double, E, NL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->smem_i64);
+}
+
+// dispatch over (T, NL, E)
+#define OQG_DISPATCH(FN, h, ...)                                                      \
+    do {                                                                              \
+        const int nl_ = (h)->hb.nl, e_ = (h)->E;                                      \
+        if ((h)->mixed) {                                                             \
+            if (nl_ == 2) { if (e_ == 8) FN<float, 2, 8>(__VA_ARGS__); else FN<float, 2, 16>(__VA_ARGS__); } \
+            else if (nl_ == 3) { if (e_ == 8) FN<float, 3, 8>(__VA_ARGS__); else FN<float, 3, 16>(__VA_ARGS__); } \
+            else { if (e_ == 8) FN<float, 4, 8>(__VA_ARGS__); else FN<float, 4, 16>(__VA_ARGS__); } \
+        } else {                                                                      \
+            if (nl_ == 2) { if (e_ == 8) FN<double, 2, 8>(__VA_ARGS__); else FN<double, 2, 16>(__VA_ARGS__); } \
+            else if (nl_ == 3) { if (e_ == 8) FN<double, 3, 8>(__VA_ARGS__); else FN<double, 3, 16>(__VA_ARGS__); } \
+            else { if (e_ == 8) FN<double, 4, 8>(__VA_ARGS__); else FN<double, 4, 16>(__VA_ARGS__); } \
+        }                                                                             \
+    } while (0)
+
+static void launch_step(oqg_handle *h, int par, double tdt) { OQG_DISPATCH(launch_step_t, h, h, par, tdt); }
+static void set_attrs(oqg_handle *h) { OQG_DISPATCH(set_attrs_t, h, h); }
+
+static void launch_solve(oqg_handle *h, double *out) {
+    const int nl = h->hb.nl;
+    if (nl == 2) { if (h->E == 8) launch_solve_t<2, 8>(h, out); else launch_solve_t<2, 16>(h, out); }
+    else if (nl == 3) { if (h->E == 8) launch_solve_t<3, 8>(h, out); else launch_solve_t<3, 16>(h, out); }
+    else { if (h->E == 8) launch_solve_t<4, 8>(h, out); else launch_solve_t<4, 16>(h, out); }
+}
+
+#define OQG_NL_T(FN, h, ...)                                                                   \
+    do {                                                                                       \
+        const int nl_ = (h)->hb.nl;                                                            \
+        if ((h)->mixed) { if (nl_ == 2) FN<float, 2>(__VA_ARGS__); else if (nl_ == 3) FN<float, 3>(__VA_ARGS__); else FN<float, 4>(__VA_ARGS__); } \
+        else { if (nl_ == 2) FN<double, 2>(__VA_ARGS__); else if (nl_ == 3) FN<double, 3>(__VA_ARGS__); else FN<double, 4>(__VA_ARGS__); } \
+    } while (0)
+
+template <class T, int NL>
+static void launch_qcomp_t(oqg_handle *h, const double *p, void *q) {
+    k_qcomp<T, NL><<<296, 256, 0, h->st>>>(h->d_bas, 0, p, (T *)q);
+}
+template <class T, int NL>
+static void launch_initc_t(oqg_handle *h, int par) {
+    k_init_constraints<T, NL><<<1, 512, 0, h->st>>>(h->d_bas, 0, par);
+}
+
+// ----------------------------------------------------------- host copies
+// host (nxp, nyp, nl) Fortran order <-> device staging [nl][nyp][px] FP64
+static int upload3(oqg_handle *h, const double *src, double *dst, int nlay) {
+    const BasinDev &b = h->hb;
+    CK(cudaMemcpy2DAsync(dst, b.px * sizeof(double), src, b.nxp * sizeof(double),
+                         b.nxp * sizeof(double), (size_t)b.nyp * nlay, cudaMemcpyHostToDevice, h->st));
+    return OQG_OK;
+}
+static int download3(oqg_handle *h, const double *src, double *dst, int nlay) {
+    const BasinDev &b = h->hb;
+    CK(cudaMemcpy2DAsync(dst, b.nxp * sizeof(double), src, b.px * sizeof(double),
+                         b.nxp * sizeof(double), (size_t)b.nyp * nlay, cudaMemcpyDeviceToHost, h->st));
+    return OQG_OK;
+}
+// staging FP64 -> field of the storage type
+static void stage_to_field(oqg_handle *h, const double *s, void *f, size_t n) {
+    if (h->mixed) k_cvt_in<float><<<296, 256, 0, h->st>>>(s, (float *)f, n);
+    else cudaMemcpyAsync(f, s, n * sizeof(double), cudaMemcpyDeviceToDevice, h->st);
+}
+static void field_to_stage(oqg_handle *h, const void *f, double *s, size_t n) {
+    if (h->mixed) k_cvt_out<float><<<296, 256, 0, h->st>>>((const float *)f, s, n);
+    else cudaMemcpyAsync(s, f, n * sizeof(double), cudaMemcpyDeviceToDevice, h->st);
+}
+
+static int push_desc(oqg_handle *h) {
+    CK(cudaMemcpyAsync(h->d_bas, &h->hb, sizeof(BasinDev), cudaMemcpyHostToDevice, h->st));
+    CK(cudaMemcpyAsync(h->d_bas64, &h->hb64, sizeof(BasinDev), cudaMemcpyHostToDevice, h->st));
+    return OQG_OK;
+}
+
+static void drop_graphs(oqg_handle *h) {
+    for (int i = 0; i < 2; ++i)
+        if (h->gexec[i]) { cudaGraphExecDestroy(h->gexec[i]); h->gexec[i] = nullptr; }
+}
+
+// Solve (Del^2 - rdm2_m) s_m = f for every mode m with f the (FP64, staging 0)
+// field; modal solutions into staging 1.  Synchronous.
+static int solve_all_modes(oqg_handle *h) {
+    const BasinDev &b = h->hb;
+    k_rhs_from_field<double><<<296, 256, 0, h->st>>>(h->d_bas64, 0, h->stage[0], (double *)b.rhs);
+    launch_solve(h, h->stage[1]);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(h->st));
+    return OQG_OK;
+}
+
+// ----------------------------------------------------------- homogeneous solutions
+// homsol_box (homog.F90:214-278) and homsol_cyclic (homog.F90:128-212); the
+// Helmholtz solves run on the device.
+static int homsol(oqg_handle *h) {
+    BasinDev &b = h->hb;
+    const int nxp = b.nxp, nyp = b.nyp, nl = b.nl, px = b.px;
+    const size_t n2 = (size_t)nyp * px;
+    std::vector<double> L(n2 * nl, 0.0), sol(n2 * nl);
+    auto solve = [&](const std::vector<double> &f) -> int {
+        CK(cudaMemcpyAsync(h->stage[0], f.data(), n2 * sizeof(double), cudaMemcpyHostToDevice, h->st));
+        int rc = solve_all_modes(h);
+        if (rc) return rc;
+        CK(cudaMemcpy(sol.data(), h->stage[1], n2 * nl * sizeof(double), cudaMemcpyDeviceToHost));
+        return OQG_OK;
+    };
+    const double xl = (nxp - 1) * b.dx, yl = (nyp - 1) * b.dy;
+    if (!b.cyclic) {
+        std::fill(L.begin(), L.begin() + n2, 1.0);
+        int rc = solve(L);
+        if (rc) return rc;
+        std::vector<double> hsb((size_t)(nl - 1) * n2, 0.0), aipohs(nl, 0.0);
+        for (int m = 1; m < nl; ++m) {
+            double *H = &hsb[(m - 1) * n2];
+            for (size_t x = 0; x < n2; ++x) H[x] = L[x] + b.rdm2[m] * sol[m * n2 + x];
+            // int_P_dA (numerics.F90:188-204)
+            double s = 0.0;
+            for (int j = 0; j < nyp; ++j)
+                for (int i = 0; i < nxp; ++i) {
+                    double w = ((i == 0 || i == nxp - 1) ? 0.5 : 1.0) * ((j == 0 || j == nyp - 1) ? 0.5 : 1.0);
+                    s += w * H[(size_t)j * px + i];
+                }
+            aipohs[m] = s * b.dx * b.dy;
+        }
+        const int n = nl - 1;
+        for (int k = 0; k < n; ++k)
+            for (int m = 1; m < nl; ++m)
+                b.cdhoc[k + n * (m - 1)] = (b.ctm2l[m + nl * (k + 1)] - b.ctm2l[m + nl * k]) * aipohs[m];
+        if (!lu_factor(n, b.cdhoc, b.lu, b.piv)) return fail(OQG_ESETUP, "Problem in DGETRF: singular cdhoc");
+        void *dst = const_cast<void *>(b.hsb);
+        if (h->mixed) {
+            std::vector<float> f(hsb.size());
+            for (size_t x = 0; x < f.size(); ++x) f[x] = (float)hsb[x];
+            CK(cudaMemcpy(dst, f.data(), f.size() * sizeof(float), cudaMemcpyHostToDevice));
+        } else {
+            CK(cudaMemcpy(dst, hsb.data(), hsb.size() * sizeof(double), cudaMemcpyHostToDevice));
+        }
+    } else {
+        std::vector<double> hbt(nyp), hbc1((size_t)nl * nyp, 0.0), hbc2((size_t)nl * nyp, 0.0);
+        for (int j = 1; j <= nyp; ++j) hbt[j - 1] = double(nyp - j) / double(nyp - 1);
+        b.hbsi = yl / xl;
+        for (int pass = 0; pass < 2; ++pass) {
+            std::fill(L.begin(), L.end(), 0.0);
+            for (int j = 0; j < nyp; ++j) {
+                double ypj = j * b.dy, ypn = (nyp - 1) * b.dy;
+                double v = pass == 0 ? (ypn - ypj) / yl : (ypj - 0.0) / yl;
+                for (int i = 0; i < nxp; ++i) L[(size_t)j * px + i] = v;
+            }
+            int rc = solve(L);
+            if (rc) return rc;
+            std::vector<double> &dst = pass == 0 ? hbc1 : hbc2;
+            for (int m = 1; m < nl; ++m)
+                for (int j = 0; j < nyp; ++j)
+                    dst[(size_t)m * nyp + j] = L[(size_t)j * px] + b.rdm2[m] * sol[m * n2 + (size_t)j * px];
+        }
+        for (int m = 1; m < nl; ++m) {
+            const double *h1 = &hbc1[(size_t)m * nyp], *h2 = &hbc2[(size_t)m * nyp];
+            double p1s = -xl * (h1[1] - h1[0]) / b.dy, p2s = -xl * (h2[1] - h2[0]) / b.dy;
+            double p1n = xl * (h1[nyp - 1] - h1[nyp - 2]) / b.dy, p2n = xl * (h2[nyp - 1] - h2[nyp - 2]) / b.dy;
+            p1s = p1s + 0.5 * b.dy * b.rdm2[m] * h1[0] * xl;
+            p2s = p2s + 0.5 * b.dy * b.rdm2[m] * h2[0] * xl;
+            p1n = p1n + 0.5 * b.dy * b.rdm2[m] * h1[nyp - 1] * xl;
+            p2n = p2n + 0.5 * b.dy * b.rdm2[m] * h2[nyp - 1] * xl;
+            double det = p1s * p2n - p2s * p1n;
+            b.hc1s[m] = p1s / det;
+            b.hc2s[m] = p2s / det;
+            b.hc1n[m] = p1n / det;
+            b.hc2n[m] = p2n / det;
+        }
+        CK(cudaMemcpy(const_cast<double *>(b.hbt), hbt.data(), nyp * sizeof(double), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(const_cast<double *>(b.hbc1), hbc1.data(), hbc1.size() * sizeof(double), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(const_cast<double *>(b.hbc2), hbc2.data(), hbc2.size() * sizeof(double), cudaMemcpyHostToDevice));
+    }
+    // the FP64 solve descriptor shares the constants
+    std::memcpy(h->hb64.cdhoc, b.cdhoc, sizeof b.cdhoc);
+    std::memcpy(h->hb64.lu, b.lu, sizeof b.lu);
+    std::memcpy(h->hb64.piv, b.piv, sizeof b.piv);
+    std::memcpy(h->hb64.hc1s, b.hc1s, sizeof b.hc1s);
+    std::memcpy(h->hb64.hc2s, b.hc2s, sizeof b.hc2s);
+    std::memcpy(h->hb64.hc1n, b.hc1n, sizeof b.hc1n);
+    std::memcpy(h->hb64.hc2n, b.hc2n, sizeof b.hc2n);
+    h->hb64.hbsi = b.hbsi;
+    return OQG_OK;
+}
+
+static void destroy_all(oqg_handle *h) {
+    if (!h) return;
+    drop_graphs(h);
+    if (h->st) cudaStreamSynchronize(h->st);
+    for (void *p : h->allocs) cudaFree(p);
+    if (h->st) cudaStreamDestroy(h->st);
+    delete h;
+}
+
+template <class T, int NL, int E>
+static void launch_phase_t(oqg_handle *h, int phase, int par, double tdt) {
+    const BasinDev &b = h->hb;
+    switch (phase) {
+        case 0: k_vort<T, NL><<<h->nv, VTHREADS, h->smem_v, h->st>>>(h->d_bas, h->d_wv, par, tdt); break;
+        case 1: k_xfwd<T, E><<<h->nx, XTHREADS, h->smem_x, h->st>>>(h->d_bas, h->d_wx, nullptr); break;
+        case 2:
+            if (b.cyclic)
+                k_ysolve<T, true, NL><<<h->nys, 32 * h->KB, h->smem_y, h->st>>>(h->d_bas, h->d_wy, tdt, 1);
+            else
+                k_ysolve<T, false, NL><<<h->nys, 32 * h->KB, h->smem_y, h->st>>>(h->d_bas, h->d_wy, tdt, 1);
+            break;
+        default: k_xinv<T, E, NL><<<h->ni, XTHREADS, h->smem_i, h->st>>>(h->d_bas, h->d_wi, par, nullptr); break;
+    }
+}
+static void launch_phase(oqg_handle *h, int phase, int par, double tdt) {
+    OQG_DISPATCH(launch_phase_t, h, h, phase, par, tdt);
+}
+
+extern "C" {
+
+const char *oqg_last_error(void) { return g_err.c_str(); }
+
+int oqg_version(char *buf, int buflen) {
+    int dev = 0, n = 0;
+    cudaDeviceProp pr{};
+    std::string s = "openqg_b200 (sm_100a)";
+    if (cudaGetDeviceCount(&n) == cudaSuccess && n > 0 && cudaGetDevice(&dev) == cudaSuccess &&
+        cudaGetDeviceProperties(&pr, dev) == cudaSuccess)
+        s += std::string("; device ") + pr.name;
+    else
+        s += "; no device";
+    if (buf && buflen > 0) {
+        std::strncpy(buf, s.c_str(), buflen - 1);
+        buf[buflen - 1] = 0;
+    }
+    return OQG_OK;
+}
+
+int oqg_create(const oqg_params *prm, oqg_handle **out) {
+    if (!prm || !out) return fail(OQG_EINVAL, "null argument");
+    *out = nullptr;
+    const oqg_params &P = *prm;
+    if (P.nl < 2 || P.nl > 4) return fail(OQG_EUNSUPPORTED, "this build handles nl in [2, 4]");
+    if (P.nxp < 5 || P.nyp < 5) return fail(OQG_EINVAL, "grid too small (nxp, nyp >= 5)");
+    if (!(P.dx > 0) || !(P.dy > 0) || P.fnot == 0.0) return fail(OQG_EINVAL, "bad dx, dy or fnot");
+    if (P.k_topo < 1 || P.k_topo > P.nl) return fail(OQG_EINVAL, "k_topo out of range");
+    for (int k = 0; k < P.nl; ++k)
+        if (!(P.h[k] > 0)) return fail(OQG_EINVAL, "layer thickness must be > 0");
+    for (int k = 0; k < P.nl - 1; ++k)
+        if (!(P.gp[k] > 0)) return fail(OQG_EINVAL, "reduced gravity must be > 0");
+    if (P.precision != OQG_FP64 && P.precision != OQG_MIXED) return fail(OQG_EINVAL, "bad precision");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(OQG_ENODEV, "no CUDA device");
+
+    oqg_handle *h = new oqg_handle();
+    h->prm = P;
+    h->prm.ddyn = nullptr;
+    h->mixed = P.precision == OQG_MIXED;
+    h->esz = h->mixed ? 4 : 8;
+    cudaGetDevice(&h->dev);
+    if (cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking) != cudaSuccess) {
+        delete h;
+        return fail(OQG_ECUDA, "cudaStreamCreate failed");
+    }
+    auto bail = [&](int code, const std::string &msg) {
+        destroy_all(h);
+        return fail(code, msg);
+    };
+
+    // ---- init-time tables (qg.F90:60-103)
+    Modes md;
+    std::string err;
+    if (!setup_modes(P.nl, P.h, P.gp, P.fnot, md, err)) return bail(OQG_ESETUP, err);
+    h->modes_amat = md.amat; h->modes_ctl2m = md.ctl2m; h->modes_ctm2l = md.ctm2l; h->modes_rdm2 = md.rdm2;
+
+    BasinDev &b = h->hb;
+    b.nxp = P.nxp; b.nyp = P.nyp; b.nl = P.nl; b.cyclic = P.cyclic ? 1 : 0;
+    b.px = rup(P.nxp, 32);
+    b.ny = P.nyp - 2;
+    if (b.cyclic) { b.nxin = P.nxp - 1; b.M = P.nxp - 1; b.nk = b.M / 2 + 1; }
+    else { b.nxin = P.nxp - 2; b.M = 2 * (P.nxp - 1); b.nk = P.nxp - 2; }
+    std::vector<int> rad;
+    if (!fft_radices(b.M, rad) || (int)rad.size() > OQG_MAXRAD)
+        return bail(OQG_EUNSUPPORTED, "x-transform length must factor into 2, 3 and 5");
+    if (b.M > 4096) return bail(OQG_EUNSUPPORTED, "x-transform length above 4096");
+    b.nrad = (int)rad.size();
+    for (int i = 0; i < b.nrad; ++i) b.rad[i] = rad[i];
+    b.pr = rup(b.nxin, 32);
+    b.pk = rup(b.nk, 32);
+    b.tiles_x = (P.nxp + VTX - 1) / VTX;
+    b.tiles_y = (P.nyp + VTY - 1) / VTY;
+    b.kt = P.k_topo - 1;
+    b.dz_sign = P.dz_sign; b.tau_sign = P.tau_sign;
+    b.suppress_period = P.suppress_period;
+    b.dx = P.dx; b.dy = P.dy; b.fnot = P.fnot; b.beta = P.beta;
+    b.fx = 1.0 / (P.dx * P.dx);
+    b.fy = 1.0 / (P.dy * P.dy);
+    b.fx_bc = b.fx * P.bcco / (0.5 * P.bcco + 1.0);
+    b.fy_bc = b.fy * P.bcco / (0.5 * P.bcco + 1.0);
+    b.bc_half1 = 0.5 * P.bcco + 1.0;
+    b.jac_fac = 1.0 / (3.0 * (2.0 * P.dx) * (2.0 * P.dy) * P.fnot);
+    b.qb_fac = P.bcco * (1.0 / (P.dx * P.dx)) / (0.5 * P.bcco + 1.0) / P.fnot;
+    for (int k = 0; k < P.nl; ++k) {
+        b.c2[k] = P.ah2[k] / P.fnot;
+        b.c4[k] = P.ah4[k] / P.fnot;
+        b.h[k] = P.h[k]; b.ah2[k] = P.ah2[k]; b.ah4[k] = P.ah4[k];
+    }
+    for (int k = 0; k < P.nl - 1; ++k) b.gp[k] = P.gp[k];
+    const double foh0 = P.fnot / P.h[0], foh1 = P.fnot / P.h[1], foht = P.fnot / P.h[b.kt];
+    b.c_ent1 = P.dz_sign * foh0;
+    b.c_wind = P.tau_sign * foh0;
+    b.c_ent2 = P.dz_sign * foh1;
+    b.c_drag = foht * P.delek / (2.0 * std::fabs(P.fnot));
+    b.delek = P.delek;
+    std::copy(md.amat.begin(), md.amat.end(), b.amat);
+    std::copy(md.ctl2m.begin(), md.ctl2m.end(), b.ctl2m);
+    std::copy(md.ctm2l.begin(), md.ctm2l.end(), b.ctm2l);
+    std::copy(md.rdm2.begin(), md.rdm2.end(), b.rdm2);
+    PivotTable pt;
+    setup_pivots(b.cyclic, P.nxp, P.nyp, P.dx, P.dy, md.rdm2, pt, b.a_tri);
+    b.ftnorm = 1.0 / (double)(b.cyclic ? b.M : 2 * (b.nxin + 1));
+
+    // ---- device memory
+    const size_t n2 = (size_t)b.nyp * b.px, n3 = n2 * b.nl;
+    for (int i = 0; i < 4; ++i) {
+        b.F[i] = dalloc<char>(h, n3 * h->esz);
+        if (!b.F[i]) return bail(OQG_ECUDA, "out of device memory");
+    }
+    b.wekp = dalloc<char>(h, n2 * h->esz);
+    std::vector<double> yp(b.nyp);
+    const double yl = (b.nyp - 1) * b.dy;
+    for (int j = 0; j < b.nyp; ++j) yp[j] = -0.5 * yl + j * b.dy;
+    double *d_yp = dalloc<double>(h, b.nyp);
+    b.yprel = d_yp;
+    b.topo_active = 0;
+    b.ddyn = nullptr;
+    if (P.ddyn) {
+        double *d_dd = dalloc<double>(h, n2);
+        if (!d_dd) return bail(OQG_ECUDA, "out of device memory");
+        CK(cudaMemcpy2D(d_dd, b.px * sizeof(double), P.ddyn, P.nxp * sizeof(double), P.nxp * sizeof(double),
+                        P.nyp, cudaMemcpyHostToDevice));
+        b.ddyn = d_dd;
+        b.topo_active = 1;
+    }
+    b.rhs = dalloc<double>(h, (size_t)b.nl * b.ny * b.pr);
+    b.spec = dalloc<double>(h, (size_t)b.nl * b.ny * b.pk * (b.cyclic ? 2 : 1));
+    std::vector<double> tw;
+    fft_twiddles(b.M, tw);
+    double *d_tw64 = dalloc<double>(h, tw.size());
+    void *d_tw = d_tw64;
+    if (h->mixed) {
+        float *d_tw32 = dalloc<float>(h, tw.size());
+        std::vector<float> tf(tw.begin(), tw.end());
+        CK(cudaMemcpy(d_tw32, tf.data(), tf.size() * sizeof(float), cudaMemcpyHostToDevice));
+        d_tw = d_tw32;
+    }
+    CK(cudaMemcpy(d_tw64, tw.data(), tw.size() * sizeof(double), cudaMemcpyHostToDevice));
+    b.tw = d_tw;
+    double *d_pt = dalloc<double>(h, pt.tab.size());
+    int *d_po = dalloc<int>(h, pt.off.size()), *d_pl = dalloc<int>(h, pt.len.size());
+    CK(cudaMemcpy(d_pt, pt.tab.data(), pt.tab.size() * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d_po, pt.off.data(), pt.off.size() * sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d_pl, pt.len.data(), pt.len.size() * sizeof(int), cudaMemcpyHostToDevice));
+    b.piv_tab = d_pt; b.piv_off = d_po; b.piv_len = d_pl;
+    if (!b.cyclic) {
+        std::vector<double> dw;
+        dst_row_sums(b.nk, dw);
+        double *d_dw = dalloc<double>(h, dw.size());
+        CK(cudaMemcpy(d_dw, dw.data(), dw.size() * sizeof(double), cudaMemcpyHostToDevice));
+        b.dst_w = d_dw;
+        b.hsb = dalloc<char>(h, (size_t)(b.nl - 1) * n2 * h->esz);
+    } else {
+        b.hbt = dalloc<double>(h, b.nyp);
+        b.hbc1 = dalloc<double>(h, (size_t)b.nl * b.nyp);
+        b.hbc2 = dalloc<double>(h, (size_t)b.nl * b.nyp);
+    }
+    b.part_tile = dalloc<double>(h, (size_t)b.tiles_x * b.tiles_y * b.nl * OQG_NQ);
+    b.part_col = dalloc<double>(h, (size_t)b.nl * b.nk);
+    b.sc = dalloc<DevScalars>(h, 1);
+    h->stage[0] = dalloc<double>(h, n3);
+    h->stage[1] = dalloc<double>(h, n3);
+    h->d_bad = dalloc<unsigned long long>(h, 1);
+    h->d_diag = dalloc<double>(h, 4 * (size_t)b.nl);
+    if (!b.sc || !h->stage[1] || !h->d_diag) return bail(OQG_ECUDA, "out of device memory");
+    CK(cudaMemcpy(d_yp, yp.data(), yp.size() * sizeof(double), cudaMemcpyHostToDevice));
+
+    // ---- launch geometry
+    h->E = b.M <= 2048 ? 8 : 16;
+    const int TT = (b.M + h->E - 1) / h->E, G = std::max(1, XTHREADS / TT);
+    const size_t t2 = 2 * h->esz;
+    const int npm = (b.ny + 1) / 2;
+    h->nv = b.tiles_x * b.tiles_y;
+    h->nx = (b.nl * npm + G - 1) / G;
+    const size_t vsz = (size_t)(b.cyclic ? 16 : 8);
+    h->KB = 16;
+    while (h->KB > 2 && (size_t)b.ny * h->KB * vsz > 100 * 1024) h->KB /= 2;
+    b.k3_blocks = b.nl * ((b.nk + h->KB - 1) / h->KB);
+    h->nys = b.k3_blocks;
+    b.k4_rows = 2;
+    h->ni = (b.ny + b.k4_rows - 1) / b.k4_rows;
+    h->smem_v = (size_t)((VTY + 6) * (VTX + 6) + (VTY + 4) * (VTX + 4) + 3 * (VTY + 2) * (VTX + 2)) * h->esz;
+    h->smem_x = (size_t)G * b.M * t2;
+    h->smem_x64 = (size_t)G * b.M * 16;
+    h->smem_y = (size_t)b.ny * h->KB * vsz;
+    const int nra = b.k4_rows + 2;
+    h->smem_i = (size_t)G * b.M * t2 + (size_t)b.nl * nra * b.nxp * h->esz;
+    h->smem_i64 = (size_t)G * b.M * 16 + (size_t)b.nl * nra * b.nxp * 8;
+    if (h->smem_i64 > 227 * 1024 || h->smem_x64 > 227 * 1024 || h->smem_y > 227 * 1024)
+        return bail(OQG_EUNSUPPORTED, "grid too large for this build's shared-memory tiling");
+    std::vector<Work> wv(h->nv), wx(h->nx), wy(h->nys), wi(h->ni);
+    for (int i = 0; i < h->nv; ++i) wv[i] = Work{0, i};
+    for (int i = 0; i < h->nx; ++i) wx[i] = Work{0, i};
+    for (int i = 0; i < h->nys; ++i) wy[i] = Work{0, i};
+    for (int i = 0; i < h->ni; ++i) wi[i] = Work{0, i};
+    h->d_wv = dalloc<Work>(h, wv.size());
+    h->d_wx = dalloc<Work>(h, wx.size());
+    h->d_wy = dalloc<Work>(h, wy.size());
+    h->d_wi = dalloc<Work>(h, wi.size());
+    CK(cudaMemcpy(h->d_wv, wv.data(), wv.size() * sizeof(Work), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(h->d_wx, wx.data(), wx.size() * sizeof(Work), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(h->d_wy, wy.data(), wy.size() * sizeof(Work), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(h->d_wi, wi.data(), wi.size() * sizeof(Work), cudaMemcpyHostToDevice));
+
+    h->hb64 = b;
+    h->hb64.tw = d_tw64;
+    h->d_bas = dalloc<BasinDev>(h, 1);
+    h->d_bas64 = dalloc<BasinDev>(h, 1);
+    set_attrs(h);
+    int rc = push_desc(h);
+    if (rc) { destroy_all(h); return rc; }
+    rc = homsol(h);
+    if (rc) { std::string m = g_err; destroy_all(h); return fail(rc, m); }
+    rc = push_desc(h);
+    if (rc) { destroy_all(h); return rc; }
+    if (cudaStreamSynchronize(h->st) != cudaSuccess || cudaGetLastError() != cudaSuccess)
+        return bail(OQG_ECUDA, "device error during setup");
+    *out = h;
+    return OQG_OK;
+}
+
+int oqg_destroy(oqg_handle *h) {
+    destroy_all(h);
+    return OQG_OK;
+}
+
+int oqg_set_state(oqg_handle *h, const double *p, const double *pm) {
+    if (!h || !p || !pm) return fail(OQG_EINVAL, "null argument");
+    const BasinDev &b = h->hb;
+    const size_t n3 = (size_t)b.nl * b.nyp * b.px;
+    int rc;
+    if ((rc = upload3(h, p, h->stage[0], b.nl))) return rc;
+    if ((rc = upload3(h, pm, h->stage[1], b.nl))) return rc;
+    const int par = h->par;
+    stage_to_field(h, h->stage[0], b.F[par], n3);
+    stage_to_field(h, h->stage[1], b.F[1 - par], n3);
+    OQG_NL_T(launch_qcomp_t, h, h, h->stage[0], b.F[2 + par]);
+    OQG_NL_T(launch_qcomp_t, h, h, h->stage[1], b.F[3 - par]);
+    OQG_NL_T(launch_initc_t, h, h, par);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(h->st));
+    return OQG_OK;
+}
+
+int oqg_set_state_full(oqg_handle *h, const double *p, const double *pm, const double *q,
+                       const double *qm, const double *dpi, const double *dpip, const double *cs,
+                       const double *cn, const double *csp, const double *cnp) {
+    if (!h || !p || !pm || !q || !qm || !dpi || !dpip) return fail(OQG_EINVAL, "null argument");
+    const BasinDev &b = h->hb;
+    const size_t n3 = (size_t)b.nl * b.nyp * b.px;
+    const int par = h->par;
+    const double *src[4] = {p, pm, q, qm};
+    const int dst[4] = {par, 1 - par, 2 + par, 3 - par};
+    for (int f = 0; f < 4; ++f) {
+        int rc = upload3(h, src[f], h->stage[0], b.nl);
+        if (rc) return rc;
+        stage_to_field(h, h->stage[0], b.F[dst[f]], n3);
+        CK(cudaStreamSynchronize(h->st));
+    }
+    DevScalars sc;
+    CK(cudaMemcpy(&sc, b.sc, sizeof sc, cudaMemcpyDeviceToHost));
+    for (int l = 0; l < b.nl - 1; ++l) { sc.dpi[l] = dpi[l]; sc.dpip[l] = dpip[l]; }
+    for (int k = 0; k < b.nl; ++k) {
+        if (cs) sc.cs[k] = cs[k];
+        if (cn) sc.cn[k] = cn[k];
+        if (csp) sc.csp[k] = csp[k];
+        if (cnp) sc.cnp[k] = cnp[k];
+    }
+    CK(cudaMemcpy(b.sc, &sc, sizeof sc, cudaMemcpyHostToDevice));
+    return OQG_OK;
+}
+
+int oqg_get_state(oqg_handle *h, double *p, double *pm, double *q, double *qm) {
+    if (!h) return fail(OQG_EINVAL, "null handle");
+    const BasinDev &b = h->hb;
+    const size_t n3 = (size_t)b.nl * b.nyp * b.px;
+    const int par = h->par;
+    double *dst[4] = {p, pm, q, qm};
+    const int src[4] = {par, 1 - par, 2 + par, 3 - par};
+    for (int f = 0; f < 4; ++f) {
+        if (!dst[f]) continue;
+        field_to_stage(h, b.F[src[f]], h->stage[0], n3);
+        int rc = download3(h, h->stage[0], dst[f], b.nl);
+        if (rc) return rc;
+        CK(cudaStreamSynchronize(h->st));
+    }
+    return OQG_OK;
+}
+
+int oqg_get_p_layer(oqg_handle *h, int k, double *out) {
+    if (!h || !out || k < 0 || k >= h->hb.nl) return fail(OQG_EINVAL, "bad argument");
+    const BasinDev &b = h->hb;
+    const size_t n2 = (size_t)b.nyp * b.px;
+    const char *src = (const char *)b.F[h->par] + k * n2 * h->esz;
+    field_to_stage(h, src, h->stage[0], n2);
+    int rc = download3(h, h->stage[0], out, 1);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(h->st));
+    return OQG_OK;
+}
+
+int oqg_get_constraints(oqg_handle *h, double *dpi, double *dpip, double *cs, double *cn,
+                        double *csp, double *cnp) {
+    if (!h) return fail(OQG_EINVAL, "null handle");
+    DevScalars sc;
+    CK(cudaStreamSynchronize(h->st));
+    CK(cudaMemcpy(&sc, h->hb.sc, sizeof sc, cudaMemcpyDeviceToHost));
+    const int nl = h->hb.nl;
+    for (int l = 0; l < nl - 1; ++l) {
+        if (dpi) dpi[l] = sc.dpi[l];
+        if (dpip) dpip[l] = sc.dpip[l];
+    }
+    for (int k = 0; k < nl; ++k) {
+        if (cs) cs[k] = sc.cs[k];
+        if (cn) cn[k] = sc.cn[k];
+        if (csp) csp[k] = sc.csp[k];
+        if (cnp) cnp[k] = sc.cnp[k];
+    }
+    return OQG_OK;
+}
+
+int oqg_set_forcing(oqg_handle *h, const double *wekp, const double *ent, double txis, double txin) {
+    if (!h) return fail(OQG_EINVAL, "null handle");
+    BasinDev &b = h->hb;
+    const size_t n2 = (size_t)b.nyp * b.px;
+    if (wekp) {
+        int rc = upload3(h, wekp, h->stage[0], 1);
+        if (rc) return rc;
+        stage_to_field(h, h->stage[0], const_cast<void *>(b.wekp), n2);
+    } else {
+        CK(cudaMemsetAsync(const_cast<void *>(b.wekp), 0, n2 * h->esz, h->st));
+    }
+    const void *old_ent = b.ent;
+    if (ent) {
+        if (!h->ent_buf) {
+            h->ent_buf = dalloc<char>(h, (size_t)(b.nl - 1) * n2 * h->esz);
+            if (!h->ent_buf) return fail(OQG_ECUDA, "out of device memory");
+        }
+        int rc = upload3(h, ent, h->stage[1], b.nl - 1);
+        if (rc) return rc;
+        stage_to_field(h, h->stage[1], h->ent_buf, (size_t)(b.nl - 1) * n2);
+        b.ent = h->ent_buf;
+    } else {
+        b.ent = nullptr;
+    }
+    h->hb64.ent = b.ent;
+    if (b.ent != old_ent) {
+        int rc = push_desc(h);
+        if (rc) return rc;
+    }
+    if (h->mixed) k_forcing_integrals<float><<<1, 512, 0, h->st>>>(h->d_bas, 0);
+    else k_forcing_integrals<double><<<1, 512, 0, h->st>>>(h->d_bas, 0);
+    double tx[2] = {txis, txin};
+    CK(cudaMemcpyAsync(&b.sc->txis, tx, 2 * sizeof(double), cudaMemcpyHostToDevice, h->st));
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(h->st));
+    return OQG_OK;
+}
+
+int oqg_step(oqg_handle *h, double tdt, int nsteps) {
+    if (!h || nsteps < 0) return fail(OQG_EINVAL, "bad argument");
+    int done = 0;
+    if (nsteps >= 2) {
+        const int par = h->par;
+        if (!h->gexec[par] || h->g_tdt[par] != tdt) {
+            if (h->gexec[par]) { cudaGraphExecDestroy(h->gexec[par]); h->gexec[par] = nullptr; }
+            cudaGraph_t g = nullptr;
+            CK(cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
+            launch_step(h, par, tdt);
+            launch_step(h, 1 - par, tdt);
+            cudaError_t e1 = cudaGetLastError();
+            cudaError_t e2 = cudaStreamEndCapture(h->st, &g);
+            if (e1 != cudaSuccess || e2 != cudaSuccess) {
+                if (g) cudaGraphDestroy(g);
+                return fail(OQG_ECUDA, std::string("graph capture: ") +
+                                           cudaGetErrorString(e1 != cudaSuccess ? e1 : e2));
+            }
+            cudaError_t e3 = cudaGraphInstantiate(&h->gexec[par], g, 0);
+            cudaGraphDestroy(g);
+            if (e3 != cudaSuccess) return fail(OQG_ECUDA, std::string("graph instantiate: ") + cudaGetErrorString(e3));
+            h->g_tdt[par] = tdt;
+        }
+        for (; done + 2 <= nsteps; done += 2) CK(cudaGraphLaunch(h->gexec[par], h->st));
+    }
+    for (; done < nsteps; ++done) {
+        launch_step(h, h->par, tdt);
+        h->par ^= 1;
+    }
+    CK(cudaGetLastError());
+    return OQG_OK;
+}
+
+int oqg_set_step_index(oqg_handle *h, long long steps_done) {
+    if (!h || steps_done < 0) return fail(OQG_EINVAL, "bad argument");
+    CK(cudaMemcpyAsync(&h->hb.sc->nt, &steps_done, sizeof(long long), cudaMemcpyHostToDevice, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    return OQG_OK;
+}
+
+int oqg_get_step_index(oqg_handle *h, long long *steps_done) {
+    if (!h || !steps_done) return fail(OQG_EINVAL, "bad argument");
+    CK(cudaStreamSynchronize(h->st));
+    CK(cudaMemcpy(steps_done, &h->hb.sc->nt, sizeof(long long), cudaMemcpyDeviceToHost));
+    return OQG_OK;
+}
+
+int oqg_suppress(oqg_handle *h) {
+    if (!h) return fail(OQG_EINVAL, "null handle");
+    if (h->mixed) k_suppress<float><<<296, 256, 0, h->st>>>(h->d_bas, 0, h->par);
+    else k_suppress<double><<<296, 256, 0, h->st>>>(h->d_bas, 0, h->par);
+    CK(cudaGetLastError());
+    return OQG_OK;
+}
+
+int oqg_sync(oqg_handle *h) {
+    if (!h) return fail(OQG_EINVAL, "null handle");
+    CK(cudaStreamSynchronize(h->st));
+    int err = 0;
+    CK(cudaMemcpy(&err, &h->hb.sc->err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (err) return fail(OQG_ECUDA, "device error flag set");
+    return OQG_OK;
+}
+
+int oqg_check_finite(oqg_handle *h, long long *bad) {
+    if (!h || !bad) return fail(OQG_EINVAL, "bad argument");
+    CK(cudaMemsetAsync(h->d_bad, 0, sizeof(unsigned long long), h->st));
+    if (h->mixed) k_check_finite<float><<<296, 256, 0, h->st>>>(h->d_bas, 0, h->par, h->d_bad);
+    else k_check_finite<double><<<296, 256, 0, h->st>>>(h->d_bas, 0, h->par, h->d_bad);
+    unsigned long long v = 0;
+    CK(cudaMemcpyAsync(&v, h->d_bad, sizeof v, cudaMemcpyDeviceToHost, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    *bad = (long long)v;
+    return v ? fail(OQG_ENAN, "non-finite values in the state") : OQG_OK;
+}
+
+int oqg_diag(oqg_handle *h, double *ekei, double *sfmin, double *sfmax, double *circ) {
+    if (!h) return fail(OQG_EINVAL, "null handle");
+    const int nl = h->hb.nl;
+    if (h->mixed) k_diag<float><<<nl, 256, 0, h->st>>>(h->d_bas, 0, h->par, h->prm.rho, h->d_diag);
+    else k_diag<double><<<nl, 256, 0, h->st>>>(h->d_bas, 0, h->par, h->prm.rho, h->d_diag);
+    std::vector<double> o(4 * nl);
+    CK(cudaMemcpyAsync(o.data(), h->d_diag, o.size() * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    for (int k = 0; k < nl; ++k) {
+        if (ekei) ekei[k] = o[4 * k];
+        if (sfmin) sfmin[k] = o[4 * k + 1];
+        if (sfmax) sfmax[k] = o[4 * k + 2];
+        if (circ) circ[k] = o[4 * k + 3];
+    }
+    return OQG_OK;
+}
+
+int oqg_solve_inhomog(oqg_handle *h, int m, const double *rhs, double *out) {
+    if (!h || !rhs || !out || m < 1 || m > h->hb.nl) return fail(OQG_EINVAL, "bad argument");
+    const BasinDev &b = h->hb;
+    const size_t n2 = (size_t)b.nyp * b.px;
+    int rc = upload3(h, rhs, h->stage[0], 1);
+    if (rc) return rc;
+    if ((rc = solve_all_modes(h))) return rc;
+    rc = download3(h, h->stage[1] + (m - 1) * n2, out, 1);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(h->st));
+    return OQG_OK;
+}
+
+int oqg_generate_homog_soln(oqg_handle *h, int m, const double *L, double *out) {
+    int rc = oqg_solve_inhomog(h, m, L, out);
+    if (rc) return rc;
+    const double r = h->hb.rdm2[m - 1];
+    const size_t n = (size_t)h->hb.nxp * h->hb.nyp;
+    for (size_t x = 0; x < n; ++x) out[x] = L[x] + r * out[x];
+    return OQG_OK;
+}
+
+int oqg_get_modes(oqg_handle *h, double *amat, double *rdm2, double *ctl2m, double *ctm2l) {
+    if (!h) return fail(OQG_EINVAL, "null handle");
+    if (amat) std::copy(h->modes_amat.begin(), h->modes_amat.end(), amat);
+    if (rdm2) std::copy(h->modes_rdm2.begin(), h->modes_rdm2.end(), rdm2);
+    if (ctl2m) std::copy(h->modes_ctl2m.begin(), h->modes_ctl2m.end(), ctl2m);
+    if (ctm2l) std::copy(h->modes_ctm2l.begin(), h->modes_ctm2l.end(), ctm2l);
+    return OQG_OK;
+}
+
+// ekman_from_tau (ekman.F90:53-83), init-time on the host.
+int oqg_ekman_from_tau(const oqg_params *prm, const double *taux, const double *tauy, double *wekp,
+                       double *txis, double *txin) {
+    if (!prm || !taux || !tauy || !wekp) return fail(OQG_EINVAL, "null argument");
+    const int nxp = prm->nxp, nyp = prm->nyp, nxt = nxp - 1, nyt = nyp - 1;
+    const double dx = prm->dx, dy = prm->dy, f0 = prm->fnot;
+    auto P = [&](const double *a, int i, int j) { return a[i + (size_t)nxp * j]; };
+    auto rowint = [&](const std::vector<double> &r) {
+        double s = 0.0;
+        for (int i = 1; i < nxp - 1; ++i) s += r[i];
+        return (0.5 * r[0] + s + 0.5 * r[nxp - 1]) * dx;
+    };
+    if (prm->cyclic) {
+        std::vector<double> r(nxp);
+        for (int i = 0; i < nxp; ++i) r[i] = P(taux, i, 0) + P(taux, i, 1);
+        if (txis) *txis = 0.5 * rowint(r);
+        for (int i = 0; i < nxp; ++i) r[i] = P(taux, i, nyp - 2) + P(taux, i, nyp - 1);
+        if (txin) *txin = 0.5 * rowint(r);
+    } else {
+        if (txis) *txis = 0.0;
+        if (txin) *txin = 0.0;
+    }
+    std::vector<double> txt((size_t)nxt * nyp), tyt((size_t)nxp * nyt), wt((size_t)nxt * nyt);
+    for (int j = 0; j < nyp; ++j)
+        for (int i = 0; i < nxt; ++i) txt[i + (size_t)nxt * j] = 0.5 * (P(taux, i + 1, j) + P(taux, i, j));
+    for (int j = 0; j < nyt; ++j)
+        for (int i = 0; i < nxp; ++i) tyt[i + (size_t)nxp * j] = 0.5 * (P(tauy, i, j + 1) + P(tauy, i, j));
+    for (int j = 0; j < nyt; ++j)
+        for (int i = 0; i < nxt; ++i)
+            wt[i + (size_t)nxt * j] = ((1.0 / (dx * f0)) * (tyt[(i + 1) + (size_t)nxp * j] - tyt[i + (size_t)nxp * j]) -
+                                       (1.0 / (dy * f0)) * (txt[i + (size_t)nxt * (j + 1)] - txt[i + (size_t)nxt * j]));
+    // map_T_to_P (numerics.F90:64-107)
+    auto T_ = [&](int i, int j) { return wt[i + (size_t)nxt * j]; };
+    auto W = [&](int i, int j) -> double & { return wekp[i + (size_t)nxp * j]; };
+    for (int j = 1; j < nyp - 1; ++j)
+        for (int i = 1; i < nxp - 1; ++i)
+            W(i, j) = 0.25 * (T_(i, j) + T_(i - 1, j) + T_(i, j - 1) + T_(i - 1, j - 1));
+    for (int i = 1; i < nxp - 1; ++i) {
+        W(i, 0) = 0.5 * (T_(i - 1, 0) + T_(i, 0));
+        W(i, nyp - 1) = 0.5 * (T_(i - 1, nyp - 2) + T_(i, nyp - 2));
+    }
+    if (prm->cyclic) {
+        for (int j = 1; j < nyp - 1; ++j) {
+            W(0, j) = 0.25 * (T_(0, j) + T_(nxp - 2, j) + T_(0, j - 1) + T_(nxp - 2, j - 1));
+            W(nxp - 1, j) = W(0, j);
+        }
+        W(0, 0) = 0.5 * (T_(0, 0) + T_(nxp - 2, 0));
+        W(0, nyp - 1) = 0.5 * (T_(0, nyp - 2) + T_(nxp - 2, nyp - 2));
+        W(nxp - 1, 0) = W(0, 0);
+        W(nxp - 1, nyp - 1) = W(0, nyp - 1);
+    } else {
+        for (int j = 1; j < nyp - 1; ++j) {
+            W(0, j) = 0.5 * (T_(0, j - 1) + T_(0, j));
+            W(nxp - 1, j) = 0.5 * (T_(nxp - 2, j - 1) + T_(nxp - 2, j));
+        }
+        W(0, 0) = T_(0, 0);
+        W(nxp - 1, 0) = T_(nxp - 2, 0);
+        W(0, nyp - 1) = T_(0, nyp - 2);
+        W(nxp - 1, nyp - 1) = T_(nxp - 2, nyp - 2);
+    }
+    return OQG_OK;
+}
+
+int oqg_device_state(oqg_handle *h, void **p, void **pm, void **q, void **qm, int *pitch, int *elem_bytes) {
+    if (!h) return fail(OQG_EINVAL, "null handle");
+    const int par = h->par;
+    if (p) *p = h->hb.F[par];
+    if (pm) *pm = h->hb.F[1 - par];
+    if (q) *q = h->hb.F[2 + par];
+    if (qm) *qm = h->hb.F[3 - par];
+    if (pitch) *pitch = h->hb.px;
+    if (elem_bytes) *elem_bytes = (int)h->esz;
+    return OQG_OK;
+}
+
+int oqg_profile_phases(oqg_handle *h, double tdt, int nsteps, double *ms) {
+    if (!h || !ms || nsteps < 1) return fail(OQG_EINVAL, "bad argument");
+    cudaEvent_t ev[5];
+    for (int i = 0; i < 5; ++i) CK(cudaEventCreate(&ev[i]));
+    double acc[4] = {0, 0, 0, 0};
+    for (int s = 0; s < nsteps; ++s) {
+        CK(cudaEventRecord(ev[0], h->st));
+        for (int ph = 0; ph < 4; ++ph) {
+            launch_phase(h, ph, h->par, tdt);
+            CK(cudaEventRecord(ev[ph + 1], h->st));
+        }
+        h->par ^= 1;
+        CK(cudaEventSynchronize(ev[4]));
+        for (int ph = 0; ph < 4; ++ph) {
+            float t = 0.f;
+            CK(cudaEventElapsedTime(&t, ev[ph], ev[ph + 1]));
+            acc[ph] += t;
+        }
+    }
+    for (int i = 0; i < 5; ++i) cudaEventDestroy(ev[i]);
+    for (int ph = 0; ph < 4; ++ph) ms[ph] = acc[ph] / nsteps;
+    CK(cudaGetLastError());
+    return OQG_OK;
+}
+
+int oqg_stream(oqg_handle *h, void **stream) {
+    if (!h || !stream) return fail(OQG_EINVAL, "bad argument");
+    *stream = (void *)h->st;
+    return OQG_OK;
+}
+
+// Ensembles: added with the batched launch path.
+int oqg_ensemble_create(const oqg_params *, int, oqg_ensemble **out) {
+    if (out) *out = nullptr;
+    return fail(OQG_EUNSUPPORTED, "ensembles are not built yet");
+}
+int oqg_ensemble_destroy(oqg_ensemble *) { return OQG_OK; }
+int oqg_ensemble_set_state(oqg_ensemble *, int, const double *, const double *) {
+    return fail(OQG_EUNSUPPORTED, "ensembles are not built yet");
+}
+int oqg_ensemble_get_state(oqg_ensemble *, int, double *, double *, double *, double *) {
+    return fail(OQG_EUNSUPPORTED, "ensembles are not built yet");
+}
+int oqg_ensemble_set_forcing(oqg_ensemble *, int, const double *, const double *, double, double) {
+    return fail(OQG_EUNSUPPORTED, "ensembles are not built yet");
+}
+int oqg_ensemble_step(oqg_ensemble *, const double *, int) {
+    return fail(OQG_EUNSUPPORTED, "ensembles are not built yet");
+}
+int oqg_ensemble_sync(oqg_ensemble *) { return fail(OQG_EUNSUPPORTED, "ensembles are not built yet"); }
+
+}  // extern "C"

@@ -1,0 +1,109 @@
+// oqg_dev.cuh -- device-side data layout of one QG basin.
+//
+// Fields are stored per basin as [layer][j][pitch] arrays of the handle's
+// storage type T (double, or float in OQG_MIXED), x fastest like the
+// reference's Fortran (nxp, nyp, nl) arrays, with rows padded to a pitch that
+// is a multiple of 32 elements.  The two time levels of p and q live in four
+// buffers whose roles swap every step (parity `par`):
+//   p = F[par], pm = F[1-par], q = F[2+par], qm = F[3-par].
+// A step writes q_new over qm and p_new over pm, so after it the parity flips.
+#pragma once
+
+#include <cstdint>
+
+#define OQG_NLMAX 8
+#define OQG_MAXRAD 16
+
+namespace oqg {
+
+// Scalars of the constraint equations and the step bookkeeping.  One writer
+// per step: the last CTA of the y-solve kernel (the scalar phase).
+struct DevScalars {
+    double dpi[OQG_NLMAX], dpip[OQG_NLMAX];              // mass constraint (constraint.F90:63-67)
+    double cs[OQG_NLMAX], cn[OQG_NLMAX];                 // channel momentum constraints
+    double csp[OQG_NLMAX], cnp[OQG_NLMAX];
+    double alpha[OQG_NLMAX];                             // box homogeneous coefficients
+    double c_bt, c_bc1[OQG_NLMAX], c_bc2[OQG_NLMAX];     // channel homogeneous coefficients
+    double ent_xn;                                       // area integral of ent layer 1
+    double int_Be_s[OQG_NLMAX], int_Be_n[OQG_NLMAX];     // channel ent strip integrals
+    double txis, txin;
+    long long nt;                                        // steps done (nt-1 of the next)
+    int suppress_flag;                                   // set for the assembly kernel
+    unsigned int counter;                                // last-CTA detection
+    int err;                                             // device error bits
+};
+
+// Device error bits
+#define OQG_DERR_SOLVE   1   // zero pivot in the constraint solve
+
+// Number of per-tile channel strip quantities per layer (vorticity kernel)
+#define OQG_NQ 10
+
+struct BasinDev {
+    // geometry
+    int nxp, nyp, nl, cyclic;
+    int px;        // field row pitch (elements)
+    int nxin;      // x-transform input length: box nxp-2, channel nxp-1
+    int nk;        // wavenumbers per row: box nxp-2 (real), channel N/2+1 (complex)
+    int ny;        // rows of the transform problem: nyp-2
+    int M;         // complex FFT length: box 2(nxp-1), channel nxp-1
+    int nrad, rad[OQG_MAXRAD];
+    int pr;        // pitch of the modal right-hand side rows (elements of T)
+    int pk;        // pitch of spectral rows (T for a box, complex T2 for a channel)
+    int tiles_x, tiles_y;
+    int kt;        // 0-based topography / drag layer
+    int dz_sign, tau_sign, topo_active, suppress_period;
+    double dx, dy, fnot, beta;
+    double fx, fy, fx_bc, fy_bc;     // 1/dx^2, 1/dy^2 and the mixed-BC factors
+    double jac_fac;                  // 1/(3 (2dx)(2dy) f0)
+    double a_tri, ftnorm;
+    double qb_fac;                   // ocqbdy factor bcco dxm2/(bcco/2+1)/f0
+    double bc_half1;                 // bcco/2 + 1 (dPdx_2bc, dPdy_2bc)
+    double c2[OQG_NLMAX], c4[OQG_NLMAX];   // ah2/f0, ah4/f0
+    double c_ent1, c_wind, c_ent2, c_drag;
+    double h[OQG_NLMAX], gp[OQG_NLMAX], ah2[OQG_NLMAX], ah4[OQG_NLMAX];
+    double delek;
+    double ctl2m[OQG_NLMAX * OQG_NLMAX];   // column-major (k, m)
+    double ctm2l[OQG_NLMAX * OQG_NLMAX];   // column-major (m, k)
+    double amat[OQG_NLMAX * OQG_NLMAX];    // column-major (k, l)
+    double rdm2[OQG_NLMAX];
+    // box constraint solve: cdhoc and its LU (column-major, n = nl-1)
+    double cdhoc[OQG_NLMAX * OQG_NLMAX], lu[OQG_NLMAX * OQG_NLMAX];
+    int piv[OQG_NLMAX];
+    // channel homogeneous constants
+    double hc1s[OQG_NLMAX], hc2s[OQG_NLMAX], hc1n[OQG_NLMAX], hc2n[OQG_NLMAX], hbsi;
+    // device buffers
+    void *F[4];                 // p/pm/q/qm roles by parity
+    const void *wekp;           // [nyp][px] T
+    const void *ent;            // [nl-1][nyp][px] T or null
+    const double *ddyn;         // [nyp][px] or null
+    const double *yprel;        // [nyp] y - yl/2 (box.F90:142-145)
+    void *rhs;                  // [nl][ny][pr] T
+    void *spec;                 // [nl][ny][pk] T or T2
+    const void *tw;             // [M] T2 twiddles exp(-2 pi i t/M)
+    const double *piv_tab;      // Thomas pivots 1/(b - a gam), compressed
+    const int *piv_off;         // [nl*nk] offset into piv_tab
+    const int *piv_len;         // [nl*nk] stored length (beyond: fixed point)
+    const double *dst_w;        // [nk] sum_i of the inverse DST basis (box)
+    const void *hsb;            // box: [nl-1][nyp][px] T hom_sol_bc
+    const double *hbt;          // channel: [nyp] barotropic homogeneous solution
+    const double *hbc1, *hbc2;  // channel: [nl][nyp]
+    double *part_tile;          // [tiles][nl][OQG_NQ]
+    double *part_col;           // [nl][nk]
+    DevScalars *sc;
+    // launch bookkeeping
+    int k3_blocks;              // CTAs of this basin in the y-solve launch
+    int k4_rows;                // interior rows per CTA of the assembly launch
+};
+
+// One entry of a launch's work list: which basin and which block of it.
+struct Work {
+    int member;
+    int block;
+};
+
+template <class T> struct C2;
+template <> struct C2<double> { typedef double2 t; };
+template <> struct C2<float> { typedef float2 t; };
+
+}  // namespace oqg

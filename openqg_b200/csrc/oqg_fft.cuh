@@ -1,0 +1,201 @@
+// oqg_fft.cuh -- shared-memory mixed-radix FFT for the x-transforms.
+//
+// The x-direction transforms of the Helmholtz inverter (qg/inhomog.F90:170-255;
+// FFTW RODFT00 for the closed box, r2c/c2r for the channel) run as complex
+// FFTs of length M over rows staged in shared memory.  Two real rows share one
+// complex transform (real and imaginary parts).  The algorithm is the Stockham
+// autosort FFT (decimation in time, e^{-2 pi i jk/M}), radices 8, 4, 2, 3 and
+// 5.  Each stage reads its R inputs into registers, synchronises, and writes
+// its outputs in place, so one buffer of M complex values serves a transform.
+// A CTA holds G transforms; TT threads serve one transform and each thread owns
+// up to E elements of it.
+#pragma once
+
+#include "oqg_dev.cuh"
+
+namespace oqg {
+
+template <class T2> __device__ __forceinline__ T2 c_mul(T2 a, T2 b) {
+    T2 r;
+    r.x = a.x * b.x - a.y * b.y;
+    r.y = a.x * b.y + a.y * b.x;
+    return r;
+}
+template <class T2> __device__ __forceinline__ T2 c_add(T2 a, T2 b) {
+    T2 r; r.x = a.x + b.x; r.y = a.y + b.y; return r;
+}
+template <class T2> __device__ __forceinline__ T2 c_sub(T2 a, T2 b) {
+    T2 r; r.x = a.x - b.x; r.y = a.y - b.y; return r;
+}
+// -i z
+template <class T2> __device__ __forceinline__ T2 c_mi(T2 z) { T2 r; r.x = z.y; r.y = -z.x; return r; }
+
+template <class T> struct FftConst;
+template <> struct FftConst<double> {
+    static __device__ __forceinline__ double s3() { return 0.86602540378443864676; }
+    static __device__ __forceinline__ double h2() { return 0.70710678118654752440; }
+    static __device__ __forceinline__ double c51() { return 0.30901699437494742410; }
+    static __device__ __forceinline__ double c52() { return -0.80901699437494742410; }
+    static __device__ __forceinline__ double s51() { return 0.95105651629515357212; }
+    static __device__ __forceinline__ double s52() { return 0.58778525229247312917; }
+};
+template <> struct FftConst<float> {
+    static __device__ __forceinline__ float s3() { return 0.86602540378443864676f; }
+    static __device__ __forceinline__ float h2() { return 0.70710678118654752440f; }
+    static __device__ __forceinline__ float c51() { return 0.30901699437494742410f; }
+    static __device__ __forceinline__ float c52() { return -0.80901699437494742410f; }
+    static __device__ __forceinline__ float s51() { return 0.95105651629515357212f; }
+    static __device__ __forceinline__ float s52() { return 0.58778525229247312917f; }
+};
+
+// In-register forward DFT of size R.
+template <class T, int R> struct Dft;
+
+template <class T> struct Dft<T, 2> {
+    typedef typename C2<T>::t T2;
+    static __device__ __forceinline__ void run(T2 *v) {
+        T2 a = v[0];
+        v[0] = c_add(a, v[1]);
+        v[1] = c_sub(a, v[1]);
+    }
+};
+
+template <class T> struct Dft<T, 4> {
+    typedef typename C2<T>::t T2;
+    static __device__ __forceinline__ void run(T2 *v) {
+        T2 t0 = c_add(v[0], v[2]), t1 = c_sub(v[0], v[2]);
+        T2 t2 = c_add(v[1], v[3]), t3 = c_mi(c_sub(v[1], v[3]));
+        v[0] = c_add(t0, t2);
+        v[1] = c_add(t1, t3);
+        v[2] = c_sub(t0, t2);
+        v[3] = c_sub(t1, t3);
+    }
+};
+
+template <class T> struct Dft<T, 8> {
+    typedef typename C2<T>::t T2;
+    static __device__ __forceinline__ void run(T2 *v) {
+        T2 e[4] = {v[0], v[2], v[4], v[6]};
+        T2 o[4] = {v[1], v[3], v[5], v[7]};
+        Dft<T, 4>::run(e);
+        Dft<T, 4>::run(o);
+        const T h = FftConst<T>::h2();
+        T2 w1, w3;
+        // o1 * (h - i h), o2 * (-i), o3 * (-h - i h)
+        w1.x = h * (o[1].x + o[1].y);
+        w1.y = h * (o[1].y - o[1].x);
+        T2 w2 = c_mi(o[2]);
+        w3.x = h * (o[3].y - o[3].x);
+        w3.y = -h * (o[3].x + o[3].y);
+        v[0] = c_add(e[0], o[0]);
+        v[4] = c_sub(e[0], o[0]);
+        v[1] = c_add(e[1], w1);
+        v[5] = c_sub(e[1], w1);
+        v[2] = c_add(e[2], w2);
+        v[6] = c_sub(e[2], w2);
+        v[3] = c_add(e[3], w3);
+        v[7] = c_sub(e[3], w3);
+    }
+};
+
+template <class T> struct Dft<T, 3> {
+    typedef typename C2<T>::t T2;
+    static __device__ __forceinline__ void run(T2 *v) {
+        const T s3 = FftConst<T>::s3();
+        T2 s = c_add(v[1], v[2]), d = c_sub(v[1], v[2]);
+        T2 m;
+        m.x = v[0].x - T(0.5) * s.x;
+        m.y = v[0].y - T(0.5) * s.y;
+        T2 jd;  // -i s3 d
+        jd.x = s3 * d.y;
+        jd.y = -s3 * d.x;
+        v[0] = c_add(v[0], s);
+        v[1] = c_add(m, jd);
+        v[2] = c_sub(m, jd);
+    }
+};
+
+template <class T> struct Dft<T, 5> {
+    typedef typename C2<T>::t T2;
+    static __device__ __forceinline__ void run(T2 *v) {
+        const T c1 = FftConst<T>::c51(), c2 = FftConst<T>::c52();
+        const T s1 = FftConst<T>::s51(), s2 = FftConst<T>::s52();
+        T2 t1 = c_add(v[1], v[4]), t2 = c_add(v[2], v[3]);
+        T2 t3 = c_sub(v[1], v[4]), t4 = c_sub(v[2], v[3]);
+        T2 a, bq, u, w;
+        a.x = v[0].x + c1 * t1.x + c2 * t2.x;
+        a.y = v[0].y + c1 * t1.y + c2 * t2.y;
+        bq.x = v[0].x + c2 * t1.x + c1 * t2.x;
+        bq.y = v[0].y + c2 * t1.y + c1 * t2.y;
+        u.x = s1 * t3.x + s2 * t4.x;      // (s1 t3 + s2 t4)
+        u.y = s1 * t3.y + s2 * t4.y;
+        w.x = s2 * t3.x - s1 * t4.x;      // (s2 t3 - s1 t4)
+        w.y = s2 * t3.y - s1 * t4.y;
+        v[0].x = v[0].x + t1.x + t2.x;
+        v[0].y = v[0].y + t1.y + t2.y;
+        v[1] = c_add(a, c_mi(u));
+        v[4] = c_sub(a, c_mi(u));
+        v[2] = c_add(bq, c_mi(w));
+        v[3] = c_sub(bq, c_mi(w));
+    }
+};
+
+// One Stockham stage of radix R on a transform of length M at z (shared).
+// All threads of the CTA must call it (it synchronises the CTA).
+template <class T, int R, int E>
+__device__ __forceinline__ void fft_stage(typename C2<T>::t *z, int M, int Ns,
+                                          const typename C2<T>::t *__restrict__ tw,
+                                          int t, int TT) {
+    typedef typename C2<T>::t T2;
+    constexpr int BMAX = (E + R - 1) / R;
+    T2 v[BMAX][R];
+    const int nb = M / R;
+    const int tstep = M / (Ns * R);
+    const bool act = t < TT;
+#pragma unroll
+    for (int b = 0; b < BMAX; ++b) {
+        int j = t + b * TT;
+        if (act && j < nb) {
+            int jm = j % Ns;
+            v[b][0] = z[j];
+#pragma unroll
+            for (int r = 1; r < R; ++r) {
+                T2 w = tw[r * jm * tstep];
+                v[b][r] = c_mul(z[j + r * nb], w);
+            }
+            Dft<T, R>::run(v[b]);
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int b = 0; b < BMAX; ++b) {
+        int j = t + b * TT;
+        if (act && j < nb) {
+            int jm = j % Ns;
+            int d = (j / Ns) * Ns * R + jm;
+#pragma unroll
+            for (int r = 0; r < R; ++r) z[d + r * Ns] = v[b][r];
+        }
+    }
+    __syncthreads();
+}
+
+// Forward FFT of the transform at z (length M, radices rad[0..nrad)).
+template <class T, int E>
+__device__ void fft_smem(typename C2<T>::t *z, int M, const int *rad, int nrad,
+                         const typename C2<T>::t *__restrict__ tw, int t, int TT) {
+    int Ns = 1;
+    for (int s = 0; s < nrad; ++s) {
+        int R = rad[s];
+        switch (R) {
+            case 8: fft_stage<T, 8, E>(z, M, Ns, tw, t, TT); break;
+            case 4: fft_stage<T, 4, E>(z, M, Ns, tw, t, TT); break;
+            case 2: fft_stage<T, 2, E>(z, M, Ns, tw, t, TT); break;
+            case 3: fft_stage<T, 3, E>(z, M, Ns, tw, t, TT); break;
+            default: fft_stage<T, 5, E>(z, M, Ns, tw, t, TT); break;
+        }
+        Ns *= R;
+    }
+}
+
+}  // namespace oqg

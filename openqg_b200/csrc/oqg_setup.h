@@ -1,0 +1,44 @@
+// oqg_setup.h -- init-time host computations of init_qg (qg/qg.F90:60-103):
+// vertical modes, Helmholtz tables, FFT plans.  Compiled without FMA
+// contraction so the tables round like the reference's FP64 arithmetic.
+#pragma once
+
+#include <string>
+#include <vector>
+
+namespace oqg {
+
+struct Modes {
+    int nl = 0;
+    std::vector<double> amat, ctl2m, ctm2l, rdm2;   // column-major nl x nl; rdm2[nl]
+};
+
+// compute_A + eigmod + derive_qg_modes (qg/modes.F90:46-246).  Returns false
+// (with a message) when the mode matrices fail the identity check.
+bool setup_modes(int nl, const double *h, const double *gp, double fnot, Modes &out,
+                 std::string &err);
+
+// Tridiagonal coefficients of init_inhomog (qg/inhomog.F90:126-141) and the
+// pivots 1/(bb - a*gam) of the Thomas forward sweep (inhomog.F90:188-195),
+// per (mode, wavenumber), stored up to their floating-point fixed point.
+struct PivotTable {
+    std::vector<double> tab;
+    std::vector<int> off, len;   // [nl * nk]
+};
+void setup_pivots(bool cyclic, int nxp, int nyp, double dx, double dy,
+                  const std::vector<double> &rdm2, PivotTable &out, double &a_tri);
+
+// Radices (8, 4, 2, 3, 5) of a transform length; false if another prime remains.
+bool fft_radices(int M, std::vector<int> &rad);
+
+// exp(-2 pi i t / M), t = 0..M-1, interleaved (re, im), correctly rounded.
+void fft_twiddles(int M, std::vector<double> &tw);
+
+// w_k = sum_{i=1..n} 2 sin(pi i k/(n+1)), k = 1..n: the x-sum of the k-th
+// inverse DST-I basis row.
+void dst_row_sums(int n, std::vector<double> &w);
+
+// DGETRF-style LU with partial pivoting (column-major); false if singular.
+bool lu_factor(int n, const double *A, double *LU, int *piv);
+
+}  // namespace oqg

@@ -1,0 +1,76 @@
+"""The C-ABI library loads and exports every entry point include/oqg.h declares
+(no GPU needed; no compute call is made without a device)."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+import oracle
+from openqg_b200 import build as oqg_build
+from openqg_b200 import core
+from openqg_b200.params import OqgParams, atmos_channel, double_gyre_tau, ocean_double_gyre
+from tests.conftest import has_gpu
+
+HEADER = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include", "oqg.h")
+
+
+def declared_functions():
+    src = open(HEADER).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"^\s*(?:const\s+)?\w+\s*\*?\s*(oqg_\w+)\s*\(", src, flags=re.M)))
+
+
+@pytest.fixture(scope="module")
+def liboqg():
+    oqg_build.build()
+    return core.lib()
+
+
+def test_header_declares_the_step_boundary():
+    names = declared_functions()
+    for must in ("oqg_create", "oqg_step", "oqg_set_state", "oqg_get_state", "oqg_set_forcing",
+                 "oqg_suppress", "oqg_destroy", "oqg_ensemble_step"):
+        assert must in names
+
+
+def test_library_exports_every_declared_symbol(liboqg):
+    missing = [n for n in declared_functions() if not hasattr(liboqg, n)]
+    assert not missing, missing
+
+
+def test_params_struct_layout_matches_header():
+    # offsets fixed by the C struct in include/oqg.h (x86-64 ABI)
+    assert OqgParams.h.offset == 56
+    assert OqgParams.bcco.offset == 56 + 4 * 64
+    assert ctypes.sizeof(OqgParams) == 56 + 4 * 64 + 24 + 16 + 8
+
+
+@pytest.mark.skipif(has_gpu(), reason="checks the no-device path")
+def test_create_without_device_reports_enodev(liboqg):
+    prm = ocean_double_gyre(33).to_c()
+    h = ctypes.c_void_p()
+    rc = liboqg.oqg_create(ctypes.byref(prm), ctypes.byref(h))
+    assert rc == 7 and not h.value
+    assert b"device" in liboqg.oqg_last_error()
+
+
+def test_create_rejects_bad_params(liboqg):
+    b = ocean_double_gyre(33)
+    prm = b.to_c()
+    prm.nl = 9
+    h = ctypes.c_void_p()
+    assert liboqg.oqg_create(ctypes.byref(prm), ctypes.byref(h)) in (1, 5)
+    assert liboqg.oqg_create(None, ctypes.byref(h)) == 1
+
+
+def test_ekman_from_tau_matches_oracle(liboqg):
+    """Init-time host routine of the library (ekman.F90:53-83)."""
+    for b in (ocean_double_gyre(65), atmos_channel(49, 25)):
+        taux, tauy = double_gyre_tau(b)
+        tauy = tauy + 1e-5 * np.cos(np.arange(b.nxp) * 0.3)[None, :]
+        wg, sg, ng = core.ekman_from_tau(b, taux, tauy)
+        wo, so, no = oracle.ekman_from_tau(b, taux, tauy)
+        assert np.array_equal(wg, wo)
+        assert sg == so and ng == no

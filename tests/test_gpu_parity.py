@@ -1,0 +1,235 @@
+"""GPU parity: the CUDA path (through the C ABI) against the FP64 oracle.
+
+Tolerances (relative L2 over the whole field), from the parity contract:
+  * FP64: psi and q within 1e-12 after 1 step and 1e-10 after 10 steps;
+  * Helmholtz solves within 1e-13 of the oracle and residual <= 1e-11
+    (src/tests/test_inhomog.F90:149);
+  * OQG_MIXED (FP32 state, stencils and transforms): psi within 1e-5 after
+    one step.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from openqg_b200.core import QG, ekman_from_tau
+from openqg_b200.params import (OQG_MIXED, Basin, atmos_channel, double_gyre_tau,
+                                initial_psi, ocean_double_gyre)
+from tests.qg_numpy import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(autouse=True)
+def _need_gpu(gpu_required):
+    pass
+
+
+def _channel_tau(b, amp=0.1):
+    yl = (b.nyp - 1) * b.dy
+    y = np.arange(b.nyp) * b.dy
+    tx = amp * np.sin(np.pi * y / yl)
+    taux = np.repeat(tx[:, None], b.nxp, axis=1)
+    return taux, np.zeros_like(taux)
+
+
+def _ent(b, seed, amp=1e-6):
+    rng = np.random.default_rng(seed)
+    e = np.zeros((b.nl - 1,) + b.shape2)
+    yy, xx = np.meshgrid(np.linspace(0, 1, b.nyp), np.linspace(0, 1, b.nxp), indexing="ij")
+    for k in range(b.nl - 1):
+        e[k] = amp * (np.sin(2 * np.pi * xx * (k + 1)) * np.cos(np.pi * yy) + 0.3 * rng.standard_normal(b.shape2))
+        if b.cyclic:
+            e[k][:, -1] = e[k][:, 0]
+    return e
+
+
+def make_pair(b: Basin, seed=1, distinct_pm=True, ent=False, amp_psi=1.0):
+    psi = initial_psi(b, seed) * amp_psi
+    p = b.fnot * psi
+    pm = b.fnot * initial_psi(b, seed + 7) * amp_psi * 0.5 + 0.5 * p if distinct_pm else p.copy()
+    taux, tauy = _channel_tau(b) if b.cyclic else double_gyre_tau(b)
+    w, ts, tn = oracle.ekman_from_tau(b, taux, tauy)
+    e = _ent(b, seed) if ent else None
+    g, o = QG(b), oracle.Oracle(b)
+    for x in (g, o):
+        x.set_state(p, pm)
+        x.set_forcing(w, e, ts, tn)
+    return g, o
+
+
+def assert_state_close(g, o, tol, what=""):
+    G = g.get_state()
+    O = o.get_state()
+    for name, a, r in zip(("p", "pm", "q", "qm"), G, O):
+        err = rel_l2(a, r)
+        assert err <= tol, "%s %s rel L2 %.3e > %.1e" % (what, name, err, tol)
+
+
+def assert_constraints_close(g, o, tol):
+    cg, co = g.constraints(), o.get_constraints()
+    for key in ("dpi", "dpip"):
+        sc = max(np.abs(co[key]).max(), 1e-300)
+        assert np.abs(cg[key] - co[key]).max() <= tol * sc, key
+    if g.b.cyclic:
+        for key in ("cs", "cn", "csp", "cnp"):
+            sc = max(np.abs(co[key]).max(), 1e-300)
+            assert np.abs(cg[key] - co[key]).max() <= tol * sc, key
+
+
+# ------------------------------------------------------------------ pieces
+BOXES = [ocean_double_gyre(129), ocean_double_gyre(65), ocean_double_gyre(513, dx=10e3),
+         Basin(nxp=81, nyp=101, dx=1e4, dy=1e4, h=[1000.0, 2000.0, 3000.0], gp=[0.02, 0.01]),
+         atmos_channel(193, 97), atmos_channel(101, 101, dx=1e4), atmos_channel(49, 25)]
+IDS = ["box129", "box65", "box513", "box81x101", "chan193x97", "chan101", "chan49x25"]
+
+
+@pytest.mark.parametrize("b", BOXES, ids=IDS)
+def test_modes_match_oracle(b):
+    g, o = QG(b), oracle.Oracle(b)
+    mg, mo = g.modes(), o.modes()
+    for k in ("amat", "ctl2m", "ctm2l"):
+        assert np.abs(mg[k] - mo[k]).max() <= 1e-14 * np.abs(mo[k]).max(), k
+    assert np.allclose(mg["rdm2"], mo["rdm2"], rtol=1e-14, atol=0)
+
+
+@pytest.mark.parametrize("b", BOXES, ids=IDS)
+def test_solve_inhomog_matches_oracle_and_residual(b):
+    g, o = QG(b), oracle.Oracle(b)
+    rng = np.random.default_rng(5)
+    rhs = rng.random(b.shape2)
+    if b.cyclic:
+        rhs[:, -1] = rhs[:, 0]
+    rdm2 = g.modes()["rdm2"]
+    for m in range(1, b.nl + 1):
+        sg = g.solve_inhomog_eqn(m, rhs)
+        so = o.solve_inhomog(m, rhs)
+        assert rel_l2(sg, so) <= 1e-13, m
+        out = o.del2(sg, 0.0) - rdm2[m - 1] * sg
+        sl = (slice(1, -1), slice(None)) if b.cyclic else (slice(1, -1), slice(1, -1))
+        res = np.abs(out[sl] - rhs[sl]).max() / np.abs(rhs[sl]).max()
+        assert res <= 1e-11, (m, res)
+
+
+@pytest.mark.parametrize("b", BOXES[:2] + BOXES[4:5], ids=["box129", "box65", "chan193x97"])
+def test_generate_homog_soln_matches_oracle(b):
+    g, o = QG(b), oracle.Oracle(b)
+    L = np.ones(b.shape2)
+    for m in range(2, b.nl + 1):
+        assert rel_l2(g.generate_homog_soln(m, L), o.generate_homog_soln(m, L)) <= 1e-14
+
+
+@pytest.mark.parametrize("b", [ocean_double_gyre(65), atmos_channel(49, 25)], ids=["box", "chan"])
+def test_init_pv_and_constraints_match(b):
+    g, o = make_pair(b)
+    assert_state_close(g, o, 1e-14, "init")
+    assert_constraints_close(g, o, 1e-13)
+
+
+def test_ekman_matches_oracle():
+    for b in (ocean_double_gyre(129), atmos_channel(193, 97)):
+        taux, tauy = (_channel_tau(b) if b.cyclic else double_gyre_tau(b))
+        tauy = tauy + 1e-5 * np.sin(np.arange(b.nxp) * 0.1)[None, :]
+        wg, sg, ng = ekman_from_tau(b, taux, tauy)
+        wo, so, no = oracle.ekman_from_tau(b, taux, tauy)
+        assert np.array_equal(wg, wo)
+        assert sg == so and ng == no
+
+
+# ------------------------------------------------------------------ whole steps
+STEP_CASES = [
+    (ocean_double_gyre(17), dict()),
+    (ocean_double_gyre(33), dict(ent=True)),
+    (ocean_double_gyre(65), dict()),
+    (ocean_double_gyre(97), dict()),
+    (ocean_double_gyre(129), dict()),
+    (ocean_double_gyre(129), dict(ent=True, distinct_pm=False)),
+    (ocean_double_gyre(513, dx=10e3), dict()),
+    (atmos_channel(193, 97), dict(amp_psi=30.0)),
+    (atmos_channel(49, 25), dict(ent=True, amp_psi=30.0)),
+    (atmos_channel(97, 65), dict(amp_psi=30.0)),
+]
+STEP_IDS = ["box17", "box33ent", "box65", "box97", "box129", "box129ent", "box513",
+            "chan193x97", "chan49ent", "chan97x65"]
+
+
+@pytest.mark.parametrize("b,kw", STEP_CASES, ids=STEP_IDS)
+def test_step_parity(b, kw):
+    g, o = make_pair(b, **kw)
+    tdt = 3600.0 if not b.cyclic else 360.0
+    g.step(tdt, 1)
+    o.step(tdt, 1)
+    assert_state_close(g, o, 1e-12, "1 step")
+    assert_constraints_close(g, o, 1e-11)
+    g.step(tdt, 9)
+    o.step(tdt, 9)
+    assert_state_close(g, o, 1e-10, "10 steps")
+    assert_constraints_close(g, o, 1e-9)
+    assert g.step_index() == 10
+
+
+def test_topography_and_drag_layer():
+    b = ocean_double_gyre(65)
+    yy, xx = np.meshgrid(np.linspace(-1, 1, b.nyp), np.linspace(-1, 1, b.nxp), indexing="ij")
+    b.ddyn = (b.fnot / b.h[-1]) * 50.0 * np.exp(-4 * (xx ** 2 + yy ** 2))
+    g, o = make_pair(b)
+    for _ in range(3):
+        g.step(3600.0, 1)
+        o.step(3600.0, 1)
+    assert_state_close(g, o, 1e-12, "topography")
+
+
+def test_graph_replay_equals_single_steps():
+    b = ocean_double_gyre(65)
+    g1, _ = make_pair(b)
+    g2, _ = make_pair(b)
+    g1.step(3600.0, 6)              # three replays of the 2-step graph
+    for _ in range(6):
+        g2.step(3600.0, 1)           # single launches
+    for a, c in zip(g1.get_state(), g2.get_state()):
+        assert np.array_equal(a, c)
+
+
+def test_explicit_suppress_matches_oracle():
+    b = ocean_double_gyre(65, suppress_period=0)
+    g, o = make_pair(b)
+    g.step(3600.0, 3)
+    o.step(3600.0, 3)
+    g.suppress()
+    o.suppress()
+    assert_state_close(g, o, 1e-12, "suppress")
+    assert_constraints_close(g, o, 1e-11)
+
+
+def test_diag_matches_oracle():
+    for b in (ocean_double_gyre(129), atmos_channel(193, 97)):
+        g, o = make_pair(b)
+        g.step(3600.0, 2)
+        o.step(3600.0, 2)
+        dg, do = g.diag(), o.diag()
+        for k in ("ekei", "sfmin", "sfmax"):
+            assert np.allclose(dg[k], do[k], rtol=1e-9, atol=1e-12 * np.abs(do[k]).max()), k
+
+
+def test_check_finite_reports_nan():
+    b = ocean_double_gyre(33)
+    g, _ = make_pair(b)
+    assert g.check_finite() == 0
+    p, pm, q, qm = g.get_state()
+    p[1, 5, 7] = np.nan
+    g.set_state(p, pm)
+    assert g.check_finite() > 0
+
+
+@pytest.mark.parametrize("b", [ocean_double_gyre(129), ocean_double_gyre(513, dx=10e3),
+                               atmos_channel(193, 97)], ids=["box129", "box513", "chan"])
+def test_mixed_precision_error_per_step(b):
+    """FP32 bulk arithmetic: psi within 1e-5 relative L2 of FP64 after a step."""
+    bm = Basin(**{**b.__dict__, "precision": OQG_MIXED, "_keep": []})
+    g, o = make_pair(bm, amp_psi=30.0 if b.cyclic else 1.0)
+    tdt = 360.0 if b.cyclic else 3600.0
+    g.step(tdt, 1)
+    o.step(tdt, 1)
+    P, _, Q, _ = g.get_state()
+    Po, _, Qo, _ = o.get_state()
+    assert rel_l2(P, Po) <= 1e-5
+    assert rel_l2(Q, Qo) <= 1e-5
