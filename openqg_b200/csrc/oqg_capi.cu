@@ -46,7 +46,7 @@ struct oqg_handle {
     std::vector<void *> allocs;
     Work *d_wv = nullptr, *d_wx = nullptr, *d_wy = nullptr, *d_wi = nullptr;
     int nv = 0, nx = 0, nys = 0, ni = 0;
-    int E = 8, KB = 16;
+    int E = 8, KB = 16, xthreads = 128;
     size_t smem_v = 0, smem_x = 0, smem_x64 = 0, smem_y = 0, smem_i = 0, smem_i64 = 0;
     double *stage[2] = {nullptr, nullptr};
     unsigned long long *d_bad = nullptr;
@@ -70,23 +70,41 @@ static X *dalloc(oqg_handle *h, size_t count) {
 // ----------------------------------------------------------- launch helpers
 static const int XTHREADS = 256;
 
+// Launch with programmatic stream serialisation: the kernel may be scheduled
+// while its predecessor drains and waits in griddepcontrol.wait for its data.
+template <typename... KArgs, typename... Args>
+static void launch_pdl(void (*kern)(KArgs...), int grid, int block, size_t smem, cudaStream_t st,
+                       Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...);
+}
+
 template <class T, int NL, int E>
 static void launch_step_t(oqg_handle *h, int par, double tdt) {
     const BasinDev &b = h->hb;
-    k_vort<T, NL><<<h->nv, VTHREADS, h->smem_v, h->st>>>(h->d_bas, h->d_wv, par, tdt);
-    k_xfwd<T, E><<<h->nx, XTHREADS, h->smem_x, h->st>>>(h->d_bas, h->d_wx, nullptr);
+    launch_pdl(k_vort<T, NL>, h->nv, VTHREADS, h->smem_v, h->st, h->d_bas, h->d_wv, par, tdt);
+    launch_pdl(k_xfwd<T, E>, h->nx, h->xthreads, h->smem_x, h->st, h->d_bas, h->d_wx, (const void *)nullptr);
     if (b.cyclic)
-        k_ysolve<T, true, NL><<<h->nys, 32 * h->KB, h->smem_y, h->st>>>(h->d_bas, h->d_wy, tdt, 1);
+        launch_pdl(k_ysolve<T, true, NL>, h->nys, 32 * h->KB, h->smem_y, h->st, h->d_bas, h->d_wy, tdt, 1);
     else
-        k_ysolve<T, false, NL><<<h->nys, 32 * h->KB, h->smem_y, h->st>>>(h->d_bas, h->d_wy, tdt, 1);
-    k_xinv<T, E, NL><<<h->ni, XTHREADS, h->smem_i, h->st>>>(h->d_bas, h->d_wi, par, nullptr);
+        launch_pdl(k_ysolve<T, false, NL>, h->nys, 32 * h->KB, h->smem_y, h->st, h->d_bas, h->d_wy, tdt, 1);
+    launch_pdl(k_xinv<T, E, NL>, h->ni, XTHREADS, h->smem_i, h->st, h->d_bas, h->d_wi, par, (double *)nullptr);
 }
 
 // FP64 solve of the modal Helmholtz problems with the rhs buffer as input;
 // modal solutions into out ([nl][nyp][px] FP64).
 template <int NL, int E>
 static void launch_solve_t(oqg_handle *h, double *out) {
-    k_xfwd<double, E><<<h->nx, XTHREADS, h->smem_x64, h->st>>>(h->d_bas64, h->d_wx, nullptr);
+    k_xfwd<double, E><<<h->nx, h->xthreads, h->smem_x64, h->st>>>(h->d_bas64, h->d_wx, nullptr);
     if (h->hb.cyclic)
         k_ysolve<double, true, NL><<<h->nys, 32 * h->KB, h->smem_y, h->st>>>(h->d_bas64, h->d_wy, 0.0, 0);
     else
@@ -302,7 +320,7 @@ static void launch_phase_t(oqg_handle *h, int phase, int par, double tdt) {
     const BasinDev &b = h->hb;
     switch (phase) {
         case 0: k_vort<T, NL><<<h->nv, VTHREADS, h->smem_v, h->st>>>(h->d_bas, h->d_wv, par, tdt); break;
-        case 1: k_xfwd<T, E><<<h->nx, XTHREADS, h->smem_x, h->st>>>(h->d_bas, h->d_wx, nullptr); break;
+        case 1: k_xfwd<T, E><<<h->nx, h->xthreads, h->smem_x, h->st>>>(h->d_bas, h->d_wx, nullptr); break;
         case 2:
             if (b.cyclic)
                 k_ysolve<T, true, NL><<<h->nys, 32 * h->KB, h->smem_y, h->st>>>(h->d_bas, h->d_wy, tdt, 1);
@@ -387,8 +405,24 @@ int oqg_create(const oqg_params *prm, oqg_handle **out) {
     for (int i = 0; i < b.nrad; ++i) b.rad[i] = rad[i];
     b.pr = rup(b.nxin, 32);
     b.pk = rup(b.nk, 32);
-    b.tiles_x = (P.nxp + VTX - 1) / VTX;
-    b.tiles_y = (P.nyp + VTY - 1) / VTY;
+    // vorticity tiles: VTX columns by vty rows, vty chosen so that the tiles
+    // fill whole waves of 2 CTAs per SM (cost ~ waves x halo'd rows)
+    {
+        int nsm = 148;
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, 0);
+        const int slots = 2 * nsm;
+        b.tiles_x = (P.nxp + VTX - 1) / VTX;
+        int best = VTYMAX;
+        long best_cost = -1;
+        for (int vt = VTYMAX; vt >= 8; --vt) {
+            const int ty = (P.nyp + vt - 1) / vt;
+            const long waves = ((long)b.tiles_x * ty + slots - 1) / slots;
+            const long cost = waves * (vt + 6);
+            if (best_cost < 0 || cost < best_cost) { best_cost = cost; best = vt; }
+        }
+        b.vty = best;
+        b.tiles_y = (P.nyp + b.vty - 1) / b.vty;
+    }
     b.kt = P.k_topo - 1;
     b.dz_sign = P.dz_sign; b.tau_sign = P.tau_sign;
     b.suppress_period = P.suppress_period;
@@ -490,21 +524,33 @@ int oqg_create(const oqg_params *prm, oqg_handle **out) {
     const size_t t2 = 2 * h->esz;
     const int npm = (b.ny + 1) / 2;
     h->nv = b.tiles_x * b.tiles_y;
-    h->nx = (b.nl * npm + G - 1) / G;
+    // forward transform: one row pair per group, CTAs of >= 128 threads
+    const int GX = std::max(1, 128 / TT);
+    h->xthreads = GX * TT;
+    h->nx = (b.nl * npm + GX - 1) / GX;
     const size_t vsz = (size_t)(b.cyclic ? 16 : 8);
-    h->KB = 16;
-    while (h->KB > 2 && (size_t)b.ny * h->KB * vsz > 100 * 1024) h->KB /= 2;
+    // y-solve: 4 columns (warps) per CTA; tile + pivots, padded columns
+    h->KB = 4;
+    const int S_ = (b.ny + 31) / 32;
+    const int LDy = (b.ny + 32) | 1;
+    (void)S_;
     b.k3_blocks = b.nl * ((b.nk + h->KB - 1) / h->KB);
     h->nys = b.k3_blocks;
     b.k4_rows = 2;
     h->ni = (b.ny + b.k4_rows - 1) / b.k4_rows;
-    h->smem_v = (size_t)((VTY + 6) * (VTX + 6) + (VTY + 4) * (VTX + 4) + 3 * (VTY + 2) * (VTX + 2)) * h->esz;
-    h->smem_x = (size_t)G * b.M * t2;
-    h->smem_x64 = (size_t)G * b.M * 16;
-    h->smem_y = (size_t)b.ny * h->KB * vsz;
-    const int nra = b.k4_rows + 2;
-    h->smem_i = (size_t)G * b.M * t2 + (size_t)b.nl * nra * b.nxp * h->esz;
-    h->smem_i64 = (size_t)G * b.M * 16 + (size_t)b.nl * nra * b.nxp * 8;
+    {
+        const int vt = b.vty;
+        h->smem_v = (size_t)(2 * ((vt + 6) * (VTX + 6) + 2 * (vt + 2) * (VTX + 2) + vt * VTX) +
+                             (vt + 4) * (VTX + 4) + (vt + 2) * (VTX + 2) + vt * VTX) * h->esz;
+    }
+    const int NTW = fft_tw_len(b.M), LB = fft_buf_len(b.M);
+    h->smem_x = (size_t)round16(NTW * (int)t2) + (size_t)GX * 2 * LB * t2;
+    h->smem_x64 = (size_t)round16(NTW * 16) + (size_t)GX * 2 * LB * 16;
+    h->smem_y = (size_t)LDy * h->KB * (vsz + 8);
+    // rows of an assembly CTA: k4_rows interior rows plus at most one wall row
+    const int nra = (b.ny > b.k4_rows) ? b.k4_rows + 1 : b.ny + 2;
+    h->smem_i = (size_t)round16(NTW * (int)t2) + (size_t)G * 2 * LB * t2 + (size_t)b.nl * nra * b.nxp * h->esz;
+    h->smem_i64 = (size_t)round16(NTW * 16) + (size_t)G * 2 * LB * 16 + (size_t)b.nl * nra * b.nxp * 8;
     if (h->smem_i64 > 227 * 1024 || h->smem_x64 > 227 * 1024 || h->smem_y > 227 * 1024)
         return bail(OQG_EUNSUPPORTED, "grid too large for this build's shared-memory tiling");
     std::vector<Work> wv(h->nv), wx(h->nx), wy(h->nys), wi(h->ni);

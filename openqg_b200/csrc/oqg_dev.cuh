@@ -51,6 +51,7 @@ struct BasinDev {
     int pr;        // pitch of the modal right-hand side rows (elements of T)
     int pk;        // pitch of spectral rows (T for a box, complex T2 for a channel)
     int tiles_x, tiles_y;
+    int vty;       // rows per tile of the vorticity kernel
     int kt;        // 0-based topography / drag layer
     int dz_sign, tau_sign, topo_active, suppress_period;
     double dx, dy, fnot, beta;

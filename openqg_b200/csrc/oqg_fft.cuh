@@ -5,10 +5,8 @@
 // FFTs of length M over rows staged in shared memory.  Two real rows share one
 // complex transform (real and imaginary parts).  The algorithm is the Stockham
 // autosort FFT (decimation in time, e^{-2 pi i jk/M}), radices 8, 4, 2, 3 and
-// 5.  Each stage reads its R inputs into registers, synchronises, and writes
-// its outputs in place, so one buffer of M complex values serves a transform.
-// A CTA holds G transforms; TT threads serve one transform and each thread owns
-// up to E elements of it.
+// 5, ping-ponging between two shared buffers of M complex values per
+// transform.  A CTA holds G transforms; TT threads serve one transform.
 #pragma once
 
 #include "oqg_dev.cuh"
@@ -140,62 +138,83 @@ template <class T> struct Dft<T, 5> {
     }
 };
 
-// One Stockham stage of radix R on a transform of length M at z (shared).
-// All threads of the CTA must call it (it synchronises the CTA).
-template <class T, int R, int E>
-__device__ __forceinline__ void fft_stage(typename C2<T>::t *z, int M, int Ns,
-                                          const typename C2<T>::t *__restrict__ tw,
-                                          int t, int TT) {
+// Shared work buffers hold element i at fpad(i) = i + i/8: with one pad per 8
+// complex values the stride-R stores of the early Stockham stages and the
+// unit-stride loads both spread over all banks.
+__device__ __forceinline__ int fpad(int i) { return i + (i >> 3); }
+__host__ __device__ __forceinline__ int fft_buf_len(int M) { return M + (M >> 3) + 4; }
+
+// exp(-2 pi i k / M) from the two-level table tw = [B(0..63), A(0..M/64)]:
+// B[l] = exp(-2 pi i l / M), A[h] = exp(-2 pi i 64 h / M).
+template <class T>
+__device__ __forceinline__ typename C2<T>::t twiddle(const typename C2<T>::t *tw, int k) {
+    return c_mul(tw[64 + (k >> 6)], tw[k & 63]);
+}
+__host__ __device__ __forceinline__ int fft_tw_len(int M) { return 64 + (M + 63) / 64 + 1; }
+
+// One Stockham stage of radix R: src -> dst (both shared, padded, length M).
+// Threads t < TT of the transform's group each take butterflies t, t+TT, ...
+// Twiddles tw (two-level table, see twiddle) are in shared memory.
+template <class T, int R>
+__device__ __forceinline__ void fft_stage(const typename C2<T>::t *__restrict__ src,
+                                          typename C2<T>::t *__restrict__ dst, int M, int Ns,
+                                          const typename C2<T>::t *__restrict__ tw, int t, int TT) {
     typedef typename C2<T>::t T2;
-    constexpr int BMAX = (E + R - 1) / R;
-    T2 v[BMAX][R];
     const int nb = M / R;
     const int tstep = M / (Ns * R);
-    const bool act = t < TT;
+    for (int j = t; j < nb; j += TT) {
+        const int q = j / Ns, jm = j - q * Ns;
+        T2 v[R];
 #pragma unroll
-    for (int b = 0; b < BMAX; ++b) {
-        int j = t + b * TT;
-        if (act && j < nb) {
-            int jm = j % Ns;
-            v[b][0] = z[j];
+        for (int r = 0; r < R; ++r) v[r] = src[fpad(j + r * nb)];
+        if (jm != 0) {
 #pragma unroll
-            for (int r = 1; r < R; ++r) {
-                T2 w = tw[r * jm * tstep];
-                v[b][r] = c_mul(z[j + r * nb], w);
-            }
-            Dft<T, R>::run(v[b]);
+            for (int r = 1; r < R; ++r) v[r] = c_mul(v[r], twiddle<T>(tw, r * jm * tstep));
         }
-    }
-    __syncthreads();
+        Dft<T, R>::run(v);
+        const int d = q * Ns * R + jm;
 #pragma unroll
-    for (int b = 0; b < BMAX; ++b) {
-        int j = t + b * TT;
-        if (act && j < nb) {
-            int jm = j % Ns;
-            int d = (j / Ns) * Ns * R + jm;
-#pragma unroll
-            for (int r = 0; r < R; ++r) z[d + r * Ns] = v[b][r];
-        }
+        for (int r = 0; r < R; ++r) dst[fpad(d + r * Ns)] = v[r];
     }
-    __syncthreads();
 }
 
-// Forward FFT of the transform at z (length M, radices rad[0..nrad)).
-template <class T, int E>
-__device__ void fft_smem(typename C2<T>::t *z, int M, const int *rad, int nrad,
-                         const typename C2<T>::t *__restrict__ tw, int t, int TT) {
+// Forward FFT of length M (radices rad[0..nrad)) from padded buffer a, using
+// padded buffer b as the second buffer of the ping-pong.  Returns the buffer
+// holding the result.  All threads of the CTA must call it (it synchronises
+// the CTA); threads with t >= TT only take part in the barriers.
+template <class T>
+__device__ typename C2<T>::t *fft_smem(typename C2<T>::t *a, typename C2<T>::t *b, int M,
+                                       const int *rad, int nrad,
+                                       const typename C2<T>::t *__restrict__ tw, int t, int TT) {
+    typedef typename C2<T>::t T2;
+    T2 *src = a, *dst = b;
     int Ns = 1;
     for (int s = 0; s < nrad; ++s) {
-        int R = rad[s];
+        const int R = rad[s];
         switch (R) {
-            case 8: fft_stage<T, 8, E>(z, M, Ns, tw, t, TT); break;
-            case 4: fft_stage<T, 4, E>(z, M, Ns, tw, t, TT); break;
-            case 2: fft_stage<T, 2, E>(z, M, Ns, tw, t, TT); break;
-            case 3: fft_stage<T, 3, E>(z, M, Ns, tw, t, TT); break;
-            default: fft_stage<T, 5, E>(z, M, Ns, tw, t, TT); break;
+            case 8: fft_stage<T, 8>(src, dst, M, Ns, tw, t, TT); break;
+            case 4: fft_stage<T, 4>(src, dst, M, Ns, tw, t, TT); break;
+            case 2: fft_stage<T, 2>(src, dst, M, Ns, tw, t, TT); break;
+            case 3: fft_stage<T, 3>(src, dst, M, Ns, tw, t, TT); break;
+            default: fft_stage<T, 5>(src, dst, M, Ns, tw, t, TT); break;
         }
+        __syncthreads();
+        T2 *x = src; src = dst; dst = x;
         Ns *= R;
     }
+    return src;
+}
+
+// 16-byte cp.async of n bytes (n a multiple of 16, both addresses 16-byte
+// aligned) by threads t < TT.
+__device__ __forceinline__ void cp_async_16(void *dst, const void *src, int nbytes, int t, int TT) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(dst);
+    const char *g = (const char *)src;
+    for (int o = t * 16; o < nbytes; o += TT * 16)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa + o), "l"(g + o) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit_wait_all() {
+    asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
 }
 
 }  // namespace oqg

@@ -27,6 +27,12 @@ namespace oqg {
 // ------------------------------------------------------------------ helpers
 template <class T> __device__ __forceinline__ T ldg(const T *p) { return __ldg(p); }
 
+// Programmatic dependent launch: the next kernel of the step may be scheduled
+// now; and wait until the previous kernel's results are visible.  Without the
+// launch attribute both are no-ops.
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 __device__ __forceinline__ double shfl_up_d(double v, int o) { return __shfl_up_sync(0xffffffffu, v, o); }
 __device__ __forceinline__ double shfl_dn_d(double v, int o) { return __shfl_down_sync(0xffffffffu, v, o); }
 
@@ -56,27 +62,36 @@ __device__ __forceinline__ double block_sum(double v, double *red) {
 
 // ------------------------------------------------------------------ k_vort
 #define VTX 64
-#define VTY 16
+#define VTYMAX 17
 #define VTHREADS 256
+
+// Geometry scalars of a basin held in registers by the stencil kernels.
+template <class T> struct Geo {
+    int nxp, nyp, cyclic;
+    T fx, fy, fxb, fyb, jac;
+    __device__ __forceinline__ explicit Geo(const BasinDev &b)
+        : nxp(b.nxp), nyp(b.nyp), cyclic(b.cyclic), fx((T)b.fx), fy((T)b.fy), fxb((T)b.fx_bc),
+          fyb((T)b.fy_bc), jac((T)b.jac_fac) {}
+};
 
 // Laplacian with the mixed wall condition (del2_P_bc, numerics.F90:410-468) at
 // tile point (r, c) of s (leading dimension ld); gi, gj are global indices
-// (canonical columns for a channel).
+// (for a channel only gj matters).
 template <class T>
-__device__ __forceinline__ T lap_bc(const T *s, int ld, int r, int c, int gi, int gj,
-                                    const BasinDev &b) {
-    const T fx = (T)b.fx, fy = (T)b.fy, fxb = (T)b.fx_bc, fyb = (T)b.fy_bc;
+__device__ __forceinline__ T lap_bc(const T *s, int ld, int r, int c, int gi, int gj, const Geo<T> &g) {
     const T v = s[r * ld + c];
+    const bool zrow = (gj == 0 || gj == g.nyp - 1);
+    const bool wall_x = !g.cyclic && (gi == 0 || gi == g.nxp - 1);
+    if (!zrow && !wall_x)
+        return g.fx * (s[r * ld + c - 1] + s[r * ld + c + 1] - (T)2 * v) +
+               g.fy * (s[(r - 1) * ld + c] + s[(r + 1) * ld + c] - (T)2 * v);
     T xp, yp;
-    const bool wall_x = !b.cyclic && (gi == 0 || gi == b.nxp - 1);
-    if (gj == 0 || gj == b.nyp - 1) xp = (T)0;
-    else if (!b.cyclic && gi == 0) xp = fxb * (s[r * ld + c + 1] - v);
-    else if (!b.cyclic && gi == b.nxp - 1) xp = -(fxb * (v - s[r * ld + c - 1]));
-    else xp = fx * (s[r * ld + c - 1] + s[r * ld + c + 1] - (T)2 * v);
+    if (zrow) xp = (T)0;
+    else if (gi == 0) xp = g.fxb * (s[r * ld + c + 1] - v);
+    else xp = -(g.fxb * (v - s[r * ld + c - 1]));
     if (wall_x) yp = (T)0;
-    else if (gj == 0) yp = fyb * (s[(r + 1) * ld + c] - v);
-    else if (gj == b.nyp - 1) yp = -(fyb * (v - s[(r - 1) * ld + c]));
-    else yp = fy * (s[(r - 1) * ld + c] + s[(r + 1) * ld + c] - (T)2 * v);
+    else if (gj == 0) yp = g.fyb * (s[(r + 1) * ld + c] - v);
+    else yp = -(g.fyb * (v - s[(r - 1) * ld + c]));
     return xp + yp;
 }
 
@@ -84,9 +99,9 @@ __device__ __forceinline__ T lap_bc(const T *s, int ld, int r, int c, int gi, in
 // the halo-1 tiles sp, sq.
 template <class T>
 __device__ __forceinline__ T arakawa(const T *sp, const T *sq, int ld, int r, int c, int gi,
-                                     int gj, const BasinDev &b) {
-    const bool zx = !b.cyclic && (gi == 0 || gi == b.nxp - 1);   // dPdx_2 = 0 here
-    const bool zy = (gj == 0 || gj == b.nyp - 1);                 // dPdy_2 = 0 here
+                                     int gj, const Geo<T> &g) {
+    const bool zx = !g.cyclic && (gi == 0 || gi == g.nxp - 1);   // dPdx_2 = 0 here
+    const bool zy = (gj == 0 || gj == g.nyp - 1);                 // dPdy_2 = 0 here
 #define SP(rr, cc) sp[(rr) * ld + (cc)]
 #define SQ(rr, cc) sq[(rr) * ld + (cc)]
     T pxc = zx ? (T)0 : SP(r, c + 1) - SP(r, c - 1);
@@ -117,46 +132,73 @@ __device__ __forceinline__ T arakawa(const T *sp, const T *sq, int ld, int r, in
 #undef SP
 #undef SQ
     T t = qxc * pyc - qyc * pxc + A - Bv + C - D;
-    return (T)b.jac_fac * t;
+    return g.jac * t;
 }
 
-// Loads rows [jlo, jlo+nr) x cols [ilo, ilo+nc) of layer k of field f into s
-// (leading dimension nc); outside the basin -> 0; channel columns wrap.
+// cp.async copy of one element into shared memory; zero-filled when !valid
+// (the source is then not read).
 template <class T>
-__device__ __forceinline__ void load_tile(T *s, const T *__restrict__ f, const BasinDev &b, int k,
-                                          int jlo, int nr, int ilo, int nc) {
-    const int N = b.nxp - 1;
-    for (int idx = threadIdx.x; idx < nr * nc; idx += blockDim.x) {
-        int r = idx / nc, c = idx - r * nc;
-        int j = jlo + r, i = ilo + c;
-        T v = (T)0;
-        if (j >= 0 && j < b.nyp) {
-            if (b.cyclic) {
-                i %= N;
-                if (i < 0) i += N;
-                v = ldg(f + ((size_t)k * b.nyp + j) * b.px + i);
-            } else if (i >= 0 && i < b.nxp) {
-                v = ldg(f + ((size_t)k * b.nyp + j) * b.px + i);
+__device__ __forceinline__ void cp_async_el(T *dst, const T *src, bool valid) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(dst);
+    const int n = valid ? (int)sizeof(T) : 0;
+    if (sizeof(T) == 8)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(src), "r"(n) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(sa), "l"(src), "r"(n) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N> __device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// Queues the copy of rows [jlo, jlo+nr) x cols [ilo, ilo+nc) of layer k of f
+// into s (leading dimension nc); outside the basin -> 0; channel columns wrap.
+// Thread layout: 64 columns x 4 rows.
+template <class T>
+__device__ __forceinline__ void load_tile_async(T *s, const T *__restrict__ f, const Geo<T> &g, int px,
+                                                int k, int jlo, int nr, int ilo, int nc) {
+    const int N = g.nxp - 1;
+    const int tx = threadIdx.x & 63, ty = threadIdx.x >> 6;
+    const T *fk = f + (size_t)k * g.nyp * px;
+    for (int r = ty; r < nr; r += 4) {
+        const int j = jlo + r;
+        const bool jv = (j >= 0 && j < g.nyp);
+        const T *row = fk + (size_t)(jv ? j : 0) * px;
+        for (int c = tx; c < nc; c += 64) {
+            int i = ilo + c;
+            bool v = jv;
+            if (g.cyclic) {
+                while (i < 0) i += N;
+                while (i >= N) i -= N;
+            } else {
+                v = v && i >= 0 && i < g.nxp;
             }
+            cp_async_el(s + r * nc + c, row + (v ? i : 0), v);
         }
-        s[idx] = v;
     }
 }
 
+// Tiles are VTX columns by b.vty rows (b.vty <= VTYMAX, chosen per basin so
+// the tiles fill whole waves); 256 threads as 64 columns x 4 rows.
 template <class T, int NL>
-__global__ void __launch_bounds__(VTHREADS)
+__global__ void __launch_bounds__(VTHREADS, 2)
 k_vort(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par, double tdt) {
+    constexpr int WPM = VTX + 6, W2 = VTX + 4, W1 = VTX + 2;
+    constexpr int UMAX = (VTYMAX + 3) / 4;
     const Work w = work[blockIdx.x];
     const BasinDev &b = bas[w.member];
+    const Geo<T> g(b);
+    const int VT = b.vty;
+    const int HPM = VT + 6, H2 = VT + 4, H1 = VT + 2;
+    const int NBUF = HPM * WPM + 2 * H1 * W1 + VT * VTX;   // one layer's inputs
     const int tile_x = w.block % b.tiles_x, tile_y = w.block / b.tiles_x;
-    const int i0 = tile_x * VTX, j0 = tile_y * VTY;
+    const int i0 = tile_x * VTX, j0 = tile_y * VT;
 
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    T *sPM = reinterpret_cast<T *>(smem_raw);
-    T *sD2 = sPM + (VTY + 6) * (VTX + 6);
-    T *sD4 = sD2 + (VTY + 4) * (VTX + 4);
-    T *sP = sD4 + (VTY + 2) * (VTX + 2);
-    T *sQ = sP + (VTY + 2) * (VTX + 2);
+    T *buf0 = reinterpret_cast<T *>(smem_raw);
+    T *sD2 = buf0 + 2 * NBUF;
+    T *sD4 = sD2 + H2 * W2;
+    T *sWK = sD4 + H1 * W1;
     __shared__ double red[32];
 
     const T *P = (const T *)b.F[par];
@@ -165,125 +207,144 @@ k_vort(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par,
     T *QM = (T *)b.F[3 - par];
     const T *WEK = (const T *)b.wekp;
     const T *ENT = (const T *)b.ent;
-    const int N = b.nxp - 1;
+    const int N = g.nxp - 1;
+    const int nyp = g.nyp, nxp = g.nxp, px = b.px, kt = b.kt;
+    const int tx = threadIdx.x & 63, ty0 = threadIdx.x >> 6;
 
-    double acc[4][NL];
+    pdl_trigger();
+    pdl_wait();
+    auto issue = [&](int k) {
+        T *bf = buf0 + (k & 1) * NBUF;
+        load_tile_async(bf, PM, g, px, k, j0 - 3, HPM, i0 - 3, WPM);
+        load_tile_async(bf + HPM * WPM, P, g, px, k, j0 - 1, H1, i0 - 1, W1);
+        load_tile_async(bf + HPM * WPM + H1 * W1, Q, g, px, k, j0 - 1, H1, i0 - 1, W1);
+        load_tile_async(bf + HPM * WPM + 2 * H1 * W1, (const T *)QM, g, px, k, j0, VT, i0, VTX);
+        if (k == 0) load_tile_async(sWK, WEK, g, px, 0, j0, VT, i0, VTX);
+        cp_async_commit();
+    };
+    issue(0);
+
+    // per-point constants, hoisted out of the layer loop
+    double ctl[NL * NL];
 #pragma unroll
-    for (int u = 0; u < 4; ++u)
+    for (int x = 0; x < NL * NL; ++x) ctl[x] = b.ctl2m[x];
+    double acc[UMAX][NL], by[UMAX];
+#pragma unroll
+    for (int u = 0; u < UMAX; ++u) {
+        const int gj = j0 + ty0 + 4 * u;
+        by[u] = (gj < nyp) ? b.beta * b.yprel[gj] : 0.0;
 #pragma unroll
         for (int m = 0; m < NL; ++m) acc[u][m] = 0.0;
+    }
+    const T c_ent1 = (T)b.c_ent1, c_wind = (T)b.c_wind, c_ent2 = (T)b.c_ent2, c_drag = (T)b.c_drag;
+    const T ttdt = (T)tdt;
+    const bool topo = b.topo_active != 0;
 
-    const int tx = threadIdx.x & (VTX - 1);
-    const int ty0 = threadIdx.x >> 6;   // 0..3
     // channel strip integrals are formed by tiles holding rows 0, 1, nyp-2, nyp-1
-    const bool strips = b.cyclic &&
-        (j0 <= 1 || j0 + VTY > b.nyp - 2);
+    const bool strips = g.cyclic && (j0 <= 1 || j0 + VT > nyp - 2);
 
 #pragma unroll 1
     for (int k = 0; k < NL; ++k) {
-        load_tile(sPM, PM, b, k, j0 - 3, VTY + 6, i0 - 3, VTX + 6);
-        load_tile(sP, P, b, k, j0 - 1, VTY + 2, i0 - 1, VTX + 2);
-        load_tile(sQ, Q, b, k, j0 - 1, VTY + 2, i0 - 1, VTX + 2);
+        if (k + 1 < NL) {
+            issue(k + 1);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
         __syncthreads();
+        const T *sPM = buf0 + (k & 1) * NBUF;
+        const T *sP = sPM + HPM * WPM;
+        const T *sQ = sP + H1 * W1;
+        const T *sQM = sQ + H1 * W1;
         // del2p on the halo-2 region
-        for (int idx = threadIdx.x; idx < (VTY + 4) * (VTX + 4); idx += blockDim.x) {
-            int r = idx / (VTX + 4), c = idx - r * (VTX + 4);
-            int gj = j0 - 2 + r, gi = i0 - 2 + c;
-            T v = (T)0;
-            if (gj >= 0 && gj < b.nyp) {
-                if (b.cyclic) {
-                    int ci = gi % N; if (ci < 0) ci += N;
-                    v = lap_bc(sPM, VTX + 6, r + 1, c + 1, ci, gj, b);
-                } else if (gi >= 0 && gi < b.nxp) {
-                    v = lap_bc(sPM, VTX + 6, r + 1, c + 1, gi, gj, b);
-                }
+        for (int r = ty0; r < H2; r += 4) {
+            const int gj = j0 - 2 + r;
+            const bool jv = gj >= 0 && gj < nyp;
+            for (int c = tx; c < W2; c += 64) {
+                const int gi = i0 - 2 + c;
+                T v = (T)0;
+                if (jv && (g.cyclic || (gi >= 0 && gi < nxp))) v = lap_bc(sPM, WPM, r + 1, c + 1, gi, gj, g);
+                sD2[r * W2 + c] = v;
             }
-            sD2[idx] = v;
         }
         __syncthreads();
         // d4p on the halo-1 region
-        for (int idx = threadIdx.x; idx < (VTY + 2) * (VTX + 2); idx += blockDim.x) {
-            int r = idx / (VTX + 2), c = idx - r * (VTX + 2);
-            int gj = j0 - 1 + r, gi = i0 - 1 + c;
-            T v = (T)0;
-            if (gj >= 0 && gj < b.nyp) {
-                if (b.cyclic) {
-                    int ci = gi % N; if (ci < 0) ci += N;
-                    v = lap_bc(sD2, VTX + 4, r + 1, c + 1, ci, gj, b);
-                } else if (gi >= 0 && gi < b.nxp) {
-                    v = lap_bc(sD2, VTX + 4, r + 1, c + 1, gi, gj, b);
-                }
+        for (int r = ty0; r < H1; r += 4) {
+            const int gj = j0 - 1 + r;
+            const bool jv = gj >= 0 && gj < nyp;
+            for (int c = tx; c < W1; c += 64) {
+                const int gi = i0 - 1 + c;
+                T v = (T)0;
+                if (jv && (g.cyclic || (gi >= 0 && gi < nxp))) v = lap_bc(sD2, W2, r + 1, c + 1, gi, gj, g);
+                sD4[r * W1 + c] = v;
             }
-            sD4[idx] = v;
         }
         __syncthreads();
 
         double sq[OQG_NQ];
 #pragma unroll
         for (int q = 0; q < OQG_NQ; ++q) sq[q] = 0.0;
+        const T c2 = (T)b.c2[k], c4 = (T)b.c4[k];
 
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
+        for (int u = 0; u < UMAX; ++u) {
             const int ty = ty0 + 4 * u;
             const int gj = j0 + ty, gi = i0 + tx;
-            if (gj >= b.nyp || gi >= b.nxp) continue;
-            int ci = gi;
-            if (b.cyclic && ci == N) ci = 0;
-            T d4 = sD4[(ty + 1) * (VTX + 2) + tx + 1];
-            T d6 = lap_bc(sD4, VTX + 2, ty + 1, tx + 1, ci, gj, b);
-            T jac = arakawa(sP, sQ, VTX + 2, ty + 1, tx + 1, ci, gj, b);
-            T dq = jac + (T)b.c2[k] * d4 - (T)b.c4[k] * d6;
-            const size_t o2 = (size_t)gj * b.px + gi;
+            if (ty >= VT || gj >= nyp || gi >= nxp) continue;
+            const T d4 = sD4[(ty + 1) * W1 + tx + 1];
+            const T d6 = lap_bc(sD4, W1, ty + 1, tx + 1, gi, gj, g);
+            const T jac = arakawa(sP, sQ, W1, ty + 1, tx + 1, gi, gj, g);
+            T dq = jac + c2 * d4 - c4 * d6;
+            const size_t o2 = (size_t)gj * px + gi;
             if (k == 0) {
-                T e1 = ENT ? ldg(ENT + o2) : (T)0;
-                dq = dq + (T)b.c_ent1 * e1 + (T)b.c_wind * ldg(WEK + o2);
+                const T e1 = ENT ? ldg(ENT + o2) : (T)0;
+                dq = dq + c_ent1 * e1 + c_wind * sWK[ty * VTX + tx];
             }
-            if (k == 1 && ENT) dq = dq - (T)b.c_ent2 * ldg(ENT + o2);
-            T d2 = sD2[(ty + 2) * (VTX + 4) + tx + 2];
-            if (k == b.kt) dq = dq - (T)b.c_drag * d2;
-            const size_t o3 = ((size_t)k * b.nyp + gj) * b.px + gi;
-            T qn = QM[o3] + (T)tdt * dq;
-            QM[o3] = qn;
+            if (k == 1 && ENT) dq = dq - c_ent2 * ldg(ENT + o2);
+            const T d2 = sD2[(ty + 2) * W2 + tx + 2];
+            if (k == kt) dq = dq - c_drag * d2;
+            const T qn = sQM[ty * VTX + tx] + ttdt * dq;
+            QM[((size_t)k * nyp + gj) * px + gi] = qn;
             // modal right-hand side, FP64 (p_modes_rhs)
-            double ql = (double)qn - b.beta * b.yprel[gj];
-            if (k == b.kt && b.topo_active) ql -= b.ddyn[(size_t)gj * b.px + gi];
+            double ql = (double)qn - by[u];
+            if (k == kt && topo) ql -= b.ddyn[o2];
 #pragma unroll
-            for (int m = 0; m < NL; ++m) acc[u][m] += ql * b.ctl2m[k + NL * m];
+            for (int m = 0; m < NL; ++m) acc[u][m] += ql * ctl[k + NL * m];
             if (strips && gi < N) {
                 // channel strip integrands (vorticity.F90:84-101, numerics.F90:374-386)
-                const int ld = VTX + 2, r = ty + 1, c = tx + 1;
+                const int r = ty + 1, c = tx + 1;
                 if (gj == 0) {
-                    T px1 = sP[(r + 1) * ld + c + 1] - sP[(r + 1) * ld + c - 1];
-                    sq[0] += (double)(sQ[r * ld + c] * px1);
-                    sq[4] += (double)(sD2[(ty + 3) * (VTX + 4) + tx + 2] - d2);
-                    sq[6] += (double)(sD4[(ty + 2) * (VTX + 2) + tx + 1] - d4);
-                    if (k == b.kt)
-                        sq[8] += (double)(sPM[(ty + 4) * (VTX + 6) + tx + 3] - sPM[(ty + 3) * (VTX + 6) + tx + 3]);
+                    const T px1 = sP[(r + 1) * W1 + c + 1] - sP[(r + 1) * W1 + c - 1];
+                    sq[0] += (double)(sQ[r * W1 + c] * px1);
+                    sq[4] += (double)(sD2[(ty + 3) * W2 + tx + 2] - d2);
+                    sq[6] += (double)(sD4[(ty + 2) * W1 + tx + 1] - d4);
+                    if (k == kt)
+                        sq[8] += (double)(sPM[(ty + 4) * WPM + tx + 3] - sPM[(ty + 3) * WPM + tx + 3]);
                 }
                 if (gj == 1) {
-                    T px1 = sP[r * ld + c + 1] - sP[r * ld + c - 1];
-                    sq[1] += (double)(sQ[r * ld + c] * px1);
+                    const T px1 = sP[r * W1 + c + 1] - sP[r * W1 + c - 1];
+                    sq[1] += (double)(sQ[r * W1 + c] * px1);
                 }
-                if (gj == b.nyp - 1) {
-                    T pxs = sP[(r - 1) * ld + c + 1] - sP[(r - 1) * ld + c - 1];
-                    sq[2] += (double)(sQ[r * ld + c] * pxs);
-                    sq[5] += (double)(d2 - sD2[(ty + 1) * (VTX + 4) + tx + 2]);
-                    sq[7] += (double)(d4 - sD4[ty * (VTX + 2) + tx + 1]);
-                    if (k == b.kt)
-                        sq[9] += (double)(sPM[(ty + 3) * (VTX + 6) + tx + 3] - sPM[(ty + 2) * (VTX + 6) + tx + 3]);
+                if (gj == nyp - 1) {
+                    const T pxs = sP[(r - 1) * W1 + c + 1] - sP[(r - 1) * W1 + c - 1];
+                    sq[2] += (double)(sQ[r * W1 + c] * pxs);
+                    sq[5] += (double)(d2 - sD2[(ty + 1) * W2 + tx + 2]);
+                    sq[7] += (double)(d4 - sD4[ty * W1 + tx + 1]);
+                    if (k == kt)
+                        sq[9] += (double)(sPM[(ty + 3) * WPM + tx + 3] - sPM[(ty + 2) * WPM + tx + 3]);
                 }
-                if (gj == b.nyp - 2) {
-                    T px1 = sP[r * ld + c + 1] - sP[r * ld + c - 1];
-                    sq[3] += (double)(sQ[r * ld + c] * px1);
+                if (gj == nyp - 2) {
+                    const T px1 = sP[r * W1 + c + 1] - sP[r * W1 + c - 1];
+                    sq[3] += (double)(sQ[r * W1 + c] * px1);
                 }
             }
         }
         if (strips) {
             double *pt = b.part_tile + ((size_t)w.block * b.nl + k) * OQG_NQ;
-#pragma unroll 1
+#pragma unroll
             for (int q = 0; q < OQG_NQ; ++q) {
-                double s = block_sum(sq[q], red);
-                if (threadIdx.x == 0) pt[q] = s;
+                double sv = block_sum(sq[q], red);
+                if (threadIdx.x == 0) pt[q] = sv;
             }
         }
         __syncthreads();
@@ -291,73 +352,90 @@ k_vort(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par,
 
     // write the modal right-hand side of the interior points
     T *RHS = (T *)b.rhs;
-    const int ioff = b.cyclic ? 0 : 1;
+    const int ioff = g.cyclic ? 0 : 1;
+    const double f0 = b.fnot;
 #pragma unroll
-    for (int u = 0; u < 4; ++u) {
-        const int gj = j0 + ty0 + 4 * u, gi = i0 + tx;
-        if (gj < 1 || gj > b.nyp - 2) continue;
+    for (int u = 0; u < UMAX; ++u) {
+        const int ty = ty0 + 4 * u;
+        const int gj = j0 + ty, gi = i0 + tx;
+        if (ty >= VT || gj < 1 || gj > nyp - 2) continue;
         const int xi = gi - ioff;
         if (xi < 0 || xi >= b.nxin) continue;
 #pragma unroll
         for (int m = 0; m < NL; ++m)
-            RHS[((size_t)m * b.ny + (gj - 1)) * b.pr + xi] = (T)(b.fnot * acc[u][m]);
+            RHS[((size_t)m * b.ny + (gj - 1)) * b.pr + xi] = (T)(f0 * acc[u][m]);
     }
 }
 
 // ------------------------------------------------------------------ k_xfwd
 // Threads per transform TT = ceil(M/E); G = blockDim/TT transforms per CTA.
+// Shared memory: the twiddle table, then per group two padded buffers of
+// fft_buf_len(M) complex values; the input rows are staged by cp.async into
+// the second buffer and expanded into the first.
+__host__ __device__ __forceinline__ int round16(int bytes) { return (bytes + 15) & ~15; }
+
 template <class T, int E>
-__global__ void k_xfwd(const BasinDev *__restrict__ bas, const Work *__restrict__ work,
-                       const void *rhs_override) {
+__global__ void __launch_bounds__(256, 3)
+k_xfwd(const BasinDev *__restrict__ bas, const Work *__restrict__ work, const void *rhs_override) {
     typedef typename C2<T>::t T2;
     const Work w = work[blockIdx.x];
     const BasinDev &b = bas[w.member];
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    T2 *zs = reinterpret_cast<T2 *>(smem_raw);
     const int M = b.M, TT = (M + E - 1) / E, G = blockDim.x / TT;
     const int g = threadIdx.x / TT, t = threadIdx.x - g * TT;
+    const int LB = fft_buf_len(M), NTW = fft_tw_len(M);
+    T2 *sTw = reinterpret_cast<T2 *>(smem_raw);
+    T2 *zs = reinterpret_cast<T2 *>(smem_raw + round16(NTW * (int)sizeof(T2)));
     const int npm = (b.ny + 1) >> 1;          // row pairs per mode
     const int pair = w.block * G + g;
     const bool live = g < G && pair < b.nl * npm;
     const int m = live ? pair / npm : 0;
     const int j = live ? 2 * (pair - m * npm) : 0;
     const bool two = live && (j + 1 < b.ny);
-    T2 *z = zs + (size_t)(g < G ? g : 0) * M;
+    T2 *za = zs + (size_t)(g < G ? g : 0) * 2 * LB;
+    T2 *zb = za + LB;
+    T *raw = reinterpret_cast<T *>(zb);
+    const int n = b.nxin;
+    const int RO = (n + 3) & ~3;              // offset of the second row (16-byte aligned)
     const T *R = (const T *)(rhs_override ? rhs_override : b.rhs);
     const T *x = R + ((size_t)m * b.ny + j) * b.pr;
-    const T *y = x + b.pr;
-    const T2 *tw = (const T2 *)b.tw;
-    const int n = b.nxin;
-    if (!b.cyclic) {
-        // odd extension of two rows: z_0 = z_{n+1} = 0, z_{M-jj} = -z_jj
-        if (live) {
+    pdl_trigger();
+    cp_async_16(sTw, b.tw, round16(NTW * (int)sizeof(T2)), threadIdx.x, blockDim.x);   // constant
+    pdl_wait();
+    if (live) {
+        cp_async_16(raw, x, round16(n * (int)sizeof(T)), t, TT);
+        if (two) cp_async_16(raw + RO, x + b.pr, round16(n * (int)sizeof(T)), t, TT);
+    }
+    cp_async_commit_wait_all();
+    __syncthreads();
+    if (live) {
+        if (!b.cyclic) {
+            // odd extension of two rows: z_0 = z_{n+1} = 0, z_{M-jj} = -z_jj
             for (int jj = t; jj < M; jj += TT) {
                 T2 v;
                 if (jj == 0 || jj == n + 1) { v.x = (T)0; v.y = (T)0; }
-                else if (jj <= n) { v.x = x[jj - 1]; v.y = two ? y[jj - 1] : (T)0; }
-                else { int s = M - jj; v.x = -x[s - 1]; v.y = two ? -y[s - 1] : (T)0; }
-                z[jj] = v;
+                else if (jj <= n) { v.x = raw[jj - 1]; v.y = two ? raw[RO + jj - 1] : (T)0; }
+                else { const int s2 = M - jj; v.x = -raw[s2 - 1]; v.y = two ? -raw[RO + s2 - 1] : (T)0; }
+                za[fpad(jj)] = v;
             }
-        }
-    } else {
-        if (live) {
+        } else {
             for (int jj = t; jj < M; jj += TT) {
                 T2 v;
-                v.x = x[jj];
-                v.y = two ? y[jj] : (T)0;
-                z[jj] = v;
+                v.x = raw[jj];
+                v.y = two ? raw[RO + jj] : (T)0;
+                za[fpad(jj)] = v;
             }
         }
     }
     __syncthreads();
-    fft_smem<T, E>(z, M, b.rad, b.nrad, tw, live ? t : TT, TT);
+    T2 *z = fft_smem<T>(za, zb, M, b.rad, b.nrad, sTw, live ? t : TT, TT);
     if (!live) return;
     if (!b.cyclic) {
         T *S = (T *)b.spec;
         T *sx = S + ((size_t)m * b.ny + j) * b.pk;
         T *sy = sx + b.pk;
         for (int kk = t; kk < n; kk += TT) {
-            T2 v = z[kk + 1];
+            const T2 v = z[fpad(kk + 1)];
             sx[kk] = -v.y;
             if (two) sy[kk] = v.x;
         }
@@ -366,12 +444,12 @@ __global__ void k_xfwd(const BasinDev *__restrict__ bas, const Work *__restrict_
         T2 *sx = S + ((size_t)m * b.ny + j) * b.pk;
         T2 *sy = sx + b.pk;
         for (int kk = t; kk < b.nk; kk += TT) {
-            T2 a = z[kk], c = z[(M - kk) % M];
+            const T2 a = z[fpad(kk)], c = z[fpad((M - kk) % M)];
             T2 X, Y;
             X.x = (T)0.5 * (a.x + c.x);
             X.y = (T)0.5 * (a.y - c.y);
             // (a - conj(c)) / (2i)
-            T dx_ = (T)0.5 * (a.x - c.x), dy_ = (T)0.5 * (a.y + c.y);
+            const T dx_ = (T)0.5 * (a.x - c.x), dy_ = (T)0.5 * (a.y + c.y);
             Y.x = dy_;
             Y.y = -dx_;
             sx[kk] = X;
@@ -418,94 +496,171 @@ __device__ __forceinline__ double yt_re(double2 v) { return v.x; }
 template <class T, int NL> __device__ void scalar_phase(const BasinDev &b, double tdt);
 
 template <class T, bool CPLX, int NL>
-__global__ void k_ysolve(const BasinDev *__restrict__ bas, const Work *__restrict__ work,
-                         double tdt, int do_scalar) {
+__global__ void __launch_bounds__(128)
+k_ysolve(const BasinDev *__restrict__ bas, const Work *__restrict__ work,
+         double tdt, int do_scalar) {
     typedef typename YT<T, CPLX>::v V;
     typedef typename YT<T, CPLX>::g Gm;
+    constexpr int KB = 4;                       // columns (warps) per CTA
+    constexpr int CH = 16;                      // rows per unrolled chunk
     const Work w = work[blockIdx.x];
     const BasinDev &b = bas[w.member];
-    const int KB = blockDim.x >> 5;
     const int lane = threadIdx.x & 31, c = threadIdx.x >> 5;
-    const int nkb = (b.nk + KB - 1) / KB;
+    const int nk = b.nk, ny = b.ny, pk = b.pk;
+    const int nkb = (nk + KB - 1) / KB;
     const int m = w.block / nkb, k0 = (w.block - m * nkb) * KB;
-    const int ny = b.ny;
+    // Lane `l` owns rows [l S, l S + S).  Columns are stored with one pad word
+    // per S rows (row j at j + j / S), so the 32 lanes of a warp reading their
+    // chunks hit distinct banks.
+    const int S_ = (ny + 31) >> 5;
+    const int LD = (ny + 32) | 1;            // > (ny-1) + (ny-1)/S, odd
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    V *tile = reinterpret_cast<V *>(smem_raw);   // [ny][KB]
+    V *tile = reinterpret_cast<V *>(smem_raw);                 // [KB][LD]
+    double *pvs = reinterpret_cast<double *>(tile + KB * LD);  // [KB][LD] pivots
     __shared__ int s_last;
 
-    Gm *S = (Gm *)b.spec + (size_t)m * ny * b.pk;
-    // load (coalesced along k)
-    for (int idx = threadIdx.x; idx < ny * KB; idx += blockDim.x) {
-        int jj = idx / KB, cc = idx - jj * KB;
-        int k = k0 + cc;
-        tile[idx] = k < b.nk ? yt_load(S[(size_t)jj * b.pk + k]) : yt_zero(V());
+    const int k = k0 + c;
+    const bool live = k < nk;
+    const int pidx = m * nk + (live ? k : 0);
+    // this warp's pivots (constant data), 16 loads in flight per lane; beyond
+    // the stored length a pivot repeats its fixed point
+    {
+        const double *piv = b.piv_tab + b.piv_off[pidx];
+        const int plen = b.piv_len[pidx];
+        for (int j0 = lane; j0 < ny; j0 += 32 * CH) {
+            double v[CH];
+#pragma unroll
+            for (int u = 0; u < CH; ++u) {
+                const int jj = j0 + 32 * u;
+                v[u] = jj < ny ? piv[min(jj, plen - 1)] : 0.0;
+            }
+#pragma unroll
+            for (int u = 0; u < CH; ++u) {
+                const int jj = j0 + 32 * u;
+                if (jj < ny) pvs[c * LD + jj + jj / S_] = v[u];
+            }
+        }
+    }
+    Gm *S = (Gm *)b.spec + (size_t)m * ny * pk;
+    pdl_trigger();
+    pdl_wait();
+    // load the spectral columns: thread -> (row, column), coalesced along k
+    for (int i0 = threadIdx.x; i0 < ny * KB; i0 += 128 * CH) {
+        V v[CH];
+#pragma unroll
+        for (int u = 0; u < CH; ++u) {
+            const int idx = i0 + 128 * u;
+            const int jj = idx >> 2, cc = idx & 3, kk = k0 + cc;
+            v[u] = (idx < ny * KB && kk < nk) ? yt_load(S[(size_t)jj * pk + kk]) : yt_zero(V());
+        }
+#pragma unroll
+        for (int u = 0; u < CH; ++u) {
+            const int idx = i0 + 128 * u;
+            const int jj = idx >> 2, cc = idx & 3;
+            if (idx < ny * KB) tile[cc * LD + jj + jj / S_] = v[u];
+        }
     }
     __syncthreads();
 
-    const int k = k0 + c;
-    if (k < b.nk) {
+    double wsum = 0.0;                          // dst_w-weighted column sum (box)
+    if (live) {
         const double a = b.a_tri;
-        const int pidx = m * b.nk + k;
-        const double *piv = b.piv_tab + b.piv_off[pidx];
-        const int plen = b.piv_len[pidx];
-        const int S_ = (ny + 31) >> 5;
+        V *col = tile + c * LD;
+        const double *pc = pvs + c * LD;
         const int s = lane * S_, e = min(s + S_, ny);
+        const int o = lane * (S_ + 1);          // padded offset of row s
+        const int n = max(e - s, 0);
         // forward elimination: u_j = f_j beta_j - a beta_j u_{j-1}
         V C = yt_zero(V());
         double D = 1.0;
-        for (int jj = s; jj < e; ++jj) {
-            double bt = piv[min(jj, plen - 1)];
-            V f = tile[jj * KB + c];
-            C = yt_axpy(yt_scale(f, bt), -a * bt, C);
-            D = -a * bt * D;
+        for (int t0 = 0; t0 < n; t0 += CH) {
+            double bt[CH];
+            V f[CH];
+#pragma unroll
+            for (int u = 0; u < CH; ++u)
+                if (t0 + u < n) { bt[u] = pc[o + t0 + u]; f[u] = col[o + t0 + u]; }
+#pragma unroll
+            for (int u = 0; u < CH; ++u)
+                if (t0 + u < n) { C = yt_axpy(yt_scale(f[u], bt[u]), -a * bt[u], C); D = -a * bt[u] * D; }
         }
-        for (int o = 1; o < 32; o <<= 1) {
-            V Co = yt_up(C, o);
-            double Do = shfl_up_d(D, o);
-            if (lane >= o) { C = yt_axpy(C, D, Co); D = D * Do; }
+        for (int q = 1; q < 32; q <<= 1) {
+            V Co = yt_up(C, q);
+            double Do = shfl_up_d(D, q);
+            if (lane >= q) { C = yt_axpy(C, D, Co); D = D * Do; }
         }
-        V u = yt_up(C, 1);
-        if (lane == 0) u = yt_zero(V());
-        for (int jj = s; jj < e; ++jj) {
-            double bt = piv[min(jj, plen - 1)];
-            V f = tile[jj * KB + c];
-            u = yt_axpy(yt_scale(f, bt), -a * bt, u);
-            tile[jj * KB + c] = u;
+        V uu = yt_up(C, 1);
+        if (lane == 0) uu = yt_zero(V());
+        for (int t0 = 0; t0 < n; t0 += CH) {
+            double bt[CH];
+            V f[CH];
+#pragma unroll
+            for (int u = 0; u < CH; ++u)
+                if (t0 + u < n) { bt[u] = pc[o + t0 + u]; f[u] = col[o + t0 + u]; }
+#pragma unroll
+            for (int u = 0; u < CH; ++u)
+                if (t0 + u < n) { uu = yt_axpy(yt_scale(f[u], bt[u]), -a * bt[u], uu); col[o + t0 + u] = uu; }
         }
         // back substitution: u_j = u'_j - a beta_j u_{j+1}
         C = yt_zero(V());
         D = 1.0;
-        for (int jj = e - 1; jj >= s; --jj) {
-            double ej = (jj == ny - 1) ? 0.0 : -a * piv[min(jj, plen - 1)];
-            C = yt_axpy(tile[jj * KB + c], ej, C);
-            D = ej * D;
+        for (int t1 = n; t1 > 0; t1 -= CH) {
+            double ej[CH];
+            V f[CH];
+#pragma unroll
+            for (int u = 0; u < CH; ++u) {
+                const int t = t1 - 1 - u;
+                if (t >= 0) { ej[u] = (s + t == ny - 1) ? 0.0 : -a * pc[o + t]; f[u] = col[o + t]; }
+            }
+#pragma unroll
+            for (int u = 0; u < CH; ++u)
+                if (t1 - 1 - u >= 0) { C = yt_axpy(f[u], ej[u], C); D = ej[u] * D; }
         }
-        for (int o = 1; o < 32; o <<= 1) {
-            V Co = yt_dn(C, o);
-            double Do = shfl_dn_d(D, o);
-            if (lane + o < 32) { C = yt_axpy(C, D, Co); D = D * Do; }
+        for (int q = 1; q < 32; q <<= 1) {
+            V Co = yt_dn(C, q);
+            double Do = shfl_dn_d(D, q);
+            if (lane + q < 32) { C = yt_axpy(C, D, Co); D = D * Do; }
         }
-        u = yt_dn(C, 1);
-        if (lane == 31) u = yt_zero(V());
+        uu = yt_dn(C, 1);
+        if (lane == 31) uu = yt_zero(V());
         double colsum = 0.0;
-        for (int jj = e - 1; jj >= s; --jj) {
-            double ej = (jj == ny - 1) ? 0.0 : -a * piv[min(jj, plen - 1)];
-            u = yt_axpy(tile[jj * KB + c], ej, u);
-            tile[jj * KB + c] = u;
-            colsum += yt_re(u);
+        for (int t1 = n; t1 > 0; t1 -= CH) {
+            double ej[CH];
+            V f[CH];
+#pragma unroll
+            for (int u = 0; u < CH; ++u) {
+                const int t = t1 - 1 - u;
+                if (t >= 0) { ej[u] = (s + t == ny - 1) ? 0.0 : -a * pc[o + t]; f[u] = col[o + t]; }
+            }
+#pragma unroll
+            for (int u = 0; u < CH; ++u) {
+                const int t = t1 - 1 - u;
+                if (t >= 0) { uu = yt_axpy(f[u], ej[u], uu); col[o + t] = uu; colsum += yt_re(uu); }
+            }
         }
-        if (!CPLX) {
-            colsum = warp_sum(colsum);
-            if (lane == 0) b.part_col[pidx] = colsum;
-        }
+        if (!CPLX) wsum = b.dst_w[k] * warp_sum(colsum);
     }
     __syncthreads();
-    for (int idx = threadIdx.x; idx < ny * KB; idx += blockDim.x) {
-        int jj = idx / KB, cc = idx - jj * KB;
-        int kk = k0 + cc;
-        if (kk < b.nk) {
-            if constexpr (CPLX) S[(size_t)jj * b.pk + kk] = yt_store2<Gm>(tile[idx]);
-            else S[(size_t)jj * b.pk + kk] = yt_store<Gm>(tile[idx]);
+    for (int i0 = threadIdx.x; i0 < ny * KB; i0 += 128 * CH) {
+#pragma unroll
+        for (int u = 0; u < CH; ++u) {
+            const int idx = i0 + 128 * u;
+            const int jj = idx >> 2, cc = idx & 3, kk = k0 + cc;
+            if (idx < ny * KB && kk < nk) {
+                if constexpr (CPLX) S[(size_t)jj * pk + kk] = yt_store2<Gm>(tile[cc * LD + jj + jj / S_]);
+                else S[(size_t)jj * pk + kk] = yt_store<Gm>(tile[cc * LD + jj + jj / S_]);
+            }
+        }
+    }
+    if (!CPLX) {
+        // one dst_w-weighted partial per CTA, summed in a fixed order
+        __shared__ double wpart[KB];
+        if (lane == 0) wpart[c] = wsum;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double t = 0.0;
+#pragma unroll
+            for (int x = 0; x < KB; ++x) t += wpart[x];
+            b.part_col[w.block] = t;
         }
     }
     if (!do_scalar) return;
@@ -524,180 +679,215 @@ __global__ void k_ysolve(const BasinDev *__restrict__ bas, const Work *__restric
 }
 
 // LU solve with the pivots of DGETRF (column-major n x n) -- DGETRS 'N'.
-template <int NL>
-__device__ void lu_solve_dev(const double *lu, const int *piv, int n, double *x) {
-    for (int i = 0; i < n; ++i)
-        if (piv[i] != i) { double t = x[i]; x[i] = x[piv[i]]; x[piv[i]] = t; }
-    for (int c = 0; c < n; ++c)
-        for (int r = c + 1; r < n; ++r) x[r] -= x[c] * lu[r + n * c];
-    for (int c = n - 1; c >= 0; --c) {
-        x[c] /= lu[c + n * c];
-        for (int r = 0; r < c; ++r) x[r] -= x[c] * lu[r + n * c];
+template <int N>
+__device__ __forceinline__ void lu_solve_dev(const double (&lu)[N * N], const int (&piv)[N], double (&x)[N]) {
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+        // row interchange i <-> piv[i]
+#pragma unroll
+        for (int r = 0; r < N; ++r)
+            if (r > i && piv[i] == r) { double t = x[i]; x[i] = x[r]; x[r] = t; }
+    }
+#pragma unroll
+    for (int c = 0; c < N; ++c)
+#pragma unroll
+        for (int r = c + 1; r < N; ++r) x[r] -= x[c] * lu[r + N * c];
+#pragma unroll
+    for (int c = N - 1; c >= 0; --c) {
+        x[c] /= lu[c + N * c];
+#pragma unroll
+        for (int r = 0; r < c; ++r) x[r] -= x[c] * lu[r + N * c];
     }
 }
 
-// solve_Ax_b (util/linalg.F90:57-93): DGETRS then the DGERFS refinement loop.
-template <int NL>
-__device__ void solve_ax_b_dev(const BasinDev &b, const double *rhs, double *x) {
-    const int n = NL - 1;
-    const double *A = b.cdhoc;
-    for (int i = 0; i < n; ++i) x[i] = rhs[i];
-    lu_solve_dev<NL>(b.lu, b.piv, n, x);
+// solve_Ax_b (util/linalg.F90:57-93): DGETRS then the DGERFS refinement loop
+// (at most 5 refinements), in registers.
+template <int N>
+__device__ __forceinline__ void solve_ax_b_dev(const double (&A)[N * N], const double (&lu)[N * N],
+                                               const int (&piv)[N], const double (&rhs)[N], double (&x)[N]) {
+#pragma unroll
+    for (int i = 0; i < N; ++i) x[i] = rhs[i];
+    lu_solve_dev<N>(lu, piv, x);
     const double eps = 1.1102230246251565e-16;
-    const double safe1 = (n + 1) * 2.2250738585072014e-308, safe2 = safe1 / eps;
+    const double safe1 = (N + 1) * 2.2250738585072014e-308, safe2 = safe1 / eps;
     double lstres = 3.0;
-    int count = 1;
-    double r[OQG_NLMAX], wv[OQG_NLMAX];
-    for (int it = 0; it < 8; ++it) {
-        for (int i = 0; i < n; ++i) r[i] = rhs[i];
-        for (int j = 0; j < n; ++j) {
-            double t = -x[j];
-            for (int i = 0; i < n; ++i) r[i] += t * A[i + n * j];
+#pragma unroll 1
+    for (int count = 1; count <= 6; ++count) {
+        double r[N], wv[N];
+#pragma unroll
+        for (int i = 0; i < N; ++i) { r[i] = rhs[i]; wv[i] = fabs(rhs[i]); }
+#pragma unroll
+        for (int j = 0; j < N; ++j) {
+            const double t = -x[j], xk = fabs(x[j]);
+#pragma unroll
+            for (int i = 0; i < N; ++i) {
+                r[i] += t * A[i + N * j];
+                wv[i] += fabs(A[i + N * j]) * xk;
+            }
         }
-        for (int i = 0; i < n; ++i) wv[i] = fabs(rhs[i]);
-        for (int j = 0; j < n; ++j) {
-            double xk = fabs(x[j]);
-            for (int i = 0; i < n; ++i) wv[i] += fabs(A[i + n * j]) * xk;
+        double sm = 0.0;
+#pragma unroll
+        for (int i = 0; i < N; ++i) {
+            const double q = (wv[i] > safe2) ? fabs(r[i]) / wv[i] : (fabs(r[i]) + safe1) / (wv[i] + safe1);
+            sm = fmax(sm, q);
         }
-        double s = 0.0;
-        for (int i = 0; i < n; ++i) {
-            double q = (wv[i] > safe2) ? fabs(r[i]) / wv[i] : (fabs(r[i]) + safe1) / (wv[i] + safe1);
-            s = fmax(s, q);
-        }
-        if (s > eps && 2.0 * s <= lstres && count <= 5) {
-            lu_solve_dev<NL>(b.lu, b.piv, n, r);
-            for (int i = 0; i < n; ++i) x[i] += r[i];
-            lstres = s;
-            ++count;
-        } else {
-            break;
-        }
+        if (!(sm > eps && 2.0 * sm <= lstres && count <= 5)) break;
+        lu_solve_dev<N>(lu, piv, r);
+#pragma unroll
+        for (int i = 0; i < N; ++i) x[i] += r[i];
+        lstres = sm;
     }
 }
 
-// The scalar phase of one step (one warp; lane 0 writes).
+// The scalar phase of one step, run by one warp of the last y-solve CTA;
+// reductions across the warp, the serial part in lane 0, all in registers.
 template <class T, int NL>
 __device__ void scalar_phase(const BasinDev &b, double tdt) {
     const int lane = threadIdx.x & 31;
     DevScalars *sc = b.sc;
-    double imode[OQG_NLMAX];
-    double S[OQG_NLMAX][OQG_NQ];
+    double imode[NL];
+    double S[NL][OQG_NQ];
     if (!b.cyclic) {
         // area integrals of the modal inhomogeneous solutions, formed from the
         // column sums of the spectral solution (the inverse DST is linear)
+        const int nkb = (b.nk + 3) / 4;       // y-solve CTAs per mode (4 columns each)
+#pragma unroll
         for (int m = 0; m < NL; ++m) {
             double s = 0.0;
-            for (int k = lane; k < b.nk; k += 32) s += b.dst_w[k] * b.part_col[m * b.nk + k];
+#pragma unroll 4
+            for (int x = lane; x < nkb; x += 32) s += b.part_col[m * nkb + x];
             s = warp_sum(s);
-            s = __shfl_sync(0xffffffffu, s, 0);
-            imode[m] = s * b.ftnorm * b.dx * b.dy;
+            imode[m] = __shfl_sync(0xffffffffu, s, 0) * b.ftnorm * b.dx * b.dy;
         }
     } else {
         const int ntile = b.tiles_x * b.tiles_y;
+#pragma unroll
         for (int k = 0; k < NL; ++k)
+#pragma unroll
             for (int q = 0; q < OQG_NQ; ++q) {
                 double s = 0.0;
                 for (int t = lane; t < ntile; t += 32) {
-                    const int ty0 = (t / b.tiles_x) * VTY;
-                    if (ty0 <= 1 || ty0 + VTY > b.nyp - 2)
-                        s += b.part_tile[((size_t)t * b.nl + k) * OQG_NQ + q];
+                    const int ty0 = (t / b.tiles_x) * b.vty;
+                    if (ty0 <= 1 || ty0 + b.vty > b.nyp - 2)
+                        s += b.part_tile[((size_t)t * NL + k) * OQG_NQ + q];
                 }
                 s = warp_sum(s);
                 S[k][q] = __shfl_sync(0xffffffffu, s, 0);
             }
     }
     if (lane != 0) return;
+    double dpi[NL], dpip[NL];
+#pragma unroll
+    for (int l = 0; l < NL - 1; ++l) { dpi[l] = sc->dpi[l]; dpip[l] = sc->dpip[l]; }
     // update_mass_constr (constraint.F90:167-179)
+    const double ent_xn = sc->ent_xn;
+#pragma unroll
     for (int l = 0; l < NL - 1; ++l) {
-        double ait = sc->dpi[l];
-        double exn = (l == 0) ? sc->ent_xn : 0.0;
-        sc->dpi[l] = sc->dpip[l] - tdt * b.gp[l] * exn;
-        sc->dpip[l] = ait;
+        const double ait = dpi[l];
+        dpi[l] = dpip[l] - tdt * b.gp[l] * (l == 0 ? ent_xn : 0.0);
+        dpip[l] = ait;
     }
+    const int supp = (b.suppress_period > 0 && (sc->nt % b.suppress_period) == 0) ? 1 : 0;
     if (!b.cyclic) {
         // box_homog (homog.F90:331-366)
-        double ik[OQG_NLMAX], rhs[OQG_NLMAX], al[OQG_NLMAX];
+        double ik[NL];
+#pragma unroll
         for (int k = 0; k < NL; ++k) {
             double s = 0.0;
+#pragma unroll
             for (int m = 0; m < NL; ++m) s += b.ctm2l[m + NL * k] * imode[m];
             ik[k] = s;
         }
-        for (int l = 0; l < NL - 1; ++l) rhs[l] = sc->dpi[l] - (ik[l + 1] - ik[l]);
-        solve_ax_b_dev<NL>(b, rhs, al);
-        for (int l = 0; l < NL - 1; ++l) sc->alpha[l] = al[l];
+        constexpr int N = (NL > 1) ? NL - 1 : 1;
+        double A[N * N], LU[N * N], rhs[N], al[N];
+        int pv[N];
+#pragma unroll
+        for (int x = 0; x < N * N; ++x) { A[x] = b.cdhoc[x]; LU[x] = b.lu[x]; }
+#pragma unroll
+        for (int x = 0; x < N; ++x) { pv[x] = b.piv[x]; rhs[x] = dpi[x] - (ik[x + 1] - ik[x]); }
+        solve_ax_b_dev<N>(A, LU, pv, rhs, al);
+#pragma unroll
+        for (int l = 0; l < N; ++l) sc->alpha[l] = al[l];
     } else {
+        double cs[NL], cn[NL], csp[NL], cnp[NL];
+#pragma unroll
+        for (int k = 0; k < NL; ++k) { cs[k] = sc->cs[k]; cn[k] = sc->cn[k]; csp[k] = sc->csp[k]; cnp[k] = sc->cnp[k]; }
         // strip integrals (vorticity.F90:84-101, numerics.F90:374-386)
-        double ajis[OQG_NLMAX], ajin[OQG_NLMAX], ap3s[OQG_NLMAX], ap3n[OQG_NLMAX];
-        double ap5s[OQG_NLMAX], ap5n[OQG_NLMAX];
         const double dx = b.dx, dy = b.dy;
-        for (int k = 0; k < NL; ++k) {
-            double a5s = (S[k][0] * dx) / (2.0 * dx), a9s = (S[k][1] * dx) / (2.0 * dx);
-            double a5n = (S[k][2] * dx) / (2.0 * dx), a9n = (S[k][3] * dx) / (2.0 * dx);
-            ajis[k] = (a5s + 2.0 * a9s) / 6.0;
-            ajin[k] = -(a5n + 2.0 * a9n) / 6.0;
-            ap3s[k] = b.ah2[k] * (S[k][4] * dx) / dy;
-            ap3n[k] = b.ah2[k] * (S[k][5] * dx) / dy;
-            ap5s[k] = b.ah4[k] * (S[k][6] * dx) / dy;
-            ap5n[k] = b.ah4[k] * (S[k][7] * dx) / dy;
-        }
-        double bdsums = (S[b.kt][8] * dx) / dy, bdsumn = (S[b.kt][9] * dx) / dy;
-        double dfac = b.fnot * b.delek / (2.0 * fabs(b.fnot));
-        double bdrins = dfac * bdsums, bdrinn = dfac * bdsumn;
-        // step_constraints (constraint.F90:182-215)
-        double rhss[OQG_NLMAX], rhsn[OQG_NLMAX];
+        double rhss[NL], rhsn[NL];
+#pragma unroll
         for (int k = 0; k < NL; ++k) {
             rhss[k] = -0.5 * dy * b.fnot * sc->int_Be_s[k];
             rhsn[k] = -0.5 * dy * b.fnot * sc->int_Be_n[k];
         }
+        // step_constraints (constraint.F90:182-215)
         rhss[0] = rhss[0] + b.tau_sign * (b.fnot / b.h[0]) * sc->txis;
         rhsn[0] = rhsn[0] - b.tau_sign * (b.fnot / b.h[0]) * sc->txin;
+        const double dfac = b.fnot * b.delek / (2.0 * fabs(b.fnot));
+        double bs = 0.0, bn = 0.0;
+#pragma unroll
+        for (int k = 0; k < NL; ++k)
+            if (k == b.kt) { bs = S[k][8]; bn = S[k][9]; }
+        const double bdrins = dfac * ((bs * dx) / dy), bdrinn = dfac * ((bn * dx) / dy);
         rhss[NL - 1] = rhss[NL - 1] + (b.fnot / b.h[NL - 1]) * bdrins;
         rhsn[NL - 1] = rhsn[NL - 1] - (b.fnot / b.h[NL - 1]) * bdrinn;
+#pragma unroll
         for (int k = 0; k < NL; ++k) {
-            rhss[k] = rhss[k] + ajis[k] - ap3s[k] + ap5s[k];
-            rhsn[k] = rhsn[k] + ajin[k] + ap3n[k] - ap5n[k];
+            const double a5s = (S[k][0] * dx) / (2.0 * dx), a9s = (S[k][1] * dx) / (2.0 * dx);
+            const double a5n = (S[k][2] * dx) / (2.0 * dx), a9n = (S[k][3] * dx) / (2.0 * dx);
+            const double ajis = (a5s + 2.0 * a9s) / 6.0, ajin = -(a5n + 2.0 * a9n) / 6.0;
+            const double ap3s = b.ah2[k] * (S[k][4] * dx) / dy, ap3n = b.ah2[k] * (S[k][5] * dx) / dy;
+            const double ap5s = b.ah4[k] * (S[k][6] * dx) / dy, ap5n = b.ah4[k] * (S[k][7] * dx) / dy;
+            rhss[k] = rhss[k] + ajis - ap3s + ap5s;
+            rhsn[k] = rhsn[k] + ajin + ap3n - ap5n;
         }
+#pragma unroll
         for (int k = 0; k < NL; ++k) {
-            double csn = sc->csp[k] + tdt * rhss[k];
-            double cnn = sc->cnp[k] + tdt * rhsn[k];
-            sc->csp[k] = sc->cs[k];
-            sc->cnp[k] = sc->cn[k];
-            sc->cs[k] = csn;
-            sc->cn[k] = cnn;
+            const double csn = csp[k] + tdt * rhss[k];
+            const double cnn = cnp[k] + tdt * rhsn[k];
+            csp[k] = cs[k];
+            cnp[k] = cn[k];
+            cs[k] = csn;
+            cn[k] = cnn;
         }
         // cyclic_homog (homog.F90:280-329).  The x-integral of row j of the
         // modal solution is dx times its zero wavenumber (before the 1/N of the
         // inverse transform, which the N-term row sum cancels).
         typedef typename C2<T>::t T2;
         const T2 *Sp = (const T2 *)b.spec;
-        double clhss[OQG_NLMAX], clhsn[OQG_NLMAX];
+        double clhss[NL], clhsn[NL];
+#pragma unroll
         for (int m = 0; m < NL; ++m) {
             double ss = 0.0, sn = 0.0;
+#pragma unroll
             for (int k = 0; k < NL; ++k) {
-                ss += b.ctl2m[k + NL * m] * sc->cs[k];
-                sn += b.ctl2m[k + NL * m] * sc->cn[k];
+                ss += b.ctl2m[k + NL * m] * cs[k];
+                sn += b.ctl2m[k + NL * m] * cn[k];
             }
-            double u0s = (double)Sp[((size_t)m * b.ny) * b.pk].x;
-            double u0n = (double)Sp[((size_t)m * b.ny + (b.ny - 1)) * b.pk].x;
+            const double u0s = (double)Sp[((size_t)m * b.ny) * b.pk].x;
+            const double u0n = (double)Sp[((size_t)m * b.ny + (b.ny - 1)) * b.pk].x;
             clhss[m] = ss + (u0s * dx) / dy;
             clhsn[m] = sn + (u0n * dx) / dy;
         }
         sc->c_bt = clhss[0] * b.hbsi;
+#pragma unroll
         for (int m = 1; m < NL; ++m) {
             sc->c_bc1[m] = b.hc2n[m] * clhss[m] - b.hc2s[m] * clhsn[m];
             sc->c_bc2[m] = b.hc1s[m] * clhsn[m] - b.hc1n[m] * clhss[m];
         }
+        // suppress_comp_mode's channel scalars (driver.F90:185-188)
+#pragma unroll
+        for (int k = 0; k < NL; ++k) {
+            if (supp) { cs[k] = 0.5 * (cs[k] + csp[k]); cn[k] = 0.5 * (cn[k] + cnp[k]); }
+            sc->cs[k] = cs[k]; sc->cn[k] = cn[k]; sc->csp[k] = csp[k]; sc->cnp[k] = cnp[k];
+        }
     }
     // suppress_comp_mode schedule (openqg.F90:485-487) and its scalar part
-    // (driver.F90:183-188)
-    const int supp = (b.suppress_period > 0 && (sc->nt % b.suppress_period) == 0) ? 1 : 0;
-    if (supp) {
-        for (int l = 0; l < NL - 1; ++l) sc->dpi[l] = 0.5 * (sc->dpi[l] + sc->dpip[l]);
-        if (b.cyclic)
-            for (int k = 0; k < NL; ++k) {
-                sc->cs[k] = 0.5 * (sc->cs[k] + sc->csp[k]);
-                sc->cn[k] = 0.5 * (sc->cn[k] + sc->cnp[k]);
-            }
+    // (driver.F90:183-184)
+#pragma unroll
+    for (int l = 0; l < NL - 1; ++l) {
+        sc->dpi[l] = supp ? 0.5 * (dpi[l] + dpip[l]) : dpi[l];
+        sc->dpip[l] = dpip[l];
     }
     sc->suppress_flag = supp;
     sc->nt += 1;
@@ -718,8 +908,8 @@ __device__ __forceinline__ void xinv_rows(const BasinDev &b, int rb, int &jlo, i
 // out != null: solve-only mode, writes the modal inhomogeneous solutions
 // (FP64, [nl][nyp][px]) and nothing else.
 template <class T, int E, int NL>
-__global__ void k_xinv(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par,
-                       double *out) {
+__global__ void __launch_bounds__(256, 2)
+k_xinv(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par, double *out) {
     typedef typename C2<T>::t T2;
     const Work w = work[blockIdx.x];
     const BasinDev &b = bas[w.member];
@@ -728,44 +918,55 @@ __global__ void k_xinv(const BasinDev *__restrict__ bas, const Work *__restrict_
     int jlo, jhi, jfirst, nra;
     xinv_rows(b, w.block, jlo, jhi, jfirst, nra);
     const int nr = jhi - jlo;                    // interior rows
-    const int nxp = b.nxp, n = b.nxin;
+    const int nxp = b.nxp, n = b.nxin, nyp = b.nyp, px = b.px;
+    const int LB = fft_buf_len(M), NTW = fft_tw_len(M);
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    T2 *zs = reinterpret_cast<T2 *>(smem_raw);
-    T *inh = reinterpret_cast<T *>(zs + (size_t)G * M);   // [NL][nra][nxp]
-    const T2 *tw = (const T2 *)b.tw;
+    T2 *sTw = reinterpret_cast<T2 *>(smem_raw);
+    T2 *zs = reinterpret_cast<T2 *>(smem_raw + round16(NTW * (int)sizeof(T2)));
+    T *inh = reinterpret_cast<T *>(zs + (size_t)G * 2 * LB);   // [NL][nra][nxp]
     const T ftn = (T)b.ftnorm;
 
     // zero the wall rows / columns of the modal fields
     for (int idx = threadIdx.x; idx < NL * nra * nxp; idx += blockDim.x) inh[idx] = (T)0;
-    __syncthreads();
+    pdl_trigger();
+    cp_async_16(sTw, b.tw, round16(NTW * (int)sizeof(T2)), threadIdx.x, blockDim.x);   // constant
+    pdl_wait();
 
     const int npr = (nr + 1) >> 1;               // row pairs per mode
     const int npairs = NL * npr;
+    // a row of the spectral buffer: n reals (box) or nk complex (channel)
+    const int rowbytes = b.cyclic ? b.nk * (int)sizeof(T2) : n * (int)sizeof(T);
+    const int RO = round16(rowbytes) / (int)sizeof(T);   // second row offset (T units)
     for (int base = 0; base < npairs; base += G) {
         const int pair = base + g;
         const bool live = g < G && pair < npairs;
         const int m = live ? pair / npr : 0;
         const int r0 = live ? 2 * (pair - m * npr) : 0;     // interior row offset
         const bool two = live && r0 + 1 < nr;
-        T2 *z = zs + (size_t)(g < G ? g : 0) * M;
+        T2 *za = zs + (size_t)(g < G ? g : 0) * 2 * LB;
+        T2 *zb = za + LB;
+        T *raw = reinterpret_cast<T *>(zb);
         const int sj = jlo + r0 - 1;                        // spectral row
-        if (!b.cyclic) {
-            const T *S = (const T *)b.spec;
-            const T *x = S + ((size_t)m * b.ny + sj) * b.pk;
-            const T *y = x + b.pk;
-            if (live)
+        const char *srow = (const char *)b.spec + ((size_t)m * b.ny + sj) * b.pk * (b.cyclic ? sizeof(T2) : sizeof(T));
+        const size_t pitchb = (size_t)b.pk * (b.cyclic ? sizeof(T2) : sizeof(T));
+        if (live) {
+            cp_async_16(raw, srow, round16(rowbytes), t, TT);
+            if (two) cp_async_16(raw + RO, srow + pitchb, round16(rowbytes), t, TT);
+        }
+        cp_async_commit_wait_all();
+        __syncthreads();
+        if (live) {
+            if (!b.cyclic) {
+                const T *x = raw, *y = raw + RO;
                 for (int jj = t; jj < M; jj += TT) {
                     T2 v;
                     if (jj == 0 || jj == n + 1) { v.x = (T)0; v.y = (T)0; }
                     else if (jj <= n) { v.x = ftn * x[jj - 1]; v.y = two ? ftn * y[jj - 1] : (T)0; }
-                    else { int s2 = M - jj; v.x = -(ftn * x[s2 - 1]); v.y = two ? -(ftn * y[s2 - 1]) : (T)0; }
-                    z[jj] = v;
+                    else { const int s2 = M - jj; v.x = -(ftn * x[s2 - 1]); v.y = two ? -(ftn * y[s2 - 1]) : (T)0; }
+                    za[fpad(jj)] = v;
                 }
-        } else {
-            const T2 *S = (const T2 *)b.spec;
-            const T2 *x = S + ((size_t)m * b.ny + sj) * b.pk;
-            const T2 *y = x + b.pk;
-            if (live)
+            } else {
+                const T2 *x = reinterpret_cast<const T2 *>(raw), *y = reinterpret_cast<const T2 *>(raw + RO);
                 for (int kk = t; kk < M; kk += TT) {
                     T2 X, Y;
                     const bool lo = kk <= M / 2;
@@ -778,30 +979,32 @@ __global__ void k_xinv(const BasinDev *__restrict__ bas, const Work *__restrict_
                     T2 v;
                     v.x = ftn * X.x - ftn * Y.y;
                     v.y = -(ftn * X.y + ftn * Y.x);
-                    z[kk] = v;
+                    za[fpad(kk)] = v;
                 }
+            }
         }
         __syncthreads();
-        fft_smem<T, E>(z, M, b.rad, b.nrad, tw, live ? t : TT, TT);
+        T2 *z = fft_smem<T>(za, zb, M, b.rad, b.nrad, sTw, live ? t : TT, TT);
         if (live) {
             const int lr = (jlo + r0) - jfirst;
             T *ox = inh + ((size_t)m * nra + lr) * nxp;
             T *oy = ox + nxp;
             if (!b.cyclic) {
                 for (int kk = t; kk < n; kk += TT) {
-                    T2 v = z[kk + 1];
+                    const T2 v = z[fpad(kk + 1)];
                     ox[kk + 1] = -v.y;
                     if (two) oy[kk + 1] = v.x;
                 }
             } else {
                 for (int i = t; i < M; i += TT) {
-                    T2 v = z[i];
+                    const T2 v = z[fpad(i)];
                     ox[i] = v.x;
                     if (two) oy[i] = -v.y;
                 }
                 if (t == 0) {
-                    ox[M] = z[0].x;
-                    if (two) oy[M] = -z[0].y;
+                    const T2 v = z[fpad(0)];
+                    ox[M] = v.x;
+                    if (two) oy[M] = -v.y;
                 }
             }
         }
@@ -810,9 +1013,9 @@ __global__ void k_xinv(const BasinDev *__restrict__ bas, const Work *__restrict_
 
     if (out) {
         for (int idx = threadIdx.x; idx < NL * nra * nxp; idx += blockDim.x) {
-            int m = idx / (nra * nxp), rem = idx - m * nra * nxp;
-            int lr = rem / nxp, i = rem - lr * nxp;
-            out[((size_t)m * b.nyp + jfirst + lr) * b.px + i] = (double)inh[idx];
+            const int m = idx / (nra * nxp), rem = idx - m * nra * nxp;
+            const int lr = rem / nxp, i = rem - lr * nxp;
+            out[((size_t)m * nyp + jfirst + lr) * px + i] = (double)inh[idx];
         }
         return;
     }
@@ -820,34 +1023,63 @@ __global__ void k_xinv(const BasinDev *__restrict__ bas, const Work *__restrict_
     // homogeneous correction + modes_to_layers, in place (modes -> layers)
     const DevScalars *sc = b.sc;
     const int supp = sc->suppress_flag;
-    const T *Pold = (const T *)b.F[par];
-    T *Pnew = (T *)b.F[1 - par];
-    for (int idx = threadIdx.x; idx < nra * nxp; idx += blockDim.x) {
-        const int lr = idx / nxp, i = idx - lr * nxp;
-        const int j = jfirst + lr;
-        double pm_[NL];
+    double ctm[NL * NL], hc[NL > 1 ? NL - 1 : 1];
 #pragma unroll
-        for (int m = 0; m < NL; ++m) pm_[m] = (double)inh[((size_t)m * nra + lr) * nxp + i];
-        if (!b.cyclic) {
-            const T *H = (const T *)b.hsb;
+    for (int x = 0; x < NL * NL; ++x) ctm[x] = b.ctm2l[x];
+    const T *__restrict__ Pold = (const T *)b.F[par];
+    T *__restrict__ Pnew = (T *)b.F[1 - par];
+    const size_t n2 = (size_t)nyp * px;
+    if (!b.cyclic) {
 #pragma unroll
-            for (int m = 1; m < NL; ++m)
-                pm_[m] = pm_[m] + sc->alpha[m - 1] * (double)H[((size_t)(m - 1) * b.nyp + j) * b.px + i];
-        } else {
-            pm_[0] = pm_[0] + sc->c_bt * b.hbt[j];
+        for (int m = 1; m < NL; ++m) hc[m - 1] = sc->alpha[m - 1];
+    }
+    const T *__restrict__ H = (const T *)b.hsb;
+    constexpr int U = 4;
+    for (int base = threadIdx.x; base < nra * nxp; base += U * blockDim.x) {
+        // gather the inputs of U points first (independent loads), then compute
+        double hv[U][NL], po[U][NL];
+        int lrs[U], is[U];
 #pragma unroll
-            for (int m = 1; m < NL; ++m)
-                pm_[m] = pm_[m] + (sc->c_bc1[m] * b.hbc1[m * b.nyp + j] + sc->c_bc2[m] * b.hbc2[m * b.nyp + j]);
+        for (int u = 0; u < U; ++u) {
+            const int idx = base + u * blockDim.x;
+            const bool ok = idx < nra * nxp;
+            const int lr = ok ? idx / nxp : 0, i = ok ? idx - lr * nxp : 0;
+            const int j = jfirst + lr;
+            lrs[u] = ok ? lr : -1;
+            is[u] = i;
+#pragma unroll
+            for (int m = 0; m < NL; ++m) {
+                po[u][m] = (ok && supp) ? (double)Pold[m * n2 + (size_t)j * px + i] : 0.0;
+                if (!b.cyclic) hv[u][m] = (ok && m >= 1) ? (double)H[((size_t)(m - 1) * nyp + j) * px + i] : 0.0;
+                else if (m == 0) hv[u][m] = ok ? b.hbt[j] : 0.0;
+                else hv[u][m] = ok ? b.hbc1[m * nyp + j] : 0.0;
+            }
         }
 #pragma unroll
-        for (int k = 0; k < NL; ++k) {
-            double s = 0.0;
+        for (int u = 0; u < U; ++u) {
+            if (lrs[u] < 0) continue;
+            const int lr = lrs[u], i = is[u], j = jfirst + lr;
+            double pm_[NL];
 #pragma unroll
-            for (int m = 0; m < NL; ++m) s += pm_[m] * b.ctm2l[m + NL * k];
-            T pn = (T)s;
-            inh[((size_t)k * nra + lr) * nxp + i] = pn;
-            const size_t o3 = ((size_t)k * b.nyp + j) * b.px + i;
-            Pnew[o3] = supp ? (T)((T)0.5 * (pn + Pold[o3])) : pn;
+            for (int m = 0; m < NL; ++m) pm_[m] = (double)inh[((size_t)m * nra + lr) * nxp + i];
+            if (!b.cyclic) {
+#pragma unroll
+                for (int m = 1; m < NL; ++m) pm_[m] = pm_[m] + hc[m - 1] * hv[u][m];
+            } else {
+                pm_[0] = pm_[0] + sc->c_bt * hv[u][0];
+#pragma unroll
+                for (int m = 1; m < NL; ++m)
+                    pm_[m] = pm_[m] + (sc->c_bc1[m] * hv[u][m] + sc->c_bc2[m] * b.hbc2[m * nyp + j]);
+            }
+#pragma unroll
+            for (int k = 0; k < NL; ++k) {
+                double s2 = 0.0;
+#pragma unroll
+                for (int m = 0; m < NL; ++m) s2 += pm_[m] * ctm[m + NL * k];
+                const T pn = (T)s2;
+                inh[((size_t)k * nra + lr) * nxp + i] = pn;
+                Pnew[k * n2 + (size_t)j * px + i] = supp ? (T)((T)0.5 * (pn + (T)po[u][k])) : pn;
+            }
         }
     }
     __syncthreads();
@@ -860,12 +1092,12 @@ __global__ void k_xinv(const BasinDev *__restrict__ bas, const Work *__restrict_
     for (int idx = threadIdx.x; idx < nra * nxp; idx += blockDim.x) {
         const int lr = idx / nxp, i = idx - lr * nxp;
         const int j = jfirst + lr;
-        const bool zon = (j == 0 || j == b.nyp - 1);
+        const bool zon = (j == 0 || j == nyp - 1);
         const bool mer = !b.cyclic && (i == 0 || i == nxp - 1);
         if (!zon && !mer) {
             if (supp)
                 for (int k = 0; k < NL; ++k) {
-                    const size_t o3 = ((size_t)k * b.nyp + j) * b.px + i;
+                    const size_t o3 = ((size_t)k * nyp + j) * px + i;
                     Qc[o3] = (T)0.5 * (Qc[o3] + Qm[o3]);
                 }
             continue;
@@ -891,10 +1123,10 @@ __global__ void k_xinv(const BasinDev *__restrict__ bas, const Work *__restrict_
             for (int c = 0; c < cnt; ++c) qv = qv - fmv;
             for (int c = 0; c < cnt; ++c) qv = qv + by;
             if (k == b.kt && b.topo_active) {
-                const T dd = (T)b.ddyn[(size_t)j * b.px + i];
+                const T dd = (T)b.ddyn[(size_t)j * px + i];
                 for (int c = 0; c < cnt; ++c) qv = qv + dd;
             }
-            const size_t o3 = ((size_t)k * b.nyp + j) * b.px + i;
+            const size_t o3 = ((size_t)k * nyp + j) * px + i;
             Qc[o3] = supp ? (T)((T)0.5 * (qv + Qm[o3])) : qv;
         }
 #undef PN

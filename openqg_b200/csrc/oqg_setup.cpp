@@ -171,12 +171,14 @@ bool fft_radices(int M, std::vector<int> &rad) {
 }
 
 void fft_twiddles(int M, std::vector<double> &tw) {
-    tw.resize(2 * (size_t)M);
+    const int ntw = 64 + (M + 63) / 64 + 1;
+    tw.assign(2 * (size_t)ntw, 0.0);
     const long double pi = 3.14159265358979323846264338327950288L;
-    for (int t = 0; t < M; ++t) {
-        const long double ang = -2.0L * pi * (long double)t / (long double)M;
-        tw[2 * t] = (double)cosl(ang);
-        tw[2 * t + 1] = (double)sinl(ang);
+    for (int e = 0; e < ntw; ++e) {
+        const long long k = e < 64 ? e : 64LL * (e - 64);
+        const long double ang = -2.0L * pi * (long double)(k % M) / (long double)M;
+        tw[2 * e] = (double)cosl(ang);
+        tw[2 * e + 1] = (double)sinl(ang);
     }
 }
 

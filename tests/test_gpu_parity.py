@@ -100,14 +100,21 @@ def test_solve_inhomog_matches_oracle_and_residual(b):
     if b.cyclic:
         rhs[:, -1] = rhs[:, 0]
     rdm2 = g.modes()["rdm2"]
+    sl = (slice(1, -1), slice(None)) if b.cyclic else (slice(1, -1), slice(1, -1))
+
+    def residual(s, m):
+        out = o.del2(s, 0.0) - rdm2[m - 1] * s
+        return np.abs(out[sl] - rhs[sl]).max() / np.abs(rhs[sl]).max()
+
     for m in range(1, b.nl + 1):
         sg = g.solve_inhomog_eqn(m, rhs)
         so = o.solve_inhomog(m, rhs)
         assert rel_l2(sg, so) <= 1e-13, m
-        out = o.del2(sg, 0.0) - rdm2[m - 1] * sg
-        sl = (slice(1, -1), slice(None)) if b.cyclic else (slice(1, -1), slice(1, -1))
-        res = np.abs(out[sl] - rhs[sl]).max() / np.abs(rhs[sl]).max()
-        assert res <= 1e-11, (m, res)
+        # test_inhomog.F90:149 uses 1e-11 on ~100-point grids; evaluating the
+        # Laplacian of the solution carries roundoff ~ eps (L / pi dx)^2, so on
+        # larger grids the bound is the oracle's own residual (x 1.5).
+        bound = 1e-11 if max(b.nxp, b.nyp) <= 129 else max(1e-11, 1.5 * residual(so, m))
+        assert residual(sg, m) <= bound, (m, residual(sg, m), bound)
 
 
 @pytest.mark.parametrize("b", BOXES[:2] + BOXES[4:5], ids=["box129", "box65", "chan193x97"])
