@@ -9,11 +9,13 @@
 #include "oqg_kernels.cuh"
 #include "oqg_setup.h"
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -210,6 +212,67 @@ static int solve_all_modes(oqg_handle *h) {
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(h->st));
     return OQG_OK;
+}
+
+// ----------------------------------------------------------- tensor maps
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_tiled() {
+    static EncodeTiledFn fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (EncodeTiledFn)p;
+    }
+    return fn;
+}
+
+// Tensor maps of the closed-box tiles of k_vort (order in oqg_kernels.cuh).
+// Returns false when the driver cannot encode them; the kernel then loads
+// the tiles with cp.async.
+static bool make_tmaps(oqg_handle *h) {
+    BasinDev &b = h->hb;
+    if (b.cyclic) return false;
+    const char *env = std::getenv("OQG_NO_TMA");
+    if (env && env[0] == '1') return false;
+    EncodeTiledFn enc = encode_tiled();
+    if (!enc) return false;
+    const CUtensorMapDataType dt = h->mixed ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
+    const cuuint64_t esz = h->esz;
+    std::vector<CUtensorMap> maps(OQG_NTMAP);
+    auto enc3 = [&](CUtensorMap *m, void *base, cuuint32_t bx, cuuint32_t by) {
+        cuuint64_t dims[3] = {(cuuint64_t)b.nxp, (cuuint64_t)b.nyp, (cuuint64_t)b.nl};
+        cuuint64_t strides[2] = {(cuuint64_t)b.px * esz, (cuuint64_t)b.nyp * b.px * esz};
+        cuuint32_t box[3] = {bx, by, 1}, es[3] = {1, 1, 1};
+        return enc(m, dt, 3, base, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                   CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+    };
+    const cuuint32_t vt = (cuuint32_t)b.vty, wpq = VTX + 8, wo = VTX;
+    bool ok = true;
+    for (int f = 0; f < 4; ++f) ok = ok && enc3(&maps[OQG_TMAP_PQ + f], b.F[f], wpq, vt + 2);
+    for (int f = 0; f < 2; ++f) ok = ok && enc3(&maps[OQG_TMAP_PM + f], b.F[f], wpq, vt + 6);
+    for (int f = 0; f < 2; ++f) ok = ok && enc3(&maps[OQG_TMAP_QM + f], b.F[2 + f], wo, vt);
+    {
+        cuuint64_t dims[2] = {(cuuint64_t)b.nxp, (cuuint64_t)b.nyp};
+        cuuint64_t strides[1] = {(cuuint64_t)b.px * esz};
+        cuuint32_t box[2] = {wo, vt}, es[2] = {1, 1};
+        ok = ok && enc(&maps[OQG_TMAP_WK], dt, 2, const_cast<void *>(b.wekp), dims, strides, box, es,
+                       CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                       CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+    }
+    if (!ok) return false;
+    void *d = dalloc<unsigned char>(h, (size_t)OQG_NTMAP * OQG_TMAP_BYTES);
+    if (!d) return false;
+    if (cudaMemcpy(d, maps.data(), (size_t)OQG_NTMAP * sizeof(CUtensorMap), cudaMemcpyHostToDevice) != cudaSuccess)
+        return false;
+    b.tmaps = d;
+    return true;
 }
 
 // ----------------------------------------------------------- homogeneous solutions
@@ -538,11 +601,7 @@ int oqg_create(const oqg_params *prm, oqg_handle **out) {
     h->nys = b.k3_blocks;
     b.k4_rows = 2;
     h->ni = (b.ny + b.k4_rows - 1) / b.k4_rows;
-    {
-        const int vt = b.vty;
-        h->smem_v = (size_t)(2 * ((vt + 6) * (VTX + 6) + 2 * (vt + 2) * (VTX + 2) + vt * VTX) +
-                             (vt + 4) * (VTX + 4) + (vt + 2) * (VTX + 2) + vt * VTX) * h->esz;
-    }
+    h->smem_v = vort_smem_bytes(b.vty, (int)h->esz);
     const int NTW = fft_tw_len(b.M), LB = fft_buf_len(b.M);
     h->smem_x = (size_t)round16(NTW * (int)t2) + (size_t)GX * 2 * LB * t2;
     h->smem_x64 = (size_t)round16(NTW * 16) + (size_t)GX * 2 * LB * 16;
@@ -567,6 +626,8 @@ int oqg_create(const oqg_params *prm, oqg_handle **out) {
     CK(cudaMemcpy(h->d_wy, wy.data(), wy.size() * sizeof(Work), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(h->d_wi, wi.data(), wi.size() * sizeof(Work), cudaMemcpyHostToDevice));
 
+    b.tmaps = nullptr;
+    make_tmaps(h);
     h->hb64 = b;
     h->hb64.tw = d_tw64;
     h->d_bas = dalloc<BasinDev>(h, 1);

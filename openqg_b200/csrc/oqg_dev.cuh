@@ -35,6 +35,7 @@ struct DevScalars {
 
 // Device error bits
 #define OQG_DERR_SOLVE   1   // zero pivot in the constraint solve
+#define OQG_DERR_TIMEOUT 2   // a bounded wait for a tile load ran out
 
 // Number of per-tile channel strip quantities per layer (vorticity kernel)
 #define OQG_NQ 10
@@ -79,6 +80,7 @@ struct BasinDev {
     const void *ent;            // [nl-1][nyp][px] T or null
     const double *ddyn;         // [nyp][px] or null
     const double *yprel;        // [nyp] y - yl/2 (box.F90:142-145)
+    const void *tmaps;          // box: OQG_NTMAP tensor maps (128 bytes each) or null
     void *rhs;                  // [nl][ny][pr] T
     void *spec;                 // [nl][ny][pk] T or T2
     const void *tw;             // [M] T2 twiddles exp(-2 pi i t/M)

@@ -21,6 +21,7 @@
 
 #include "oqg_dev.cuh"
 #include "oqg_fft.cuh"
+#include "oqg_tma.cuh"
 
 namespace oqg {
 
@@ -61,17 +62,24 @@ __device__ __forceinline__ double block_sum(double v, double *red) {
 }
 
 // ------------------------------------------------------------------ k_vort
-#define VTX 64
-#define VTYMAX 17
-#define VTHREADS 256
+#define VTX 60          // output columns of a vorticity tile
+#define VTYMAX 17       // output rows of a vorticity tile (at most)
+#define VTHREADS 256    // 64 column lanes x 4 row strips
 
-// Geometry scalars of a basin held in registers by the stencil kernels.
+// Geometry scalars of a basin used by the stencils.
 template <class T> struct Geo {
     int nxp, nyp, cyclic;
     T fx, fy, fxb, fyb, jac;
     __device__ __forceinline__ explicit Geo(const BasinDev &b)
         : nxp(b.nxp), nyp(b.nyp), cyclic(b.cyclic), fx((T)b.fx), fy((T)b.fy), fxb((T)b.fx_bc),
           fyb((T)b.fy_bc), jac((T)b.jac_fac) {}
+};
+// The same scalars read from a shared table at each use (K = fx, fy, fxb,
+// fyb, jac), which leaves registers to the stencil windows.
+template <class T> struct GeoS {
+    int nxp, nyp, cyclic;
+    const T *K;
+    __device__ __forceinline__ T fxv() const { return K[0]; }
 };
 
 // Laplacian with the mixed wall condition (del2_P_bc, numerics.F90:410-468) at
@@ -135,6 +143,65 @@ __device__ __forceinline__ T arakawa(const T *sp, const T *sq, int ld, int r, in
     return g.jac * t;
 }
 
+// Laplacian with the mixed wall condition from the five stencil values
+// (W, E, S, N, C), the register form of lap_bc.
+template <class T> __device__ __forceinline__ T gfx(const Geo<T> &g) { return g.fx; }
+template <class T> __device__ __forceinline__ T gfy(const Geo<T> &g) { return g.fy; }
+template <class T> __device__ __forceinline__ T gfxb(const Geo<T> &g) { return g.fxb; }
+template <class T> __device__ __forceinline__ T gfyb(const Geo<T> &g) { return g.fyb; }
+template <class T> __device__ __forceinline__ T gjac(const Geo<T> &g) { return g.jac; }
+template <class T> __device__ __forceinline__ T gfx(const GeoS<T> &g) { return g.K[0]; }
+template <class T> __device__ __forceinline__ T gfy(const GeoS<T> &g) { return g.K[1]; }
+template <class T> __device__ __forceinline__ T gfxb(const GeoS<T> &g) { return g.K[2]; }
+template <class T> __device__ __forceinline__ T gfyb(const GeoS<T> &g) { return g.K[3]; }
+template <class T> __device__ __forceinline__ T gjac(const GeoS<T> &g) { return g.K[4]; }
+
+template <class T, class G>
+__device__ __forceinline__ T lap5(T wv, T ev, T sv, T nv, T c, int gi, int gj, const G &g) {
+    const bool zrow = (gj == 0 || gj == g.nyp - 1);
+    const bool wall_x = !g.cyclic && (gi == 0 || gi == g.nxp - 1);
+    if (!zrow && !wall_x) return gfx(g) * (wv + ev - (T)2 * c) + gfy(g) * (sv + nv - (T)2 * c);
+    T xp, yp;
+    if (zrow) xp = (T)0;
+    else if (gi == 0) xp = gfxb(g) * (ev - c);
+    else xp = -(gfxb(g) * (c - wv));
+    if (wall_x) yp = (T)0;
+    else if (gj == 0) yp = gfyb(g) * (nv - c);
+    else yp = -(gfyb(g) * (c - sv));
+    return xp + yp;
+}
+
+// Arakawa Jacobian from 3 x 3 windows of p and q (row 0 = j-1, col 0 = i-1).
+template <class T, class G>
+__device__ __forceinline__ T arakawa3(const T (&p)[3][3], const T (&q)[3][3], int gi, int gj,
+                                      const G &g) {
+    const bool zx = !g.cyclic && (gi == 0 || gi == g.nxp - 1);   // dPdx_2 = 0 here
+    const bool zy = (gj == 0 || gj == g.nyp - 1);                 // dPdy_2 = 0 here
+    const T pxc = zx ? (T)0 : p[1][2] - p[1][0];
+    const T pyc = zy ? (T)0 : p[2][1] - p[0][1];
+    const T qxc = zx ? (T)0 : q[1][2] - q[1][0];
+    const T qyc = zy ? (T)0 : q[2][1] - q[0][1];
+    T A = (T)0, Bv = (T)0, C = (T)0, D = (T)0;
+    if (!zx) {
+        const T pyR = zy ? (T)0 : p[2][2] - p[0][2];
+        const T pyL = zy ? (T)0 : p[2][0] - p[0][0];
+        const T qyR = zy ? (T)0 : q[2][2] - q[0][2];
+        const T qyL = zy ? (T)0 : q[2][0] - q[0][0];
+        A = q[1][2] * pyR - q[1][0] * pyL;
+        D = p[1][2] * qyR - p[1][0] * qyL;
+    }
+    if (!zy) {
+        const T pxU = zx ? (T)0 : p[2][2] - p[2][0];
+        const T pxD = zx ? (T)0 : p[0][2] - p[0][0];
+        const T qxU = zx ? (T)0 : q[2][2] - q[2][0];
+        const T qxD = zx ? (T)0 : q[0][2] - q[0][0];
+        Bv = q[2][1] * pxU - q[0][1] * pxD;
+        C = p[2][1] * qxU - p[0][1] * qxD;
+    }
+    const T t = qxc * pyc - qyc * pxc + A - Bv + C - D;
+    return gjac(g) * t;
+}
+
 // cp.async copy of one element into shared memory; zero-filled when !valid
 // (the source is then not read).
 template <class T>
@@ -154,8 +221,8 @@ template <int N> __device__ __forceinline__ void cp_async_wait() {
 // Queues the copy of rows [jlo, jlo+nr) x cols [ilo, ilo+nc) of layer k of f
 // into s (leading dimension nc); outside the basin -> 0; channel columns wrap.
 // Thread layout: 64 columns x 4 rows.
-template <class T>
-__device__ __forceinline__ void load_tile_async(T *s, const T *__restrict__ f, const Geo<T> &g, int px,
+template <class T, class G>
+__device__ __forceinline__ void load_tile_async(T *s, const T *__restrict__ f, const G &g, int px,
                                                 int k, int jlo, int nr, int ilo, int nc) {
     const int N = g.nxp - 1;
     const int tx = threadIdx.x & 63, ty = threadIdx.x >> 6;
@@ -179,167 +246,309 @@ __device__ __forceinline__ void load_tile_async(T *s, const T *__restrict__ f, c
 }
 
 // Tiles are VTX columns by b.vty rows (b.vty <= VTYMAX, chosen per basin so
-// the tiles fill whole waves); 256 threads as 64 columns x 4 rows.
+// that the tiles fill whole waves).  Shared tiles per layer (origin, pitch):
+//   pm     rows j0-3 .. j0+vty+2, cols from i0-4   (LPQ = VTX+8 = 68)
+//   p, q   rows j0-1 .. j0+vty,   cols from i0-4   (LPQ)
+//   qm     rows j0 .. j0+vty-1,   cols from i0     (LO = VTX)
+//   d2     rows j0-2 .. j0+vty+1, cols from i0-2   (L2 = VTX+4 = 64), computed
+//   d4     rows j0-1 .. j0+vty,   cols from i0-1   (L1 = VTX+2), computed
+// The x-origins are multiples of 4 elements (16 bytes), as tensor loads need.
+// Closed-box tiles arrive by TMA (one thread issues, an mbarrier counts the
+// bytes); channel tiles wrap periodically and come by cp.async.  Thread
+// (lane x, strip y) owns column x of each phase and marches down a strip of
+// rows with a rolling window of the stencil in registers.
+struct VortLayout {
+    int HPM, H2, H1, VT;
+    int pm, p, q, qm, nbuf;     // offsets within a layer buffer (elements)
+    int d2, d4, wk, by, total;  // offsets after the two layer buffers
+};
+__host__ __device__ __forceinline__ int vort_round(int n, int esz) {
+    const int a = 128 / esz;
+    return (n + a - 1) / a * a;
+}
+__host__ __device__ __forceinline__ VortLayout vort_layout(int vt, int esz) {
+    constexpr int LPQ = VTX + 8, L2 = VTX + 4, L1 = VTX + 2, LO = VTX;
+    VortLayout L;
+    L.VT = vt;
+    L.HPM = vt + 6;
+    L.H2 = vt + 4;
+    L.H1 = vt + 2;
+    L.pm = 0;
+    L.p = L.pm + vort_round(L.HPM * LPQ, esz);
+    L.q = L.p + vort_round(L.H1 * LPQ, esz);
+    L.qm = L.q + vort_round(L.H1 * LPQ, esz);
+    L.nbuf = L.qm + vort_round(vt * LO, esz);
+    L.d2 = 2 * L.nbuf;
+    L.d4 = L.d2 + vort_round(L.H2 * L2, esz);
+    L.wk = L.d4 + vort_round(L.H1 * L1, esz);
+    L.by = L.wk + vort_round(vt * LO, esz);
+    L.total = L.by + vort_round(vt * 8 / esz + 1, esz);   // vt doubles
+    return L;
+}
+// Dynamic shared bytes of k_vort (plus slack to align the base to 128 bytes).
+__host__ __device__ __forceinline__ size_t vort_smem_bytes(int vt, int esz) {
+    return (size_t)vort_layout(vt, esz).total * esz + 128;
+}
+
+// Tensor maps of a box basin, in this order: p/q-shaped boxes of F[0..3],
+// pm-shaped boxes of F[0], F[1], qm-shaped boxes of F[2], F[3], wekp.
+#define OQG_TMAP_PQ 0
+#define OQG_TMAP_PM 4
+#define OQG_TMAP_QM 6
+#define OQG_TMAP_WK 8
+#define OQG_NTMAP 9
+#define OQG_TMAP_BYTES 128
+
 template <class T, int NL>
 __global__ void __launch_bounds__(VTHREADS, 2)
 k_vort(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par, double tdt) {
-    constexpr int WPM = VTX + 6, W2 = VTX + 4, W1 = VTX + 2;
-    constexpr int UMAX = (VTYMAX + 3) / 4;
+    constexpr int LPQ = VTX + 8, L2 = VTX + 4, L1 = VTX + 2, LO = VTX;
+    constexpr int RMAX = (VTYMAX + 3) / 4;     // output rows per strip
     const Work w = work[blockIdx.x];
     const BasinDev &b = bas[w.member];
-    const Geo<T> g(b);
+    // uniform constants in shared memory: fx fy fxb fyb jac | c_ent1 c_wind
+    // c_ent2 c_drag tdt | c2[k] | c4[k]; FP64 ctl2m
+    __shared__ T sK[10 + 2 * OQG_NLMAX];
+    __shared__ double sCtl[NL * NL];
+    if (threadIdx.x < 10 + 2 * NL) {
+        const int i = threadIdx.x;
+        T v;
+        if (i == 0) v = (T)b.fx; else if (i == 1) v = (T)b.fy; else if (i == 2) v = (T)b.fx_bc;
+        else if (i == 3) v = (T)b.fy_bc; else if (i == 4) v = (T)b.jac_fac; else if (i == 5) v = (T)b.c_ent1;
+        else if (i == 6) v = (T)b.c_wind; else if (i == 7) v = (T)b.c_ent2; else if (i == 8) v = (T)b.c_drag;
+        else if (i == 9) v = (T)tdt; else if (i < 10 + NL) v = (T)b.c2[i - 10]; else v = (T)b.c4[i - 10 - NL];
+        sK[i] = v;
+    }
+    if (threadIdx.x < NL * NL) sCtl[threadIdx.x] = b.ctl2m[threadIdx.x];
+    GeoS<T> g;
+    g.nxp = b.nxp; g.nyp = b.nyp; g.cyclic = b.cyclic; g.K = sK;
     const int VT = b.vty;
-    const int HPM = VT + 6, H2 = VT + 4, H1 = VT + 2;
-    const int NBUF = HPM * WPM + 2 * H1 * W1 + VT * VTX;   // one layer's inputs
+    const VortLayout LY = vort_layout(VT, (int)sizeof(T));
+    const int HPM = LY.HPM, H2 = LY.H2, H1 = LY.H1;
     const int tile_x = w.block % b.tiles_x, tile_y = w.block / b.tiles_x;
     const int i0 = tile_x * VTX, j0 = tile_y * VT;
 
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    T *buf0 = reinterpret_cast<T *>(smem_raw);
-    T *sD2 = buf0 + 2 * NBUF;
-    T *sD4 = sD2 + H2 * W2;
-    T *sWK = sD4 + H1 * W1;
+    T *sm = reinterpret_cast<T *>(((uintptr_t)smem_raw + 127) & ~(uintptr_t)127);
+    T *sD2 = sm + LY.d2;
+    T *sD4 = sm + LY.d4;
+    T *sWK = sm + LY.wk;
+    double *sBY = reinterpret_cast<double *>(sm + LY.by);
     __shared__ double red[32];
+    __shared__ __align__(8) unsigned long long bars[2];
 
-    const T *P = (const T *)b.F[par];
-    const T *PM = (const T *)b.F[1 - par];
-    const T *Q = (const T *)b.F[2 + par];
     T *QM = (T *)b.F[3 - par];
-    const T *WEK = (const T *)b.wekp;
     const T *ENT = (const T *)b.ent;
+    const double *__restrict__ DD = b.ddyn;
     const int N = g.nxp - 1;
     const int nyp = g.nyp, nxp = g.nxp, px = b.px, kt = b.kt;
-    const int tx = threadIdx.x & 63, ty0 = threadIdx.x >> 6;
+    const int tx = threadIdx.x & 63, ty = threadIdx.x >> 6;
+    const bool tma = !g.cyclic && b.tmaps != nullptr;
+    const unsigned char *tm = (const unsigned char *)b.tmaps;
+    DevScalars *scal = b.sc;
 
+    if (tma && threadIdx.x == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        mbar_init_fence();
+    }
+    // beta * yprel of the tile's rows (constant)
+    for (int r = threadIdx.x; r < VT; r += blockDim.x) {
+        const int gj = j0 + r;
+        sBY[r] = gj < nyp ? b.beta * b.yprel[gj] : 0.0;
+    }
+    __syncthreads();
     pdl_trigger();
     pdl_wait();
+
     auto issue = [&](int k) {
-        T *bf = buf0 + (k & 1) * NBUF;
-        load_tile_async(bf, PM, g, px, k, j0 - 3, HPM, i0 - 3, WPM);
-        load_tile_async(bf + HPM * WPM, P, g, px, k, j0 - 1, H1, i0 - 1, W1);
-        load_tile_async(bf + HPM * WPM + H1 * W1, Q, g, px, k, j0 - 1, H1, i0 - 1, W1);
-        load_tile_async(bf + HPM * WPM + 2 * H1 * W1, (const T *)QM, g, px, k, j0, VT, i0, VTX);
-        if (k == 0) load_tile_async(sWK, WEK, g, px, 0, j0, VT, i0, VTX);
-        cp_async_commit();
+        T *bf = sm + (k & 1) * LY.nbuf;
+        if (tma) {
+            if (threadIdx.x == 0) {
+                fence_proxy_async();
+                unsigned bytes = (unsigned)((HPM * LPQ + 2 * H1 * LPQ + VT * LO) * sizeof(T));
+                if (k == 0) bytes += (unsigned)(VT * LO * sizeof(T));
+                unsigned long long *bar = &bars[k & 1];
+                mbar_expect_tx(bar, bytes);
+                tma_load_3d(bf + LY.pm, tm + (OQG_TMAP_PM + 1 - par) * OQG_TMAP_BYTES, i0 - 4, j0 - 3, k, bar);
+                tma_load_3d(bf + LY.p, tm + (OQG_TMAP_PQ + par) * OQG_TMAP_BYTES, i0 - 4, j0 - 1, k, bar);
+                tma_load_3d(bf + LY.q, tm + (OQG_TMAP_PQ + 2 + par) * OQG_TMAP_BYTES, i0 - 4, j0 - 1, k, bar);
+                tma_load_3d(bf + LY.qm, tm + (OQG_TMAP_QM + 1 - par) * OQG_TMAP_BYTES, i0, j0, k, bar);
+                if (k == 0) tma_load_2d(sWK, tm + OQG_TMAP_WK * OQG_TMAP_BYTES, i0, j0, bar);
+            }
+        } else {
+            load_tile_async(bf + LY.pm, (const T *)b.F[1 - par], g, px, k, j0 - 3, HPM, i0 - 4, LPQ);
+            load_tile_async(bf + LY.p, (const T *)b.F[par], g, px, k, j0 - 1, H1, i0 - 4, LPQ);
+            load_tile_async(bf + LY.q, (const T *)b.F[2 + par], g, px, k, j0 - 1, H1, i0 - 4, LPQ);
+            load_tile_async(bf + LY.qm, (const T *)QM, g, px, k, j0, VT, i0, LO);
+            if (k == 0) load_tile_async(sWK, (const T *)b.wekp, g, px, 0, j0, VT, i0, LO);
+            cp_async_commit();
+        }
     };
     issue(0);
 
-    // per-point constants, hoisted out of the layer loop
-    double ctl[NL * NL];
+    // strips of rows: [ty*R, ty*R + R) of each region
+    const int R2 = (H2 + 3) >> 2, R1 = (H1 + 3) >> 2, R0 = (VT + 3) >> 2;
+    const int r0 = ty * R0;
+    double acc[RMAX][NL];
 #pragma unroll
-    for (int x = 0; x < NL * NL; ++x) ctl[x] = b.ctl2m[x];
-    double acc[UMAX][NL], by[UMAX];
-#pragma unroll
-    for (int u = 0; u < UMAX; ++u) {
-        const int gj = j0 + ty0 + 4 * u;
-        by[u] = (gj < nyp) ? b.beta * b.yprel[gj] : 0.0;
+    for (int u = 0; u < RMAX; ++u)
 #pragma unroll
         for (int m = 0; m < NL; ++m) acc[u][m] = 0.0;
-    }
-    const T c_ent1 = (T)b.c_ent1, c_wind = (T)b.c_wind, c_ent2 = (T)b.c_ent2, c_drag = (T)b.c_drag;
-    const T ttdt = (T)tdt;
     const bool topo = b.topo_active != 0;
-
     // channel strip integrals are formed by tiles holding rows 0, 1, nyp-2, nyp-1
     const bool strips = g.cyclic && (j0 <= 1 || j0 + VT > nyp - 2);
+    // in-domain test of a column (a channel has none outside)
+    auto colok = [&](int gi) { return g.cyclic || (gi >= 0 && gi < nxp); };
 
 #pragma unroll 1
     for (int k = 0; k < NL; ++k) {
-        if (k + 1 < NL) {
-            issue(k + 1);
-            cp_async_wait<1>();
+        if (k + 1 < NL) issue(k + 1);
+        if (tma) {
+            const bool ok = mbar_wait_bounded(&bars[k & 1], (k >> 1) & 1, OQG_WAIT_LIMIT);
+            if (__syncthreads_or(!ok)) {
+                // a tile never arrived: report, drain what is in flight, stop
+                if (threadIdx.x == 0) {
+                    atomicOr(&scal->err, OQG_DERR_TIMEOUT);
+                    mbar_wait_bounded(&bars[k & 1], (k >> 1) & 1, OQG_WAIT_LIMIT);
+                    if (k + 1 < NL) mbar_wait_bounded(&bars[(k + 1) & 1], ((k + 1) >> 1) & 1, OQG_WAIT_LIMIT);
+                }
+                __syncthreads();
+                return;
+            }
         } else {
-            cp_async_wait<0>();
+            if (k + 1 < NL) cp_async_wait<1>();
+            else cp_async_wait<0>();
+            __syncthreads();
         }
-        __syncthreads();
-        const T *sPM = buf0 + (k & 1) * NBUF;
-        const T *sP = sPM + HPM * WPM;
-        const T *sQ = sP + H1 * W1;
-        const T *sQM = sQ + H1 * W1;
-        // del2p on the halo-2 region
-        for (int r = ty0; r < H2; r += 4) {
-            const int gj = j0 - 2 + r;
-            const bool jv = gj >= 0 && gj < nyp;
-            for (int c = tx; c < W2; c += 64) {
-                const int gi = i0 - 2 + c;
+        const T *sPM = sm + (k & 1) * LY.nbuf + LY.pm;
+        const T *sP = sm + (k & 1) * LY.nbuf + LY.p;
+        const T *sQ = sm + (k & 1) * LY.nbuf + LY.q;
+        const T *sQM = sm + (k & 1) * LY.nbuf + LY.qm;
+        // ---- del2(pm) on rows j0-2.., cols i0-2.. (column tx of L2 = 64)
+        {
+            const int gi = i0 - 2 + tx, cs = tx + 2;          // column in the pm tile
+            const bool cv = colok(gi);
+            const int rb = ty * R2, re = min(rb + R2, H2);
+            T sv = sPM[rb * LPQ + cs], cv_ = sPM[(rb + 1) * LPQ + cs];
+            for (int r = rb; r < re; ++r) {
+                const T nv = sPM[(r + 2) * LPQ + cs];
+                const T wv = sPM[(r + 1) * LPQ + cs - 1], ev = sPM[(r + 1) * LPQ + cs + 1];
+                const int gj = j0 - 2 + r;
                 T v = (T)0;
-                if (jv && (g.cyclic || (gi >= 0 && gi < nxp))) v = lap_bc(sPM, WPM, r + 1, c + 1, gi, gj, g);
-                sD2[r * W2 + c] = v;
+                if (cv && gj >= 0 && gj < nyp) v = lap5(wv, ev, sv, nv, cv_, gi, gj, g);
+                sD2[r * L2 + tx] = v;
+                sv = cv_;
+                cv_ = nv;
             }
         }
         __syncthreads();
-        // d4p on the halo-1 region
-        for (int r = ty0; r < H1; r += 4) {
-            const int gj = j0 - 1 + r;
-            const bool jv = gj >= 0 && gj < nyp;
-            for (int c = tx; c < W1; c += 64) {
-                const int gi = i0 - 1 + c;
+        // ---- del4 on rows j0-1.., cols i0-1.. (column tx < L1 = 62)
+        if (tx < L1) {
+            const int gi = i0 - 1 + tx, cs = tx + 1;          // column in the d2 tile
+            const bool cv = colok(gi);
+            const int rb = ty * R1, re = min(rb + R1, H1);
+            T sv = sD2[rb * L2 + cs], cv_ = sD2[(rb + 1) * L2 + cs];
+            for (int r = rb; r < re; ++r) {
+                const T nv = sD2[(r + 2) * L2 + cs];
+                const T wv = sD2[(r + 1) * L2 + cs - 1], ev = sD2[(r + 1) * L2 + cs + 1];
+                const int gj = j0 - 1 + r;
                 T v = (T)0;
-                if (jv && (g.cyclic || (gi >= 0 && gi < nxp))) v = lap_bc(sD2, W2, r + 1, c + 1, gi, gj, g);
-                sD4[r * W1 + c] = v;
+                if (cv && gj >= 0 && gj < nyp) v = lap5(wv, ev, sv, nv, cv_, gi, gj, g);
+                sD4[r * L1 + tx] = v;
+                sv = cv_;
+                cv_ = nv;
             }
         }
         __syncthreads();
 
-        double sq[OQG_NQ];
+        // ---- outputs: column tx < VTX, rows r0 .. r0+R0-1 of the tile
+        if (tx < VTX) {
+            const int gi = i0 + tx;
+            const int c1 = tx + 1;                          // column in the d4 tile
+            const int cp = tx + 4;                          // column in the p/q tiles
+            int ci = gi;
+            if (g.cyclic && ci == N) ci = 0;
+            // rolling windows: d4 (column), p and q (3 x 3)
+            T d4s = sD4[r0 * L1 + c1], d4c = sD4[(r0 + 1) * L1 + c1];
+            T pw[3][3], qw[3][3];
 #pragma unroll
-        for (int q = 0; q < OQG_NQ; ++q) sq[q] = 0.0;
-        const T c2 = (T)b.c2[k], c4 = (T)b.c4[k];
-
+            for (int a = 0; a < 2; ++a)
 #pragma unroll
-        for (int u = 0; u < UMAX; ++u) {
-            const int ty = ty0 + 4 * u;
-            const int gj = j0 + ty, gi = i0 + tx;
-            if (ty >= VT || gj >= nyp || gi >= nxp) continue;
-            const T d4 = sD4[(ty + 1) * W1 + tx + 1];
-            const T d6 = lap_bc(sD4, W1, ty + 1, tx + 1, gi, gj, g);
-            const T jac = arakawa(sP, sQ, W1, ty + 1, tx + 1, gi, gj, g);
-            T dq = jac + c2 * d4 - c4 * d6;
-            const size_t o2 = (size_t)gj * px + gi;
-            if (k == 0) {
-                const T e1 = ENT ? ldg(ENT + o2) : (T)0;
-                dq = dq + c_ent1 * e1 + c_wind * sWK[ty * VTX + tx];
-            }
-            if (k == 1 && ENT) dq = dq - c_ent2 * ldg(ENT + o2);
-            const T d2 = sD2[(ty + 2) * W2 + tx + 2];
-            if (k == kt) dq = dq - c_drag * d2;
-            const T qn = sQM[ty * VTX + tx] + ttdt * dq;
-            QM[((size_t)k * nyp + gj) * px + gi] = qn;
-            // modal right-hand side, FP64 (p_modes_rhs)
-            double ql = (double)qn - by[u];
-            if (k == kt && topo) ql -= b.ddyn[o2];
+                for (int cc = 0; cc < 3; ++cc) {
+                    pw[a + 1][cc] = sP[(r0 + a) * LPQ + cp - 1 + cc];
+                    qw[a + 1][cc] = sQ[(r0 + a) * LPQ + cp - 1 + cc];
+                }
 #pragma unroll
-            for (int m = 0; m < NL; ++m) acc[u][m] += ql * ctl[k + NL * m];
-            if (strips && gi < N) {
-                // channel strip integrands (vorticity.F90:84-101, numerics.F90:374-386)
-                const int r = ty + 1, c = tx + 1;
-                if (gj == 0) {
-                    const T px1 = sP[(r + 1) * W1 + c + 1] - sP[(r + 1) * W1 + c - 1];
-                    sq[0] += (double)(sQ[r * W1 + c] * px1);
-                    sq[4] += (double)(sD2[(ty + 3) * W2 + tx + 2] - d2);
-                    sq[6] += (double)(sD4[(ty + 2) * W1 + tx + 1] - d4);
-                    if (k == kt)
-                        sq[8] += (double)(sPM[(ty + 4) * WPM + tx + 3] - sPM[(ty + 3) * WPM + tx + 3]);
+            for (int u = 0; u < RMAX; ++u) {
+                const int r = r0 + u;
+                if (u >= R0 || r >= VT) break;
+                // shift the windows down one row and load the new bottom row
+                const T d4n = sD4[(r + 2) * L1 + c1];
+                const T d4w = sD4[(r + 1) * L1 + c1 - 1], d4e = sD4[(r + 1) * L1 + c1 + 1];
+#pragma unroll
+                for (int cc = 0; cc < 3; ++cc) {
+                    pw[0][cc] = pw[1][cc]; pw[1][cc] = pw[2][cc];
+                    qw[0][cc] = qw[1][cc]; qw[1][cc] = qw[2][cc];
+                    pw[2][cc] = sP[(r + 2) * LPQ + cp - 1 + cc];
+                    qw[2][cc] = sQ[(r + 2) * LPQ + cp - 1 + cc];
                 }
-                if (gj == 1) {
-                    const T px1 = sP[r * W1 + c + 1] - sP[r * W1 + c - 1];
-                    sq[1] += (double)(sQ[r * W1 + c] * px1);
+                const int gj = j0 + r;
+                if (gj < nyp && gi < nxp) {
+                    const T d6 = lap5(d4w, d4e, d4s, d4n, d4c, ci, gj, g);
+                    const T jac = arakawa3(pw, qw, ci, gj, g);
+                    T dq = jac + sK[10 + k] * d4c - sK[10 + NL + k] * d6;
+                    const size_t o2 = (size_t)gj * px + gi;
+                    if (k == 0) {
+                        const T e1 = ENT ? ldg(ENT + o2) : (T)0;
+                        dq = dq + sK[5] * e1 + sK[6] * sWK[r * LO + tx];
+                    }
+                    if (k == 1 && ENT) dq = dq - sK[7] * ldg(ENT + o2);
+                    if (k == kt) dq = dq - sK[8] * sD2[(r + 2) * L2 + tx + 2];
+                    const T qn = sQM[r * LO + tx] + sK[9] * dq;
+                    QM[((size_t)k * nyp + gj) * px + gi] = qn;
+                    // modal right-hand side, FP64 (p_modes_rhs)
+                    double ql = (double)qn - sBY[r];
+                    if (k == kt && topo) ql -= DD[o2];
+#pragma unroll
+                    for (int m = 0; m < NL; ++m) acc[u][m] += ql * sCtl[k + NL * m];
                 }
-                if (gj == nyp - 1) {
-                    const T pxs = sP[(r - 1) * W1 + c + 1] - sP[(r - 1) * W1 + c - 1];
-                    sq[2] += (double)(sQ[r * W1 + c] * pxs);
-                    sq[5] += (double)(d2 - sD2[(ty + 1) * W2 + tx + 2]);
-                    sq[7] += (double)(d4 - sD4[ty * W1 + tx + 1]);
-                    if (k == kt)
-                        sq[9] += (double)(sPM[(ty + 3) * WPM + tx + 3] - sPM[(ty + 2) * WPM + tx + 3]);
-                }
-                if (gj == nyp - 2) {
-                    const T px1 = sP[r * W1 + c + 1] - sP[r * W1 + c - 1];
-                    sq[3] += (double)(sQ[r * W1 + c] * px1);
-                }
+                d4s = d4c;
+                d4c = d4n;
             }
         }
         if (strips) {
+            // channel strip integrands (vorticity.F90:84-101, numerics.F90:374-386)
+            // of the rows 0, 1, nyp-2, nyp-1 held by this tile
+            double sq[OQG_NQ];
+#pragma unroll
+            for (int q = 0; q < OQG_NQ; ++q) sq[q] = 0.0;
+            const int gi = i0 + tx;
+            if (ty == 0 && tx < VTX && gi < N) {
+                for (int r = 0; r < VT; ++r) {
+                    const int gj = j0 + r;
+                    if (!(gj == 0 || gj == 1 || gj == nyp - 2 || gj == nyp - 1)) continue;
+                    const int c = tx + 4;                   // p/q tile column
+                    const T qc = sQ[(r + 1) * LPQ + c];
+                    const T d2 = sD2[(r + 2) * L2 + tx + 2], d4 = sD4[(r + 1) * L1 + tx + 1];
+                    if (gj == 0) {
+                        sq[0] += (double)(qc * (sP[(r + 2) * LPQ + c + 1] - sP[(r + 2) * LPQ + c - 1]));
+                        sq[4] += (double)(sD2[(r + 3) * L2 + tx + 2] - d2);
+                        sq[6] += (double)(sD4[(r + 2) * L1 + tx + 1] - d4);
+                        if (k == kt)
+                            sq[8] += (double)(sPM[(r + 4) * LPQ + tx + 4] - sPM[(r + 3) * LPQ + tx + 4]);
+                    }
+                    if (gj == 1) sq[1] += (double)(qc * (sP[(r + 1) * LPQ + c + 1] - sP[(r + 1) * LPQ + c - 1]));
+                    if (gj == nyp - 1) {
+                        sq[2] += (double)(qc * (sP[r * LPQ + c + 1] - sP[r * LPQ + c - 1]));
+                        sq[5] += (double)(d2 - sD2[(r + 1) * L2 + tx + 2]);
+                        sq[7] += (double)(d4 - sD4[r * L1 + tx + 1]);
+                        if (k == kt)
+                            sq[9] += (double)(sPM[(r + 3) * LPQ + tx + 4] - sPM[(r + 2) * LPQ + tx + 4]);
+                    }
+                    if (gj == nyp - 2) sq[3] += (double)(qc * (sP[(r + 1) * LPQ + c + 1] - sP[(r + 1) * LPQ + c - 1]));
+                }
+            }
             double *pt = b.part_tile + ((size_t)w.block * b.nl + k) * OQG_NQ;
 #pragma unroll
             for (int q = 0; q < OQG_NQ; ++q) {
@@ -354,16 +563,18 @@ k_vort(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par,
     T *RHS = (T *)b.rhs;
     const int ioff = g.cyclic ? 0 : 1;
     const double f0 = b.fnot;
+    if (tx < VTX) {
 #pragma unroll
-    for (int u = 0; u < UMAX; ++u) {
-        const int ty = ty0 + 4 * u;
-        const int gj = j0 + ty, gi = i0 + tx;
-        if (ty >= VT || gj < 1 || gj > nyp - 2) continue;
-        const int xi = gi - ioff;
-        if (xi < 0 || xi >= b.nxin) continue;
+        for (int u = 0; u < RMAX; ++u) {
+            const int r = r0 + u;
+            const int gj = j0 + r, gi = i0 + tx;
+            if (u >= R0 || r >= VT || gj < 1 || gj > nyp - 2) continue;
+            const int xi = gi - ioff;
+            if (xi < 0 || xi >= b.nxin) continue;
 #pragma unroll
-        for (int m = 0; m < NL; ++m)
-            RHS[((size_t)m * b.ny + (gj - 1)) * b.pr + xi] = (T)(f0 * acc[u][m]);
+            for (int m = 0; m < NL; ++m)
+                RHS[((size_t)m * b.ny + (gj - 1)) * b.pr + xi] = (T)(f0 * acc[u][m]);
+        }
     }
 }
 
