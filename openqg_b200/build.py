@@ -14,7 +14,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "liboqg.so")
 SOURCES = ["oqg_capi.cu", "oqg_setup.cpp"]
-DEPS = SOURCES + ["oqg_dev.cuh", "oqg_fft.cuh", "oqg_kernels.cuh", "oqg_setup.h",
+DEPS = SOURCES + ["oqg_dev.cuh", "oqg_fft.cuh", "oqg_kernels.cuh", "oqg_tma.cuh", "oqg_setup.h",
                   os.path.join("..", "..", "include", "oqg.h")]
 
 NVCC_FLAGS = [

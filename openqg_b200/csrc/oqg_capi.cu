@@ -70,7 +70,7 @@ static X *dalloc(oqg_handle *h, size_t count) {
 }
 
 // ----------------------------------------------------------- launch helpers
-static const int XTHREADS = 256;
+static const int XTHREADS = XINV_FFT_THREADS;
 
 // Launch with programmatic stream serialisation: the kernel may be scheduled
 // while its predecessor drains and waits in griddepcontrol.wait for its data.
@@ -96,10 +96,11 @@ static void launch_step_t(oqg_handle *h, int par, double tdt) {
     launch_pdl(k_vort<T, NL>, h->nv, VTHREADS, h->smem_v, h->st, h->d_bas, h->d_wv, par, tdt);
     launch_pdl(k_xfwd<T, E>, h->nx, h->xthreads, h->smem_x, h->st, h->d_bas, h->d_wx, (const void *)nullptr);
     if (b.cyclic)
-        launch_pdl(k_ysolve<T, true, NL>, h->nys, 32 * h->KB, h->smem_y, h->st, h->d_bas, h->d_wy, tdt, 1);
+        launch_pdl(k_ysolve<T, true, NL>, h->nys, 32 * h->KB, h->smem_y, h->st, h->d_bas, h->d_wy);
     else
-        launch_pdl(k_ysolve<T, false, NL>, h->nys, 32 * h->KB, h->smem_y, h->st, h->d_bas, h->d_wy, tdt, 1);
-    launch_pdl(k_xinv<T, E, NL>, h->ni, XTHREADS, h->smem_i, h->st, h->d_bas, h->d_wi, par, (double *)nullptr);
+        launch_pdl(k_ysolve<T, false, NL>, h->nys, 32 * h->KB, h->smem_y, h->st, h->d_bas, h->d_wy);
+    launch_pdl(k_xinv<T, E, NL>, h->ni, XINV_THREADS, h->smem_i, h->st, h->d_bas, h->d_wi, par, tdt,
+               (double *)nullptr);
 }
 
 // FP64 solve of the modal Helmholtz problems with the rhs buffer as input;
@@ -108,10 +109,10 @@ template <int NL, int E>
 static void launch_solve_t(oqg_handle *h, double *out) {
     k_xfwd<double, E><<<h->nx, h->xthreads, h->smem_x64, h->st>>>(h->d_bas64, h->d_wx, nullptr);
     if (h->hb.cyclic)
-        k_ysolve<double, true, NL><<<h->nys, 32 * h->KB, h->smem_y, h->st>>>(h->d_bas64, h->d_wy, 0.0, 0);
+        k_ysolve<double, true, NL><<<h->nys, 32 * h->KB, h->smem_y, h->st>>>(h->d_bas64, h->d_wy);
     else
-        k_ysolve<double, false, NL><<<h->nys, 32 * h->KB, h->smem_y, h->st>>>(h->d_bas64, h->d_wy, 0.0, 0);
-    k_xinv<double, E, NL><<<h->ni, XTHREADS, h->smem_i64, h->st>>>(h->d_bas64, h->d_wi, 0, out);
+        k_ysolve<double, false, NL><<<h->nys, 32 * h->KB, h->smem_y, h->st>>>(h->d_bas64, h->d_wy);
+    k_xinv<double, E, NL><<<h->ni, XINV_THREADS, h->smem_i64, h->st>>>(h->d_bas64, h->d_wi, 0, 0.0, out);
 }
 
 template <class T, int NL, int E>
@@ -386,11 +387,11 @@ static void launch_phase_t(oqg_handle *h, int phase, int par, double tdt) {
         case 1: k_xfwd<T, E><<<h->nx, h->xthreads, h->smem_x, h->st>>>(h->d_bas, h->d_wx, nullptr); break;
         case 2:
             if (b.cyclic)
-                k_ysolve<T, true, NL><<<h->nys, 32 * h->KB, h->smem_y, h->st>>>(h->d_bas, h->d_wy, tdt, 1);
+                k_ysolve<T, true, NL><<<h->nys, 32 * h->KB, h->smem_y, h->st>>>(h->d_bas, h->d_wy);
             else
-                k_ysolve<T, false, NL><<<h->nys, 32 * h->KB, h->smem_y, h->st>>>(h->d_bas, h->d_wy, tdt, 1);
+                k_ysolve<T, false, NL><<<h->nys, 32 * h->KB, h->smem_y, h->st>>>(h->d_bas, h->d_wy);
             break;
-        default: k_xinv<T, E, NL><<<h->ni, XTHREADS, h->smem_i, h->st>>>(h->d_bas, h->d_wi, par, nullptr); break;
+        default: k_xinv<T, E, NL><<<h->ni, XINV_THREADS, h->smem_i, h->st>>>(h->d_bas, h->d_wi, par, tdt, nullptr); break;
     }
 }
 static void launch_phase(oqg_handle *h, int phase, int par, double tdt) {
@@ -573,12 +574,14 @@ int oqg_create(const oqg_params *prm, oqg_handle **out) {
     }
     b.part_tile = dalloc<double>(h, (size_t)b.tiles_x * b.tiles_y * b.nl * OQG_NQ);
     b.part_col = dalloc<double>(h, (size_t)b.nl * b.nk);
-    b.sc = dalloc<DevScalars>(h, 1);
+    b.st = dalloc<DevState>(h, 2);
+    b.frc = dalloc<DevForcing>(h, 1);
+    b.err = dalloc<int>(h, 1);
     h->stage[0] = dalloc<double>(h, n3);
     h->stage[1] = dalloc<double>(h, n3);
     h->d_bad = dalloc<unsigned long long>(h, 1);
     h->d_diag = dalloc<double>(h, 4 * (size_t)b.nl);
-    if (!b.sc || !h->stage[1] || !h->d_diag) return bail(OQG_ECUDA, "out of device memory");
+    if (!b.st || !b.frc || !b.err || !h->stage[1] || !h->d_diag) return bail(OQG_ECUDA, "out of device memory");
     CK(cudaMemcpy(d_yp, yp.data(), yp.size() * sizeof(double), cudaMemcpyHostToDevice));
 
     // ---- launch geometry
@@ -587,8 +590,8 @@ int oqg_create(const oqg_params *prm, oqg_handle **out) {
     const size_t t2 = 2 * h->esz;
     const int npm = (b.ny + 1) / 2;
     h->nv = b.tiles_x * b.tiles_y;
-    // forward transform: one row pair per group, CTAs of >= 128 threads
-    const int GX = std::max(1, 128 / TT);
+    // forward transform: one row pair per group, CTAs of >= 256 threads
+    const int GX = std::max(1, 256 / TT);
     h->xthreads = GX * TT;
     h->nx = (b.nl * npm + GX - 1) / GX;
     const size_t vsz = (size_t)(b.cyclic ? 16 : 8);
@@ -597,8 +600,7 @@ int oqg_create(const oqg_params *prm, oqg_handle **out) {
     const int S_ = (b.ny + 31) / 32;
     const int LDy = (b.ny + 32) | 1;
     (void)S_;
-    b.k3_blocks = b.nl * ((b.nk + h->KB - 1) / h->KB);
-    h->nys = b.k3_blocks;
+    h->nys = b.nl * ((b.nk + h->KB - 1) / h->KB);
     b.k4_rows = 2;
     h->ni = (b.ny + b.k4_rows - 1) / b.k4_rows;
     h->smem_v = vort_smem_bytes(b.vty, (int)h->esz);
@@ -683,8 +685,8 @@ int oqg_set_state_full(oqg_handle *h, const double *p, const double *pm, const d
         stage_to_field(h, h->stage[0], b.F[dst[f]], n3);
         CK(cudaStreamSynchronize(h->st));
     }
-    DevScalars sc;
-    CK(cudaMemcpy(&sc, b.sc, sizeof sc, cudaMemcpyDeviceToHost));
+    DevState sc;
+    CK(cudaMemcpy(&sc, b.st + par, sizeof sc, cudaMemcpyDeviceToHost));
     for (int l = 0; l < b.nl - 1; ++l) { sc.dpi[l] = dpi[l]; sc.dpip[l] = dpip[l]; }
     for (int k = 0; k < b.nl; ++k) {
         if (cs) sc.cs[k] = cs[k];
@@ -692,7 +694,7 @@ int oqg_set_state_full(oqg_handle *h, const double *p, const double *pm, const d
         if (csp) sc.csp[k] = csp[k];
         if (cnp) sc.cnp[k] = cnp[k];
     }
-    CK(cudaMemcpy(b.sc, &sc, sizeof sc, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(b.st + par, &sc, sizeof sc, cudaMemcpyHostToDevice));
     return OQG_OK;
 }
 
@@ -728,9 +730,9 @@ int oqg_get_p_layer(oqg_handle *h, int k, double *out) {
 int oqg_get_constraints(oqg_handle *h, double *dpi, double *dpip, double *cs, double *cn,
                         double *csp, double *cnp) {
     if (!h) return fail(OQG_EINVAL, "null handle");
-    DevScalars sc;
+    DevState sc;
     CK(cudaStreamSynchronize(h->st));
-    CK(cudaMemcpy(&sc, h->hb.sc, sizeof sc, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(&sc, h->hb.st + h->par, sizeof sc, cudaMemcpyDeviceToHost));
     const int nl = h->hb.nl;
     for (int l = 0; l < nl - 1; ++l) {
         if (dpi) dpi[l] = sc.dpi[l];
@@ -777,7 +779,7 @@ int oqg_set_forcing(oqg_handle *h, const double *wekp, const double *ent, double
     if (h->mixed) k_forcing_integrals<float><<<1, 512, 0, h->st>>>(h->d_bas, 0);
     else k_forcing_integrals<double><<<1, 512, 0, h->st>>>(h->d_bas, 0);
     double tx[2] = {txis, txin};
-    CK(cudaMemcpyAsync(&b.sc->txis, tx, 2 * sizeof(double), cudaMemcpyHostToDevice, h->st));
+    CK(cudaMemcpyAsync(&b.frc->txis, tx, 2 * sizeof(double), cudaMemcpyHostToDevice, h->st));
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(h->st));
     return OQG_OK;
@@ -818,7 +820,7 @@ int oqg_step(oqg_handle *h, double tdt, int nsteps) {
 
 int oqg_set_step_index(oqg_handle *h, long long steps_done) {
     if (!h || steps_done < 0) return fail(OQG_EINVAL, "bad argument");
-    CK(cudaMemcpyAsync(&h->hb.sc->nt, &steps_done, sizeof(long long), cudaMemcpyHostToDevice, h->st));
+    CK(cudaMemcpyAsync(&h->hb.st[h->par].nt, &steps_done, sizeof(long long), cudaMemcpyHostToDevice, h->st));
     CK(cudaStreamSynchronize(h->st));
     return OQG_OK;
 }
@@ -826,7 +828,7 @@ int oqg_set_step_index(oqg_handle *h, long long steps_done) {
 int oqg_get_step_index(oqg_handle *h, long long *steps_done) {
     if (!h || !steps_done) return fail(OQG_EINVAL, "bad argument");
     CK(cudaStreamSynchronize(h->st));
-    CK(cudaMemcpy(steps_done, &h->hb.sc->nt, sizeof(long long), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(steps_done, &h->hb.st[h->par].nt, sizeof(long long), cudaMemcpyDeviceToHost));
     return OQG_OK;
 }
 
@@ -842,7 +844,7 @@ int oqg_sync(oqg_handle *h) {
     if (!h) return fail(OQG_EINVAL, "null handle");
     CK(cudaStreamSynchronize(h->st));
     int err = 0;
-    CK(cudaMemcpy(&err, &h->hb.sc->err, sizeof(int), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(&err, h->hb.err, sizeof(int), cudaMemcpyDeviceToHost));
     if (err) return fail(OQG_ECUDA, "device error flag set");
     return OQG_OK;
 }

@@ -16,25 +16,25 @@
 
 namespace oqg {
 
-// Scalars of the constraint equations and the step bookkeeping.  One writer
-// per step: the last CTA of the y-solve kernel (the scalar phase).
-struct DevScalars {
+// Scalars of the constraint equations and the step counter.  Two copies,
+// by step parity: a step with parity `par` reads st[par] and its assembly
+// kernel (CTA 0) writes the next values to st[1-par].
+struct DevState {
     double dpi[OQG_NLMAX], dpip[OQG_NLMAX];              // mass constraint (constraint.F90:63-67)
     double cs[OQG_NLMAX], cn[OQG_NLMAX];                 // channel momentum constraints
     double csp[OQG_NLMAX], cnp[OQG_NLMAX];
-    double alpha[OQG_NLMAX];                             // box homogeneous coefficients
-    double c_bt, c_bc1[OQG_NLMAX], c_bc2[OQG_NLMAX];     // channel homogeneous coefficients
+    long long nt;                                        // steps done (nt-1 of the next)
+    long long pad_;
+};
+
+// Forcing scalars that depend only on the forcing fields.
+struct DevForcing {
     double ent_xn;                                       // area integral of ent layer 1
     double int_Be_s[OQG_NLMAX], int_Be_n[OQG_NLMAX];     // channel ent strip integrals
     double txis, txin;
-    long long nt;                                        // steps done (nt-1 of the next)
-    int suppress_flag;                                   // set for the assembly kernel
-    unsigned int counter;                                // last-CTA detection
-    int err;                                             // device error bits
 };
 
 // Device error bits
-#define OQG_DERR_SOLVE   1   // zero pivot in the constraint solve
 #define OQG_DERR_TIMEOUT 2   // a bounded wait for a tile load ran out
 
 // Number of per-tile channel strip quantities per layer (vorticity kernel)
@@ -92,10 +92,11 @@ struct BasinDev {
     const double *hbt;          // channel: [nyp] barotropic homogeneous solution
     const double *hbc1, *hbc2;  // channel: [nl][nyp]
     double *part_tile;          // [tiles][nl][OQG_NQ]
-    double *part_col;           // [nl][nk]
-    DevScalars *sc;
+    double *part_col;           // [y-solve CTAs]: dst_w-weighted column sums
+    DevState *st;               // [2] by step parity
+    DevForcing *frc;
+    int *err;                   // device error bits
     // launch bookkeeping
-    int k3_blocks;              // CTAs of this basin in the y-solve launch
     int k4_rows;                // interior rows per CTA of the assembly launch
 };
 

@@ -178,14 +178,22 @@ __device__ __forceinline__ void fft_stage(const typename C2<T>::t *__restrict__ 
     }
 }
 
+// Barrier `id` over the first `n` threads of the CTA (n a multiple of 32);
+// n = 0: all threads of the CTA (__syncthreads).
+__device__ __forceinline__ void bar_sync(int id, int n) {
+    if (n == 0) __syncthreads();
+    else asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory");
+}
+
 // Forward FFT of length M (radices rad[0..nrad)) from padded buffer a, using
 // padded buffer b as the second buffer of the ping-pong.  Returns the buffer
-// holding the result.  All threads of the CTA must call it (it synchronises
-// the CTA); threads with t >= TT only take part in the barriers.
+// holding the result.  The nbar threads that synchronise on barrier bar_id
+// must all call it; threads with t >= TT only take part in the barriers.
 template <class T>
 __device__ typename C2<T>::t *fft_smem(typename C2<T>::t *a, typename C2<T>::t *b, int M,
                                        const int *rad, int nrad,
-                                       const typename C2<T>::t *__restrict__ tw, int t, int TT) {
+                                       const typename C2<T>::t *__restrict__ tw, int t, int TT,
+                                       int bar_id, int nbar) {
     typedef typename C2<T>::t T2;
     T2 *src = a, *dst = b;
     int Ns = 1;
@@ -198,7 +206,7 @@ __device__ typename C2<T>::t *fft_smem(typename C2<T>::t *a, typename C2<T>::t *
             case 3: fft_stage<T, 3>(src, dst, M, Ns, tw, t, TT); break;
             default: fft_stage<T, 5>(src, dst, M, Ns, tw, t, TT); break;
         }
-        __syncthreads();
+        bar_sync(bar_id, nbar);
         T2 *x = src; src = dst; dst = x;
         Ns *= R;
     }

@@ -65,6 +65,8 @@ __device__ __forceinline__ double block_sum(double v, double *red) {
 #define VTX 60          // output columns of a vorticity tile
 #define VTYMAX 17       // output rows of a vorticity tile (at most)
 #define VTHREADS 256    // 64 column lanes x 4 row strips
+#define XINV_FFT_THREADS 256                    // transform threads of k_xinv
+#define XINV_THREADS (XINV_FFT_THREADS + 32)    // plus the scalar-phase warp
 
 // Geometry scalars of a basin used by the stencils.
 template <class T> struct Geo {
@@ -304,6 +306,7 @@ __global__ void __launch_bounds__(VTHREADS, 2)
 k_vort(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par, double tdt) {
     constexpr int LPQ = VTX + 8, L2 = VTX + 4, L1 = VTX + 2, LO = VTX;
     constexpr int RMAX = (VTYMAX + 3) / 4;     // output rows per strip
+    constexpr int R2MAX = (VTYMAX + 4 + 3) / 4, R1MAX = (VTYMAX + 2 + 3) / 4;
     const Work w = work[blockIdx.x];
     const BasinDev &b = bas[w.member];
     // uniform constants in shared memory: fx fy fxb fyb jac | c_ent1 c_wind
@@ -345,7 +348,6 @@ k_vort(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par,
     const int tx = threadIdx.x & 63, ty = threadIdx.x >> 6;
     const bool tma = !g.cyclic && b.tmaps != nullptr;
     const unsigned char *tm = (const unsigned char *)b.tmaps;
-    DevScalars *scal = b.sc;
 
     if (tma && threadIdx.x == 0) {
         mbar_init(&bars[0], 1);
@@ -409,7 +411,7 @@ k_vort(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par,
             if (__syncthreads_or(!ok)) {
                 // a tile never arrived: report, drain what is in flight, stop
                 if (threadIdx.x == 0) {
-                    atomicOr(&scal->err, OQG_DERR_TIMEOUT);
+                    atomicOr(b.err, OQG_DERR_TIMEOUT);
                     mbar_wait_bounded(&bars[k & 1], (k >> 1) & 1, OQG_WAIT_LIMIT);
                     if (k + 1 < NL) mbar_wait_bounded(&bars[(k + 1) & 1], ((k + 1) >> 1) & 1, OQG_WAIT_LIMIT);
                 }
@@ -429,17 +431,22 @@ k_vort(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par,
         {
             const int gi = i0 - 2 + tx, cs = tx + 2;          // column in the pm tile
             const bool cv = colok(gi);
-            const int rb = ty * R2, re = min(rb + R2, H2);
-            T sv = sPM[rb * LPQ + cs], cv_ = sPM[(rb + 1) * LPQ + cs];
-            for (int r = rb; r < re; ++r) {
-                const T nv = sPM[(r + 2) * LPQ + cs];
-                const T wv = sPM[(r + 1) * LPQ + cs - 1], ev = sPM[(r + 1) * LPQ + cs + 1];
-                const int gj = j0 - 2 + r;
-                T v = (T)0;
-                if (cv && gj >= 0 && gj < nyp) v = lap5(wv, ev, sv, nv, cv_, gi, gj, g);
-                sD2[r * L2 + tx] = v;
-                sv = cv_;
-                cv_ = nv;
+            const int rb = ty * R2;
+            const T *col = sPM + rb * LPQ + cs;
+            T sv = col[0], cv_ = col[LPQ];
+#pragma unroll
+            for (int u = 0; u < R2MAX; ++u) {
+                const int r = rb + u;
+                if (u < R2 && r < H2) {
+                    const T nv = col[(u + 2) * LPQ];
+                    const T wv = col[(u + 1) * LPQ - 1], ev = col[(u + 1) * LPQ + 1];
+                    const int gj = j0 - 2 + r;
+                    T v = (T)0;
+                    if (cv && gj >= 0 && gj < nyp) v = lap5(wv, ev, sv, nv, cv_, gi, gj, g);
+                    sD2[r * L2 + tx] = v;
+                    sv = cv_;
+                    cv_ = nv;
+                }
             }
         }
         __syncthreads();
@@ -447,74 +454,92 @@ k_vort(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par,
         if (tx < L1) {
             const int gi = i0 - 1 + tx, cs = tx + 1;          // column in the d2 tile
             const bool cv = colok(gi);
-            const int rb = ty * R1, re = min(rb + R1, H1);
-            T sv = sD2[rb * L2 + cs], cv_ = sD2[(rb + 1) * L2 + cs];
-            for (int r = rb; r < re; ++r) {
-                const T nv = sD2[(r + 2) * L2 + cs];
-                const T wv = sD2[(r + 1) * L2 + cs - 1], ev = sD2[(r + 1) * L2 + cs + 1];
-                const int gj = j0 - 1 + r;
-                T v = (T)0;
-                if (cv && gj >= 0 && gj < nyp) v = lap5(wv, ev, sv, nv, cv_, gi, gj, g);
-                sD4[r * L1 + tx] = v;
-                sv = cv_;
-                cv_ = nv;
+            const int rb = ty * R1;
+            const T *col = sD2 + rb * L2 + cs;
+            T sv = col[0], cv_ = col[L2];
+#pragma unroll
+            for (int u = 0; u < R1MAX; ++u) {
+                const int r = rb + u;
+                if (u < R1 && r < H1) {
+                    const T nv = col[(u + 2) * L2];
+                    const T wv = col[(u + 1) * L2 - 1], ev = col[(u + 1) * L2 + 1];
+                    const int gj = j0 - 1 + r;
+                    T v = (T)0;
+                    if (cv && gj >= 0 && gj < nyp) v = lap5(wv, ev, sv, nv, cv_, gi, gj, g);
+                    sD4[r * L1 + tx] = v;
+                    sv = cv_;
+                    cv_ = nv;
+                }
             }
         }
         __syncthreads();
 
-        // ---- outputs: column tx < VTX, rows r0 .. r0+R0-1 of the tile
+        // ---- outputs: column tx < VTX, rows r0 .. r0+R0-1 of the tile.
+        // Only points off the solid walls are stepped: on a wall the Arakawa
+        // Jacobian is zero and the stepped q is replaced by ocqbdy
+        // (vorsubs.F90:58-114) in the assembly kernel, so the interior
+        // stencils are the whole computation here.
         if (tx < VTX) {
             const int gi = i0 + tx;
-            const int c1 = tx + 1;                          // column in the d4 tile
-            const int cp = tx + 4;                          // column in the p/q tiles
-            int ci = gi;
-            if (g.cyclic && ci == N) ci = 0;
+            const bool xin = g.cyclic ? (gi < nxp) : (gi >= 1 && gi <= nxp - 2);
+            const T *d4col = sD4 + r0 * L1 + tx + 1;       // column in the d4 tile
+            const T *pcol = sP + r0 * LPQ + tx + 4;         // column in the p/q tiles
+            const T *qcol = sQ + r0 * LPQ + tx + 4;
+            const T fx = gfx(g), fy = gfy(g);
             // rolling windows: d4 (column), p and q (3 x 3)
-            T d4s = sD4[r0 * L1 + c1], d4c = sD4[(r0 + 1) * L1 + c1];
+            T d4s = d4col[0], d4c = d4col[L1];
             T pw[3][3], qw[3][3];
 #pragma unroll
             for (int a = 0; a < 2; ++a)
 #pragma unroll
                 for (int cc = 0; cc < 3; ++cc) {
-                    pw[a + 1][cc] = sP[(r0 + a) * LPQ + cp - 1 + cc];
-                    qw[a + 1][cc] = sQ[(r0 + a) * LPQ + cp - 1 + cc];
+                    pw[a + 1][cc] = pcol[a * LPQ - 1 + cc];
+                    qw[a + 1][cc] = qcol[a * LPQ - 1 + cc];
                 }
 #pragma unroll
             for (int u = 0; u < RMAX; ++u) {
                 const int r = r0 + u;
-                if (u >= R0 || r >= VT) break;
-                // shift the windows down one row and load the new bottom row
-                const T d4n = sD4[(r + 2) * L1 + c1];
-                const T d4w = sD4[(r + 1) * L1 + c1 - 1], d4e = sD4[(r + 1) * L1 + c1 + 1];
-#pragma unroll
-                for (int cc = 0; cc < 3; ++cc) {
-                    pw[0][cc] = pw[1][cc]; pw[1][cc] = pw[2][cc];
-                    qw[0][cc] = qw[1][cc]; qw[1][cc] = qw[2][cc];
-                    pw[2][cc] = sP[(r + 2) * LPQ + cp - 1 + cc];
-                    qw[2][cc] = sQ[(r + 2) * LPQ + cp - 1 + cc];
-                }
                 const int gj = j0 + r;
-                if (gj < nyp && gi < nxp) {
-                    const T d6 = lap5(d4w, d4e, d4s, d4n, d4c, ci, gj, g);
-                    const T jac = arakawa3(pw, qw, ci, gj, g);
-                    T dq = jac + sK[10 + k] * d4c - sK[10 + NL + k] * d6;
-                    const size_t o2 = (size_t)gj * px + gi;
-                    if (k == 0) {
-                        const T e1 = ENT ? ldg(ENT + o2) : (T)0;
-                        dq = dq + sK[5] * e1 + sK[6] * sWK[r * LO + tx];
-                    }
-                    if (k == 1 && ENT) dq = dq - sK[7] * ldg(ENT + o2);
-                    if (k == kt) dq = dq - sK[8] * sD2[(r + 2) * L2 + tx + 2];
-                    const T qn = sQM[r * LO + tx] + sK[9] * dq;
-                    QM[((size_t)k * nyp + gj) * px + gi] = qn;
-                    // modal right-hand side, FP64 (p_modes_rhs)
-                    double ql = (double)qn - sBY[r];
-                    if (k == kt && topo) ql -= DD[o2];
+                if (u < R0 && r < VT) {
+                    // shift the windows down one row and load the new bottom row
+                    const T d4n = d4col[(u + 2) * L1];
+                    const T d4w = d4col[(u + 1) * L1 - 1], d4e = d4col[(u + 1) * L1 + 1];
 #pragma unroll
-                    for (int m = 0; m < NL; ++m) acc[u][m] += ql * sCtl[k + NL * m];
+                    for (int cc = 0; cc < 3; ++cc) {
+                        pw[0][cc] = pw[1][cc]; pw[1][cc] = pw[2][cc];
+                        qw[0][cc] = qw[1][cc]; qw[1][cc] = qw[2][cc];
+                        pw[2][cc] = pcol[(u + 2) * LPQ - 1 + cc];
+                        qw[2][cc] = qcol[(u + 2) * LPQ - 1 + cc];
+                    }
+                    if (xin && gj >= 1 && gj <= nyp - 2) {
+                        const T d6 = fx * (d4w + d4e - (T)2 * d4c) + fy * (d4s + d4n - (T)2 * d4c);
+                        // Arakawa J(q, p), numerics.F90:370-372
+                        const T pxc = pw[1][2] - pw[1][0], pyc = pw[2][1] - pw[0][1];
+                        const T qxc = qw[1][2] - qw[1][0], qyc = qw[2][1] - qw[0][1];
+                        const T A = qw[1][2] * (pw[2][2] - pw[0][2]) - qw[1][0] * (pw[2][0] - pw[0][0]);
+                        const T Dd = pw[1][2] * (qw[2][2] - qw[0][2]) - pw[1][0] * (qw[2][0] - qw[0][0]);
+                        const T Bv = qw[2][1] * (pw[2][2] - pw[2][0]) - qw[0][1] * (pw[0][2] - pw[0][0]);
+                        const T Cc = pw[2][1] * (qw[2][2] - qw[2][0]) - pw[0][1] * (qw[0][2] - qw[0][0]);
+                        const T jac = gjac(g) * (qxc * pyc - qyc * pxc + A - Bv + Cc - Dd);
+                        T dq = jac + sK[10 + k] * d4c - sK[10 + NL + k] * d6;
+                        const size_t o2 = (size_t)gj * px + gi;
+                        if (k == 0) {
+                            const T e1 = ENT ? ldg(ENT + o2) : (T)0;
+                            dq = dq + sK[5] * e1 + sK[6] * sWK[r * LO + tx];
+                        }
+                        if (k == 1 && ENT) dq = dq - sK[7] * ldg(ENT + o2);
+                        if (k == kt) dq = dq - sK[8] * sD2[(r + 2) * L2 + tx + 2];
+                        const T qn = sQM[r * LO + tx] + sK[9] * dq;
+                        QM[((size_t)k * nyp + gj) * px + gi] = qn;
+                        // modal right-hand side, FP64 (p_modes_rhs)
+                        double ql = (double)qn - sBY[r];
+                        if (k == kt && topo) ql -= DD[o2];
+#pragma unroll
+                        for (int m = 0; m < NL; ++m) acc[u][m] += ql * sCtl[k + NL * m];
+                    }
+                    d4s = d4c;
+                    d4c = d4n;
                 }
-                d4s = d4c;
-                d4c = d4n;
             }
         }
         if (strips) {
@@ -639,7 +664,7 @@ k_xfwd(const BasinDev *__restrict__ bas, const Work *__restrict__ work, const vo
         }
     }
     __syncthreads();
-    T2 *z = fft_smem<T>(za, zb, M, b.rad, b.nrad, sTw, live ? t : TT, TT);
+    T2 *z = fft_smem<T>(za, zb, M, b.rad, b.nrad, sTw, live ? t : TT, TT, 0, 0);
     if (!live) return;
     if (!b.cyclic) {
         T *S = (T *)b.spec;
@@ -704,12 +729,10 @@ __device__ __forceinline__ double yt_re(double v) { return v; }
 __device__ __forceinline__ double yt_re(double2 v) { return v.x; }
 
 // forward declaration of the scalar phase
-template <class T, int NL> __device__ void scalar_phase(const BasinDev &b, double tdt);
 
 template <class T, bool CPLX, int NL>
 __global__ void __launch_bounds__(128)
-k_ysolve(const BasinDev *__restrict__ bas, const Work *__restrict__ work,
-         double tdt, int do_scalar) {
+k_ysolve(const BasinDev *__restrict__ bas, const Work *__restrict__ work) {
     typedef typename YT<T, CPLX>::v V;
     typedef typename YT<T, CPLX>::g Gm;
     constexpr int KB = 4;                       // columns (warps) per CTA
@@ -728,8 +751,6 @@ k_ysolve(const BasinDev *__restrict__ bas, const Work *__restrict__ work,
     extern __shared__ __align__(16) unsigned char smem_raw[];
     V *tile = reinterpret_cast<V *>(smem_raw);                 // [KB][LD]
     double *pvs = reinterpret_cast<double *>(tile + KB * LD);  // [KB][LD] pivots
-    __shared__ int s_last;
-
     const int k = k0 + c;
     const bool live = k < nk;
     const int pidx = m * nk + (live ? k : 0);
@@ -784,15 +805,11 @@ k_ysolve(const BasinDev *__restrict__ bas, const Work *__restrict__ work,
         // forward elimination: u_j = f_j beta_j - a beta_j u_{j-1}
         V C = yt_zero(V());
         double D = 1.0;
-        for (int t0 = 0; t0 < n; t0 += CH) {
-            double bt[CH];
-            V f[CH];
-#pragma unroll
-            for (int u = 0; u < CH; ++u)
-                if (t0 + u < n) { bt[u] = pc[o + t0 + u]; f[u] = col[o + t0 + u]; }
-#pragma unroll
-            for (int u = 0; u < CH; ++u)
-                if (t0 + u < n) { C = yt_axpy(yt_scale(f[u], bt[u]), -a * bt[u], C); D = -a * bt[u] * D; }
+#pragma unroll 8
+        for (int t = 0; t < n; ++t) {
+            const double bt = pc[o + t];
+            C = yt_axpy(yt_scale(col[o + t], bt), -a * bt, C);
+            D = -a * bt * D;
         }
         for (int q = 1; q < 32; q <<= 1) {
             V Co = yt_up(C, q);
@@ -801,30 +818,20 @@ k_ysolve(const BasinDev *__restrict__ bas, const Work *__restrict__ work,
         }
         V uu = yt_up(C, 1);
         if (lane == 0) uu = yt_zero(V());
-        for (int t0 = 0; t0 < n; t0 += CH) {
-            double bt[CH];
-            V f[CH];
-#pragma unroll
-            for (int u = 0; u < CH; ++u)
-                if (t0 + u < n) { bt[u] = pc[o + t0 + u]; f[u] = col[o + t0 + u]; }
-#pragma unroll
-            for (int u = 0; u < CH; ++u)
-                if (t0 + u < n) { uu = yt_axpy(yt_scale(f[u], bt[u]), -a * bt[u], uu); col[o + t0 + u] = uu; }
+#pragma unroll 8
+        for (int t = 0; t < n; ++t) {
+            const double bt = pc[o + t];
+            uu = yt_axpy(yt_scale(col[o + t], bt), -a * bt, uu);
+            col[o + t] = uu;
         }
         // back substitution: u_j = u'_j - a beta_j u_{j+1}
         C = yt_zero(V());
         D = 1.0;
-        for (int t1 = n; t1 > 0; t1 -= CH) {
-            double ej[CH];
-            V f[CH];
-#pragma unroll
-            for (int u = 0; u < CH; ++u) {
-                const int t = t1 - 1 - u;
-                if (t >= 0) { ej[u] = (s + t == ny - 1) ? 0.0 : -a * pc[o + t]; f[u] = col[o + t]; }
-            }
-#pragma unroll
-            for (int u = 0; u < CH; ++u)
-                if (t1 - 1 - u >= 0) { C = yt_axpy(f[u], ej[u], C); D = ej[u] * D; }
+#pragma unroll 8
+        for (int t = n - 1; t >= 0; --t) {
+            const double ej = (s + t == ny - 1) ? 0.0 : -a * pc[o + t];
+            C = yt_axpy(col[o + t], ej, C);
+            D = ej * D;
         }
         for (int q = 1; q < 32; q <<= 1) {
             V Co = yt_dn(C, q);
@@ -834,19 +841,12 @@ k_ysolve(const BasinDev *__restrict__ bas, const Work *__restrict__ work,
         uu = yt_dn(C, 1);
         if (lane == 31) uu = yt_zero(V());
         double colsum = 0.0;
-        for (int t1 = n; t1 > 0; t1 -= CH) {
-            double ej[CH];
-            V f[CH];
-#pragma unroll
-            for (int u = 0; u < CH; ++u) {
-                const int t = t1 - 1 - u;
-                if (t >= 0) { ej[u] = (s + t == ny - 1) ? 0.0 : -a * pc[o + t]; f[u] = col[o + t]; }
-            }
-#pragma unroll
-            for (int u = 0; u < CH; ++u) {
-                const int t = t1 - 1 - u;
-                if (t >= 0) { uu = yt_axpy(f[u], ej[u], uu); col[o + t] = uu; colsum += yt_re(uu); }
-            }
+#pragma unroll 8
+        for (int t = n - 1; t >= 0; --t) {
+            const double ej = (s + t == ny - 1) ? 0.0 : -a * pc[o + t];
+            uu = yt_axpy(col[o + t], ej, uu);
+            col[o + t] = uu;
+            colsum += yt_re(uu);
         }
         if (!CPLX) wsum = b.dst_w[k] * warp_sum(colsum);
     }
@@ -874,19 +874,6 @@ k_ysolve(const BasinDev *__restrict__ bas, const Work *__restrict__ work,
             b.part_col[w.block] = t;
         }
     }
-    if (!do_scalar) return;
-    // last CTA of this basin runs the scalar phase
-    __threadfence();
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        unsigned int old = atomicAdd(&b.sc->counter, 1u);
-        s_last = (old == (unsigned int)(b.k3_blocks - 1));
-    }
-    __syncthreads();
-    if (!s_last) return;
-    __threadfence();
-    if (threadIdx.x < 32) scalar_phase<T, NL>(b, tdt);
-    if (threadIdx.x == 0) b.sc->counter = 0u;
 }
 
 // LU solve with the pivots of DGETRF (column-major n x n) -- DGETRS 'N'.
@@ -950,17 +937,35 @@ __device__ __forceinline__ void solve_ax_b_dev(const double (&A)[N * N], const d
     }
 }
 
-// The scalar phase of one step, run by one warp of the last y-solve CTA;
-// reductions across the warp, the serial part in lane 0, all in registers.
+// Per-step scalars the assembly needs: the homogeneous-correction
+// coefficients and the suppress_comp_mode flag of this step.
+struct XinvScal {
+    double alpha[OQG_NLMAX];                             // box
+    double c_bt, c_bc1[OQG_NLMAX], c_bc2[OQG_NLMAX];     // channel
+    double S[OQG_NLMAX][OQG_NQ];                         // channel strip sums (scratch)
+    int supp;
+};
+
+// The scalar phase of one step, run by one warp of every assembly CTA from
+// the current state st[par] (all CTAs compute the same values); CTA 0 also
+// writes the next state st[1-par].
+//   update_mass_constr (constraint.F90:167-179);
+//   box_homog's area integrals and 2x2 solve (homog.F90:331-366), from the
+//     dst_w-weighted spectral column sums of the y-solve (the inverse DST is
+//     linear, so the area integral of the modal solution is known before it);
+//   or, for a channel, the strip integrals of the vorticity kernel,
+//     step_constraints (constraint.F90:182-215) and cyclic_homog
+//     (homog.F90:280-329);
+//   the suppress_comp_mode schedule and its scalar part (openqg.F90:485-487,
+//     driver.F90:183-188).
 template <class T, int NL>
-__device__ void scalar_phase(const BasinDev &b, double tdt) {
+__device__ void scalar_phase(const BasinDev &b, double tdt, int par, bool writer, XinvScal *out) {
     const int lane = threadIdx.x & 31;
-    DevScalars *sc = b.sc;
+    const DevState *st = b.st + par;
+    const DevForcing *fr = b.frc;
     double imode[NL];
-    double S[NL][OQG_NQ];
+    double (*S)[OQG_NQ] = out->S;
     if (!b.cyclic) {
-        // area integrals of the modal inhomogeneous solutions, formed from the
-        // column sums of the spectral solution (the inverse DST is linear)
         const int nkb = (b.nk + 3) / 4;       // y-solve CTAs per mode (4 columns each)
 #pragma unroll
         for (int m = 0; m < NL; ++m) {
@@ -971,34 +976,31 @@ __device__ void scalar_phase(const BasinDev &b, double tdt) {
             imode[m] = __shfl_sync(0xffffffffu, s, 0) * b.ftnorm * b.dx * b.dy;
         }
     } else {
+        // strip sums over the tiles touching rows 0, 1, nyp-2, nyp-1
         const int ntile = b.tiles_x * b.tiles_y;
-#pragma unroll
-        for (int k = 0; k < NL; ++k)
-#pragma unroll
-            for (int q = 0; q < OQG_NQ; ++q) {
-                double s = 0.0;
-                for (int t = lane; t < ntile; t += 32) {
-                    const int ty0 = (t / b.tiles_x) * b.vty;
-                    if (ty0 <= 1 || ty0 + b.vty > b.nyp - 2)
-                        s += b.part_tile[((size_t)t * NL + k) * OQG_NQ + q];
-                }
-                s = warp_sum(s);
-                S[k][q] = __shfl_sync(0xffffffffu, s, 0);
+#pragma unroll 1
+        for (int kq = 0; kq < NL * OQG_NQ; ++kq) {
+            double s = 0.0;
+            for (int t = lane; t < ntile; t += 32) {
+                const int ty0 = (t / b.tiles_x) * b.vty;
+                if (ty0 <= 1 || ty0 + b.vty > b.nyp - 2) s += b.part_tile[(size_t)t * NL * OQG_NQ + kq];
             }
+            s = warp_sum(s);
+            if (lane == 0) S[kq / OQG_NQ][kq % OQG_NQ] = s;
+        }
+        __syncwarp();
     }
     if (lane != 0) return;
-    double dpi[NL], dpip[NL];
-#pragma unroll
-    for (int l = 0; l < NL - 1; ++l) { dpi[l] = sc->dpi[l]; dpip[l] = sc->dpip[l]; }
+    DevState ns;                                          // the next state
+    const long long nt = st->nt;
+    const double ent_xn = fr->ent_xn;
     // update_mass_constr (constraint.F90:167-179)
-    const double ent_xn = sc->ent_xn;
 #pragma unroll
     for (int l = 0; l < NL - 1; ++l) {
-        const double ait = dpi[l];
-        dpi[l] = dpip[l] - tdt * b.gp[l] * (l == 0 ? ent_xn : 0.0);
-        dpip[l] = ait;
+        ns.dpi[l] = st->dpip[l] - tdt * b.gp[l] * (l == 0 ? ent_xn : 0.0);
+        ns.dpip[l] = st->dpi[l];
     }
-    const int supp = (b.suppress_period > 0 && (sc->nt % b.suppress_period) == 0) ? 1 : 0;
+    const int supp = (b.suppress_period > 0 && (nt % b.suppress_period) == 0) ? 1 : 0;
     if (!b.cyclic) {
         // box_homog (homog.F90:331-366)
         double ik[NL];
@@ -1015,25 +1017,24 @@ __device__ void scalar_phase(const BasinDev &b, double tdt) {
 #pragma unroll
         for (int x = 0; x < N * N; ++x) { A[x] = b.cdhoc[x]; LU[x] = b.lu[x]; }
 #pragma unroll
-        for (int x = 0; x < N; ++x) { pv[x] = b.piv[x]; rhs[x] = dpi[x] - (ik[x + 1] - ik[x]); }
+        for (int x = 0; x < N; ++x) { pv[x] = b.piv[x]; rhs[x] = ns.dpi[x] - (ik[x + 1] - ik[x]); }
         solve_ax_b_dev<N>(A, LU, pv, rhs, al);
 #pragma unroll
-        for (int l = 0; l < N; ++l) sc->alpha[l] = al[l];
+        for (int l = 0; l < N; ++l) out->alpha[l] = al[l];
     } else {
         double cs[NL], cn[NL], csp[NL], cnp[NL];
 #pragma unroll
-        for (int k = 0; k < NL; ++k) { cs[k] = sc->cs[k]; cn[k] = sc->cn[k]; csp[k] = sc->csp[k]; cnp[k] = sc->cnp[k]; }
-        // strip integrals (vorticity.F90:84-101, numerics.F90:374-386)
+        for (int k = 0; k < NL; ++k) { cs[k] = st->cs[k]; cn[k] = st->cn[k]; csp[k] = st->csp[k]; cnp[k] = st->cnp[k]; }
         const double dx = b.dx, dy = b.dy;
         double rhss[NL], rhsn[NL];
 #pragma unroll
         for (int k = 0; k < NL; ++k) {
-            rhss[k] = -0.5 * dy * b.fnot * sc->int_Be_s[k];
-            rhsn[k] = -0.5 * dy * b.fnot * sc->int_Be_n[k];
+            rhss[k] = -0.5 * dy * b.fnot * fr->int_Be_s[k];
+            rhsn[k] = -0.5 * dy * b.fnot * fr->int_Be_n[k];
         }
         // step_constraints (constraint.F90:182-215)
-        rhss[0] = rhss[0] + b.tau_sign * (b.fnot / b.h[0]) * sc->txis;
-        rhsn[0] = rhsn[0] - b.tau_sign * (b.fnot / b.h[0]) * sc->txin;
+        rhss[0] = rhss[0] + b.tau_sign * (b.fnot / b.h[0]) * fr->txis;
+        rhsn[0] = rhsn[0] - b.tau_sign * (b.fnot / b.h[0]) * fr->txin;
         const double dfac = b.fnot * b.delek / (2.0 * fabs(b.fnot));
         double bs = 0.0, bn = 0.0;
 #pragma unroll
@@ -1080,28 +1081,32 @@ __device__ void scalar_phase(const BasinDev &b, double tdt) {
             clhss[m] = ss + (u0s * dx) / dy;
             clhsn[m] = sn + (u0n * dx) / dy;
         }
-        sc->c_bt = clhss[0] * b.hbsi;
+        out->c_bt = clhss[0] * b.hbsi;
 #pragma unroll
         for (int m = 1; m < NL; ++m) {
-            sc->c_bc1[m] = b.hc2n[m] * clhss[m] - b.hc2s[m] * clhsn[m];
-            sc->c_bc2[m] = b.hc1s[m] * clhsn[m] - b.hc1n[m] * clhss[m];
+            out->c_bc1[m] = b.hc2n[m] * clhss[m] - b.hc2s[m] * clhsn[m];
+            out->c_bc2[m] = b.hc1s[m] * clhsn[m] - b.hc1n[m] * clhss[m];
         }
         // suppress_comp_mode's channel scalars (driver.F90:185-188)
 #pragma unroll
         for (int k = 0; k < NL; ++k) {
             if (supp) { cs[k] = 0.5 * (cs[k] + csp[k]); cn[k] = 0.5 * (cn[k] + cnp[k]); }
-            sc->cs[k] = cs[k]; sc->cn[k] = cn[k]; sc->csp[k] = csp[k]; sc->cnp[k] = cnp[k];
+            ns.cs[k] = cs[k]; ns.cn[k] = cn[k]; ns.csp[k] = csp[k]; ns.cnp[k] = cnp[k];
         }
     }
-    // suppress_comp_mode schedule (openqg.F90:485-487) and its scalar part
-    // (driver.F90:183-184)
+    out->supp = supp;
+    if (!writer) return;
+    DevState *nx = b.st + (1 - par);
 #pragma unroll
     for (int l = 0; l < NL - 1; ++l) {
-        sc->dpi[l] = supp ? 0.5 * (dpi[l] + dpip[l]) : dpi[l];
-        sc->dpip[l] = dpip[l];
+        nx->dpi[l] = supp ? 0.5 * (ns.dpi[l] + ns.dpip[l]) : ns.dpi[l];
+        nx->dpip[l] = ns.dpip[l];
     }
-    sc->suppress_flag = supp;
-    sc->nt += 1;
+    if (b.cyclic) {
+#pragma unroll
+        for (int k = 0; k < NL; ++k) { nx->cs[k] = ns.cs[k]; nx->cn[k] = ns.cn[k]; nx->csp[k] = ns.csp[k]; nx->cnp[k] = ns.cnp[k]; }
+    }
+    nx->nt = nt + 1;
 }
 
 // ------------------------------------------------------------------ k_xinv
@@ -1116,15 +1121,20 @@ __device__ __forceinline__ void xinv_rows(const BasinDev &b, int rb, int &jlo, i
     nra = jlast - jfirst + 1;
 }
 
+// The last warp of the CTA runs the scalar phase of the step while the
+// other nfft = blockDim.x - 32 threads run the inverse transforms; those
+// synchronise among themselves on named barrier 1.
 // out != null: solve-only mode, writes the modal inhomogeneous solutions
-// (FP64, [nl][nyp][px]) and nothing else.
+// (FP64, [nl][nyp][px]) and nothing else (no scalar phase).
 template <class T, int E, int NL>
-__global__ void __launch_bounds__(256, 2)
-k_xinv(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par, double *out) {
+__global__ void __maxnreg__(96)
+k_xinv(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par, double tdt, double *out) {
     typedef typename C2<T>::t T2;
     const Work w = work[blockIdx.x];
     const BasinDev &b = bas[w.member];
-    const int M = b.M, TT = (M + E - 1) / E, G = blockDim.x / TT;
+    const int nfft = blockDim.x - 32;
+    const bool fft_thread = (int)threadIdx.x < nfft;
+    const int M = b.M, TT = (M + E - 1) / E, G = nfft / TT;
     const int g = threadIdx.x / TT, t = threadIdx.x - g * TT;
     int jlo, jhi, jfirst, nra;
     xinv_rows(b, w.block, jlo, jhi, jfirst, nra);
@@ -1132,15 +1142,20 @@ k_xinv(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par,
     const int nxp = b.nxp, n = b.nxin, nyp = b.nyp, px = b.px;
     const int LB = fft_buf_len(M), NTW = fft_tw_len(M);
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ XinvScal sS;
     T2 *sTw = reinterpret_cast<T2 *>(smem_raw);
     T2 *zs = reinterpret_cast<T2 *>(smem_raw + round16(NTW * (int)sizeof(T2)));
     T *inh = reinterpret_cast<T *>(zs + (size_t)G * 2 * LB);   // [NL][nra][nxp]
     const T ftn = (T)b.ftnorm;
 
-    // zero the wall rows / columns of the modal fields
-    for (int idx = threadIdx.x; idx < NL * nra * nxp; idx += blockDim.x) inh[idx] = (T)0;
     pdl_trigger();
-    cp_async_16(sTw, b.tw, round16(NTW * (int)sizeof(T2)), threadIdx.x, blockDim.x);   // constant
+    if (!fft_thread) {
+        pdl_wait();
+        if (!out) scalar_phase<T, NL>(b, tdt, par, blockIdx.x == 0, &sS);
+    } else {
+    // zero the wall rows / columns of the modal fields
+    for (int idx = threadIdx.x; idx < NL * nra * nxp; idx += nfft) inh[idx] = (T)0;
+    cp_async_16(sTw, b.tw, round16(NTW * (int)sizeof(T2)), threadIdx.x, nfft);   // constant
     pdl_wait();
 
     const int npr = (nr + 1) >> 1;               // row pairs per mode
@@ -1165,7 +1180,7 @@ k_xinv(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par,
             if (two) cp_async_16(raw + RO, srow + pitchb, round16(rowbytes), t, TT);
         }
         cp_async_commit_wait_all();
-        __syncthreads();
+        bar_sync(1, nfft);
         if (live) {
             if (!b.cyclic) {
                 const T *x = raw, *y = raw + RO;
@@ -1194,8 +1209,8 @@ k_xinv(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par,
                 }
             }
         }
-        __syncthreads();
-        T2 *z = fft_smem<T>(za, zb, M, b.rad, b.nrad, sTw, live ? t : TT, TT);
+        bar_sync(1, nfft);
+        T2 *z = fft_smem<T>(za, zb, M, b.rad, b.nrad, sTw, live ? t : TT, TT, 1, nfft);
         if (live) {
             const int lr = (jlo + r0) - jfirst;
             T *ox = inh + ((size_t)m * nra + lr) * nxp;
@@ -1219,8 +1234,10 @@ k_xinv(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par,
                 }
             }
         }
-        __syncthreads();
+        bar_sync(1, nfft);
     }
+    }   // fft threads
+    __syncthreads();
 
     if (out) {
         for (int idx = threadIdx.x; idx < NL * nra * nxp; idx += blockDim.x) {
@@ -1232,8 +1249,8 @@ k_xinv(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par,
     }
 
     // homogeneous correction + modes_to_layers, in place (modes -> layers)
-    const DevScalars *sc = b.sc;
-    const int supp = sc->suppress_flag;
+    const XinvScal *sc = &sS;
+    const int supp = sc->supp;
     double ctm[NL * NL], hc[NL > 1 ? NL - 1 : 1];
 #pragma unroll
     for (int x = 0; x < NL * NL; ++x) ctm[x] = b.ctm2l[x];
@@ -1473,7 +1490,7 @@ __global__ void k_init_constraints(const BasinDev *__restrict__ bas, int member,
     }
     __syncthreads();
     if (threadIdx.x != 0) return;
-    DevScalars *sc = b.sc;
+    DevState *sc = b.st + par;
     for (int k = 0; k < NL - 1; ++k) {
         sc->dpip[k] = b.dz_sign * (ipm[k] - ipm[k + 1]);
         sc->dpi[k] = b.dz_sign * (ip[k] - ip[k + 1]);
@@ -1501,7 +1518,7 @@ template <class T>
 __global__ void k_forcing_integrals(const BasinDev *__restrict__ bas, int member) {
     const BasinDev &b = bas[member];
     __shared__ double red[32];
-    DevScalars *sc = b.sc;
+    DevForcing *sc = b.frc;
     const T *E = (const T *)b.ent;
     const size_t n2 = (size_t)b.nyp * b.px;
     double exn = 0.0, s1 = 0.0, s2 = 0.0, n1 = 0.0, n2v = 0.0;
@@ -1553,7 +1570,7 @@ __global__ void k_suppress(const BasinDev *__restrict__ bas, int member, int par
         P[i] = (T)0.5 * (P[i] + PM[i]);
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
-        DevScalars *sc = b.sc;
+        DevState *sc = b.st + par;
         for (int l = 0; l < b.nl - 1; ++l) sc->dpi[l] = 0.5 * (sc->dpi[l] + sc->dpip[l]);
         if (b.cyclic)
             for (int k = 0; k < b.nl; ++k) {
