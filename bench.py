@@ -222,6 +222,20 @@ def run_reference(args):
     return 0
 
 
+def max_over_ranks(ms, pg, device):
+    """Max of a per-rank time over all ranks; every rank calls it."""
+    import torch
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    if pg is not None:
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_value(total_ms, ws, cells, msteps, steps):
+    """Whole-job Mcell-layer-steps/s of ws replicas that each ran the same work."""
+    return ws * cells * msteps * steps / (total_ms / 1e3) / 1e6
+
+
 def time_batches(g, tdt, msteps, steps, flush):
     import torch
     s = torch.cuda.ExternalStream(g.stream())
@@ -281,11 +295,8 @@ def run_ours(args):
     with Clocks(uuid) as clk:
         total_ms = time_batches(g, tdt, msteps, args.steps, flush)
         barrier()
-    tmax = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
-    if pg:
-        pg.all_reduce(tmax, op=pg.ReduceOp.MAX)
-    total_ms = float(tmax.item())
-    value = ws * cells * msteps * args.steps / (total_ms / 1e3) / 1e6
+    total_ms = max_over_ranks(total_ms, pg, "cuda")
+    value = replica_value(total_ms, ws, cells, msteps, args.steps)
 
     # variant: the same basin with FP32 bulk arithmetic
     variants = {}
@@ -297,11 +308,8 @@ def run_ours(args):
         for _ in range(args.warmup):
             gm.step(tdt, msteps)
         barrier()
-        tm = time_batches(gm, tdt, msteps, args.steps, flush)
-        tmm = torch.tensor([tm], dtype=torch.float64, device="cuda")
-        if pg:
-            pg.all_reduce(tmm, op=pg.ReduceOp.MAX)
-        variants["mixed_fp32_bulk"] = ws * cells * msteps * args.steps / (float(tmm.item()) / 1e3) / 1e6
+        tm = max_over_ranks(time_batches(gm, tdt, msteps, args.steps, flush), pg, "cuda")
+        variants["mixed_fp32_bulk"] = replica_value(tm, ws, cells, msteps, args.steps)
         gm.close()
 
     # e2e through the C ABI with pinned host buffers
@@ -330,12 +338,8 @@ def run_ours(args):
     for _ in range(e2e_steps):
         exchange_step()
     g.sync()
-    e2e_s = time.perf_counter() - t0
-    te = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
-    if pg:
-        pg.all_reduce(te, op=pg.ReduceOp.MAX)
-    e2e_s = float(te.item())
-    e2e_value = ws * cells * msteps * e2e_steps / e2e_s / 1e6
+    e2e_ms = max_over_ranks((time.perf_counter() - t0) * 1e3, pg, "cuda")
+    e2e_value = replica_value(e2e_ms, ws, cells, msteps, e2e_steps)
     h2d = msteps * (b.nxp * b.nyp * 8) * b.nl        # wekp + (nl-1) ent layers
     d2h = msteps * b.nxp * b.nyp * 8
 

@@ -7,14 +7,15 @@
 //   k_xfwd   forward x-transform of solve_inhomog_box / _cyclic
 //            (qg/inhomog.F90:170-255): DST-I (box) or r2c FFT (channel).
 //   k_ysolve Thomas solve in y per (mode, wavenumber) (inhomog.F90:187-199),
-//            one warp per column as a warp-parallel affine scan; its last CTA
-//            runs the scalar phase: update_mass_constr (constraint.F90:167-179),
-//            box_homog's 2x2 solve (homog.F90:331-366) or step_constraints +
-//            cyclic_homog (constraint.F90:182-215, homog.F90:280-329), and the
-//            suppress_comp_mode schedule (openqg.F90:485-487).
+//            one warp per column as a warp-parallel affine scan.
 //   k_xinv   inverse x-transform + homogeneous correction + modes_to_layers
 //            (modes.F90:268-284) + ocqbdy (vorsubs.F90:58-114) +
-//            suppress_comp_mode (driver.F90:174-189).
+//            suppress_comp_mode (driver.F90:174-189).  One warp of each CTA
+//            runs the scalar phase meanwhile: update_mass_constr
+//            (constraint.F90:167-179), box_homog's 2x2 solve (homog.F90:331-366)
+//            or step_constraints + cyclic_homog (constraint.F90:182-215,
+//            homog.F90:280-329), and the suppress_comp_mode schedule
+//            (openqg.F90:485-487).
 // Every launch takes a work list, so one launch serves one basin or an
 // ensemble of basins of uneven size.
 #pragma once
@@ -22,6 +23,8 @@
 #include "oqg_dev.cuh"
 #include "oqg_fft.cuh"
 #include "oqg_tma.cuh"
+
+#include <type_traits>
 
 namespace oqg {
 
@@ -221,11 +224,15 @@ template <int N> __device__ __forceinline__ void cp_async_wait() {
 }
 
 // Queues the copy of rows [jlo, jlo+nr) x cols [ilo, ilo+nc) of layer k of f
-// into s (leading dimension nc); outside the basin -> 0; channel columns wrap.
+// into s (leading dimension nc); outside the basin -> 0.  Channel columns of
+// a halo tile wrap with period nxp-1; an `own` tile (the CTA's output columns
+// only) reads columns < nxp as stored, including the duplicate column nxp-1,
+// and zeros beyond, so it never reads a column that another CTA writes.
 // Thread layout: 64 columns x 4 rows.
 template <class T, class G>
 __device__ __forceinline__ void load_tile_async(T *s, const T *__restrict__ f, const G &g, int px,
-                                                int k, int jlo, int nr, int ilo, int nc) {
+                                                int k, int jlo, int nr, int ilo, int nc,
+                                                bool own = false) {
     const int N = g.nxp - 1;
     const int tx = threadIdx.x & 63, ty = threadIdx.x >> 6;
     const T *fk = f + (size_t)k * g.nyp * px;
@@ -236,7 +243,7 @@ __device__ __forceinline__ void load_tile_async(T *s, const T *__restrict__ f, c
         for (int c = tx; c < nc; c += 64) {
             int i = ilo + c;
             bool v = jv;
-            if (g.cyclic) {
+            if (g.cyclic && !own) {
                 while (i < 0) i += N;
                 while (i >= N) i -= N;
             } else {
@@ -382,8 +389,8 @@ k_vort(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par,
             load_tile_async(bf + LY.pm, (const T *)b.F[1 - par], g, px, k, j0 - 3, HPM, i0 - 4, LPQ);
             load_tile_async(bf + LY.p, (const T *)b.F[par], g, px, k, j0 - 1, H1, i0 - 4, LPQ);
             load_tile_async(bf + LY.q, (const T *)b.F[2 + par], g, px, k, j0 - 1, H1, i0 - 4, LPQ);
-            load_tile_async(bf + LY.qm, (const T *)QM, g, px, k, j0, VT, i0, LO);
-            if (k == 0) load_tile_async(sWK, (const T *)b.wekp, g, px, 0, j0, VT, i0, LO);
+            load_tile_async(bf + LY.qm, (const T *)QM, g, px, k, j0, VT, i0, LO, true);
+            if (k == 0) load_tile_async(sWK, (const T *)b.wekp, g, px, 0, j0, VT, i0, LO, true);
             cp_async_commit();
         }
     };
@@ -402,12 +409,19 @@ k_vort(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par,
     const bool strips = g.cyclic && (j0 <= 1 || j0 + VT > nyp - 2);
     // in-domain test of a column (a channel has none outside)
     auto colok = [&](int gi) { return g.cyclic || (gi >= 0 && gi < nxp); };
+    // the del2 region (rows j0-2 .. j0+VT+1, columns i0-2 .. i0+VTX+1) lies
+    // strictly inside the walls, and every output column exists
+    const bool interior = (j0 - 2 >= 1 && j0 + VT + 1 <= nyp - 2) &&
+                          (g.cyclic ? (i0 + VTX <= nxp) : (i0 - 2 >= 1 && i0 + VTX + 1 <= nxp - 2));
 
 #pragma unroll 1
     for (int k = 0; k < NL; ++k) {
         if (k + 1 < NL) issue(k + 1);
         if (tma) {
-            const bool ok = mbar_wait_bounded(&bars[k & 1], (k >> 1) & 1, OQG_WAIT_LIMIT);
+            // one thread polls the barrier; the CTA barrier then publishes
+            // the tile to the others without spinning warps taking issue slots
+            bool ok = true;
+            if (threadIdx.x == 0) ok = mbar_wait_bounded(&bars[k & 1], (k >> 1) & 1, OQG_WAIT_LIMIT);
             if (__syncthreads_or(!ok)) {
                 // a tile never arrived: report, drain what is in flight, stop
                 if (threadIdx.x == 0) {
@@ -427,121 +441,130 @@ k_vort(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par,
         const T *sP = sm + (k & 1) * LY.nbuf + LY.p;
         const T *sQ = sm + (k & 1) * LY.nbuf + LY.q;
         const T *sQM = sm + (k & 1) * LY.nbuf + LY.qm;
-        // ---- del2(pm) on rows j0-2.., cols i0-2.. (column tx of L2 = 64)
-        {
-            const int gi = i0 - 2 + tx, cs = tx + 2;          // column in the pm tile
-            const bool cv = colok(gi);
-            const int rb = ty * R2;
-            const T *col = sPM + rb * LPQ + cs;
-            T sv = col[0], cv_ = col[LPQ];
-#pragma unroll
-            for (int u = 0; u < R2MAX; ++u) {
-                const int r = rb + u;
-                if (u < R2 && r < H2) {
-                    const T nv = col[(u + 2) * LPQ];
-                    const T wv = col[(u + 1) * LPQ - 1], ev = col[(u + 1) * LPQ + 1];
-                    const int gj = j0 - 2 + r;
-                    T v = (T)0;
-                    if (cv && gj >= 0 && gj < nyp) v = lap5(wv, ev, sv, nv, cv_, gi, gj, g);
-                    sD2[r * L2 + tx] = v;
-                    sv = cv_;
-                    cv_ = nv;
-                }
-            }
-        }
-        __syncthreads();
-        // ---- del4 on rows j0-1.., cols i0-1.. (column tx < L1 = 62)
-        if (tx < L1) {
-            const int gi = i0 - 1 + tx, cs = tx + 1;          // column in the d2 tile
-            const bool cv = colok(gi);
-            const int rb = ty * R1;
-            const T *col = sD2 + rb * L2 + cs;
-            T sv = col[0], cv_ = col[L2];
-#pragma unroll
-            for (int u = 0; u < R1MAX; ++u) {
-                const int r = rb + u;
-                if (u < R1 && r < H1) {
-                    const T nv = col[(u + 2) * L2];
-                    const T wv = col[(u + 1) * L2 - 1], ev = col[(u + 1) * L2 + 1];
-                    const int gj = j0 - 1 + r;
-                    T v = (T)0;
-                    if (cv && gj >= 0 && gj < nyp) v = lap5(wv, ev, sv, nv, cv_, gi, gj, g);
-                    sD4[r * L1 + tx] = v;
-                    sv = cv_;
-                    cv_ = nv;
-                }
-            }
-        }
-        __syncthreads();
-
-        // ---- outputs: column tx < VTX, rows r0 .. r0+R0-1 of the tile.
-        // Only points off the solid walls are stepped: on a wall the Arakawa
-        // Jacobian is zero and the stepped q is replaced by ocqbdy
-        // (vorsubs.F90:58-114) in the assembly kernel, so the interior
-        // stencils are the whole computation here.
-        if (tx < VTX) {
-            const int gi = i0 + tx;
-            const bool xin = g.cyclic ? (gi < nxp) : (gi >= 1 && gi <= nxp - 2);
-            const T *d4col = sD4 + r0 * L1 + tx + 1;       // column in the d4 tile
-            const T *pcol = sP + r0 * LPQ + tx + 4;         // column in the p/q tiles
-            const T *qcol = sQ + r0 * LPQ + tx + 4;
+        // The layer's stencils; I: every point of the tile and its halo is
+        // off the walls, so the wall rules and range tests drop out.
+        auto layer = [&](auto inner) {
+            constexpr bool I = decltype(inner)::value;
             const T fx = gfx(g), fy = gfy(g);
-            // rolling windows: d4 (column), p and q (3 x 3)
-            T d4s = d4col[0], d4c = d4col[L1];
-            T pw[3][3], qw[3][3];
-#pragma unroll
-            for (int a = 0; a < 2; ++a)
-#pragma unroll
-                for (int cc = 0; cc < 3; ++cc) {
-                    pw[a + 1][cc] = pcol[a * LPQ - 1 + cc];
-                    qw[a + 1][cc] = qcol[a * LPQ - 1 + cc];
-                }
-#pragma unroll
-            for (int u = 0; u < RMAX; ++u) {
-                const int r = r0 + u;
-                const int gj = j0 + r;
-                if (u < R0 && r < VT) {
-                    // shift the windows down one row and load the new bottom row
-                    const T d4n = d4col[(u + 2) * L1];
-                    const T d4w = d4col[(u + 1) * L1 - 1], d4e = d4col[(u + 1) * L1 + 1];
-#pragma unroll
-                    for (int cc = 0; cc < 3; ++cc) {
-                        pw[0][cc] = pw[1][cc]; pw[1][cc] = pw[2][cc];
-                        qw[0][cc] = qw[1][cc]; qw[1][cc] = qw[2][cc];
-                        pw[2][cc] = pcol[(u + 2) * LPQ - 1 + cc];
-                        qw[2][cc] = qcol[(u + 2) * LPQ - 1 + cc];
+            // ---- del2(pm) on rows j0-2.., cols i0-2.. (column tx of L2 = 64)
+            {
+                const int gi = i0 - 2 + tx, cs = tx + 2;          // column in the pm tile
+                const bool cv = colok(gi);
+                const int rb = ty * R2;
+                const T *col = sPM + rb * LPQ + cs;
+                T sv = col[0], cv_ = col[LPQ];
+    #pragma unroll
+                for (int u = 0; u < R2MAX; ++u) {
+                    const int r = rb + u;
+                    if (u < R2 && r < H2) {
+                        const T nv = col[(u + 2) * LPQ];
+                        const T wv = col[(u + 1) * LPQ - 1], ev = col[(u + 1) * LPQ + 1];
+                        const int gj = j0 - 2 + r;
+                        T v = (T)0;
+                        if (I) v = fx * (wv + ev - (T)2 * cv_) + fy * (sv + nv - (T)2 * cv_);
+                        else if (cv && gj >= 0 && gj < nyp) v = lap5(wv, ev, sv, nv, cv_, gi, gj, g);
+                        sD2[r * L2 + tx] = v;
+                        sv = cv_;
+                        cv_ = nv;
                     }
-                    if (xin && gj >= 1 && gj <= nyp - 2) {
-                        const T d6 = fx * (d4w + d4e - (T)2 * d4c) + fy * (d4s + d4n - (T)2 * d4c);
-                        // Arakawa J(q, p), numerics.F90:370-372
-                        const T pxc = pw[1][2] - pw[1][0], pyc = pw[2][1] - pw[0][1];
-                        const T qxc = qw[1][2] - qw[1][0], qyc = qw[2][1] - qw[0][1];
-                        const T A = qw[1][2] * (pw[2][2] - pw[0][2]) - qw[1][0] * (pw[2][0] - pw[0][0]);
-                        const T Dd = pw[1][2] * (qw[2][2] - qw[0][2]) - pw[1][0] * (qw[2][0] - qw[0][0]);
-                        const T Bv = qw[2][1] * (pw[2][2] - pw[2][0]) - qw[0][1] * (pw[0][2] - pw[0][0]);
-                        const T Cc = pw[2][1] * (qw[2][2] - qw[2][0]) - pw[0][1] * (qw[0][2] - qw[0][0]);
-                        const T jac = gjac(g) * (qxc * pyc - qyc * pxc + A - Bv + Cc - Dd);
-                        T dq = jac + sK[10 + k] * d4c - sK[10 + NL + k] * d6;
-                        const size_t o2 = (size_t)gj * px + gi;
-                        if (k == 0) {
-                            const T e1 = ENT ? ldg(ENT + o2) : (T)0;
-                            dq = dq + sK[5] * e1 + sK[6] * sWK[r * LO + tx];
-                        }
-                        if (k == 1 && ENT) dq = dq - sK[7] * ldg(ENT + o2);
-                        if (k == kt) dq = dq - sK[8] * sD2[(r + 2) * L2 + tx + 2];
-                        const T qn = sQM[r * LO + tx] + sK[9] * dq;
-                        QM[((size_t)k * nyp + gj) * px + gi] = qn;
-                        // modal right-hand side, FP64 (p_modes_rhs)
-                        double ql = (double)qn - sBY[r];
-                        if (k == kt && topo) ql -= DD[o2];
-#pragma unroll
-                        for (int m = 0; m < NL; ++m) acc[u][m] += ql * sCtl[k + NL * m];
-                    }
-                    d4s = d4c;
-                    d4c = d4n;
                 }
             }
-        }
+            __syncthreads();
+            // ---- del4 on rows j0-1.., cols i0-1.. (column tx < L1 = 62)
+            if (tx < L1) {
+                const int gi = i0 - 1 + tx, cs = tx + 1;          // column in the d2 tile
+                const bool cv = colok(gi);
+                const int rb = ty * R1;
+                const T *col = sD2 + rb * L2 + cs;
+                T sv = col[0], cv_ = col[L2];
+    #pragma unroll
+                for (int u = 0; u < R1MAX; ++u) {
+                    const int r = rb + u;
+                    if (u < R1 && r < H1) {
+                        const T nv = col[(u + 2) * L2];
+                        const T wv = col[(u + 1) * L2 - 1], ev = col[(u + 1) * L2 + 1];
+                        const int gj = j0 - 1 + r;
+                        T v = (T)0;
+                        if (I) v = fx * (wv + ev - (T)2 * cv_) + fy * (sv + nv - (T)2 * cv_);
+                        else if (cv && gj >= 0 && gj < nyp) v = lap5(wv, ev, sv, nv, cv_, gi, gj, g);
+                        sD4[r * L1 + tx] = v;
+                        sv = cv_;
+                        cv_ = nv;
+                    }
+                }
+            }
+            __syncthreads();
+
+            // ---- outputs: column tx < VTX, rows r0 .. r0+R0-1 of the tile.
+            // Only points off the solid walls are stepped: on a wall the Arakawa
+            // Jacobian is zero and the stepped q is replaced by ocqbdy
+            // (vorsubs.F90:58-114) in the assembly kernel, so the interior
+            // stencils are the whole computation here.
+            if (tx < VTX) {
+                const int gi = i0 + tx;
+                const bool xin = g.cyclic ? (gi < nxp) : (gi >= 1 && gi <= nxp - 2);
+                const T *d4col = sD4 + r0 * L1 + tx + 1;       // column in the d4 tile
+                const T *pcol = sP + r0 * LPQ + tx + 4;         // column in the p/q tiles
+                const T *qcol = sQ + r0 * LPQ + tx + 4;
+                // rolling windows: d4 (column), p and q (3 x 3)
+                T d4s = d4col[0], d4c = d4col[L1];
+                T pw[3][3], qw[3][3];
+    #pragma unroll
+                for (int a = 0; a < 2; ++a)
+    #pragma unroll
+                    for (int cc = 0; cc < 3; ++cc) {
+                        pw[a + 1][cc] = pcol[a * LPQ - 1 + cc];
+                        qw[a + 1][cc] = qcol[a * LPQ - 1 + cc];
+                    }
+    #pragma unroll
+                for (int u = 0; u < RMAX; ++u) {
+                    const int r = r0 + u;
+                    const int gj = j0 + r;
+                    if (u < R0 && r < VT) {
+                        // shift the windows down one row and load the new bottom row
+                        const T d4n = d4col[(u + 2) * L1];
+                        const T d4w = d4col[(u + 1) * L1 - 1], d4e = d4col[(u + 1) * L1 + 1];
+    #pragma unroll
+                        for (int cc = 0; cc < 3; ++cc) {
+                            pw[0][cc] = pw[1][cc]; pw[1][cc] = pw[2][cc];
+                            qw[0][cc] = qw[1][cc]; qw[1][cc] = qw[2][cc];
+                            pw[2][cc] = pcol[(u + 2) * LPQ - 1 + cc];
+                            qw[2][cc] = qcol[(u + 2) * LPQ - 1 + cc];
+                        }
+                        if (I || (xin && gj >= 1 && gj <= nyp - 2)) {
+                            const T d6 = fx * (d4w + d4e - (T)2 * d4c) + fy * (d4s + d4n - (T)2 * d4c);
+                            // Arakawa J(q, p), numerics.F90:370-372
+                            const T pxc = pw[1][2] - pw[1][0], pyc = pw[2][1] - pw[0][1];
+                            const T qxc = qw[1][2] - qw[1][0], qyc = qw[2][1] - qw[0][1];
+                            const T A = qw[1][2] * (pw[2][2] - pw[0][2]) - qw[1][0] * (pw[2][0] - pw[0][0]);
+                            const T Dd = pw[1][2] * (qw[2][2] - qw[0][2]) - pw[1][0] * (qw[2][0] - qw[0][0]);
+                            const T Bv = qw[2][1] * (pw[2][2] - pw[2][0]) - qw[0][1] * (pw[0][2] - pw[0][0]);
+                            const T Cc = pw[2][1] * (qw[2][2] - qw[2][0]) - pw[0][1] * (qw[0][2] - qw[0][0]);
+                            const T jac = gjac(g) * (qxc * pyc - qyc * pxc + A - Bv + Cc - Dd);
+                            T dq = jac + sK[10 + k] * d4c - sK[10 + NL + k] * d6;
+                            const size_t o2 = (size_t)gj * px + gi;
+                            if (k == 0) {
+                                const T e1 = ENT ? ldg(ENT + o2) : (T)0;
+                                dq = dq + sK[5] * e1 + sK[6] * sWK[r * LO + tx];
+                            }
+                            if (k == 1 && ENT) dq = dq - sK[7] * ldg(ENT + o2);
+                            if (k == kt) dq = dq - sK[8] * sD2[(r + 2) * L2 + tx + 2];
+                            const T qn = sQM[r * LO + tx] + sK[9] * dq;
+                            QM[((size_t)k * nyp + gj) * px + gi] = qn;
+                            // modal right-hand side, FP64 (p_modes_rhs)
+                            double ql = (double)qn - sBY[r];
+                            if (k == kt && topo) ql -= DD[o2];
+    #pragma unroll
+                            for (int m = 0; m < NL; ++m) acc[u][m] += ql * sCtl[k + NL * m];
+                        }
+                        d4s = d4c;
+                        d4c = d4n;
+                    }
+                }
+            }
+        };
+        if (interior) layer(std::true_type{});
+        else layer(std::false_type{});
         if (strips) {
             // channel strip integrands (vorticity.F90:84-101, numerics.F90:374-386)
             // of the rows 0, 1, nyp-2, nyp-1 held by this tile
@@ -727,8 +750,6 @@ template <> __device__ __forceinline__ double2 yt_store2<double2>(double2 v) { r
 template <> __device__ __forceinline__ float2 yt_store2<float2>(double2 v) { return make_float2((float)v.x, (float)v.y); }
 __device__ __forceinline__ double yt_re(double v) { return v; }
 __device__ __forceinline__ double yt_re(double2 v) { return v.x; }
-
-// forward declaration of the scalar phase
 
 template <class T, bool CPLX, int NL>
 __global__ void __launch_bounds__(128)
