@@ -113,10 +113,21 @@ class Clocks:
         os.close(fd)
         q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap,"
+             "clocks.mem,pstate")
         cmd = ["nvidia-smi", "--query-gpu=" + q, "--format=csv,noheader,nounits", "-lms", "200"]
         if self.uuid:
             cmd += ["-i", self.uuid]
+        # compute processes on this GPU besides this one (a shared GPU slows the step)
+        self.others = None
+        try:
+            qa = ["nvidia-smi", "--query-compute-apps=pid", "--format=csv,noheader"]
+            if self.uuid:
+                qa += ["-i", self.uuid]
+            pids = subprocess.run(qa, capture_output=True, text=True, timeout=10).stdout.split()
+            self.others = len([x for x in pids if x.strip().isdigit() and int(x) != os.getpid()])
+        except Exception:
+            pass
         try:
             self.proc = subprocess.Popen(cmd, stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except Exception:
@@ -146,8 +157,11 @@ class Clocks:
         sm = [float(r[1]) for r in rows]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower().startswith("active")})
+        mem = [float(r[9]) for r in rows if len(r) > 9 and r[9].replace(".", "").isdigit()]
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": float(rows[0][2]),
-                "reasons": reasons, "samples": len(rows)}
+                "mem_mhz": statistics.median(mem) if mem else None,
+                "pstates": sorted({r[10] for r in rows if len(r) > 10}),
+                "reasons": reasons, "samples": len(rows), "other_processes": self.others}
 
 
 def cpu_sample(b, p, w, ts, tn, tdt, seconds, threads):
