@@ -43,6 +43,7 @@ extern "C" {
 #define OQG_ESETUP       6  /* init-time check failed (e.g. mode matrix
                                product not the identity, singular LU)   */
 #define OQG_ENODEV       7  /* no CUDA device                            */
+#define OQG_ESCRATCH     8  /* problem larger than a fixed scratch area  */
 
 /* precision modes */
 #define OQG_FP64   0  /* everything FP64, the reference's arithmetic            */
@@ -145,6 +146,32 @@ int oqg_check_finite(oqg_handle *h, long long *bad);
  * total circulation circ (Sv).  Any pointer may be NULL. */
 int oqg_diag(oqg_handle *h, double *ekei, double *sfmin, double *sfmax,
              double *circ);
+
+/* oqg_diag without any allocation: no counterpart in the reference.
+ *
+ * For callers that must not allocate device memory at call time: a host
+ * whose GPU memory is wholly reserved by another allocator (a framework's
+ * caching pool, a fixed partition of the device), or a monitor that runs
+ * between steps of a time-critical loop, where cudaMalloc/cudaFree would
+ * block on or synchronise the device.  Results equal oqg_diag's (the kinetic
+ * energy to rounding: rows are summed first, then layers).
+ *
+ * Its scratch is a 256 KiB array compiled into the library (32768 doubles);
+ * a basin fits when 40 + 4*nl*nyp <= 32768 (nl*nyp <= 8182), otherwise the
+ * call returns OQG_ESCRATCH and does nothing.  It calls no cudaMalloc,
+ * cudaFree or other allocating routine, and reports failures by status code
+ * alone (oqg_last_error is not updated).
+ *
+ * The first call on a device looks up the array's address on that device
+ * (the handle's device must be current; OQG_EINVAL otherwise), which may make
+ * the CUDA runtime load the library's device code: make that first call
+ * before any stream capture.  Every call clears the scratch's completion
+ * counter on the handle's stream before its kernel.  There is one array per
+ * device: calls that overlap in time on the same device (any handles,
+ * streams or host threads) race on it and corrupt each other's results, so
+ * callers must serialise them. */
+int oqg_diag_noalloc(oqg_handle *h, double *ekei, double *sfmin, double *sfmax,
+                     double *circ);
 
 /* solve_inhomog_eqn (inhomog.F90:156-168): (Del^2 - rdm2(m)) out = rhs with
  * out = 0 on solid boundaries; m is the 1-based mode; rhs, out (nxp, nyp). */

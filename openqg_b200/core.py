@@ -60,6 +60,7 @@ def lib():
     L.oqg_sync.argtypes = [vp]
     L.oqg_check_finite.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
     L.oqg_diag.argtypes = [vp, _dp, _dp, _dp, _dp]
+    L.oqg_diag_noalloc.argtypes = [vp, _dp, _dp, _dp, _dp]
     L.oqg_solve_inhomog.argtypes = [vp, ctypes.c_int, _dp, _dp]
     L.oqg_generate_homog_soln.argtypes = [vp, ctypes.c_int, _dp, _dp]
     L.oqg_get_modes.argtypes = [vp, _dp, _dp, _dp, _dp]
@@ -196,6 +197,16 @@ class QG:
         nl = self.b.nl
         e, smin, smax, c = (np.empty(nl) for _ in range(4))
         _check(lib().oqg_diag(self.h, _p(e), _p(smin), _p(smax), _p(c)), "oqg_diag")
+        return dict(ekei=e, sfmin=smin, sfmax=smax, circ=c)
+
+    def diag_noalloc(self):
+        """diag() through oqg_diag_noalloc: scratch in the library's fixed
+        device array, no allocation; it reports failures by status only."""
+        nl = self.b.nl
+        e, smin, smax, c = (np.empty(nl) for _ in range(4))
+        rc = lib().oqg_diag_noalloc(self.h, _p(e), _p(smin), _p(smax), _p(c))
+        if rc != 0:
+            raise OqgError(rc, "oqg_diag_noalloc", "status only")
         return dict(ekei=e, sfmin=smin, sfmax=smax, circ=c)
 
     # pieces of the path -----------------------------------------------------------

@@ -7,6 +7,7 @@
 #include "../../include/oqg.h"
 #include "oqg_dev.cuh"
 #include "oqg_kernels.cuh"
+#include "oqg_noalloc.cuh"
 #include "oqg_setup.h"
 
 #include <cuda.h>
@@ -17,6 +18,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1012,6 +1014,58 @@ int oqg_profile_phases(oqg_handle *h, double tdt, int nsteps, double *ms) {
 int oqg_stream(oqg_handle *h, void **stream) {
     if (!h || !stream) return fail(OQG_EINVAL, "bad argument");
     *stream = (void *)h->st;
+    return OQG_OK;
+}
+
+// Address of g_noalloc_scratch on each device, found once per device by
+// oqg_diag_noalloc.  Finding it (and the first touch of the kernels that use
+// it) lets the CUDA runtime load the library's device code on that device,
+// which is the only step of that entry point that may allocate; later calls
+// only read this table.
+#define OQG_NOALLOC_MAXDEV 64
+static std::mutex g_noalloc_mu;
+static double *g_noalloc_ptr[OQG_NOALLOC_MAXDEV] = {};
+
+int oqg_diag_noalloc(oqg_handle *h, double *ekei, double *sfmin, double *sfmax, double *circ) {
+    if (!h) return OQG_EINVAL;
+    const BasinDev &b = h->hb;
+    if (noalloc_doubles(b.nl, b.nyp) > OQG_NOALLOC_DOUBLES) return OQG_ESCRATCH;
+    int cur = -1;
+    if (cudaGetDevice(&cur) != cudaSuccess) return OQG_ECUDA;
+    if (cur != h->dev) return OQG_EINVAL;          // the handle's device must be current
+    if (cur < 0 || cur >= OQG_NOALLOC_MAXDEV) return OQG_EUNSUPPORTED;
+    double *scr = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(g_noalloc_mu);
+        if (!g_noalloc_ptr[cur]) {
+            void *p = nullptr;
+            if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return OQG_ECUDA;
+            cudaFuncAttributes fa;
+            if (cudaFuncGetAttributes(&fa, k_diag_rows<double>) != cudaSuccess ||
+                cudaFuncGetAttributes(&fa, k_diag_rows<float>) != cudaSuccess)
+                return OQG_ECUDA;
+            g_noalloc_ptr[cur] = (double *)p;
+        }
+        scr = g_noalloc_ptr[cur];
+    }
+    // the completion ticket must read zero when the kernel starts; every
+    // partial and result slot is written before it is read
+    if (cudaMemsetAsync(scr, 0, sizeof(unsigned long long), h->st) != cudaSuccess) return OQG_ECUDA;
+    const dim3 grid((unsigned)b.nyp, (unsigned)b.nl);
+    if (h->mixed) k_diag_rows<float><<<grid, 128, 0, h->st>>>(h->d_bas, 0, h->par, h->prm.rho, scr);
+    else k_diag_rows<double><<<grid, 128, 0, h->st>>>(h->d_bas, 0, h->par, h->prm.rho, scr);
+    if (cudaGetLastError() != cudaSuccess) return OQG_ECUDA;
+    double o[4 * OQG_NLMAX];
+    if (cudaMemcpyAsync(o, scr + OQG_NOALLOC_OUT, 4 * (size_t)b.nl * sizeof(double), cudaMemcpyDeviceToHost,
+                        h->st) != cudaSuccess)
+        return OQG_ECUDA;
+    if (cudaStreamSynchronize(h->st) != cudaSuccess) return OQG_ECUDA;
+    for (int k = 0; k < b.nl; ++k) {
+        if (ekei) ekei[k] = o[4 * k];
+        if (sfmin) sfmin[k] = o[4 * k + 1];
+        if (sfmax) sfmax[k] = o[4 * k + 2];
+        if (circ) circ[k] = o[4 * k + 3];
+    }
     return OQG_OK;
 }
 

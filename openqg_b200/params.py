@@ -34,6 +34,7 @@ OQG_MIXED = 1
 STATUS = {
     0: "OQG_OK", 1: "OQG_EINVAL", 2: "OQG_ECUDA", 3: "OQG_ENAN",
     4: "OQG_ETIMEOUT", 5: "OQG_EUNSUPPORTED", 6: "OQG_ESETUP", 7: "OQG_ENODEV",
+    8: "OQG_ESCRATCH",
 }
 
 _D8 = ctypes.c_double * OQG_MAX_NL
