@@ -1017,6 +1017,12 @@ int oqg_stream(oqg_handle *h, void **stream) {
     return OQG_OK;
 }
 
+// Scratch of oqg_diag_noalloc (layout in oqg_noalloc.cuh).  Every GPU that
+// loads the library holds these 256 KiB until the process exits.  Host code
+// must not pass the name itself to a kernel: on the host it is only a
+// stand-in symbol; the device address comes from cudaGetSymbolAddress.
+static __device__ __align__(256) double g_noalloc_scratch[OQG_NOALLOC_DOUBLES];
+
 // Address of g_noalloc_scratch on each device, found once per device by
 // oqg_diag_noalloc.  Finding it (and the first touch of the kernels that use
 // it) lets the CUDA runtime load the library's device code on that device,

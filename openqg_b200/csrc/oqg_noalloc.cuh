@@ -3,9 +3,10 @@
 //
 // The handle's own diagnostics (k_diag) write into a buffer that oqg_create
 // allocated.  This variant keeps its per-row partial sums, its completion
-// ticket and its results in g_noalloc_scratch instead, a file-scope device
-// array of OQG_NOALLOC_DOUBLES doubles (256 KiB) that the CUDA runtime places
-// when it loads the library's device code, so a call needs no allocation.
+// ticket and its results in g_noalloc_scratch instead (defined in
+// oqg_capi.cu), a file-scope device array of OQG_NOALLOC_DOUBLES doubles
+// (256 KiB) that the CUDA runtime places when it loads the library's device
+// code, so a call needs no allocation.
 //
 // Layout of the array (in doubles):
 //   [0]                      completion ticket (64-bit counter; 0 at launch)
@@ -21,8 +22,6 @@ namespace oqg {
 #define OQG_NOALLOC_DOUBLES 32768                            // 256 KiB
 #define OQG_NOALLOC_OUT 8                                    // first result slot
 #define OQG_NOALLOC_PART (OQG_NOALLOC_OUT + 4 * OQG_NLMAX)   // first partial slot
-
-static __device__ __align__(256) double g_noalloc_scratch[OQG_NOALLOC_DOUBLES];
 
 __host__ __device__ __forceinline__ long long noalloc_doubles(int nl, int nyp) {
     return OQG_NOALLOC_PART + 4LL * nl * nyp;
