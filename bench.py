@@ -64,6 +64,59 @@ def make_basin(name, precision):
     return b, tdt, label
 
 
+ENSEMBLE_SIZES = (65, 97, 129, 193, 257)
+
+
+def make_ensemble(precision, members=256, seed=0):
+    """The batched-ensemble configuration: square 3-layer ocean basins at
+    dx = 20 km with sizes drawn uniformly from ENSEMBLE_SIZES; per member a
+    wind amplitude in [0.05, 0.15] N/m^2, ah4 in [1e10, 4e10] m^4/s and its
+    own seeded initial stream function (std 1e3 m^2/s)."""
+    from openqg_b200.core import ekman_from_tau
+    from openqg_b200.params import double_gyre_tau, initial_psi, ocean_double_gyre
+    rng = np.random.default_rng(seed)
+    sizes = rng.choice(ENSEMBLE_SIZES, size=members)
+    amps = rng.uniform(0.05, 0.15, size=members)
+    ah4s = rng.uniform(1e10, 4e10, size=members)
+    basins, inputs = [], []
+    for i in range(members):
+        b = ocean_double_gyre(int(sizes[i]), dx=20e3, ah4=float(ah4s[i]), precision=precision)
+        p = b.fnot * initial_psi(b, seed=1000 + i)
+        w, ts, tn = ekman_from_tau(b, *double_gyre_tau(b, amp=float(amps[i])))
+        basins.append(b)
+        inputs.append((p, w, ts, tn))
+    return basins, inputs
+
+
+def run_ensemble(precision, steps, warmup, msteps, flush, tdt=3600.0):
+    """Whole-ensemble Mcell-layer-steps/s (all members, one launch per phase)."""
+    import torch
+    from openqg_b200.core import Ensemble
+    basins, inputs = make_ensemble(precision)
+    e = Ensemble(basins)
+    for i, (p, w, ts, tn) in enumerate(inputs):
+        e.set_state(i, p, p)
+        e.set_forcing(i, w, None, ts, tn)
+    for _ in range(warmup):
+        e.step(tdt, msteps)
+    e.sync()
+    s = torch.cuda.ExternalStream(e.stream())
+    total = 0.0
+    for _ in range(steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        e.step(tdt, msteps)
+        e1.record(s)
+        e1.synchronize()
+        total += e0.elapsed_time(e1)
+    e.sync()
+    cells = sum(b.nxp * b.nyp * b.nl for b in basins)
+    e.close()
+    return cells, total
+
+
 def initial_inputs(b, seed, reference=False):
     """Seeded initial pressure and the double-gyre Ekman pumping.  The
     reference arm computes the pumping with the CPU restatement."""
@@ -325,6 +378,14 @@ def run_ours(args):
         tm = max_over_ranks(time_batches(gm, tdt, msteps, args.steps, flush), pg, "cuda")
         variants["mixed_fp32_bulk"] = replica_value(tm, ws, cells, msteps, args.steps)
         gm.close()
+        # the batched ensemble: 256 basins of uneven size, one launch per phase
+        for vprec, vname in ((OQG_MIXED, "ensemble256_mixed"), (OQG_FP64, "ensemble256_fp64")):
+            cells_e, te = run_ensemble(vprec, args.steps, args.warmup, msteps, flush)
+            te = max_over_ranks(te, pg, "cuda")
+            variants[vname] = replica_value(te, ws, cells_e, msteps, args.steps)
+        variants["ensemble_config"] = ("256 ocean 3-layer boxes, sizes uniform in %s, dx 20 km, "
+                                       "per-member wind 0.05-0.15 N/m^2 and ah4 1e10-4e10; %d "
+                                       "cell-layers per step" % (list(ENSEMBLE_SIZES), cells_e))
 
     # e2e through the C ABI with pinned host buffers
     L = lib()

@@ -201,8 +201,8 @@ int oqg_device_state(oqg_handle *h, void **p, void **pm, void **q, void **qm,
 /* Runs nsteps steps as separate launches with CUDA events between the four
  * kernels of each step, on the handle's stream, and returns the mean device
  * time per launch (ms) of each phase: ms[0] vorticity step + modal RHS,
- * ms[1] forward x-transform, ms[2] y-solve + scalar phase, ms[3] inverse
- * x-transform + assembly.  For measurement; the state advances normally. */
+ * ms[1] forward x-transform, ms[2] y-solve, ms[3] inverse x-transform +
+ * scalar phase + assembly.  For measurement; the state advances normally. */
 int oqg_profile_phases(oqg_handle *h, double tdt, int nsteps, double *ms);
 
 /* CUDA stream of the handle (a cudaStream_t). */
@@ -211,7 +211,10 @@ int oqg_stream(oqg_handle *h, void **stream);
 /* ---------------------------------------------------------------------
  * Ensembles: many independent basins of uneven size stepped together by one
  * launch per phase (captured in a CUDA graph).  Members keep the semantics of
- * a single handle.
+ * a single handle and give bit-identical results; they must share nl and
+ * precision, and be all closed boxes or all channels (OQG_EINVAL /
+ * OQG_EUNSUPPORTED otherwise).  Per-member calls (set_state, set_forcing,
+ * get_state) wait for the ensemble's stream first.  member is 0-based.
  * ------------------------------------------------------------------- */
 typedef struct oqg_ensemble oqg_ensemble;
 
@@ -227,6 +230,8 @@ int oqg_ensemble_set_forcing(oqg_ensemble *e, int member, const double *wekp,
 /* tdt[member] per member; nsteps for all. */
 int oqg_ensemble_step(oqg_ensemble *e, const double *tdt, int nsteps);
 int oqg_ensemble_sync(oqg_ensemble *e);
+/* The CUDA stream (cudaStream_t) the ensemble's steps run on. */
+int oqg_ensemble_stream(oqg_ensemble *e, void **stream);
 
 #ifdef __cplusplus
 }

@@ -68,6 +68,14 @@ def lib():
     L.oqg_device_state.argtypes = [vp] + [ctypes.POINTER(vp)] * 4 + [ctypes.POINTER(ctypes.c_int)] * 2
     L.oqg_stream.argtypes = [vp, ctypes.POINTER(vp)]
     L.oqg_profile_phases.argtypes = [vp, ctypes.c_double, ctypes.c_int, _dp]
+    L.oqg_ensemble_create.argtypes = [vp, ctypes.c_int, ctypes.POINTER(vp)]
+    L.oqg_ensemble_destroy.argtypes = [vp]
+    L.oqg_ensemble_set_state.argtypes = [vp, ctypes.c_int, _dp, _dp]
+    L.oqg_ensemble_get_state.argtypes = [vp, ctypes.c_int, _dp, _dp, _dp, _dp]
+    L.oqg_ensemble_set_forcing.argtypes = [vp, ctypes.c_int, _dp, _dp, ctypes.c_double, ctypes.c_double]
+    L.oqg_ensemble_step.argtypes = [vp, _dp, ctypes.c_int]
+    L.oqg_ensemble_sync.argtypes = [vp]
+    L.oqg_ensemble_stream.argtypes = [vp, ctypes.POINTER(vp)]
     _lib = L
     return L
 
@@ -278,3 +286,65 @@ def ekman_from_tau(basin: Basin, taux, tauy):
                                     ctypes.cast(ctypes.byref(ts), _dp),
                                     ctypes.cast(ctypes.byref(tn), _dp)), "oqg_ekman_from_tau")
     return w, ts.value, tn.value
+
+
+class Ensemble:
+    """Many basins of uneven size stepped together: one launch per phase of
+    the step for all members (oqg_ensemble_*).  Members share nl, precision
+    and kind (all boxes or all channels)."""
+
+    def __init__(self, members):
+        self.members = list(members)
+        self._prm = [b.to_c() for b in self.members]
+        arr = (type(self._prm[0]) * len(self._prm))(*self._prm)
+        self._arr = arr
+        e = ctypes.c_void_p()
+        _check(lib().oqg_ensemble_create(ctypes.cast(arr, ctypes.c_void_p), len(self._prm), ctypes.byref(e)),
+               "oqg_ensemble_create")
+        self.e = e
+
+    def close(self):
+        if getattr(self, "e", None):
+            lib().oqg_ensemble_destroy(self.e)
+            self.e = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __len__(self):
+        return len(self.members)
+
+    def set_state(self, i: int, p, pm):
+        b = self.members[i]
+        p, pm = _f64(p, b.shape3), _f64(pm, b.shape3)
+        _check(lib().oqg_ensemble_set_state(self.e, i, _p(p), _p(pm)), "oqg_ensemble_set_state")
+
+    def set_forcing(self, i: int, wekp=None, ent=None, txis=0.0, txin=0.0):
+        b = self.members[i]
+        wekp = _f64(wekp, b.shape2)
+        ent = _f64(ent, (b.nl - 1,) + b.shape2) if ent is not None else None
+        _check(lib().oqg_ensemble_set_forcing(self.e, i, _p(wekp), _p(ent), float(txis), float(txin)),
+               "oqg_ensemble_set_forcing")
+
+    def get_state(self, i: int):
+        sh = self.members[i].shape3
+        p, pm, q, qm = (np.empty(sh) for _ in range(4))
+        _check(lib().oqg_ensemble_get_state(self.e, i, _p(p), _p(pm), _p(q), _p(qm)), "oqg_ensemble_get_state")
+        return p, pm, q, qm
+
+    def step(self, tdt, nsteps: int = 1):
+        """tdt: one value for all members or one per member."""
+        t = np.broadcast_to(np.asarray(tdt, dtype=np.float64), (len(self.members),)).copy()
+        self._tdt = t
+        _check(lib().oqg_ensemble_step(self.e, _p(t), int(nsteps)), "oqg_ensemble_step")
+
+    def sync(self):
+        _check(lib().oqg_ensemble_sync(self.e), "oqg_ensemble_sync")
+
+    def stream(self) -> int:
+        s = ctypes.c_void_p()
+        _check(lib().oqg_ensemble_stream(self.e, ctypes.byref(s)), "oqg_ensemble_stream")
+        return s.value or 0

@@ -117,17 +117,43 @@ static void launch_solve_t(oqg_handle *h, double *out) {
     k_xinv<double, E, NL><<<h->ni, XINV_THREADS, h->smem_i64, h->st>>>(h->d_bas64, h->d_wi, 0, 0.0, out);
 }
 
+// The dynamic shared-memory limit of a kernel is a property of the function
+// on a device, shared by every handle: it only ever rises, to the largest
+// size any handle or ensemble on that device launches with.
+static std::mutex g_smem_mu;
+static std::vector<std::pair<std::pair<int, const void *>, int>> g_smem_set;
+
+static void raise_smem(const void *fn, size_t bytes) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lk(g_smem_mu);
+    for (auto &e : g_smem_set)
+        if (e.first.first == dev && e.first.second == fn) {
+            if ((int)bytes > e.second && cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                              (int)bytes) == cudaSuccess)
+                e.second = (int)bytes;
+            return;
+        }
+    if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) == cudaSuccess)
+        g_smem_set.push_back({{dev, fn}, (int)bytes});
+}
+
+template <class T, int NL, int E>
+static void raise_step_smem(size_t v, size_t x, size_t y, size_t i) {
+    raise_smem((const void *)k_vort<T, NL>, v);
+    raise_smem((const void *)k_xfwd<T, E>, x);
+    raise_smem((const void *)k_ysolve<T, true, NL>, y);
+    raise_smem((const void *)k_ysolve<T, false, NL>, y);
+    raise_smem((const void *)k_xinv<T, E, NL>, i);
+}
+
 template <class T, int NL, int E>
 static void set_attrs_t(oqg_handle *h) {
-    cudaFuncSetAttribute(k_vort<T, NL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->smem_v);
-    cudaFuncSetAttribute(k_xfwd<T, E>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->smem_x);
-    cudaFuncSetAttribute(k_ysolve<T, true, NL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->smem_y);
-    cudaFuncSetAttribute(k_ysolve<T, false, NL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->smem_y);
-    cudaFuncSetAttribute(k_xinv<T, E, NL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->smem_i);
-    cudaFuncSetAttribute(k_xfwd<double, E>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->smem_x64);
-    cudaFuncSetAttribute(k_ysolve<double, true, NL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->smem_y);
-    cudaFuncSetAttribute(k_ysolve<double, false, NL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->smem_y);
-    cudaFuncSetAttribute(k_xinv<double, E, NL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->smem_i64);
+    raise_step_smem<T, NL, E>(h->smem_v, h->smem_x, h->smem_y, h->smem_i);
+    raise_smem((const void *)k_xfwd<double, E>, h->smem_x64);
+    raise_smem((const void *)k_ysolve<double, true, NL>, h->smem_y);
+    raise_smem((const void *)k_ysolve<double, false, NL>, h->smem_y);
+    raise_smem((const void *)k_xinv<double, E, NL>, h->smem_i64);
 }
 
 // dispatch over (T, NL, E)
@@ -398,6 +424,72 @@ static void launch_phase_t(oqg_handle *h, int phase, int par, double tdt) {
 }
 static void launch_phase(oqg_handle *h, int phase, int par, double tdt) {
     OQG_DISPATCH(launch_phase_t, h, h, phase, par, tdt);
+}
+
+// ----------------------------------------------------------- ensembles
+// An ensemble steps many basins of uneven size with one launch per phase:
+// every member is a full handle (its fields, tables and homogeneous
+// solutions, made by oqg_create), and the ensemble holds an array of their
+// descriptors and one work list per kernel that concatenates the members'
+// blocks, the largest members first so that small ones fill the tail.
+struct oqg_ensemble {
+    int dev = 0;
+    cudaStream_t st = nullptr;
+    std::vector<oqg_handle *> m;
+    std::vector<BasinDev> hb;          // descriptors as uploaded (tdt_m per member)
+    bool mixed = false;
+    int nl = 3, E = 8, cyclic = 0;
+    BasinDev *d_bas = nullptr;
+    Work *d_wv = nullptr, *d_wx = nullptr, *d_wy = nullptr, *d_wi = nullptr;
+    int nv = 0, nx = 0, nys = 0, ni = 0;
+    size_t smem_v = 0, smem_x = 0, smem_y = 0, smem_i = 0;
+    int par = 0;
+    cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+    std::vector<void *> allocs;
+};
+
+#define OQG_DISPATCH_E(FN, e, ...)                                                    \
+    do {                                                                              \
+        const int nl_ = (e)->nl, e_ = (e)->E;                                         \
+        if ((e)->mixed) {                                                             \
+            if (nl_ == 2) { if (e_ == 8) FN<float, 2, 8>(__VA_ARGS__); else FN<float, 2, 16>(__VA_ARGS__); } \
+            else if (nl_ == 3) { if (e_ == 8) FN<float, 3, 8>(__VA_ARGS__); else FN<float, 3, 16>(__VA_ARGS__); } \
+            else { if (e_ == 8) FN<float, 4, 8>(__VA_ARGS__); else FN<float, 4, 16>(__VA_ARGS__); } \
+        } else {                                                                      \
+            if (nl_ == 2) { if (e_ == 8) FN<double, 2, 8>(__VA_ARGS__); else FN<double, 2, 16>(__VA_ARGS__); } \
+            else if (nl_ == 3) { if (e_ == 8) FN<double, 3, 8>(__VA_ARGS__); else FN<double, 3, 16>(__VA_ARGS__); } \
+            else { if (e_ == 8) FN<double, 4, 8>(__VA_ARGS__); else FN<double, 4, 16>(__VA_ARGS__); } \
+        }                                                                             \
+    } while (0)
+
+// One step of every member: the kernels read each member's step from its
+// descriptor (tdt = 0).
+template <class T, int NL, int E>
+static void launch_ens_step_t(oqg_ensemble *e, int par) {
+    launch_pdl(k_vort<T, NL>, e->nv, VTHREADS, e->smem_v, e->st, e->d_bas, e->d_wv, par, 0.0);
+    launch_pdl(k_xfwd<T, E>, e->nx, XTHREADS, e->smem_x, e->st, e->d_bas, e->d_wx, (const void *)nullptr);
+    if (e->cyclic)
+        launch_pdl(k_ysolve<T, true, NL>, e->nys, 128, e->smem_y, e->st, e->d_bas, e->d_wy);
+    else
+        launch_pdl(k_ysolve<T, false, NL>, e->nys, 128, e->smem_y, e->st, e->d_bas, e->d_wy);
+    launch_pdl(k_xinv<T, E, NL>, e->ni, XINV_THREADS, e->smem_i, e->st, e->d_bas, e->d_wi, par, 0.0,
+               (double *)nullptr);
+}
+template <class T, int NL, int E>
+static void raise_ens_smem_t(oqg_ensemble *e) {
+    raise_step_smem<T, NL, E>(e->smem_v, e->smem_x, e->smem_y, e->smem_i);
+}
+static void launch_ens_step(oqg_ensemble *e, int par) { OQG_DISPATCH_E(launch_ens_step_t, e, e, par); }
+
+static void ens_free(oqg_ensemble *e) {
+    if (!e) return;
+    if (e->st) cudaStreamSynchronize(e->st);
+    for (int i = 0; i < 2; ++i)
+        if (e->gexec[i]) cudaGraphExecDestroy(e->gexec[i]);
+    for (void *p : e->allocs) cudaFree(p);
+    for (oqg_handle *h : e->m) destroy_all(h);
+    if (e->st) cudaStreamDestroy(e->st);
+    delete e;
 }
 
 extern "C" {
@@ -1075,24 +1167,199 @@ int oqg_diag_noalloc(oqg_handle *h, double *ekei, double *sfmin, double *sfmax, 
     return OQG_OK;
 }
 
-// Ensembles: added with the batched launch path.
-int oqg_ensemble_create(const oqg_params *, int, oqg_ensemble **out) {
-    if (out) *out = nullptr;
-    return fail(OQG_EUNSUPPORTED, "ensembles are not built yet");
+// ---- ensembles (oqg_ensemble_*)
+int oqg_ensemble_create(const oqg_params *members, int nmembers, oqg_ensemble **out) {
+    if (!members || nmembers < 1 || !out) return fail(OQG_EINVAL, "bad argument");
+    *out = nullptr;
+    for (int i = 1; i < nmembers; ++i) {
+        if (members[i].nl != members[0].nl || members[i].precision != members[0].precision)
+            return fail(OQG_EINVAL, "ensemble members must share nl and precision");
+        if ((members[i].cyclic != 0) != (members[0].cyclic != 0))
+            return fail(OQG_EUNSUPPORTED, "ensemble members must be all boxes or all channels");
+    }
+    oqg_ensemble *e = new oqg_ensemble();
+    cudaGetDevice(&e->dev);
+    if (cudaStreamCreateWithFlags(&e->st, cudaStreamNonBlocking) != cudaSuccess) {
+        delete e;
+        return fail(OQG_ECUDA, "cudaStreamCreate failed");
+    }
+    for (int i = 0; i < nmembers; ++i) {
+        oqg_handle *h = nullptr;
+        const int rc = oqg_create(&members[i], &h);
+        if (rc) {
+            std::string msg = "member " + std::to_string(i) + ": " + g_err;
+            ens_free(e);
+            return fail(rc, msg);
+        }
+        e->m.push_back(h);
+    }
+    e->mixed = e->m[0]->mixed;
+    e->nl = e->m[0]->hb.nl;
+    e->cyclic = e->m[0]->hb.cyclic;
+    e->E = 8;
+    for (oqg_handle *h : e->m)
+        if (h->hb.M > 2048) e->E = 16;
+    const size_t esz = e->m[0]->esz, t2 = 2 * esz, vsz = e->cyclic ? 16 : 8;
+    // launch sizes per member, with the ensemble's E and fixed block sizes
+    std::vector<int> order(nmembers);
+    for (int i = 0; i < nmembers; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int c) {
+        return (long)e->m[a]->hb.nxp * e->m[a]->hb.nyp > (long)e->m[c]->hb.nxp * e->m[c]->hb.nyp;
+    });
+    std::vector<Work> wv, wx, wy, wi;
+    for (int i : order) {
+        const BasinDev &b = e->m[i]->hb;
+        const int TT = (b.M + e->E - 1) / e->E;
+        const int G = std::max(1, XTHREADS / TT);
+        const int NTW = fft_tw_len(b.M), LB = fft_buf_len(b.M);
+        const int npm = (b.ny + 1) / 2;
+        const int nvb = b.tiles_x * b.tiles_y;
+        const int nxb = (b.nl * npm + G - 1) / G;
+        const int nyb = b.nl * ((b.nk + 3) / 4);
+        const int nib = (b.ny + b.k4_rows - 1) / b.k4_rows;
+        for (int k = 0; k < nvb; ++k) wv.push_back(Work{i, k});
+        for (int k = 0; k < nxb; ++k) wx.push_back(Work{i, k});
+        for (int k = 0; k < nyb; ++k) wy.push_back(Work{i, k});
+        for (int k = 0; k < nib; ++k) wi.push_back(Work{i, k});
+        const int nra = (b.ny > b.k4_rows) ? b.k4_rows + 1 : b.ny + 2;
+        e->smem_v = std::max(e->smem_v, vort_smem_bytes(b.vty, (int)esz));
+        e->smem_x = std::max(e->smem_x, (size_t)round16(NTW * (int)t2) + (size_t)G * 2 * LB * t2);
+        e->smem_y = std::max(e->smem_y, (size_t)((b.ny + 32) | 1) * 4 * (vsz + 8));
+        e->smem_i = std::max(e->smem_i, (size_t)round16(NTW * (int)t2) + (size_t)G * 2 * LB * t2 +
+                                            (size_t)b.nl * nra * b.nxp * esz);
+    }
+    if (e->smem_x > 227 * 1024 || e->smem_i > 227 * 1024 || e->smem_v > 227 * 1024) {
+        ens_free(e);
+        return fail(OQG_EUNSUPPORTED, "ensemble member too large for the shared-memory tiling");
+    }
+    e->nv = (int)wv.size(); e->nx = (int)wx.size(); e->nys = (int)wy.size(); e->ni = (int)wi.size();
+    auto up = [&](const void *src, size_t bytes) -> void * {
+        void *d = nullptr;
+        if (cudaMalloc(&d, bytes) != cudaSuccess) return nullptr;
+        e->allocs.push_back(d);
+        if (cudaMemcpy(d, src, bytes, cudaMemcpyHostToDevice) != cudaSuccess) return nullptr;
+        return d;
+    };
+    e->hb.resize(nmembers);
+    for (int i = 0; i < nmembers; ++i) e->hb[i] = e->m[i]->hb;
+    e->d_bas = (BasinDev *)up(e->hb.data(), e->hb.size() * sizeof(BasinDev));
+    e->d_wv = (Work *)up(wv.data(), wv.size() * sizeof(Work));
+    e->d_wx = (Work *)up(wx.data(), wx.size() * sizeof(Work));
+    e->d_wy = (Work *)up(wy.data(), wy.size() * sizeof(Work));
+    e->d_wi = (Work *)up(wi.data(), wi.size() * sizeof(Work));
+    if (!e->d_bas || !e->d_wv || !e->d_wx || !e->d_wy || !e->d_wi) {
+        ens_free(e);
+        return fail(OQG_ECUDA, "out of device memory");
+    }
+    OQG_DISPATCH_E(raise_ens_smem_t, e, e);
+    *out = e;
+    return OQG_OK;
 }
-int oqg_ensemble_destroy(oqg_ensemble *) { return OQG_OK; }
-int oqg_ensemble_set_state(oqg_ensemble *, int, const double *, const double *) {
-    return fail(OQG_EUNSUPPORTED, "ensembles are not built yet");
+
+int oqg_ensemble_destroy(oqg_ensemble *e) {
+    ens_free(e);
+    return OQG_OK;
 }
-int oqg_ensemble_get_state(oqg_ensemble *, int, double *, double *, double *, double *) {
-    return fail(OQG_EUNSUPPORTED, "ensembles are not built yet");
+
+// Member calls run on the member's own stream: the ensemble's stream is
+// drained first, and the member sees the ensemble's step parity.
+static int ens_member(oqg_ensemble *e, int member, oqg_handle **h) {
+    if (!e || member < 0 || member >= (int)e->m.size()) return fail(OQG_EINVAL, "bad member");
+    CK(cudaStreamSynchronize(e->st));
+    *h = e->m[member];
+    (*h)->par = e->par;
+    return OQG_OK;
 }
-int oqg_ensemble_set_forcing(oqg_ensemble *, int, const double *, const double *, double, double) {
-    return fail(OQG_EUNSUPPORTED, "ensembles are not built yet");
+
+// The member's descriptor may have changed (forcing buffers): upload it again.
+static int ens_refresh(oqg_ensemble *e, int member) {
+    const double tdt = e->hb[member].tdt_m;
+    e->hb[member] = e->m[member]->hb;
+    e->hb[member].tdt_m = tdt;
+    CK(cudaMemcpyAsync(e->d_bas + member, &e->hb[member], sizeof(BasinDev), cudaMemcpyHostToDevice, e->st));
+    CK(cudaStreamSynchronize(e->st));
+    return OQG_OK;
 }
-int oqg_ensemble_step(oqg_ensemble *, const double *, int) {
-    return fail(OQG_EUNSUPPORTED, "ensembles are not built yet");
+
+int oqg_ensemble_set_state(oqg_ensemble *e, int member, const double *p, const double *pm) {
+    oqg_handle *h = nullptr;
+    int rc = ens_member(e, member, &h);
+    if (rc) return rc;
+    return oqg_set_state(h, p, pm);
 }
-int oqg_ensemble_sync(oqg_ensemble *) { return fail(OQG_EUNSUPPORTED, "ensembles are not built yet"); }
+
+int oqg_ensemble_get_state(oqg_ensemble *e, int member, double *p, double *pm, double *q, double *qm) {
+    oqg_handle *h = nullptr;
+    int rc = ens_member(e, member, &h);
+    if (rc) return rc;
+    return oqg_get_state(h, p, pm, q, qm);
+}
+
+int oqg_ensemble_set_forcing(oqg_ensemble *e, int member, const double *wekp, const double *ent, double txis,
+                             double txin) {
+    oqg_handle *h = nullptr;
+    int rc = ens_member(e, member, &h);
+    if (rc) return rc;
+    if ((rc = oqg_set_forcing(h, wekp, ent, txis, txin))) return rc;
+    return ens_refresh(e, member);
+}
+
+int oqg_ensemble_step(oqg_ensemble *e, const double *tdt, int nsteps) {
+    if (!e || !tdt || nsteps < 0) return fail(OQG_EINVAL, "bad argument");
+    const int n = (int)e->m.size();
+    bool changed = false;
+    for (int i = 0; i < n; ++i) {
+        if (!(tdt[i] > 0.0)) return fail(OQG_EINVAL, "tdt must be > 0 for every member");
+        if (e->hb[i].tdt_m != tdt[i]) { e->hb[i].tdt_m = tdt[i]; changed = true; }
+    }
+    if (changed) {
+        CK(cudaMemcpyAsync(e->d_bas, e->hb.data(), n * sizeof(BasinDev), cudaMemcpyHostToDevice, e->st));
+        CK(cudaStreamSynchronize(e->st));
+    }
+    int done = 0;
+    if (nsteps >= 2) {
+        const int par = e->par;
+        if (!e->gexec[par]) {
+            cudaGraph_t g = nullptr;
+            CK(cudaStreamBeginCapture(e->st, cudaStreamCaptureModeThreadLocal));
+            launch_ens_step(e, par);
+            launch_ens_step(e, 1 - par);
+            cudaError_t e1 = cudaGetLastError();
+            cudaError_t e2 = cudaStreamEndCapture(e->st, &g);
+            if (e1 != cudaSuccess || e2 != cudaSuccess) {
+                if (g) cudaGraphDestroy(g);
+                return fail(OQG_ECUDA, std::string("graph capture: ") +
+                                           cudaGetErrorString(e1 != cudaSuccess ? e1 : e2));
+            }
+            cudaError_t e3 = cudaGraphInstantiate(&e->gexec[par], g, 0);
+            cudaGraphDestroy(g);
+            if (e3 != cudaSuccess) return fail(OQG_ECUDA, std::string("graph instantiate: ") + cudaGetErrorString(e3));
+        }
+        for (; done + 2 <= nsteps; done += 2) CK(cudaGraphLaunch(e->gexec[par], e->st));
+    }
+    for (; done < nsteps; ++done) {
+        launch_ens_step(e, e->par);
+        e->par ^= 1;
+    }
+    CK(cudaGetLastError());
+    return OQG_OK;
+}
+
+int oqg_ensemble_stream(oqg_ensemble *e, void **stream) {
+    if (!e || !stream) return fail(OQG_EINVAL, "bad argument");
+    *stream = (void *)e->st;
+    return OQG_OK;
+}
+
+int oqg_ensemble_sync(oqg_ensemble *e) {
+    if (!e) return fail(OQG_EINVAL, "null ensemble");
+    CK(cudaStreamSynchronize(e->st));
+    for (size_t i = 0; i < e->m.size(); ++i) {
+        int err = 0;
+        CK(cudaMemcpy(&err, e->m[i]->hb.err, sizeof(int), cudaMemcpyDeviceToHost));
+        if (err) return fail(OQG_ECUDA, "device error flag set in member " + std::to_string(i));
+    }
+    return OQG_OK;
+}
 
 }  // extern "C"

@@ -98,6 +98,8 @@ struct BasinDev {
     int *err;                   // device error bits
     // launch bookkeeping
     int k4_rows;                // interior rows per CTA of the assembly launch
+    double tdt_m;               // leapfrog step of this member when a launch
+                                // passes tdt = 0 (ensembles: one per member)
 };
 
 // One entry of a launch's work list: which basin and which block of it.

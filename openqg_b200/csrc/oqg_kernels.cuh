@@ -308,6 +308,7 @@ __host__ __device__ __forceinline__ size_t vort_smem_bytes(int vt, int esz) {
 #define OQG_NTMAP 9
 #define OQG_TMAP_BYTES 128
 
+// tdt = 0: each member steps with its own b.tdt_m (ensemble launches).
 template <class T, int NL>
 __global__ void __launch_bounds__(VTHREADS, 2)
 k_vort(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par, double tdt) {
@@ -326,7 +327,7 @@ k_vort(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par,
         if (i == 0) v = (T)b.fx; else if (i == 1) v = (T)b.fy; else if (i == 2) v = (T)b.fx_bc;
         else if (i == 3) v = (T)b.fy_bc; else if (i == 4) v = (T)b.jac_fac; else if (i == 5) v = (T)b.c_ent1;
         else if (i == 6) v = (T)b.c_wind; else if (i == 7) v = (T)b.c_ent2; else if (i == 8) v = (T)b.c_drag;
-        else if (i == 9) v = (T)tdt; else if (i < 10 + NL) v = (T)b.c2[i - 10]; else v = (T)b.c4[i - 10 - NL];
+        else if (i == 9) v = (T)(tdt != 0.0 ? tdt : b.tdt_m); else if (i < 10 + NL) v = (T)b.c2[i - 10]; else v = (T)b.c4[i - 10 - NL];
         sK[i] = v;
     }
     if (threadIdx.x < NL * NL) sCtl[threadIdx.x] = b.ctl2m[threadIdx.x];
@@ -1147,6 +1148,7 @@ __device__ __forceinline__ void xinv_rows(const BasinDev &b, int rb, int &jlo, i
 // synchronise among themselves on named barrier 1.
 // out != null: solve-only mode, writes the modal inhomogeneous solutions
 // (FP64, [nl][nyp][px]) and nothing else (no scalar phase).
+// tdt = 0: each member steps with its own b.tdt_m (ensemble launches).
 template <class T, int E, int NL>
 __global__ void __maxnreg__(96)
 k_xinv(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par, double tdt, double *out) {
@@ -1172,7 +1174,7 @@ k_xinv(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par,
     pdl_trigger();
     if (!fft_thread) {
         pdl_wait();
-        if (!out) scalar_phase<T, NL>(b, tdt, par, blockIdx.x == 0, &sS);
+        if (!out) scalar_phase<T, NL>(b, tdt != 0.0 ? tdt : b.tdt_m, par, w.block == 0, &sS);
     } else {
     // zero the wall rows / columns of the modal fields
     for (int idx = threadIdx.x; idx < NL * nra * nxp; idx += nfft) inh[idx] = (T)0;

@@ -74,3 +74,21 @@ def test_ekman_from_tau_matches_oracle(liboqg):
         wo, so, no = oracle.ekman_from_tau(b, taux, tauy)
         assert np.array_equal(wg, wo)
         assert sg == so and ng == no
+
+
+def test_ensemble_create_checks_members_before_any_device_call(liboqg):
+    import ctypes
+    from openqg_b200.params import atmos_channel, ocean_double_gyre
+    a, c = ocean_double_gyre(33), atmos_channel(49, 25)
+    c.h = [2000.0, 3000.0]
+    c.gp = [1.2]
+    two = [a.to_c(), c.to_c()]
+    arr = (type(two[0]) * 2)(*two)
+    e = ctypes.c_void_p()
+    # members of different nl: OQG_EINVAL
+    assert liboqg.oqg_ensemble_create(ctypes.cast(arr, ctypes.c_void_p), 2, ctypes.byref(e)) == 1
+    # a box with a channel: OQG_EUNSUPPORTED
+    b3 = atmos_channel(49, 25).to_c()
+    arr2 = (type(b3) * 2)(a.to_c(), b3)
+    assert liboqg.oqg_ensemble_create(ctypes.cast(arr2, ctypes.c_void_p), 2, ctypes.byref(e)) == 5
+    assert not e.value

@@ -1,0 +1,108 @@
+"""Batched ensembles (oqg_ensemble_*): members of uneven size stepped by one
+launch per phase must give exactly what each member gives as a single
+handle, and so inherit the single handle's parity with the oracle."""
+import numpy as np
+import pytest
+
+import oracle
+from openqg_b200.core import QG, Ensemble
+from openqg_b200.params import OQG_MIXED, atmos_channel, double_gyre_tau, initial_psi, ocean_double_gyre
+from tests.qg_numpy import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(autouse=True)
+def _need_gpu(gpu_required):
+    pass
+
+
+def _channel_tau(b, amp=0.1):
+    yl = (b.nyp - 1) * b.dy
+    y = np.arange(b.nyp) * b.dy
+    taux = np.repeat((amp * np.sin(np.pi * y / yl))[:, None], b.nxp, axis=1)
+    return taux, np.zeros_like(taux)
+
+
+def _inputs(b, seed):
+    amp = 30.0 if b.cyclic else 1.0
+    p = b.fnot * initial_psi(b, seed) * amp
+    pm = 0.5 * p + 0.25 * b.fnot * initial_psi(b, seed + 11) * amp
+    taux, tauy = _channel_tau(b, 0.05 + 0.02 * seed) if b.cyclic else double_gyre_tau(b)
+    if not b.cyclic:
+        taux = taux * (0.5 + 0.25 * seed)
+    return p, pm, oracle.ekman_from_tau(b, taux, tauy)
+
+
+def _run_pair(members, tdts, nsteps):
+    e = Ensemble(members)
+    singles = []
+    for i, b in enumerate(members):
+        p, pm, (w, ts, tn) = _inputs(b, i + 1)
+        e.set_state(i, p, pm)
+        e.set_forcing(i, w, None, ts, tn)
+        g = QG(b)
+        g.set_state(p, pm)
+        g.set_forcing(w, None, ts, tn)
+        singles.append(g)
+    e.step(tdts, nsteps)
+    e.sync()
+    for g, t in zip(singles, np.broadcast_to(tdts, (len(members),))):
+        g.step(float(t), nsteps)
+    return e, singles
+
+
+def _assert_same(e, singles):
+    for i, g in enumerate(singles):
+        for name, a, c in zip(("p", "pm", "q", "qm"), e.get_state(i), g.get_state()):
+            assert np.array_equal(a, c), "member %d %s rel L2 %.3e" % (i, name, rel_l2(a, c))
+
+
+def test_box_ensemble_equals_single_handles():
+    members = [ocean_double_gyre(n) for n in (65, 129, 33, 97)]
+    members[1].ah4 = [3e10] * 3
+    e, singles = _run_pair(members, 3600.0, 5)      # 2 graph replays + 1 launch
+    _assert_same(e, singles)
+    e.step(3600.0, 3)
+    for g in singles:
+        g.step(3600.0, 3)
+    _assert_same(e, singles)
+
+
+def test_box_ensemble_member_matches_oracle():
+    members = [ocean_double_gyre(97), ocean_double_gyre(65)]
+    e = Ensemble(members)
+    orc = []
+    for i, b in enumerate(members):
+        p, pm, (w, ts, tn) = _inputs(b, i + 1)
+        e.set_state(i, p, pm)
+        e.set_forcing(i, w, None, ts, tn)
+        o = oracle.Oracle(b)
+        o.set_state(p, pm)
+        o.set_forcing(w, None, ts, tn)
+        orc.append(o)
+    e.step(3600.0, 10)
+    for o in orc:
+        o.step(3600.0, 10)
+    for i, o in enumerate(orc):
+        for name, a, c in zip(("p", "q"), e.get_state(i)[::2], o.get_state()[::2]):
+            assert rel_l2(a, c) <= 1e-10, (i, name)
+
+
+def test_channel_ensemble_equals_single_handles():
+    members = [atmos_channel(49, 25), atmos_channel(97, 65), atmos_channel(193, 97)]
+    e, singles = _run_pair(members, 360.0, 4)
+    _assert_same(e, singles)
+
+
+def test_per_member_step_and_mixed_precision():
+    members = [ocean_double_gyre(n, precision=OQG_MIXED) for n in (129, 65, 97)]
+    tdts = np.array([3600.0, 1800.0, 2400.0])
+    e, singles = _run_pair(members, tdts, 4)
+    _assert_same(e, singles)
+
+
+def test_ensemble_rejects_bad_members():
+    from openqg_b200.core import OqgError
+    with pytest.raises(OqgError):
+        Ensemble([ocean_double_gyre(33), atmos_channel(49, 25)])
