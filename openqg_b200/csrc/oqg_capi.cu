@@ -637,7 +637,7 @@ int oqg_create(const oqg_params *prm, oqg_handle **out) {
     b.rhs = dalloc<double>(h, (size_t)b.nl * b.ny * b.pr);
     b.spec = dalloc<double>(h, (size_t)b.nl * b.ny * b.pk * (b.cyclic ? 2 : 1));
     std::vector<double> tw;
-    fft_twiddles(b.M, tw);
+    fft_stage_twiddles(b.M, rad, tw);
     double *d_tw64 = dalloc<double>(h, tw.size());
     void *d_tw = d_tw64;
     if (h->mixed) {
@@ -698,14 +698,14 @@ int oqg_create(const oqg_params *prm, oqg_handle **out) {
     b.k4_rows = 2;
     h->ni = (b.ny + b.k4_rows - 1) / b.k4_rows;
     h->smem_v = vort_smem_bytes(b.vty, (int)h->esz);
-    const int NTW = fft_tw_len(b.M), LB = fft_buf_len(b.M);
-    h->smem_x = (size_t)round16(NTW * (int)t2) + (size_t)GX * 2 * LB * t2;
-    h->smem_x64 = (size_t)round16(NTW * 16) + (size_t)GX * 2 * LB * 16;
+    const int LB = fft_buf_len(b.M);
+    h->smem_x = (size_t)GX * 2 * LB * t2;
+    h->smem_x64 = (size_t)GX * 2 * LB * 16;
     h->smem_y = (size_t)LDy * h->KB * (vsz + 8);
     // rows of an assembly CTA: k4_rows interior rows plus at most one wall row
     const int nra = (b.ny > b.k4_rows) ? b.k4_rows + 1 : b.ny + 2;
-    h->smem_i = (size_t)round16(NTW * (int)t2) + (size_t)G * 2 * LB * t2 + (size_t)b.nl * nra * b.nxp * h->esz;
-    h->smem_i64 = (size_t)round16(NTW * 16) + (size_t)G * 2 * LB * 16 + (size_t)b.nl * nra * b.nxp * 8;
+    h->smem_i = (size_t)G * 2 * LB * t2 + (size_t)b.nl * nra * b.nxp * h->esz;
+    h->smem_i64 = (size_t)G * 2 * LB * 16 + (size_t)b.nl * nra * b.nxp * 8;
     if (h->smem_i64 > 227 * 1024 || h->smem_x64 > 227 * 1024 || h->smem_y > 227 * 1024)
         return bail(OQG_EUNSUPPORTED, "grid too large for this build's shared-memory tiling");
     std::vector<Work> wv(h->nv), wx(h->nx), wy(h->nys), wi(h->ni);
@@ -1211,7 +1211,7 @@ int oqg_ensemble_create(const oqg_params *members, int nmembers, oqg_ensemble **
         const BasinDev &b = e->m[i]->hb;
         const int TT = (b.M + e->E - 1) / e->E;
         const int G = std::max(1, XTHREADS / TT);
-        const int NTW = fft_tw_len(b.M), LB = fft_buf_len(b.M);
+        const int LB = fft_buf_len(b.M);
         const int npm = (b.ny + 1) / 2;
         const int nvb = b.tiles_x * b.tiles_y;
         const int nxb = (b.nl * npm + G - 1) / G;
@@ -1223,10 +1223,9 @@ int oqg_ensemble_create(const oqg_params *members, int nmembers, oqg_ensemble **
         for (int k = 0; k < nib; ++k) wi.push_back(Work{i, k});
         const int nra = (b.ny > b.k4_rows) ? b.k4_rows + 1 : b.ny + 2;
         e->smem_v = std::max(e->smem_v, vort_smem_bytes(b.vty, (int)esz));
-        e->smem_x = std::max(e->smem_x, (size_t)round16(NTW * (int)t2) + (size_t)G * 2 * LB * t2);
+        e->smem_x = std::max(e->smem_x, (size_t)G * 2 * LB * t2);
         e->smem_y = std::max(e->smem_y, (size_t)((b.ny + 32) | 1) * 4 * (vsz + 8));
-        e->smem_i = std::max(e->smem_i, (size_t)round16(NTW * (int)t2) + (size_t)G * 2 * LB * t2 +
-                                            (size_t)b.nl * nra * b.nxp * esz);
+        e->smem_i = std::max(e->smem_i, (size_t)G * 2 * LB * t2 + (size_t)b.nl * nra * b.nxp * esz);
     }
     if (e->smem_x > 227 * 1024 || e->smem_i > 227 * 1024 || e->smem_v > 227 * 1024) {
         ens_free(e);

@@ -83,7 +83,7 @@ struct BasinDev {
     const void *tmaps;          // box: OQG_NTMAP tensor maps (128 bytes each) or null
     void *rhs;                  // [nl][ny][pr] T
     void *spec;                 // [nl][ny][pk] T or T2
-    const void *tw;             // [M] T2 twiddles exp(-2 pi i t/M)
+    const void *tw;             // [M] T2 per-stage FFT twiddles (fft_stage_twiddles)
     const double *piv_tab;      // Thomas pivots 1/(b - a gam), compressed
     const int *piv_off;         // [nl*nk] offset into piv_tab
     const int *piv_len;         // [nl*nk] stored length (beyond: fixed point)

@@ -144,32 +144,26 @@ template <class T> struct Dft<T, 5> {
 __device__ __forceinline__ int fpad(int i) { return i + (i >> 3); }
 __host__ __device__ __forceinline__ int fft_buf_len(int M) { return M + (M >> 3) + 4; }
 
-// exp(-2 pi i k / M) from the two-level table tw = [B(0..63), A(0..M/64)]:
-// B[l] = exp(-2 pi i l / M), A[h] = exp(-2 pi i 64 h / M).
-template <class T>
-__device__ __forceinline__ typename C2<T>::t twiddle(const typename C2<T>::t *tw, int k) {
-    return c_mul(tw[64 + (k >> 6)], tw[k & 63]);
-}
-__host__ __device__ __forceinline__ int fft_tw_len(int M) { return 64 + (M + 63) / 64 + 1; }
-
 // One Stockham stage of radix R: src -> dst (both shared, padded, length M).
 // Threads t < TT of the transform's group each take butterflies t, t+TT, ...
-// Twiddles tw (two-level table, see twiddle) are in shared memory.
+// tws: this stage's twiddles in global memory (read through L1), entry
+// jm (R-1) + r - 1 = exp(-2 pi i r jm / (Ns R)).  lg = log2(Ns) when Ns is a
+// power of two (no integer division), else -1.
 template <class T, int R>
 __device__ __forceinline__ void fft_stage(const typename C2<T>::t *__restrict__ src,
-                                          typename C2<T>::t *__restrict__ dst, int M, int Ns,
-                                          const typename C2<T>::t *__restrict__ tw, int t, int TT) {
+                                          typename C2<T>::t *__restrict__ dst, int M, int Ns, int lg,
+                                          const typename C2<T>::t *__restrict__ tws, int t, int TT) {
     typedef typename C2<T>::t T2;
     const int nb = M / R;
-    const int tstep = M / (Ns * R);
     for (int j = t; j < nb; j += TT) {
-        const int q = j / Ns, jm = j - q * Ns;
+        const int q = lg >= 0 ? (j >> lg) : j / Ns, jm = j - q * Ns;
         T2 v[R];
 #pragma unroll
         for (int r = 0; r < R; ++r) v[r] = src[fpad(j + r * nb)];
         if (jm != 0) {
+            const T2 *w = tws + jm * (R - 1);
 #pragma unroll
-            for (int r = 1; r < R; ++r) v[r] = c_mul(v[r], twiddle<T>(tw, r * jm * tstep));
+            for (int r = 1; r < R; ++r) v[r] = c_mul(v[r], __ldg(w + r - 1));
         }
         Dft<T, R>::run(v);
         const int d = q * Ns * R + jm;
@@ -187,8 +181,10 @@ __device__ __forceinline__ void bar_sync(int id, int n) {
 
 // Forward FFT of length M (radices rad[0..nrad)) from padded buffer a, using
 // padded buffer b as the second buffer of the ping-pong.  Returns the buffer
-// holding the result.  The nbar threads that synchronise on barrier bar_id
-// must all call it; threads with t >= TT only take part in the barriers.
+// holding the result.  tw: the per-stage twiddle tables (global memory; the
+// stage after Ns starts at entry Ns - 1).  The nbar threads that synchronise
+// on barrier bar_id must all call it; threads with t >= TT only take part in
+// the barriers.
 template <class T>
 __device__ typename C2<T>::t *fft_smem(typename C2<T>::t *a, typename C2<T>::t *b, int M,
                                        const int *rad, int nrad,
@@ -199,12 +195,14 @@ __device__ typename C2<T>::t *fft_smem(typename C2<T>::t *a, typename C2<T>::t *
     int Ns = 1;
     for (int s = 0; s < nrad; ++s) {
         const int R = rad[s];
+        const int lg = (Ns & (Ns - 1)) == 0 ? __ffs(Ns) - 1 : -1;
+        const T2 *tws = tw + (Ns - 1);
         switch (R) {
-            case 8: fft_stage<T, 8>(src, dst, M, Ns, tw, t, TT); break;
-            case 4: fft_stage<T, 4>(src, dst, M, Ns, tw, t, TT); break;
-            case 2: fft_stage<T, 2>(src, dst, M, Ns, tw, t, TT); break;
-            case 3: fft_stage<T, 3>(src, dst, M, Ns, tw, t, TT); break;
-            default: fft_stage<T, 5>(src, dst, M, Ns, tw, t, TT); break;
+            case 8: fft_stage<T, 8>(src, dst, M, Ns, lg, tws, t, TT); break;
+            case 4: fft_stage<T, 4>(src, dst, M, Ns, lg, tws, t, TT); break;
+            case 2: fft_stage<T, 2>(src, dst, M, Ns, lg, tws, t, TT); break;
+            case 3: fft_stage<T, 3>(src, dst, M, Ns, lg, tws, t, TT); break;
+            default: fft_stage<T, 5>(src, dst, M, Ns, lg, tws, t, TT); break;
         }
         bar_sync(bar_id, nbar);
         T2 *x = src; src = dst; dst = x;

@@ -629,9 +629,9 @@ k_vort(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par,
 
 // ------------------------------------------------------------------ k_xfwd
 // Threads per transform TT = ceil(M/E); G = blockDim/TT transforms per CTA.
-// Shared memory: the twiddle table, then per group two padded buffers of
-// fft_buf_len(M) complex values; the input rows are staged by cp.async into
-// the second buffer and expanded into the first.
+// Shared memory: per group two padded buffers of fft_buf_len(M) complex
+// values; the input rows are staged by cp.async into the second buffer and
+// expanded into the first.  The stage twiddles are read from global memory.
 __host__ __device__ __forceinline__ int round16(int bytes) { return (bytes + 15) & ~15; }
 
 template <class T, int E>
@@ -643,9 +643,8 @@ k_xfwd(const BasinDev *__restrict__ bas, const Work *__restrict__ work, const vo
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int M = b.M, TT = (M + E - 1) / E, G = blockDim.x / TT;
     const int g = threadIdx.x / TT, t = threadIdx.x - g * TT;
-    const int LB = fft_buf_len(M), NTW = fft_tw_len(M);
-    T2 *sTw = reinterpret_cast<T2 *>(smem_raw);
-    T2 *zs = reinterpret_cast<T2 *>(smem_raw + round16(NTW * (int)sizeof(T2)));
+    const int LB = fft_buf_len(M);
+    T2 *zs = reinterpret_cast<T2 *>(smem_raw);
     const int npm = (b.ny + 1) >> 1;          // row pairs per mode
     const int pair = w.block * G + g;
     const bool live = g < G && pair < b.nl * npm;
@@ -660,7 +659,6 @@ k_xfwd(const BasinDev *__restrict__ bas, const Work *__restrict__ work, const vo
     const T *R = (const T *)(rhs_override ? rhs_override : b.rhs);
     const T *x = R + ((size_t)m * b.ny + j) * b.pr;
     pdl_trigger();
-    cp_async_16(sTw, b.tw, round16(NTW * (int)sizeof(T2)), threadIdx.x, blockDim.x);   // constant
     pdl_wait();
     if (live) {
         cp_async_16(raw, x, round16(n * (int)sizeof(T)), t, TT);
@@ -688,7 +686,7 @@ k_xfwd(const BasinDev *__restrict__ bas, const Work *__restrict__ work, const vo
         }
     }
     __syncthreads();
-    T2 *z = fft_smem<T>(za, zb, M, b.rad, b.nrad, sTw, live ? t : TT, TT, 0, 0);
+    T2 *z = fft_smem<T>(za, zb, M, b.rad, b.nrad, (const T2 *)b.tw, live ? t : TT, TT, 0, 0);
     if (!live) return;
     if (!b.cyclic) {
         T *S = (T *)b.spec;
@@ -1163,11 +1161,10 @@ k_xinv(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par,
     xinv_rows(b, w.block, jlo, jhi, jfirst, nra);
     const int nr = jhi - jlo;                    // interior rows
     const int nxp = b.nxp, n = b.nxin, nyp = b.nyp, px = b.px;
-    const int LB = fft_buf_len(M), NTW = fft_tw_len(M);
+    const int LB = fft_buf_len(M);
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ XinvScal sS;
-    T2 *sTw = reinterpret_cast<T2 *>(smem_raw);
-    T2 *zs = reinterpret_cast<T2 *>(smem_raw + round16(NTW * (int)sizeof(T2)));
+    T2 *zs = reinterpret_cast<T2 *>(smem_raw);
     T *inh = reinterpret_cast<T *>(zs + (size_t)G * 2 * LB);   // [NL][nra][nxp]
     const T ftn = (T)b.ftnorm;
 
@@ -1178,7 +1175,6 @@ k_xinv(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par,
     } else {
     // zero the wall rows / columns of the modal fields
     for (int idx = threadIdx.x; idx < NL * nra * nxp; idx += nfft) inh[idx] = (T)0;
-    cp_async_16(sTw, b.tw, round16(NTW * (int)sizeof(T2)), threadIdx.x, nfft);   // constant
     pdl_wait();
 
     const int npr = (nr + 1) >> 1;               // row pairs per mode
@@ -1233,7 +1229,7 @@ k_xinv(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par,
             }
         }
         bar_sync(1, nfft);
-        T2 *z = fft_smem<T>(za, zb, M, b.rad, b.nrad, sTw, live ? t : TT, TT, 1, nfft);
+        T2 *z = fft_smem<T>(za, zb, M, b.rad, b.nrad, (const T2 *)b.tw, live ? t : TT, TT, 1, nfft);
         if (live) {
             const int lr = (jlo + r0) - jfirst;
             T *ox = inh + ((size_t)m * nra + lr) * nxp;

@@ -170,15 +170,21 @@ bool fft_radices(int M, std::vector<int> &rad) {
     return m == 1;
 }
 
-void fft_twiddles(int M, std::vector<double> &tw) {
-    const int ntw = 64 + (M + 63) / 64 + 1;
-    tw.assign(2 * (size_t)ntw, 0.0);
+void fft_stage_twiddles(int M, const std::vector<int> &rad, std::vector<double> &tw) {
+    tw.assign(2 * (size_t)std::max(M, 1), 0.0);
     const long double pi = 3.14159265358979323846264338327950288L;
-    for (int e = 0; e < ntw; ++e) {
-        const long long k = e < 64 ? e : 64LL * (e - 64);
-        const long double ang = -2.0L * pi * (long double)(k % M) / (long double)M;
-        tw[2 * e] = (double)cosl(ang);
-        tw[2 * e + 1] = (double)sinl(ang);
+    long long Ns = 1;
+    for (int R : rad) {
+        // stage of radix R after Ns: entries (jm, r) at Ns-1 + jm (R-1) + r-1
+        for (long long jm = 0; jm < Ns; ++jm)
+            for (int r = 1; r < R; ++r) {
+                const long long k = (long long)r * jm;       // exponent k / (Ns R)
+                const long double ang = -2.0L * pi * (long double)(k % (Ns * R)) / (long double)(Ns * R);
+                const size_t e = (size_t)(Ns - 1 + jm * (R - 1) + (r - 1));
+                tw[2 * e] = (double)cosl(ang);
+                tw[2 * e + 1] = (double)sinl(ang);
+            }
+        Ns *= R;
     }
 }
 

@@ -31,11 +31,12 @@ void setup_pivots(bool cyclic, int nxp, int nyp, double dx, double dy,
 // Radices (8, 4, 2, 3, 5) of a transform length; false if another prime remains.
 bool fft_radices(int M, std::vector<int> &rad);
 
-// Two-level twiddle table of a length-M transform, interleaved (re, im),
-// correctly rounded: entries 0..63 are exp(-2 pi i l / M), entries 64.. are
-// exp(-2 pi i 64 h / M), h = 0..M/64; exp(-2 pi i k / M) is their product
-// for l = k mod 64, h = k / 64.  ntw = 64 + ceil(M/64) + 1 entries.
-void fft_twiddles(int M, std::vector<double> &tw);
+// Twiddles of every Stockham stage of a length-M transform with radices rad,
+// interleaved (re, im) and correctly rounded: the stage of radix R that
+// follows Ns = product of the earlier radices holds exp(-2 pi i r jm/(Ns R))
+// for jm < Ns, 1 <= r < R at entry Ns - 1 + jm (R-1) + r - 1; M - 1 entries
+// in all (the table has M).
+void fft_stage_twiddles(int M, const std::vector<int> &rad, std::vector<double> &tw);
 
 // w_k = sum_{i=1..n} 2 sin(pi i k/(n+1)), k = 1..n: the x-sum of the k-th
 // inverse DST-I basis row.
