@@ -102,6 +102,24 @@ struct BasinDev {
                                 // passes tdt = 0 (ensembles: one per member)
 };
 
+// Division of ints in [0, 2^31) by a divisor d >= 1 fixed for a loop, by a
+// multiply-high and a shift (Granlund and Montgomery's method with a 33-bit
+// multiplier 2^32 + m): q = (umulhi(m, n) + n) >> s, s = ceil(log2 d),
+// m = floor(2^32 (2^s - d) / d) + 1.
+struct FastDiv {
+    unsigned m = 1;
+    int s = 0;
+    FastDiv() = default;
+    __host__ __device__ __forceinline__ explicit FastDiv(int d) {
+        s = 0;
+        while ((1u << s) < (unsigned)d) ++s;
+        m = (unsigned)(((1ull << 32) * ((1ull << s) - (unsigned long long)d)) / (unsigned long long)d + 1ull);
+    }
+    __device__ __forceinline__ int div(int n) const {
+        return (int)((__umulhi(m, (unsigned)n) + (unsigned)n) >> s);
+    }
+};
+
 // One entry of a launch's work list: which basin and which block of it.
 struct Work {
     int member;

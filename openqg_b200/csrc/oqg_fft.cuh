@@ -148,15 +148,16 @@ __host__ __device__ __forceinline__ int fft_buf_len(int M) { return M + (M >> 3)
 // Threads t < TT of the transform's group each take butterflies t, t+TT, ...
 // tws: this stage's twiddles in global memory (read through L1), entry
 // jm (R-1) + r - 1 = exp(-2 pi i r jm / (Ns R)).  lg = log2(Ns) when Ns is a
-// power of two (no integer division), else -1.
+// power of two (a shift), else -1 (fd divides by Ns).
 template <class T, int R>
 __device__ __forceinline__ void fft_stage(const typename C2<T>::t *__restrict__ src,
                                           typename C2<T>::t *__restrict__ dst, int M, int Ns, int lg,
-                                          const typename C2<T>::t *__restrict__ tws, int t, int TT) {
+                                          FastDiv fd, const typename C2<T>::t *__restrict__ tws, int t,
+                                          int TT) {
     typedef typename C2<T>::t T2;
     const int nb = M / R;
     for (int j = t; j < nb; j += TT) {
-        const int q = lg >= 0 ? (j >> lg) : j / Ns, jm = j - q * Ns;
+        const int q = lg >= 0 ? (j >> lg) : fd.div(j), jm = j - q * Ns;
         T2 v[R];
 #pragma unroll
         for (int r = 0; r < R; ++r) v[r] = src[fpad(j + r * nb)];
@@ -197,12 +198,14 @@ __device__ typename C2<T>::t *fft_smem(typename C2<T>::t *a, typename C2<T>::t *
         const int R = rad[s];
         const int lg = (Ns & (Ns - 1)) == 0 ? __ffs(Ns) - 1 : -1;
         const T2 *tws = tw + (Ns - 1);
+        FastDiv fd;
+        if (lg < 0) fd = FastDiv(Ns);
         switch (R) {
-            case 8: fft_stage<T, 8>(src, dst, M, Ns, lg, tws, t, TT); break;
-            case 4: fft_stage<T, 4>(src, dst, M, Ns, lg, tws, t, TT); break;
-            case 2: fft_stage<T, 2>(src, dst, M, Ns, lg, tws, t, TT); break;
-            case 3: fft_stage<T, 3>(src, dst, M, Ns, lg, tws, t, TT); break;
-            default: fft_stage<T, 5>(src, dst, M, Ns, lg, tws, t, TT); break;
+            case 8: fft_stage<T, 8>(src, dst, M, Ns, lg, fd, tws, t, TT); break;
+            case 4: fft_stage<T, 4>(src, dst, M, Ns, lg, fd, tws, t, TT); break;
+            case 2: fft_stage<T, 2>(src, dst, M, Ns, lg, fd, tws, t, TT); break;
+            case 3: fft_stage<T, 3>(src, dst, M, Ns, lg, fd, tws, t, TT); break;
+            default: fft_stage<T, 5>(src, dst, M, Ns, lg, fd, tws, t, TT); break;
         }
         bar_sync(bar_id, nbar);
         T2 *x = src; src = dst; dst = x;

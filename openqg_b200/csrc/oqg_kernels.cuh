@@ -768,6 +768,7 @@ k_ysolve(const BasinDev *__restrict__ bas, const Work *__restrict__ work) {
     // chunks hit distinct banks.
     const int S_ = (ny + 31) >> 5;
     const int LD = (ny + 32) | 1;            // > (ny-1) + (ny-1)/S, odd
+    const FastDiv fdS(S_);
     extern __shared__ __align__(16) unsigned char smem_raw[];
     V *tile = reinterpret_cast<V *>(smem_raw);                 // [KB][LD]
     double *pvs = reinterpret_cast<double *>(tile + KB * LD);  // [KB][LD] pivots
@@ -789,7 +790,7 @@ k_ysolve(const BasinDev *__restrict__ bas, const Work *__restrict__ work) {
 #pragma unroll
             for (int u = 0; u < CH; ++u) {
                 const int jj = j0 + 32 * u;
-                if (jj < ny) pvs[c * LD + jj + jj / S_] = v[u];
+                if (jj < ny) pvs[c * LD + jj + fdS.div(jj)] = v[u];
             }
         }
     }
@@ -809,7 +810,7 @@ k_ysolve(const BasinDev *__restrict__ bas, const Work *__restrict__ work) {
         for (int u = 0; u < CH; ++u) {
             const int idx = i0 + 128 * u;
             const int jj = idx >> 2, cc = idx & 3;
-            if (idx < ny * KB) tile[cc * LD + jj + jj / S_] = v[u];
+            if (idx < ny * KB) tile[cc * LD + jj + fdS.div(jj)] = v[u];
         }
     }
     __syncthreads();
@@ -877,8 +878,8 @@ k_ysolve(const BasinDev *__restrict__ bas, const Work *__restrict__ work) {
             const int idx = i0 + 128 * u;
             const int jj = idx >> 2, cc = idx & 3, kk = k0 + cc;
             if (idx < ny * KB && kk < nk) {
-                if constexpr (CPLX) S[(size_t)jj * pk + kk] = yt_store2<Gm>(tile[cc * LD + jj + jj / S_]);
-                else S[(size_t)jj * pk + kk] = yt_store<Gm>(tile[cc * LD + jj + jj / S_]);
+                if constexpr (CPLX) S[(size_t)jj * pk + kk] = yt_store2<Gm>(tile[cc * LD + jj + fdS.div(jj)]);
+                else S[(size_t)jj * pk + kk] = yt_store<Gm>(tile[cc * LD + jj + fdS.div(jj)]);
             }
         }
     }
@@ -1281,6 +1282,7 @@ k_xinv(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par,
         for (int m = 1; m < NL; ++m) hc[m - 1] = sc->alpha[m - 1];
     }
     const T *__restrict__ H = (const T *)b.hsb;
+    const FastDiv fdx(nxp);
     constexpr int U = 4;
     for (int base = threadIdx.x; base < nra * nxp; base += U * blockDim.x) {
         // gather the inputs of U points first (independent loads), then compute
@@ -1290,7 +1292,7 @@ k_xinv(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par,
         for (int u = 0; u < U; ++u) {
             const int idx = base + u * blockDim.x;
             const bool ok = idx < nra * nxp;
-            const int lr = ok ? idx / nxp : 0, i = ok ? idx - lr * nxp : 0;
+            const int lr = ok ? fdx.div(idx) : 0, i = ok ? idx - lr * nxp : 0;
             const int j = jfirst + lr;
             lrs[u] = ok ? lr : -1;
             is[u] = i;
@@ -1337,7 +1339,7 @@ k_xinv(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par,
     const T *Qm = (const T *)b.F[2 + par];
     const T fac = (T)b.qb_fac;
     for (int idx = threadIdx.x; idx < nra * nxp; idx += blockDim.x) {
-        const int lr = idx / nxp, i = idx - lr * nxp;
+        const int lr = fdx.div(idx), i = idx - lr * nxp;
         const int j = jfirst + lr;
         const bool zon = (j == 0 || j == nyp - 1);
         const bool mer = !b.cyclic && (i == 0 || i == nxp - 1);
