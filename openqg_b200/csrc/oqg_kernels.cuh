@@ -750,6 +750,74 @@ template <> __device__ __forceinline__ float2 yt_store2<float2>(double2 v) { ret
 __device__ __forceinline__ double yt_re(double v) { return v; }
 __device__ __forceinline__ double yt_re(double2 v) { return v.x; }
 
+// The column solve of one warp with each lane's rows [s, s+n) (n <= SM)
+// held in registers through all four passes: forward elimination as an
+// affine scan (chunk pass, warp scan of the chunk maps, chunk pass), then back
+// substitution the same way from the bottom.  col/pc: the column and its
+// pivots in shared memory at padded offset o.
+#define YREG 16
+template <class V, int SM>
+__device__ __forceinline__ void ysolve_chunk_regs(V *col, const double *pc, double a, int lane, int s, int n,
+                                                  int o, int ny, double &colsum) {
+    V x[SM];
+    double bt[SM];
+#pragma unroll
+    for (int t = 0; t < SM; ++t) {
+        x[t] = t < n ? col[o + t] : yt_zero(V());
+        bt[t] = t < n ? pc[o + t] : 0.0;
+    }
+    // forward elimination: u_j = f_j beta_j - a beta_j u_{j-1}
+    V C = yt_zero(V());
+    double D = 1.0;
+#pragma unroll
+    for (int t = 0; t < SM; ++t)
+        if (t < n) {
+            C = yt_axpy(yt_scale(x[t], bt[t]), -a * bt[t], C);
+            D = -a * bt[t] * D;
+        }
+    for (int q = 1; q < 32; q <<= 1) {
+        V Co = yt_up(C, q);
+        double Do = shfl_up_d(D, q);
+        if (lane >= q) { C = yt_axpy(C, D, Co); D = D * Do; }
+    }
+    V uu = yt_up(C, 1);
+    if (lane == 0) uu = yt_zero(V());
+#pragma unroll
+    for (int t = 0; t < SM; ++t)
+        if (t < n) {
+            uu = yt_axpy(yt_scale(x[t], bt[t]), -a * bt[t], uu);
+            x[t] = uu;
+        }
+    // back substitution: u_j = u'_j - a beta_j u_{j+1}
+    C = yt_zero(V());
+    D = 1.0;
+#pragma unroll
+    for (int t = SM - 1; t >= 0; --t)
+        if (t < n) {
+            const double ej = (s + t == ny - 1) ? 0.0 : -a * bt[t];
+            C = yt_axpy(x[t], ej, C);
+            D = ej * D;
+        }
+    for (int q = 1; q < 32; q <<= 1) {
+        V Co = yt_dn(C, q);
+        double Do = shfl_dn_d(D, q);
+        if (lane + q < 32) { C = yt_axpy(C, D, Co); D = D * Do; }
+    }
+    uu = yt_dn(C, 1);
+    if (lane == 31) uu = yt_zero(V());
+#pragma unroll
+    for (int t = SM - 1; t >= 0; --t)
+        if (t < n) {
+            const double ej = (s + t == ny - 1) ? 0.0 : -a * bt[t];
+            uu = yt_axpy(x[t], ej, uu);
+            x[t] = uu;
+            colsum += yt_re(uu);
+        }
+#pragma unroll
+    for (int t = 0; t < SM; ++t)
+        if (t < n) col[o + t] = x[t];
+}
+
 template <class T, bool CPLX, int NL>
 __global__ void __launch_bounds__(128)
 k_ysolve(const BasinDev *__restrict__ bas, const Work *__restrict__ work) {
@@ -823,51 +891,54 @@ k_ysolve(const BasinDev *__restrict__ bas, const Work *__restrict__ work) {
         const int s = lane * S_, e = min(s + S_, ny);
         const int o = lane * (S_ + 1);          // padded offset of row s
         const int n = max(e - s, 0);
-        // forward elimination: u_j = f_j beta_j - a beta_j u_{j-1}
-        V C = yt_zero(V());
-        double D = 1.0;
-#pragma unroll 8
-        for (int t = 0; t < n; ++t) {
-            const double bt = pc[o + t];
-            C = yt_axpy(yt_scale(col[o + t], bt), -a * bt, C);
-            D = -a * bt * D;
-        }
-        for (int q = 1; q < 32; q <<= 1) {
-            V Co = yt_up(C, q);
-            double Do = shfl_up_d(D, q);
-            if (lane >= q) { C = yt_axpy(C, D, Co); D = D * Do; }
-        }
-        V uu = yt_up(C, 1);
-        if (lane == 0) uu = yt_zero(V());
-#pragma unroll 8
-        for (int t = 0; t < n; ++t) {
-            const double bt = pc[o + t];
-            uu = yt_axpy(yt_scale(col[o + t], bt), -a * bt, uu);
-            col[o + t] = uu;
-        }
-        // back substitution: u_j = u'_j - a beta_j u_{j+1}
-        C = yt_zero(V());
-        D = 1.0;
-#pragma unroll 8
-        for (int t = n - 1; t >= 0; --t) {
-            const double ej = (s + t == ny - 1) ? 0.0 : -a * pc[o + t];
-            C = yt_axpy(col[o + t], ej, C);
-            D = ej * D;
-        }
-        for (int q = 1; q < 32; q <<= 1) {
-            V Co = yt_dn(C, q);
-            double Do = shfl_dn_d(D, q);
-            if (lane + q < 32) { C = yt_axpy(C, D, Co); D = D * Do; }
-        }
-        uu = yt_dn(C, 1);
-        if (lane == 31) uu = yt_zero(V());
         double colsum = 0.0;
+        if (S_ <= YREG) ysolve_chunk_regs<V, YREG>(col, pc, a, lane, s, n, o, ny, colsum);
+        else {
+            // forward elimination: u_j = f_j beta_j - a beta_j u_{j-1}
+            V C = yt_zero(V());
+            double D = 1.0;
 #pragma unroll 8
-        for (int t = n - 1; t >= 0; --t) {
-            const double ej = (s + t == ny - 1) ? 0.0 : -a * pc[o + t];
-            uu = yt_axpy(col[o + t], ej, uu);
-            col[o + t] = uu;
-            colsum += yt_re(uu);
+            for (int t = 0; t < n; ++t) {
+                const double bt = pc[o + t];
+                C = yt_axpy(yt_scale(col[o + t], bt), -a * bt, C);
+                D = -a * bt * D;
+            }
+            for (int q = 1; q < 32; q <<= 1) {
+                V Co = yt_up(C, q);
+                double Do = shfl_up_d(D, q);
+                if (lane >= q) { C = yt_axpy(C, D, Co); D = D * Do; }
+            }
+            V uu = yt_up(C, 1);
+            if (lane == 0) uu = yt_zero(V());
+#pragma unroll 8
+            for (int t = 0; t < n; ++t) {
+                const double bt = pc[o + t];
+                uu = yt_axpy(yt_scale(col[o + t], bt), -a * bt, uu);
+                col[o + t] = uu;
+            }
+            // back substitution: u_j = u'_j - a beta_j u_{j+1}
+            C = yt_zero(V());
+            D = 1.0;
+#pragma unroll 8
+            for (int t = n - 1; t >= 0; --t) {
+                const double ej = (s + t == ny - 1) ? 0.0 : -a * pc[o + t];
+                C = yt_axpy(col[o + t], ej, C);
+                D = ej * D;
+            }
+            for (int q = 1; q < 32; q <<= 1) {
+                V Co = yt_dn(C, q);
+                double Do = shfl_dn_d(D, q);
+                if (lane + q < 32) { C = yt_axpy(C, D, Co); D = D * Do; }
+            }
+            uu = yt_dn(C, 1);
+            if (lane == 31) uu = yt_zero(V());
+#pragma unroll 8
+            for (int t = n - 1; t >= 0; --t) {
+                const double ej = (s + t == ny - 1) ? 0.0 : -a * pc[o + t];
+                uu = yt_axpy(col[o + t], ej, uu);
+                col[o + t] = uu;
+                colsum += yt_re(uu);
+            }
         }
         if (!CPLX) wsum = b.dst_w[k] * warp_sum(colsum);
     }
