@@ -50,7 +50,7 @@ struct oqg_handle {
     std::vector<void *> allocs;
     Work *d_wv = nullptr, *d_wx = nullptr, *d_wy = nullptr, *d_wi = nullptr;
     int nv = 0, nx = 0, nys = 0, ni = 0;
-    int E = 8, KB = 16, xthreads = 128;
+    int E = 8, KB = 16, xthreads = 128, xi_threads = 64;
     size_t smem_v = 0, smem_x = 0, smem_x64 = 0, smem_y = 0, smem_i = 0, smem_i64 = 0;
     double *stage[2] = {nullptr, nullptr};
     unsigned long long *d_bad = nullptr;
@@ -72,10 +72,25 @@ static X *dalloc(oqg_handle *h, size_t count) {
 }
 
 // ----------------------------------------------------------- launch helpers
-static const int XTHREADS = XINV_FFT_THREADS;
+static const int XTHREADS = 256;   // forward-transform CTA size (ensembles)
 
 // Launch with programmatic stream serialisation: the kernel may be scheduled
 // while its predecessor drains and waits in griddepcontrol.wait for its data.
+// Inverse-transform CTA: transform threads for all NL row pairs of a CTA in
+// one round where they fit (XINV_E values per thread), plus the scalar warp.
+static int xinv_fft_threads(int M, int nl) {
+    const int tt = (M + XINV_E - 1) / XINV_E;
+    int nfft = std::min(XINV_FFT_MAX, rup(nl * tt, 32));
+    return std::max(nfft, rup(tt, 32));
+}
+// Dynamic shared bytes of k_xinv for nfft transform threads (element size esz).
+static size_t xinv_smem(int M, int nl, int nra, int nxp, int nfft, size_t esz) {
+    const int tt = (M + XINV_E - 1) / XINV_E, G = nfft / tt;
+    const size_t set = (size_t)G * fft_buf_len(M) * 2 * esz;
+    const size_t inh = (size_t)nl * nra * nxp * esz;
+    return G >= nl ? std::max(2 * set, set + inh) : 2 * set + inh;
+}
+
 template <typename... KArgs, typename... Args>
 static void launch_pdl(void (*kern)(KArgs...), int grid, int block, size_t smem, cudaStream_t st,
                        Args... args) {
@@ -101,7 +116,7 @@ static void launch_step_t(oqg_handle *h, int par, double tdt) {
         launch_pdl(k_ysolve<T, true, NL>, h->nys, 32 * h->KB, h->smem_y, h->st, h->d_bas, h->d_wy);
     else
         launch_pdl(k_ysolve<T, false, NL>, h->nys, 32 * h->KB, h->smem_y, h->st, h->d_bas, h->d_wy);
-    launch_pdl(k_xinv<T, E, NL>, h->ni, XINV_THREADS, h->smem_i, h->st, h->d_bas, h->d_wi, par, tdt,
+    launch_pdl(k_xinv<T, NL>, h->ni, h->xi_threads, h->smem_i, h->st, h->d_bas, h->d_wi, par, tdt,
                (double *)nullptr);
 }
 
@@ -114,7 +129,7 @@ static void launch_solve_t(oqg_handle *h, double *out) {
         k_ysolve<double, true, NL><<<h->nys, 32 * h->KB, h->smem_y, h->st>>>(h->d_bas64, h->d_wy);
     else
         k_ysolve<double, false, NL><<<h->nys, 32 * h->KB, h->smem_y, h->st>>>(h->d_bas64, h->d_wy);
-    k_xinv<double, E, NL><<<h->ni, XINV_THREADS, h->smem_i64, h->st>>>(h->d_bas64, h->d_wi, 0, 0.0, out);
+    k_xinv<double, NL><<<h->ni, h->xi_threads, h->smem_i64, h->st>>>(h->d_bas64, h->d_wi, 0, 0.0, out);
 }
 
 // The dynamic shared-memory limit of a kernel is a property of the function
@@ -144,7 +159,7 @@ static void raise_step_smem(size_t v, size_t x, size_t y, size_t i) {
     raise_smem((const void *)k_xfwd<T, E>, x);
     raise_smem((const void *)k_ysolve<T, true, NL>, y);
     raise_smem((const void *)k_ysolve<T, false, NL>, y);
-    raise_smem((const void *)k_xinv<T, E, NL>, i);
+    raise_smem((const void *)k_xinv<T, NL>, i);
 }
 
 template <class T, int NL, int E>
@@ -153,7 +168,7 @@ static void set_attrs_t(oqg_handle *h) {
     raise_smem((const void *)k_xfwd<double, E>, h->smem_x64);
     raise_smem((const void *)k_ysolve<double, true, NL>, h->smem_y);
     raise_smem((const void *)k_ysolve<double, false, NL>, h->smem_y);
-    raise_smem((const void *)k_xinv<double, E, NL>, h->smem_i64);
+    raise_smem((const void *)k_xinv<double, NL>, h->smem_i64);
 }
 
 // dispatch over (T, NL, E)
@@ -419,7 +434,7 @@ static void launch_phase_t(oqg_handle *h, int phase, int par, double tdt) {
             else
                 k_ysolve<T, false, NL><<<h->nys, 32 * h->KB, h->smem_y, h->st>>>(h->d_bas, h->d_wy);
             break;
-        default: k_xinv<T, E, NL><<<h->ni, XINV_THREADS, h->smem_i, h->st>>>(h->d_bas, h->d_wi, par, tdt, nullptr); break;
+        default: k_xinv<T, NL><<<h->ni, h->xi_threads, h->smem_i, h->st>>>(h->d_bas, h->d_wi, par, tdt, nullptr); break;
     }
 }
 static void launch_phase(oqg_handle *h, int phase, int par, double tdt) {
@@ -443,6 +458,7 @@ struct oqg_ensemble {
     Work *d_wv = nullptr, *d_wx = nullptr, *d_wy = nullptr, *d_wi = nullptr;
     int nv = 0, nx = 0, nys = 0, ni = 0;
     size_t smem_v = 0, smem_x = 0, smem_y = 0, smem_i = 0;
+    int xi_threads = 64;
     int par = 0;
     cudaGraphExec_t gexec[2] = {nullptr, nullptr};
     std::vector<void *> allocs;
@@ -472,7 +488,7 @@ static void launch_ens_step_t(oqg_ensemble *e, int par) {
         launch_pdl(k_ysolve<T, true, NL>, e->nys, 128, e->smem_y, e->st, e->d_bas, e->d_wy);
     else
         launch_pdl(k_ysolve<T, false, NL>, e->nys, 128, e->smem_y, e->st, e->d_bas, e->d_wy);
-    launch_pdl(k_xinv<T, E, NL>, e->ni, XINV_THREADS, e->smem_i, e->st, e->d_bas, e->d_wi, par, 0.0,
+    launch_pdl(k_xinv<T, NL>, e->ni, e->xi_threads, e->smem_i, e->st, e->d_bas, e->d_wi, par, 0.0,
                (double *)nullptr);
 }
 template <class T, int NL, int E>
@@ -680,7 +696,7 @@ int oqg_create(const oqg_params *prm, oqg_handle **out) {
 
     // ---- launch geometry
     h->E = b.M <= 2048 ? 8 : 16;
-    const int TT = (b.M + h->E - 1) / h->E, G = std::max(1, XTHREADS / TT);
+    const int TT = (b.M + h->E - 1) / h->E;
     const size_t t2 = 2 * h->esz;
     const int npm = (b.ny + 1) / 2;
     h->nv = b.tiles_x * b.tiles_y;
@@ -704,8 +720,10 @@ int oqg_create(const oqg_params *prm, oqg_handle **out) {
     h->smem_y = (size_t)LDy * h->KB * (vsz + 8);
     // rows of an assembly CTA: k4_rows interior rows plus at most one wall row
     const int nra = (b.ny > b.k4_rows) ? b.k4_rows + 1 : b.ny + 2;
-    h->smem_i = (size_t)G * 2 * LB * t2 + (size_t)b.nl * nra * b.nxp * h->esz;
-    h->smem_i64 = (size_t)G * 2 * LB * 16 + (size_t)b.nl * nra * b.nxp * 8;
+    const int nfft_i = xinv_fft_threads(b.M, b.nl);
+    h->xi_threads = nfft_i + 32;
+    h->smem_i = xinv_smem(b.M, b.nl, nra, b.nxp, nfft_i, h->esz);
+    h->smem_i64 = xinv_smem(b.M, b.nl, nra, b.nxp, nfft_i, 8);
     if (h->smem_i64 > 227 * 1024 || h->smem_x64 > 227 * 1024 || h->smem_y > 227 * 1024)
         return bail(OQG_EUNSUPPORTED, "grid too large for this build's shared-memory tiling");
     std::vector<Work> wv(h->nv), wx(h->nx), wy(h->nys), wi(h->ni);
@@ -1207,6 +1225,9 @@ int oqg_ensemble_create(const oqg_params *members, int nmembers, oqg_ensemble **
         return (long)e->m[a]->hb.nxp * e->m[a]->hb.nyp > (long)e->m[c]->hb.nxp * e->m[c]->hb.nyp;
     });
     std::vector<Work> wv, wx, wy, wi;
+    int nfft_e = 32;
+    for (oqg_handle *h : e->m) nfft_e = std::max(nfft_e, xinv_fft_threads(h->hb.M, h->hb.nl));
+    e->xi_threads = nfft_e + 32;
     for (int i : order) {
         const BasinDev &b = e->m[i]->hb;
         const int TT = (b.M + e->E - 1) / e->E;
@@ -1225,7 +1246,7 @@ int oqg_ensemble_create(const oqg_params *members, int nmembers, oqg_ensemble **
         e->smem_v = std::max(e->smem_v, vort_smem_bytes(b.vty, (int)esz));
         e->smem_x = std::max(e->smem_x, (size_t)G * 2 * LB * t2);
         e->smem_y = std::max(e->smem_y, (size_t)((b.ny + 32) | 1) * 4 * (vsz + 8));
-        e->smem_i = std::max(e->smem_i, (size_t)G * 2 * LB * t2 + (size_t)b.nl * nra * b.nxp * esz);
+        e->smem_i = std::max(e->smem_i, xinv_smem(b.M, b.nl, nra, b.nxp, nfft_e, esz));
     }
     if (e->smem_x > 227 * 1024 || e->smem_i > 227 * 1024 || e->smem_v > 227 * 1024) {
         ens_free(e);

@@ -68,8 +68,8 @@ __device__ __forceinline__ double block_sum(double v, double *red) {
 #define VTX 60          // output columns of a vorticity tile
 #define VTYMAX 17       // output rows of a vorticity tile (at most)
 #define VTHREADS 256    // 64 column lanes x 4 row strips
-#define XINV_FFT_THREADS 256                    // transform threads of k_xinv
-#define XINV_THREADS (XINV_FFT_THREADS + 32)    // plus the scalar-phase warp
+#define XINV_E 16           // complex values per transform thread in k_xinv
+#define XINV_FFT_MAX 512    // at most this many transform threads per k_xinv CTA
 
 // Geometry scalars of a basin used by the stencils.
 template <class T> struct Geo {
@@ -1219,7 +1219,7 @@ __device__ __forceinline__ void xinv_rows(const BasinDev &b, int rb, int &jlo, i
 // out != null: solve-only mode, writes the modal inhomogeneous solutions
 // (FP64, [nl][nyp][px]) and nothing else (no scalar phase).
 // tdt = 0: each member steps with its own b.tdt_m (ensemble launches).
-template <class T, int E, int NL>
+template <class T, int NL>
 __global__ void __maxnreg__(96)
 k_xinv(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par, double tdt, double *out) {
     typedef typename C2<T>::t T2;
@@ -1227,17 +1227,25 @@ k_xinv(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par,
     const BasinDev &b = bas[w.member];
     const int nfft = blockDim.x - 32;
     const bool fft_thread = (int)threadIdx.x < nfft;
-    const int M = b.M, TT = (M + E - 1) / E, G = nfft / TT;
+    const int M = b.M, TT = (M + XINV_E - 1) / XINV_E, G = nfft / TT;
     const int g = threadIdx.x / TT, t = threadIdx.x - g * TT;
     int jlo, jhi, jfirst, nra;
     xinv_rows(b, w.block, jlo, jhi, jfirst, nra);
     const int nr = jhi - jlo;                    // interior rows
     const int nxp = b.nxp, n = b.nxin, nyp = b.nyp, px = b.px;
     const int LB = fft_buf_len(M);
+    const int npr = (nr + 1) >> 1;               // row pairs per mode
+    const int npairs = NL * npr;
+    const bool one_round = G >= npairs;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ XinvScal sS;
-    T2 *zs = reinterpret_cast<T2 *>(smem_raw);
-    T *inh = reinterpret_cast<T *>(zs + (size_t)G * 2 * LB);   // [NL][nra][nxp]
+    // Two sets of G transform buffers; each transform starts in the set that
+    // makes its last stage end in set A, and its spectral rows are staged in
+    // the other.  With every row pair in one round the modal rows inh alias
+    // set B once the transforms are done; otherwise they follow both sets.
+    T2 *setA = reinterpret_cast<T2 *>(smem_raw), *setB = setA + (size_t)G * LB;
+    T2 *set_in = (b.nrad & 1) ? setB : setA, *set_st = (b.nrad & 1) ? setA : setB;
+    T *inh = one_round ? reinterpret_cast<T *>(setB) : reinterpret_cast<T *>(setA + (size_t)2 * G * LB);
     const T ftn = (T)b.ftnorm;
 
     pdl_trigger();
@@ -1246,11 +1254,10 @@ k_xinv(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par,
         if (!out) scalar_phase<T, NL>(b, tdt != 0.0 ? tdt : b.tdt_m, par, w.block == 0, &sS);
     } else {
     // zero the wall rows / columns of the modal fields
-    for (int idx = threadIdx.x; idx < NL * nra * nxp; idx += nfft) inh[idx] = (T)0;
+    if (!one_round)
+        for (int idx = threadIdx.x; idx < NL * nra * nxp; idx += nfft) inh[idx] = (T)0;
     pdl_wait();
 
-    const int npr = (nr + 1) >> 1;               // row pairs per mode
-    const int npairs = NL * npr;
     // a row of the spectral buffer: n reals (box) or nk complex (channel)
     const int rowbytes = b.cyclic ? b.nk * (int)sizeof(T2) : n * (int)sizeof(T);
     const int RO = round16(rowbytes) / (int)sizeof(T);   // second row offset (T units)
@@ -1260,8 +1267,8 @@ k_xinv(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par,
         const int m = live ? pair / npr : 0;
         const int r0 = live ? 2 * (pair - m * npr) : 0;     // interior row offset
         const bool two = live && r0 + 1 < nr;
-        T2 *za = zs + (size_t)(g < G ? g : 0) * 2 * LB;
-        T2 *zb = za + LB;
+        T2 *za = set_in + (size_t)(g < G ? g : 0) * LB;
+        T2 *zb = set_st + (size_t)(g < G ? g : 0) * LB;
         T *raw = reinterpret_cast<T *>(zb);
         const int sj = jlo + r0 - 1;                        // spectral row
         const char *srow = (const char *)b.spec + ((size_t)m * b.ny + sj) * b.pk * (b.cyclic ? sizeof(T2) : sizeof(T));
@@ -1302,6 +1309,11 @@ k_xinv(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par,
         }
         bar_sync(1, nfft);
         T2 *z = fft_smem<T>(za, zb, M, b.rad, b.nrad, (const T2 *)b.tw, live ? t : TT, TT, 1, nfft);
+        if (one_round) {
+            // set B is free now: clear it for the modal rows
+            for (int idx = threadIdx.x; idx < NL * nra * nxp; idx += nfft) inh[idx] = (T)0;
+            bar_sync(1, nfft);
+        }
         if (live) {
             const int lr = (jlo + r0) - jfirst;
             T *ox = inh + ((size_t)m * nra + lr) * nxp;
