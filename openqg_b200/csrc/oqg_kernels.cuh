@@ -71,140 +71,34 @@ __device__ __forceinline__ double block_sum(double v, double *red) {
 #define XINV_E 16           // complex values per transform thread in k_xinv
 #define XINV_FFT_MAX 512    // at most this many transform threads per k_xinv CTA
 
-// Geometry scalars of a basin used by the stencils.
-template <class T> struct Geo {
-    int nxp, nyp, cyclic;
-    T fx, fy, fxb, fyb, jac;
-    __device__ __forceinline__ explicit Geo(const BasinDev &b)
-        : nxp(b.nxp), nyp(b.nyp), cyclic(b.cyclic), fx((T)b.fx), fy((T)b.fy), fxb((T)b.fx_bc),
-          fyb((T)b.fy_bc), jac((T)b.jac_fac) {}
-};
-// The same scalars read from a shared table at each use (K = fx, fy, fxb,
-// fyb, jac), which leaves registers to the stencil windows.
+// Geometry of a basin for the stencils; the coefficients sit in a shared
+// table (K = fx, fy, fxb, fyb, jac) that the kernel fills once.
 template <class T> struct GeoS {
     int nxp, nyp, cyclic;
     const T *K;
-    __device__ __forceinline__ T fxv() const { return K[0]; }
 };
-
-// Laplacian with the mixed wall condition (del2_P_bc, numerics.F90:410-468) at
-// tile point (r, c) of s (leading dimension ld); gi, gj are global indices
-// (for a channel only gj matters).
-template <class T>
-__device__ __forceinline__ T lap_bc(const T *s, int ld, int r, int c, int gi, int gj, const Geo<T> &g) {
-    const T v = s[r * ld + c];
-    const bool zrow = (gj == 0 || gj == g.nyp - 1);
-    const bool wall_x = !g.cyclic && (gi == 0 || gi == g.nxp - 1);
-    if (!zrow && !wall_x)
-        return g.fx * (s[r * ld + c - 1] + s[r * ld + c + 1] - (T)2 * v) +
-               g.fy * (s[(r - 1) * ld + c] + s[(r + 1) * ld + c] - (T)2 * v);
-    T xp, yp;
-    if (zrow) xp = (T)0;
-    else if (gi == 0) xp = g.fxb * (s[r * ld + c + 1] - v);
-    else xp = -(g.fxb * (v - s[r * ld + c - 1]));
-    if (wall_x) yp = (T)0;
-    else if (gj == 0) yp = g.fyb * (s[(r + 1) * ld + c] - v);
-    else yp = -(g.fyb * (v - s[(r - 1) * ld + c]));
-    return xp + yp;
-}
-
-// Arakawa Jacobian J(q, p) (numerics.F90:340-373) at tile point (r, c) of
-// the halo-1 tiles sp, sq.
-template <class T>
-__device__ __forceinline__ T arakawa(const T *sp, const T *sq, int ld, int r, int c, int gi,
-                                     int gj, const Geo<T> &g) {
-    const bool zx = !g.cyclic && (gi == 0 || gi == g.nxp - 1);   // dPdx_2 = 0 here
-    const bool zy = (gj == 0 || gj == g.nyp - 1);                 // dPdy_2 = 0 here
-#define SP(rr, cc) sp[(rr) * ld + (cc)]
-#define SQ(rr, cc) sq[(rr) * ld + (cc)]
-    T pxc = zx ? (T)0 : SP(r, c + 1) - SP(r, c - 1);
-    T pyc = zy ? (T)0 : SP(r + 1, c) - SP(r - 1, c);
-    T qxc = zx ? (T)0 : SQ(r, c + 1) - SQ(r, c - 1);
-    T qyc = zy ? (T)0 : SQ(r + 1, c) - SQ(r - 1, c);
-    T A = (T)0, Bv = (T)0, C = (T)0, D = (T)0;
-    if (!zx) {
-        // dPdx_2(q * dPdy_2(p)) and dPdx_2(p * dPdy_2(q)) at column gi: values
-        // at gi +- 1 of row gj; dPdy_2 is zero on the zonal walls.
-        T pyR = zy ? (T)0 : SP(r + 1, c + 1) - SP(r - 1, c + 1);
-        T pyL = zy ? (T)0 : SP(r + 1, c - 1) - SP(r - 1, c - 1);
-        T qyR = zy ? (T)0 : SQ(r + 1, c + 1) - SQ(r - 1, c + 1);
-        T qyL = zy ? (T)0 : SQ(r + 1, c - 1) - SQ(r - 1, c - 1);
-        A = SQ(r, c + 1) * pyR - SQ(r, c - 1) * pyL;
-        D = SP(r, c + 1) * qyR - SP(r, c - 1) * qyL;
-    }
-    if (!zy) {
-        // dPdy_2(q * dPdx_2(p)) and dPdy_2(p * dPdx_2(q)) at row gj: dPdx_2 at
-        // column gi is zero on box walls.
-        T pxU = zx ? (T)0 : SP(r + 1, c + 1) - SP(r + 1, c - 1);
-        T pxD = zx ? (T)0 : SP(r - 1, c + 1) - SP(r - 1, c - 1);
-        T qxU = zx ? (T)0 : SQ(r + 1, c + 1) - SQ(r + 1, c - 1);
-        T qxD = zx ? (T)0 : SQ(r - 1, c + 1) - SQ(r - 1, c - 1);
-        Bv = SQ(r + 1, c) * pxU - SQ(r - 1, c) * pxD;
-        C = SP(r + 1, c) * qxU - SP(r - 1, c) * qxD;
-    }
-#undef SP
-#undef SQ
-    T t = qxc * pyc - qyc * pxc + A - Bv + C - D;
-    return g.jac * t;
-}
-
-// Laplacian with the mixed wall condition from the five stencil values
-// (W, E, S, N, C), the register form of lap_bc.
-template <class T> __device__ __forceinline__ T gfx(const Geo<T> &g) { return g.fx; }
-template <class T> __device__ __forceinline__ T gfy(const Geo<T> &g) { return g.fy; }
-template <class T> __device__ __forceinline__ T gfxb(const Geo<T> &g) { return g.fxb; }
-template <class T> __device__ __forceinline__ T gfyb(const Geo<T> &g) { return g.fyb; }
-template <class T> __device__ __forceinline__ T gjac(const Geo<T> &g) { return g.jac; }
 template <class T> __device__ __forceinline__ T gfx(const GeoS<T> &g) { return g.K[0]; }
 template <class T> __device__ __forceinline__ T gfy(const GeoS<T> &g) { return g.K[1]; }
 template <class T> __device__ __forceinline__ T gfxb(const GeoS<T> &g) { return g.K[2]; }
 template <class T> __device__ __forceinline__ T gfyb(const GeoS<T> &g) { return g.K[3]; }
 template <class T> __device__ __forceinline__ T gjac(const GeoS<T> &g) { return g.K[4]; }
 
-template <class T, class G>
-__device__ __forceinline__ T lap5(T wv, T ev, T sv, T nv, T c, int gi, int gj, const G &g) {
-    const bool zrow = (gj == 0 || gj == g.nyp - 1);
-    const bool wall_x = !g.cyclic && (gi == 0 || gi == g.nxp - 1);
-    if (!zrow && !wall_x) return gfx(g) * (wv + ev - (T)2 * c) + gfy(g) * (sv + nv - (T)2 * c);
-    T xp, yp;
+// Laplacian with the mixed wall condition (del2_P_bc, numerics.F90:410-468)
+// from the five stencil values (W, E, S, N, C): the interior formula, or on
+// a wall the one-sided mixed-BC terms, chosen by selects (no divergent
+// branches).  fx, fy: 1/dx^2, 1/dy^2; fxb, fyb: their mixed-BC factors.
+template <class T>
+__device__ __forceinline__ T lap5_sel(T wv, T ev, T sv, T nv, T c, bool zrow, bool wl, bool wr, bool jlo,
+                                      bool jhi, T fx, T fy, T fxb, T fyb) {
+    T xp = fx * (wv + ev - (T)2 * c);
+    if (wl) xp = fxb * (ev - c);
+    if (wr) xp = -(fxb * (c - wv));
     if (zrow) xp = (T)0;
-    else if (gi == 0) xp = gfxb(g) * (ev - c);
-    else xp = -(gfxb(g) * (c - wv));
-    if (wall_x) yp = (T)0;
-    else if (gj == 0) yp = gfyb(g) * (nv - c);
-    else yp = -(gfyb(g) * (c - sv));
+    T yp = fy * (sv + nv - (T)2 * c);
+    if (jlo) yp = fyb * (nv - c);
+    if (jhi) yp = -(fyb * (c - sv));
+    if (wl || wr) yp = (T)0;
     return xp + yp;
-}
-
-// Arakawa Jacobian from 3 x 3 windows of p and q (row 0 = j-1, col 0 = i-1).
-template <class T, class G>
-__device__ __forceinline__ T arakawa3(const T (&p)[3][3], const T (&q)[3][3], int gi, int gj,
-                                      const G &g) {
-    const bool zx = !g.cyclic && (gi == 0 || gi == g.nxp - 1);   // dPdx_2 = 0 here
-    const bool zy = (gj == 0 || gj == g.nyp - 1);                 // dPdy_2 = 0 here
-    const T pxc = zx ? (T)0 : p[1][2] - p[1][0];
-    const T pyc = zy ? (T)0 : p[2][1] - p[0][1];
-    const T qxc = zx ? (T)0 : q[1][2] - q[1][0];
-    const T qyc = zy ? (T)0 : q[2][1] - q[0][1];
-    T A = (T)0, Bv = (T)0, C = (T)0, D = (T)0;
-    if (!zx) {
-        const T pyR = zy ? (T)0 : p[2][2] - p[0][2];
-        const T pyL = zy ? (T)0 : p[2][0] - p[0][0];
-        const T qyR = zy ? (T)0 : q[2][2] - q[0][2];
-        const T qyL = zy ? (T)0 : q[2][0] - q[0][0];
-        A = q[1][2] * pyR - q[1][0] * pyL;
-        D = p[1][2] * qyR - p[1][0] * qyL;
-    }
-    if (!zy) {
-        const T pxU = zx ? (T)0 : p[2][2] - p[2][0];
-        const T pxD = zx ? (T)0 : p[0][2] - p[0][0];
-        const T qxU = zx ? (T)0 : q[2][2] - q[2][0];
-        const T qxD = zx ? (T)0 : q[0][2] - q[0][0];
-        Bv = q[2][1] * pxU - q[0][1] * pxD;
-        C = p[2][1] * qxU - p[0][1] * qxD;
-    }
-    const T t = qxc * pyc - qyc * pxc + A - Bv + C - D;
-    return gjac(g) * t;
 }
 
 // cp.async copy of one element into shared memory; zero-filled when !valid
@@ -446,11 +340,12 @@ k_vort(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par,
         // off the walls, so the wall rules and range tests drop out.
         auto layer = [&](auto inner) {
             constexpr bool I = decltype(inner)::value;
-            const T fx = gfx(g), fy = gfy(g);
+            const T fx = gfx(g), fy = gfy(g), fxb = gfxb(g), fyb = gfyb(g);
             // ---- del2(pm) on rows j0-2.., cols i0-2.. (column tx of L2 = 64)
             {
                 const int gi = i0 - 2 + tx, cs = tx + 2;          // column in the pm tile
                 const bool cv = colok(gi);
+                const bool wl = !g.cyclic && gi == 0, wr = !g.cyclic && gi == nxp - 1;
                 const int rb = ty * R2;
                 const T *col = sPM + rb * LPQ + cs;
                 T sv = col[0], cv_ = col[LPQ];
@@ -463,7 +358,9 @@ k_vort(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par,
                         const int gj = j0 - 2 + r;
                         T v = (T)0;
                         if (I) v = fx * (wv + ev - (T)2 * cv_) + fy * (sv + nv - (T)2 * cv_);
-                        else if (cv && gj >= 0 && gj < nyp) v = lap5(wv, ev, sv, nv, cv_, gi, gj, g);
+                        else if (cv && gj >= 0 && gj < nyp)
+                            v = lap5_sel(wv, ev, sv, nv, cv_, gj == 0 || gj == nyp - 1, wl, wr, gj == 0,
+                                         gj == nyp - 1, fx, fy, fxb, fyb);
                         sD2[r * L2 + tx] = v;
                         sv = cv_;
                         cv_ = nv;
@@ -475,6 +372,7 @@ k_vort(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par,
             if (tx < L1) {
                 const int gi = i0 - 1 + tx, cs = tx + 1;          // column in the d2 tile
                 const bool cv = colok(gi);
+                const bool wl = !g.cyclic && gi == 0, wr = !g.cyclic && gi == nxp - 1;
                 const int rb = ty * R1;
                 const T *col = sD2 + rb * L2 + cs;
                 T sv = col[0], cv_ = col[L2];
@@ -487,7 +385,9 @@ k_vort(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par,
                         const int gj = j0 - 1 + r;
                         T v = (T)0;
                         if (I) v = fx * (wv + ev - (T)2 * cv_) + fy * (sv + nv - (T)2 * cv_);
-                        else if (cv && gj >= 0 && gj < nyp) v = lap5(wv, ev, sv, nv, cv_, gi, gj, g);
+                        else if (cv && gj >= 0 && gj < nyp)
+                            v = lap5_sel(wv, ev, sv, nv, cv_, gj == 0 || gj == nyp - 1, wl, wr, gj == 0,
+                                         gj == nyp - 1, fx, fy, fxb, fyb);
                         sD4[r * L1 + tx] = v;
                         sv = cv_;
                         cv_ = nv;
