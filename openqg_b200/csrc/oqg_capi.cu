@@ -53,12 +53,15 @@ struct oqg_handle {
     int E = 8, KB = 16, xthreads = 128, xi_threads = 64;
     size_t smem_v = 0, smem_x = 0, smem_x64 = 0, smem_y = 0, smem_i = 0, smem_i64 = 0;
     double *stage[2] = {nullptr, nullptr};
+    double *hrow = nullptr;     // contiguous host-order copy buffer [nl][nyp][nxp]
     unsigned long long *d_bad = nullptr;
     double *d_diag = nullptr;
     void *ent_buf = nullptr;
     int par = 0;
     cudaGraphExec_t gexec[2] = {nullptr, nullptr};
     double g_tdt[2] = {0.0, 0.0};
+    cudaGraphExec_t g1exec[2] = {nullptr, nullptr};   // one step, by parity
+    double g1_tdt[2] = {0.0, 0.0};
     std::vector<double> modes_amat, modes_ctl2m, modes_ctm2l, modes_rdm2;
 };
 
@@ -226,6 +229,28 @@ static int download3(oqg_handle *h, const double *src, double *dst, int nlay) {
                          b.nxp * sizeof(double), (size_t)b.nyp * nlay, cudaMemcpyDeviceToHost, h->st));
     return OQG_OK;
 }
+// Host rows -> field: one contiguous copy of nlay layers (faster than a
+// pitched copy), then unpacked on the device into the pitched field of the
+// storage type.
+static int upload_rows(oqg_handle *h, const double *src, void *field, int nlay) {
+    const BasinDev &b = h->hb;
+    const size_t nrows = (size_t)b.nyp * nlay;
+    CK(cudaMemcpyAsync(h->hrow, src, nrows * b.nxp * sizeof(double), cudaMemcpyHostToDevice, h->st));
+    if (h->mixed) k_rows_in<float><<<296, 256, 0, h->st>>>(h->hrow, (float *)field, b.nxp, b.px, nrows);
+    else k_rows_in<double><<<296, 256, 0, h->st>>>(h->hrow, (double *)field, b.nxp, b.px, nrows);
+    CK(cudaGetLastError());
+    return OQG_OK;
+}
+// Field -> host rows: packed on the device, then one contiguous copy.
+static int download_rows(oqg_handle *h, const void *field, double *dst, int nlay) {
+    const BasinDev &b = h->hb;
+    const size_t nrows = (size_t)b.nyp * nlay;
+    if (h->mixed) k_rows_out<float><<<296, 256, 0, h->st>>>((const float *)field, h->hrow, b.nxp, b.px, nrows);
+    else k_rows_out<double><<<296, 256, 0, h->st>>>((const double *)field, h->hrow, b.nxp, b.px, nrows);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(dst, h->hrow, nrows * b.nxp * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+    return OQG_OK;
+}
 // staging FP64 -> field of the storage type
 static void stage_to_field(oqg_handle *h, const double *s, void *f, size_t n) {
     if (h->mixed) k_cvt_in<float><<<296, 256, 0, h->st>>>(s, (float *)f, n);
@@ -243,8 +268,27 @@ static int push_desc(oqg_handle *h) {
 }
 
 static void drop_graphs(oqg_handle *h) {
-    for (int i = 0; i < 2; ++i)
+    for (int i = 0; i < 2; ++i) {
         if (h->gexec[i]) { cudaGraphExecDestroy(h->gexec[i]); h->gexec[i] = nullptr; }
+        if (h->g1exec[i]) { cudaGraphExecDestroy(h->g1exec[i]); h->g1exec[i] = nullptr; }
+    }
+}
+
+// Captures `count` steps starting at parity par into an executable graph.
+static int capture_steps(oqg_handle *h, int par, double tdt, int count, cudaGraphExec_t *out) {
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
+    for (int i = 0; i < count; ++i) launch_step(h, (par + i) & 1, tdt);
+    cudaError_t e1 = cudaGetLastError();
+    cudaError_t e2 = cudaStreamEndCapture(h->st, &g);
+    if (e1 != cudaSuccess || e2 != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        return fail(OQG_ECUDA, std::string("graph capture: ") + cudaGetErrorString(e1 != cudaSuccess ? e1 : e2));
+    }
+    cudaError_t e3 = cudaGraphInstantiate(out, g, 0);
+    cudaGraphDestroy(g);
+    if (e3 != cudaSuccess) return fail(OQG_ECUDA, std::string("graph instantiate: ") + cudaGetErrorString(e3));
+    return OQG_OK;
 }
 
 // Solve (Del^2 - rdm2_m) s_m = f for every mode m with f the (FP64, staging 0)
@@ -686,9 +730,11 @@ int oqg_create(const oqg_params *prm, oqg_handle **out) {
     b.part_col = dalloc<double>(h, (size_t)b.nl * b.nk);
     b.st = dalloc<DevState>(h, 2);
     b.frc = dalloc<DevForcing>(h, 1);
+    b.ent_rows = dalloc<double>(h, b.nyp);
     b.err = dalloc<int>(h, 1);
     h->stage[0] = dalloc<double>(h, n3);
     h->stage[1] = dalloc<double>(h, n3);
+    h->hrow = dalloc<double>(h, (size_t)b.nl * b.nyp * b.nxp);
     h->d_bad = dalloc<unsigned long long>(h, 1);
     h->d_diag = dalloc<double>(h, 4 * (size_t)b.nl);
     if (!b.st || !b.frc || !b.err || !h->stage[1] || !h->d_diag) return bail(OQG_ECUDA, "out of device memory");
@@ -832,8 +878,7 @@ int oqg_get_p_layer(oqg_handle *h, int k, double *out) {
     const BasinDev &b = h->hb;
     const size_t n2 = (size_t)b.nyp * b.px;
     const char *src = (const char *)b.F[h->par] + k * n2 * h->esz;
-    field_to_stage(h, src, h->stage[0], n2);
-    int rc = download3(h, h->stage[0], out, 1);
+    int rc = download_rows(h, src, out, 1);
     if (rc) return rc;
     CK(cudaStreamSynchronize(h->st));
     return OQG_OK;
@@ -864,9 +909,8 @@ int oqg_set_forcing(oqg_handle *h, const double *wekp, const double *ent, double
     BasinDev &b = h->hb;
     const size_t n2 = (size_t)b.nyp * b.px;
     if (wekp) {
-        int rc = upload3(h, wekp, h->stage[0], 1);
+        int rc = upload_rows(h, wekp, const_cast<void *>(b.wekp), 1);
         if (rc) return rc;
-        stage_to_field(h, h->stage[0], const_cast<void *>(b.wekp), n2);
     } else {
         CK(cudaMemsetAsync(const_cast<void *>(b.wekp), 0, n2 * h->esz, h->st));
     }
@@ -876,9 +920,8 @@ int oqg_set_forcing(oqg_handle *h, const double *wekp, const double *ent, double
             h->ent_buf = dalloc<char>(h, (size_t)(b.nl - 1) * n2 * h->esz);
             if (!h->ent_buf) return fail(OQG_ECUDA, "out of device memory");
         }
-        int rc = upload3(h, ent, h->stage[1], b.nl - 1);
+        int rc = upload_rows(h, ent, h->ent_buf, b.nl - 1);
         if (rc) return rc;
-        stage_to_field(h, h->stage[1], h->ent_buf, (size_t)(b.nl - 1) * n2);
         b.ent = h->ent_buf;
     } else {
         b.ent = nullptr;
@@ -887,6 +930,10 @@ int oqg_set_forcing(oqg_handle *h, const double *wekp, const double *ent, double
     if (b.ent != old_ent) {
         int rc = push_desc(h);
         if (rc) return rc;
+    }
+    if (b.ent) {
+        if (h->mixed) k_ent_rows<float><<<b.nyp, 128, 0, h->st>>>(h->d_bas, 0);
+        else k_ent_rows<double><<<b.nyp, 128, 0, h->st>>>(h->d_bas, 0);
     }
     if (h->mixed) k_forcing_integrals<float><<<1, 512, 0, h->st>>>(h->d_bas, 0);
     else k_forcing_integrals<double><<<1, 512, 0, h->st>>>(h->d_bas, 0);
@@ -900,30 +947,27 @@ int oqg_set_forcing(oqg_handle *h, const double *wekp, const double *ent, double
 int oqg_step(oqg_handle *h, double tdt, int nsteps) {
     if (!h || nsteps < 0) return fail(OQG_EINVAL, "bad argument");
     int done = 0;
+    // pairs of steps replay a two-step graph, a remaining step a one-step
+    // graph, each cached per step parity and step length
     if (nsteps >= 2) {
         const int par = h->par;
         if (!h->gexec[par] || h->g_tdt[par] != tdt) {
             if (h->gexec[par]) { cudaGraphExecDestroy(h->gexec[par]); h->gexec[par] = nullptr; }
-            cudaGraph_t g = nullptr;
-            CK(cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
-            launch_step(h, par, tdt);
-            launch_step(h, 1 - par, tdt);
-            cudaError_t e1 = cudaGetLastError();
-            cudaError_t e2 = cudaStreamEndCapture(h->st, &g);
-            if (e1 != cudaSuccess || e2 != cudaSuccess) {
-                if (g) cudaGraphDestroy(g);
-                return fail(OQG_ECUDA, std::string("graph capture: ") +
-                                           cudaGetErrorString(e1 != cudaSuccess ? e1 : e2));
-            }
-            cudaError_t e3 = cudaGraphInstantiate(&h->gexec[par], g, 0);
-            cudaGraphDestroy(g);
-            if (e3 != cudaSuccess) return fail(OQG_ECUDA, std::string("graph instantiate: ") + cudaGetErrorString(e3));
+            int rc = capture_steps(h, par, tdt, 2, &h->gexec[par]);
+            if (rc) return rc;
             h->g_tdt[par] = tdt;
         }
         for (; done + 2 <= nsteps; done += 2) CK(cudaGraphLaunch(h->gexec[par], h->st));
     }
-    for (; done < nsteps; ++done) {
-        launch_step(h, h->par, tdt);
+    if (done < nsteps) {
+        const int par = h->par;
+        if (!h->g1exec[par] || h->g1_tdt[par] != tdt) {
+            if (h->g1exec[par]) { cudaGraphExecDestroy(h->g1exec[par]); h->g1exec[par] = nullptr; }
+            int rc = capture_steps(h, par, tdt, 1, &h->g1exec[par]);
+            if (rc) return rc;
+            h->g1_tdt[par] = tdt;
+        }
+        CK(cudaGraphLaunch(h->g1exec[par], h->st));
         h->par ^= 1;
     }
     CK(cudaGetLastError());

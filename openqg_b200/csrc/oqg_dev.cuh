@@ -95,6 +95,7 @@ struct BasinDev {
     double *part_col;           // [y-solve CTAs]: dst_w-weighted column sums
     DevState *st;               // [2] by step parity
     DevForcing *frc;
+    double *ent_rows;           // [nyp] row sums of the ent area integral
     int *err;                   // device error bits
     // launch bookkeeping
     int k4_rows;                // interior rows per CTA of the assembly launch

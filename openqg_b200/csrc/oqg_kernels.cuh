@@ -1427,6 +1427,25 @@ __global__ void k_cvt_out(const T *src, double *dst, size_t n) {
         dst[i] = (double)src[i];
 }
 
+// Host-order rows (nxp contiguous FP64 values per row) <-> pitched field rows
+// of type T: the unpacking and packing of contiguous host copies.
+template <class T>
+__global__ void k_rows_in(const double *src, T *dst, int nxp, int px, size_t nrows) {
+    const size_t n = nrows * (size_t)nxp;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const size_t r = i / (size_t)nxp, c = i - r * nxp;
+        dst[r * px + c] = (T)src[i];
+    }
+}
+template <class T>
+__global__ void k_rows_out(const T *src, double *dst, int nxp, int px, size_t nrows) {
+    const size_t n = nrows * (size_t)nxp;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const size_t r = i / (size_t)nxp, c = i - r * nxp;
+        dst[i] = (double)src[r * px + c];
+    }
+}
+
 // Trapezoid weight of int_P_dA (numerics.F90:188-204) at (i, j).
 __device__ __forceinline__ double trap_w(const BasinDev &b, int i, int j) {
     double w = 1.0;
@@ -1515,9 +1534,22 @@ __global__ void k_init_constraints(const BasinDev *__restrict__ bas, int member,
     }
 }
 
+// Row sums of the ent area integral (int_P_dA, numerics.F90:165-204): one
+// CTA per row j writes sum_i trap_x(i) ent(i, j, 1) to ent_rows[j].
+template <class T>
+__global__ void __launch_bounds__(128) k_ent_rows(const BasinDev *__restrict__ bas, int member) {
+    const BasinDev &b = bas[member];
+    __shared__ double red[32];
+    const T *E = (const T *)b.ent + (size_t)blockIdx.x * b.px;
+    double s = 0.0;
+    for (int i = threadIdx.x; i < b.nxp; i += blockDim.x) s += trap_x(b, i) * (double)E[i];
+    s = block_sum(s, red);
+    if (threadIdx.x == 0) b.ent_rows[blockIdx.x] = s;
+}
+
 // Forcing integrals that depend only on ent: ent_xn = int_P_dA(ent(:,:,1))
-// (pressure.F90:52-54) and the channel strip integrals int_Be_s/n
-// (vorticity.F90:122-128).  One CTA.
+// (pressure.F90:52-54) from the row sums of k_ent_rows, in a fixed order,
+// and the channel strip integrals int_Be_s/n (vorticity.F90:122-128).  One CTA.
 template <class T>
 __global__ void k_forcing_integrals(const BasinDev *__restrict__ bas, int member) {
     const BasinDev &b = bas[member];
@@ -1527,7 +1559,10 @@ __global__ void k_forcing_integrals(const BasinDev *__restrict__ bas, int member
     const size_t n2 = (size_t)b.nyp * b.px;
     double exn = 0.0, s1 = 0.0, s2 = 0.0, n1 = 0.0, n2v = 0.0;
     if (E) {
-        exn = area_integral(b, E, red);
+        double s = 0.0;
+        for (int j = threadIdx.x; j < b.nyp; j += blockDim.x)
+            s += ((j == 0 || j == b.nyp - 1) ? 0.5 : 1.0) * b.ent_rows[j];
+        exn = block_sum(s, red) * b.dx * b.dy;
         if (b.cyclic) {
             s1 = row_integral(b, E, 0, -1, red);
             n1 = row_integral(b, E, b.nyp - 1, -1, red);
