@@ -51,6 +51,8 @@ WORKLOADS = {
                     "atmosphere channel 193x97x3, dx 80 km (coupled config atmosphere)"),
     "ocean1025": (dict(kind="box", n=1025, dx=10e3), 3600.0,
                   "ocean double gyre 1025x1025x3 box, dx 10 km"),
+    "ocean2049": (dict(kind="box", n=2049, dx=5e3, ah4=1e9), 1200.0,
+                  "eddy-resolving ocean 2049x2049x3 box, dx 5 km, ah4 1e9, dt 600 s"),
 }
 
 
@@ -58,7 +60,7 @@ def make_basin(name, precision):
     from openqg_b200.params import atmos_channel, ocean_double_gyre
     kw, tdt, label = WORKLOADS[name]
     if kw["kind"] == "box":
-        b = ocean_double_gyre(kw["n"], dx=kw["dx"], precision=precision)
+        b = ocean_double_gyre(kw["n"], dx=kw["dx"], ah4=kw.get("ah4", 2.0e10), precision=precision)
     else:
         b = atmos_channel(kw["nxp"], kw["nyp"], dx=kw["dx"], precision=precision)
     return b, tdt, label

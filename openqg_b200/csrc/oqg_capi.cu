@@ -86,10 +86,12 @@ static int xinv_fft_threads(int M, int nl) {
     int nfft = std::min(XINV_FFT_MAX, rup(nl * tt, 32));
     return std::max(nfft, rup(tt, 32));
 }
-// Dynamic shared bytes of k_xinv for nfft transform threads (element size esz).
-static size_t xinv_smem(int M, int nl, int nra, int nxp, int nfft, size_t esz) {
+// Dynamic shared bytes of k_xinv for nfft transform threads (element size
+// esz); split: the modal rows live in global memory instead.
+static size_t xinv_smem(int M, int nl, int nra, int nxp, int nfft, size_t esz, bool split = false) {
     const int tt = (M + XINV_E - 1) / XINV_E, G = nfft / tt;
     const size_t set = (size_t)G * fft_buf_len(M) * 2 * esz;
+    if (split) return 2 * set;
     const size_t inh = (size_t)nl * nra * nxp * esz;
     return G >= nl ? std::max(2 * set, set + inh) : 2 * set + inh;
 }
@@ -766,10 +768,24 @@ int oqg_create(const oqg_params *prm, oqg_handle **out) {
     h->smem_y = (size_t)LDy * h->KB * (vsz + 8);
     // rows of an assembly CTA: k4_rows interior rows plus at most one wall row
     const int nra = (b.ny > b.k4_rows) ? b.k4_rows + 1 : b.ny + 2;
-    const int nfft_i = xinv_fft_threads(b.M, b.nl);
+    int nfft_i = xinv_fft_threads(b.M, b.nl);
+    bool split = false;
+    b.inh_g = nullptr;
+    if (xinv_smem(b.M, b.nl, nra, b.nxp, nfft_i, 8) > 227 * 1024) {
+        // wide grid: the modal rows go to a global buffer, and a round holds
+        // as many FP64 transforms as shared memory does
+        split = true;
+        const int tt = (b.M + XINV_E - 1) / XINV_E;
+        const size_t per = 2 * (size_t)fft_buf_len(b.M) * 16;
+        const int G = std::max(1, std::min(b.nl, (int)((227 * 1024) / per)));
+        nfft_i = std::min(XINV_FFT_MAX, rup(G * tt, 32));
+        if ((nfft_i / tt) * per > 227 * 1024) nfft_i = rup(tt, 32);
+        b.inh_g = dalloc<char>(h, (size_t)b.nl * b.nyp * b.px * 8);
+        if (!b.inh_g) return bail(OQG_ECUDA, "out of device memory");
+    }
     h->xi_threads = nfft_i + 32;
-    h->smem_i = xinv_smem(b.M, b.nl, nra, b.nxp, nfft_i, h->esz);
-    h->smem_i64 = xinv_smem(b.M, b.nl, nra, b.nxp, nfft_i, 8);
+    h->smem_i = xinv_smem(b.M, b.nl, nra, b.nxp, nfft_i, h->esz, split);
+    h->smem_i64 = xinv_smem(b.M, b.nl, nra, b.nxp, nfft_i, 8, split);
     if (h->smem_i64 > 227 * 1024 || h->smem_x64 > 227 * 1024 || h->smem_y > 227 * 1024)
         return bail(OQG_EUNSUPPORTED, "grid too large for this build's shared-memory tiling");
     std::vector<Work> wv(h->nv), wx(h->nx), wy(h->nys), wi(h->ni);
@@ -1290,7 +1306,7 @@ int oqg_ensemble_create(const oqg_params *members, int nmembers, oqg_ensemble **
         e->smem_v = std::max(e->smem_v, vort_smem_bytes(b.vty, (int)esz));
         e->smem_x = std::max(e->smem_x, (size_t)G * 2 * LB * t2);
         e->smem_y = std::max(e->smem_y, (size_t)((b.ny + 32) | 1) * 4 * (vsz + 8));
-        e->smem_i = std::max(e->smem_i, xinv_smem(b.M, b.nl, nra, b.nxp, nfft_e, esz));
+        e->smem_i = std::max(e->smem_i, xinv_smem(b.M, b.nl, nra, b.nxp, nfft_e, esz, b.inh_g != nullptr));
     }
     if (e->smem_x > 227 * 1024 || e->smem_i > 227 * 1024 || e->smem_v > 227 * 1024) {
         ens_free(e);

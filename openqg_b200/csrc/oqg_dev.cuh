@@ -96,6 +96,7 @@ struct BasinDev {
     DevState *st;               // [2] by step parity
     DevForcing *frc;
     double *ent_rows;           // [nyp] row sums of the ent area integral
+    void *inh_g;                // wide grids: modal rows of k_xinv, [nl][nyp][px] (8-byte slots)
     int *err;                   // device error bits
     // launch bookkeeping
     int k4_rows;                // interior rows per CTA of the assembly launch

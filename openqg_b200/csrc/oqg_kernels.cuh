@@ -1143,9 +1143,20 @@ k_xinv(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par,
     // makes its last stage end in set A, and its spectral rows are staged in
     // the other.  With every row pair in one round the modal rows inh alias
     // set B once the transforms are done; otherwise they follow both sets.
+    // Grids too wide for the modal rows in shared memory keep them in the
+    // global buffer b.inh_g ([nl][nyp][px], rows of this CTA only).
     T2 *setA = reinterpret_cast<T2 *>(smem_raw), *setB = setA + (size_t)G * LB;
     T2 *set_in = (b.nrad & 1) ? setB : setA, *set_st = (b.nrad & 1) ? setA : setB;
-    T *inh = one_round ? reinterpret_cast<T *>(setB) : reinterpret_cast<T *>(setA + (size_t)2 * G * LB);
+    const bool split = b.inh_g != nullptr;
+    const bool alias = one_round && !split;
+    T *inh;
+    size_t ms, rs;                               // mode and row strides of inh
+    if (split) { inh = (T *)b.inh_g + (size_t)jfirst * px; ms = (size_t)nyp * px; rs = px; }
+    else {
+        inh = alias ? reinterpret_cast<T *>(setB) : reinterpret_cast<T *>(setA + (size_t)2 * G * LB);
+        ms = (size_t)nra * nxp;
+        rs = nxp;
+    }
     const T ftn = (T)b.ftnorm;
 
     pdl_trigger();
@@ -1154,8 +1165,10 @@ k_xinv(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par,
         if (!out) scalar_phase<T, NL>(b, tdt != 0.0 ? tdt : b.tdt_m, par, w.block == 0, &sS);
     } else {
     // zero the wall rows / columns of the modal fields
-    if (!one_round)
-        for (int idx = threadIdx.x; idx < NL * nra * nxp; idx += nfft) inh[idx] = (T)0;
+    if (!alias)
+        for (int m = 0; m < NL; ++m)
+            for (int lr = 0; lr < nra; ++lr)
+                for (int i = threadIdx.x; i < nxp; i += nfft) inh[m * ms + lr * rs + i] = (T)0;
     pdl_wait();
 
     // a row of the spectral buffer: n reals (box) or nk complex (channel)
@@ -1209,15 +1222,15 @@ k_xinv(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par,
         }
         bar_sync(1, nfft);
         T2 *z = fft_smem<T>(za, zb, M, b.rad, b.nrad, (const T2 *)b.tw, live ? t : TT, TT, 1, nfft);
-        if (one_round) {
+        if (alias) {
             // set B is free now: clear it for the modal rows
             for (int idx = threadIdx.x; idx < NL * nra * nxp; idx += nfft) inh[idx] = (T)0;
             bar_sync(1, nfft);
         }
         if (live) {
             const int lr = (jlo + r0) - jfirst;
-            T *ox = inh + ((size_t)m * nra + lr) * nxp;
-            T *oy = ox + nxp;
+            T *ox = inh + m * ms + lr * rs;
+            T *oy = ox + rs;
             if (!b.cyclic) {
                 for (int kk = t; kk < n; kk += TT) {
                     const T2 v = z[fpad(kk + 1)];
@@ -1246,7 +1259,7 @@ k_xinv(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par,
         for (int idx = threadIdx.x; idx < NL * nra * nxp; idx += blockDim.x) {
             const int m = idx / (nra * nxp), rem = idx - m * nra * nxp;
             const int lr = rem / nxp, i = rem - lr * nxp;
-            out[((size_t)m * nyp + jfirst + lr) * px + i] = (double)inh[idx];
+            out[((size_t)m * nyp + jfirst + lr) * px + i] = (double)inh[m * ms + lr * rs + i];
         }
         return;
     }
@@ -1293,7 +1306,7 @@ k_xinv(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par,
             const int lr = lrs[u], i = is[u], j = jfirst + lr;
             double pm_[NL];
 #pragma unroll
-            for (int m = 0; m < NL; ++m) pm_[m] = (double)inh[((size_t)m * nra + lr) * nxp + i];
+            for (int m = 0; m < NL; ++m) pm_[m] = (double)inh[m * ms + lr * rs + i];
             if (!b.cyclic) {
 #pragma unroll
                 for (int m = 1; m < NL; ++m) pm_[m] = pm_[m] + hc[m - 1] * hv[u][m];
@@ -1309,7 +1322,7 @@ k_xinv(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par,
 #pragma unroll
                 for (int m = 0; m < NL; ++m) s2 += pm_[m] * ctm[m + NL * k];
                 const T pn = (T)s2;
-                inh[((size_t)k * nra + lr) * nxp + i] = pn;
+                inh[k * ms + lr * rs + i] = pn;
                 Pnew[k * n2 + (size_t)j * px + i] = supp ? (T)((T)0.5 * (pn + (T)po[u][k])) : pn;
             }
         }
@@ -1335,7 +1348,7 @@ k_xinv(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par,
             continue;
         }
         const int cnt = (zon ? 1 : 0) + (mer ? 1 : 0);
-#define PN(kk, rr, ii) inh[((size_t)(kk) * nra + (rr)) * nxp + (ii)]
+#define PN(kk, rr, ii) inh[(kk) * ms + (rr) * rs + (ii)]
         T pv[NL];
 #pragma unroll
         for (int k = 0; k < NL; ++k) pv[k] = PN(k, lr, i);
