@@ -753,7 +753,7 @@ int oqg_create(const oqg_params *prm, oqg_handle **out) {
     h->xthreads = GX * TT;
     h->nx = (b.nl * npm + GX - 1) / GX;
     const size_t vsz = (size_t)(b.cyclic ? 16 : 8);
-    // y-solve: 4 columns (warps) per CTA; tile + pivots, padded columns
+    // y-solve: 4 columns (warps) per CTA; the padded column tile (pivots come through L1)
     h->KB = 4;
     const int S_ = (b.ny + 31) / 32;
     const int LDy = (b.ny + 32) | 1;
@@ -765,7 +765,7 @@ int oqg_create(const oqg_params *prm, oqg_handle **out) {
     const int LB = fft_buf_len(b.M);
     h->smem_x = (size_t)GX * 2 * LB * t2;
     h->smem_x64 = (size_t)GX * 2 * LB * 16;
-    h->smem_y = (size_t)LDy * h->KB * (vsz + 8);
+    h->smem_y = (size_t)LDy * h->KB * vsz;
     // rows of an assembly CTA: k4_rows interior rows plus at most one wall row
     const int nra = (b.ny > b.k4_rows) ? b.k4_rows + 1 : b.ny + 2;
     int nfft_i = xinv_fft_threads(b.M, b.nl);
@@ -1305,7 +1305,7 @@ int oqg_ensemble_create(const oqg_params *members, int nmembers, oqg_ensemble **
         const int nra = (b.ny > b.k4_rows) ? b.k4_rows + 1 : b.ny + 2;
         e->smem_v = std::max(e->smem_v, vort_smem_bytes(b.vty, (int)esz));
         e->smem_x = std::max(e->smem_x, (size_t)G * 2 * LB * t2);
-        e->smem_y = std::max(e->smem_y, (size_t)((b.ny + 32) | 1) * 4 * (vsz + 8));
+        e->smem_y = std::max(e->smem_y, (size_t)((b.ny + 32) | 1) * 4 * vsz);
         e->smem_i = std::max(e->smem_i, xinv_smem(b.M, b.nl, nra, b.nxp, nfft_e, esz, b.inh_g != nullptr));
     }
     if (e->smem_x > 227 * 1024 || e->smem_i > 227 * 1024 || e->smem_v > 227 * 1024) {

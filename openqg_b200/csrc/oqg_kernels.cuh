@@ -653,18 +653,19 @@ __device__ __forceinline__ double yt_re(double2 v) { return v.x; }
 // The column solve of one warp with each lane's rows [s, s+n) (n <= SM)
 // held in registers through all four passes: forward elimination as an
 // affine scan (chunk pass, warp scan of the chunk maps, chunk pass), then back
-// substitution the same way from the bottom.  col/pc: the column and its
-// pivots in shared memory at padded offset o.
+// substitution the same way from the bottom.  col: the column in shared
+// memory at padded offset o; piv: its pivots (global, plen stored).
 #define YREG 16
 template <class V, int SM>
-__device__ __forceinline__ void ysolve_chunk_regs(V *col, const double *pc, double a, int lane, int s, int n,
+__device__ __forceinline__ void ysolve_chunk_regs(V *col, const double *__restrict__ piv, int plen, double a,
+                                                  int lane, int s, int n,
                                                   int o, int ny, double &colsum) {
     V x[SM];
     double bt[SM];
 #pragma unroll
     for (int t = 0; t < SM; ++t) {
         x[t] = t < n ? col[o + t] : yt_zero(V());
-        bt[t] = t < n ? pc[o + t] : 0.0;
+        bt[t] = t < n ? __ldg(piv + min(s + t, plen - 1)) : 0.0;
     }
     // forward elimination: u_j = f_j beta_j - a beta_j u_{j-1}
     V C = yt_zero(V());
@@ -739,29 +740,13 @@ k_ysolve(const BasinDev *__restrict__ bas, const Work *__restrict__ work) {
     const FastDiv fdS(S_);
     extern __shared__ __align__(16) unsigned char smem_raw[];
     V *tile = reinterpret_cast<V *>(smem_raw);                 // [KB][LD]
-    double *pvs = reinterpret_cast<double *>(tile + KB * LD);  // [KB][LD] pivots
     const int k = k0 + c;
     const bool live = k < nk;
     const int pidx = m * nk + (live ? k : 0);
-    // this warp's pivots (constant data), 16 loads in flight per lane; beyond
-    // the stored length a pivot repeats its fixed point
-    {
-        const double *piv = b.piv_tab + b.piv_off[pidx];
-        const int plen = b.piv_len[pidx];
-        for (int j0 = lane; j0 < ny; j0 += 32 * CH) {
-            double v[CH];
-#pragma unroll
-            for (int u = 0; u < CH; ++u) {
-                const int jj = j0 + 32 * u;
-                v[u] = jj < ny ? piv[min(jj, plen - 1)] : 0.0;
-            }
-#pragma unroll
-            for (int u = 0; u < CH; ++u) {
-                const int jj = j0 + 32 * u;
-                if (jj < ny) pvs[c * LD + jj + fdS.div(jj)] = v[u];
-            }
-        }
-    }
+    // this warp's pivots (constant data, read through L1); beyond the stored
+    // length a pivot repeats its fixed point
+    const double *__restrict__ piv = b.piv_tab + b.piv_off[pidx];
+    const int plen = b.piv_len[pidx];
     Gm *S = (Gm *)b.spec + (size_t)m * ny * pk;
     pdl_trigger();
     pdl_wait();
@@ -787,19 +772,18 @@ k_ysolve(const BasinDev *__restrict__ bas, const Work *__restrict__ work) {
     if (live) {
         const double a = b.a_tri;
         V *col = tile + c * LD;
-        const double *pc = pvs + c * LD;
         const int s = lane * S_, e = min(s + S_, ny);
         const int o = lane * (S_ + 1);          // padded offset of row s
         const int n = max(e - s, 0);
         double colsum = 0.0;
-        if (S_ <= YREG) ysolve_chunk_regs<V, YREG>(col, pc, a, lane, s, n, o, ny, colsum);
+        if (S_ <= YREG) ysolve_chunk_regs<V, YREG>(col, piv, plen, a, lane, s, n, o, ny, colsum);
         else {
             // forward elimination: u_j = f_j beta_j - a beta_j u_{j-1}
             V C = yt_zero(V());
             double D = 1.0;
 #pragma unroll 8
             for (int t = 0; t < n; ++t) {
-                const double bt = pc[o + t];
+                const double bt = __ldg(piv + min(s + t, plen - 1));
                 C = yt_axpy(yt_scale(col[o + t], bt), -a * bt, C);
                 D = -a * bt * D;
             }
@@ -812,7 +796,7 @@ k_ysolve(const BasinDev *__restrict__ bas, const Work *__restrict__ work) {
             if (lane == 0) uu = yt_zero(V());
 #pragma unroll 8
             for (int t = 0; t < n; ++t) {
-                const double bt = pc[o + t];
+                const double bt = __ldg(piv + min(s + t, plen - 1));
                 uu = yt_axpy(yt_scale(col[o + t], bt), -a * bt, uu);
                 col[o + t] = uu;
             }
@@ -821,7 +805,7 @@ k_ysolve(const BasinDev *__restrict__ bas, const Work *__restrict__ work) {
             D = 1.0;
 #pragma unroll 8
             for (int t = n - 1; t >= 0; --t) {
-                const double ej = (s + t == ny - 1) ? 0.0 : -a * pc[o + t];
+                const double ej = (s + t == ny - 1) ? 0.0 : -a * __ldg(piv + min(s + t, plen - 1));
                 C = yt_axpy(col[o + t], ej, C);
                 D = ej * D;
             }
@@ -834,7 +818,7 @@ k_ysolve(const BasinDev *__restrict__ bas, const Work *__restrict__ work) {
             if (lane == 31) uu = yt_zero(V());
 #pragma unroll 8
             for (int t = n - 1; t >= 0; --t) {
-                const double ej = (s + t == ny - 1) ? 0.0 : -a * pc[o + t];
+                const double ej = (s + t == ny - 1) ? 0.0 : -a * __ldg(piv + min(s + t, plen - 1));
                 uu = yt_axpy(col[o + t], ej, uu);
                 col[o + t] = uu;
                 colsum += yt_re(uu);
