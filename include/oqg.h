@@ -23,6 +23,7 @@
  *   solve_inhomog_eqn / generate_homog_soln         src/qg/inhomog.F90:146-168
  *   ekman_from_tau                                  src/coupler/ekman.F90:53-83
  *   qg_diagno (ekei, sfmin, sfmax, circ)            src/diagnostics/qg_monitor.F90:289-376
+ *   qg_diagno (the full monitor record)             src/diagnostics/qg_monitor.F90:219-383
  */
 #ifndef OQG_H
 #define OQG_H
@@ -172,6 +173,37 @@ int oqg_diag(oqg_handle *h, double *ekei, double *sfmin, double *sfmax,
  * callers must serialise them. */
 int oqg_diag_noalloc(oqg_handle *h, double *ekei, double *sfmin, double *sfmax,
                      double *circ);
+
+/* The monitor record of qg_diagno (qg_monitor.F90:219-383): forcing means,
+ * interface displacement, energetics, jet, transports and stream-function
+ * extrema; arrays of length nl (nl-1 for the interface quantities).  tsec and
+ * et2m carry state from one call to the next (pket is the rate of change of
+ * the interface potential energy since the previous call), as in the
+ * reference's qg_monitor_type. */
+typedef struct oqg_qg_monitor {
+    double tsec;                       /* time of the previous call (s)         */
+    double wepm, wapm;                 /* mean Ekman pumping, mean |pumping|    */
+    double entm, enam;                 /* mean entrainment, mean |entrainment|  */
+    double etam[OQG_MAX_NL], et2m[OQG_MAX_NL], pket[OQG_MAX_NL];
+    double pken;                       /* rho gp1 <eta1 ent1>                   */
+    double utau;                       /* wind work rho int(tau . u_geo)        */
+    double pavg[OQG_MAX_NL], qavg[OQG_MAX_NL];
+    double ah2d[OQG_MAX_NL], ah4d[OQG_MAX_NL];   /* viscous dissipation        */
+    double ekei[OQG_MAX_NL];                     /* layer kinetic energy       */
+    double val[OQG_MAX_NL];                      /* jet strength               */
+    int    pos[OQG_MAX_NL];                      /* jet row (1-based)          */
+    double circ[OQG_MAX_NL], ctot;               /* circulation (Sv)           */
+    double btdg;                                 /* bottom Ekman drag          */
+    double sfmin[OQG_MAX_NL], sfmax[OQG_MAX_NL]; /* stream-function extrema    */
+    double ermas[OQG_MAX_NL], emfr[OQG_MAX_NL];  /* channel continuity check   */
+} oqg_qg_monitor;
+
+/* qg_diagno (qg_monitor.F90:219-383) on the device from the current state
+ * and forcing: taux, tauy (nxp, nyp) are the wind stress the Ekman pumping
+ * came from (NULL: utau = 0); tsec the model time; tdt the leapfrog step (for
+ * the channel continuity check).  mon is read (tsec, et2m) and written. */
+int oqg_diagno(oqg_handle *h, const double *taux, const double *tauy, double tsec,
+               double tdt, oqg_qg_monitor *mon);
 
 /* solve_inhomog_eqn (inhomog.F90:156-168): (Del^2 - rdm2(m)) out = rhs with
  * out = 0 on solid boundaries; m is the 1-based mode; rhs, out (nxp, nyp). */

@@ -20,7 +20,7 @@ from typing import Optional
 
 import numpy as np
 
-from .params import Basin, STATUS
+from .params import Basin, QgMonitor, STATUS
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "liboqg.so")
@@ -61,6 +61,7 @@ def lib():
     L.oqg_check_finite.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
     L.oqg_diag.argtypes = [vp, _dp, _dp, _dp, _dp]
     L.oqg_diag_noalloc.argtypes = [vp, _dp, _dp, _dp, _dp]
+    L.oqg_diagno.argtypes = [vp, _dp, _dp, ctypes.c_double, ctypes.c_double, ctypes.POINTER(QgMonitor)]
     L.oqg_solve_inhomog.argtypes = [vp, ctypes.c_int, _dp, _dp]
     L.oqg_generate_homog_soln.argtypes = [vp, ctypes.c_int, _dp, _dp]
     L.oqg_get_modes.argtypes = [vp, _dp, _dp, _dp, _dp]
@@ -206,6 +207,15 @@ class QG:
         e, smin, smax, c = (np.empty(nl) for _ in range(4))
         _check(lib().oqg_diag(self.h, _p(e), _p(smin), _p(smax), _p(c)), "oqg_diag")
         return dict(ekei=e, sfmin=smin, sfmax=smax, circ=c)
+
+    def diagno(self, taux=None, tauy=None, tsec=0.0, tdt=0.0, mon: Optional[QgMonitor] = None):
+        """qg_diagno (qg_monitor.F90:219-383) on the device.  mon carries the
+        time-rate state between calls; returns (dict of the record, mon)."""
+        mon = mon if mon is not None else QgMonitor()
+        tx = _f64(taux, self.b.shape2)
+        ty = _f64(tauy, self.b.shape2)
+        _check(lib().oqg_diagno(self.h, _p(tx), _p(ty), float(tsec), float(tdt), ctypes.byref(mon)), "oqg_diagno")
+        return mon.as_dict(self.b.nl), mon
 
     def diag_noalloc(self):
         """diag() through oqg_diag_noalloc: scratch in the library's fixed

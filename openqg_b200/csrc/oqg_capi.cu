@@ -54,6 +54,7 @@ struct oqg_handle {
     size_t smem_v = 0, smem_x = 0, smem_x64 = 0, smem_y = 0, smem_i = 0, smem_i64 = 0;
     double *stage[2] = {nullptr, nullptr};
     double *hrow = nullptr;     // contiguous host-order copy buffer [nl][nyp][nxp]
+    double *dg = nullptr;       // qg_diagno scratch, made on its first call
     unsigned long long *d_bad = nullptr;
     double *d_diag = nullptr;
     void *ent_buf = nullptr;
@@ -1046,6 +1047,114 @@ int oqg_diag(oqg_handle *h, double *ekei, double *sfmin, double *sfmax, double *
         if (sfmin) sfmin[k] = o[4 * k + 1];
         if (sfmax) sfmax[k] = o[4 * k + 2];
         if (circ) circ[k] = o[4 * k + 3];
+    }
+    return OQG_OK;
+}
+
+int oqg_diagno(oqg_handle *h, const double *taux, const double *tauy, double tsec, double tdt,
+               oqg_qg_monitor *mon) {
+    if (!h || !mon) return fail(OQG_EINVAL, "bad argument");
+    const BasinDev &b = h->hb;
+    const int nl = b.nl, nyp = b.nyp, nxp = b.nxp;
+    const size_t n2 = (size_t)nyp * b.px, n3 = n2 * nl;
+    const size_t nrow = (size_t)OQG_DGQ * nl * nyp;
+    if (!h->dg) {
+        h->dg = dalloc<double>(h, 8 * n3 + 2 * n2 + nrow);
+        if (!h->dg) return fail(OQG_ECUDA, "out of device memory");
+    }
+    double *V = h->dg, *tau = h->dg + 8 * n3, *R = tau + 2 * n2;
+    const bool have_tau = taux && tauy;
+    if (have_tau) {
+        int rc = upload3(h, taux, tau, 1);
+        if (!rc) rc = upload3(h, tauy, tau + n2, 1);
+        if (rc) return rc;
+    }
+    if (h->mixed) k_dg_vel<float><<<296, 256, 0, h->st>>>(h->d_bas, 0, h->par, V);
+    else k_dg_vel<double><<<296, 256, 0, h->st>>>(h->d_bas, 0, h->par, V);
+    // del2 of ug, vg into slots 4 and 6, then del4 into 5 and 7
+    k_dg_del2<<<296, 256, 0, h->st>>>(h->d_bas, 0, V, V + 4 * n3, 1);
+    k_dg_del2<<<296, 256, 0, h->st>>>(h->d_bas, 0, V + n3, V + 6 * n3, 1);
+    k_dg_del2<<<296, 256, 0, h->st>>>(h->d_bas, 0, V + 4 * n3, V + 5 * n3, 1);
+    k_dg_del2<<<296, 256, 0, h->st>>>(h->d_bas, 0, V + 6 * n3, V + 7 * n3, 1);
+    const dim3 grid((unsigned)nyp, (unsigned)nl);
+    if (h->mixed) k_dg_rows<float><<<grid, 128, 0, h->st>>>(h->d_bas, 0, h->par, V, have_tau ? tau : nullptr, R);
+    else k_dg_rows<double><<<grid, 128, 0, h->st>>>(h->d_bas, 0, h->par, V, have_tau ? tau : nullptr, R);
+    CK(cudaGetLastError());
+    std::vector<double> r(nrow);
+    CK(cudaMemcpyAsync(r.data(), R, nrow * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+    DevState stt;
+    CK(cudaMemcpyAsync(&stt, b.st + h->par, sizeof stt, cudaMemcpyDeviceToHost, h->st));
+    // p at the two west corners, for circ and the reference pressure
+    std::vector<double> corner(2 * nl);
+    for (int k = 0; k < nl; ++k) {
+        field_to_stage(h, (const char *)b.F[h->par] + k * n2 * h->esz, h->stage[0] + k * n2, n2);
+    }
+    for (int k = 0; k < nl; ++k) {
+        CK(cudaMemcpyAsync(&corner[2 * k], h->stage[0] + k * n2, sizeof(double), cudaMemcpyDeviceToHost, h->st));
+        CK(cudaMemcpyAsync(&corner[2 * k + 1], h->stage[0] + k * n2 + (size_t)(nyp - 1) * b.px, sizeof(double),
+                           cudaMemcpyDeviceToHost, h->st));
+    }
+    CK(cudaStreamSynchronize(h->st));
+    const oqg_params &P = h->prm;
+    const double dx = b.dx, dy = b.dy, xl = (nxp - 1) * dx, yl = (nyp - 1) * dy, area = xl * yl;
+    // int_P_dA of integrand q, layer k: rows in order with the y trapezoid weights
+    auto I = [&](int q, int k) {
+        double s = 0.0;
+        const double *row = &r[((size_t)q * nl + k) * nyp];
+        for (int j = 0; j < nyp; ++j) s += ((j == 0 || j == nyp - 1) ? 0.5 : 1.0) * row[j];
+        return s * dx * dy;
+    };
+    mon->wepm = I(14, 0) / area;
+    mon->wapm = I(15, 0) / area;
+    mon->entm = I(16, 0) / area;
+    mon->enam = I(17, 0) / area;
+    const double tprev = mon->tsec;
+    for (int k = 0; k < nl - 1; ++k) {
+        mon->etam[k] = I(11, k) / area;
+        const double et2now = I(12, k) / area;
+        mon->pket[k] = tsec > tprev ? 0.5 * P.rho * P.gp[k] * (et2now - mon->et2m[k]) / (tsec - tprev) : 0.0;
+        mon->et2m[k] = et2now;
+    }
+    mon->pken = nl > 1 ? P.rho * P.gp[0] * I(13, 0) / area : 0.0;
+    mon->tsec = tsec;
+    mon->utau = have_tau ? P.rho * (I(19, 0) + I(18, 0)) : 0.0;
+    mon->ctot = 0.0;
+    for (int k = 0; k < nl; ++k) {
+        mon->pavg[k] = I(0, k) / area;
+        mon->qavg[k] = I(1, k) / area;
+        mon->ah2d[k] = -P.rho * P.ah2[k] * P.h[k] * (I(2, k) + I(3, k));
+        mon->ah4d[k] = P.rho * P.ah4[k] * P.h[k] * (I(4, k) + I(5, k));
+        mon->ekei[k] = 0.5 * P.rho * P.h[k] * (I(6, k) + I(7, k));
+        // jet: |int_P_dx u| / xl per row, over the first nyp-1 rows
+        const double *ru = &r[((size_t)8 * nl + k) * nyp];
+        int jm = 0;
+        for (int j = 1; j < nyp - 1; ++j)
+            if (std::fabs(ru[j] * dx) / xl > std::fabs(ru[jm] * dx) / xl) jm = j;
+        mon->pos[k] = jm + 1;
+        mon->val[k] = std::fabs(ru[jm] * dx) / xl;
+        const double p00 = corner[2 * k], p0n = corner[2 * k + 1];
+        mon->circ[k] = 1.0e-6 * ((p00 - p0n) / P.fnot);
+        mon->ctot += mon->circ[k];
+        double pomin = 1e308, pomax = -1e308;
+        for (int j = 0; j < nyp; ++j) {
+            pomin = std::min(pomin, r[((size_t)20 * nl + k) * nyp + j]);
+            pomax = std::max(pomax, r[((size_t)21 * nl + k) * nyp + j]);
+        }
+        const double poref = P.fnot > 0 ? p00 : p0n;
+        const double e1 = std::min(pomin / P.fnot, pomax / P.fnot), e2 = std::max(pomin / P.fnot, pomax / P.fnot);
+        mon->sfmin[k] = 1.0e-6 * (P.h[k] * (e1 - poref / P.fnot));
+        mon->sfmax[k] = 1.0e-6 * (P.h[k] * (e2 - poref / P.fnot));
+    }
+    const int kt = P.k_topo - 1;
+    mon->btdg = 0.5 * P.rho * P.delek * std::fabs(P.fnot) * (I(9, kt) + I(10, kt));
+    for (int k = 0; k < OQG_MAX_NL; ++k) { mon->ermas[k] = 0.0; mon->emfr[k] = 0.0; }
+    if (b.cyclic) {
+        for (int k = 0; k < nl - 1; ++k) {
+            const double est1 = P.dz_sign * (I(0, k) - I(0, k + 1)), est2 = stt.dpi[k];
+            const double edif = est1 - est2, esum = std::fabs(est1) + std::fabs(est2);
+            mon->ermas[k] = edif;
+            mon->emfr[k] = esum > 1.0e-13 * xl * yl * tdt * P.gp[k] ? 2.0 * edif / esum : 0.0;
+        }
     }
     return OQG_OK;
 }

@@ -1691,4 +1691,136 @@ __global__ void k_diag(const BasinDev *__restrict__ bas, int member, int par, do
     }
 }
 
+// ------------------------------------------------------------------ qg_diagno
+// The monitor record of qg_diagno (qg_monitor.F90:219-383) on the device:
+// velocity fields, their wall Laplacians, then per-row sums of every
+// integrand; the host adds the rows in a fixed order.
+
+// dPdx_2bc / dPdy_2bc (numerics.F90:470-513) of layer field P at (i, j).
+template <class T>
+__device__ __forceinline__ void dpdxy_bc(const T *P, const BasinDev &b, int i, int j, double &dpx, double &dpy) {
+    const int nxp = b.nxp, nyp = b.nyp, px = b.px;
+    const double ah = b.bc_half1;
+    const double pv = (double)P[(size_t)j * px + i];
+    if (j == 0 || j == nyp - 1) dpx = 0.0;
+    else if (b.cyclic && (i == 0 || i == nxp - 1))
+        dpx = ((double)P[(size_t)j * px + 1] - (double)P[(size_t)j * px + nxp - 2]) / (2.0 * b.dx);
+    else if (i == 0) dpx = ((double)P[(size_t)j * px + 1] - pv) / (b.dx * ah);
+    else if (i == nxp - 1) dpx = (pv - (double)P[(size_t)j * px + i - 1]) / (b.dx * ah);
+    else dpx = ((double)P[(size_t)j * px + i + 1] - (double)P[(size_t)j * px + i - 1]) / (2.0 * b.dx);
+    if (!b.cyclic && (i == 0 || i == nxp - 1)) dpy = 0.0;
+    else if (j == 0) dpy = ((double)P[(size_t)px + i] - pv) / (b.dy * ah);
+    else if (j == nyp - 1) dpy = (pv - (double)P[(size_t)(j - 1) * px + i]) / (b.dy * ah);
+    else dpy = ((double)P[(size_t)(j + 1) * px + i] - (double)P[(size_t)(j - 1) * px + i]) / (2.0 * b.dy);
+}
+
+// Lagged (from pm) and current (from p) geostrophic velocities, FP64:
+// V[0..3] = ug, vg, uc, vc, each [nl][nyp][px].
+template <class T>
+__global__ void k_dg_vel(const BasinDev *__restrict__ bas, int member, int par, double *V) {
+    const BasinDev &b = bas[member];
+    const size_t n2 = (size_t)b.nyp * b.px, n3 = n2 * b.nl;
+    const T *P = (const T *)b.F[par], *PM = (const T *)b.F[1 - par];
+    for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < (size_t)b.nl * b.nyp * b.nxp;
+         idx += (size_t)gridDim.x * blockDim.x) {
+        const size_t k = idx / ((size_t)b.nyp * b.nxp), rem = idx - k * b.nyp * b.nxp;
+        const int j = (int)(rem / b.nxp), i = (int)(rem - (size_t)j * b.nxp);
+        const size_t o = k * n2 + (size_t)j * b.px + i;
+        double dx, dy;
+        dpdxy_bc(PM + k * n2, b, i, j, dx, dy);
+        V[o] = -dy / b.fnot;
+        V[n3 + o] = dx / b.fnot;
+        dpdxy_bc(P + k * n2, b, i, j, dx, dy);
+        V[2 * n3 + o] = -dy / b.fnot;
+        V[3 * n3 + o] = dx / b.fnot;
+    }
+}
+
+// del2_P_bc (numerics.F90:410-425) of nf FP64 fields [nl][nyp][px] each.
+__global__ void k_dg_del2(const BasinDev *__restrict__ bas, int member, const double *in, double *out, int nf) {
+    const BasinDev &b = bas[member];
+    const size_t n2 = (size_t)b.nyp * b.px;
+    const double afac = b.fx_bc / b.fx;   // alpha/(alpha/2+1)
+    const size_t tot = (size_t)nf * b.nl * b.nyp * b.nxp;
+    for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < tot; idx += (size_t)gridDim.x * blockDim.x) {
+        const size_t f = idx / ((size_t)b.nyp * b.nxp), rem = idx - f * b.nyp * b.nxp;
+        const int j = (int)(rem / b.nxp), i = (int)(rem - (size_t)j * b.nxp);
+        out[f * n2 + (size_t)j * b.px + i] = lap_bc_g(in + f * n2, b, i, j, afac);
+    }
+}
+
+#define OQG_DGQ 22   // row sums per (layer, row) of k_dg_rows
+
+// One CTA per (row j, layer k): trapezoid-in-x row sums (int_P_dx / dx) of
+// the qg_diagno integrands, into R[(q nl + k) nyp + j]; q 20 and 21 are the
+// row minimum and maximum of p.  V: ug, vg, uc, vc, del2 u, del4 u, del2 v,
+// del4 v (FP64 [nl][nyp][px] each); tau: taux, tauy rows (or null).
+template <class T>
+__global__ void __launch_bounds__(128) k_dg_rows(const BasinDev *__restrict__ bas, int member, int par,
+                                                 const double *V, const double *tau, double *R) {
+    const BasinDev &b = bas[member];
+    const int j = blockIdx.x, k = blockIdx.y, nl = b.nl, nxp = b.nxp, nyp = b.nyp;
+    const size_t n2 = (size_t)nyp * b.px, n3 = n2 * nl, o0 = (size_t)k * n2 + (size_t)j * b.px;
+    const T *P = (const T *)b.F[par], *Q = (const T *)b.F[2 + par];
+    const T *WK = (const T *)b.wekp, *EN = (const T *)b.ent;
+    __shared__ double red[32];
+    double s[OQG_DGQ];
+#pragma unroll
+    for (int q = 0; q < OQG_DGQ; ++q) s[q] = 0.0;
+    double pmin = 1e308, pmax = -1e308;
+    const double gpk = k < nl - 1 ? b.gp[k] : 1.0;
+    for (int i = threadIdx.x; i < nxp; i += blockDim.x) {
+        const double w = trap_x(b, i);
+        const size_t o = o0 + i, oj = (size_t)j * b.px + i;
+        const double pv = (double)P[o];
+        const double ug = V[o], vg = V[n3 + o], uc = V[2 * n3 + o], vc = V[3 * n3 + o];
+        s[0] += w * pv;
+        s[1] += w * (double)Q[o];
+        s[2] += w * (uc * V[4 * n3 + o]);
+        s[3] += w * (vc * V[6 * n3 + o]);
+        s[4] += w * (uc * V[5 * n3 + o]);
+        s[5] += w * (vc * V[7 * n3 + o]);
+        s[6] += w * (uc * uc);
+        s[7] += w * (vc * vc);
+        s[8] += w * uc;
+        s[9] += w * (ug * ug);
+        s[10] += w * (vg * vg);
+        if (k < nl - 1) {
+            const double eta = b.dz_sign * (pv - (double)P[o + n2]) / gpk;
+            s[11] += w * eta;
+            s[12] += w * (eta * eta);
+            if (k == 0) s[13] += w * (eta * (EN ? (double)EN[oj] : 0.0));
+        }
+        if (k == 0) {
+            const double wk = (double)WK[oj], e1 = EN ? (double)EN[oj] : 0.0;
+            s[14] += w * wk;
+            s[15] += w * fabs(wk);
+            s[16] += w * e1;
+            s[17] += w * fabs(e1);
+            if (tau) {
+                s[18] += w * (tau[oj] * uc);
+                s[19] += w * (tau[n2 + oj] * vc);
+            }
+        }
+        pmin = fmin(pmin, pv);
+        pmax = fmax(pmax, pv);
+    }
+    for (int q = 0; q < 20; ++q) {
+        const double v = block_sum(s[q], red);
+        if (threadIdx.x == 0) R[((size_t)q * nl + k) * nyp + j] = v;
+    }
+    __shared__ double mn[32], mx[32];
+    for (int o = 16; o > 0; o >>= 1) {
+        pmin = fmin(pmin, __shfl_down_sync(0xffffffffu, pmin, o));
+        pmax = fmax(pmax, __shfl_down_sync(0xffffffffu, pmax, o));
+    }
+    if ((threadIdx.x & 31) == 0) { mn[threadIdx.x >> 5] = pmin; mx[threadIdx.x >> 5] = pmax; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int wv = 1; wv < (int)(blockDim.x >> 5); ++wv) { pmin = fmin(pmin, mn[wv]); pmax = fmax(pmax, mx[wv]); }
+        R[((size_t)20 * nl + k) * nyp + j] = pmin;
+        R[((size_t)21 * nl + k) * nyp + j] = pmax;
+    }
+}
+
 }  // namespace oqg

@@ -57,6 +57,33 @@ class OqgParams(ctypes.Structure):
     ]
 
 
+class QgMonitor(ctypes.Structure):
+    """oqg_qg_monitor of include/oqg.h: the qg_diagno record
+    (qg_monitor.F90:219-383)."""
+    _fields_ = [("tsec", ctypes.c_double), ("wepm", ctypes.c_double), ("wapm", ctypes.c_double),
+                ("entm", ctypes.c_double), ("enam", ctypes.c_double),
+                ("etam", ctypes.c_double * OQG_MAX_NL), ("et2m", ctypes.c_double * OQG_MAX_NL),
+                ("pket", ctypes.c_double * OQG_MAX_NL), ("pken", ctypes.c_double), ("utau", ctypes.c_double),
+                ("pavg", ctypes.c_double * OQG_MAX_NL), ("qavg", ctypes.c_double * OQG_MAX_NL),
+                ("ah2d", ctypes.c_double * OQG_MAX_NL), ("ah4d", ctypes.c_double * OQG_MAX_NL),
+                ("ekei", ctypes.c_double * OQG_MAX_NL), ("val", ctypes.c_double * OQG_MAX_NL),
+                ("pos", ctypes.c_int * OQG_MAX_NL), ("circ", ctypes.c_double * OQG_MAX_NL),
+                ("ctot", ctypes.c_double), ("btdg", ctypes.c_double),
+                ("sfmin", ctypes.c_double * OQG_MAX_NL), ("sfmax", ctypes.c_double * OQG_MAX_NL),
+                ("ermas", ctypes.c_double * OQG_MAX_NL), ("emfr", ctypes.c_double * OQG_MAX_NL)]
+
+    def as_dict(self, nl: int) -> dict:
+        out = {}
+        for name, typ in self._fields_:
+            v = getattr(self, name)
+            if hasattr(typ, "_length_"):
+                n = nl - 1 if name in ("etam", "et2m", "pket", "ermas", "emfr") else nl
+                out[name] = np.array(v[:n])
+            else:
+                out[name] = float(v)
+        return out
+
+
 @dataclass
 class Basin:
     """One QG basin (the `box_type`, `topog_type` and `qg_type` parameters)."""

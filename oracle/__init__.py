@@ -20,7 +20,7 @@ import subprocess
 
 import numpy as np
 
-from openqg_b200.params import Basin
+from openqg_b200.params import Basin, QgMonitor
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _SO = os.path.join(_HERE, "build", "liboqg_oracle.so")
@@ -62,6 +62,8 @@ def lib():
         L.orc_set_step_index.argtypes = [ctypes.c_void_p, ctypes.c_longlong]
         L.orc_suppress.argtypes = [ctypes.c_void_p]
         L.orc_diag.argtypes = [ctypes.c_void_p, _dp, _dp, _dp, _dp]
+        L.orc_diagno.argtypes = [ctypes.c_void_p, _dp, _dp, ctypes.c_double, ctypes.c_double,
+                                 ctypes.POINTER(QgMonitor)]
         L.orc_solve_inhomog.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, _dp]
         L.orc_generate_homog_soln.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, _dp]
         L.orc_set_rdm2.argtypes = [ctypes.c_void_p, _dp]
@@ -149,6 +151,14 @@ class Oracle:
         e, smin, smax, c = (np.empty(nl) for _ in range(4))
         lib().orc_diag(self.h, _p(e), _p(smin), _p(smax), _p(c))
         return dict(ekei=e, sfmin=smin, sfmax=smax, circ=c)
+
+    def diagno(self, taux=None, tauy=None, tsec=0.0, tdt=0.0, mon=None):
+        """qg_diagno (qg_monitor.F90:219-383); mon carries state between calls."""
+        mon = mon if mon is not None else QgMonitor()
+        tx = None if taux is None else np.ascontiguousarray(taux, dtype=np.float64)
+        ty = None if tauy is None else np.ascontiguousarray(tauy, dtype=np.float64)
+        lib().orc_diagno(self.h, _p(tx), _p(ty), float(tsec), float(tdt), ctypes.byref(mon))
+        return mon.as_dict(self.b.nl), mon
 
     # pieces of the path ---------------------------------------------------
     def solve_inhomog(self, m, rhs):

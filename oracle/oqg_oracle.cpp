@@ -1356,6 +1356,124 @@ int orc_diag(void *h, double *ekei, double *sfmin, double *sfmax, double *circ) 
     return 0;
 }
 
+// qg_diagno, qg_monitor.F90:219-383 (with check_continuity :571-606 for a
+// channel).  The jet search runs over the first nyp-1 rows, the extent of the
+// reference's ujeto array.
+int orc_diagno(void *h, const double *taux, const double *tauy, double tsec, double tdt,
+               oqg_qg_monitor *mon) {
+    Model &M = *static_cast<Model *>(h);
+    const Box &b = M.b;
+    const int nxp = b.nxp, nyp = b.nyp, nl = b.nl;
+    const size_t n2 = M.n2();
+    const double area = b.xl * b.yl;
+    auto avg = [&](const std::vector<double> &f) { return int_P_dA(b, f.data()) / area; };
+    std::vector<double> t1(n2), t2(n2);
+    // Ekman velocity and entrainment means (:254-263)
+    for (size_t x = 0; x < n2; ++x) { t1[x] = M.wekp[x]; t2[x] = std::fabs(M.wekp[x]); }
+    mon->wepm = avg(t1);
+    mon->wapm = avg(t2);
+    const bool have_ent = !M.ent.empty();
+    for (size_t x = 0; x < n2; ++x) { t1[x] = have_ent ? M.ent[x] : 0.0; t2[x] = std::fabs(t1[x]); }
+    mon->entm = avg(t1);
+    mon->enam = avg(t2);
+    // interface displacement (:265-287)
+    std::vector<double> eta(n2);
+    const double tprev = mon->tsec;
+    for (int k = 0; k < nl - 1; ++k) {
+        for (size_t x = 0; x < n2; ++x) eta[x] = b.dz_sign * (M.p[n2 * k + x] - M.p[n2 * (k + 1) + x]) / M.gp[k];
+        mon->etam[k] = avg(eta);
+        for (size_t x = 0; x < n2; ++x) t1[x] = eta[x] * eta[x];
+        const double et2now = avg(t1);
+        mon->pket[k] = tsec > tprev ? 0.5 * M.rho * M.gp[k] * (et2now - mon->et2m[k]) / (tsec - tprev) : 0.0;
+        mon->et2m[k] = et2now;
+        if (k == 0) {
+            for (size_t x = 0; x < n2; ++x) t1[x] = eta[x] * (have_ent ? M.ent[x] : 0.0);
+            mon->pken = M.rho * M.gp[0] * avg(t1);
+        }
+    }
+    mon->tsec = tsec;
+    // lagged and current geostrophic velocities (:291-304)
+    std::vector<double> ug(n2 * nl), vg(n2 * nl), uc(n2 * nl), vc(n2 * nl), dx(n2), dy(n2);
+    for (int k = 0; k < nl; ++k) {
+        dPdx_2bc(b, &M.pm[n2 * k], M.bcco, dx.data());
+        dPdy_2bc(b, &M.pm[n2 * k], M.bcco, dy.data());
+        for (size_t x = 0; x < n2; ++x) { ug[n2 * k + x] = -dy[x] / b.fnot; vg[n2 * k + x] = dx[x] / b.fnot; }
+        dPdy_2bc(b, &M.p[n2 * k], M.bcco, dy.data());
+        dPdx_2bc(b, &M.p[n2 * k], M.bcco, dx.data());
+        for (size_t x = 0; x < n2; ++x) { uc[n2 * k + x] = -dy[x] / b.fnot; vc[n2 * k + x] = dx[x] / b.fnot; }
+    }
+    // wind work (:306-309)
+    if (taux && tauy) {
+        for (size_t x = 0; x < n2; ++x) { t1[x] = taux[x] * uc[x]; t2[x] = tauy[x] * vc[x]; }
+        mon->utau = M.rho * (int_P_dA(b, t2.data()) + int_P_dA(b, t1.data()));
+    } else {
+        mon->utau = 0.0;
+    }
+    for (int k = 0; k < nl; ++k) {
+        mon->pavg[k] = int_P_dA(b, &M.p[n2 * k]) / area;
+        mon->qavg[k] = int_P_dA(b, &M.q[n2 * k]) / area;
+    }
+    // lagged del^2 and del^4 of u, v (:316-320)
+    std::vector<double> d2u(n2), d4u(n2), d2v(n2), d4v(n2);
+    std::vector<double> ujeto(nyp);
+    for (int k = 0; k < nl; ++k) {
+        const double *U = &ug[n2 * k], *V = &vg[n2 * k], *Uc = &uc[n2 * k], *Vc = &vc[n2 * k];
+        del2_bc(b, U, M.bcco, d2u.data());
+        del2_bc(b, d2u.data(), M.bcco, d4u.data());
+        del2_bc(b, V, M.bcco, d2v.data());
+        del2_bc(b, d2v.data(), M.bcco, d4v.data());
+        for (size_t x = 0; x < n2; ++x) { t1[x] = Uc[x] * d2u[x]; t2[x] = Vc[x] * d2v[x]; }
+        mon->ah2d[k] = -M.rho * M.ah2[k] * b.h[k] * (int_P_dA(b, t1.data()) + int_P_dA(b, t2.data()));
+        for (size_t x = 0; x < n2; ++x) { t1[x] = Uc[x] * d4u[x]; t2[x] = Vc[x] * d4v[x]; }
+        mon->ah4d[k] = M.rho * M.ah4[k] * b.h[k] * (int_P_dA(b, t1.data()) + int_P_dA(b, t2.data()));
+        for (size_t x = 0; x < n2; ++x) { t1[x] = Uc[x] * Uc[x]; t2[x] = Vc[x] * Vc[x]; }
+        mon->ekei[k] = 0.5 * M.rho * b.h[k] * (int_P_dA(b, t1.data()) + int_P_dA(b, t2.data()));
+        std::vector<double> row(nxp);
+        for (int j = 0; j < nyp; ++j) {
+            for (int i = 0; i < nxp; ++i) row[i] = Uc[IX(i, j)];
+            ujeto[j] = std::fabs(int_P_dx(b, row.data())) / b.xl;
+        }
+        int jm = 0;
+        for (int j = 1; j < nyp - 1; ++j)
+            if (ujeto[j] > ujeto[jm]) jm = j;
+        mon->pos[k] = jm + 1;
+        mon->val[k] = ujeto[jm];
+        const double *p = &M.p[n2 * k];
+        mon->circ[k] = 1.0e-6 * ((p[IX(0, 0)] - p[IX(0, nyp - 1)]) / b.fnot);
+    }
+    mon->ctot = 0.0;
+    for (int k = 0; k < nl; ++k) mon->ctot += mon->circ[k];
+    // bottom drag, lagged velocities (:357-360)
+    {
+        const int kt = M.k_topo;
+        for (size_t x = 0; x < n2; ++x) { t1[x] = ug[n2 * kt + x] * ug[n2 * kt + x]; t2[x] = vg[n2 * kt + x] * vg[n2 * kt + x]; }
+        mon->btdg = 0.5 * M.rho * M.delek * std::fabs(b.fnot) * (int_P_dA(b, t1.data()) + int_P_dA(b, t2.data()));
+    }
+    // stream-function extrema (:362-382)
+    for (int k = 0; k < nl; ++k) {
+        const double *p = &M.p[n2 * k];
+        const double poref = b.fnot > 0 ? p[IX(0, 0)] : p[IX(0, nyp - 1)];
+        double pomin = p[0], pomax = p[0];
+        for (size_t x = 1; x < n2; ++x) { pomin = std::min(pomin, p[x]); pomax = std::max(pomax, p[x]); }
+        const double e1 = std::min(pomin / b.fnot, pomax / b.fnot), e2 = std::max(pomin / b.fnot, pomax / b.fnot);
+        mon->sfmin[k] = 1.0e-6 * (b.h[k] * (e1 - poref / b.fnot));
+        mon->sfmax[k] = 1.0e-6 * (b.h[k] * (e2 - poref / b.fnot));
+    }
+    // check_continuity (:571-606), channel only
+    for (int k = 0; k < OQG_MAX_NL; ++k) { mon->ermas[k] = 0.0; mon->emfr[k] = 0.0; }
+    if (b.cyclic) {
+        std::vector<double> ip(nl);
+        for (int k = 0; k < nl; ++k) ip[k] = int_P_dA(b, &M.p[n2 * k]);
+        for (int k = 0; k < nl - 1; ++k) {
+            const double est1 = b.dz_sign * (ip[k] - ip[k + 1]), est2 = M.dpi[k];
+            const double edif = est1 - est2, esum = std::fabs(est1) + std::fabs(est2);
+            mon->ermas[k] = edif;
+            mon->emfr[k] = esum > 1.0e-13 * b.xl * b.yl * tdt * M.gp[k] ? 2.0 * edif / esum : 0.0;
+        }
+    }
+    return 0;
+}
+
 int orc_solve_inhomog(void *h, int m, const double *rhs, double *out) {
     Model &M = *static_cast<Model *>(h);
     if (m < 1 || m > M.b.nl) return OQG_EINVAL;

@@ -217,3 +217,26 @@ def test_channel_steps_finite_and_periodic():
     P, PM, Q, QM = o.get_state()
     assert np.isfinite(P).all() and np.isfinite(Q).all()
     assert np.array_equal(P[:, :, -1], P[:, :, 0])
+
+
+def test_diagno_record_consistent():
+    """The oracle's qg_diagno: its ekei is diag's, the double-gyre pumping
+    averages to zero, the energy rate pket follows from two calls, and
+    ctot sums circ."""
+    b = ocean_double_gyre(33)
+    o = oracle.Oracle(b)
+    p = b.fnot * initial_psi(b, 1)
+    o.set_state(p, p)
+    taux, tauy = double_gyre_tau(b)
+    w, ts, tn = oracle.ekman_from_tau(b, taux, tauy)
+    o.set_forcing(w, None, ts, tn)
+    o.step(3600.0, 3)
+    d1, mon = o.diagno(taux, tauy, tsec=100.0, tdt=3600.0)
+    assert np.allclose(d1["ekei"], o.diag()["ekei"], rtol=1e-12)
+    assert abs(d1["wepm"]) <= 1e-10 * d1["wapm"]
+    assert d1["ctot"] == pytest.approx(np.sum(d1["circ"]))
+    et2_first = d1["et2m"].copy()
+    o.step(3600.0, 1)
+    d2, _ = o.diagno(taux, tauy, tsec=3700.0, tdt=3600.0, mon=mon)
+    want = 0.5 * b.rho * np.array(b.gp) * (d2["et2m"] - et2_first) / 3600.0
+    assert np.allclose(d2["pket"], want, rtol=1e-12)
