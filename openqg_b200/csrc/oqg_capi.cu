@@ -63,6 +63,9 @@ struct oqg_handle {
     double g_tdt[2] = {0.0, 0.0};
     cudaGraphExec_t g1exec[2] = {nullptr, nullptr};   // one step, by parity
     double g1_tdt[2] = {0.0, 0.0};
+    cudaGraphExec_t gbig[2] = {nullptr, nullptr};     // gbig_n (even) steps, by parity
+    double gbig_tdt[2] = {0.0, 0.0};
+    int gbig_n[2] = {0, 0};
     std::vector<double> modes_amat, modes_ctl2m, modes_ctm2l, modes_rdm2;
 };
 
@@ -274,6 +277,7 @@ static void drop_graphs(oqg_handle *h) {
     for (int i = 0; i < 2; ++i) {
         if (h->gexec[i]) { cudaGraphExecDestroy(h->gexec[i]); h->gexec[i] = nullptr; }
         if (h->g1exec[i]) { cudaGraphExecDestroy(h->g1exec[i]); h->g1exec[i] = nullptr; }
+        if (h->gbig[i]) { cudaGraphExecDestroy(h->gbig[i]); h->gbig[i] = nullptr; }
     }
 }
 
@@ -964,9 +968,22 @@ int oqg_set_forcing(oqg_handle *h, const double *wekp, const double *ent, double
 int oqg_step(oqg_handle *h, double tdt, int nsteps) {
     if (!h || nsteps < 0) return fail(OQG_EINVAL, "bad argument");
     int done = 0;
-    // pairs of steps replay a two-step graph, a remaining step a one-step
-    // graph, each cached per step parity and step length
-    if (nsteps >= 2) {
+    // runs of steps replay a graph of up to 16 steps (one host launch for
+    // many steps), pairs a two-step graph and a last step a one-step graph,
+    // each cached per step parity and step length
+    if (nsteps >= 4) {
+        const int par = h->par;
+        const int want = std::min(nsteps & ~1, 16);
+        if (!h->gbig[par] || h->gbig_tdt[par] != tdt) {
+            if (h->gbig[par]) { cudaGraphExecDestroy(h->gbig[par]); h->gbig[par] = nullptr; }
+            int rc = capture_steps(h, par, tdt, want, &h->gbig[par]);
+            if (rc) return rc;
+            h->gbig_tdt[par] = tdt;
+            h->gbig_n[par] = want;
+        }
+        for (; done + h->gbig_n[par] <= nsteps; done += h->gbig_n[par]) CK(cudaGraphLaunch(h->gbig[par], h->st));
+    }
+    if (nsteps - done >= 2) {
         const int par = h->par;
         if (!h->gexec[par] || h->g_tdt[par] != tdt) {
             if (h->gexec[par]) { cudaGraphExecDestroy(h->gexec[par]); h->gexec[par] = nullptr; }
