@@ -173,6 +173,17 @@ __device__ __forceinline__ void fft_stage(const typename C2<T>::t *__restrict__ 
     }
 }
 
+// The radix-3 and radix-5 stages out of line: most transform lengths are
+// powers of two, and keeping these stages out of the hot loop's code leaves
+// more of the instruction cache to it.
+template <class T, int R>
+__device__ __noinline__ void fft_stage_cold(const typename C2<T>::t *__restrict__ src,
+                                            typename C2<T>::t *__restrict__ dst, int M, int Ns, int lg,
+                                            FastDiv fd, const typename C2<T>::t *__restrict__ tws, int t,
+                                            int TT) {
+    fft_stage<T, R>(src, dst, M, Ns, lg, fd, tws, t, TT);
+}
+
 // Barrier `id` over the first `n` threads of the CTA (n a multiple of 32);
 // n = 0: all threads of the CTA (__syncthreads).
 __device__ __forceinline__ void bar_sync(int id, int n) {
@@ -204,8 +215,8 @@ __device__ typename C2<T>::t *fft_smem(typename C2<T>::t *a, typename C2<T>::t *
             case 8: fft_stage<T, 8>(src, dst, M, Ns, lg, fd, tws, t, TT); break;
             case 4: fft_stage<T, 4>(src, dst, M, Ns, lg, fd, tws, t, TT); break;
             case 2: fft_stage<T, 2>(src, dst, M, Ns, lg, fd, tws, t, TT); break;
-            case 3: fft_stage<T, 3>(src, dst, M, Ns, lg, fd, tws, t, TT); break;
-            default: fft_stage<T, 5>(src, dst, M, Ns, lg, fd, tws, t, TT); break;
+            case 3: fft_stage_cold<T, 3>(src, dst, M, Ns, lg, fd, tws, t, TT); break;
+            default: fft_stage_cold<T, 5>(src, dst, M, Ns, lg, fd, tws, t, TT); break;
         }
         bar_sync(bar_id, nbar);
         T2 *x = src; src = dst; dst = x;

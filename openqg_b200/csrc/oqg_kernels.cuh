@@ -935,7 +935,8 @@ struct XinvScal {
 //   the suppress_comp_mode schedule and its scalar part (openqg.F90:485-487,
 //     driver.F90:183-188).
 template <class T, int NL>
-__device__ void scalar_phase(const BasinDev &b, double tdt, int par, bool writer, XinvScal *out) {
+__device__ __noinline__ void scalar_phase(const BasinDev &b, double tdt, int par, bool writer,
+                                          XinvScal *out) {
     const int lane = threadIdx.x & 31;
     const DevState *st = b.st + par;
     const DevForcing *fr = b.frc;
