@@ -291,6 +291,32 @@ def run_reference(args):
     return 0
 
 
+def bind_to_gpu_numa(device_index):
+    """Pins this process to the host CPUs local to the GPU (from sysfs), so
+    pinned host buffers and the copy engines sit on the same NUMA node.
+    Returns the CPU count bound to, or None when the topology is unknown."""
+    import torch
+    try:
+        pr = torch.cuda.get_device_properties(device_index)
+        bus = "%04x:%02x:%02x.0" % (pr.pci_domain_id, pr.pci_bus_id, pr.pci_device_id)
+        with open("/sys/bus/pci/devices/%s/local_cpulist" % bus) as f:
+            spec = f.read().strip()
+        cpus = set()
+        for part in spec.split(","):
+            if "-" in part:
+                a, b = part.split("-")
+                cpus.update(range(int(a), int(b) + 1))
+            elif part:
+                cpus.add(int(part))
+        cpus &= os.sched_getaffinity(0)
+        if cpus:
+            os.sched_setaffinity(0, cpus)
+            return len(cpus)
+    except Exception:
+        pass
+    return None
+
+
 def max_over_ranks(ms, pg, device):
     """Max of a per-rank time over all ranks; every rank calls it."""
     import torch
@@ -326,6 +352,7 @@ def run_ours(args):
     import torch
     ws, rank, local = dist()
     torch.cuda.set_device(local)
+    numa_cpus = bind_to_gpu_numa(local)
     pg = None
     if ws > 1:
         import datetime
@@ -468,6 +495,7 @@ def run_ours(args):
                 "d2h_bytes_per_step": d2h, "timer": "host clock, median of %d steps" % e2e_steps,
                 "pattern": "per model step: upload wekp+ent, step, read p(:,:,1)"},
         "gpu_launches": args.steps * msteps * 4,
+        "host_cpus_bound": numa_cpus,
         "clocks": clk.summary(),
         "variants": variants,
     }
