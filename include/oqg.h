@@ -24,6 +24,7 @@
  *   ekman_from_tau                                  src/coupler/ekman.F90:53-83
  *   qg_diagno (ekei, sfmin, sfmax, circ)            src/diagnostics/qg_monitor.F90:289-376
  *   qg_diagno (the full monitor record)             src/diagnostics/qg_monitor.F90:219-383
+ *   valids (p, q and Ekman-pumping bounds)          src/diagnostics/valsubs.F90:46-139
  */
 #ifndef OQG_H
 #define OQG_H
@@ -204,6 +205,15 @@ typedef struct oqg_qg_monitor {
  * the channel continuity check).  mon is read (tsec, et2m) and written. */
 int oqg_diagno(oqg_handle *h, const double *taux, const double *tauy, double tsec,
                double tdt, oqg_qg_monitor *mon);
+
+/* The QG part of the validity scan valids (valsubs.F90:46-139): extremes of
+ * p and q over all layers and of the Ekman pumping wekp, each compared with
+ * its bound (|min| or |max| >= bound is invalid, as in the reference).
+ * ext[6] = pmin, pmax, qmin, qmax, wmin, wmax; *ok = 1 when all are valid.
+ * Non-finite values also make *ok = 0 (the reference's comparisons let a
+ * NaN pass); *nonfinite counts them.  Pointers other than ok may be NULL. */
+int oqg_valids(oqg_handle *h, double pext, double qext, double wext, double *ext,
+               long long *nonfinite, int *ok);
 
 /* solve_inhomog_eqn (inhomog.F90:156-168): (Del^2 - rdm2(m)) out = rhs with
  * out = 0 on solid boundaries; m is the 1-based mode; rhs, out (nxp, nyp). */

@@ -61,6 +61,8 @@ def lib():
     L.oqg_check_finite.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
     L.oqg_diag.argtypes = [vp, _dp, _dp, _dp, _dp]
     L.oqg_diag_noalloc.argtypes = [vp, _dp, _dp, _dp, _dp]
+    L.oqg_valids.argtypes = [vp, ctypes.c_double, ctypes.c_double, ctypes.c_double, _dp,
+                             ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_int)]
     L.oqg_diagno.argtypes = [vp, _dp, _dp, ctypes.c_double, ctypes.c_double, ctypes.POINTER(QgMonitor)]
     L.oqg_solve_inhomog.argtypes = [vp, ctypes.c_int, _dp, _dp]
     L.oqg_generate_homog_soln.argtypes = [vp, ctypes.c_int, _dp, _dp]
@@ -216,6 +218,17 @@ class QG:
         ty = _f64(tauy, self.b.shape2)
         _check(lib().oqg_diagno(self.h, _p(tx), _p(ty), float(tsec), float(tdt), ctypes.byref(mon)), "oqg_diagno")
         return mon.as_dict(self.b.nl), mon
+
+    def valids(self, pext: float, qext: float, wext: float):
+        """valids (valsubs.F90:46-139) for p, q and wekp: (ok, extremes dict,
+        count of non-finite values)."""
+        ext = np.empty(6)
+        bad = ctypes.c_longlong()
+        ok = ctypes.c_int()
+        _check(lib().oqg_valids(self.h, float(pext), float(qext), float(wext), _p(ext), ctypes.byref(bad),
+                                ctypes.byref(ok)), "oqg_valids")
+        names = ("pmin", "pmax", "qmin", "qmax", "wmin", "wmax")
+        return bool(ok.value), dict(zip(names, ext)), bad.value
 
     def diag_noalloc(self):
         """diag() through oqg_diag_noalloc: scratch in the library's fixed

@@ -55,6 +55,7 @@ struct oqg_handle {
     double *stage[2] = {nullptr, nullptr};
     double *hrow = nullptr;     // contiguous host-order copy buffer [nl][nyp][nxp]
     double *dg = nullptr;       // qg_diagno scratch, made on its first call
+    double *vs = nullptr;       // valids partials, made on its first call
     unsigned long long *d_bad = nullptr;
     double *d_diag = nullptr;
     void *ent_buf = nullptr;
@@ -1173,6 +1174,33 @@ int oqg_diagno(oqg_handle *h, const double *taux, const double *tauy, double tse
             mon->emfr[k] = esum > 1.0e-13 * xl * yl * tdt * P.gp[k] ? 2.0 * edif / esum : 0.0;
         }
     }
+    return OQG_OK;
+}
+
+int oqg_valids(oqg_handle *h, double pext, double qext, double wext, double *ext, long long *nonfinite, int *ok) {
+    if (!h || !ok) return fail(OQG_EINVAL, "bad argument");
+    const int nb = 296;
+    if (!h->vs) {
+        h->vs = dalloc<double>(h, (size_t)nb * 7);
+        if (!h->vs) return fail(OQG_ECUDA, "out of device memory");
+    }
+    if (h->mixed) k_valids<float><<<nb, 256, 0, h->st>>>(h->d_bas, 0, h->par, h->vs);
+    else k_valids<double><<<nb, 256, 0, h->st>>>(h->d_bas, 0, h->par, h->vs);
+    CK(cudaGetLastError());
+    std::vector<double> r((size_t)nb * 7);
+    CK(cudaMemcpyAsync(r.data(), h->vs, r.size() * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    double e[6] = {1e308, -1e308, 1e308, -1e308, 1e308, -1e308}, bad = 0.0;
+    for (int c = 0; c < nb; ++c) {
+        for (int q = 0; q < 6; ++q) e[q] = (q & 1) ? std::max(e[q], r[c * 7 + q]) : std::min(e[q], r[c * 7 + q]);
+        bad += r[c * 7 + 6];
+    }
+    const bool valid = bad == 0.0 && std::fabs(e[0]) < pext && std::fabs(e[1]) < pext && std::fabs(e[2]) < qext &&
+                       std::fabs(e[3]) < qext && std::fabs(e[4]) < wext && std::fabs(e[5]) < wext;
+    if (ext)
+        for (int q = 0; q < 6; ++q) ext[q] = e[q];
+    if (nonfinite) *nonfinite = (long long)bad;
+    *ok = valid ? 1 : 0;
     return OQG_OK;
 }
 

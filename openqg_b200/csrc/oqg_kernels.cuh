@@ -1692,6 +1692,52 @@ __global__ void k_diag(const BasinDev *__restrict__ bas, int member, int par, do
     }
 }
 
+// ------------------------------------------------------------------ valids
+// Extremes of p, q (all layers) and wekp for the validity scan (valsubs.F90:
+// 46-139), and the count of non-finite values among them: per CTA into
+// out[blockIdx.x * 7 + (pmin, pmax, qmin, qmax, wmin, wmax, nonfinite)].
+template <class T>
+__global__ void __launch_bounds__(256) k_valids(const BasinDev *__restrict__ bas, int member, int par, double *out) {
+    const BasinDev &b = bas[member];
+    const T *P = (const T *)b.F[par], *Q = (const T *)b.F[2 + par], *W = (const T *)b.wekp;
+    const size_t n2 = (size_t)b.nyp * b.px;
+    double v[6] = {1e308, -1e308, 1e308, -1e308, 1e308, -1e308};
+    double bad = 0.0;
+    const size_t tot = (size_t)b.nl * b.nyp * b.nxp;
+    for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < tot; idx += (size_t)gridDim.x * blockDim.x) {
+        const size_t k = idx / ((size_t)b.nyp * b.nxp), rem = idx - k * b.nyp * b.nxp;
+        const size_t j = rem / b.nxp, i = rem - j * b.nxp;
+        const size_t o = k * n2 + j * b.px + i;
+        const double pv = (double)P[o], qv = (double)Q[o];
+        if (!isfinite(pv)) bad += 1.0; else { v[0] = fmin(v[0], pv); v[1] = fmax(v[1], pv); }
+        if (!isfinite(qv)) bad += 1.0; else { v[2] = fmin(v[2], qv); v[3] = fmax(v[3], qv); }
+        if (k == 0) {
+            const double wv = (double)W[j * b.px + i];
+            if (!isfinite(wv)) bad += 1.0; else { v[4] = fmin(v[4], wv); v[5] = fmax(v[5], wv); }
+        }
+    }
+    __shared__ double red[7][8];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int q = 0; q < 6; ++q) {
+        double x = v[q];
+        for (int o = 16; o > 0; o >>= 1) {
+            const double y = __shfl_down_sync(0xffffffffu, x, o);
+            x = (q & 1) ? fmax(x, y) : fmin(x, y);
+        }
+        if (lane == 0) red[q][wid] = x;
+    }
+    for (int o = 16; o > 0; o >>= 1) bad += __shfl_down_sync(0xffffffffu, bad, o);
+    if (lane == 0) red[6][wid] = bad;
+    __syncthreads();
+    if (threadIdx.x < 7) {
+        const int q = threadIdx.x;
+        double x = red[q][0];
+        for (int w = 1; w < (int)(blockDim.x >> 5); ++w)
+            x = q == 6 ? x + red[q][w] : ((q & 1) ? fmax(x, red[q][w]) : fmin(x, red[q][w]));
+        out[blockIdx.x * 7 + q] = x;
+    }
+}
+
 // ------------------------------------------------------------------ qg_diagno
 // The monitor record of qg_diagno (qg_monitor.F90:219-383) on the device:
 // velocity fields, their wall Laplacians, then per-row sums of every

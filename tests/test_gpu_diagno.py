@@ -80,3 +80,30 @@ def test_diagno_matches_oracle(kind):
     d = g.diag()
     _close(dg["ekei"], d["ekei"], "ekei vs diag")
     g.close()
+
+
+def test_valids_extremes_and_bounds():
+    """valids (valsubs.F90:46-139): the extremes equal numpy's over the state,
+    a bound below an extreme flags the state, and a NaN does too."""
+    b = ocean_double_gyre(65)
+    p = b.fnot * initial_psi(b, 6)
+    w, ts, tn = oracle.ekman_from_tau(b, *double_gyre_tau(b))
+    g = QG(b)
+    g.set_state(p, p)
+    g.set_forcing(w, None, ts, tn)
+    g.step(3600.0, 3)
+    P, _, Q, _ = g.get_state()
+    ok, ext, bad = g.valids(1e30, 1e30, 1e30)
+    assert ok and bad == 0
+    assert ext["pmin"] == P.min() and ext["pmax"] == P.max()
+    assert ext["qmin"] == Q.min() and ext["qmax"] == Q.max()
+    assert ext["wmin"] == w.min() and ext["wmax"] == w.max()
+    ok, _, _ = g.valids(0.5 * max(abs(P.min()), abs(P.max())), 1e30, 1e30)
+    assert not ok
+    P2, PM2, Q2, QM2 = g.get_state()
+    c = g.constraints()
+    P2[1, 10, 10] = np.nan
+    g.set_state_full(P2, PM2, Q2, QM2, c["dpi"], c["dpip"])
+    ok, _, bad = g.valids(1e30, 1e30, 1e30)
+    assert not ok and bad == 1
+    g.close()
