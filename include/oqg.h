@@ -253,7 +253,7 @@ int oqg_stream(oqg_handle *h, void **stream);
 /* ---------------------------------------------------------------------
  * Ensembles: many independent basins of uneven size stepped together by one
  * launch per phase (captured in a CUDA graph).  Members keep the semantics of
- * a single handle and give bit-identical results; they must share nl and
+ * a single handle and match its results to rounding; they must share nl and
  * precision, and be all closed boxes or all channels (OQG_EINVAL /
  * OQG_EUNSUPPORTED otherwise).  Per-member calls (set_state, set_forcing,
  * get_state) wait for the ensemble's stream first.  member is 0-based.

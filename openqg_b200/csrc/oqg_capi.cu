@@ -580,7 +580,10 @@ int oqg_version(char *buf, int buflen) {
     return OQG_OK;
 }
 
-int oqg_create(const oqg_params *prm, oqg_handle **out) {
+// batched: a member of an ensemble, whose tiles need not fill whole waves on
+// their own (the ensemble's work list does), so the vorticity tiles take the
+// tallest height and the least halo.
+static int create_impl(const oqg_params *prm, oqg_handle **out, bool batched) {
     if (!prm || !out) return fail(OQG_EINVAL, "null argument");
     *out = nullptr;
     const oqg_params &P = *prm;
@@ -640,7 +643,7 @@ int oqg_create(const oqg_params *prm, oqg_handle **out) {
         b.tiles_x = (P.nxp + VTX - 1) / VTX;
         int best = VTYMAX;
         long best_cost = -1;
-        for (int vt = VTYMAX; vt >= 8; --vt) {
+        for (int vt = VTYMAX; vt >= 8 && !batched; --vt) {
             const int ty = (P.nyp + vt - 1) / vt;
             const long waves = ((long)b.tiles_x * ty + slots - 1) / slots;
             const long cost = waves * (vt + 6);
@@ -826,6 +829,8 @@ int oqg_create(const oqg_params *prm, oqg_handle **out) {
     *out = h;
     return OQG_OK;
 }
+
+int oqg_create(const oqg_params *prm, oqg_handle **out) { return create_impl(prm, out, false); }
 
 int oqg_destroy(oqg_handle *h) {
     destroy_all(h);
@@ -1417,7 +1422,7 @@ int oqg_ensemble_create(const oqg_params *members, int nmembers, oqg_ensemble **
     }
     for (int i = 0; i < nmembers; ++i) {
         oqg_handle *h = nullptr;
-        const int rc = oqg_create(&members[i], &h);
+        const int rc = create_impl(&members[i], &h, true);
         if (rc) {
             std::string msg = "member " + std::to_string(i) + ": " + g_err;
             ens_free(e);

@@ -1,6 +1,6 @@
 """Batched ensembles (oqg_ensemble_*): members of uneven size stepped by one
-launch per phase must give exactly what each member gives as a single
-handle, and so inherit the single handle's parity with the oracle."""
+launch per phase must give what each member gives as a single handle (to
+rounding), and so inherit the single handle's parity with the oracle."""
 import numpy as np
 import pytest
 
@@ -53,9 +53,12 @@ def _run_pair(members, tdts, nsteps):
 
 
 def _assert_same(e, singles):
+    # members tile the vorticity kernel with the tallest tiles, single handles
+    # with tiles fitted to whole waves; the channel strip sums and the wall
+    # rows then round differently, so the match is to rounding, not bits
     for i, g in enumerate(singles):
         for name, a, c in zip(("p", "pm", "q", "qm"), e.get_state(i), g.get_state()):
-            assert np.array_equal(a, c), "member %d %s rel L2 %.3e" % (i, name, rel_l2(a, c))
+            assert rel_l2(a, c) <= 1e-13, "member %d %s rel L2 %.3e" % (i, name, rel_l2(a, c))
 
 
 def test_box_ensemble_equals_single_handles():
