@@ -29,6 +29,7 @@ scaling); the time is the max over ranks.
 import argparse
 import ctypes
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -117,6 +118,72 @@ def run_ensemble(precision, steps, warmup, msteps, flush, tdt=3600.0):
     cells = sum(b.nxp * b.nyp * b.nl for b in basins)
     e.close()
     return cells, total
+
+
+def run_adjoint(reps=3, nsteps=200, every=20, tdt=3600.0):
+    """The differentiable configuration: 3-layer ocean box at 257x257, dx
+    20 km, 200 leapfrog steps, J = ekei(1) of the final state, gradients with
+    respect to the initial stream function and the wind forcing, checkpoint
+    every 20 steps with recomputation.  Device times between CUDA events on
+    the handle's stream (host waits inside a pass included) of the plain
+    forward run, the checkpointed forward, the reverse pass (recompute +
+    adjoint) and 200 adjoint steps alone; medians over reps after one
+    untimed repetition."""
+    import torch
+    from openqg_b200.adjoint import AdjointRun, ekei
+    from openqg_b200.core import QG, lib
+    from openqg_b200.params import ocean_double_gyre
+    b = ocean_double_gyre(257, dx=20e3)
+    p, w, ts, tn = initial_inputs(b, seed=5)
+    g = QG(b)
+    g.set_forcing(w, None, ts, tn)
+    s = torch.cuda.ExternalStream(g.stream())
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        fn()
+        e1.record(s)
+        e1.synchronize()
+        return e0.elapsed_time(e1)
+
+    run = AdjointRun(g, every)
+    L = lib()
+    slot = ctypes.c_void_p(run.slots[0].data_ptr())
+    fwd, ck, bwd, adj = [], [], [], []
+    gnorm = 0.0
+    for _ in range(reps + 1):
+        g.set_state(p, p)
+        g.set_step_index(0)
+        fwd.append(timed(lambda: g.step(tdt, nsteps)))
+        g.set_state(p, p)
+        g.set_step_index(0)
+        ck.append(timed(lambda: run.forward(nsteps, tdt)))
+        pf = torch.as_tensor(g.get_state()[0], device="cuda").requires_grad_(True)
+        (gp,) = torch.autograd.grad(ekei(b, pf)[0], [pf])
+        out = {}
+        bwd.append(timed(lambda: out.update(run.backward(lp=gp))))
+        gnorm = float(out["gp0"].norm()) + float(out["lwekp"].norm())
+        L.oqg_pq_save(g.h, slot)
+
+        def adj_only():
+            for i in range(nsteps):
+                L.oqg_adj_step(g.h, slot, ctypes.c_double(tdt), ctypes.c_longlong(2 + i % 20))
+
+        adj.append(timed(adj_only))
+    g.close()
+    med = lambda x: statistics.median(x[1:]) / nsteps
+    if not math.isfinite(gnorm):
+        raise RuntimeError("non-finite adjoint gradient")
+    f, c, r, a = med(fwd), med(ck), med(bwd), med(adj)
+    return {"workload": "ocean 257x257x3 box, dx 20 km, %d steps, checkpoint every %d, J = ekei(1), "
+                        "gradient w.r.t. initial psi and wind forcing" % (nsteps, every),
+            "forward_ms_per_step": f, "checkpointed_forward_ms_per_step": c,
+            "reverse_ms_per_step": r, "adjoint_step_ms": a,
+            "reverse_over_forward": r / f, "adjoint_step_over_forward_step": a / f,
+            "launches_per_adjoint_step": 7,
+            "timer": "CUDA events on the handle's stream, median of %d runs" % reps}
 
 
 def initial_inputs(b, seed, reference=False):
@@ -451,6 +518,8 @@ def run_ours(args):
         variants["ensemble_config"] = ("256 ocean 3-layer boxes, sizes uniform in %s, dx 20 km, "
                                        "per-member wind 0.05-0.15 N/m^2 and ah4 1e10-4e10; %d "
                                        "cell-layers per step" % (list(ENSEMBLE_SIZES), cells_e))
+        # the adjoint: reverse pass and adjoint step against the forward step
+        variants["adjoint257"] = run_adjoint()
 
     # dominant kernel, timed alone, against the HBM roofline
     g.set_forcing(w, None, ts, tn)

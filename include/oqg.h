@@ -29,6 +29,8 @@
 #ifndef OQG_H
 #define OQG_H
 
+#include <stddef.h>
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -274,6 +276,55 @@ int oqg_ensemble_step(oqg_ensemble *e, const double *tdt, int nsteps);
 int oqg_ensemble_sync(oqg_ensemble *e);
 /* The CUDA stream (cudaStream_t) the ensemble's steps run on. */
 int oqg_ensemble_stream(oqg_ensemble *e, void **stream);
+
+/* ---------------------------------------------------------------------
+ * State slots and the adjoint step.  The reference has no adjoint (its model
+ * is run forward only); these entry points have no counterpart in it.  They
+ * serve gradient computation through the step (reverse mode with
+ * checkpoint-every-k recomputation), closed box in FP64 only
+ * (OQG_EUNSUPPORTED otherwise).  Slot buffers are device memory the caller
+ * owns; copies are queued on the handle's stream.
+ * ------------------------------------------------------------------- */
+
+/* Bytes of a full-state slot (p, pm, q, qm, the constraint scalars and the
+ * step counter) and of a p-and-q slot.  Either pointer may be NULL. */
+int oqg_state_bytes(oqg_handle *h, size_t *full, size_t *pq);
+/* Full state to / from a slot: a loaded handle continues bit for bit. */
+int oqg_state_save(oqg_handle *h, void *dst);
+int oqg_state_load(oqg_handle *h, const void *src);
+/* p and q of the current state to a slot: what oqg_adj_step needs of the
+ * input state of the step it reverses. */
+int oqg_pq_save(oqg_handle *h, void *dst);
+
+/* Sets the adjoint state: the gradient of an objective with respect to the
+ * state after the last step, lp, lpm, lq, lqm (nxp, nyp, nl) in host or
+ * device memory, NULL for zero; ldpi, ldpip (nl-1) host arrays or NULL.  The
+ * accumulated wind adjoint is zeroed.  Makes the adjoint buffers on first use. */
+int oqg_adj_set(oqg_handle *h, const double *lp, const double *lpm,
+                const double *lq, const double *lqm, const double *ldpi,
+                const double *ldpip);
+/* Reads the adjoint state and the accumulated gradient with respect to
+ * wekp, lwekp (nxp, nyp).  Any pointer may be NULL. */
+int oqg_adj_get(oqg_handle *h, double *lp, double *lpm, double *lq,
+                double *lqm, double *ldpi, double *ldpip, double *lwekp);
+/* Reverses step number step_no (1-based; suppress_comp_mode is transposed
+ * when it followed that step, mod(step_no-1, suppress_period) == 0): the
+ * adjoint state of the step's output becomes that of its input.  pq is a
+ * slot holding p and q of the step's input state (oqg_pq_save).  Queued on
+ * the handle's stream; steps are reversed last first. */
+int oqg_adj_step(oqg_handle *h, const void *pq, double tdt, long long step_no);
+/* One segment of a checkpointed reverse run, queued without host waits:
+ * loads the full-state slot ckpt (the state before step first_step_no),
+ * recomputes the segment's n steps keeping p and q of each step's input in
+ * the slots (n slots of slot_stride bytes from `slots`, device memory), then
+ * reverses the n steps last first. */
+int oqg_adj_segment(oqg_handle *h, const void *ckpt, void *slots,
+                    size_t slot_stride, int n, double tdt,
+                    long long first_step_no);
+/* The transpose of oqg_set_state applied to the adjoint state: gradients
+ * with respect to the p and pm given to oqg_set_state, gp, gpm (nxp, nyp, nl)
+ * in host or device memory (either may be NULL). */
+int oqg_adj_initial(oqg_handle *h, double *gp, double *gpm);
 
 #ifdef __cplusplus
 }

@@ -79,6 +79,15 @@ def lib():
     L.oqg_ensemble_step.argtypes = [vp, _dp, ctypes.c_int]
     L.oqg_ensemble_sync.argtypes = [vp]
     L.oqg_ensemble_stream.argtypes = [vp, ctypes.POINTER(vp)]
+    L.oqg_state_bytes.argtypes = [vp, ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_size_t)]
+    L.oqg_state_save.argtypes = [vp, vp]
+    L.oqg_state_load.argtypes = [vp, vp]
+    L.oqg_pq_save.argtypes = [vp, vp]
+    L.oqg_adj_set.argtypes = [vp, vp, vp, vp, vp, _dp, _dp]
+    L.oqg_adj_get.argtypes = [vp, vp, vp, vp, vp, _dp, _dp, vp]
+    L.oqg_adj_step.argtypes = [vp, vp, ctypes.c_double, ctypes.c_longlong]
+    L.oqg_adj_initial.argtypes = [vp, vp, vp]
+    L.oqg_adj_segment.argtypes = [vp, vp, vp, ctypes.c_size_t, ctypes.c_int, ctypes.c_double, ctypes.c_longlong]
     _lib = L
     return L
 

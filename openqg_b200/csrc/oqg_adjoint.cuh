@@ -1,0 +1,394 @@
+// oqg_adjoint.cuh -- the adjoint of the closed-box QG step, FP64.
+//
+// The step (step_qg, core.F90:16-33, then suppress_comp_mode when it is due)
+// maps the state (p, pm, q, qm, dpi, dpip) and the Ekman pumping wekp to the
+// next state.  It is affine in everything but the Arakawa Jacobian, which is
+// bilinear in (p, q); so its transpose, for the input state of the step, is a
+// chain of transposed linear operators:
+//
+//   suppress_comp_mode^T   lam_p' <- lam_p/2, lam_pm' <- lam_pm + lam_p/2, ...
+//   ocqbdy^T               the wall q's dependence on the new p
+//   modes_to_layers^T      nu_m = sum_k ctm2l(m,k) lam_p_k
+//   box_homog^T            alpha's adjoint <hsb_m, nu_m>, the transposed
+//                          (nl-1) constraint solve, the area integrals' weights
+//   Helmholtz^T            the modal solve itself: the five-point operator with
+//                          zero walls, less rdm2_m, is symmetric, so its
+//                          inverse is applied again (the forward solver)
+//   p_modes_rhs^T          lam_qnew_k = lam_q_k + f0 sum_m ctl2m(k,m) s_m
+//   leapfrog^T             lam_qm = lam_qnew; dq's adjoint g = tdt lam_qnew
+//   vort_step^T            the Jacobian's two transposes, the friction chain
+//                          L^T L^T (L^T) and the drag's L^T, the wind's weight
+//
+// Every kernel writes each output point once, gathering the terms of the
+// forward stencils that read it, so results do not depend on thread order.
+// Fields are FP64 [nl][nyp][px] (the handle's layout).  The forward operators:
+//   L   del2_P_bc (numerics.F90:410-468): 5-point Laplacian, mixed-BC
+//       one-sided terms on the walls, zero in the corners;
+//   t   the Arakawa sum of jacobian (numerics.F90:340-388): the step's
+//       Jacobian is jac_fac t(p, q), nonzero at interior points only;
+//   O   ocqbdy (vorsubs.F90:58-114): wall q from the new p; a corner takes
+//       the meridional-wall difference and the A p term twice.
+#pragma once
+
+#include "oqg_kernels.cuh"
+
+#define OQG_ADJ_CTAS 296     // CTAs of the grid-stride adjoint kernels
+#define OQG_ADJ_THREADS 256
+
+namespace oqg {
+
+// Weight of f at (iy + dxo, jy + dyo) in (L f)(iy, jy).
+__device__ __forceinline__ double lap_weight(const BasinDev &b, int iy, int jy, int dxo, int dyo) {
+    const int nxp = b.nxp, nyp = b.nyp;
+    const bool zrow = (jy == 0 || jy == nyp - 1);
+    const bool wl = iy == 0, wr = iy == nxp - 1;
+    double w = 0.0;
+    if (!zrow && dyo == 0) {   // dP2dx2_bc
+        if (wl) w += dxo == 1 ? b.fx_bc : (dxo == 0 ? -b.fx_bc : 0.0);
+        else if (wr) w += dxo == -1 ? b.fx_bc : (dxo == 0 ? -b.fx_bc : 0.0);
+        else w += dxo == 0 ? -2.0 * b.fx : b.fx;
+    }
+    if (!(wl || wr) && dxo == 0) {   // dP2dy2_bc
+        if (jy == 0) w += dyo == 1 ? b.fy_bc : (dyo == 0 ? -b.fy_bc : 0.0);
+        else if (jy == nyp - 1) w += dyo == -1 ? b.fy_bc : (dyo == 0 ? -b.fy_bc : 0.0);
+        else w += dyo == 0 ? -2.0 * b.fy : b.fy;
+    }
+    return w;
+}
+
+// (L^T g)(i, j) of one layer field g.
+__device__ __forceinline__ double lapT_at(const BasinDev &b, const double *g, int i, int j) {
+    const int di[5] = {0, 1, -1, 0, 0}, dj[5] = {0, 0, 0, 1, -1};
+    double s = 0.0;
+#pragma unroll
+    for (int t = 0; t < 5; ++t) {
+        const int iy = i + di[t], jy = j + dj[t];
+        if (iy < 0 || iy >= b.nxp || jy < 0 || jy >= b.nyp) continue;
+        const double w = lap_weight(b, iy, jy, -di[t], -dj[t]);
+        if (w != 0.0) s += w * g[(size_t)jy * b.px + iy];
+    }
+    return s;
+}
+
+struct AdjFields {
+    double *lp, *lpm, *lq, *lqm;   // adjoint of the state after the step
+    double *nu, *s, *t1;           // scratch: modal adjoint, modal solution, L^T g
+    double *lw;                    // accumulated adjoint of wekp [nyp][px]
+    double *part;                  // [OQG_ADJ_CTAS][nl-1] partial dots
+    double *scal;                  // lam_dpi [0, 8), lam_dpip [8, 16)
+};
+
+// suppress_comp_mode^T (driver.F90:174-189): x' = (x + xm)/2 for x = p, q, dpi.
+__global__ void k_adj_suppress(const BasinDev *__restrict__ bas, AdjFields a) {
+    const BasinDev &b = bas[0];
+    const size_t n = (size_t)b.nl * b.nyp * b.px;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const double hp = 0.5 * a.lp[i], hq = 0.5 * a.lq[i];
+        a.lp[i] = hp;
+        a.lpm[i] += hp;
+        a.lq[i] = hq;
+        a.lqm[i] += hq;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+        for (int l = 0; l < b.nl - 1; ++l) {
+            const double h = 0.5 * a.scal[l];
+            a.scal[l] = h;
+            a.scal[8 + l] += h;
+        }
+}
+
+// ocqbdy^T and modes_to_layers^T: nu_m = sum_k ctm2l(m,k) (lam_p + O^T lam_q)_k
+// at every point, and per-CTA partial dots <hsb_{m-1}, nu_m>, m >= 1.
+template <int NL>
+__global__ void __launch_bounds__(OQG_ADJ_THREADS) k_adj_wall(const BasinDev *__restrict__ bas, AdjFields a) {
+    const BasinDev &b = bas[0];
+    const int nxp = b.nxp, nyp = b.nyp, px = b.px;
+    const size_t n2 = (size_t)nyp * px;
+    const double fac = b.qb_fac;
+    const double *hsb = (const double *)b.hsb;
+    __shared__ double red[32];
+    double dot[NL > 1 ? NL - 1 : 1];
+#pragma unroll
+    for (int m = 0; m < NL - 1; ++m) dot[m] = 0.0;
+    for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < (size_t)nyp * nxp;
+         idx += (size_t)gridDim.x * blockDim.x) {
+        const int j = (int)(idx / nxp), i = (int)(idx - (size_t)j * nxp);
+        const size_t o = (size_t)j * px + i;
+        const bool zon = (j == 0 || j == nyp - 1), mer = (i == 0 || i == nxp - 1);
+        const int cnt = (zon ? 1 : 0) + (mer ? 1 : 0);
+        double lq[NL], lpt[NL];
+#pragma unroll
+        for (int k = 0; k < NL; ++k) lq[k] = cnt ? a.lq[k * n2 + o] : 0.0;
+#pragma unroll
+        for (int k = 0; k < NL; ++k) {
+            double s = a.lp[k * n2 + o];
+            if (cnt) {
+                s -= fac * lq[k];
+                double av = 0.0;
+#pragma unroll
+                for (int kk = 0; kk < NL; ++kk) av += b.amat[kk + NL * k] * lq[kk];
+                s -= cnt * b.fnot * av;
+            }
+            // x as the inner neighbour of a wall point
+            const double *L = a.lq + k * n2;
+            if (i == 1) s += fac * L[(size_t)j * px];
+            if (i == nxp - 2) s += fac * L[(size_t)j * px + nxp - 1];
+            if (i >= 1 && i <= nxp - 2) {
+                if (j == 1) s += fac * L[i];
+                if (j == nyp - 2) s += fac * L[(size_t)(nyp - 1) * px + i];
+            }
+            lpt[k] = s;
+        }
+#pragma unroll
+        for (int m = 0; m < NL; ++m) {
+            double v = 0.0;
+#pragma unroll
+            for (int k = 0; k < NL; ++k) v += b.ctm2l[m + NL * k] * lpt[k];
+            a.nu[m * n2 + o] = v;
+            if (m >= 1) dot[m - 1] += hsb[(m - 1) * n2 + o] * v;
+        }
+    }
+#pragma unroll
+    for (int m = 0; m < NL - 1; ++m) {
+        const double v = block_sum(dot[m], red);
+        if (threadIdx.x == 0) a.part[blockIdx.x * (NL - 1) + m] = v;
+    }
+}
+
+// box_homog^T: the adjoint of alpha from the partial dots, the transposed
+// constraint solve (cdhoc^T with the LU of DGETRF: U^T, then L^T, then the row
+// interchanges in reverse), the adjoint of the modal area integrals; then
+// the modal right-hand sides rhs_m = nu_m + lam_im_m dx dy on the interior.
+// CTA 0 also carries the constraint adjoints through update_mass_constr.
+template <int NL>
+__global__ void __launch_bounds__(OQG_ADJ_THREADS) k_adj_rhs(const BasinDev *__restrict__ bas, AdjFields a,
+                                                             int nparts) {
+    const BasinDev &b = bas[0];
+    constexpr int N = NL - 1;
+    __shared__ double lim[NL];
+    if (threadIdx.x < 32) {
+        // warp 0 adds the partial dots (fixed lanes and shuffle order)
+        double la[N], z[N];
+#pragma unroll
+        for (int m = 0; m < N; ++m) la[m] = 0.0;
+        for (int c = threadIdx.x; c < nparts; c += 32)
+#pragma unroll
+            for (int m = 0; m < N; ++m) la[m] += a.part[c * N + m];
+#pragma unroll
+        for (int m = 0; m < N; ++m) la[m] = __shfl_sync(0xffffffffu, warp_sum(la[m]), 0);
+#pragma unroll
+        for (int c = 0; c < N; ++c) {
+            double v = la[c];
+#pragma unroll
+            for (int r = 0; r < c; ++r) v -= b.lu[r + N * c] * z[r];
+            z[c] = v / b.lu[c + N * c];
+        }
+#pragma unroll
+        for (int c = N - 1; c >= 0; --c) {
+#pragma unroll
+            for (int r = c + 1; r < N; ++r) z[c] -= b.lu[r + N * c] * z[r];
+        }
+#pragma unroll
+        for (int i = N - 1; i >= 0; --i) {
+            const int r = b.piv[i];
+            if (r != i) { const double t = z[i]; z[i] = z[r]; z[r] = t; }
+        }
+        // z = lam_r; r_l = dpi_l - (ik_{l+1} - ik_l)
+        double lik[NL];
+#pragma unroll
+        for (int k = 0; k < NL; ++k) lik[k] = 0.0;
+#pragma unroll
+        for (int l = 0; l < N; ++l) { lik[l + 1] -= z[l]; lik[l] += z[l]; }
+        if (threadIdx.x == 0)
+#pragma unroll
+            for (int m = 0; m < NL; ++m) {
+                double v = 0.0;
+#pragma unroll
+                for (int k = 0; k < NL; ++k) v += b.ctm2l[m + NL * k] * lik[k];
+                lim[m] = v * b.dx * b.dy;
+            }
+        if (blockIdx.x == 0 && threadIdx.x == 0)
+#pragma unroll
+            for (int l = 0; l < N; ++l) {   // dpi' = dpip, dpip' = dpi
+                const double ldpi = a.scal[l];
+                a.scal[l] = a.scal[8 + l];
+                a.scal[8 + l] = ldpi + z[l];
+            }
+    }
+    __syncthreads();
+    const int n = b.nxin, ny = b.ny;
+    const size_t n2 = (size_t)b.nyp * b.px;
+    double *rhs = (double *)b.rhs;
+    for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < (size_t)NL * ny * n;
+         idx += (size_t)gridDim.x * blockDim.x) {
+        const int m = (int)(idx / ((size_t)ny * n));
+        const int rem = (int)(idx - (size_t)m * ny * n);
+        const int jj = rem / n, xi = rem - jj * n;
+        rhs[((size_t)m * ny + jj) * b.pr + xi] = a.nu[m * n2 + (size_t)(jj + 1) * b.px + xi + 1] + lim[m];
+    }
+}
+
+// p_modes_rhs^T and the leapfrog: lam_qnew_k = lam_q_k + f0 sum_m ctl2m(k,m)
+// s_m at interior points, zero on the walls (the step's own wall q is
+// replaced by ocqbdy).
+template <int NL>
+__device__ __forceinline__ double lam_qnew(const BasinDev &b, const AdjFields &a, int k, int i, int j) {
+    if (i <= 0 || i >= b.nxp - 1 || j <= 0 || j >= b.nyp - 1) return 0.0;
+    const size_t n2 = (size_t)b.nyp * b.px, o = (size_t)j * b.px + i;
+    double v = 0.0;
+#pragma unroll
+    for (int m = 0; m < NL; ++m) v += b.ctl2m[k + NL * m] * a.s[m * n2 + o];
+    return a.lq[k * n2 + o] + b.fnot * v;
+}
+
+// vort_step^T, first part: with g = lam_qnew (computed here for the 3x3
+// block around each point from lam_q and the modal solutions s),
+//   lam_qm_in = g                                     (into nu)
+//   lam_q_in  = lam_qm_out + tdt jac_fac t_q^T(g; p)   (into lqm, in place)
+//   lam_p_in  = lam_pm_out + tdt jac_fac t_p^T(g; q)   (into lpm, in place)
+//   t1 = L^T g,  lw += tdt c_wind g_1
+// P, Q: p and q of the step's input state.
+template <int NL>
+__global__ void __launch_bounds__(OQG_ADJ_THREADS) k_adj_vort(const BasinDev *__restrict__ bas, AdjFields a,
+                                                              const double *__restrict__ P,
+                                                              const double *__restrict__ Q, double tdt) {
+    const BasinDev &b = bas[0];
+    const int nxp = b.nxp, nyp = b.nyp, px = b.px;
+    const size_t n2 = (size_t)nyp * px;
+    const double s = tdt * b.jac_fac;
+    for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < (size_t)NL * nyp * nxp;
+         idx += (size_t)gridDim.x * blockDim.x) {
+        const int k = (int)(idx / ((size_t)nyp * nxp));
+        const int rem = (int)(idx - (size_t)k * nyp * nxp);
+        const int j = rem / nxp, i = rem - j * nxp;
+        const size_t o = k * n2 + (size_t)j * px + i;
+        double g3[3][3];   // g at (i + a, j + c), [c + 1][a + 1]
+#pragma unroll
+        for (int c = -1; c <= 1; ++c)
+#pragma unroll
+            for (int e = -1; e <= 1; ++e) g3[c + 1][e + 1] = lam_qnew<NL>(b, a, k, i + e, j + c);
+        const double *p = P + k * n2, *q = Q + k * n2;
+#define AT(f, ii, jj) f[(size_t)(jj) * px + (ii)]
+        double sq = 0.0, sp = 0.0;
+        // every interior y = x - (e, c) whose Arakawa stencil holds x
+#pragma unroll
+        for (int c = -1; c <= 1; ++c)
+#pragma unroll
+            for (int e = -1; e <= 1; ++e) {
+                if (e == 0 && c == 0) continue;   // t(y) does not read q(y) or p(y)
+                const double gy = g3[1 - c][1 - e];
+                if (gy == 0.0) continue;          // walls and outside
+                const int iy = i - e, jy = j - c;
+                double cq, cp;
+                if (c == 0) {          // x = y +- e_x
+                    const double dpy = (AT(p, iy, jy + 1) - AT(p, iy, jy - 1)) + (AT(p, iy + e, jy + 1) - AT(p, iy + e, jy - 1));
+                    const double dqy = (AT(q, iy, jy + 1) - AT(q, iy, jy - 1)) + (AT(q, iy + e, jy + 1) - AT(q, iy + e, jy - 1));
+                    cq = e * dpy;
+                    cp = -e * dqy;
+                } else if (e == 0) {   // x = y +- e_y
+                    const double dpx = (AT(p, iy + 1, jy) - AT(p, iy - 1, jy)) + (AT(p, iy + 1, jy + c) - AT(p, iy - 1, jy + c));
+                    const double dqx = (AT(q, iy + 1, jy) - AT(q, iy - 1, jy)) + (AT(q, iy + 1, jy + c) - AT(q, iy - 1, jy + c));
+                    cq = -c * dpx;
+                    cp = c * dqx;
+                } else {               // diagonal x = y + (e, c)
+                    cq = (double)(e * c) * (AT(p, iy, jy + c) - AT(p, iy + e, jy));
+                    cp = (double)(e * c) * (AT(q, iy + e, jy) - AT(q, iy, jy + c));
+                }
+                sq += cq * gy;
+                sp += cp * gy;
+            }
+#undef AT
+        // L^T g from the cross of g3
+        double t1 = 0.0;
+        {
+            const int di[5] = {0, 1, -1, 0, 0}, dj[5] = {0, 0, 0, 1, -1};
+#pragma unroll
+            for (int t = 0; t < 5; ++t) {
+                const int iy = i + di[t], jy = j + dj[t];
+                const double gy = g3[dj[t] + 1][di[t] + 1];
+                if (gy != 0.0) t1 += lap_weight(b, iy, jy, -di[t], -dj[t]) * gy;
+            }
+        }
+        const double g = g3[1][1];
+        a.nu[o] = g;
+        a.lqm[o] += s * sq;
+        a.lpm[o] += s * sp;
+        a.t1[o] = t1;
+        if (k == 0) a.lw[(size_t)j * px + i] += tdt * b.c_wind * g;
+    }
+}
+
+// vort_step^T, friction and drag: lam_pm_in = tdt (c2 L^T t1 - c4 L^T L^T t1
+// - [k = kt] c_drag t1), the inner L^T t1 taken at the five points of the
+// outer one; written over lp.
+template <int NL>
+__global__ void __launch_bounds__(OQG_ADJ_THREADS) k_adj_fric(const BasinDev *__restrict__ bas, AdjFields a,
+                                                              double tdt) {
+    const BasinDev &b = bas[0];
+    const int nxp = b.nxp, nyp = b.nyp, px = b.px;
+    const size_t n2 = (size_t)nyp * px;
+    for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < (size_t)NL * nyp * nxp;
+         idx += (size_t)gridDim.x * blockDim.x) {
+        const int k = (int)(idx / ((size_t)nyp * nxp));
+        const int rem = (int)(idx - (size_t)k * nyp * nxp);
+        const int j = rem / nxp, i = rem - j * nxp;
+        const size_t o = k * n2 + (size_t)j * px + i;
+        const double *t1 = a.t1 + k * n2;
+        const int di[5] = {0, 1, -1, 0, 0}, dj[5] = {0, 0, 0, 1, -1};
+        double t2c = 0.0, t3 = 0.0;   // (L^T t1)(x), (L^T L^T t1)(x)
+#pragma unroll
+        for (int t = 0; t < 5; ++t) {
+            const int iy = i + di[t], jy = j + dj[t];
+            if (iy < 0 || iy >= nxp || jy < 0 || jy >= nyp) continue;
+            const double w = lap_weight(b, iy, jy, -di[t], -dj[t]);
+            if (t == 0) {
+                t2c = lapT_at(b, t1, iy, jy);
+                t3 += w * t2c;
+            } else if (w != 0.0) {
+                t3 += w * lapT_at(b, t1, iy, jy);
+            }
+        }
+        double v = b.c2[k] * t2c - b.c4[k] * t3;
+        if (k == b.kt) v -= b.c_drag * a.t1[o];
+        a.lp[o] = tdt * v;
+    }
+}
+
+// The transpose of set_state (qcomp, vorsubs.F90:27-56; init_mass_constr,
+// constraint.F90:145-165) applied to the adjoint state:
+//   g_p  = lam_p  + L^T lam_q / f0  - f0 A^T lam_q  + M^T lam_dpi
+//   g_pm = lam_pm + L^T lam_qm / f0 - f0 A^T lam_qm + M^T lam_dpip
+// with M^T d at layer k = dz_sign w (d_k - d_{k-1}) (trapezoid weights w dx dy).
+template <int NL>
+__global__ void __launch_bounds__(OQG_ADJ_THREADS) k_adj_init(const BasinDev *__restrict__ bas, AdjFields a,
+                                                              double *gp, double *gpm) {
+    const BasinDev &b = bas[0];
+    const int nxp = b.nxp, nyp = b.nyp, px = b.px;
+    const size_t n2 = (size_t)nyp * px;
+    for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < (size_t)nyp * nxp;
+         idx += (size_t)gridDim.x * blockDim.x) {
+        const int j = (int)(idx / nxp), i = (int)(idx - (size_t)j * nxp);
+        const size_t o = (size_t)j * px + i;
+        const double w = ((i == 0 || i == nxp - 1) ? 0.5 : 1.0) * ((j == 0 || j == nyp - 1) ? 0.5 : 1.0) * b.dx * b.dy;
+        for (int f = 0; f < 2; ++f) {
+            const double *LP = f ? a.lpm : a.lp, *LQ = f ? a.lqm : a.lq, *LD = a.scal + (f ? 8 : 0);
+            double *G = f ? gpm : gp;
+            double lq[NL];
+#pragma unroll
+            for (int k = 0; k < NL; ++k) lq[k] = LQ[k * n2 + o];
+#pragma unroll
+            for (int l = 0; l < NL; ++l) {
+                double v = LP[l * n2 + o] + lapT_at(b, LQ + l * n2, i, j) / b.fnot;
+                double av = 0.0;
+#pragma unroll
+                for (int k = 0; k < NL; ++k) av += b.amat[k + NL * l] * lq[k];
+                v -= b.fnot * av;
+                const double dl = (l < NL - 1 ? LD[l] : 0.0) - (l > 0 ? LD[l - 1] : 0.0);
+                v += b.dz_sign * w * dl;
+                G[l * n2 + o] = v;
+            }
+        }
+    }
+}
+
+}  // namespace oqg

@@ -7,6 +7,7 @@
 #include "../../include/oqg.h"
 #include "oqg_dev.cuh"
 #include "oqg_kernels.cuh"
+#include "oqg_adjoint.cuh"
 #include "oqg_noalloc.cuh"
 #include "oqg_setup.h"
 
@@ -68,6 +69,8 @@ struct oqg_handle {
     double gbig_tdt[2] = {0.0, 0.0};
     int gbig_n[2] = {0, 0};
     std::vector<double> modes_amat, modes_ctl2m, modes_ctm2l, modes_rdm2;
+    double *adj = nullptr;      // adjoint buffers, made on the first oqg_adj_set
+    AdjFields af{};             // their current roles
 };
 
 template <class X>
@@ -1598,6 +1601,205 @@ int oqg_ensemble_sync(oqg_ensemble *e) {
         CK(cudaMemcpy(&err, e->m[i]->hb.err, sizeof(int), cudaMemcpyDeviceToHost));
         if (err) return fail(OQG_ECUDA, "device error flag set in member " + std::to_string(i));
     }
+    return OQG_OK;
+}
+
+}  // extern "C"
+
+// ===================================================================== adjoint
+// The adjoint of the closed-box FP64 step (kernels in oqg_adjoint.cuh): one
+// reversed step is seven launches on the handle's stream (eight when a
+// suppress_comp_mode is transposed), the modal solve among them being the
+// forward solver's own three kernels.
+template <int NL>
+static void launch_adj_step_t(oqg_handle *h, const double *P, const double *Q, double tdt, bool supp) {
+    AdjFields &a = h->af;
+    const BasinDev *d = h->d_bas64;
+    if (supp) k_adj_suppress<<<OQG_ADJ_CTAS, OQG_ADJ_THREADS, 0, h->st>>>(d, a);
+    k_adj_wall<NL><<<OQG_ADJ_CTAS, OQG_ADJ_THREADS, 0, h->st>>>(d, a);
+    k_adj_rhs<NL><<<OQG_ADJ_CTAS, OQG_ADJ_THREADS, 0, h->st>>>(d, a, OQG_ADJ_CTAS);
+    launch_solve(h, a.s);
+    k_adj_vort<NL><<<OQG_ADJ_CTAS, OQG_ADJ_THREADS, 0, h->st>>>(d, a, P, Q, tdt);
+    k_adj_fric<NL><<<OQG_ADJ_CTAS, OQG_ADJ_THREADS, 0, h->st>>>(d, a, tdt);
+    // the state adjoints change roles: (p, pm, q, qm) of the step's input
+    // (nu now holds lam_qm; the old lam_q buffer becomes the scratch)
+    std::swap(a.lp, a.lpm);
+    double *lq_old = a.lq;
+    a.lq = a.lqm;
+    a.lqm = a.nu;
+    a.nu = lq_old;
+}
+
+static int adj_check(oqg_handle *h, bool need_bufs) {
+    if (!h) return fail(OQG_EINVAL, "null handle");
+    if (h->hb.cyclic || h->mixed)
+        return fail(OQG_EUNSUPPORTED, "the adjoint covers the closed box in FP64 only");
+    if (need_bufs && !h->adj) return fail(OQG_EINVAL, "no adjoint state: call oqg_adj_set first");
+    return OQG_OK;
+}
+
+// (nxp, nyp, nlay) Fortran-order array, host or device memory, <-> pitched field
+static int put_field(oqg_handle *h, const double *src, double *dst, int nlay) {
+    const BasinDev &b = h->hb;
+    CK(cudaMemcpy2DAsync(dst, b.px * sizeof(double), src, b.nxp * sizeof(double), b.nxp * sizeof(double),
+                         (size_t)b.nyp * nlay, cudaMemcpyDefault, h->st));
+    return OQG_OK;
+}
+static int get_field(oqg_handle *h, const double *src, double *dst, int nlay) {
+    const BasinDev &b = h->hb;
+    CK(cudaMemcpy2DAsync(dst, b.nxp * sizeof(double), src, b.px * sizeof(double), b.nxp * sizeof(double),
+                         (size_t)b.nyp * nlay, cudaMemcpyDefault, h->st));
+    return OQG_OK;
+}
+
+static size_t state_field_bytes(const oqg_handle *h) {
+    const BasinDev &b = h->hb;
+    return (size_t)b.nl * b.nyp * b.px * h->esz;
+}
+
+extern "C" {
+
+int oqg_state_bytes(oqg_handle *h, size_t *full, size_t *pq) {
+    if (!h) return fail(OQG_EINVAL, "null handle");
+    const size_t f = state_field_bytes(h);
+    if (full) *full = 4 * f + sizeof(DevState);
+    if (pq) *pq = 2 * f;
+    return OQG_OK;
+}
+
+int oqg_state_save(oqg_handle *h, void *dst) {
+    if (!h || !dst) return fail(OQG_EINVAL, "bad argument");
+    const BasinDev &b = h->hb;
+    const size_t f = state_field_bytes(h);
+    const int par = h->par, src[4] = {par, 1 - par, 2 + par, 3 - par};
+    char *o = (char *)dst;
+    for (int i = 0; i < 4; ++i) CK(cudaMemcpyAsync(o + i * f, b.F[src[i]], f, cudaMemcpyDefault, h->st));
+    CK(cudaMemcpyAsync(o + 4 * f, b.st + par, sizeof(DevState), cudaMemcpyDefault, h->st));
+    return OQG_OK;
+}
+
+int oqg_state_load(oqg_handle *h, const void *src) {
+    if (!h || !src) return fail(OQG_EINVAL, "bad argument");
+    const BasinDev &b = h->hb;
+    const size_t f = state_field_bytes(h);
+    const int par = h->par, dst[4] = {par, 1 - par, 2 + par, 3 - par};
+    const char *s = (const char *)src;
+    for (int i = 0; i < 4; ++i) CK(cudaMemcpyAsync(b.F[dst[i]], s + i * f, f, cudaMemcpyDefault, h->st));
+    CK(cudaMemcpyAsync(b.st + par, s + 4 * f, sizeof(DevState), cudaMemcpyDefault, h->st));
+    return OQG_OK;
+}
+
+int oqg_pq_save(oqg_handle *h, void *dst) {
+    if (!h || !dst) return fail(OQG_EINVAL, "bad argument");
+    const BasinDev &b = h->hb;
+    const size_t f = state_field_bytes(h);
+    CK(cudaMemcpyAsync(dst, b.F[h->par], f, cudaMemcpyDefault, h->st));
+    CK(cudaMemcpyAsync((char *)dst + f, b.F[2 + h->par], f, cudaMemcpyDefault, h->st));
+    return OQG_OK;
+}
+
+int oqg_adj_set(oqg_handle *h, const double *lp, const double *lpm, const double *lq, const double *lqm,
+                const double *ldpi, const double *ldpip) {
+    int rc = adj_check(h, false);
+    if (rc) return rc;
+    const BasinDev &b = h->hb;
+    const size_t n2 = (size_t)b.nyp * b.px, n3 = n2 * b.nl;
+    const size_t nparts = (size_t)OQG_ADJ_CTAS * (b.nl - 1);
+    if (!h->adj) {
+        h->adj = dalloc<double>(h, 7 * n3 + n2 + nparts + 16);
+        if (!h->adj) return fail(OQG_ECUDA, "cudaMalloc of the adjoint buffers failed");
+        double *x = h->adj;
+        AdjFields &a = h->af;
+        a.lp = x; a.lpm = x + n3; a.lq = x + 2 * n3; a.lqm = x + 3 * n3;
+        a.nu = x + 4 * n3; a.s = x + 5 * n3; a.t1 = x + 6 * n3;
+        a.lw = x + 7 * n3; a.part = a.lw + n2; a.scal = a.part + nparts;
+    }
+    const AdjFields &a = h->af;
+    double *dst[4] = {a.lp, a.lpm, a.lq, a.lqm};
+    const double *src[4] = {lp, lpm, lq, lqm};
+    for (int f = 0; f < 4; ++f) {
+        CK(cudaMemsetAsync(dst[f], 0, n3 * sizeof(double), h->st));
+        if (src[f] && (rc = put_field(h, src[f], dst[f], b.nl))) return rc;
+    }
+    CK(cudaMemsetAsync(a.lw, 0, n2 * sizeof(double), h->st));
+    double sc[16] = {0.0};
+    for (int l = 0; l < b.nl - 1; ++l) {
+        sc[l] = ldpi ? ldpi[l] : 0.0;
+        sc[8 + l] = ldpip ? ldpip[l] : 0.0;
+    }
+    CK(cudaMemcpyAsync(a.scal, sc, sizeof sc, cudaMemcpyHostToDevice, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    return OQG_OK;
+}
+
+int oqg_adj_get(oqg_handle *h, double *lp, double *lpm, double *lq, double *lqm, double *ldpi, double *ldpip,
+                double *lwekp) {
+    int rc = adj_check(h, true);
+    if (rc) return rc;
+    const BasinDev &b = h->hb;
+    const AdjFields &a = h->af;
+    const double *src[4] = {a.lp, a.lpm, a.lq, a.lqm};
+    double *dst[4] = {lp, lpm, lq, lqm};
+    for (int f = 0; f < 4; ++f)
+        if (dst[f] && (rc = get_field(h, src[f], dst[f], b.nl))) return rc;
+    if (lwekp && (rc = get_field(h, a.lw, lwekp, 1))) return rc;
+    double sc[16];
+    CK(cudaMemcpyAsync(sc, a.scal, sizeof sc, cudaMemcpyDeviceToHost, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    for (int l = 0; l < b.nl - 1; ++l) {
+        if (ldpi) ldpi[l] = sc[l];
+        if (ldpip) ldpip[l] = sc[8 + l];
+    }
+    return OQG_OK;
+}
+
+int oqg_adj_step(oqg_handle *h, const void *pq, double tdt, long long step_no) {
+    int rc = adj_check(h, true);
+    if (rc) return rc;
+    if (!pq || step_no < 1) return fail(OQG_EINVAL, "bad argument");
+    const BasinDev &b = h->hb;
+    const size_t n3 = (size_t)b.nl * b.nyp * b.px;
+    const double *P = (const double *)pq, *Q = P + n3;
+    const int per = h->prm.suppress_period;
+    const bool supp = per > 0 && (step_no - 1) % per == 0;
+    if (b.nl == 2) launch_adj_step_t<2>(h, P, Q, tdt, supp);
+    else if (b.nl == 3) launch_adj_step_t<3>(h, P, Q, tdt, supp);
+    else launch_adj_step_t<4>(h, P, Q, tdt, supp);
+    CK(cudaGetLastError());
+    return OQG_OK;
+}
+
+int oqg_adj_segment(oqg_handle *h, const void *ckpt, void *slots, size_t slot_stride, int n, double tdt,
+                    long long first_step_no) {
+    int rc = adj_check(h, true);
+    if (rc) return rc;
+    if (!ckpt || !slots || n < 1 || first_step_no < 1) return fail(OQG_EINVAL, "bad argument");
+    size_t pqb = 0;
+    oqg_state_bytes(h, nullptr, &pqb);
+    if (slot_stride < pqb) return fail(OQG_EINVAL, "slot stride smaller than a p-and-q slot");
+    char *sl = (char *)slots;
+    if ((rc = oqg_state_load(h, ckpt))) return rc;
+    for (int i = 0; i < n; ++i) {
+        if ((rc = oqg_pq_save(h, sl + i * slot_stride))) return rc;
+        if (i < n - 1 && (rc = oqg_step(h, tdt, 1))) return rc;
+    }
+    for (int i = n - 1; i >= 0; --i)
+        if ((rc = oqg_adj_step(h, sl + i * slot_stride, tdt, first_step_no + i))) return rc;
+    return OQG_OK;
+}
+
+int oqg_adj_initial(oqg_handle *h, double *gp, double *gpm) {
+    int rc = adj_check(h, true);
+    if (rc) return rc;
+    const BasinDev &b = h->hb;
+    const AdjFields &a = h->af;
+    if (b.nl == 2) k_adj_init<2><<<OQG_ADJ_CTAS, OQG_ADJ_THREADS, 0, h->st>>>(h->d_bas64, a, a.nu, a.s);
+    else if (b.nl == 3) k_adj_init<3><<<OQG_ADJ_CTAS, OQG_ADJ_THREADS, 0, h->st>>>(h->d_bas64, a, a.nu, a.s);
+    else k_adj_init<4><<<OQG_ADJ_CTAS, OQG_ADJ_THREADS, 0, h->st>>>(h->d_bas64, a, a.nu, a.s);
+    CK(cudaGetLastError());
+    if (gp && (rc = get_field(h, a.nu, gp, b.nl))) return rc;
+    if (gpm && (rc = get_field(h, a.s, gpm, b.nl))) return rc;
+    CK(cudaStreamSynchronize(h->st));
     return OQG_OK;
 }
 
