@@ -596,11 +596,19 @@ def main():
     ap.add_argument("--ref-model-steps", type=int, default=2)
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-variants", dest="variants", action="store_false")
+    ap.add_argument("--adjoint-only", action="store_true",
+                    help="time only the adjoint configuration (one repetition of 40 steps) and "
+                         "print its figures; for profiling")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         return run_reference(args)
+    if args.adjoint_only:
+        import torch
+        torch.cuda.set_device(0)
+        print(json.dumps(run_adjoint(reps=1, nsteps=40)), flush=True)
+        return 0
     return run_ours(args)
 
 

@@ -72,10 +72,12 @@ __device__ __forceinline__ double lapT_at(const BasinDev &b, const double *g, in
 
 struct AdjFields {
     double *lp, *lpm, *lq, *lqm;   // adjoint of the state after the step
-    double *nu, *s, *t1;           // scratch: modal adjoint, modal solution, L^T g
+    double *nu, *s, *t1;           // scratch: next lam_qm, modal solution, L^T g
+    double *phi;                   // modal solutions of a unit interior rhs [nl][nyp][px]
     double *lw;                    // accumulated adjoint of wekp [nyp][px]
     double *part;                  // [OQG_ADJ_CTAS][nl-1] partial dots
-    double *scal;                  // lam_dpi [0, 8), lam_dpip [8, 16)
+    double *scal;                  // lam_dpi [0, 8), lam_dpip [8, 16), c_m [16, 24)
+    unsigned int *ticket;          // CTAs of k_adj_wall done (0 between launches)
 };
 
 // suppress_comp_mode^T (driver.F90:174-189): x' = (x + xm)/2 for x = p, q, dpi.
@@ -97,19 +99,44 @@ __global__ void k_adj_suppress(const BasinDev *__restrict__ bas, AdjFields a) {
         }
 }
 
-// ocqbdy^T and modes_to_layers^T: nu_m = sum_k ctm2l(m,k) (lam_p + O^T lam_q)_k
-// at every point, and per-CTA partial dots <hsb_{m-1}, nu_m>, m >= 1.
+// Unit right-hand side on the interior of every mode (for phi).
+__global__ void k_adj_unit_rhs(const BasinDev *__restrict__ bas) {
+    const BasinDev &b = bas[0];
+    double *rhs = (double *)b.rhs;
+    const int n = b.nxin, ny = b.ny;
+    for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < (size_t)b.nl * ny * n;
+         idx += (size_t)gridDim.x * blockDim.x) {
+        const int m = (int)(idx / ((size_t)ny * n));
+        const int rem = (int)(idx - (size_t)m * ny * n);
+        const int jj = rem / n, xi = rem - jj * n;
+        rhs[((size_t)m * ny + jj) * b.pr + xi] = 1.0;
+    }
+}
+
+// ocqbdy^T, modes_to_layers^T and box_homog^T.  Per point
+//   nu_m = sum_k ctm2l(m,k) (lam_p + O^T lam_q)_k,
+// written as the modal solve's right-hand side on the interior; per CTA the
+// partial dots <hsb_{m-1}, nu_m>, m >= 1.  The last CTA to finish adds the
+// partial dots of all CTAs (fixed order), takes the transposed constraint
+// solve (cdhoc^T with the LU of DGETRF: U^T, then L^T, then the row
+// interchanges in reverse) and the adjoint of the modal area integrals,
+// c_m = dx dy sum_k ctm2l(m,k) lam_ik_k: the modal solution's adjoint is
+// then S_m(nu_m) + c_m phi_m, S_m linear and phi_m = S_m(1).  It also
+// carries the constraint adjoints through update_mass_constr.
 template <int NL>
 __global__ void __launch_bounds__(OQG_ADJ_THREADS) k_adj_wall(const BasinDev *__restrict__ bas, AdjFields a) {
     const BasinDev &b = bas[0];
-    const int nxp = b.nxp, nyp = b.nyp, px = b.px;
+    constexpr int N = NL - 1;
+    const int nxp = b.nxp, nyp = b.nyp, px = b.px, ny = b.ny;
     const size_t n2 = (size_t)nyp * px;
     const double fac = b.qb_fac;
     const double *hsb = (const double *)b.hsb;
+    double *rhs = (double *)b.rhs;
     __shared__ double red[32];
-    double dot[NL > 1 ? NL - 1 : 1];
+    __shared__ int last;
+    double dot[N];
 #pragma unroll
-    for (int m = 0; m < NL - 1; ++m) dot[m] = 0.0;
+    for (int m = 0; m < N; ++m) dot[m] = 0.0;
     for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < (size_t)nyp * nxp;
          idx += (size_t)gridDim.x * blockDim.x) {
         const int j = (int)(idx / nxp), i = (int)(idx - (size_t)j * nxp);
@@ -144,110 +171,102 @@ __global__ void __launch_bounds__(OQG_ADJ_THREADS) k_adj_wall(const BasinDev *__
             double v = 0.0;
 #pragma unroll
             for (int k = 0; k < NL; ++k) v += b.ctm2l[m + NL * k] * lpt[k];
-            a.nu[m * n2 + o] = v;
             if (m >= 1) dot[m - 1] += hsb[(m - 1) * n2 + o] * v;
+            if (!cnt) rhs[((size_t)m * ny + j - 1) * b.pr + i - 1] = v;
         }
     }
 #pragma unroll
-    for (int m = 0; m < NL - 1; ++m) {
+    for (int m = 0; m < N; ++m) {
         const double v = block_sum(dot[m], red);
-        if (threadIdx.x == 0) a.part[blockIdx.x * (NL - 1) + m] = v;
+        if (threadIdx.x == 0) a.part[blockIdx.x * N + m] = v;
     }
-}
-
-// box_homog^T: the adjoint of alpha from the partial dots, the transposed
-// constraint solve (cdhoc^T with the LU of DGETRF: U^T, then L^T, then the row
-// interchanges in reverse), the adjoint of the modal area integrals; then
-// the modal right-hand sides rhs_m = nu_m + lam_im_m dx dy on the interior.
-// CTA 0 also carries the constraint adjoints through update_mass_constr.
-template <int NL>
-__global__ void __launch_bounds__(OQG_ADJ_THREADS) k_adj_rhs(const BasinDev *__restrict__ bas, AdjFields a,
-                                                             int nparts) {
-    const BasinDev &b = bas[0];
-    constexpr int N = NL - 1;
-    __shared__ double lim[NL];
-    if (threadIdx.x < 32) {
-        // warp 0 adds the partial dots (fixed lanes and shuffle order)
-        double la[N], z[N];
-#pragma unroll
-        for (int m = 0; m < N; ++m) la[m] = 0.0;
-        for (int c = threadIdx.x; c < nparts; c += 32)
-#pragma unroll
-            for (int m = 0; m < N; ++m) la[m] += a.part[c * N + m];
-#pragma unroll
-        for (int m = 0; m < N; ++m) la[m] = __shfl_sync(0xffffffffu, warp_sum(la[m]), 0);
-#pragma unroll
-        for (int c = 0; c < N; ++c) {
-            double v = la[c];
-#pragma unroll
-            for (int r = 0; r < c; ++r) v -= b.lu[r + N * c] * z[r];
-            z[c] = v / b.lu[c + N * c];
-        }
-#pragma unroll
-        for (int c = N - 1; c >= 0; --c) {
-#pragma unroll
-            for (int r = c + 1; r < N; ++r) z[c] -= b.lu[r + N * c] * z[r];
-        }
-#pragma unroll
-        for (int i = N - 1; i >= 0; --i) {
-            const int r = b.piv[i];
-            if (r != i) { const double t = z[i]; z[i] = z[r]; z[r] = t; }
-        }
-        // z = lam_r; r_l = dpi_l - (ik_{l+1} - ik_l)
-        double lik[NL];
-#pragma unroll
-        for (int k = 0; k < NL; ++k) lik[k] = 0.0;
-#pragma unroll
-        for (int l = 0; l < N; ++l) { lik[l + 1] -= z[l]; lik[l] += z[l]; }
-        if (threadIdx.x == 0)
-#pragma unroll
-            for (int m = 0; m < NL; ++m) {
-                double v = 0.0;
-#pragma unroll
-                for (int k = 0; k < NL; ++k) v += b.ctm2l[m + NL * k] * lik[k];
-                lim[m] = v * b.dx * b.dy;
-            }
-        if (blockIdx.x == 0 && threadIdx.x == 0)
-#pragma unroll
-            for (int l = 0; l < N; ++l) {   // dpi' = dpip, dpip' = dpi
-                const double ldpi = a.scal[l];
-                a.scal[l] = a.scal[8 + l];
-                a.scal[8 + l] = ldpi + z[l];
-            }
+    if (threadIdx.x == 0) {
+        __threadfence();
+        last = atomicAdd(a.ticket, 1u) == gridDim.x - 1;
     }
     __syncthreads();
-    const int n = b.nxin, ny = b.ny;
-    const size_t n2 = (size_t)b.nyp * b.px;
-    double *rhs = (double *)b.rhs;
-    for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < (size_t)NL * ny * n;
-         idx += (size_t)gridDim.x * blockDim.x) {
-        const int m = (int)(idx / ((size_t)ny * n));
-        const int rem = (int)(idx - (size_t)m * ny * n);
-        const int jj = rem / n, xi = rem - jj * n;
-        rhs[((size_t)m * ny + jj) * b.pr + xi] = a.nu[m * n2 + (size_t)(jj + 1) * b.px + xi + 1] + lim[m];
+    if (!last || threadIdx.x >= 32) return;
+    __threadfence();
+    double la[N], z[N];
+#pragma unroll
+    for (int m = 0; m < N; ++m) la[m] = 0.0;
+    for (int c = threadIdx.x; c < (int)gridDim.x; c += 32)
+#pragma unroll
+        for (int m = 0; m < N; ++m) la[m] += __ldcg(a.part + c * N + m);
+#pragma unroll
+    for (int m = 0; m < N; ++m) la[m] = warp_sum(la[m]);
+    if (threadIdx.x != 0) return;
+#pragma unroll
+    for (int c = 0; c < N; ++c) {
+        double v = la[c];
+#pragma unroll
+        for (int r = 0; r < c; ++r) v -= b.lu[r + N * c] * z[r];
+        z[c] = v / b.lu[c + N * c];
     }
+#pragma unroll
+    for (int c = N - 1; c >= 0; --c) {
+#pragma unroll
+        for (int r = c + 1; r < N; ++r) z[c] -= b.lu[r + N * c] * z[r];
+    }
+#pragma unroll
+    for (int i = N - 1; i >= 0; --i) {
+        const int r = b.piv[i];
+        if (r != i) { const double t = z[i]; z[i] = z[r]; z[r] = t; }
+    }
+    // z = lam_r; r_l = dpi_l - (ik_{l+1} - ik_l)
+    double lik[NL];
+#pragma unroll
+    for (int k = 0; k < NL; ++k) lik[k] = 0.0;
+#pragma unroll
+    for (int l = 0; l < N; ++l) { lik[l + 1] -= z[l]; lik[l] += z[l]; }
+#pragma unroll
+    for (int m = 0; m < NL; ++m) {
+        double v = 0.0;
+#pragma unroll
+        for (int k = 0; k < NL; ++k) v += b.ctm2l[m + NL * k] * lik[k];
+        a.scal[16 + m] = v * b.dx * b.dy;
+    }
+#pragma unroll
+    for (int l = 0; l < N; ++l) {   // dpi' = dpip, dpip' = dpi
+        const double ldpi = a.scal[l];
+        a.scal[l] = a.scal[8 + l];
+        a.scal[8 + l] = ldpi + z[l];
+    }
+    *a.ticket = 0u;
 }
 
 // p_modes_rhs^T and the leapfrog: lam_qnew_k = lam_q_k + f0 sum_m ctl2m(k,m)
-// s_m at interior points, zero on the walls (the step's own wall q is
-// replaced by ocqbdy).
+// (s_m + c_m phi_m) at interior points, zero on the walls (the step's own
+// wall q is replaced by ocqbdy).  wk[m] = f0 ctl2m(k,m), wc[m] = wk[m] c_m.
 template <int NL>
-__device__ __forceinline__ double lam_qnew(const BasinDev &b, const AdjFields &a, int k, int i, int j) {
+__device__ __forceinline__ double lam_qnew(const BasinDev &b, const AdjFields &a, const double (&wk)[NL],
+                                           const double (&wc)[NL], int k, int i, int j) {
     if (i <= 0 || i >= b.nxp - 1 || j <= 0 || j >= b.nyp - 1) return 0.0;
     const size_t n2 = (size_t)b.nyp * b.px, o = (size_t)j * b.px + i;
-    double v = 0.0;
+    double v = a.lq[k * n2 + o];
 #pragma unroll
-    for (int m = 0; m < NL; ++m) v += b.ctl2m[k + NL * m] * a.s[m * n2 + o];
-    return a.lq[k * n2 + o] + b.fnot * v;
+    for (int m = 0; m < NL; ++m) v += wk[m] * a.s[m * n2 + o] + wc[m] * a.phi[m * n2 + o];
+    return v;
+}
+
+// The Arakawa sum t(p, q) at the centre of 3x3 blocks P, Q ([dy+1][dx+1]).
+__device__ __forceinline__ double arakawa9(const double (&P)[3][3], const double (&Q)[3][3]) {
+    return (Q[1][2] - Q[1][0]) * (P[2][1] - P[0][1]) - (Q[2][1] - Q[0][1]) * (P[1][2] - P[1][0]) +
+           Q[1][2] * (P[2][2] - P[0][2]) - Q[1][0] * (P[2][0] - P[0][0]) - Q[2][1] * (P[2][2] - P[2][0]) +
+           Q[0][1] * (P[0][2] - P[0][0]) + P[2][1] * (Q[2][2] - Q[2][0]) - P[0][1] * (Q[0][2] - Q[0][0]) -
+           P[1][2] * (Q[2][2] - Q[0][2]) + P[1][0] * (Q[2][0] - Q[0][0]);
 }
 
 // vort_step^T, first part: with g = lam_qnew (computed here for the 3x3
-// block around each point from lam_q and the modal solutions s),
+// block around each point),
 //   lam_qm_in = g                                     (into nu)
 //   lam_q_in  = lam_qm_out + tdt jac_fac t_q^T(g; p)   (into lqm, in place)
 //   lam_p_in  = lam_pm_out + tdt jac_fac t_p^T(g; q)   (into lpm, in place)
 //   t1 = L^T g,  lw += tdt c_wind g_1
-// P, Q: p and q of the step's input state.
+// P, Q: p and q of the step's input state.  Where the whole 3x3 block is
+// interior, the Arakawa sum's skew symmetry (it conserves energy and
+// enstrophy, numerics.F90:340-388) gives t_q^T(g; p) = -t(p, g) and
+// t_p^T(g; q) = -t(g, q), and L^T = L; elsewhere the terms are gathered.
 template <int NL>
 __global__ void __launch_bounds__(OQG_ADJ_THREADS) k_adj_vort(const BasinDev *__restrict__ bas, AdjFields a,
                                                               const double *__restrict__ P,
@@ -256,59 +275,70 @@ __global__ void __launch_bounds__(OQG_ADJ_THREADS) k_adj_vort(const BasinDev *__
     const int nxp = b.nxp, nyp = b.nyp, px = b.px;
     const size_t n2 = (size_t)nyp * px;
     const double s = tdt * b.jac_fac;
-    for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < (size_t)NL * nyp * nxp;
-         idx += (size_t)gridDim.x * blockDim.x) {
-        const int k = (int)(idx / ((size_t)nyp * nxp));
-        const int rem = (int)(idx - (size_t)k * nyp * nxp);
+    const int plane = nyp * nxp;
+    for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < NL * plane; idx += gridDim.x * blockDim.x) {
+        const int k = idx / plane, rem = idx - k * plane;
         const int j = rem / nxp, i = rem - j * nxp;
         const size_t o = k * n2 + (size_t)j * px + i;
-        double g3[3][3];   // g at (i + a, j + c), [c + 1][a + 1]
+        double wk[NL], wc[NL];
+#pragma unroll
+        for (int m = 0; m < NL; ++m) {
+            wk[m] = b.fnot * b.ctl2m[k + NL * m];
+            wc[m] = wk[m] * a.scal[16 + m];
+        }
+        double g3[3][3];   // g at (i + e, j + c), [c + 1][e + 1]
 #pragma unroll
         for (int c = -1; c <= 1; ++c)
 #pragma unroll
-            for (int e = -1; e <= 1; ++e) g3[c + 1][e + 1] = lam_qnew<NL>(b, a, k, i + e, j + c);
+            for (int e = -1; e <= 1; ++e) g3[c + 1][e + 1] = lam_qnew<NL>(b, a, wk, wc, k, i + e, j + c);
         const double *p = P + k * n2, *q = Q + k * n2;
 #define AT(f, ii, jj) f[(size_t)(jj) * px + (ii)]
-        double sq = 0.0, sp = 0.0;
-        // every interior y = x - (e, c) whose Arakawa stencil holds x
+        double sq = 0.0, sp = 0.0, t1 = 0.0;
+        if (i >= 2 && i <= nxp - 3 && j >= 2 && j <= nyp - 3) {
+            double p3[3][3], q3[3][3];
 #pragma unroll
-        for (int c = -1; c <= 1; ++c)
+            for (int c = -1; c <= 1; ++c)
 #pragma unroll
-            for (int e = -1; e <= 1; ++e) {
-                if (e == 0 && c == 0) continue;   // t(y) does not read q(y) or p(y)
-                const double gy = g3[1 - c][1 - e];
-                if (gy == 0.0) continue;          // walls and outside
-                const int iy = i - e, jy = j - c;
-                double cq, cp;
-                if (c == 0) {          // x = y +- e_x
-                    const double dpy = (AT(p, iy, jy + 1) - AT(p, iy, jy - 1)) + (AT(p, iy + e, jy + 1) - AT(p, iy + e, jy - 1));
-                    const double dqy = (AT(q, iy, jy + 1) - AT(q, iy, jy - 1)) + (AT(q, iy + e, jy + 1) - AT(q, iy + e, jy - 1));
-                    cq = e * dpy;
-                    cp = -e * dqy;
-                } else if (e == 0) {   // x = y +- e_y
-                    const double dpx = (AT(p, iy + 1, jy) - AT(p, iy - 1, jy)) + (AT(p, iy + 1, jy + c) - AT(p, iy - 1, jy + c));
-                    const double dqx = (AT(q, iy + 1, jy) - AT(q, iy - 1, jy)) + (AT(q, iy + 1, jy + c) - AT(q, iy - 1, jy + c));
-                    cq = -c * dpx;
-                    cp = c * dqx;
-                } else {               // diagonal x = y + (e, c)
-                    cq = (double)(e * c) * (AT(p, iy, jy + c) - AT(p, iy + e, jy));
-                    cp = (double)(e * c) * (AT(q, iy + e, jy) - AT(q, iy, jy + c));
+                for (int e = -1; e <= 1; ++e) {
+                    p3[c + 1][e + 1] = AT(p, i + e, j + c);
+                    q3[c + 1][e + 1] = AT(q, i + e, j + c);
                 }
-                sq += cq * gy;
-                sp += cp * gy;
-            }
-#undef AT
-        // L^T g from the cross of g3
-        double t1 = 0.0;
-        {
+            sq = -arakawa9(p3, g3);
+            sp = -arakawa9(g3, q3);
+            t1 = b.fx * (g3[1][0] + g3[1][2] - 2.0 * g3[1][1]) + b.fy * (g3[0][1] + g3[2][1] - 2.0 * g3[1][1]);
+        } else {
+            // every interior y = x - (e, c) whose Arakawa stencil holds x
+            for (int c = -1; c <= 1; ++c)
+                for (int e = -1; e <= 1; ++e) {
+                    if (e == 0 && c == 0) continue;   // t(y) does not read q(y) or p(y)
+                    const double gy = g3[1 - c][1 - e];
+                    if (gy == 0.0) continue;          // walls and outside
+                    const int iy = i - e, jy = j - c;
+                    double cq, cp;
+                    if (c == 0) {          // x = y +- e_x
+                        const double dpy = (AT(p, iy, jy + 1) - AT(p, iy, jy - 1)) + (AT(p, iy + e, jy + 1) - AT(p, iy + e, jy - 1));
+                        const double dqy = (AT(q, iy, jy + 1) - AT(q, iy, jy - 1)) + (AT(q, iy + e, jy + 1) - AT(q, iy + e, jy - 1));
+                        cq = e * dpy;
+                        cp = -e * dqy;
+                    } else if (e == 0) {   // x = y +- e_y
+                        const double dpx = (AT(p, iy + 1, jy) - AT(p, iy - 1, jy)) + (AT(p, iy + 1, jy + c) - AT(p, iy - 1, jy + c));
+                        const double dqx = (AT(q, iy + 1, jy) - AT(q, iy - 1, jy)) + (AT(q, iy + 1, jy + c) - AT(q, iy - 1, jy + c));
+                        cq = -c * dpx;
+                        cp = c * dqx;
+                    } else {               // diagonal x = y + (e, c)
+                        cq = (double)(e * c) * (AT(p, iy, jy + c) - AT(p, iy + e, jy));
+                        cp = (double)(e * c) * (AT(q, iy + e, jy) - AT(q, iy, jy + c));
+                    }
+                    sq += cq * gy;
+                    sp += cp * gy;
+                }
             const int di[5] = {0, 1, -1, 0, 0}, dj[5] = {0, 0, 0, 1, -1};
-#pragma unroll
             for (int t = 0; t < 5; ++t) {
-                const int iy = i + di[t], jy = j + dj[t];
                 const double gy = g3[dj[t] + 1][di[t] + 1];
-                if (gy != 0.0) t1 += lap_weight(b, iy, jy, -di[t], -dj[t]) * gy;
+                if (gy != 0.0) t1 += lap_weight(b, i + di[t], j + dj[t], -di[t], -dj[t]) * gy;
             }
         }
+#undef AT
         const double g = g3[1][1];
         a.nu[o] = g;
         a.lqm[o] += s * sq;
@@ -320,32 +350,44 @@ __global__ void __launch_bounds__(OQG_ADJ_THREADS) k_adj_vort(const BasinDev *__
 
 // vort_step^T, friction and drag: lam_pm_in = tdt (c2 L^T t1 - c4 L^T L^T t1
 // - [k = kt] c_drag t1), the inner L^T t1 taken at the five points of the
-// outer one; written over lp.
+// outer one (L^T = L three points or more from the walls); written over lp.
 template <int NL>
 __global__ void __launch_bounds__(OQG_ADJ_THREADS) k_adj_fric(const BasinDev *__restrict__ bas, AdjFields a,
                                                               double tdt) {
     const BasinDev &b = bas[0];
     const int nxp = b.nxp, nyp = b.nyp, px = b.px;
     const size_t n2 = (size_t)nyp * px;
-    for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < (size_t)NL * nyp * nxp;
-         idx += (size_t)gridDim.x * blockDim.x) {
-        const int k = (int)(idx / ((size_t)nyp * nxp));
-        const int rem = (int)(idx - (size_t)k * nyp * nxp);
+    const double fx = b.fx, fy = b.fy;
+    const int plane = nyp * nxp;
+    for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < NL * plane; idx += gridDim.x * blockDim.x) {
+        const int k = idx / plane, rem = idx - k * plane;
         const int j = rem / nxp, i = rem - j * nxp;
         const size_t o = k * n2 + (size_t)j * px + i;
         const double *t1 = a.t1 + k * n2;
-        const int di[5] = {0, 1, -1, 0, 0}, dj[5] = {0, 0, 0, 1, -1};
         double t2c = 0.0, t3 = 0.0;   // (L^T t1)(x), (L^T L^T t1)(x)
-#pragma unroll
-        for (int t = 0; t < 5; ++t) {
-            const int iy = i + di[t], jy = j + dj[t];
-            if (iy < 0 || iy >= nxp || jy < 0 || jy >= nyp) continue;
-            const double w = lap_weight(b, iy, jy, -di[t], -dj[t]);
-            if (t == 0) {
-                t2c = lapT_at(b, t1, iy, jy);
-                t3 += w * t2c;
-            } else if (w != 0.0) {
-                t3 += w * lapT_at(b, t1, iy, jy);
+        if (i >= 3 && i <= nxp - 4 && j >= 3 && j <= nyp - 4) {
+#define T1(ii, jj) t1[(size_t)(j + (jj)) * px + i + (ii)]
+            const double c0 = T1(0, 0), w1 = T1(-1, 0), e1 = T1(1, 0), s1 = T1(0, -1), n1 = T1(0, 1);
+            const double lap_c = fx * (w1 + e1 - 2.0 * c0) + fy * (s1 + n1 - 2.0 * c0);
+            const double lap_w = fx * (T1(-2, 0) + c0 - 2.0 * w1) + fy * (T1(-1, -1) + T1(-1, 1) - 2.0 * w1);
+            const double lap_e = fx * (c0 + T1(2, 0) - 2.0 * e1) + fy * (T1(1, -1) + T1(1, 1) - 2.0 * e1);
+            const double lap_s = fx * (T1(-1, -1) + T1(1, -1) - 2.0 * s1) + fy * (T1(0, -2) + c0 - 2.0 * s1);
+            const double lap_n = fx * (T1(-1, 1) + T1(1, 1) - 2.0 * n1) + fy * (c0 + T1(0, 2) - 2.0 * n1);
+#undef T1
+            t2c = lap_c;
+            t3 = fx * (lap_w + lap_e - 2.0 * lap_c) + fy * (lap_s + lap_n - 2.0 * lap_c);
+        } else {
+            const int di[5] = {0, 1, -1, 0, 0}, dj[5] = {0, 0, 0, 1, -1};
+            for (int t = 0; t < 5; ++t) {
+                const int iy = i + di[t], jy = j + dj[t];
+                if (iy < 0 || iy >= nxp || jy < 0 || jy >= nyp) continue;
+                const double w = lap_weight(b, iy, jy, -di[t], -dj[t]);
+                if (t == 0) {
+                    t2c = lapT_at(b, t1, iy, jy);
+                    t3 += w * t2c;
+                } else if (w != 0.0) {
+                    t3 += w * lapT_at(b, t1, iy, jy);
+                }
             }
         }
         double v = b.c2[k] * t2c - b.c4[k] * t3;
