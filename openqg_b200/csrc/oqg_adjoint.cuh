@@ -72,7 +72,7 @@ __device__ __forceinline__ double lapT_at(const BasinDev &b, const double *g, in
 
 struct AdjFields {
     double *lp, *lpm, *lq, *lqm;   // adjoint of the state after the step
-    double *nu, *s, *t1;           // scratch: next lam_qm, modal solution, L^T g
+    double *nu, *s;                // next lam_qm (scratch between steps), modal solution
     double *phi;                   // modal solutions of a unit interior rhs [nl][nyp][px]
     double *lw;                    // accumulated adjoint of wekp [nyp][px]
     double *part;                  // [OQG_ADJ_CTAS][nl-1] partial dots
@@ -257,142 +257,157 @@ __device__ __forceinline__ double arakawa9(const double (&P)[3][3], const double
            P[1][2] * (Q[2][2] - Q[0][2]) + P[1][0] * (Q[2][0] - Q[0][0]);
 }
 
-// vort_step^T, first part: with g = lam_qnew (computed here for the 3x3
-// block around each point),
-//   lam_qm_in = g                                     (into nu)
-//   lam_q_in  = lam_qm_out + tdt jac_fac t_q^T(g; p)   (into lqm, in place)
-//   lam_p_in  = lam_pm_out + tdt jac_fac t_p^T(g; q)   (into lpm, in place)
-//   t1 = L^T g,  lw += tdt c_wind g_1
-// P, Q: p and q of the step's input state.  Where the whole 3x3 block is
-// interior, the Arakawa sum's skew symmetry (it conserves energy and
-// enstrophy, numerics.F90:340-388) gives t_q^T(g; p) = -t(p, g) and
-// t_p^T(g; q) = -t(g, q), and L^T = L; elsewhere the terms are gathered.
+// vort_step^T, on 2-D tiles of ADJ_TX x ADJ_TY points of one layer.  With
+// g = lam_qnew (staged with a halo of 3),
+//   lam_qm_in = g                                          (into nu)
+//   lam_q_in  = lam_qm_out + tdt jac_fac t_q^T(g; p)        (into lqm, in place)
+//   lam_p_in  = lam_pm_out + tdt jac_fac t_p^T(g; q)        (into lpm, in place)
+//   lam_pm_in = tdt (c2 t2 - c4 t3 - [k = kt] c_drag t1)    (into lp)
+//   lw += tdt c_wind g (layer 1)
+// with t1 = L^T g, t2 = L^T t1, t3 = L^T t2 built in shared memory (halos
+// 2, 1, 0).  g is zero off the interior, so t1 is the plain five-point sum
+// of g; the wall rows of L enter t2 and t3.  P, Q: p and q of the step's
+// input state (halo 1: every term of the Arakawa sum's transpose reads the
+// 3x3 block around its point).  Where that block is interior, the sum's skew
+// symmetry (it conserves energy and enstrophy, numerics.F90:340-388) gives
+// t_q^T(g; p) = -t(p, g) and t_p^T(g; q) = -t(g, q).
+#define ADJ_TX 32
+#define ADJ_TY 16
+
 template <int NL>
-__global__ void __launch_bounds__(OQG_ADJ_THREADS) k_adj_vort(const BasinDev *__restrict__ bas, AdjFields a,
-                                                              const double *__restrict__ P,
-                                                              const double *__restrict__ Q, double tdt) {
+__global__ void __launch_bounds__(256, 3) k_adj_vort(const BasinDev *__restrict__ bas, AdjFields a,
+                                                  const double *__restrict__ P, const double *__restrict__ Q,
+                                                  double tdt, int tiles_x, int tiles_y) {
     const BasinDev &b = bas[0];
     const int nxp = b.nxp, nyp = b.nyp, px = b.px;
     const size_t n2 = (size_t)nyp * px;
-    const double s = tdt * b.jac_fac;
-    const int plane = nyp * nxp;
-    for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < NL * plane; idx += gridDim.x * blockDim.x) {
-        const int k = idx / plane, rem = idx - k * plane;
-        const int j = rem / nxp, i = rem - j * nxp;
-        const size_t o = k * n2 + (size_t)j * px + i;
-        double wk[NL], wc[NL];
+    constexpr int GW = ADJ_TX + 6, GH = ADJ_TY + 6;   // g, halo 3
+    constexpr int AW = ADJ_TX + 4, AH = ADJ_TY + 4;   // t1, halo 2
+    constexpr int BW = ADJ_TX + 2, BH = ADJ_TY + 2;   // t2, p, q, halo 1
+    __shared__ double G[GH][GW], T1[AH][AW], T2[BH][BW], Ps[BH][BW], Qs[BH][BW];
+    const int tile = blockIdx.x % (tiles_x * tiles_y), k = blockIdx.x / (tiles_x * tiles_y);
+    const int x0 = (tile % tiles_x) * ADJ_TX, y0 = (tile / tiles_x) * ADJ_TY;
+    const double fx = b.fx, fy = b.fy;
+    double wk[NL], wc[NL];
 #pragma unroll
-        for (int m = 0; m < NL; ++m) {
-            wk[m] = b.fnot * b.ctl2m[k + NL * m];
-            wc[m] = wk[m] * a.scal[16 + m];
+    for (int m = 0; m < NL; ++m) {
+        wk[m] = b.fnot * b.ctl2m[k + NL * m];
+        wc[m] = wk[m] * a.scal[16 + m];
+    }
+    const double *p = P + k * n2, *q = Q + k * n2;
+    for (int e = threadIdx.x; e < GH * GW; e += blockDim.x) {
+        const int r = e / GW, c = e - r * GW;
+        G[r][c] = lam_qnew<NL>(b, a, wk, wc, k, x0 - 3 + c, y0 - 3 + r);
+    }
+    for (int e = threadIdx.x; e < BH * BW; e += blockDim.x) {
+        const int r = e / BW, c = e - r * BW;
+        const int i = x0 - 1 + c, j = y0 - 1 + r;
+        const bool in = i >= 0 && i < nxp && j >= 0 && j < nyp;
+        Ps[r][c] = in ? p[(size_t)j * px + i] : 0.0;
+        Qs[r][c] = in ? q[(size_t)j * px + i] : 0.0;
+    }
+    __syncthreads();
+    // t1 = L^T g: g vanishes off the interior, where L's rows are the plain ones
+    for (int e = threadIdx.x; e < AH * AW; e += blockDim.x) {
+        const int r = e / AW, c = e - r * AW;
+        const int i = x0 - 2 + c, j = y0 - 2 + r;
+        double v = 0.0;
+        if (i >= 0 && i < nxp && j >= 0 && j < nyp)
+            v = fx * (G[r + 1][c] + G[r + 1][c + 2] - 2.0 * G[r + 1][c + 1]) +
+                fy * (G[r][c + 1] + G[r + 2][c + 1] - 2.0 * G[r + 1][c + 1]);
+        T1[r][c] = v;
+    }
+    __syncthreads();
+    // t2 = L^T t1 (the wall rows of L enter here)
+    const int di[5] = {0, 1, -1, 0, 0}, dj[5] = {0, 0, 0, 1, -1};
+    for (int e = threadIdx.x; e < BH * BW; e += blockDim.x) {
+        const int r = e / BW, c = e - r * BW;
+        const int i = x0 - 1 + c, j = y0 - 1 + r;
+        double v = 0.0;
+        if (i >= 2 && i <= nxp - 3 && j >= 2 && j <= nyp - 3) {
+            v = fx * (T1[r + 1][c] + T1[r + 1][c + 2] - 2.0 * T1[r + 1][c + 1]) +
+                fy * (T1[r][c + 1] + T1[r + 2][c + 1] - 2.0 * T1[r + 1][c + 1]);
+        } else if (i >= 0 && i < nxp && j >= 0 && j < nyp) {
+#pragma unroll
+            for (int t = 0; t < 5; ++t) {
+                const int iy = i + di[t], jy = j + dj[t];
+                if (iy < 0 || iy >= nxp || jy < 0 || jy >= nyp) continue;
+                v += lap_weight(b, iy, jy, -di[t], -dj[t]) * T1[r + 1 + dj[t]][c + 1 + di[t]];
+            }
         }
-        double g3[3][3];   // g at (i + e, j + c), [c + 1][e + 1]
+        T2[r][c] = v;
+    }
+    __syncthreads();
+    const double s = tdt * b.jac_fac;
+    const int cx = threadIdx.x & 31;
+    for (int ry = threadIdx.x >> 5; ry < ADJ_TY; ry += 8) {
+        const int i = x0 + cx, j = y0 + ry;
+        if (i >= nxp || j >= nyp) continue;
+        const int rg = ry + 3, cg = cx + 3;   // in G
+        const int rb = ry + 1, cb = cx + 1;   // in T2, Ps, Qs
+        double g3[3][3], p3[3][3], q3[3][3];
 #pragma unroll
         for (int c = -1; c <= 1; ++c)
 #pragma unroll
-            for (int e = -1; e <= 1; ++e) g3[c + 1][e + 1] = lam_qnew<NL>(b, a, wk, wc, k, i + e, j + c);
-        const double *p = P + k * n2, *q = Q + k * n2;
-#define AT(f, ii, jj) f[(size_t)(jj) * px + (ii)]
-        double sq = 0.0, sp = 0.0, t1 = 0.0;
+            for (int e = -1; e <= 1; ++e) {
+                g3[c + 1][e + 1] = G[rg + c][cg + e];
+                p3[c + 1][e + 1] = Ps[rb + c][cb + e];
+                q3[c + 1][e + 1] = Qs[rb + c][cb + e];
+            }
+        double sq = 0.0, sp = 0.0, t3 = 0.0;
         if (i >= 2 && i <= nxp - 3 && j >= 2 && j <= nyp - 3) {
-            double p3[3][3], q3[3][3];
-#pragma unroll
-            for (int c = -1; c <= 1; ++c)
-#pragma unroll
-                for (int e = -1; e <= 1; ++e) {
-                    p3[c + 1][e + 1] = AT(p, i + e, j + c);
-                    q3[c + 1][e + 1] = AT(q, i + e, j + c);
-                }
             sq = -arakawa9(p3, g3);
             sp = -arakawa9(g3, q3);
-            t1 = b.fx * (g3[1][0] + g3[1][2] - 2.0 * g3[1][1]) + b.fy * (g3[0][1] + g3[2][1] - 2.0 * g3[1][1]);
+            t3 = fx * (T2[rb][cb - 1] + T2[rb][cb + 1] - 2.0 * T2[rb][cb]) +
+                 fy * (T2[rb - 1][cb] + T2[rb + 1][cb] - 2.0 * T2[rb][cb]);
         } else {
-            // every interior y = x - (e, c) whose Arakawa stencil holds x
+            // every interior y = x - (e, c) whose Arakawa stencil holds x;
+            // P3, Q3 index the 3x3 block around x
+#define P3(ii, jj) p3[(jj) + 1][(ii) + 1]
+#define Q3(ii, jj) q3[(jj) + 1][(ii) + 1]
+#pragma unroll
             for (int c = -1; c <= 1; ++c)
+#pragma unroll
                 for (int e = -1; e <= 1; ++e) {
                     if (e == 0 && c == 0) continue;   // t(y) does not read q(y) or p(y)
                     const double gy = g3[1 - c][1 - e];
                     if (gy == 0.0) continue;          // walls and outside
-                    const int iy = i - e, jy = j - c;
                     double cq, cp;
-                    if (c == 0) {          // x = y +- e_x
-                        const double dpy = (AT(p, iy, jy + 1) - AT(p, iy, jy - 1)) + (AT(p, iy + e, jy + 1) - AT(p, iy + e, jy - 1));
-                        const double dqy = (AT(q, iy, jy + 1) - AT(q, iy, jy - 1)) + (AT(q, iy + e, jy + 1) - AT(q, iy + e, jy - 1));
+                    if (c == 0) {          // x = y + (e, 0), y = x - (e, 0)
+                        const double dpy = (P3(-e, 1) - P3(-e, -1)) + (P3(0, 1) - P3(0, -1));
+                        const double dqy = (Q3(-e, 1) - Q3(-e, -1)) + (Q3(0, 1) - Q3(0, -1));
                         cq = e * dpy;
                         cp = -e * dqy;
-                    } else if (e == 0) {   // x = y +- e_y
-                        const double dpx = (AT(p, iy + 1, jy) - AT(p, iy - 1, jy)) + (AT(p, iy + 1, jy + c) - AT(p, iy - 1, jy + c));
-                        const double dqx = (AT(q, iy + 1, jy) - AT(q, iy - 1, jy)) + (AT(q, iy + 1, jy + c) - AT(q, iy - 1, jy + c));
+                    } else if (e == 0) {   // x = y + (0, c)
+                        const double dpx = (P3(1, -c) - P3(-1, -c)) + (P3(1, 0) - P3(-1, 0));
+                        const double dqx = (Q3(1, -c) - Q3(-1, -c)) + (Q3(1, 0) - Q3(-1, 0));
                         cq = -c * dpx;
                         cp = c * dqx;
                     } else {               // diagonal x = y + (e, c)
-                        cq = (double)(e * c) * (AT(p, iy, jy + c) - AT(p, iy + e, jy));
-                        cp = (double)(e * c) * (AT(q, iy + e, jy) - AT(q, iy, jy + c));
+                        cq = (double)(e * c) * (P3(-e, 0) - P3(0, -c));
+                        cp = (double)(e * c) * (Q3(0, -c) - Q3(-e, 0));
                     }
                     sq += cq * gy;
                     sp += cp * gy;
                 }
-            const int di[5] = {0, 1, -1, 0, 0}, dj[5] = {0, 0, 0, 1, -1};
+#undef P3
+#undef Q3
+#pragma unroll
             for (int t = 0; t < 5; ++t) {
-                const double gy = g3[dj[t] + 1][di[t] + 1];
-                if (gy != 0.0) t1 += lap_weight(b, i + di[t], j + dj[t], -di[t], -dj[t]) * gy;
+                const int iy = i + di[t], jy = j + dj[t];
+                if (iy < 0 || iy >= nxp || jy < 0 || jy >= nyp) continue;
+                t3 += lap_weight(b, iy, jy, -di[t], -dj[t]) * T2[rb + dj[t]][cb + di[t]];
             }
         }
-#undef AT
+        const size_t o = k * n2 + (size_t)j * px + i;
         const double g = g3[1][1];
         a.nu[o] = g;
         a.lqm[o] += s * sq;
         a.lpm[o] += s * sp;
-        a.t1[o] = t1;
-        if (k == 0) a.lw[(size_t)j * px + i] += tdt * b.c_wind * g;
-    }
-}
-
-// vort_step^T, friction and drag: lam_pm_in = tdt (c2 L^T t1 - c4 L^T L^T t1
-// - [k = kt] c_drag t1), the inner L^T t1 taken at the five points of the
-// outer one (L^T = L three points or more from the walls); written over lp.
-template <int NL>
-__global__ void __launch_bounds__(OQG_ADJ_THREADS) k_adj_fric(const BasinDev *__restrict__ bas, AdjFields a,
-                                                              double tdt) {
-    const BasinDev &b = bas[0];
-    const int nxp = b.nxp, nyp = b.nyp, px = b.px;
-    const size_t n2 = (size_t)nyp * px;
-    const double fx = b.fx, fy = b.fy;
-    const int plane = nyp * nxp;
-    for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < NL * plane; idx += gridDim.x * blockDim.x) {
-        const int k = idx / plane, rem = idx - k * plane;
-        const int j = rem / nxp, i = rem - j * nxp;
-        const size_t o = k * n2 + (size_t)j * px + i;
-        const double *t1 = a.t1 + k * n2;
-        double t2c = 0.0, t3 = 0.0;   // (L^T t1)(x), (L^T L^T t1)(x)
-        if (i >= 3 && i <= nxp - 4 && j >= 3 && j <= nyp - 4) {
-#define T1(ii, jj) t1[(size_t)(j + (jj)) * px + i + (ii)]
-            const double c0 = T1(0, 0), w1 = T1(-1, 0), e1 = T1(1, 0), s1 = T1(0, -1), n1 = T1(0, 1);
-            const double lap_c = fx * (w1 + e1 - 2.0 * c0) + fy * (s1 + n1 - 2.0 * c0);
-            const double lap_w = fx * (T1(-2, 0) + c0 - 2.0 * w1) + fy * (T1(-1, -1) + T1(-1, 1) - 2.0 * w1);
-            const double lap_e = fx * (c0 + T1(2, 0) - 2.0 * e1) + fy * (T1(1, -1) + T1(1, 1) - 2.0 * e1);
-            const double lap_s = fx * (T1(-1, -1) + T1(1, -1) - 2.0 * s1) + fy * (T1(0, -2) + c0 - 2.0 * s1);
-            const double lap_n = fx * (T1(-1, 1) + T1(1, 1) - 2.0 * n1) + fy * (c0 + T1(0, 2) - 2.0 * n1);
-#undef T1
-            t2c = lap_c;
-            t3 = fx * (lap_w + lap_e - 2.0 * lap_c) + fy * (lap_s + lap_n - 2.0 * lap_c);
-        } else {
-            const int di[5] = {0, 1, -1, 0, 0}, dj[5] = {0, 0, 0, 1, -1};
-            for (int t = 0; t < 5; ++t) {
-                const int iy = i + di[t], jy = j + dj[t];
-                if (iy < 0 || iy >= nxp || jy < 0 || jy >= nyp) continue;
-                const double w = lap_weight(b, iy, jy, -di[t], -dj[t]);
-                if (t == 0) {
-                    t2c = lapT_at(b, t1, iy, jy);
-                    t3 += w * t2c;
-                } else if (w != 0.0) {
-                    t3 += w * lapT_at(b, t1, iy, jy);
-                }
-            }
-        }
-        double v = b.c2[k] * t2c - b.c4[k] * t3;
-        if (k == b.kt) v -= b.c_drag * a.t1[o];
+        double v = b.c2[k] * T2[rb][cb] - b.c4[k] * t3;
+        if (k == b.kt) v -= b.c_drag * T1[ry + 2][cx + 2];
         a.lp[o] = tdt * v;
+        if (k == 0) a.lw[(size_t)j * px + i] += tdt * b.c_wind * g;
     }
 }
 

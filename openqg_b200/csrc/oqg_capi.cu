@@ -1608,7 +1608,7 @@ int oqg_ensemble_sync(oqg_ensemble *e) {
 
 // ===================================================================== adjoint
 // The adjoint of the closed-box FP64 step (kernels in oqg_adjoint.cuh): one
-// reversed step is six launches on the handle's stream (seven when a
+// reversed step is five launches on the handle's stream (six when a
 // suppress_comp_mode is transposed), the modal solve among them being the
 // forward solver's own three kernels.
 template <int NL>
@@ -1621,8 +1621,8 @@ static void launch_adj_step_t(oqg_handle *h, const double *P, const double *Q, d
     if (supp) k_adj_suppress<<<gl, OQG_ADJ_THREADS, 0, h->st>>>(d, a);
     k_adj_wall<NL><<<OQG_ADJ_CTAS, OQG_ADJ_THREADS, 0, h->st>>>(d, a);
     launch_solve(h, a.s);
-    k_adj_vort<NL><<<gl, OQG_ADJ_THREADS, 0, h->st>>>(d, a, P, Q, tdt);
-    k_adj_fric<NL><<<gl, OQG_ADJ_THREADS, 0, h->st>>>(d, a, tdt);
+    const int tx = (b.nxp + ADJ_TX - 1) / ADJ_TX, ty = (b.nyp + ADJ_TY - 1) / ADJ_TY;
+    k_adj_vort<NL><<<tx * ty * NL, 256, 0, h->st>>>(d, a, P, Q, tdt, tx, ty);
     // the state adjoints change roles: (p, pm, q, qm) of the step's input
     // (nu now holds lam_qm; the old lam_q buffer becomes the scratch)
     std::swap(a.lp, a.lpm);
@@ -1708,13 +1708,13 @@ int oqg_adj_set(oqg_handle *h, const double *lp, const double *lpm, const double
     const size_t n2 = (size_t)b.nyp * b.px, n3 = n2 * b.nl;
     const size_t nparts = (size_t)OQG_ADJ_CTAS * (b.nl - 1);
     if (!h->adj) {
-        h->adj = dalloc<double>(h, 8 * n3 + n2 + nparts + 32 + 1);
+        h->adj = dalloc<double>(h, 7 * n3 + n2 + nparts + 32 + 1);
         if (!h->adj) return fail(OQG_ECUDA, "cudaMalloc of the adjoint buffers failed");
         double *x = h->adj;
         AdjFields &a = h->af;
         a.lp = x; a.lpm = x + n3; a.lq = x + 2 * n3; a.lqm = x + 3 * n3;
-        a.nu = x + 4 * n3; a.s = x + 5 * n3; a.t1 = x + 6 * n3; a.phi = x + 7 * n3;
-        a.lw = x + 8 * n3; a.part = a.lw + n2; a.scal = a.part + nparts;
+        a.nu = x + 4 * n3; a.s = x + 5 * n3; a.phi = x + 6 * n3;
+        a.lw = x + 7 * n3; a.part = a.lw + n2; a.scal = a.part + nparts;
         a.ticket = (unsigned int *)(a.scal + 32);
         // phi_m = S_m(1): the modal solutions of a unit interior rhs
         k_adj_unit_rhs<<<OQG_ADJ_CTAS, OQG_ADJ_THREADS, 0, h->st>>>(h->d_bas64);
