@@ -120,20 +120,24 @@ def run_ensemble(precision, steps, warmup, msteps, flush, tdt=3600.0):
     return cells, total
 
 
-def run_adjoint(reps=3, nsteps=200, every=20, tdt=3600.0):
-    """The differentiable configuration: 3-layer ocean box at 257x257, dx
-    20 km, 200 leapfrog steps, J = ekei(1) of the final state, gradients with
-    respect to the initial stream function and the wind forcing, checkpoint
-    every 20 steps with recomputation.  Device times between CUDA events on
-    the handle's stream (host waits inside a pass included) of the plain
-    forward run, the checkpointed forward, the reverse pass (recompute +
-    adjoint) and 200 adjoint steps alone; medians over reps after one
-    untimed repetition."""
+# box sizes of the adjoint runs: n -> (dx, ah4, tdt)
+ADJOINT_BOXES = {257: (20e3, 2.0e10, 3600.0), 1025: (5e3, 1.0e9, 1200.0), 2049: (5e3, 1.0e9, 1200.0)}
+
+
+def run_adjoint(reps=3, n=257, dx=20e3, ah4=2.0e10, nsteps=200, every=20, tdt=3600.0):
+    """The differentiable configuration (default: 3-layer ocean box at
+    257x257, dx 20 km, 200 leapfrog steps, checkpoint every 20 steps with
+    recomputation), J = ekei(1) of the final state, gradients with respect to
+    the initial stream function and the wind forcing.  Device times between
+    CUDA events on the handle's stream (host waits inside a pass included) of
+    the plain forward run, the checkpointed forward, the reverse pass
+    (recompute + adjoint) and nsteps adjoint steps alone; medians over reps
+    after one untimed repetition."""
     import torch
     from openqg_b200.adjoint import AdjointRun, ekei
     from openqg_b200.core import QG, lib
     from openqg_b200.params import ocean_double_gyre
-    b = ocean_double_gyre(257, dx=20e3)
+    b = ocean_double_gyre(n, dx=dx, ah4=ah4)
     p, w, ts, tn = initial_inputs(b, seed=5)
     g = QG(b)
     g.set_forcing(w, None, ts, tn)
@@ -168,8 +172,11 @@ def run_adjoint(reps=3, nsteps=200, every=20, tdt=3600.0):
         L.oqg_pq_save(g.h, slot)
 
         def adj_only():
+            # an NVTX range marks these launches for a profiler's filter
+            torch.cuda.nvtx.range_push("adjoint_steps")
             for i in range(nsteps):
                 L.oqg_adj_step(g.h, slot, ctypes.c_double(tdt), ctypes.c_longlong(2 + i % 20))
+            torch.cuda.nvtx.range_pop()
 
         adj.append(timed(adj_only))
     g.close()
@@ -177,8 +184,9 @@ def run_adjoint(reps=3, nsteps=200, every=20, tdt=3600.0):
     if not math.isfinite(gnorm):
         raise RuntimeError("non-finite adjoint gradient")
     f, c, r, a = med(fwd), med(ck), med(bwd), med(adj)
-    return {"workload": "ocean 257x257x3 box, dx 20 km, %d steps, checkpoint every %d, J = ekei(1), "
-                        "gradient w.r.t. initial psi and wind forcing" % (nsteps, every),
+    return {"workload": "ocean %dx%dx3 box, dx %g km, ah4 %g, tdt %g s, %d steps, checkpoint every %d, "
+                        "J = ekei(1), gradient w.r.t. initial psi and wind forcing"
+                        % (n, n, dx / 1e3, ah4, tdt, nsteps, every),
             "forward_ms_per_step": f, "checkpointed_forward_ms_per_step": c,
             "reverse_ms_per_step": r, "adjoint_step_ms": a,
             "reverse_over_forward": r / f, "adjoint_step_over_forward_step": a / f,
@@ -520,6 +528,9 @@ def run_ours(args):
                                        "cell-layers per step" % (list(ENSEMBLE_SIZES), cells_e))
         # the adjoint: reverse pass and adjoint step against the forward step
         variants["adjoint257"] = run_adjoint()
+        # the eddy-resolving box: forward + adjoint over 100 steps, checkpoint every 10
+        dx, ah4, tdt = ADJOINT_BOXES[2049]
+        variants["adjoint2049"] = run_adjoint(reps=1, n=2049, dx=dx, ah4=ah4, nsteps=100, every=10, tdt=tdt)
 
     # dominant kernel, timed alone, against the HBM roofline
     g.set_forcing(w, None, ts, tn)
@@ -599,6 +610,8 @@ def main():
     ap.add_argument("--adjoint-only", action="store_true",
                     help="time only the adjoint configuration (one repetition of 40 steps) and "
                          "print its figures; for profiling")
+    ap.add_argument("--adjoint-n", type=int, default=257, choices=sorted(ADJOINT_BOXES),
+                    help="box size of --adjoint-only")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -607,7 +620,9 @@ def main():
     if args.adjoint_only:
         import torch
         torch.cuda.set_device(0)
-        print(json.dumps(run_adjoint(reps=1, nsteps=40)), flush=True)
+        dx, ah4, tdt = ADJOINT_BOXES[args.adjoint_n]
+        print(json.dumps(run_adjoint(reps=1, n=args.adjoint_n, dx=dx, ah4=ah4, nsteps=40, every=20, tdt=tdt)),
+              flush=True)
         return 0
     return run_ours(args)
 

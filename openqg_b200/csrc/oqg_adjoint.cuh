@@ -82,6 +82,8 @@ struct AdjFields {
 
 // suppress_comp_mode^T (driver.F90:174-189): x' = (x + xm)/2 for x = p, q, dpi.
 __global__ void k_adj_suppress(const BasinDev *__restrict__ bas, AdjFields a) {
+    pdl_trigger();
+    pdl_wait();
     const BasinDev &b = bas[0];
     const size_t n = (size_t)b.nl * b.nyp * b.px;
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
@@ -125,6 +127,8 @@ __global__ void k_adj_unit_rhs(const BasinDev *__restrict__ bas) {
 // carries the constraint adjoints through update_mass_constr.
 template <int NL>
 __global__ void __launch_bounds__(OQG_ADJ_THREADS) k_adj_wall(const BasinDev *__restrict__ bas, AdjFields a) {
+    pdl_trigger();
+    pdl_wait();
     const BasinDev &b = bas[0];
     constexpr int N = NL - 1;
     const int nxp = b.nxp, nyp = b.nyp, px = b.px, ny = b.ny;
@@ -278,6 +282,8 @@ template <int NL>
 __global__ void __launch_bounds__(256, 3) k_adj_vort(const BasinDev *__restrict__ bas, AdjFields a,
                                                   const double *__restrict__ P, const double *__restrict__ Q,
                                                   double tdt, int tiles_x, int tiles_y) {
+    pdl_trigger();
+    pdl_wait();
     const BasinDev &b = bas[0];
     const int nxp = b.nxp, nyp = b.nyp, px = b.px;
     const size_t n2 = (size_t)nyp * px;

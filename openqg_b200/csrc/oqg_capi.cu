@@ -134,9 +134,21 @@ static void launch_step_t(oqg_handle *h, int par, double tdt) {
 }
 
 // FP64 solve of the modal Helmholtz problems with the rhs buffer as input;
-// modal solutions into out ([nl][nyp][px] FP64).
+// modal solutions into out ([nl][nyp][px] FP64).  pdl: launched with
+// programmatic stream serialisation (each kernel waits for its predecessor
+// in griddepcontrol.wait before its first dependent read).
 template <int NL, int E>
-static void launch_solve_t(oqg_handle *h, double *out) {
+static void launch_solve_t(oqg_handle *h, double *out, bool pdl) {
+    if (pdl) {
+        launch_pdl(k_xfwd<double, E>, h->nx, h->xthreads, h->smem_x64, h->st, h->d_bas64, h->d_wx,
+                   (const void *)nullptr);
+        if (h->hb.cyclic)
+            launch_pdl(k_ysolve<double, true, NL>, h->nys, 32 * h->KB, h->smem_y, h->st, h->d_bas64, h->d_wy);
+        else
+            launch_pdl(k_ysolve<double, false, NL>, h->nys, 32 * h->KB, h->smem_y, h->st, h->d_bas64, h->d_wy);
+        launch_pdl(k_xinv<double, NL>, h->ni, h->xi_threads, h->smem_i64, h->st, h->d_bas64, h->d_wi, 0, 0.0, out);
+        return;
+    }
     k_xfwd<double, E><<<h->nx, h->xthreads, h->smem_x64, h->st>>>(h->d_bas64, h->d_wx, nullptr);
     if (h->hb.cyclic)
         k_ysolve<double, true, NL><<<h->nys, 32 * h->KB, h->smem_y, h->st>>>(h->d_bas64, h->d_wy);
@@ -202,11 +214,11 @@ static void set_attrs_t(oqg_handle *h) {
 static void launch_step(oqg_handle *h, int par, double tdt) { OQG_DISPATCH(launch_step_t, h, h, par, tdt); }
 static void set_attrs(oqg_handle *h) { OQG_DISPATCH(set_attrs_t, h, h); }
 
-static void launch_solve(oqg_handle *h, double *out) {
+static void launch_solve(oqg_handle *h, double *out, bool pdl = false) {
     const int nl = h->hb.nl;
-    if (nl == 2) { if (h->E == 8) launch_solve_t<2, 8>(h, out); else launch_solve_t<2, 16>(h, out); }
-    else if (nl == 3) { if (h->E == 8) launch_solve_t<3, 8>(h, out); else launch_solve_t<3, 16>(h, out); }
-    else { if (h->E == 8) launch_solve_t<4, 8>(h, out); else launch_solve_t<4, 16>(h, out); }
+    if (nl == 2) { if (h->E == 8) launch_solve_t<2, 8>(h, out, pdl); else launch_solve_t<2, 16>(h, out, pdl); }
+    else if (nl == 3) { if (h->E == 8) launch_solve_t<3, 8>(h, out, pdl); else launch_solve_t<3, 16>(h, out, pdl); }
+    else { if (h->E == 8) launch_solve_t<4, 8>(h, out, pdl); else launch_solve_t<4, 16>(h, out, pdl); }
 }
 
 #define OQG_NL_T(FN, h, ...)                                                                   \
@@ -1618,11 +1630,14 @@ static void launch_adj_step_t(oqg_handle *h, const double *P, const double *Q, d
     const BasinDev &b = h->hb;
     // one point of one layer per thread
     const int gl = std::min((NL * b.nyp * b.nxp + OQG_ADJ_THREADS - 1) / OQG_ADJ_THREADS, 148 * 64);
-    if (supp) k_adj_suppress<<<gl, OQG_ADJ_THREADS, 0, h->st>>>(d, a);
-    k_adj_wall<NL><<<OQG_ADJ_CTAS, OQG_ADJ_THREADS, 0, h->st>>>(d, a);
-    launch_solve(h, a.s);
+    // a chain with programmatic stream serialisation: every kernel waits in
+    // griddepcontrol.wait before it touches memory, and every CTA of the
+    // chain waits before it exits, so a wait covers all earlier kernels
+    if (supp) launch_pdl(k_adj_suppress, gl, OQG_ADJ_THREADS, 0, h->st, d, a);
+    launch_pdl(k_adj_wall<NL>, OQG_ADJ_CTAS, OQG_ADJ_THREADS, 0, h->st, d, a);
+    launch_solve(h, a.s, true);
     const int tx = (b.nxp + ADJ_TX - 1) / ADJ_TX, ty = (b.nyp + ADJ_TY - 1) / ADJ_TY;
-    k_adj_vort<NL><<<tx * ty * NL, 256, 0, h->st>>>(d, a, P, Q, tdt, tx, ty);
+    launch_pdl(k_adj_vort<NL>, tx * ty * NL, 256, 0, h->st, d, a, P, Q, tdt, tx, ty);
     // the state adjoints change roles: (p, pm, q, qm) of the step's input
     // (nu now holds lam_qm; the old lam_q buffer becomes the scratch)
     std::swap(a.lp, a.lpm);

@@ -148,7 +148,7 @@ def test_checkpointed_run_matches_autograd_through_steps():
     dcurl = curl.detach().cuda().requires_grad_(True)
     pf = QGRun.apply(dpsi, dcurl, g, n, TDT, 5)
     Jd = _objective(b, pf)
-    assert abs(float(Jd) - float(J)) <= 1e-12 * abs(float(J))
+    assert abs(float(Jd.detach()) - float(J.detach())) <= 1e-12 * abs(float(J.detach()))
     Jd.backward()
     assert rel_l2(dpsi.grad.cpu().numpy(), gpsi.numpy()) <= 1e-9
     assert rel_l2(dcurl.grad.cpu().numpy(), gcurl.numpy()) <= 1e-9
@@ -231,4 +231,40 @@ def test_state_slots_round_trip():
     fq = f[n3:2 * n3].reshape(b.nl, b.nyp, px)[:, :, :b.nxp]
     assert np.array_equal(fp, p) and np.array_equal(fq, q)
     assert nb >= 2 * n3 * 8
+    g.close()
+
+
+def test_one_step_vjp_eddy_resolving_box():
+    """The eddy-resolving box (2049x2049x3, dx 5 km, ah4 1e9; its rows are
+    wide enough for the split-mode inverse transform): one reversed step
+    against autograd through the restated step, run by torch on the GPU."""
+    b = ocean_double_gyre(2049, dx=5.0e3, ah4=1.0e9)
+    g, o = QG(b), oracle.Oracle(b)
+    st = _state(b, g, nsteps=2, seed=3)
+    wekp = _forcing(b)
+    dev = torch.device("cuda")
+    tb = TorchBox(b, o, device=dev)
+    xs = [torch.tensor(a, dtype=torch.float64, device=dev, requires_grad=True) for a in st]
+    w = torch.tensor(wekp, dtype=torch.float64, device=dev, requires_grad=True)
+    out = tb.step(*xs, w, 1200.0, suppress=False)
+    gen = torch.Generator(device=dev).manual_seed(7)
+    cot = [torch.randn(t.shape, dtype=torch.float64, device=dev, generator=gen)
+           / t.detach().abs().max().clamp_min(1e-30) for t in out]
+    grads = torch.autograd.grad(out, xs + [w], cot)
+    torch.cuda.synchronize()
+    L = lib()
+    c4, c5 = cot[4].cpu().numpy(), cot[5].cpu().numpy()
+    seeds = [c.contiguous() for c in cot[:4]]
+    _check(L.oqg_adj_set(g.h, *[_ptr(x) for x in seeds], _dp(c4), _dp(c5)), "adj_set")
+    run = AdjointRun(g, every=1)
+    _check(L.oqg_pq_save(g.h, _ptr(run.slots[0])), "pq_save")
+    _check(L.oqg_adj_step(g.h, _ptr(run.slots[0]), ctypes.c_double(1200.0), ctypes.c_longlong(3)), "adj_step")
+    res = [torch.empty(b.shape3, dtype=torch.float64, device=dev) for _ in range(4)]
+    lw = torch.empty(b.shape2, dtype=torch.float64, device=dev)
+    l1, l2 = np.empty(b.nl - 1), np.empty(b.nl - 1)
+    _check(L.oqg_adj_get(g.h, *[_ptr(r) for r in res], _dp(l1), _dp(l2), _ptr(lw)), "adj_get")
+    mine = res + [torch.tensor(l1, device=dev), torch.tensor(l2, device=dev), lw]
+    for name, a, r in zip(["p", "pm", "q", "qm", "dpi", "dpip", "wekp"], mine, grads):
+        err = float((a - r).norm() / r.norm())
+        assert err <= 1e-9, "lambda_%s: rel L2 %.3e" % (name, err)
     g.close()
