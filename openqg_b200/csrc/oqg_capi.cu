@@ -71,6 +71,8 @@ struct oqg_handle {
     std::vector<double> modes_amat, modes_ctl2m, modes_ctm2l, modes_rdm2;
     double *adj = nullptr;      // adjoint buffers, made on the first oqg_adj_set
     AdjFields af{};             // their current roles
+    cudaEvent_t up_ev = nullptr;   // oqg_set_forcing: the host arrays have been read
+    double frc_host[2] = {0.0, 0.0};   // txis, txin as last queued for the device
 };
 
 template <class X>
@@ -484,6 +486,7 @@ static void destroy_all(oqg_handle *h) {
     if (!h) return;
     drop_graphs(h);
     if (h->st) cudaStreamSynchronize(h->st);
+    if (h->up_ev) cudaEventDestroy(h->up_ev);
     for (void *p : h->allocs) cudaFree(p);
     if (h->st) cudaStreamDestroy(h->st);
     delete h;
@@ -949,21 +952,34 @@ int oqg_get_constraints(oqg_handle *h, double *dpi, double *dpip, double *cs, do
 int oqg_set_forcing(oqg_handle *h, const double *wekp, const double *ent, double txis, double txin) {
     if (!h) return fail(OQG_EINVAL, "null handle");
     BasinDev &b = h->hb;
-    const size_t n2 = (size_t)b.nyp * b.px;
+    const size_t n2 = (size_t)b.nyp * b.px, plane = (size_t)b.nyp * b.nxp;
+    if (ent && !h->ent_buf) {
+        h->ent_buf = dalloc<char>(h, (size_t)(b.nl - 1) * n2 * h->esz);
+        if (!h->ent_buf) return fail(OQG_ECUDA, "out of device memory");
+    }
+    if (!h->up_ev && cudaEventCreateWithFlags(&h->up_ev, cudaEventDisableTiming) != cudaSuccess)
+        return fail(OQG_ECUDA, "cudaEventCreate failed");
+    // both host arrays cross in back-to-back copies into the contiguous
+    // staging rows (wekp in layer 0, ent in layers 1..nl-1); the call waits
+    // only until the copies have read the caller's buffers, and the unpack
+    // and integral kernels run on the stream after it returns
+    if (wekp)
+        CK(cudaMemcpyAsync(h->hrow, wekp, plane * sizeof(double), cudaMemcpyHostToDevice, h->st));
+    if (ent)
+        CK(cudaMemcpyAsync(h->hrow + plane, ent, (b.nl - 1) * plane * sizeof(double), cudaMemcpyHostToDevice,
+                           h->st));
+    CK(cudaEventRecord(h->up_ev, h->st));
     if (wekp) {
-        int rc = upload_rows(h, wekp, const_cast<void *>(b.wekp), 1);
-        if (rc) return rc;
+        if (h->mixed) k_rows_in<float><<<296, 256, 0, h->st>>>(h->hrow, (float *)b.wekp, b.nxp, b.px, b.nyp);
+        else k_rows_in<double><<<296, 256, 0, h->st>>>(h->hrow, (double *)b.wekp, b.nxp, b.px, b.nyp);
     } else {
         CK(cudaMemsetAsync(const_cast<void *>(b.wekp), 0, n2 * h->esz, h->st));
     }
     const void *old_ent = b.ent;
     if (ent) {
-        if (!h->ent_buf) {
-            h->ent_buf = dalloc<char>(h, (size_t)(b.nl - 1) * n2 * h->esz);
-            if (!h->ent_buf) return fail(OQG_ECUDA, "out of device memory");
-        }
-        int rc = upload_rows(h, ent, h->ent_buf, b.nl - 1);
-        if (rc) return rc;
+        const size_t nr = (size_t)(b.nl - 1) * b.nyp;
+        if (h->mixed) k_rows_in<float><<<296, 256, 0, h->st>>>(h->hrow + plane, (float *)h->ent_buf, b.nxp, b.px, nr);
+        else k_rows_in<double><<<296, 256, 0, h->st>>>(h->hrow + plane, (double *)h->ent_buf, b.nxp, b.px, nr);
         b.ent = h->ent_buf;
     } else {
         b.ent = nullptr;
@@ -979,10 +995,12 @@ int oqg_set_forcing(oqg_handle *h, const double *wekp, const double *ent, double
     }
     if (h->mixed) k_forcing_integrals<float><<<1, 512, 0, h->st>>>(h->d_bas, 0);
     else k_forcing_integrals<double><<<1, 512, 0, h->st>>>(h->d_bas, 0);
-    double tx[2] = {txis, txin};
-    CK(cudaMemcpyAsync(&b.frc->txis, tx, 2 * sizeof(double), cudaMemcpyHostToDevice, h->st));
+    // the two scalars are copied from the handle, not from this stack frame
+    h->frc_host[0] = txis;
+    h->frc_host[1] = txin;
+    CK(cudaMemcpyAsync(&b.frc->txis, h->frc_host, 2 * sizeof(double), cudaMemcpyHostToDevice, h->st));
     CK(cudaGetLastError());
-    CK(cudaStreamSynchronize(h->st));
+    CK(cudaEventSynchronize(h->up_ev));
     return OQG_OK;
 }
 
@@ -1555,6 +1573,8 @@ int oqg_ensemble_set_forcing(oqg_ensemble *e, int member, const double *wekp, co
     int rc = ens_member(e, member, &h);
     if (rc) return rc;
     if ((rc = oqg_set_forcing(h, wekp, ent, txis, txin))) return rc;
+    // the ensemble steps on its own stream: the member's forcing must be in place
+    CK(cudaStreamSynchronize(h->st));
     return ens_refresh(e, member);
 }
 

@@ -268,3 +268,43 @@ def test_one_step_vjp_eddy_resolving_box():
         err = float((a - r).norm() / r.norm())
         assert err <= 1e-9, "lambda_%s: rel L2 %.3e" % (name, err)
     g.close()
+
+
+def test_gradient_differentiable_configuration():
+    """The differentiable configuration itself: 3-layer ocean at 257x257,
+    dx 20 km, 200 leapfrog steps, J = ekei(1) of the final state, checkpoint
+    every 20 steps; gradients with respect to the initial psi (FP64) and the
+    wind-stress curl field (FP32) against central differences (eps 1e-4
+    relative) along 16 seeded random directions."""
+    b = ocean_double_gyre(257, dx=20.0e3)
+    g = QG(b)
+    n, every = 200, 20
+    psi0 = torch.tensor(initial_psi(b, seed=11), dtype=torch.float64, device="cuda")
+    curl0 = torch.tensor(b.fnot * _forcing(b), dtype=torch.float32, device="cuda")
+
+    def J(psi, curl):
+        with torch.no_grad():
+            return float(_objective(b, QGRun.apply(psi, curl, g, n, TDT, every)))
+
+    psi = psi0.clone().requires_grad_(True)
+    curl = curl0.clone().requires_grad_(True)
+    _objective(b, QGRun.apply(psi, curl, g, n, TDT, every)).backward()
+    gpsi, gcurl = psi.grad.double(), curl.grad.double()
+    gen = torch.Generator(device="cuda").manual_seed(2024)
+    worst = 0.0
+    for d in range(16):
+        dp = torch.randn(b.shape3, dtype=torch.float64, device="cuda", generator=gen)
+        dp[:, [0, -1], :] = 0.0
+        dp[:, :, [0, -1]] = 0.0
+        dc = torch.randn(b.shape2, dtype=torch.float64, device="cuda", generator=gen)
+        eps_p = 1e-4 * float(psi0.norm()) / float(dp.norm())
+        eps_c = 1e-4 * float(curl0.double().norm()) / float(dc.norm())
+        cp = (curl0.double() + eps_c * dc).float()
+        cm = (curl0.double() - eps_c * dc).float()
+        fd = (J(psi0 + eps_p * dp, cp) - J(psi0 - eps_p * dp, cm)) / 2.0
+        # the FP32 control moves by what FP32 represents of the step
+        dcp = (cp.double() - cm.double()) / 2.0
+        an = eps_p * float((gpsi * dp).sum()) + float((gcurl * dcp).sum())
+        worst = max(worst, abs(fd - an) / abs(an))
+        assert abs(fd - an) <= 1e-6 * abs(an), "direction %d: fd %.12e adjoint %.12e" % (d, fd, an)
+    g.close()
