@@ -67,7 +67,10 @@ class AdjointRun:
         self.nsteps, self.tdt = int(nsteps), float(tdt)
         self.n0 = qg.step_index()
         nseg = (self.nsteps + self.every - 1) // self.every
-        self.ckpt = torch.empty((nseg + 1, self.full_bytes), dtype=torch.uint8, device=self.device)
+        shape = (nseg + 1, self.full_bytes)
+        if self.ckpt is None or tuple(self.ckpt.shape) != shape:
+            self.ckpt = None   # release the old slots before making the new ones
+            self.ckpt = torch.empty(shape, dtype=torch.uint8, device=self.device)
         torch.cuda.synchronize(self.device)
         for s in range(nseg):
             _check(lib().oqg_state_save(qg.h, _ptr(self.ckpt[s])), "oqg_state_save")

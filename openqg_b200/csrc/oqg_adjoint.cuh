@@ -301,11 +301,15 @@ __global__ void __launch_bounds__(256, 3) k_adj_vort(const BasinDev *__restrict_
         wc[m] = wk[m] * a.scal[16 + m];
     }
     const double *p = P + k * n2, *q = Q + k * n2;
-    for (int e = threadIdx.x; e < GH * GW; e += blockDim.x) {
+    // constant strides (256 threads) let the staging loops unroll and keep
+    // their loads in flight together
+#pragma unroll
+    for (int e = threadIdx.x; e < GH * GW; e += 256) {
         const int r = e / GW, c = e - r * GW;
         G[r][c] = lam_qnew<NL>(b, a, wk, wc, k, x0 - 3 + c, y0 - 3 + r);
     }
-    for (int e = threadIdx.x; e < BH * BW; e += blockDim.x) {
+#pragma unroll
+    for (int e = threadIdx.x; e < BH * BW; e += 256) {
         const int r = e / BW, c = e - r * BW;
         const int i = x0 - 1 + c, j = y0 - 1 + r;
         const bool in = i >= 0 && i < nxp && j >= 0 && j < nyp;
@@ -314,7 +318,8 @@ __global__ void __launch_bounds__(256, 3) k_adj_vort(const BasinDev *__restrict_
     }
     __syncthreads();
     // t1 = L^T g: g vanishes off the interior, where L's rows are the plain ones
-    for (int e = threadIdx.x; e < AH * AW; e += blockDim.x) {
+#pragma unroll
+    for (int e = threadIdx.x; e < AH * AW; e += 256) {
         const int r = e / AW, c = e - r * AW;
         const int i = x0 - 2 + c, j = y0 - 2 + r;
         double v = 0.0;
@@ -326,7 +331,7 @@ __global__ void __launch_bounds__(256, 3) k_adj_vort(const BasinDev *__restrict_
     __syncthreads();
     // t2 = L^T t1 (the wall rows of L enter here)
     const int di[5] = {0, 1, -1, 0, 0}, dj[5] = {0, 0, 0, 1, -1};
-    for (int e = threadIdx.x; e < BH * BW; e += blockDim.x) {
+    for (int e = threadIdx.x; e < BH * BW; e += 256) {
         const int r = e / BW, c = e - r * BW;
         const int i = x0 - 1 + c, j = y0 - 1 + r;
         double v = 0.0;
