@@ -32,7 +32,7 @@
 
 #include "oqg_kernels.cuh"
 
-#define OQG_ADJ_CTAS 296     // CTAs of the grid-stride adjoint kernels
+#define OQG_ADJ_CTAS 592     // CTAs of the grid-stride adjoint kernels (4 per SM)
 #define OQG_ADJ_THREADS 256
 
 namespace oqg {
