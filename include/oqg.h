@@ -278,6 +278,52 @@ int oqg_ensemble_sync(oqg_ensemble *e);
 int oqg_ensemble_stream(oqg_ensemble *e, void **stream);
 
 /* ---------------------------------------------------------------------
+ * The ocean half of the coupler on the device: the Ekman fields from the
+ * wind stress and the ocean mixed-layer step, writing the QG handle's
+ * forcing (wekp, ent) in place, so the layer-1 pressure, the pumping and the
+ * entrainment never cross to the host.  Replaces, for a closed box:
+ *   ekman_from_tau                          src/coupler/ekman.F90:53-83
+ *   step_oml (with adv_diff, del2_T, ...)   src/mixed/omlsubs.F90:69-119,
+ *                                           src/mixed/mixed_layer.F90:16-95
+ *   the ocean step's exchange               src/driver.F90:95-107
+ * ------------------------------------------------------------------- */
+typedef struct oqg_oml oqg_oml;
+
+/* init_ocean_ml (omlsubs.F90:27-67) and the temp_type fields it reads. */
+typedef struct oqg_oml_params {
+    double hm;          /* mixed-layer depth (m), the box's hm               */
+    double rho_cp;      /* rho * cp of sea water (J m^-3 K^-1)              */
+    double t1_rel;      /* T_bar - T(1) (K)                                  */
+    double dt_12;       /* T(1) - T(2) (K)                                   */
+    double st2d, st4d;  /* Laplacian / biharmonic sst diffusivities          */
+    double ycexp;       /* coefficient of the geostrophic advection          */
+    int    fluxn, fluxs;/* heat-flux condition at the northern / southern wall */
+    double nval, sval;  /* the wall temperatures of those conditions (K)     */
+} oqg_oml_params;
+
+/* The mixed layer of the basin of handle qg (a closed box); sst starts at
+ * zero (init_mixed, mixed.F90:73-99).  OQG_EINVAL for a heat-flux condition
+ * on the wrong hemisphere's wall, as the reference's init stops. */
+int oqg_oml_create(oqg_handle *qg, const oqg_oml_params *prm, oqg_oml **out);
+/* Frees the mixed layer; it does not touch the handle, so it may come before
+ * or after oqg_destroy of qg.  No other call may follow oqg_destroy of qg. */
+int oqg_oml_destroy(oqg_oml *m);
+/* sst and its lagged value, (nxt, nyt) = (nxp-1, nyp-1), host or device. */
+int oqg_oml_set_sst(oqg_oml *m, const double *sst, const double *sstm);
+int oqg_oml_get_sst(oqg_oml *m, double *sst, double *sstm);
+/* One ocean coupling step before step_qg (driver.F90:95-103): ekman_from_tau
+ * of taux, tauy (nxp, nyp) with the box's hm, then step_oml with the handle's
+ * current p(:,:,1) and the net heat flux fnetoc (nxt, nyt).  The handle's
+ * wekp becomes map_T_to_P(wekt); when compute_ent, its ent becomes the
+ * layer 1/2 entrainment (other layers zero), otherwise ent is kept.
+ * Arrays in host or device memory. */
+int oqg_ocean_forcing(oqg_oml *m, const double *taux, const double *tauy,
+                      const double *fnetoc, int compute_ent, double tdto);
+/* The handle's forcing, wekp (nxp, nyp) and ent (nxp, nyp, nl-1), copied
+ * to host arrays (either may be NULL). */
+int oqg_get_forcing(oqg_handle *h, double *wekp, double *ent);
+
+/* ---------------------------------------------------------------------
  * State slots and the adjoint step.  The reference has no adjoint (its model
  * is run forward only); these entry points have no counterpart in it.  They
  * serve gradient computation through the step (reverse mode with

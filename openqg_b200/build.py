@@ -15,7 +15,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "liboqg.so")
 SOURCES = ["oqg_capi.cu", "oqg_setup.cpp"]
 DEPS = SOURCES + ["oqg_dev.cuh", "oqg_fft.cuh", "oqg_kernels.cuh", "oqg_tma.cuh", "oqg_setup.h",
-                  "oqg_adjoint.cuh", "oqg_noalloc.cuh",
+                  "oqg_adjoint.cuh", "oqg_noalloc.cuh", "oqg_mixed.cuh",
                   os.path.join("..", "..", "include", "oqg.h")]
 
 NVCC_FLAGS = [

@@ -20,7 +20,7 @@ from typing import Optional
 
 import numpy as np
 
-from .params import Basin, QgMonitor, STATUS
+from .params import Basin, OqgOmlParams, QgMonitor, STATUS
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "liboqg.so")
@@ -87,6 +87,12 @@ def lib():
     L.oqg_adj_get.argtypes = [vp, vp, vp, vp, vp, _dp, _dp, vp]
     L.oqg_adj_step.argtypes = [vp, vp, ctypes.c_double, ctypes.c_longlong]
     L.oqg_adj_initial.argtypes = [vp, vp, vp]
+    L.oqg_oml_create.argtypes = [vp, ctypes.POINTER(OqgOmlParams), ctypes.POINTER(vp)]
+    L.oqg_oml_destroy.argtypes = [vp]
+    L.oqg_oml_set_sst.argtypes = [vp, vp, vp]
+    L.oqg_oml_get_sst.argtypes = [vp, vp, vp]
+    L.oqg_ocean_forcing.argtypes = [vp, vp, vp, vp, ctypes.c_int, ctypes.c_double]
+    L.oqg_get_forcing.argtypes = [vp, _dp, _dp]
     L.oqg_adj_segment.argtypes = [vp, vp, vp, ctypes.c_size_t, ctypes.c_int, ctypes.c_double, ctypes.c_longlong]
     _lib = L
     return L
@@ -380,3 +386,58 @@ class Ensemble:
         s = ctypes.c_void_p()
         _check(lib().oqg_ensemble_stream(self.e, ctypes.byref(s)), "oqg_ensemble_stream")
         return s.value or 0
+
+
+class OceanMixedLayer:
+    """The ocean mixed layer of a closed basin on the device (step_oml,
+    omlsubs.F90:69-119) coupled to a QG handle: `forcing(taux, tauy, fnetoc,
+    compute_ent, tdto)` runs ekman_from_tau and step_oml and leaves wekp and
+    ent in the handle's forcing for its next step (driver.F90:95-107).
+    Arrays are numpy FP64: wind stress (nyp, nxp), T-grid fields (nyt, nxt)."""
+
+    def __init__(self, qg: QG, hm: float, rho_cp: float, t1_rel: float, dt_12: float, st2d: float = 0.0,
+                 st4d: float = 0.0, ycexp: float = 1.0, fluxn: bool = False, fluxs: bool = False,
+                 nval: float = 0.0, sval: float = 0.0):
+        self.qg = qg
+        self._prm = OqgOmlParams(hm, rho_cp, t1_rel, dt_12, st2d, st4d, ycexp, int(fluxn), int(fluxs), nval, sval)
+        h = ctypes.c_void_p()
+        _check(lib().oqg_oml_create(qg.h, ctypes.byref(self._prm), ctypes.byref(h)), "oqg_oml_create")
+        self.h = h
+        self.tshape = (qg.b.nyp - 1, qg.b.nxp - 1)
+
+    def close(self):
+        # the mixed layer's buffers are freed without touching the QG handle,
+        # so this is safe before or after the handle's close()
+        if getattr(self, "h", None) is not None and self.h.value:
+            lib().oqg_oml_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_sst(self, sst, sstm):
+        a, am = _f64(sst, self.tshape), _f64(sstm, self.tshape)
+        _check(lib().oqg_oml_set_sst(self.h, a.ctypes.data, am.ctypes.data), "oqg_oml_set_sst")
+
+    def get_sst(self):
+        a, am = np.empty(self.tshape), np.empty(self.tshape)
+        _check(lib().oqg_oml_get_sst(self.h, a.ctypes.data, am.ctypes.data), "oqg_oml_get_sst")
+        return a, am
+
+    def forcing(self, taux, tauy, fnetoc, compute_ent: bool, tdto: float):
+        b = self.qg.b
+        tx, ty = _f64(taux, b.shape2), _f64(tauy, b.shape2)
+        fn = _f64(fnetoc, self.tshape)
+        _check(lib().oqg_ocean_forcing(self.h, tx.ctypes.data, ty.ctypes.data, fn.ctypes.data, int(compute_ent),
+                                       float(tdto)), "oqg_ocean_forcing")
+
+
+def get_forcing(qg: QG):
+    """The handle's forcing (wekp (nyp, nxp), ent (nl-1, nyp, nxp))."""
+    b = qg.b
+    w, e = np.empty(b.shape2), np.empty((b.nl - 1,) + b.shape2)
+    _check(lib().oqg_get_forcing(qg.h, _p(w), _p(e)), "oqg_get_forcing")
+    return w, e

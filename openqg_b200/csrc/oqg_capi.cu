@@ -8,6 +8,7 @@
 #include "oqg_dev.cuh"
 #include "oqg_kernels.cuh"
 #include "oqg_adjoint.cuh"
+#include "oqg_mixed.cuh"
 #include "oqg_noalloc.cuh"
 #include "oqg_setup.h"
 
@@ -1842,6 +1843,160 @@ int oqg_adj_initial(oqg_handle *h, double *gp, double *gpm) {
     CK(cudaGetLastError());
     if (gp && (rc = get_field(h, a.nu, gp, b.nl))) return rc;
     if (gpm && (rc = get_field(h, a.s, gpm, b.nl))) return rc;
+    CK(cudaStreamSynchronize(h->st));
+    return OQG_OK;
+}
+
+}  // extern "C"
+
+// ================================================================ mixed layer
+// The ocean mixed layer (step_oml) and the Ekman fields from the wind stress,
+// on the device, feeding the QG handle's forcing (kernels in oqg_mixed.cuh).
+struct oqg_oml {
+    oqg_handle *h = nullptr;
+    oqg_oml_params prm{};
+    std::vector<void *> allocs;
+    OmlDev o{};
+};
+
+extern "C" {
+
+int oqg_oml_create(oqg_handle *h, const oqg_oml_params *prm, oqg_oml **out) {
+    if (!h || !prm || !out) return fail(OQG_EINVAL, "null argument");
+    *out = nullptr;
+    const BasinDev &b = h->hb;
+    if (b.cyclic) return fail(OQG_EUNSUPPORTED, "the ocean mixed layer needs a closed box");
+    if (!(prm->hm > 0.0) || !(prm->rho_cp > 0.0) || prm->dt_12 == 0.0)
+        return fail(OQG_EINVAL, "hm and rho_cp must be > 0 and dt_12 nonzero");
+    // heat-flux conditions against the hemisphere (omlsubs.F90:45-66)
+    if (prm->fluxs && b.fnot < 0.0)
+        return fail(OQG_EINVAL, "southern heat-flux condition with fnot < 0 (southern hemisphere)");
+    if (prm->fluxn && b.fnot > 0.0)
+        return fail(OQG_EINVAL, "northern heat-flux condition with fnot > 0 (northern hemisphere)");
+    oqg_oml *m = new oqg_oml();
+    m->h = h;
+    m->prm = *prm;
+    OmlDev &o = m->o;
+    o.nxp = b.nxp; o.nyp = b.nyp; o.nxt = b.nxp - 1; o.nyt = b.nyp - 1;
+    o.tau_sign = b.tau_sign; o.fluxn = prm->fluxn != 0; o.fluxs = prm->fluxs != 0;
+    o.dx = b.dx; o.dy = b.dy; o.fnot = b.fnot; o.hm = prm->hm; o.rho_cp = prm->rho_cp;
+    o.t1_rel = prm->t1_rel; o.dt_12 = prm->dt_12; o.st2d = prm->st2d; o.st4d = prm->st4d;
+    o.ycexp = prm->ycexp; o.nval = prm->nval; o.sval = prm->sval;
+    const size_t nt = (size_t)o.nxt * o.nyt, np = (size_t)o.nxp * o.nyp;
+    const size_t total = 6 * nt + 2 * np + OQG_OML_CTAS;
+    void *x = nullptr;
+    if (cudaMalloc(&x, total * sizeof(double)) != cudaSuccess) {
+        delete m;
+        return fail(OQG_ECUDA, "cudaMalloc of the mixed-layer buffers failed");
+    }
+    m->allocs.push_back(x);
+    double *d = (double *)x;
+    o.data = d; o.datam = d + nt; o.d2 = d + 2 * nt; o.wekt = d + 3 * nt; o.xfo = d + 4 * nt;
+    double *fn = d + 5 * nt;
+    o.fnet = fn;
+    o.taux = d + 6 * nt;
+    o.tauy = d + 6 * nt + np;
+    o.part = d + 6 * nt + 2 * np;
+    if (cudaMemsetAsync(x, 0, total * sizeof(double), h->st) != cudaSuccess ||
+        cudaStreamSynchronize(h->st) != cudaSuccess) {
+        cudaFree(x);
+        delete m;
+        return fail(OQG_ECUDA, "cudaMemset of the mixed-layer buffers failed");
+    }
+    *out = m;
+    return OQG_OK;
+}
+
+int oqg_oml_destroy(oqg_oml *m) {
+    if (!m) return OQG_OK;
+    // the handle may be gone already: cudaFree waits for the device by itself
+    for (void *p : m->allocs) cudaFree(p);
+    delete m;
+    return OQG_OK;
+}
+
+int oqg_oml_set_sst(oqg_oml *m, const double *sst, const double *sstm) {
+    if (!m || !sst || !sstm) return fail(OQG_EINVAL, "null argument");
+    const size_t bytes = (size_t)m->o.nxt * m->o.nyt * sizeof(double);
+    CK(cudaMemcpyAsync(m->o.data, sst, bytes, cudaMemcpyDefault, m->h->st));
+    CK(cudaMemcpyAsync(m->o.datam, sstm, bytes, cudaMemcpyDefault, m->h->st));
+    CK(cudaStreamSynchronize(m->h->st));
+    return OQG_OK;
+}
+
+int oqg_oml_get_sst(oqg_oml *m, double *sst, double *sstm) {
+    if (!m) return fail(OQG_EINVAL, "null argument");
+    const size_t bytes = (size_t)m->o.nxt * m->o.nyt * sizeof(double);
+    if (sst) CK(cudaMemcpyAsync(sst, m->o.data, bytes, cudaMemcpyDefault, m->h->st));
+    if (sstm) CK(cudaMemcpyAsync(sstm, m->o.datam, bytes, cudaMemcpyDefault, m->h->st));
+    CK(cudaStreamSynchronize(m->h->st));
+    return OQG_OK;
+}
+
+int oqg_ocean_forcing(oqg_oml *m, const double *taux, const double *tauy, const double *fnetoc, int compute_ent,
+                      double tdto) {
+    if (!m || !taux || !tauy || !fnetoc) return fail(OQG_EINVAL, "null argument");
+    if (!(tdto > 0.0)) return fail(OQG_EINVAL, "tdto must be > 0");
+    oqg_handle *h = m->h;
+    BasinDev &b = h->hb;
+    OmlDev &o = m->o;
+    const size_t nt = (size_t)o.nxt * o.nyt, np = (size_t)o.nxp * o.nyp, n2 = (size_t)b.nyp * b.px;
+    if (compute_ent && !h->ent_buf) {
+        h->ent_buf = dalloc<char>(h, (size_t)(b.nl - 1) * n2 * h->esz);
+        if (!h->ent_buf) return fail(OQG_ECUDA, "out of device memory");
+    }
+    if (!h->up_ev && cudaEventCreateWithFlags(&h->up_ev, cudaEventDisableTiming) != cudaSuccess)
+        return fail(OQG_ECUDA, "cudaEventCreate failed");
+    CK(cudaMemcpyAsync(const_cast<double *>(o.taux), taux, np * sizeof(double), cudaMemcpyDefault, h->st));
+    CK(cudaMemcpyAsync(const_cast<double *>(o.tauy), tauy, np * sizeof(double), cudaMemcpyDefault, h->st));
+    CK(cudaMemcpyAsync(const_cast<double *>(o.fnet), fnetoc, nt * sizeof(double), cudaMemcpyDefault, h->st));
+    CK(cudaEventRecord(h->up_ev, h->st));
+    const int grid = std::min((int)((nt + 255) / 256), OQG_OML_CTAS);
+    k_oml_pre<<<grid, 256, 0, h->st>>>(o);
+    const void *p1 = b.F[h->par];   // layer 1 of the current p (driver.F90:96-103)
+    if (h->mixed) k_oml_step<float><<<OQG_OML_CTAS, 256, 0, h->st>>>(o, (const float *)p1, b.px, tdto, compute_ent);
+    else k_oml_step<double><<<OQG_OML_CTAS, 256, 0, h->st>>>(o, (const double *)p1, b.px, tdto, compute_ent);
+    const int gp = std::min((int)((np + 255) / 256), 148 * 8);
+    if (h->mixed)
+        k_oml_post<float><<<gp, 256, 0, h->st>>>(o, (float *)b.wekp, (float *)h->ent_buf, b.px, b.nl, compute_ent,
+                                                 OQG_OML_CTAS);
+    else
+        k_oml_post<double><<<gp, 256, 0, h->st>>>(o, (double *)b.wekp, (double *)h->ent_buf, b.px, b.nl,
+                                                  compute_ent, OQG_OML_CTAS);
+    CK(cudaGetLastError());
+    std::swap(o.data, o.datam);   // datam <- data, data <- the new sst
+    if (compute_ent && b.ent != h->ent_buf) {
+        b.ent = h->ent_buf;
+        h->hb64.ent = b.ent;
+        int rc = push_desc(h);
+        if (rc) return rc;
+    }
+    if (b.ent) {
+        if (h->mixed) k_ent_rows<float><<<b.nyp, 128, 0, h->st>>>(h->d_bas, 0);
+        else k_ent_rows<double><<<b.nyp, 128, 0, h->st>>>(h->d_bas, 0);
+    }
+    if (h->mixed) k_forcing_integrals<float><<<1, 512, 0, h->st>>>(h->d_bas, 0);
+    else k_forcing_integrals<double><<<1, 512, 0, h->st>>>(h->d_bas, 0);
+    h->frc_host[0] = 0.0;   // txis, txin: zero for a closed box (ekman.F90:60-70)
+    h->frc_host[1] = 0.0;
+    CK(cudaMemcpyAsync(&b.frc->txis, h->frc_host, 2 * sizeof(double), cudaMemcpyHostToDevice, h->st));
+    CK(cudaGetLastError());
+    CK(cudaEventSynchronize(h->up_ev));
+    return OQG_OK;
+}
+
+int oqg_get_forcing(oqg_handle *h, double *wekp, double *ent) {
+    if (!h) return fail(OQG_EINVAL, "null handle");
+    const BasinDev &b = h->hb;
+    int rc;
+    if (wekp && (rc = download_rows(h, b.wekp, wekp, 1))) return rc;
+    if (ent) {
+        if (b.ent) {
+            if ((rc = download_rows(h, b.ent, ent, b.nl - 1))) return rc;
+        } else {
+            std::fill(ent, ent + (size_t)(b.nl - 1) * b.nyp * b.nxp, 0.0);
+        }
+    }
     CK(cudaStreamSynchronize(h->st));
     return OQG_OK;
 }

@@ -1,0 +1,167 @@
+// oqg_mixed.cuh -- the ocean mixed layer's step and the Ekman fields that
+// feed it, on the device (closed box, FP64 arithmetic).
+//
+//   ekman_from_tau   src/coupler/ekman.F90:53-83
+//   step_oml         src/mixed/omlsubs.F90:69-119
+//   adv_diff         src/mixed/mixed_layer.F90:16-95
+//   del2_T, avg_T, map_T_to_x_face / y_face, c_grid_advection, dPdx, dPdy,
+//   map_T_to_P       src/glam/numerics.F90:64-163, 223-309, 392-408
+//
+// T-grid fields are [nyt][nxt] (nxt = nxp-1, nyt = nyp-1), the wind stress
+// [nyp][nxp], all FP64 and contiguous.  The QG layer-1 pressure is read from
+// the handle's state and the results land in the handle's forcing fields.
+#pragma once
+
+#include "oqg_kernels.cuh"
+
+#define OQG_OML_CTAS 296
+
+namespace oqg {
+
+struct OmlDev {
+    int nxp, nyp, nxt, nyt, tau_sign, fluxn, fluxs;
+    double dx, dy, fnot, hm, rho_cp, t1_rel, dt_12, st2d, st4d, ycexp, nval, sval;
+    const double *taux, *tauy;   // [nyp][nxp]
+    const double *fnet;          // [nyt][nxt] net heat flux into the ocean
+    double *data, *datam;        // sst and its lagged value [nyt][nxt]
+    double *d2, *wekt, *xfo;     // del2_T(datam), T-grid Ekman pumping, entrainment [nyt][nxt]
+    double *part;                // [OQG_OML_CTAS] partial sums of xfo
+};
+
+// del2_T (numerics.F90:109-145) of t at T point (i, j), closed box.
+__device__ __forceinline__ double oml_del2(const OmlDev &o, const double *t, int i, int j, bool nflux, double nval,
+                                           bool sflux, double sval) {
+    const int nxt = o.nxt, nyt = o.nyt;
+    const double c = t[(size_t)j * nxt + i];
+    const double left = i == 0 ? 0.0 : c - t[(size_t)j * nxt + i - 1];
+    const double right = i == nxt - 1 ? 0.0 : t[(size_t)j * nxt + i + 1] - c;
+    const double bot = j == 0 ? (sflux ? c - sval : 0.0) : c - t[(size_t)(j - 1) * nxt + i];
+    const double top = j == nyt - 1 ? (nflux ? nval - c : 0.0) : t[(size_t)(j + 1) * nxt + i] - c;
+    return (1.0 / (o.dx * o.dx)) * (right - left + top - bot);
+}
+
+// Ekman pumping at T points (ekman.F90:78-80) and del2_T of the lagged sst.
+__global__ void k_oml_pre(OmlDev o) {
+    for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < o.nxt * o.nyt; idx += gridDim.x * blockDim.x) {
+        const int j = idx / o.nxt, i = idx - j * o.nxt;
+        const double *tx = o.taux, *ty = o.tauy;
+        const int nxp = o.nxp;
+        // map_P_to_y_face / map_P_to_x_face of the stress
+        const double tyw = 0.5 * (ty[(size_t)(j + 1) * nxp + i] + ty[(size_t)j * nxp + i]);
+        const double tye = 0.5 * (ty[(size_t)(j + 1) * nxp + i + 1] + ty[(size_t)j * nxp + i + 1]);
+        const double txs = 0.5 * (tx[(size_t)j * nxp + i + 1] + tx[(size_t)j * nxp + i]);
+        const double txn = 0.5 * (tx[(size_t)(j + 1) * nxp + i + 1] + tx[(size_t)(j + 1) * nxp + i]);
+        o.wekt[idx] = (1.0 / (o.dx * o.fnot)) * (tye - tyw) - (1.0 / (o.dy * o.fnot)) * (txn - txs);
+        o.d2[idx] = oml_del2(o, o.datam, i, j, o.fluxn, o.nval, o.fluxs, o.sval);
+    }
+}
+
+// step_oml at T points: advection (C grid, geostrophic from the layer-1
+// pressure P1 plus Ekman), Laplacian and biharmonic diffusion, heat and
+// Ekman forcing, the convective adjustment and, when ent is computed, the
+// layer 1/2 entrainment xfo with per-CTA partial sums for its mean.  The new
+// sst overwrites datam (the host then swaps data and datam).
+template <class T>
+__global__ void __launch_bounds__(256) k_oml_step(OmlDev o, const T *__restrict__ P1, int px, double tdto,
+                                                   int compute_ent) {
+    __shared__ double red[32];
+    const int nxt = o.nxt, nyt = o.nyt, nxp = o.nxp, nyp = o.nyp;
+    const double ce = o.tau_sign / (o.fnot * o.hm), cg = o.ycexp / o.fnot;
+    const double *tx = o.taux, *ty = o.tauy, *t = o.data;
+    auto p = [&](int i, int j) { return (double)P1[(size_t)j * px + i]; };
+    // vel_u * mixed_x on the x-face of column f (0..nxt), row j
+    auto uflux = [&](int f, int j) {
+        if (f == 0 || f == nxp - 1) return 0.0;   // no normal flow through the walls
+        const double dpdy = (1.0 / o.dy) * (p(f, j + 1) - p(f, j));
+        const double uek = ce * (0.5 * (ty[(size_t)(j + 1) * nxp + f] + ty[(size_t)j * nxp + f]));
+        const double vel = -cg * dpdy + uek;
+        const double mx = 0.5 * (t[(size_t)j * nxt + f - 1] + t[(size_t)j * nxt + f]);
+        return vel * mx;
+    };
+    // vel_v * mixed_y on the y-face of row g (0..nyt), column i
+    auto vflux = [&](int i, int g) {
+        const double vek = -ce * (0.5 * (tx[(size_t)g * nxp + i + 1] + tx[(size_t)g * nxp + i]));
+        double vel, my;
+        if (g == 0) {
+            vel = o.fluxs ? vek : 0.0;
+            my = o.fluxs ? t[i] : 0.5 * (t[i] + o.sval);
+        } else if (g == nyp - 1) {
+            vel = o.fluxn ? vek : 0.0;
+            my = o.fluxn ? t[(size_t)(nyt - 1) * nxt + i] : 0.5 * (t[(size_t)(nyt - 1) * nxt + i] + o.nval);
+        } else {
+            const double dpdx = (1.0 / o.dx) * (p(i + 1, g) - p(i, g));
+            vel = cg * dpdx + vek;
+            my = 0.5 * (t[(size_t)(g - 1) * nxt + i] + t[(size_t)g * nxt + i]);
+        }
+        return vel * my;
+    };
+    double xs = 0.0;
+    for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < nxt * nyt; idx += gridDim.x * blockDim.x) {
+        const int j = idx / nxt, i = idx - j * nxt;
+        const double adv = (-1.0 / o.dx) * (uflux(i + 1, j) - uflux(i, j)) + (-1.0 / o.dy) * (vflux(i, j + 1) - vflux(i, j));
+        const double d4 = oml_del2(o, o.d2, i, j, false, 0.0, false, 0.0);
+        const double ad = adv + o.st2d * o.d2[idx] - o.st4d * d4;
+        const double dm = o.datam[idx], wk = o.wekt[idx];
+        const double half = 0.5 * wk * (dm - o.t1_rel);
+        const double sstnew = dm + tdto * (ad + (1.0 / (o.rho_cp * o.hm)) * o.fnet[idx] + (1.0 / o.hm) * (wk * dm - half));
+        const double conv = fmax(0.0, o.t1_rel - sstnew);
+        o.datam[idx] = sstnew + conv;
+        if (compute_ent) {
+            const double x = (-1.0 / o.dt_12) * half - (o.hm / (tdto * o.dt_12)) * conv;
+            o.xfo[idx] = x;
+            xs += x;
+        }
+    }
+    if (compute_ent) {
+        const double v = block_sum(xs, red);
+        if (threadIdx.x == 0) o.part[blockIdx.x] = v;
+    }
+}
+
+// map_T_to_P (numerics.F90:64-107) of a T-grid field at p point (i, j), the
+// constant c subtracted from every T value first.
+__device__ __forceinline__ double oml_t2p(const OmlDev &o, const double *t, double c, int i, int j) {
+    const int nxt = o.nxt, nyt = o.nyt, nxp = o.nxp, nyp = o.nyp;
+    auto T_ = [&](int a, int bb) { return t[(size_t)bb * nxt + a] - c; };
+    const bool w = i == 0, e = i == nxp - 1, s = j == 0, n = j == nyp - 1;
+    if ((w || e) && (s || n)) return T_(w ? 0 : nxt - 1, s ? 0 : nyt - 1);
+    if (s || n) {
+        const int r = s ? 0 : nyt - 1;
+        return 0.5 * (T_(i - 1, r) + T_(i, r));
+    }
+    if (w || e) {
+        const int cc = w ? 0 : nxt - 1;
+        return 0.5 * (T_(cc, j - 1) + T_(cc, j));
+    }
+    return 0.25 * (T_(i, j) + T_(i - 1, j) + T_(i, j - 1) + T_(i - 1, j - 1));
+}
+
+// The QG forcing from the mixed layer: wekp = map_T_to_P(wekt) and, when
+// computed, ent(:,:,1) = map_T_to_P(xfo - avg_T(xfo)), ent(:,:,2:) = 0, into
+// the handle's pitched fields.  Every CTA adds the partial sums in the same
+// order (deterministic mean).
+template <class T>
+__global__ void __launch_bounds__(256) k_oml_post(OmlDev o, T *wekp, T *ent, int px, int nl, int compute_ent,
+                                                   int nparts) {
+    __shared__ double avg;
+    if (threadIdx.x < 32) {
+        double s = 0.0;
+        if (compute_ent)
+            for (int c = threadIdx.x; c < nparts; c += 32) s += o.part[c];
+        s = warp_sum(s);
+        if (threadIdx.x == 0) avg = s / ((double)o.nxt * o.nyt);
+    }
+    __syncthreads();
+    const size_t n2 = (size_t)o.nyp * px;
+    for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < o.nxp * o.nyp; idx += gridDim.x * blockDim.x) {
+        const int j = idx / o.nxp, i = idx - j * o.nxp;
+        const size_t op = (size_t)j * px + i;
+        wekp[op] = (T)oml_t2p(o, o.wekt, 0.0, i, j);
+        if (compute_ent) {
+            ent[op] = (T)oml_t2p(o, o.xfo, avg, i, j);
+            for (int k = 1; k < nl - 1; ++k) ent[k * n2 + op] = (T)0;
+        }
+    }
+}
+
+}  // namespace oqg

@@ -40,6 +40,17 @@ STATUS = {
 _D8 = ctypes.c_double * OQG_MAX_NL
 
 
+class OqgOmlParams(ctypes.Structure):
+    """ctypes mirror of `oqg_oml_params` (include/oqg.h): the ocean mixed
+    layer's parameters (init_ocean_ml, omlsubs.F90:27-67)."""
+    _fields_ = [
+        ("hm", ctypes.c_double), ("rho_cp", ctypes.c_double), ("t1_rel", ctypes.c_double),
+        ("dt_12", ctypes.c_double), ("st2d", ctypes.c_double), ("st4d", ctypes.c_double),
+        ("ycexp", ctypes.c_double), ("fluxn", ctypes.c_int), ("fluxs", ctypes.c_int),
+        ("nval", ctypes.c_double), ("sval", ctypes.c_double),
+    ]
+
+
 class OqgParams(ctypes.Structure):
     """ctypes mirror of `oqg_params` (include/oqg.h)."""
     _fields_ = [

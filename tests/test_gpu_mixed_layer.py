@@ -1,0 +1,118 @@
+"""The ocean mixed layer and Ekman fields on the device (oqg_ocean_forcing)
+against the CPU restatement (oracle/mixed_layer.py).
+
+Tolerances (relative L2):
+  * sst, its lagged value, wekp and ent after each coupling step: 1e-12
+    (FP64 arithmetic on the same inputs; sums differ in order only);
+  * a coupled run (forcing then step_qg, five times) against the oracle's
+    mixed layer feeding the C++ oracle's QG step: p and q 1e-11, sst 1e-11;
+  * an OQG_MIXED handle (FP32 forcing fields): wekp and ent 1e-6.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from oracle.mixed_layer import OmlOracle, OmlParams, ekman
+from openqg_b200.core import QG, OceanMixedLayer, OqgError, get_forcing
+from openqg_b200.params import OQG_MIXED, atmos_channel, double_gyre_tau, initial_psi, ocean_double_gyre
+from tests.qg_numpy import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+TDT = 3600.0
+
+
+@pytest.fixture(autouse=True)
+def _need_gpu(gpu_required):
+    pass
+
+
+def _setup(n=65, precision=0, fluxs=True, seed=2):
+    b = ocean_double_gyre(n, dx=20.0e3, precision=precision)
+    prm = OmlParams(hm=100.0, rho_cp=4.0e6, t1_rel=10.0, dt_12=5.0, st2d=2.0e3, st4d=1.0e11, ycexp=1.0,
+                    fluxs=fluxs, sval=14.0)
+    rng = np.random.default_rng(seed)
+    nyt, nxt = b.nyp - 1, b.nxp - 1
+    yy = np.linspace(0.0, 1.0, nyt)[:, None]
+    sst = prm.t1_rel + 2.0 + 3.0 * np.cos(np.pi * yy) + 0.3 * rng.standard_normal((nyt, nxt))
+    sstm = sst + 0.05 * rng.standard_normal((nyt, nxt))
+    taux, tauy = double_gyre_tau(b)
+    tauy = tauy + 0.02 * rng.standard_normal(tauy.shape)
+    fnet = 40.0 * rng.standard_normal((nyt, nxt))
+    p = b.fnot * initial_psi(b, seed=seed)
+    g = QG(b)
+    g.set_state(p, p)
+    m = OceanMixedLayer(g, prm.hm, prm.rho_cp, prm.t1_rel, prm.dt_12, prm.st2d, prm.st4d, prm.ycexp,
+                        prm.fluxn, prm.fluxs, prm.nval, prm.sval)
+    m.set_sst(sst, sstm)
+    o = OmlOracle(b, prm)
+    o.data, o.datam = sst.copy(), sstm.copy()
+    return b, prm, g, m, o, taux, tauy, fnet, p
+
+
+def test_forcing_matches_oracle():
+    b, prm, g, m, o, taux, tauy, fnet, _ = _setup()
+    uek, vek, wekt, wekp = ekman(taux, tauy, b.dx, b.dy, b.fnot, prm.hm)
+    ent = np.zeros((b.nl - 1,) + b.shape2)
+    for it, ce in enumerate((True, False, True)):
+        p1 = g.get_state()[0][0]
+        m.forcing(taux, tauy, fnet, ce, TDT)
+        o.step(p1, uek, vek, wekt, fnet, ce, TDT, ent)
+        sst, sstm = m.get_sst()
+        assert rel_l2(sst, o.data) <= 1e-12, it
+        assert rel_l2(sstm, o.datam) <= 1e-12, it
+        w, e = get_forcing(g)
+        assert rel_l2(w, wekp) <= 1e-12
+        assert rel_l2(e, ent) <= 1e-12, it
+        g.step(TDT, 1)
+    m.close()
+    g.close()
+
+
+def test_coupled_run_matches_oracle():
+    """Five ocean steps of the coupled pattern: the mixed layer's forcing,
+    then step_qg with it, on the device and on the CPU."""
+    b, prm, g, m, o, taux, tauy, fnet, p = _setup(seed=5)
+    q = oracle.Oracle(b)
+    q.set_state(p, p)
+    uek, vek, wekt, wekp = ekman(taux, tauy, b.dx, b.dy, b.fnot, prm.hm)
+    ent = np.zeros((b.nl - 1,) + b.shape2)
+    for _ in range(5):
+        p1 = q.get_state()[0][0]
+        o.step(p1, uek, vek, wekt, fnet, True, TDT, ent)
+        q.set_forcing(wekp, ent, 0.0, 0.0)
+        q.step(TDT, 1)
+        m.forcing(taux, tauy, fnet, True, TDT)
+        g.step(TDT, 1)
+    for a, r in zip(g.get_state(), q.get_state()):
+        assert rel_l2(a, r) <= 1e-11
+    assert rel_l2(m.get_sst()[0], o.data) <= 1e-11
+    m.close()
+    g.close()
+
+
+def test_mixed_precision_handle_forcing():
+    b, prm, g, m, o, taux, tauy, fnet, _ = _setup(precision=OQG_MIXED, seed=7)
+    uek, vek, wekt, wekp = ekman(taux, tauy, b.dx, b.dy, b.fnot, prm.hm)
+    ent = np.zeros((b.nl - 1,) + b.shape2)
+    p1 = g.get_state()[0][0]          # the FP32 state, widened
+    m.forcing(taux, tauy, fnet, True, TDT)
+    o.step(p1, uek, vek, wekt, fnet, True, TDT, ent)
+    assert rel_l2(m.get_sst()[0], o.data) <= 1e-12
+    w, e = get_forcing(g)
+    assert rel_l2(w, wekp) <= 1e-6
+    assert rel_l2(e, ent) <= 1e-6
+    m.close()
+    g.close()
+
+
+def test_rejected_setups():
+    b = ocean_double_gyre(33)
+    g = QG(b)
+    with pytest.raises(OqgError):        # northern flux condition in the northern hemisphere
+        OceanMixedLayer(g, 100.0, 4.0e6, 10.0, 5.0, fluxn=True)
+    g.close()
+    c = QG(atmos_channel(33, 17))
+    with pytest.raises(OqgError):        # the ocean mixed layer needs a closed box
+        OceanMixedLayer(c, 100.0, 4.0e6, 10.0, 5.0)
+    c.close()

@@ -1,0 +1,64 @@
+"""The ocean mixed-layer restatement (oracle/mixed_layer.py), pinned by the
+properties of the reference's equations (the reference has no tests of this
+code) and, for its Ekman part, by the C++ oracle's ekman_from_tau.
+
+  * ekman: wekp within 1e-14 of oracle.ekman_from_tau;
+  * adv_diff with no-flux walls conserves heat: its sum over the T cells
+    vanishes to rounding (the C-grid fluxes and the del2_T differences
+    telescope, and both velocities vanish on the walls);
+  * the entrainment's T-grid field has zero mean (omlsubs.F90:110-112);
+  * the convective adjustment leaves sst >= T_bar - T_(1) everywhere
+    (sstnew + max(0, T1_rel - sstnew), omlsubs.F90:101, 117).
+"""
+import numpy as np
+
+import oracle
+from oracle.mixed_layer import OmlOracle, OmlParams, ekman
+from openqg_b200.params import double_gyre_tau, initial_psi, ocean_double_gyre
+
+
+def _case(n=33, seed=0, **kw):
+    b = ocean_double_gyre(n, dx=40.0e3)
+    prm = OmlParams(st2d=2.0e3, st4d=1.0e11, ycexp=1.0, **kw)
+    o = OmlOracle(b, prm)
+    rng = np.random.default_rng(seed)
+    nyt, nxt = b.nyp - 1, b.nxp - 1
+    yy = np.linspace(0.0, 1.0, nyt)[:, None]
+    o.data = prm.t1_rel + 2.0 + 3.0 * np.cos(np.pi * yy) + 0.3 * rng.standard_normal((nyt, nxt))
+    o.datam = o.data + 0.05 * rng.standard_normal((nyt, nxt))
+    taux, tauy = double_gyre_tau(b)
+    tauy = tauy + 0.02 * rng.standard_normal(tauy.shape)
+    p1 = b.fnot * initial_psi(b, seed=seed)[0]
+    return b, prm, o, taux, tauy, p1, rng
+
+
+def test_ekman_matches_cpp_oracle():
+    b, prm, _, taux, tauy, _, _ = _case()
+    _, _, _, wekp = ekman(taux, tauy, b.dx, b.dy, b.fnot, prm.hm)
+    w, _, _ = oracle.ekman_from_tau(b, taux, tauy)
+    ref = w.reshape(b.shape2)
+    assert np.linalg.norm(wekp - ref) <= 1e-14 * np.linalg.norm(ref)
+
+
+def test_adv_diff_conserves_heat_with_no_flux_walls():
+    b, prm, o, taux, tauy, p1, _ = _case()
+    uek, vek, _, _ = ekman(taux, tauy, b.dx, b.dy, b.fnot, prm.hm)
+    dp_dx = (p1[:, 1:] - p1[:, :-1]) / b.dx
+    dp_dy = (p1[1:, :] - p1[:-1, :]) / b.dy
+    a = o.adv_diff(dp_dx, dp_dy, uek, vek)
+    assert abs(a.sum()) <= 1e-12 * np.abs(a).sum()
+
+
+def test_entrainment_has_zero_mean_and_sst_is_adjusted():
+    b, prm, o, taux, tauy, p1, rng = _case(seed=3)
+    uek, vek, wekt, _ = ekman(taux, tauy, b.dx, b.dy, b.fnot, prm.hm)
+    fnet = 50.0 * rng.standard_normal(wekt.shape)
+    ent = np.ones((b.nl - 1, b.nyp, b.nxp))
+    xfo = o.step(p1, uek, vek, wekt, fnet, True, 3600.0, ent)
+    assert abs(xfo.sum()) <= 1e-12 * np.abs(xfo).sum()
+    assert np.all(ent[1:] == 0.0)
+    assert np.all(o.data >= prm.t1_rel)
+    # without compute_ent the entrainment is left as it was
+    ent2 = ent.copy()
+    o.step(p1, uek, vek, wekt, fnet, False, 3600.0, ent2)
+    assert np.array_equal(ent2, ent)
