@@ -194,6 +194,52 @@ def run_adjoint(reps=3, n=257, dx=20e3, ah4=2.0e10, nsteps=200, every=20, tdt=36
             "timer": "CUDA events on the handle's stream, median of %d runs" % reps}
 
 
+def coupled_e2e(g, b, tdt, msteps, nbatch):
+    """The ocean step of the coupled driver (driver.F90:95-107) with the mixed
+    layer on the device: per model step the wind stress (taux, tauy at p
+    points) and the net heat flux (T points) cross from pinned host memory,
+    oqg_ocean_forcing runs ekman_from_tau and step_oml into the handle's
+    forcing, and step_qg runs; p(:,:,1) and ent stay on the device.  Host
+    clock, median over nbatch batches of msteps model steps."""
+    import torch
+    from openqg_b200.core import OceanMixedLayer, lib
+    from openqg_b200.params import double_gyre_tau
+    L = lib()
+    taux, tauy = double_gyre_tau(b)
+    nyt, nxt = b.nyp - 1, b.nxp - 1
+    yy = np.linspace(0.0, 1.0, nyt)[:, None]
+    sst = 12.0 + 3.0 * np.cos(np.pi * yy) * np.ones((1, nxt))
+    m = OceanMixedLayer(g, hm=100.0, rho_cp=4.0e6, t1_rel=10.0, dt_12=5.0, st2d=2.0e3, st4d=0.0, ycexp=1.0)
+    m.set_sst(sst, sst)
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64)).pin_memory()
+    tx, ty = pin(taux), pin(tauy)
+    fn = pin(20.0 * np.cos(np.pi * yy) * np.ones((1, nxt)))
+    args = [ctypes.c_void_p(t.data_ptr()) for t in (tx, ty, fn)]
+
+    def batch():
+        for _ in range(msteps):
+            rc = L.oqg_ocean_forcing(m.h, *args, 1, ctypes.c_double(tdt))
+            rc |= L.oqg_step(g.h, ctypes.c_double(tdt), 1)
+            if rc:
+                raise RuntimeError(L.oqg_last_error().decode())
+        g.sync()
+
+    batch()
+    times = []
+    for _ in range(nbatch):
+        t0 = time.perf_counter()
+        batch()
+        times.append((time.perf_counter() - t0) * 1e3)
+    m.close()
+    ms = statistics.median(times)
+    cells = b.nxp * b.nyp * b.nl
+    return {"value": cells * msteps / (ms / 1e3) / 1e6, "unit": "Mcell-layer-steps/s",
+            "h2d_bytes_per_step": msteps * (2 * b.nxp * b.nyp + nxt * nyt) * 8, "d2h_bytes_per_step": 0,
+            "pattern": "per model step: upload taux, tauy, fnetoc; ekman + ocean mixed layer + step on the "
+                       "device (p(:,:,1), wekp and ent stay there)",
+            "timer": "host clock, median of %d steps" % nbatch}
+
+
 def initial_inputs(b, seed, reference=False):
     """Seeded initial pressure and the double-gyre Ekman pumping.  The
     reference arm computes the pumping with the CPU restatement."""
@@ -504,6 +550,9 @@ def run_ours(args):
     e2e_value = replica_value(e2e_ms, ws, cells, msteps, e2e_steps)
     h2d = msteps * (b.nxp * b.nyp * 8) * b.nl        # wekp + (nl-1) ent layers
     d2h = msteps * b.nxp * b.nyp * 8
+    coupled = None
+    if prec == OQG_FP64 and not b.cyclic:
+        coupled = coupled_e2e(g, b, tdt, msteps, e2e_steps)
 
     # variant: the same basin with FP32 bulk arithmetic
     variants = {}
@@ -574,6 +623,7 @@ def run_ours(args):
         "e2e": {"value": e2e_value, "unit": "Mcell-layer-steps/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "timer": "host clock, median of %d steps" % e2e_steps,
                 "pattern": "per model step: upload wekp+ent, step, read p(:,:,1)"},
+        "e2e_coupled_ocean": coupled,
         "gpu_launches": args.steps * msteps * 4,
         "host_cpus_bound": numa_cpus,
         "clocks": clk.summary(),
