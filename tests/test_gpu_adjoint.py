@@ -34,9 +34,14 @@ def _need_gpu(gpu_required):
     pass
 
 
-def _basin(n=33):
+def _basin(n=33, nl=3):
     b = ocean_double_gyre(n, dx=40.0e3, ah4=2.0e11)
     b.ah2 = [300.0, 200.0, 100.0]   # exercise the Laplacian friction too
+    if nl == 2:
+        b.h, b.gp, b.ah2, b.ah4 = [1000.0, 3000.0], [0.02], [300.0, 100.0], [2.0e11] * 2
+    elif nl == 4:
+        b.h, b.gp = [300.0, 500.0, 800.0, 2400.0], [0.04, 0.02, 0.01]
+        b.ah2, b.ah4 = [300.0, 200.0, 150.0, 100.0], [2.0e11] * 4
     return b
 
 
@@ -67,10 +72,11 @@ def _dp(a):
     return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
 
 
-@pytest.mark.parametrize("step_no", [1, 2])
-def test_one_step_vjp_matches_autograd(step_no):
-    """step_no 1 is followed by suppress_comp_mode (period 25), step 2 is not."""
-    b = _basin()
+@pytest.mark.parametrize("step_no,nl", [(1, 3), (2, 3), (2, 2), (2, 4)])
+def test_one_step_vjp_matches_autograd(step_no, nl):
+    """step_no 1 is followed by suppress_comp_mode (period 25), step 2 is not;
+    nl 2 and 4 take the transposed constraint solve with 1 and 3 unknowns."""
+    b = _basin(nl=nl)
     g, o = QG(b), oracle.Oracle(b)
     st = _state(b, g)
     wekp = _forcing(b)

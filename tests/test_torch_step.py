@@ -3,6 +3,7 @@ the autograd reference of the adjoint, pinned against the C++ oracle: states
 within 1e-13 relative L2 over three steps (the first followed by
 suppress_comp_mode), and set_state's q, qm and mass constraints."""
 import numpy as np
+import pytest
 import torch
 
 import oracle
@@ -11,9 +12,14 @@ from openqg_b200.params import double_gyre_tau, initial_psi, ocean_double_gyre
 from tests.qg_numpy import rel_l2
 
 
-def _setup(n=33, seed=1):
+def _setup(n=33, seed=1, nl=3):
     b = ocean_double_gyre(n, dx=40.0e3, ah4=2.0e11)
     b.ah2 = [300.0, 200.0, 100.0]
+    if nl == 2:
+        b.h, b.gp, b.ah2, b.ah4 = [1000.0, 3000.0], [0.02], [300.0, 100.0], [2.0e11] * 2
+    elif nl == 4:
+        b.h, b.gp = [300.0, 500.0, 800.0, 2400.0], [0.04, 0.02, 0.01]
+        b.ah2, b.ah4 = [300.0, 200.0, 150.0, 100.0], [2.0e11] * 4
     o = oracle.Oracle(b)
     p = b.fnot * initial_psi(b, seed=seed)
     pm = p + 0.05 * b.fnot * initial_psi(b, seed=seed + 5)
@@ -36,8 +42,9 @@ def test_init_state_matches_oracle():
     assert rel_l2(st[5].numpy(), c["dpip"]) <= 1e-13
 
 
-def test_steps_match_oracle():
-    b, o, p, pm, w = _setup()
+@pytest.mark.parametrize("nl", [2, 3, 4])
+def test_steps_match_oracle(nl):
+    b, o, p, pm, w = _setup(nl=nl)
     tb = TorchBox(b, o)
     st = tb.init_state(torch.tensor(p), torch.tensor(pm))
     W = torch.tensor(w)
