@@ -278,7 +278,7 @@ __device__ __forceinline__ double arakawa9(const double (&P)[3][3], const double
 #define ADJ_TX 32
 #define ADJ_TY 16
 
-template <int NL>
+template <int NL, bool ALL>
 __global__ void __launch_bounds__(256, 3) k_adj_vort(const BasinDev *__restrict__ bas, AdjFields a,
                                                   const double *__restrict__ P, const double *__restrict__ Q,
                                                   double tdt, int tiles_x, int tiles_y) {
@@ -290,24 +290,67 @@ __global__ void __launch_bounds__(256, 3) k_adj_vort(const BasinDev *__restrict_
     constexpr int GW = ADJ_TX + 6, GH = ADJ_TY + 6;   // g, halo 3
     constexpr int AW = ADJ_TX + 4, AH = ADJ_TY + 4;   // t1, halo 2
     constexpr int BW = ADJ_TX + 2, BH = ADJ_TY + 2;   // t2, p, q, halo 1
-    __shared__ double G[GH][GW], T1[AH][AW], T2[BH][BW], Ps[BH][BW], Qs[BH][BW];
-    const int tile = blockIdx.x % (tiles_x * tiles_y), k = blockIdx.x / (tiles_x * tiles_y);
+    constexpr int NG = ALL ? NL : 1;                  // layers of g held at once
+    __shared__ double G[NG][GH][GW], T1[AH][AW], T2[BH][BW], Ps[BH][BW], Qs[BH][BW];
+    const int tile = blockIdx.x % (tiles_x * tiles_y);
     const int x0 = (tile % tiles_x) * ADJ_TX, y0 = (tile / tiles_x) * ADJ_TY;
     const double fx = b.fx, fy = b.fy;
-    double wk[NL], wc[NL];
+    if (ALL) {
+        // every layer's g from one pass over the modal solutions (each s_m
+        // and phi_m value is read once for all layers)
+        __shared__ double sW[2][NL][NL];   // f0 ctl2m(k,m) and its product with c_m
+        if (threadIdx.x < NL * NL) {
+            const int k = threadIdx.x / NL, m = threadIdx.x - k * NL;
+            sW[0][k][m] = b.fnot * b.ctl2m[k + NL * m];
+            sW[1][k][m] = sW[0][k][m] * a.scal[16 + m];
+        }
+        __syncthreads();
+        for (int e = threadIdx.x; e < GH * GW; e += 256) {
+            const int r = e / GW, c = e - r * GW;
+            const int i = x0 - 3 + c, j = y0 - 3 + r;
+            if (i <= 0 || i >= nxp - 1 || j <= 0 || j >= nyp - 1) {
 #pragma unroll
-    for (int m = 0; m < NL; ++m) {
-        wk[m] = b.fnot * b.ctl2m[k + NL * m];
-        wc[m] = wk[m] * a.scal[16 + m];
+                for (int k = 0; k < NL; ++k) G[k % NG][r][c] = 0.0;
+                continue;
+            }
+            const size_t o = (size_t)j * px + i;
+            double sv[NL], pv[NL];
+#pragma unroll
+            for (int m = 0; m < NL; ++m) {
+                sv[m] = a.s[m * n2 + o];
+                pv[m] = a.phi[m * n2 + o];
+            }
+#pragma unroll
+            for (int k = 0; k < NL; ++k) {
+                double v = a.lq[k * n2 + o];
+#pragma unroll
+                for (int m = 0; m < NL; ++m) v += sW[0][k][m] * sv[m] + sW[1][k][m] * pv[m];
+                G[k % NG][r][c] = v;
+            }
+        }
+    }
+#pragma unroll 1
+    for (int kk = 0; kk < (ALL ? NL : 1); ++kk) {
+    const int k = ALL ? kk : blockIdx.x / (tiles_x * tiles_y);
+    double (*Gk)[GW] = G[ALL ? kk : 0];
+    if (!ALL) {
+        double wk[NL], wc[NL];
+#pragma unroll
+        for (int m = 0; m < NL; ++m) {
+            wk[m] = b.fnot * b.ctl2m[k + NL * m];
+            wc[m] = wk[m] * a.scal[16 + m];
+        }
+        // constant strides (256 threads) let the staging loop unroll and keep
+        // its loads in flight together
+#pragma unroll
+        for (int e = threadIdx.x; e < GH * GW; e += 256) {
+            const int r = e / GW, c = e - r * GW;
+            Gk[r][c] = lam_qnew<NL>(b, a, wk, wc, k, x0 - 3 + c, y0 - 3 + r);
+        }
+    } else if (kk > 0) {
+        __syncthreads();   // the previous layer's tiles are no longer read
     }
     const double *p = P + k * n2, *q = Q + k * n2;
-    // constant strides (256 threads) let the staging loops unroll and keep
-    // their loads in flight together
-#pragma unroll
-    for (int e = threadIdx.x; e < GH * GW; e += 256) {
-        const int r = e / GW, c = e - r * GW;
-        G[r][c] = lam_qnew<NL>(b, a, wk, wc, k, x0 - 3 + c, y0 - 3 + r);
-    }
 #pragma unroll
     for (int e = threadIdx.x; e < BH * BW; e += 256) {
         const int r = e / BW, c = e - r * BW;
@@ -324,8 +367,8 @@ __global__ void __launch_bounds__(256, 3) k_adj_vort(const BasinDev *__restrict_
         const int i = x0 - 2 + c, j = y0 - 2 + r;
         double v = 0.0;
         if (i >= 0 && i < nxp && j >= 0 && j < nyp)
-            v = fx * (G[r + 1][c] + G[r + 1][c + 2] - 2.0 * G[r + 1][c + 1]) +
-                fy * (G[r][c + 1] + G[r + 2][c + 1] - 2.0 * G[r + 1][c + 1]);
+            v = fx * (Gk[r + 1][c] + Gk[r + 1][c + 2] - 2.0 * Gk[r + 1][c + 1]) +
+                fy * (Gk[r][c + 1] + Gk[r + 2][c + 1] - 2.0 * Gk[r + 1][c + 1]);
         T1[r][c] = v;
     }
     __syncthreads();
@@ -361,7 +404,7 @@ __global__ void __launch_bounds__(256, 3) k_adj_vort(const BasinDev *__restrict_
         for (int c = -1; c <= 1; ++c)
 #pragma unroll
             for (int e = -1; e <= 1; ++e) {
-                g3[c + 1][e + 1] = G[rg + c][cg + e];
+                g3[c + 1][e + 1] = Gk[rg + c][cg + e];
                 p3[c + 1][e + 1] = Ps[rb + c][cb + e];
                 q3[c + 1][e + 1] = Qs[rb + c][cb + e];
             }
@@ -420,6 +463,7 @@ __global__ void __launch_bounds__(256, 3) k_adj_vort(const BasinDev *__restrict_
         a.lp[o] = tdt * v;
         if (k == 0) a.lw[(size_t)j * px + i] += tdt * b.c_wind * g;
     }
+    }   // layers
 }
 
 // The transpose of set_state (qcomp, vorsubs.F90:27-56; init_mass_constr,

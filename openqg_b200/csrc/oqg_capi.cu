@@ -1658,7 +1658,14 @@ static void launch_adj_step_t(oqg_handle *h, const double *P, const double *Q, d
     launch_pdl(k_adj_wall<NL>, OQG_ADJ_CTAS, OQG_ADJ_THREADS, 0, h->st, d, a);
     launch_solve(h, a.s, true);
     const int tx = (b.nxp + ADJ_TX - 1) / ADJ_TX, ty = (b.nyp + ADJ_TY - 1) / ADJ_TY;
-    launch_pdl(k_adj_vort<NL>, tx * ty * NL, 256, 0, h->st, d, a, P, Q, tdt, tx, ty);
+    // large grids: one CTA per tile for all layers (the modal solutions are
+    // read once); small ones: one CTA per tile and layer, to fill the GPU
+    bool all = false;
+    if constexpr (NL <= 3) all = tx * ty >= 3 * 148 * 3;
+    if constexpr (NL <= 3) {
+        if (all) launch_pdl(k_adj_vort<NL, true>, tx * ty, 256, 0, h->st, d, a, P, Q, tdt, tx, ty);
+    }
+    if (!all) launch_pdl(k_adj_vort<NL, false>, tx * ty * NL, 256, 0, h->st, d, a, P, Q, tdt, tx, ty);
     // the state adjoints change roles: (p, pm, q, qm) of the step's input
     // (nu now holds lam_qm; the old lam_q buffer becomes the scratch)
     std::swap(a.lp, a.lpm);
