@@ -491,6 +491,8 @@ def run_ours(args):
     g = QG(b)
     g.set_state(p, p)
     g.set_forcing(w, None, ts, tn)
+    # the vorticity tile height, measured on this GPU (oqg_autotune)
+    tile_rows, tune_ms = g.autotune(tdt, 20)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")   # 256 MiB > L2
     for _ in range(args.warmup):
         g.step(tdt, msteps)
@@ -561,6 +563,7 @@ def run_ours(args):
         gm = QG(bm)
         gm.set_state(p, p)
         gm.set_forcing(w, None, ts, tn)
+        gm.autotune(tdt, 20)
         for _ in range(args.warmup):
             gm.step(tdt, msteps)
         barrier()
@@ -617,6 +620,8 @@ def run_ours(args):
         "data": "synthetic",
         "config": {"workload": label, "nxp": b.nxp, "nyp": b.nyp, "nl": b.nl,
                    "model_steps_per_step": msteps, "tdt_s": tdt,
+                   "tile_rows": tile_rows,
+                   "autotune_ms_per_step": {str(k): round(v, 5) for k, v in tune_ms.items()},
                    "l2": "flushed (256 MiB write) before every timed step",
                    "parallelism": "replicas" if ws > 1 else "single basin"},
         "roofline": roof,

@@ -252,6 +252,18 @@ int oqg_profile_phases(oqg_handle *h, double tdt, int nsteps, double *ms);
 /* CUDA stream of the handle (a cudaStream_t). */
 int oqg_stream(oqg_handle *h, void **stream);
 
+/* Measures the vorticity kernel's tile heights (8..17 rows of 60 columns)
+ * on the device: for each, nsteps (>= 2) steps of tdt from the handle's
+ * current state, timed with CUDA events; keeps the fastest, restores the
+ * state, and records the height for the basin's shape and precision, so
+ * handles created afterwards in this process start from it.  *best_vty
+ * (may be NULL) gets the height; ms (NULL or >= 18 doubles) gets the time
+ * per step of each height at index height.  Results do not depend on the
+ * height (each point is computed the same way in any tile). */
+int oqg_autotune(oqg_handle *h, double tdt, int nsteps, int *best_vty, double *ms);
+/* Current tile height of the vorticity kernel. */
+int oqg_get_vty(oqg_handle *h, int *vty);
+
 /* ---------------------------------------------------------------------
  * Ensembles: many independent basins of uneven size stepped together by one
  * launch per phase (captured in a CUDA graph).  Members keep the semantics of

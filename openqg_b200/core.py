@@ -93,6 +93,8 @@ def lib():
     L.oqg_oml_get_sst.argtypes = [vp, vp, vp]
     L.oqg_ocean_forcing.argtypes = [vp, vp, vp, vp, ctypes.c_int, ctypes.c_double]
     L.oqg_get_forcing.argtypes = [vp, _dp, _dp]
+    L.oqg_autotune.argtypes = [vp, ctypes.c_double, ctypes.c_int, ctypes.POINTER(ctypes.c_int), _dp]
+    L.oqg_get_vty.argtypes = [vp, ctypes.POINTER(ctypes.c_int)]
     L.oqg_adj_segment.argtypes = [vp, vp, vp, ctypes.c_size_t, ctypes.c_int, ctypes.c_double, ctypes.c_longlong]
     _lib = L
     return L
@@ -290,6 +292,19 @@ class QG:
         ms = np.zeros(4)
         _check(lib().oqg_profile_phases(self.h, float(tdt), int(nsteps), _p(ms)), "oqg_profile_phases")
         return ms
+
+    def autotune(self, tdt: float, nsteps: int = 20):
+        """Measures the vorticity kernel's tile heights on the device and keeps
+        the fastest (oqg_autotune); returns (height, {height: ms per step})."""
+        best = ctypes.c_int()
+        ms = np.full(18, np.nan)
+        _check(lib().oqg_autotune(self.h, float(tdt), int(nsteps), ctypes.byref(best), _p(ms)), "oqg_autotune")
+        return best.value, {v: float(ms[v]) for v in range(8, 18) if np.isfinite(ms[v])}
+
+    def tile_rows(self) -> int:
+        v = ctypes.c_int()
+        _check(lib().oqg_get_vty(self.h, ctypes.byref(v)), "oqg_get_vty")
+        return v.value
 
     def stream(self) -> int:
         s = ctypes.c_void_p()

@@ -381,7 +381,7 @@ static bool make_tmaps(oqg_handle *h) {
                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
     }
     if (!ok) return false;
-    void *d = dalloc<unsigned char>(h, (size_t)OQG_NTMAP * OQG_TMAP_BYTES);
+    void *d = b.tmaps ? const_cast<void *>(b.tmaps) : dalloc<unsigned char>(h, (size_t)OQG_NTMAP * OQG_TMAP_BYTES);
     if (!d) return false;
     if (cudaMemcpy(d, maps.data(), (size_t)OQG_NTMAP * sizeof(CUtensorMap), cudaMemcpyHostToDevice) != cudaSuccess)
         return false;
@@ -602,6 +602,33 @@ int oqg_version(char *buf, int buflen) {
 // batched: a member of an ensemble, whose tiles need not fill whole waves on
 // their own (the ensemble's work list does), so the vorticity tiles take the
 // tallest height and the least halo.
+// Tile heights of the vorticity kernel measured by oqg_autotune, per basin
+// shape and precision; a handle created later with the same shape starts
+// from the measured height instead of the waves model.
+struct TunedVty {
+    int nxp, nyp, nl, cyclic, mixed, vty;
+};
+static std::mutex g_tuned_mu;
+static std::vector<TunedVty> g_tuned;
+
+static int tuned_vty(const oqg_params &P, bool mixed) {
+    std::lock_guard<std::mutex> lk(g_tuned_mu);
+    for (const TunedVty &t : g_tuned)
+        if (t.nxp == P.nxp && t.nyp == P.nyp && t.nl == P.nl && t.cyclic == (P.cyclic != 0) && t.mixed == (int)mixed)
+            return t.vty;
+    return 0;
+}
+
+static void record_vty(const oqg_params &P, bool mixed, int vty) {
+    std::lock_guard<std::mutex> lk(g_tuned_mu);
+    for (TunedVty &t : g_tuned)
+        if (t.nxp == P.nxp && t.nyp == P.nyp && t.nl == P.nl && t.cyclic == (P.cyclic != 0) && t.mixed == (int)mixed) {
+            t.vty = vty;
+            return;
+        }
+    g_tuned.push_back(TunedVty{P.nxp, P.nyp, P.nl, P.cyclic != 0, (int)mixed, vty});
+}
+
 static int create_impl(const oqg_params *prm, oqg_handle **out, bool batched) {
     if (!prm || !out) return fail(OQG_EINVAL, "null argument");
     *out = nullptr;
@@ -668,6 +695,8 @@ static int create_impl(const oqg_params *prm, oqg_handle **out, bool batched) {
             const long cost = waves * (vt + 6);
             if (best_cost < 0 || cost < best_cost) { best_cost = cost; best = vt; }
         }
+        const int tuned = tuned_vty(P, h->mixed);
+        if (tuned > 0 && !batched) best = tuned;
         b.vty = best;
         b.tiles_y = (P.nyp + b.vty - 1) / b.vty;
     }
@@ -756,7 +785,8 @@ static int create_impl(const oqg_params *prm, oqg_handle **out, bool batched) {
         b.hbc1 = dalloc<double>(h, (size_t)b.nl * b.nyp);
         b.hbc2 = dalloc<double>(h, (size_t)b.nl * b.nyp);
     }
-    b.part_tile = dalloc<double>(h, (size_t)b.tiles_x * b.tiles_y * b.nl * OQG_NQ);
+    // sized for the shortest tiles (8 rows), so oqg_autotune can retile in place
+    b.part_tile = dalloc<double>(h, (size_t)b.tiles_x * ((P.nyp + 7) / 8) * b.nl * OQG_NQ);
     b.part_col = dalloc<double>(h, (size_t)b.nl * b.nk);
     b.st = dalloc<DevState>(h, 2);
     b.frc = dalloc<DevForcing>(h, 1);
@@ -821,7 +851,7 @@ static int create_impl(const oqg_params *prm, oqg_handle **out, bool batched) {
     for (int i = 0; i < h->nx; ++i) wx[i] = Work{0, i};
     for (int i = 0; i < h->nys; ++i) wy[i] = Work{0, i};
     for (int i = 0; i < h->ni; ++i) wi[i] = Work{0, i};
-    h->d_wv = dalloc<Work>(h, wv.size());
+    h->d_wv = dalloc<Work>(h, (size_t)b.tiles_x * ((P.nyp + 7) / 8));
     h->d_wx = dalloc<Work>(h, wx.size());
     h->d_wy = dalloc<Work>(h, wy.size());
     h->d_wi = dalloc<Work>(h, wi.size());
@@ -2005,6 +2035,76 @@ int oqg_get_forcing(oqg_handle *h, double *wekp, double *ent) {
         }
     }
     CK(cudaStreamSynchronize(h->st));
+    return OQG_OK;
+}
+
+}  // extern "C"
+
+// ================================================================ autotuning
+// Rebuilds the vorticity kernel's tiling for tile height vt: the work list,
+// the tensor maps, the shared-memory size; drops the captured graphs.
+static int set_vty(oqg_handle *h, int vt) {
+    BasinDev &b = h->hb;
+    b.vty = vt;
+    b.tiles_y = (b.nyp + vt - 1) / vt;
+    h->nv = b.tiles_x * b.tiles_y;
+    std::vector<Work> wv(h->nv);
+    for (int i = 0; i < h->nv; ++i) wv[i] = Work{0, i};
+    CK(cudaMemcpy(h->d_wv, wv.data(), wv.size() * sizeof(Work), cudaMemcpyHostToDevice));
+    if (b.tmaps && !make_tmaps(h)) return fail(OQG_ECUDA, "tensor maps could not be encoded");
+    h->smem_v = vort_smem_bytes(vt, (int)h->esz);
+    set_attrs(h);
+    h->hb64.vty = b.vty;
+    h->hb64.tiles_y = b.tiles_y;
+    h->hb64.tmaps = b.tmaps;
+    drop_graphs(h);
+    return push_desc(h);
+}
+
+extern "C" {
+
+int oqg_get_vty(oqg_handle *h, int *vty) {
+    if (!h || !vty) return fail(OQG_EINVAL, "bad argument");
+    *vty = h->hb.vty;
+    return OQG_OK;
+}
+
+int oqg_autotune(oqg_handle *h, double tdt, int nsteps, int *best_vty, double *ms) {
+    if (!h || nsteps < 2 || !(tdt > 0.0)) return fail(OQG_EINVAL, "bad argument");
+    size_t full = 0;
+    oqg_state_bytes(h, &full, nullptr);
+    void *save = nullptr;
+    if (cudaMalloc(&save, full) != cudaSuccess) return fail(OQG_ECUDA, "cudaMalloc of the state copy failed");
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    int rc = oqg_state_save(h, save);
+    int best = h->hb.vty;
+    float best_ms = -1.0f;
+    for (int vt = 8; vt <= VTYMAX && rc == OQG_OK; ++vt) {
+        if ((rc = set_vty(h, vt))) break;
+        // warm up (captures the graphs), then time nsteps from the saved state
+        if ((rc = oqg_state_load(h, save)) || (rc = oqg_step(h, tdt, nsteps))) break;
+        if ((rc = oqg_state_load(h, save))) break;
+        if (cudaStreamSynchronize(h->st) != cudaSuccess) { rc = fail(OQG_ECUDA, "autotune warm-up failed"); break; }
+        cudaEventRecord(e0, h->st);
+        if ((rc = oqg_step(h, tdt, nsteps))) break;
+        cudaEventRecord(e1, h->st);
+        if (cudaEventSynchronize(e1) != cudaSuccess) { rc = fail(OQG_ECUDA, "autotune timing failed"); break; }
+        float t = 0.0f;
+        cudaEventElapsedTime(&t, e0, e1);
+        if (ms) ms[vt] = t / nsteps;
+        if (best_ms < 0.0f || t < best_ms) { best_ms = t; best = vt; }
+    }
+    if (rc == OQG_OK) rc = set_vty(h, best);
+    if (rc == OQG_OK) rc = oqg_state_load(h, save);
+    if (rc == OQG_OK && cudaStreamSynchronize(h->st) != cudaSuccess) rc = fail(OQG_ECUDA, "autotune restore failed");
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(save);
+    if (rc) return rc;
+    record_vty(h->prm, h->mixed, best);
+    if (best_vty) *best_vty = best;
     return OQG_OK;
 }
 
