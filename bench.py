@@ -100,6 +100,8 @@ def run_ensemble(precision, steps, warmup, msteps, flush, tdt=3600.0):
     for i, (p, w, ts, tn) in enumerate(inputs):
         e.set_state(i, p, p)
         e.set_forcing(i, w, None, ts, tn)
+    # one vorticity tile height for all members, measured (oqg_ensemble_autotune)
+    tile_rows, _ = e.autotune(tdt, 4)
     for _ in range(warmup):
         e.step(tdt, msteps)
     e.sync()
@@ -117,7 +119,7 @@ def run_ensemble(precision, steps, warmup, msteps, flush, tdt=3600.0):
     e.sync()
     cells = sum(b.nxp * b.nyp * b.nl for b in basins)
     e.close()
-    return cells, total
+    return cells, total, tile_rows
 
 
 # box sizes of the adjoint runs: n -> (dx, ah4, tdt)
@@ -572,9 +574,10 @@ def run_ours(args):
         gm.close()
         # the batched ensemble: 256 basins of uneven size, one launch per phase
         for vprec, vname in ((OQG_MIXED, "ensemble256_mixed"), (OQG_FP64, "ensemble256_fp64")):
-            cells_e, te = run_ensemble(vprec, args.steps, args.warmup, msteps, flush)
+            cells_e, te, rows_e = run_ensemble(vprec, args.steps, args.warmup, msteps, flush)
             te = max_over_ranks(te, pg, "cuda")
             variants[vname] = replica_value(te, ws, cells_e, msteps, args.steps)
+            variants[vname + "_tile_rows"] = rows_e
         variants["ensemble_config"] = ("256 ocean 3-layer boxes, sizes uniform in %s, dx 20 km, "
                                        "per-member wind 0.05-0.15 N/m^2 and ah4 1e10-4e10; %d "
                                        "cell-layers per step" % (list(ENSEMBLE_SIZES), cells_e))

@@ -288,6 +288,10 @@ int oqg_ensemble_step(oqg_ensemble *e, const double *tdt, int nsteps);
 int oqg_ensemble_sync(oqg_ensemble *e);
 /* The CUDA stream (cudaStream_t) the ensemble's steps run on. */
 int oqg_ensemble_stream(oqg_ensemble *e, void **stream);
+/* oqg_autotune for an ensemble: one vorticity tile height for all members,
+ * measured over nsteps steps (tdt per member) from the members' current
+ * states, which are restored.  best_vty / ms as for oqg_autotune. */
+int oqg_ensemble_autotune(oqg_ensemble *e, const double *tdt, int nsteps, int *best_vty, double *ms);
 
 /* ---------------------------------------------------------------------
  * The ocean half of the coupler on the device: the Ekman fields from the

@@ -93,6 +93,7 @@ def lib():
     L.oqg_oml_get_sst.argtypes = [vp, vp, vp]
     L.oqg_ocean_forcing.argtypes = [vp, vp, vp, vp, ctypes.c_int, ctypes.c_double]
     L.oqg_get_forcing.argtypes = [vp, _dp, _dp]
+    L.oqg_ensemble_autotune.argtypes = [vp, _dp, ctypes.c_int, ctypes.POINTER(ctypes.c_int), _dp]
     L.oqg_autotune.argtypes = [vp, ctypes.c_double, ctypes.c_int, ctypes.POINTER(ctypes.c_int), _dp]
     L.oqg_get_vty.argtypes = [vp, ctypes.POINTER(ctypes.c_int)]
     L.oqg_adj_segment.argtypes = [vp, vp, vp, ctypes.c_size_t, ctypes.c_int, ctypes.c_double, ctypes.c_longlong]
@@ -396,6 +397,17 @@ class Ensemble:
 
     def sync(self):
         _check(lib().oqg_ensemble_sync(self.e), "oqg_ensemble_sync")
+
+    def autotune(self, tdt, nsteps: int = 10):
+        """One vorticity tile height for all members, measured on the device
+        from the members' current states (restored afterwards); returns
+        (height, {height: ms per ensemble step})."""
+        t = np.broadcast_to(np.asarray(tdt, dtype=np.float64), (len(self.members),)).copy()
+        best = ctypes.c_int()
+        ms = np.full(18, np.nan)
+        _check(lib().oqg_ensemble_autotune(self.e, _p(t), int(nsteps), ctypes.byref(best), _p(ms)),
+               "oqg_ensemble_autotune")
+        return best.value, {v: float(ms[v]) for v in range(8, 18) if np.isfinite(ms[v])}
 
     def stream(self) -> int:
         s = ctypes.c_void_p()

@@ -533,6 +533,7 @@ struct oqg_ensemble {
     int par = 0;
     cudaGraphExec_t gexec[2] = {nullptr, nullptr};
     std::vector<void *> allocs;
+    size_t wv_cap = 0;                 // entries the vorticity work list can hold
 };
 
 #define OQG_DISPATCH_E(FN, e, ...)                                                    \
@@ -1536,6 +1537,7 @@ int oqg_ensemble_create(const oqg_params *members, int nmembers, oqg_ensemble **
         return fail(OQG_EUNSUPPORTED, "ensemble member too large for the shared-memory tiling");
     }
     e->nv = (int)wv.size(); e->nx = (int)wx.size(); e->nys = (int)wy.size(); e->ni = (int)wi.size();
+    e->wv_cap = wv.size();
     auto up = [&](const void *src, size_t bytes) -> void * {
         void *d = nullptr;
         if (cudaMalloc(&d, bytes) != cudaSuccess) return nullptr;
@@ -2104,6 +2106,108 @@ int oqg_autotune(oqg_handle *h, double tdt, int nsteps, int *best_vty, double *m
     cudaFree(save);
     if (rc) return rc;
     record_vty(h->prm, h->mixed, best);
+    if (best_vty) *best_vty = best;
+    return OQG_OK;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------- ensemble autotuning
+// All members retiled to tile height vt: member descriptors and tensor maps,
+// the concatenated vorticity work list (largest members first), the shared
+// memory, the graphs.
+static int ens_set_vty(oqg_ensemble *e, int vt) {
+    const int n = (int)e->m.size();
+    std::vector<int> order(n);
+    for (int i = 0; i < n; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int c) {
+        return (long)e->m[a]->hb.nxp * e->m[a]->hb.nyp > (long)e->m[c]->hb.nxp * e->m[c]->hb.nyp;
+    });
+    std::vector<Work> wv;
+    for (int i = 0; i < n; ++i) {
+        oqg_handle *h = e->m[i];
+        BasinDev &b = h->hb;
+        b.vty = vt;
+        b.tiles_y = (b.nyp + vt - 1) / vt;
+        if (b.tmaps && !make_tmaps(h)) return fail(OQG_ECUDA, "tensor maps could not be encoded");
+        h->hb64.vty = b.vty;
+        h->hb64.tiles_y = b.tiles_y;
+        h->hb64.tmaps = b.tmaps;
+        int rc = push_desc(h);
+        if (rc) return rc;
+        CK(cudaStreamSynchronize(h->st));
+        e->hb[i].vty = b.vty;
+        e->hb[i].tiles_y = b.tiles_y;
+        e->hb[i].tmaps = b.tmaps;
+    }
+    for (int i : order)
+        for (int k = 0; k < e->hb[i].tiles_x * e->hb[i].tiles_y; ++k) wv.push_back(Work{i, k});
+    if (wv.size() > e->wv_cap) {
+        void *d = nullptr;
+        if (cudaMalloc(&d, wv.size() * sizeof(Work)) != cudaSuccess) return fail(OQG_ECUDA, "out of device memory");
+        e->allocs.push_back(d);
+        e->d_wv = (Work *)d;
+        e->wv_cap = wv.size();
+    }
+    CK(cudaMemcpy(e->d_wv, wv.data(), wv.size() * sizeof(Work), cudaMemcpyHostToDevice));
+    e->nv = (int)wv.size();
+    e->smem_v = vort_smem_bytes(vt, (int)e->m[0]->esz);
+    OQG_DISPATCH_E(raise_ens_smem_t, e, e);
+    CK(cudaMemcpy(e->d_bas, e->hb.data(), n * sizeof(BasinDev), cudaMemcpyHostToDevice));
+    for (int i = 0; i < 2; ++i)
+        if (e->gexec[i]) { cudaGraphExecDestroy(e->gexec[i]); e->gexec[i] = nullptr; }
+    return OQG_OK;
+}
+
+extern "C" {
+
+int oqg_ensemble_autotune(oqg_ensemble *e, const double *tdt, int nsteps, int *best_vty, double *ms) {
+    if (!e || !tdt || nsteps < 2) return fail(OQG_EINVAL, "bad argument");
+    const int n = (int)e->m.size();
+    CK(cudaStreamSynchronize(e->st));
+    // every member's state, saved in the ensemble's current parity
+    std::vector<size_t> off(n + 1, 0);
+    for (int i = 0; i < n; ++i) {
+        size_t full = 0;
+        oqg_state_bytes(e->m[i], &full, nullptr);
+        off[i + 1] = off[i] + (full + 255) / 256 * 256;
+    }
+    char *save = nullptr;
+    if (cudaMalloc(&save, off[n]) != cudaSuccess) return fail(OQG_ECUDA, "cudaMalloc of the state copies failed");
+    auto each = [&](bool load) -> int {
+        for (int i = 0; i < n; ++i) {
+            oqg_handle *h = e->m[i];
+            h->par = e->par;
+            const int rc = load ? oqg_state_load(h, save + off[i]) : oqg_state_save(h, save + off[i]);
+            if (rc) return rc;
+            CK(cudaStreamSynchronize(h->st));
+        }
+        return OQG_OK;
+    };
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    int rc = each(false);
+    int best = e->hb[0].vty;
+    float best_ms = -1.0f;
+    for (int vt = 8; vt <= VTYMAX && rc == OQG_OK; ++vt) {
+        if ((rc = ens_set_vty(e, vt)) || (rc = each(true)) || (rc = oqg_ensemble_step(e, tdt, nsteps))) break;
+        if ((rc = oqg_ensemble_sync(e)) || (rc = each(true))) break;
+        cudaEventRecord(e0, e->st);
+        if ((rc = oqg_ensemble_step(e, tdt, nsteps))) break;
+        cudaEventRecord(e1, e->st);
+        if (cudaEventSynchronize(e1) != cudaSuccess) { rc = fail(OQG_ECUDA, "autotune timing failed"); break; }
+        float t = 0.0f;
+        cudaEventElapsedTime(&t, e0, e1);
+        if (ms) ms[vt] = t / nsteps;
+        if (best_ms < 0.0f || t < best_ms) { best_ms = t; best = vt; }
+    }
+    if (rc == OQG_OK) rc = ens_set_vty(e, best);
+    if (rc == OQG_OK) rc = each(true);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(save);
+    if (rc) return rc;
     if (best_vty) *best_vty = best;
     return OQG_OK;
 }

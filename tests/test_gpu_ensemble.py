@@ -53,7 +53,7 @@ def _run_pair(members, tdts, nsteps):
 
 
 def _assert_same(e, singles):
-    # members tile the vorticity kernel with the tallest tiles, single handles
+    # members tile the vorticity kernel with the tallest (or a tuned) height, single handles
     # with tiles fitted to whole waves; the channel strip sums and the wall
     # rows then round differently, so the match is to rounding, not bits
     for i, g in enumerate(singles):
@@ -109,3 +109,22 @@ def test_ensemble_rejects_bad_members():
     from openqg_b200.core import OqgError
     with pytest.raises(OqgError):
         Ensemble([ocean_double_gyre(33), atmos_channel(49, 25)])
+
+
+def test_ensemble_autotune_keeps_states_and_results():
+    """oqg_ensemble_autotune retiles every member to the measured height; the
+    members' states are restored, and stepping on matches single handles."""
+    members = [ocean_double_gyre(n, dx=20e3) for n in (129, 65, 97)]
+    e, singles = _run_pair(members, 3600.0, 2)
+    before = [e.get_state(i) for i in range(len(members))]
+    best, ms = e.autotune(3600.0, 4)
+    assert 8 <= best <= 17
+    assert sorted(ms) == list(range(8, 18))
+    for i in range(len(members)):
+        for a, r in zip(e.get_state(i), before[i]):
+            assert np.array_equal(a, r)
+    e.step(3600.0, 6)
+    e.sync()
+    for g in singles:
+        g.step(3600.0, 6)
+    _assert_same(e, singles)
