@@ -27,10 +27,17 @@ def _need_gpu(gpu_required):
     pass
 
 
-def _setup(n=65, precision=0, fluxs=True, seed=2):
+def _setup(n=65, precision=0, fluxs=True, seed=2, south=False, nl=3):
     b = ocean_double_gyre(n, dx=20.0e3, precision=precision)
+    if south:                      # southern hemisphere: the northern wall may carry the flux
+        b.fnot = -b.fnot
+    if nl == 2:
+        b.h, b.gp, b.ah2, b.ah4 = [1000.0, 3000.0], [0.02], [0.0, 0.0], [2.0e10] * 2
+    elif nl == 4:
+        b.h, b.gp = [300.0, 500.0, 800.0, 2400.0], [0.04, 0.02, 0.01]
+        b.ah2, b.ah4 = [0.0] * 4, [2.0e10] * 4
     prm = OmlParams(hm=100.0, rho_cp=4.0e6, t1_rel=10.0, dt_12=5.0, st2d=2.0e3, st4d=1.0e11, ycexp=1.0,
-                    fluxs=fluxs, sval=14.0)
+                    fluxs=fluxs and not south, fluxn=south, sval=14.0, nval=8.0)
     rng = np.random.default_rng(seed)
     nyt, nxt = b.nyp - 1, b.nxp - 1
     yy = np.linspace(0.0, 1.0, nyt)[:, None]
@@ -50,8 +57,11 @@ def _setup(n=65, precision=0, fluxs=True, seed=2):
     return b, prm, g, m, o, taux, tauy, fnet, p
 
 
-def test_forcing_matches_oracle():
-    b, prm, g, m, o, taux, tauy, fnet, _ = _setup()
+@pytest.mark.parametrize("south,nl", [(False, 3), (True, 3), (False, 2), (False, 4)])
+def test_forcing_matches_oracle(south, nl):
+    """Northern hemisphere with the southern flux condition, southern
+    hemisphere with the northern one; 2, 3 and 4 layers."""
+    b, prm, g, m, o, taux, tauy, fnet, _ = _setup(south=south, nl=nl)
     uek, vek, wekt, wekp = ekman(taux, tauy, b.dx, b.dy, b.fnot, prm.hm)
     ent = np.zeros((b.nl - 1,) + b.shape2)
     for it, ce in enumerate((True, False, True)):
