@@ -9,7 +9,7 @@ import pytest
 
 import oracle
 from openqg_b200.core import QG
-from openqg_b200.params import OQG_MIXED, double_gyre_tau, initial_psi, ocean_double_gyre
+from openqg_b200.params import OQG_MIXED, atmos_channel, double_gyre_tau, initial_psi, ocean_double_gyre
 from tests.qg_numpy import rel_l2
 
 pytestmark = pytest.mark.gpu
@@ -22,28 +22,37 @@ def _need_gpu(gpu_required):
 
 def _handle(b, seed=1):
     g = QG(b)
-    p = b.fnot * initial_psi(b, seed=seed)
-    w, ts, tn = oracle.ekman_from_tau(b, *double_gyre_tau(b))
+    p = b.fnot * initial_psi(b, seed=seed) * (30.0 if b.cyclic else 1.0)
+    if b.cyclic:
+        y = np.arange(b.nyp) * b.dy
+        taux = np.repeat((0.05 * np.sin(np.pi * y / y[-1]))[:, None], b.nxp, axis=1)
+        w, ts, tn = oracle.ekman_from_tau(b, taux, np.zeros_like(taux))
+    else:
+        w, ts, tn = oracle.ekman_from_tau(b, *double_gyre_tau(b))
     g.set_state(p, p)
     g.set_forcing(w, None, ts, tn)
     return g
 
 
-@pytest.mark.parametrize("precision", [0, OQG_MIXED])
-def test_autotune_keeps_state_and_results(precision):
-    b = ocean_double_gyre(161, dx=20e3, precision=precision)
+@pytest.mark.parametrize("precision,channel", [(0, False), (OQG_MIXED, False), (0, True)])
+def test_autotune_keeps_state_and_results(precision, channel):
+    """Box (tiles by TMA) in FP64 and mixed; channel (tiles by cp.async, strip
+    sums over the tiles of the boundary rows)."""
+    b = (atmos_channel(193, 97, precision=precision) if channel
+         else ocean_double_gyre(161, dx=20e3, precision=precision))
     g, ref = _handle(b), _handle(b)
-    g.step(3600.0, 3)
-    ref.step(3600.0, 3)
+    tdt = 360.0 if channel else 3600.0
+    g.step(tdt, 3)
+    ref.step(tdt, 3)
     before = g.get_state()
-    best, ms = g.autotune(3600.0, 6)
+    best, ms = g.autotune(tdt, 6)
     assert 8 <= best <= 17 and g.tile_rows() == best
     assert sorted(ms) == list(range(8, 18)) and all(v > 0 for v in ms.values())
     for a, r in zip(g.get_state(), before):
         assert np.array_equal(a, r)
     assert g.step_index() == 3
-    g.step(3600.0, 5)
-    ref.step(3600.0, 5)
+    g.step(tdt, 5)
+    ref.step(tdt, 5)
     tol = 1e-12 if precision == 0 else 1e-6
     for a, r in zip(g.get_state(), ref.get_state()):
         assert rel_l2(a, r) <= tol
