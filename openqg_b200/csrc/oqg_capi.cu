@@ -1930,7 +1930,7 @@ int oqg_oml_create(oqg_handle *h, const oqg_oml_params *prm, oqg_oml **out) {
     }
     m->allocs.push_back(x);
     double *d = (double *)x;
-    o.data = d; o.datam = d + nt; o.d2 = d + 2 * nt; o.wekt = d + 3 * nt; o.xfo = d + 4 * nt;
+    o.data = d; o.datam = d + nt; o.snew = d + 2 * nt; o.wekt = d + 3 * nt; o.xfo = d + 4 * nt;
     double *fn = d + 5 * nt;
     o.fnet = fn;
     o.taux = d + 6 * nt;
@@ -1990,30 +1990,28 @@ int oqg_ocean_forcing(oqg_oml *m, const double *taux, const double *tauy, const 
     CK(cudaMemcpyAsync(const_cast<double *>(o.tauy), tauy, np * sizeof(double), cudaMemcpyDefault, h->st));
     CK(cudaMemcpyAsync(const_cast<double *>(o.fnet), fnetoc, nt * sizeof(double), cudaMemcpyDefault, h->st));
     CK(cudaEventRecord(h->up_ev, h->st));
-    const int grid = std::min((int)((nt + 255) / 256), OQG_OML_CTAS);
-    k_oml_pre<<<grid, 256, 0, h->st>>>(o);
     const void *p1 = b.F[h->par];   // layer 1 of the current p (driver.F90:96-103)
     if (h->mixed) k_oml_step<float><<<OQG_OML_CTAS, 256, 0, h->st>>>(o, (const float *)p1, b.px, tdto, compute_ent);
     else k_oml_step<double><<<OQG_OML_CTAS, 256, 0, h->st>>>(o, (const double *)p1, b.px, tdto, compute_ent);
-    const int gp = std::min((int)((np + 255) / 256), 148 * 8);
     if (h->mixed)
-        k_oml_post<float><<<gp, 256, 0, h->st>>>(o, (float *)b.wekp, (float *)h->ent_buf, b.px, b.nl, compute_ent,
-                                                 OQG_OML_CTAS);
+        k_oml_post<float><<<b.nyp, 128, 0, h->st>>>(o, (float *)b.wekp, (float *)h->ent_buf, b.ent_rows, b.px, b.nl,
+                                                    compute_ent, OQG_OML_CTAS);
     else
-        k_oml_post<double><<<gp, 256, 0, h->st>>>(o, (double *)b.wekp, (double *)h->ent_buf, b.px, b.nl,
-                                                  compute_ent, OQG_OML_CTAS);
+        k_oml_post<double><<<b.nyp, 128, 0, h->st>>>(o, (double *)b.wekp, (double *)h->ent_buf, b.ent_rows, b.px,
+                                                     b.nl, compute_ent, OQG_OML_CTAS);
     CK(cudaGetLastError());
-    std::swap(o.data, o.datam);   // datam <- data, data <- the new sst
+    // datam <- data, data <- the new sst; the old datam becomes the next scratch
+    double *dm_old = o.datam;
+    o.datam = o.data;
+    o.data = o.snew;
+    o.snew = dm_old;
     if (compute_ent && b.ent != h->ent_buf) {
         b.ent = h->ent_buf;
         h->hb64.ent = b.ent;
         int rc = push_desc(h);
         if (rc) return rc;
     }
-    if (b.ent) {
-        if (h->mixed) k_ent_rows<float><<<b.nyp, 128, 0, h->st>>>(h->d_bas, 0);
-        else k_ent_rows<double><<<b.nyp, 128, 0, h->st>>>(h->d_bas, 0);
-    }
+    // (ent_rows came with the entrainment from k_oml_post)
     if (h->mixed) k_forcing_integrals<float><<<1, 512, 0, h->st>>>(h->d_bas, 0);
     else k_forcing_integrals<double><<<1, 512, 0, h->st>>>(h->d_bas, 0);
     h->frc_host[0] = 0.0;   // txis, txin: zero for a closed box (ekman.F90:60-70)

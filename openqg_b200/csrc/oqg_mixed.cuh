@@ -24,7 +24,7 @@ struct OmlDev {
     const double *taux, *tauy;   // [nyp][nxp]
     const double *fnet;          // [nyt][nxt] net heat flux into the ocean
     double *data, *datam;        // sst and its lagged value [nyt][nxt]
-    double *d2, *wekt, *xfo;     // del2_T(datam), T-grid Ekman pumping, entrainment [nyt][nxt]
+    double *snew, *wekt, *xfo;   // the next sst, T-grid Ekman pumping, entrainment [nyt][nxt]
     double *part;                // [OQG_OML_CTAS] partial sums of xfo
 };
 
@@ -40,27 +40,24 @@ __device__ __forceinline__ double oml_del2(const OmlDev &o, const double *t, int
     return (1.0 / (o.dx * o.dx)) * (right - left + top - bot);
 }
 
-// Ekman pumping at T points (ekman.F90:78-80) and del2_T of the lagged sst.
-__global__ void k_oml_pre(OmlDev o) {
-    for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < o.nxt * o.nyt; idx += gridDim.x * blockDim.x) {
-        const int j = idx / o.nxt, i = idx - j * o.nxt;
-        const double *tx = o.taux, *ty = o.tauy;
-        const int nxp = o.nxp;
-        // map_P_to_y_face / map_P_to_x_face of the stress
-        const double tyw = 0.5 * (ty[(size_t)(j + 1) * nxp + i] + ty[(size_t)j * nxp + i]);
-        const double tye = 0.5 * (ty[(size_t)(j + 1) * nxp + i + 1] + ty[(size_t)j * nxp + i + 1]);
-        const double txs = 0.5 * (tx[(size_t)j * nxp + i + 1] + tx[(size_t)j * nxp + i]);
-        const double txn = 0.5 * (tx[(size_t)(j + 1) * nxp + i + 1] + tx[(size_t)(j + 1) * nxp + i]);
-        o.wekt[idx] = (1.0 / (o.dx * o.fnot)) * (tye - tyw) - (1.0 / (o.dy * o.fnot)) * (txn - txs);
-        o.d2[idx] = oml_del2(o, o.datam, i, j, o.fluxn, o.nval, o.fluxs, o.sval);
-    }
+// Ekman pumping at T point (i, j) (ekman.F90:78-80) from map_P_to_y_face /
+// map_P_to_x_face of the stress.
+__device__ __forceinline__ double oml_wekt(const OmlDev &o, int i, int j) {
+    const double *tx = o.taux, *ty = o.tauy;
+    const int nxp = o.nxp;
+    const double tyw = 0.5 * (ty[(size_t)(j + 1) * nxp + i] + ty[(size_t)j * nxp + i]);
+    const double tye = 0.5 * (ty[(size_t)(j + 1) * nxp + i + 1] + ty[(size_t)j * nxp + i + 1]);
+    const double txs = 0.5 * (tx[(size_t)j * nxp + i + 1] + tx[(size_t)j * nxp + i]);
+    const double txn = 0.5 * (tx[(size_t)(j + 1) * nxp + i + 1] + tx[(size_t)(j + 1) * nxp + i]);
+    return (1.0 / (o.dx * o.fnot)) * (tye - tyw) - (1.0 / (o.dy * o.fnot)) * (txn - txs);
 }
 
-// step_oml at T points: advection (C grid, geostrophic from the layer-1
-// pressure P1 plus Ekman), Laplacian and biharmonic diffusion, heat and
-// Ekman forcing, the convective adjustment and, when ent is computed, the
-// layer 1/2 entrainment xfo with per-CTA partial sums for its mean.  The new
-// sst overwrites datam (the host then swaps data and datam).
+// step_oml at T points: the Ekman pumping, advection (C grid, geostrophic
+// from the layer-1 pressure P1 plus Ekman), Laplacian and biharmonic
+// diffusion (del2_T of the lagged sst taken at the five points of the outer
+// del2_T), heat and Ekman forcing, the convective adjustment and, when ent is
+// computed, the layer 1/2 entrainment xfo with per-CTA partial sums for its
+// mean.  The new sst goes to snew (the host then rotates snew, data, datam).
 template <class T>
 __global__ void __launch_bounds__(256) k_oml_step(OmlDev o, const T *__restrict__ P1, int px, double tdto,
                                                    int compute_ent) {
@@ -69,6 +66,7 @@ __global__ void __launch_bounds__(256) k_oml_step(OmlDev o, const T *__restrict_
     const double ce = o.tau_sign / (o.fnot * o.hm), cg = o.ycexp / o.fnot;
     const double *tx = o.taux, *ty = o.tauy, *t = o.data;
     auto p = [&](int i, int j) { return (double)P1[(size_t)j * px + i]; };
+    auto d2 = [&](int i, int j) { return oml_del2(o, o.datam, i, j, o.fluxn, o.nval, o.fluxs, o.sval); };
     // vel_u * mixed_x on the x-face of column f (0..nxt), row j
     auto uflux = [&](int f, int j) {
         if (f == 0 || f == nxp - 1) return 0.0;   // no normal flow through the walls
@@ -98,14 +96,22 @@ __global__ void __launch_bounds__(256) k_oml_step(OmlDev o, const T *__restrict_
     double xs = 0.0;
     for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < nxt * nyt; idx += gridDim.x * blockDim.x) {
         const int j = idx / nxt, i = idx - j * nxt;
+        const double wk = oml_wekt(o, i, j);
+        o.wekt[idx] = wk;
         const double adv = (-1.0 / o.dx) * (uflux(i + 1, j) - uflux(i, j)) + (-1.0 / o.dy) * (vflux(i, j + 1) - vflux(i, j));
-        const double d4 = oml_del2(o, o.d2, i, j, false, 0.0, false, 0.0);
-        const double ad = adv + o.st2d * o.d2[idx] - o.st4d * d4;
-        const double dm = o.datam[idx], wk = o.wekt[idx];
+        // del2_T (no flux) of del2_T(datam): the inner one at the five points
+        const double d2c = d2(i, j);
+        const double left = i == 0 ? 0.0 : d2c - d2(i - 1, j);
+        const double right = i == nxt - 1 ? 0.0 : d2(i + 1, j) - d2c;
+        const double bot = j == 0 ? 0.0 : d2c - d2(i, j - 1);
+        const double top = j == nyt - 1 ? 0.0 : d2(i, j + 1) - d2c;
+        const double d4 = (1.0 / (o.dx * o.dx)) * (right - left + top - bot);
+        const double ad = adv + o.st2d * d2c - o.st4d * d4;
+        const double dm = o.datam[idx];
         const double half = 0.5 * wk * (dm - o.t1_rel);
         const double sstnew = dm + tdto * (ad + (1.0 / (o.rho_cp * o.hm)) * o.fnet[idx] + (1.0 / o.hm) * (wk * dm - half));
         const double conv = fmax(0.0, o.t1_rel - sstnew);
-        o.datam[idx] = sstnew + conv;
+        o.snew[idx] = sstnew + conv;
         if (compute_ent) {
             const double x = (-1.0 / o.dt_12) * half - (o.hm / (tdto * o.dt_12)) * conv;
             o.xfo[idx] = x;
@@ -136,13 +142,16 @@ __device__ __forceinline__ double oml_t2p(const OmlDev &o, const double *t, doub
     return 0.25 * (T_(i, j) + T_(i - 1, j) + T_(i, j - 1) + T_(i - 1, j - 1));
 }
 
-// The QG forcing from the mixed layer: wekp = map_T_to_P(wekt) and, when
-// computed, ent(:,:,1) = map_T_to_P(xfo - avg_T(xfo)), ent(:,:,2:) = 0, into
-// the handle's pitched fields.  Every CTA adds the partial sums in the same
-// order (deterministic mean).
+// The QG forcing from the mixed layer, one CTA of 128 threads per p row j:
+// wekp = map_T_to_P(wekt) and, when computed, ent(:,:,1) =
+// map_T_to_P(xfo - avg_T(xfo)), ent(:,:,2:) = 0, into the handle's pitched
+// fields, with the trapezoid row sum of ent(:,:,1) into ent_rows[j] (as
+// k_ent_rows forms it, for the forcing integrals).  Every CTA adds the
+// partial sums of xfo in the same order (deterministic mean).
 template <class T>
-__global__ void __launch_bounds__(256) k_oml_post(OmlDev o, T *wekp, T *ent, int px, int nl, int compute_ent,
-                                                   int nparts) {
+__global__ void __launch_bounds__(128) k_oml_post(OmlDev o, T *wekp, T *ent, double *ent_rows, int px, int nl,
+                                                   int compute_ent, int nparts) {
+    __shared__ double red[32];
     __shared__ double avg;
     if (threadIdx.x < 32) {
         double s = 0.0;
@@ -153,14 +162,21 @@ __global__ void __launch_bounds__(256) k_oml_post(OmlDev o, T *wekp, T *ent, int
     }
     __syncthreads();
     const size_t n2 = (size_t)o.nyp * px;
-    for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < o.nxp * o.nyp; idx += gridDim.x * blockDim.x) {
-        const int j = idx / o.nxp, i = idx - j * o.nxp;
+    const int j = blockIdx.x;
+    double rs = 0.0;
+    for (int i = threadIdx.x; i < o.nxp; i += blockDim.x) {
         const size_t op = (size_t)j * px + i;
         wekp[op] = (T)oml_t2p(o, o.wekt, 0.0, i, j);
         if (compute_ent) {
-            ent[op] = (T)oml_t2p(o, o.xfo, avg, i, j);
+            const T v = (T)oml_t2p(o, o.xfo, avg, i, j);
+            ent[op] = v;
+            rs += ((i == 0 || i == o.nxp - 1) ? 0.5 : 1.0) * (double)v;
             for (int k = 1; k < nl - 1; ++k) ent[k * n2 + op] = (T)0;
         }
+    }
+    if (compute_ent) {
+        rs = block_sum(rs, red);
+        if (threadIdx.x == 0) ent_rows[j] = rs;
     }
 }
 
