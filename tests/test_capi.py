@@ -92,3 +92,36 @@ def test_ensemble_create_checks_members_before_any_device_call(liboqg):
     arr2 = (type(b3) * 2)(a.to_c(), b3)
     assert liboqg.oqg_ensemble_create(ctypes.cast(arr2, ctypes.c_void_p), 2, ctypes.byref(e)) == 5
     assert not e.value
+
+
+def test_oml_params_struct_layout_matches_header():
+    from openqg_b200.params import OqgOmlParams
+    # seven doubles, two ints, two doubles (x86-64 ABI)
+    assert OqgOmlParams.fluxn.offset == 56
+    assert OqgOmlParams.nval.offset == 64
+    assert ctypes.sizeof(OqgOmlParams) == 80
+
+
+def test_added_entry_points_reject_null_arguments(liboqg):
+    """The adjoint, state-slot, autotuning and mixed-layer entry points check
+    their arguments before any device call."""
+    L = liboqg
+    assert L.oqg_adj_set(None, None, None, None, None, None, None) == 1
+    assert L.oqg_adj_get(None, None, None, None, None, None, None, None) == 1
+    assert L.oqg_adj_step(None, None, ctypes.c_double(1.0), ctypes.c_longlong(1)) == 1
+    assert L.oqg_adj_segment(None, None, None, ctypes.c_size_t(0), 1, ctypes.c_double(1.0),
+                             ctypes.c_longlong(1)) == 1
+    assert L.oqg_adj_initial(None, None, None) == 1
+    assert L.oqg_state_bytes(None, None, None) == 1
+    assert L.oqg_state_save(None, None) == 1
+    assert L.oqg_state_load(None, None) == 1
+    assert L.oqg_pq_save(None, None) == 1
+    assert L.oqg_autotune(None, ctypes.c_double(1.0), 4, None, None) == 1
+    assert L.oqg_ensemble_autotune(None, None, 4, None, None) == 1
+    assert L.oqg_get_vty(None, None) == 1
+    assert L.oqg_oml_create(None, None, None) == 1
+    assert L.oqg_oml_destroy(None) == 0
+    assert L.oqg_oml_set_sst(None, None, None) == 1
+    assert L.oqg_oml_get_sst(None, None, None) == 1
+    assert L.oqg_ocean_forcing(None, None, None, None, 1, ctypes.c_double(1.0)) == 1
+    assert L.oqg_get_forcing(None, None, None) == 1
