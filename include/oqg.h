@@ -339,6 +339,52 @@ int oqg_ocean_forcing(oqg_oml *m, const double *taux, const double *tauy,
  * to host arrays (either may be NULL). */
 int oqg_get_forcing(oqg_handle *h, double *wekp, double *ent);
 
+/* The atmosphere half: the Ekman fields of a channel and the atmospheric
+ * mixed-layer step, writing the atmosphere handle's wekp, ent, txis, txin.
+ * Replaces, for a zonally periodic channel:
+ *   ekman_from_tau (with txis, txin)        src/coupler/ekman.F90:53-83
+ *   step_aml, compute_new_aml,
+ *   compute_atmos_entrainment               src/mixed/amlsubs.F90:184-326
+ *   the atmosphere step's exchange          src/driver.F90:113-143
+ * The radiation scheme that supplies fnetat (compute_forcing) and the
+ * entrainment coefficients (init_entrain_coeff, set_xc1ast) stays with the
+ * caller: its results are passed in. */
+typedef struct oqg_aml oqg_aml;
+
+/* init_atmos_ml (amlsubs.F90:61-98) and the coefficients it derives. */
+typedef struct oqg_aml_params {
+    double hm;              /* the box's mixed-layer depth (m)               */
+    double rho_cp;          /* rho * cp of air                               */
+    double t1_rel, dt_12;   /* T_bar - T(1), T(1) - T(2) (K)                 */
+    double hmamin, hmadmp;  /* height floor (m) and damping                  */
+    double xcexp;           /* entrainment coupling coefficient              */
+    double at2d, at4d;      /* temperature diffusivities                     */
+    double ahmd;            /* height diffusivity                            */
+    double bface, dface;    /* entrainment coefficients (init_entrain_coeff) */
+    double aface[OQG_MAX_NL];   /* of eta(1..nl-1)                           */
+} oqg_aml_params;
+
+/* The atmospheric mixed layer of channel handle qg; xc1ast (nxt, nyt) from
+ * set_xc1ast and the topography dtop (nxp, nyp) or NULL (flat), host or
+ * device memory.  ast starts at 0 and hmixa at hm (init_atmos_ml). */
+int oqg_aml_create(oqg_handle *qg, const oqg_aml_params *prm, const double *xc1ast,
+                   const double *dtop, oqg_aml **out);
+/* Frees the mixed layer without touching the handle (either order). */
+int oqg_aml_destroy(oqg_aml *m);
+/* ast, its lagged value, hmixa and its lagged value, (nxt, nyt) each. */
+int oqg_aml_set_state(oqg_aml *m, const double *ast, const double *astm,
+                      const double *hmixa, const double *hmixam);
+int oqg_aml_get_state(oqg_aml *m, double *ast, double *astm, double *hmixa,
+                      double *hmixam);
+/* One atmosphere coupling step before step_qg (driver.F90:113-143):
+ * ekman_from_tau of taux, tauy (nxp, nyp) with the box's hm, then step_aml
+ * with the handle's current p(:,:,1), eta from its lagged pressure
+ * (pm_k - pm_{k+1}) / gp_k, and the net heat flux fnetat (nxt, nyt).  The
+ * handle's wekp, txis, txin become the Ekman forcing; when compute_ent, its
+ * ent becomes the layer 1/2 entrainment (other layers zero). */
+int oqg_atmos_forcing(oqg_aml *m, const double *taux, const double *tauy,
+                      const double *fnetat, int compute_ent, double tdta);
+
 /* ---------------------------------------------------------------------
  * State slots and the adjoint step.  The reference has no adjoint (its model
  * is run forward only); these entry points have no counterpart in it.  They

@@ -20,7 +20,7 @@ from typing import Optional
 
 import numpy as np
 
-from .params import Basin, OqgOmlParams, QgMonitor, STATUS
+from .params import Basin, OqgAmlParams, OqgOmlParams, QgMonitor, STATUS
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "liboqg.so")
@@ -93,6 +93,11 @@ def lib():
     L.oqg_oml_get_sst.argtypes = [vp, vp, vp]
     L.oqg_ocean_forcing.argtypes = [vp, vp, vp, vp, ctypes.c_int, ctypes.c_double]
     L.oqg_get_forcing.argtypes = [vp, _dp, _dp]
+    L.oqg_aml_create.argtypes = [vp, ctypes.POINTER(OqgAmlParams), vp, vp, ctypes.POINTER(vp)]
+    L.oqg_aml_destroy.argtypes = [vp]
+    L.oqg_aml_set_state.argtypes = [vp, vp, vp, vp, vp]
+    L.oqg_aml_get_state.argtypes = [vp, vp, vp, vp, vp]
+    L.oqg_atmos_forcing.argtypes = [vp, vp, vp, vp, ctypes.c_int, ctypes.c_double]
     L.oqg_ensemble_autotune.argtypes = [vp, _dp, ctypes.c_int, ctypes.POINTER(ctypes.c_int), _dp]
     L.oqg_autotune.argtypes = [vp, ctypes.c_double, ctypes.c_int, ctypes.POINTER(ctypes.c_int), _dp]
     L.oqg_get_vty.argtypes = [vp, ctypes.POINTER(ctypes.c_int)]
@@ -468,3 +473,57 @@ def get_forcing(qg: QG):
     w, e = np.empty(b.shape2), np.empty((b.nl - 1,) + b.shape2)
     _check(lib().oqg_get_forcing(qg.h, _p(w), _p(e)), "oqg_get_forcing")
     return w, e
+
+
+class AtmosMixedLayer:
+    """The atmospheric mixed layer of a channel on the device (step_aml,
+    amlsubs.F90:184-326) coupled to a QG handle: `forcing(taux, tauy, fnetat,
+    compute_ent, tdta)` runs ekman_from_tau and step_aml and leaves wekp,
+    txis, txin and ent in the handle's forcing (driver.F90:113-143).  The
+    radiation-derived inputs (aface, bface, dface, xc1ast, fnetat) come from
+    the caller.  Arrays are numpy FP64: stress and dtop (nyp, nxp), T-grid
+    fields (nyt, nxt)."""
+
+    def __init__(self, qg: QG, xc1ast, dtop=None, *, hm, rho_cp, t1_rel, dt_12, hmamin, hmadmp, xcexp,
+                 at2d, at4d, ahmd, aface, bface, dface):
+        from .params import OQG_MAX_NL
+        self.qg = qg
+        b = qg.b
+        self.tshape = (b.nyp - 1, b.nxp - 1)
+        af = (ctypes.c_double * OQG_MAX_NL)(*([float(a) for a in aface] + [0.0] * (OQG_MAX_NL - len(aface))))
+        self._prm = OqgAmlParams(hm, rho_cp, t1_rel, dt_12, hmamin, hmadmp, xcexp, at2d, at4d, ahmd, bface, dface,
+                                 af)
+        xc = _f64(xc1ast, self.tshape)
+        dt = _f64(dtop, b.shape2) if dtop is not None else None
+        h = ctypes.c_void_p()
+        _check(lib().oqg_aml_create(qg.h, ctypes.byref(self._prm), xc.ctypes.data,
+                                    None if dt is None else dt.ctypes.data, ctypes.byref(h)), "oqg_aml_create")
+        self.h = h
+
+    def close(self):
+        # freed without touching the QG handle: safe before or after its close()
+        if getattr(self, "h", None) is not None and self.h.value:
+            lib().oqg_aml_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_state(self, ast, astm, hmixa, hmixam):
+        a = [_f64(x, self.tshape) for x in (ast, astm, hmixa, hmixam)]
+        _check(lib().oqg_aml_set_state(self.h, *[x.ctypes.data for x in a]), "oqg_aml_set_state")
+
+    def get_state(self):
+        a = [np.empty(self.tshape) for _ in range(4)]
+        _check(lib().oqg_aml_get_state(self.h, *[x.ctypes.data for x in a]), "oqg_aml_get_state")
+        return a
+
+    def forcing(self, taux, tauy, fnetat, compute_ent: bool, tdta: float):
+        b = self.qg.b
+        tx, ty = _f64(taux, b.shape2), _f64(tauy, b.shape2)
+        fn = _f64(fnetat, self.tshape)
+        _check(lib().oqg_atmos_forcing(self.h, tx.ctypes.data, ty.ctypes.data, fn.ctypes.data, int(compute_ent),
+                                       float(tdta)), "oqg_atmos_forcing")

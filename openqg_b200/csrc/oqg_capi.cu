@@ -2211,3 +2211,146 @@ int oqg_ensemble_autotune(oqg_ensemble *e, const double *tdt, int nsteps, int *b
 }
 
 }  // extern "C"
+
+// ======================================================= atmospheric mixed layer
+struct oqg_aml {
+    oqg_handle *h = nullptr;
+    std::vector<void *> allocs;
+    AmlDev o{};
+};
+
+extern "C" {
+
+int oqg_aml_create(oqg_handle *h, const oqg_aml_params *prm, const double *xc1ast, const double *dtop,
+                   oqg_aml **out) {
+    if (!h || !prm || !out) return fail(OQG_EINVAL, "null argument");
+    *out = nullptr;
+    const BasinDev &b = h->hb;
+    if (!b.cyclic) return fail(OQG_EUNSUPPORTED, "the atmospheric mixed layer needs a zonally periodic channel");
+    if (!(prm->hm > 0.0) || !(prm->rho_cp > 0.0) || prm->dt_12 == 0.0)
+        return fail(OQG_EINVAL, "hm and rho_cp must be > 0 and dt_12 nonzero");
+    oqg_aml *m = new oqg_aml();
+    m->h = h;
+    AmlDev &o = m->o;
+    o.nxp = b.nxp; o.nyp = b.nyp; o.nxt = b.nxp - 1; o.nyt = b.nyp - 1; o.nl = b.nl; o.tau_sign = b.tau_sign;
+    o.dx = b.dx; o.dy = b.dy; o.fnot = b.fnot; o.hm = prm->hm; o.rho_cp = prm->rho_cp; o.t1_rel = prm->t1_rel;
+    o.dt_12 = prm->dt_12; o.hmamin = prm->hmamin; o.hmadmp = prm->hmadmp; o.xcexp = prm->xcexp;
+    o.at2d = prm->at2d; o.at4d = prm->at4d; o.ahmd = prm->ahmd; o.bface = prm->bface; o.dface = prm->dface;
+    for (int k = 0; k < OQG_NLMAX; ++k) {
+        o.aface[k] = k < b.nl - 1 ? prm->aface[k] : 0.0;
+        o.gp[k] = k < b.nl - 1 ? b.gp[k] : 1.0;
+    }
+    const size_t nt = (size_t)o.nxt * o.nyt, np = (size_t)o.nxp * o.nyp;
+    const size_t total = 10 * nt + 3 * np;
+    void *x = nullptr;
+    if (cudaMalloc(&x, total * sizeof(double)) != cudaSuccess) {
+        delete m;
+        return fail(OQG_ECUDA, "cudaMalloc of the mixed-layer buffers failed");
+    }
+    m->allocs.push_back(x);
+    double *d = (double *)x;
+    o.ast = d; o.astm = d + nt; o.asn = d + 2 * nt; o.hmx = d + 3 * nt; o.hmxm = d + 4 * nt; o.hmn = d + 5 * nt;
+    o.wekt = d + 6 * nt; o.xfa = d + 7 * nt;
+    double *xc = d + 8 * nt, *fn = d + 9 * nt;
+    o.xc1ast = xc;
+    o.fnet = fn;
+    o.taux = d + 10 * nt;
+    o.tauy = d + 10 * nt + np;
+    double *dt = d + 10 * nt + 2 * np;
+    o.dtop = dtop ? dt : nullptr;
+    bool ok = cudaMemsetAsync(x, 0, total * sizeof(double), h->st) == cudaSuccess;
+    // init_atmos_ml: ast starts at 0, hmixa at the box's hm (amlsubs.F90:88-91)
+    std::vector<double> hm0(nt, prm->hm);
+    ok = ok && cudaMemcpyAsync(o.hmx, hm0.data(), nt * sizeof(double), cudaMemcpyHostToDevice, h->st) == cudaSuccess;
+    ok = ok && cudaMemcpyAsync(o.hmxm, hm0.data(), nt * sizeof(double), cudaMemcpyHostToDevice, h->st) == cudaSuccess;
+    if (xc1ast) ok = ok && cudaMemcpyAsync(xc, xc1ast, nt * sizeof(double), cudaMemcpyDefault, h->st) == cudaSuccess;
+    if (dtop) ok = ok && cudaMemcpyAsync(dt, dtop, np * sizeof(double), cudaMemcpyDefault, h->st) == cudaSuccess;
+    ok = ok && cudaStreamSynchronize(h->st) == cudaSuccess;
+    if (!ok) {
+        cudaFree(x);
+        delete m;
+        return fail(OQG_ECUDA, "setting up the mixed-layer buffers failed");
+    }
+    *out = m;
+    return OQG_OK;
+}
+
+int oqg_aml_destroy(oqg_aml *m) {
+    if (!m) return OQG_OK;
+    // the handle may be gone already: cudaFree waits for the device by itself
+    for (void *p : m->allocs) cudaFree(p);
+    delete m;
+    return OQG_OK;
+}
+
+int oqg_aml_set_state(oqg_aml *m, const double *ast, const double *astm, const double *hmixa, const double *hmixam) {
+    if (!m || !ast || !astm || !hmixa || !hmixam) return fail(OQG_EINVAL, "null argument");
+    const size_t bytes = (size_t)m->o.nxt * m->o.nyt * sizeof(double);
+    const double *src[4] = {ast, astm, hmixa, hmixam};
+    double *dst[4] = {m->o.ast, m->o.astm, m->o.hmx, m->o.hmxm};
+    for (int f = 0; f < 4; ++f) CK(cudaMemcpyAsync(dst[f], src[f], bytes, cudaMemcpyDefault, m->h->st));
+    CK(cudaStreamSynchronize(m->h->st));
+    return OQG_OK;
+}
+
+int oqg_aml_get_state(oqg_aml *m, double *ast, double *astm, double *hmixa, double *hmixam) {
+    if (!m) return fail(OQG_EINVAL, "null argument");
+    const size_t bytes = (size_t)m->o.nxt * m->o.nyt * sizeof(double);
+    double *dst[4] = {ast, astm, hmixa, hmixam};
+    const double *src[4] = {m->o.ast, m->o.astm, m->o.hmx, m->o.hmxm};
+    for (int f = 0; f < 4; ++f)
+        if (dst[f]) CK(cudaMemcpyAsync(dst[f], src[f], bytes, cudaMemcpyDefault, m->h->st));
+    CK(cudaStreamSynchronize(m->h->st));
+    return OQG_OK;
+}
+
+int oqg_atmos_forcing(oqg_aml *m, const double *taux, const double *tauy, const double *fnetat, int compute_ent,
+                      double tdta) {
+    if (!m || !taux || !tauy || !fnetat) return fail(OQG_EINVAL, "null argument");
+    if (!(tdta > 0.0)) return fail(OQG_EINVAL, "tdta must be > 0");
+    oqg_handle *h = m->h;
+    BasinDev &b = h->hb;
+    AmlDev &o = m->o;
+    const size_t nt = (size_t)o.nxt * o.nyt, np = (size_t)o.nxp * o.nyp, n2 = (size_t)b.nyp * b.px;
+    if (compute_ent && !h->ent_buf) {
+        h->ent_buf = dalloc<char>(h, (size_t)(b.nl - 1) * n2 * h->esz);
+        if (!h->ent_buf) return fail(OQG_ECUDA, "out of device memory");
+    }
+    if (!h->up_ev && cudaEventCreateWithFlags(&h->up_ev, cudaEventDisableTiming) != cudaSuccess)
+        return fail(OQG_ECUDA, "cudaEventCreate failed");
+    CK(cudaMemcpyAsync(const_cast<double *>(o.taux), taux, np * sizeof(double), cudaMemcpyDefault, h->st));
+    CK(cudaMemcpyAsync(const_cast<double *>(o.tauy), tauy, np * sizeof(double), cudaMemcpyDefault, h->st));
+    CK(cudaMemcpyAsync(const_cast<double *>(o.fnet), fnetat, nt * sizeof(double), cudaMemcpyDefault, h->st));
+    CK(cudaEventRecord(h->up_ev, h->st));
+    const void *p1 = b.F[h->par], *pm = b.F[1 - h->par];   // driver.F90:127-135
+    const int grid = std::min((int)((nt + 255) / 256), 148 * 8);
+    if (h->mixed) {
+        k_aml_step<float><<<grid, 256, 0, h->st>>>(o, (const float *)p1, b.px, tdta, compute_ent);
+        k_aml_post<float><<<b.nyp, 128, 0, h->st>>>(o, (const float *)pm, (float *)b.wekp, (float *)h->ent_buf,
+                                                    b.ent_rows, b.px, compute_ent);
+    } else {
+        k_aml_step<double><<<grid, 256, 0, h->st>>>(o, (const double *)p1, b.px, tdta, compute_ent);
+        k_aml_post<double><<<b.nyp, 128, 0, h->st>>>(o, (const double *)pm, (double *)b.wekp,
+                                                     (double *)h->ent_buf, b.ent_rows, b.px, compute_ent);
+    }
+    k_aml_strips<<<1, 128, 0, h->st>>>(o, b.frc);
+    CK(cudaGetLastError());
+    // lagged <- current, current <- new; the old lagged buffers become scratch
+    double *a_old = o.astm, *h_old = o.hmxm;
+    o.astm = o.ast; o.ast = o.asn; o.asn = a_old;
+    o.hmxm = o.hmx; o.hmx = o.hmn; o.hmn = h_old;
+    if (compute_ent && b.ent != h->ent_buf) {
+        b.ent = h->ent_buf;
+        h->hb64.ent = b.ent;
+        int rc = push_desc(h);
+        if (rc) return rc;
+    }
+    // the channel's forcing integrals (ent_xn and the ent strip integrals)
+    if (h->mixed) k_forcing_integrals<float><<<1, 512, 0, h->st>>>(h->d_bas, 0);
+    else k_forcing_integrals<double><<<1, 512, 0, h->st>>>(h->d_bas, 0);
+    CK(cudaGetLastError());
+    CK(cudaEventSynchronize(h->up_ev));
+    return OQG_OK;
+}
+
+}  // extern "C"

@@ -180,4 +180,196 @@ __global__ void __launch_bounds__(128) k_oml_post(OmlDev o, T *wekp, T *ent, dou
     }
 }
 
+
+// ---------------------------------------------------------------- atmosphere
+// The atmospheric mixed layer of a zonally periodic channel (step_aml,
+// amlsubs.F90:184-326): temperature ast and height hmixa, advected and
+// diffused like the ocean's sst with the cyclic branches of the numerics.
+struct AmlDev {
+    int nxp, nyp, nxt, nyt, nl, tau_sign;
+    double dx, dy, fnot, hm, rho_cp, t1_rel, dt_12, hmamin, hmadmp, xcexp, at2d, at4d, ahmd, bface, dface;
+    double aface[OQG_NLMAX], gp[OQG_NLMAX];
+    const double *taux, *tauy;       // [nyp][nxp]
+    const double *fnet;              // [nyt][nxt] net heat flux into the mixed layer (fnetat)
+    double *ast, *astm, *asn;        // temperature, lagged, next [nyt][nxt]
+    double *hmx, *hmxm, *hmn;        // height, lagged, next
+    double *wekt, *xfa;              // Ekman pumping, entrainment at T points
+    const double *xc1ast;            // set_xc1ast (amlsubs.F90:137-182) [nyt][nxt]
+    const double *dtop;              // topography at p points [nyp][nxp] or null
+};
+
+// del2_T (numerics.F90:109-145) in a channel (cyclic in x).
+__device__ __forceinline__ double aml_del2(const AmlDev &o, const double *t, int i, int j, bool nflux, double nval,
+                                           bool sflux, double sval) {
+    const int nxt = o.nxt, nyt = o.nyt;
+    const double *row = t + (size_t)j * nxt;
+    const double c = row[i];
+    const double left = c - row[i == 0 ? nxt - 1 : i - 1];
+    const double right = row[i == nxt - 1 ? 0 : i + 1] - c;
+    const double bot = j == 0 ? (sflux ? c - sval : 0.0) : c - t[(size_t)(j - 1) * nxt + i];
+    const double top = j == nyt - 1 ? (nflux ? nval - c : 0.0) : t[(size_t)(j + 1) * nxt + i] - c;
+    return (1.0 / (o.dx * o.dx)) * (right - left + top - bot);
+}
+
+// adv_diff (mixed_layer.F90:16-58) of one mixed field at T point (i, j) in a
+// channel: t the current field (advected), tm the lagged one (diffused).
+template <class T>
+__device__ __forceinline__ double aml_adv_diff(const AmlDev &o, const T *__restrict__ P1, int px, const double *t,
+                                               const double *tm, double d2c, double d4c, bool nflux, double nval,
+                                               bool sflux, double sval, int i, int j) {
+    const int nxt = o.nxt, nyt = o.nyt, nxp = o.nxp, nyp = o.nyp;
+    const double ce = o.tau_sign / (o.fnot * o.hm), cg = 1.0 / o.fnot;   // ycexp = 1 (init_atmos_ml)
+    const double *tx = o.taux, *ty = o.tauy;
+    auto p = [&](int a, int bb) { return (double)P1[(size_t)bb * px + a]; };
+    auto uflux = [&](int f) {          // x-face f of row j, 0..nxt (no wall)
+        const double dpdy = (1.0 / o.dy) * (p(f, j + 1) - p(f, j));
+        const double uek = ce * (0.5 * (ty[(size_t)(j + 1) * nxp + f] + ty[(size_t)j * nxp + f]));
+        const double vel = -cg * dpdy + uek;
+        const double mx = (f == 0 || f == nxt) ? 0.5 * (t[(size_t)j * nxt] + t[(size_t)j * nxt + nxt - 1])
+                                               : 0.5 * (t[(size_t)j * nxt + f - 1] + t[(size_t)j * nxt + f]);
+        return vel * mx;
+    };
+    auto vflux = [&](int g) {          // y-face g of column i, 0..nyt
+        const double vek = -ce * (0.5 * (tx[(size_t)g * nxp + i + 1] + tx[(size_t)g * nxp + i]));
+        double vel, my;
+        if (g == 0) {
+            vel = sflux ? vek : 0.0;
+            my = sflux ? t[i] : 0.5 * (t[i] + sval);
+        } else if (g == nyp - 1) {
+            vel = nflux ? vek : 0.0;
+            my = nflux ? t[(size_t)(nyt - 1) * nxt + i] : 0.5 * (t[(size_t)(nyt - 1) * nxt + i] + nval);
+        } else {
+            const double dpdx = (1.0 / o.dx) * (p(i + 1, g) - p(i, g));
+            vel = cg * dpdx + vek;
+            my = 0.5 * (t[(size_t)(g - 1) * nxt + i] + t[(size_t)g * nxt + i]);
+        }
+        return vel * my;
+    };
+    const double adv = (-1.0 / o.dx) * (uflux(i + 1) - uflux(i)) + (-1.0 / o.dy) * (vflux(j + 1) - vflux(j));
+    // del2_T (no flux) of del2_T(tm): the inner one at the five points
+    auto d2 = [&](int a, int bb) { return aml_del2(o, tm, a, bb, nflux, nval, sflux, sval); };
+    const double e2 = d2(i, j);
+    double e4 = 0.0;
+    if (d4c != 0.0) {
+        const double left = e2 - d2(i == 0 ? nxt - 1 : i - 1, j);
+        const double right = d2(i == nxt - 1 ? 0 : i + 1, j) - e2;
+        const double bot = j == 0 ? 0.0 : e2 - d2(i, j - 1);
+        const double top = j == nyt - 1 ? 0.0 : d2(i, j + 1) - e2;
+        e4 = (1.0 / (o.dx * o.dx)) * (right - left + top - bot);
+    }
+    return adv + d2c * e2 - d4c * e4;
+}
+
+// step_aml at T points: the Ekman pumping, both fields' advection and
+// diffusion, compute_new_aml (:231-285: height with its diabatic term and
+// floor, temperature with the heat and Ekman terms, the convective
+// correction) and the T-grid part of the entrainment (:302-306).  The new
+// fields go to asn, hmn (the host then rotates the buffers).
+template <class T>
+__global__ void __launch_bounds__(256) k_aml_step(AmlDev o, const T *__restrict__ P1, int px, double tdta,
+                                                   int compute_ent) {
+    const int nxt = o.nxt, nyt = o.nyt;
+    for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < nxt * nyt; idx += gridDim.x * blockDim.x) {
+        const int j = idx / nxt, i = idx - j * nxt;
+        const double *tx = o.taux, *ty = o.tauy;
+        const int nxp = o.nxp;
+        const double tyw = 0.5 * (ty[(size_t)(j + 1) * nxp + i] + ty[(size_t)j * nxp + i]);
+        const double tye = 0.5 * (ty[(size_t)(j + 1) * nxp + i + 1] + ty[(size_t)j * nxp + i + 1]);
+        const double txs = 0.5 * (tx[(size_t)j * nxp + i + 1] + tx[(size_t)j * nxp + i]);
+        const double txn = 0.5 * (tx[(size_t)(j + 1) * nxp + i + 1] + tx[(size_t)(j + 1) * nxp + i]);
+        const double wk = (1.0 / (o.dx * o.fnot)) * (tye - tyw) - (1.0 / (o.dy * o.fnot)) * (txn - txs);
+        o.wekt[idx] = wk;
+        const double tmrhs0 = aml_adv_diff(o, P1, px, o.ast, o.astm, o.at2d, o.at4d, false, 0.0, false, 0.0, i, j);
+        const double dhdt = aml_adv_diff(o, P1, px, o.hmx, o.hmxm, o.ahmd, 0.0, true, o.hm, true, o.hm, i, j);
+        const double am = o.astm[idx], hm_ = o.hmxm[idx];
+        const double dT = o.t1_rel - am;
+        const double hdrcdt = o.hmadmp / o.rho_cp;
+        double hnew = o.hm, dT_fix = 0.0;
+        if (dT >= 2.0 * hdrcdt * tdta) {
+            const double diab = hdrcdt * (hm_ - o.hm) / dT;
+            hnew = hm_ + tdta * (dhdt - diab);
+            const double fix = fmax(o.hmamin - hnew, 0.0);
+            hnew = hnew + fix;
+            dT_fix = fix * dT / hm_;
+        }
+        const double tmrhs = tmrhs0 + (1.0 / o.rho_cp) * o.fnet[idx] / hm_ - (1.0 / o.hm) * wk * am;
+        double astnew = am + tdta * tmrhs + dT_fix;
+        const double conv = fmin(0.0, o.t1_rel - astnew);
+        astnew = astnew + conv;
+        if (compute_ent)
+            o.xfa[idx] = o.xcexp * o.bface * (hm_ - o.hm) + o.dface * (o.xcexp * am + (1.0 - o.xcexp) * o.xc1ast[idx]) +
+                         (o.xcexp / (tdta * o.dt_12)) * o.hmx[idx] * conv;
+        o.asn[idx] = astnew;
+        o.hmn[idx] = hnew;
+    }
+}
+
+// map_T_to_P (numerics.F90:64-107, cyclic branches) at p point (i, j).
+__device__ __forceinline__ double aml_t2p(const AmlDev &o, const double *t, int i, int j) {
+    const int nxt = o.nxt, nyt = o.nyt, nxp = o.nxp, nyp = o.nyp;
+    auto T_ = [&](int a, int bb) { return t[(size_t)bb * nxt + a]; };
+    const bool s = j == 0, n = j == nyp - 1;
+    if (i == 0 || i == nxp - 1) {
+        if (s) return 0.5 * (T_(0, 0) + T_(nxt - 1, 0));
+        if (n) return 0.5 * (T_(0, nyt - 1) + T_(nxt - 1, nyt - 1));
+        return 0.25 * (T_(0, j) + T_(nxt - 1, j) + T_(0, j - 1) + T_(nxt - 1, j - 1));
+    }
+    if (s || n) {
+        const int r = s ? 0 : nyt - 1;
+        return 0.5 * (T_(i - 1, r) + T_(i, r));
+    }
+    return 0.25 * (T_(i, j) + T_(i - 1, j) + T_(i, j - 1) + T_(i - 1, j - 1));
+}
+
+// The QG forcing from the atmospheric mixed layer, one CTA of 128 threads
+// per p row: wekp = map_T_to_P(wekt) and, when computed, ent(:,:,1) =
+// map_T_to_P(xfa) + sum_k aface(k) eta(k) + bface dtop with eta(k) =
+// (pm_k - pm_{k+1}) / gp_k from the handle's lagged pressure (driver.F90:
+// 128-131; amlsubs.F90:308-323), ent(:,:,2:) = 0, and its row sums.
+template <class T>
+__global__ void __launch_bounds__(128) k_aml_post(AmlDev o, const T *__restrict__ PM, T *wekp, T *ent,
+                                                   double *ent_rows, int px, int compute_ent) {
+    __shared__ double red[32];
+    const size_t n2 = (size_t)o.nyp * px;
+    const int j = blockIdx.x;
+    double rs = 0.0;
+    for (int i = threadIdx.x; i < o.nxp; i += blockDim.x) {
+        const size_t op = (size_t)j * px + i;
+        wekp[op] = (T)aml_t2p(o, o.wekt, i, j);
+        if (compute_ent) {
+            double e1 = aml_t2p(o, o.xfa, i, j);
+            for (int k = 0; k < o.nl - 1; ++k)
+                e1 = e1 + o.aface[k] * (((double)PM[k * n2 + op] - (double)PM[(k + 1) * n2 + op]) / o.gp[k]);
+            e1 = e1 + o.bface * (o.dtop ? o.dtop[(size_t)j * o.nxp + i] : 0.0);
+            const T v = (T)e1;
+            ent[op] = v;
+            rs += ((i == 0 || i == o.nxp - 1) ? 0.5 : 1.0) * (double)v;
+            for (int k = 1; k < o.nl - 1; ++k) ent[k * n2 + op] = (T)0;
+        }
+    }
+    if (compute_ent) {
+        rs = block_sum(rs, red);
+        if (threadIdx.x == 0) ent_rows[j] = rs;
+    }
+}
+
+// The boundary stress integrals of a channel (ekman.F90:60-70):
+// txis = int_P_dx(taux(:,1) + taux(:,2)) / 2, txin likewise at the north.
+__global__ void __launch_bounds__(128) k_aml_strips(AmlDev o, DevForcing *frc) {
+    __shared__ double red[32];
+    const int nxp = o.nxp;
+    double s = 0.0, n = 0.0;
+    for (int i = threadIdx.x; i < nxp; i += blockDim.x) {
+        const double w = (i == 0 || i == nxp - 1) ? 0.5 : 1.0;
+        s += w * (o.taux[i] + o.taux[(size_t)nxp + i]);
+        n += w * (o.taux[(size_t)(o.nyp - 2) * nxp + i] + o.taux[(size_t)(o.nyp - 1) * nxp + i]);
+    }
+    s = block_sum(s, red);
+    n = block_sum(n, red);
+    if (threadIdx.x == 0) {
+        frc->txis = 0.5 * (s * o.dx);
+        frc->txin = 0.5 * (n * o.dx);
+    }
+}
+
 }  // namespace oqg

@@ -51,6 +51,14 @@ class OqgOmlParams(ctypes.Structure):
     ]
 
 
+class OqgAmlParams(ctypes.Structure):
+    """ctypes mirror of `oqg_aml_params` (include/oqg.h): the atmospheric
+    mixed layer's parameters (init_atmos_ml, amlsubs.F90:61-131)."""
+    _fields_ = [(n, ctypes.c_double) for n in ("hm", "rho_cp", "t1_rel", "dt_12", "hmamin", "hmadmp", "xcexp",
+                                               "at2d", "at4d", "ahmd", "bface", "dface")] + \
+        [("aface", ctypes.c_double * OQG_MAX_NL)]
+
+
 class OqgParams(ctypes.Structure):
     """ctypes mirror of `oqg_params` (include/oqg.h)."""
     _fields_ = [

@@ -134,3 +134,150 @@ class OmlOracle:
         self.datam = self.data.copy()
         self.data = sstnew + dT_conv
         return xfo
+
+
+# ---------------------------------------------------------------- the channel
+# The atmosphere's zonally periodic channel: the same equations with the
+# cyclic branches of the numerics (column nxp-1 of a p field repeats column 0).
+
+def map_T_to_P_cyclic(t):
+    """numerics.F90:64-107, cyclic branches: (nyt, nxt) -> (nyp, nxp)."""
+    nyt, nxt = t.shape
+    o = np.empty((nyt + 1, nxt + 1))
+    o[1:-1, 1:-1] = 0.25 * (t[1:, 1:] + t[1:, :-1] + t[:-1, 1:] + t[:-1, :-1])
+    o[0, 1:-1] = 0.5 * (t[0, :-1] + t[0, 1:])
+    o[-1, 1:-1] = 0.5 * (t[-1, :-1] + t[-1, 1:])
+    o[1:-1, 0] = 0.25 * (t[1:, 0] + t[1:, -1] + t[:-1, 0] + t[:-1, -1])
+    o[0, 0] = 0.5 * (t[0, 0] + t[0, -1])
+    o[-1, 0] = 0.5 * (t[-1, 0] + t[-1, -1])
+    o[:, -1] = o[:, 0]
+    return o
+
+
+def ekman_cyclic(taux, tauy, dx, dy, fnot, hm, tau_sign=-1):
+    """ekman_from_tau (ekman.F90:53-83) for a channel: uek, vek, wekt, wekp
+    and the boundary stress integrals txis, txin (:60-70)."""
+    def int_P_dx(r):
+        return (0.5 * r[0] + r[1:-1].sum() + 0.5 * r[-1]) * dx
+    txis = 0.5 * int_P_dx(taux[0] + taux[1])
+    txin = 0.5 * int_P_dx(taux[-2] + taux[-1])
+    taux_t = 0.5 * (taux[:, 1:] + taux[:, :-1])
+    tauy_t = 0.5 * (tauy[1:, :] + tauy[:-1, :])
+    uek = (tau_sign / (fnot * hm)) * tauy_t
+    vek = (-tau_sign / (fnot * hm)) * taux_t
+    wekt = ((1.0 / (dx * fnot)) * (tauy_t[:, 1:] - tauy_t[:, :-1])
+            - (1.0 / (dy * fnot)) * (taux_t[1:, :] - taux_t[:-1, :]))
+    return uek, vek, wekt, map_T_to_P_cyclic(wekt), txis, txin
+
+
+def del2_T_cyclic(t, dx, north_flux, north_val, south_flux, south_val):
+    """numerics.F90:109-145, cyclic in x."""
+    nyt, nxt = t.shape
+    dt_x = np.empty((nyt, nxt + 1))
+    dt_x[:, 1:nxt] = t[:, 1:] - t[:, :-1]
+    dt_x[:, 0] = t[:, 0] - t[:, -1]
+    dt_x[:, nxt] = dt_x[:, 0]
+    dt_y = np.zeros((nyt + 1, nxt))
+    if south_flux:
+        dt_y[0] = t[0] - south_val
+    dt_y[1:nyt] = t[1:] - t[:-1]
+    if north_flux:
+        dt_y[nyt] = north_val - t[-1]
+    return (1.0 / (dx * dx)) * (dt_x[:, 1:] - dt_x[:, :-1] + dt_y[1:] - dt_y[:-1])
+
+
+def adv_diff_cyclic(data, datam, dp_dx, dp_dy, uek, vek, fnot, dx, dy, d2, d4, ycexp, fluxn, fluxs, nval, sval):
+    """mixed_layer.F90:16-95 in a channel (no wall in x, so vel_u is kept)."""
+    t = data
+    nyt, nxt = t.shape
+    vel_u = (-ycexp / fnot) * dp_dy + uek
+    vel_v = (ycexp / fnot) * dp_dx + vek
+    vel_v[0] = vek[0] if fluxs else 0.0
+    vel_v[-1] = vek[-1] if fluxn else 0.0
+    mx = np.empty((nyt, nxt + 1))
+    mx[:, 0] = 0.5 * (t[:, 0] + t[:, -1])
+    mx[:, 1:nxt] = 0.5 * (t[:, :-1] + t[:, 1:])
+    mx[:, nxt] = mx[:, 0]
+    my = np.empty((nyt + 1, nxt))
+    my[0] = t[0] if fluxs else 0.5 * (t[0] + sval)
+    my[1:nyt] = 0.5 * (t[:-1] + t[1:])
+    my[nyt] = t[-1] if fluxn else 0.5 * (t[-1] + nval)
+    uT, vT = vel_u * mx, vel_v * my
+    adv = (-1.0 / dx) * (uT[:, 1:] - uT[:, :-1]) + (-1.0 / dy) * (vT[1:] - vT[:-1])
+    e2 = del2_T_cyclic(datam, dx, fluxn, nval, fluxs, sval)
+    e4 = del2_T_cyclic(e2, dx, False, 0.0, False, 0.0)
+    return adv + d2 * e2 - d4 * e4
+
+
+@dataclass
+class AmlParams:
+    """The atmospheric mixed layer's parameters (init_atmos_ml,
+    amlsubs.F90:61-98) and its entrainment coefficients (init_entrain_coeff,
+    :100-131, which the radiation scheme provides)."""
+    hm: float = 1000.0         # the box's mixed-layer depth (m)
+    rho_cp: float = 1.0e3      # rho * cp of air (J m^-3 K^-1)
+    t1_rel: float = -5.0       # T_bar - T_(1) (K)
+    dt_12: float = 20.0        # T(1) - T(2) (K)
+    hmamin: float = 100.0      # minimum mixed-layer height (m)
+    hmadmp: float = 0.5        # mixed-layer height damping
+    xcexp: float = 1.0         # entrainment coupling coefficient
+    at2d: float = 2.5e4        # temperature diffusivities
+    at4d: float = 0.0
+    ahmd: float = 2.0e4        # height diffusivity
+    aface: tuple = (0.0, 0.0)  # entrainment coefficients of eta(1..nl-1)
+    bface: float = 0.0
+    dface: float = 0.0
+
+
+class AmlOracle:
+    """The atmospheric mixed layer of a channel: ast and hmixa with their
+    lagged values, xc1ast (set_xc1ast) and the topography dtop given."""
+
+    def __init__(self, basin, prm: AmlParams, xc1ast, dtop):
+        self.b, self.prm = basin, prm
+        nyt, nxt = basin.nyp - 1, basin.nxp - 1
+        self.ast = np.zeros((nyt, nxt))
+        self.astm = np.zeros((nyt, nxt))
+        self.hmx = np.full((nyt, nxt), prm.hm)
+        self.hmxm = np.full((nyt, nxt), prm.hm)
+        self.xc1ast = np.asarray(xc1ast, dtype=np.float64)
+        self.dtop = np.asarray(dtop, dtype=np.float64)
+
+    def step(self, p1, uek, vek, wekt, eta, fnetat, compute_ent, tdta, ent):
+        """step_aml (amlsubs.F90:184-229) with compute_new_aml (:231-285) and
+        compute_atmos_entrainment (:287-326)."""
+        b, m = self.b, self.prm
+        dp_dx = (1.0 / b.dx) * (p1[:, 1:] - p1[:, :-1])
+        dp_dy = (1.0 / b.dy) * (p1[1:, :] - p1[:-1, :])
+        tmrhs = adv_diff_cyclic(self.ast, self.astm, dp_dx, dp_dy, uek, vek, b.fnot, b.dx, b.dy,
+                                m.at2d, m.at4d, 1.0, False, False, 0.0, 0.0)
+        dhdt = adv_diff_cyclic(self.hmx, self.hmxm, dp_dx, dp_dy, uek, vek, b.fnot, b.dx, b.dy,
+                               m.ahmd, 0.0, 1.0, True, True, m.hm, m.hm)
+        dT = m.t1_rel - self.astm
+        hdrcdt = m.hmadmp / m.rho_cp
+        hnew = np.full(dT.shape, m.hm)
+        dT_fix = np.zeros(dT.shape)
+        act = dT >= 2.0 * hdrcdt * tdta
+        with np.errstate(divide="ignore", invalid="ignore"):
+            diab = hdrcdt * (self.hmxm - m.hm) / dT
+            hn = self.hmxm + tdta * (dhdt - diab)
+            fix = np.maximum(m.hmamin - hn, 0.0)
+            hn = hn + fix
+            dfix = fix * dT / self.hmxm
+        hnew[act] = hn[act]
+        dT_fix[act] = dfix[act]
+        tmrhs = tmrhs + (1.0 / m.rho_cp) * fnetat / self.hmxm - (1.0 / m.hm) * wekt * self.astm
+        astnew = self.astm + tdta * tmrhs + dT_fix
+        dT_conv = np.minimum(0.0, m.t1_rel - astnew)
+        astnew = astnew + dT_conv
+        if compute_ent:
+            xfa = (m.xcexp * m.bface * (self.hmxm - m.hm)
+                   + m.dface * (m.xcexp * self.astm + (1.0 - m.xcexp) * self.xc1ast)
+                   + (m.xcexp / (tdta * m.dt_12)) * self.hmx * dT_conv)
+            ent[:] = 0.0
+            e1 = map_T_to_P_cyclic(xfa)
+            for k in range(b.nl - 1):
+                e1 = e1 + m.aface[k] * eta[k]
+            ent[0] = e1 + m.bface * self.dtop
+        self.astm, self.ast = self.ast, astnew
+        self.hmxm, self.hmx = self.hmx, hnew

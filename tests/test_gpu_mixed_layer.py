@@ -126,3 +126,95 @@ def test_rejected_setups():
     with pytest.raises(OqgError):        # the ocean mixed layer needs a closed box
         OceanMixedLayer(c, 100.0, 4.0e6, 10.0, 5.0)
     c.close()
+
+
+# ---------------------------------------------------------------- atmosphere
+from oracle.mixed_layer import AmlOracle, AmlParams, ekman_cyclic  # noqa: E402
+from openqg_b200.core import AtmosMixedLayer  # noqa: E402
+
+TDTA = 360.0
+
+
+def _atmos_setup(seed=4, nl=3):
+    b = atmos_channel(65, 33)
+    if nl == 2:
+        b.h, b.gp, b.ah4 = [4000.0, 5000.0], [0.8], [2.0e13] * 2
+    rng = np.random.default_rng(seed)
+    nyt, nxt = b.nyp - 1, b.nxp - 1
+    prm = AmlParams(aface=tuple(rng.uniform(-1e-6, 1e-6, b.nl - 1)), bface=3e-7, dface=1e-5)
+    xc1ast = 0.5 * rng.standard_normal((nyt, nxt))
+    dtop = 50.0 * rng.standard_normal(b.shape2)
+    dtop[:, -1] = dtop[:, 0]
+    y = np.arange(b.nyp) * b.dy
+    taux = np.repeat((0.1 * np.sin(np.pi * y / y[-1]))[:, None], b.nxp, axis=1) + 0.01 * rng.standard_normal(b.shape2)
+    tauy = 0.01 * rng.standard_normal(b.shape2)
+    taux[:, -1] = taux[:, 0]
+    tauy[:, -1] = tauy[:, 0]
+    fnet = 30.0 * rng.standard_normal((nyt, nxt))
+    ast = prm.t1_rel - 2.0 + rng.standard_normal((nyt, nxt))
+    astm = ast + 0.1 * rng.standard_normal((nyt, nxt))
+    hmx = prm.hm + 50.0 * rng.standard_normal((nyt, nxt))
+    hmxm = hmx + 5.0 * rng.standard_normal((nyt, nxt))
+    p = b.fnot * 30.0 * initial_psi(b, seed=seed)
+    g = QG(b)
+    g.set_state(p, p)
+    m = AtmosMixedLayer(g, xc1ast, dtop, hm=prm.hm, rho_cp=prm.rho_cp, t1_rel=prm.t1_rel, dt_12=prm.dt_12,
+                        hmamin=prm.hmamin, hmadmp=prm.hmadmp, xcexp=prm.xcexp, at2d=prm.at2d, at4d=prm.at4d,
+                        ahmd=prm.ahmd, aface=prm.aface, bface=prm.bface, dface=prm.dface)
+    m.set_state(ast, astm, hmx, hmxm)
+    o = AmlOracle(b, prm, xc1ast, dtop)
+    o.ast, o.astm, o.hmx, o.hmxm = ast.copy(), astm.copy(), hmx.copy(), hmxm.copy()
+    return b, prm, g, m, o, taux, tauy, fnet, p
+
+
+def _eta(b, pm):
+    return np.stack([(pm[k] - pm[k + 1]) / b.gp[k] for k in range(b.nl - 1)])
+
+
+@pytest.mark.parametrize("nl", [3, 2])
+def test_atmos_forcing_matches_oracle(nl):
+    b, prm, g, m, o, taux, tauy, fnet, _ = _atmos_setup(nl=nl)
+    uek, vek, wekt, wekp, txis, txin = ekman_cyclic(taux, tauy, b.dx, b.dy, b.fnot, prm.hm)
+    ent = np.zeros((b.nl - 1,) + b.shape2)
+    for it, ce in enumerate((True, False, True)):
+        p, pm, _, _ = g.get_state()
+        m.forcing(taux, tauy, fnet, ce, TDTA)
+        o.step(p[0], uek, vek, wekt, _eta(b, pm), fnet, ce, TDTA, ent)
+        for name, a, r in zip(("ast", "astm", "hmixa", "hmixam"), m.get_state(), (o.ast, o.astm, o.hmx, o.hmxm)):
+            assert rel_l2(a, r) <= 1e-12, (it, name)
+        w, e = get_forcing(g)
+        assert rel_l2(w, wekp) <= 1e-12
+        assert rel_l2(e, ent) <= 1e-12, it
+        g.step(TDTA, 1)
+    m.close()
+    g.close()
+
+
+def test_atmos_coupled_run_matches_oracle():
+    """Four atmosphere steps of the coupled pattern: the mixed layer's forcing
+    (with txis, txin), then step_qg, on the device and on the CPU."""
+    b, prm, g, m, o, taux, tauy, fnet, p = _atmos_setup(seed=6)
+    q = oracle.Oracle(b)
+    q.set_state(p, p)
+    uek, vek, wekt, wekp, txis, txin = ekman_cyclic(taux, tauy, b.dx, b.dy, b.fnot, prm.hm)
+    ent = np.zeros((b.nl - 1,) + b.shape2)
+    for _ in range(4):
+        qp, qpm, _, _ = q.get_state()
+        o.step(qp[0], uek, vek, wekt, _eta(b, qpm), fnet, True, TDTA, ent)
+        q.set_forcing(wekp, ent, txis, txin)
+        q.step(TDTA, 1)
+        m.forcing(taux, tauy, fnet, True, TDTA)
+        g.step(TDTA, 1)
+    for a, r in zip(g.get_state(), q.get_state()):
+        assert rel_l2(a, r) <= 1e-11
+    assert rel_l2(m.get_state()[0], o.ast) <= 1e-11
+    m.close()
+    g.close()
+
+
+def test_atmos_rejects_a_box():
+    g = QG(ocean_double_gyre(33))
+    with pytest.raises(OqgError):
+        AtmosMixedLayer(g, np.zeros((32, 32)), None, hm=1000.0, rho_cp=1e3, t1_rel=-5.0, dt_12=20.0, hmamin=100.0,
+                        hmadmp=0.5, xcexp=1.0, at2d=0.0, at4d=0.0, ahmd=0.0, aface=(0.0, 0.0), bface=0.0, dface=0.0)
+    g.close()

@@ -62,3 +62,61 @@ def test_entrainment_has_zero_mean_and_sst_is_adjusted():
     ent2 = ent.copy()
     o.step(p1, uek, vek, wekt, fnet, False, 3600.0, ent2)
     assert np.array_equal(ent2, ent)
+
+
+# ---------------------------------------------------------------- atmosphere
+from oracle.mixed_layer import AmlOracle, AmlParams, adv_diff_cyclic, ekman_cyclic  # noqa: E402
+from openqg_b200.params import atmos_channel  # noqa: E402
+
+
+def _channel_case(seed=0):
+    b = atmos_channel(65, 33)
+    rng = np.random.default_rng(seed)
+    y = np.arange(b.nyp) * b.dy
+    taux = np.repeat((0.1 * np.sin(np.pi * y / y[-1]))[:, None], b.nxp, axis=1) + 0.01 * rng.standard_normal(b.shape2)
+    tauy = 0.01 * rng.standard_normal(b.shape2)
+    taux[:, -1] = taux[:, 0]
+    tauy[:, -1] = tauy[:, 0]
+    p1 = b.fnot * 30.0 * initial_psi(b, seed=seed)[0]
+    return b, rng, taux, tauy, p1
+
+
+def test_channel_ekman_matches_cpp_oracle():
+    b, _, taux, tauy, _ = _channel_case()
+    _, _, _, wekp, txis, txin = ekman_cyclic(taux, tauy, b.dx, b.dy, b.fnot, 1000.0)
+    w, ts, tn = oracle.ekman_from_tau(b, taux, tauy)
+    ref = w.reshape(b.shape2)
+    assert np.linalg.norm(wekp - ref) <= 1e-14 * np.linalg.norm(ref)
+    assert abs(txis - ts) <= 1e-14 * abs(ts) and abs(txin - tn) <= 1e-14 * abs(tn)
+
+
+def test_channel_adv_diff_conserves_with_no_flux_walls():
+    b, rng, taux, tauy, p1 = _channel_case(1)
+    uek, vek, _, _, _, _ = ekman_cyclic(taux, tauy, b.dx, b.dy, b.fnot, 1000.0)
+    nyt, nxt = b.nyp - 1, b.nxp - 1
+    t = 3.0 * rng.standard_normal((nyt, nxt))
+    dp_dx = (p1[:, 1:] - p1[:, :-1]) / b.dx
+    dp_dy = (p1[1:, :] - p1[:-1, :]) / b.dy
+    a = adv_diff_cyclic(t, t + 0.1, dp_dx, dp_dy, uek, vek, b.fnot, b.dx, b.dy, 2.5e4, 1e12, 1.0,
+                        False, False, 0.0, 0.0)
+    assert abs(a.sum()) <= 1e-12 * np.abs(a).sum()
+
+
+def test_atmos_step_bounds():
+    """After step_aml the temperature is at most T_bar - T_(1) (the
+    convective correction, amlsubs.F90:278-283) and the height at least
+    hmamin wherever it was stepped."""
+    b, rng, taux, tauy, p1 = _channel_case(2)
+    prm = AmlParams(aface=(1e-6, -2e-7), bface=3e-7, dface=1e-5)
+    nyt, nxt = b.nyp - 1, b.nxp - 1
+    o = AmlOracle(b, prm, xc1ast=0.5 * rng.standard_normal((nyt, nxt)), dtop=np.zeros(b.shape2))
+    o.ast = prm.t1_rel - 2.0 + rng.standard_normal((nyt, nxt))
+    o.astm = o.ast + 0.1 * rng.standard_normal((nyt, nxt))
+    uek, vek, wekt, _, _, _ = ekman_cyclic(taux, tauy, b.dx, b.dy, b.fnot, prm.hm)
+    eta = rng.standard_normal((b.nl - 1,) + b.shape2)
+    eta[..., -1] = eta[..., 0]          # a channel field repeats column 0
+    ent = np.zeros((b.nl - 1,) + b.shape2)
+    o.step(p1, uek, vek, wekt, eta, 30.0 * rng.standard_normal((nyt, nxt)), True, 360.0, ent)
+    assert np.all(o.ast <= prm.t1_rel)
+    assert np.all(o.hmx >= prm.hmamin)
+    assert np.array_equal(ent[0][:, -1], ent[0][:, 0]) and np.all(ent[1:] == 0.0)
