@@ -125,3 +125,14 @@ def test_added_entry_points_reject_null_arguments(liboqg):
     assert L.oqg_oml_get_sst(None, None, None) == 1
     assert L.oqg_ocean_forcing(None, None, None, None, 1, ctypes.c_double(1.0)) == 1
     assert L.oqg_get_forcing(None, None, None) == 1
+    assert L.oqg_aml_create(None, None, None, None, None) == 1
+    assert L.oqg_aml_destroy(None) == 0
+    assert L.oqg_aml_set_state(None, None, None, None, None) == 1
+    assert L.oqg_aml_get_state(None, None, None, None, None) == 1
+    assert L.oqg_atmos_forcing(None, None, None, None, 1, ctypes.c_double(1.0)) == 1
+
+
+def test_aml_params_struct_layout_matches_header():
+    from openqg_b200.params import OqgAmlParams
+    assert OqgAmlParams.aface.offset == 12 * 8
+    assert ctypes.sizeof(OqgAmlParams) == 12 * 8 + 8 * 8
