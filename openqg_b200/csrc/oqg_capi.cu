@@ -254,18 +254,6 @@ static int download3(oqg_handle *h, const double *src, double *dst, int nlay) {
                          b.nxp * sizeof(double), (size_t)b.nyp * nlay, cudaMemcpyDeviceToHost, h->st));
     return OQG_OK;
 }
-// Host rows -> field: one contiguous copy of nlay layers (faster than a
-// pitched copy), then unpacked on the device into the pitched field of the
-// storage type.
-static int upload_rows(oqg_handle *h, const double *src, void *field, int nlay) {
-    const BasinDev &b = h->hb;
-    const size_t nrows = (size_t)b.nyp * nlay;
-    CK(cudaMemcpyAsync(h->hrow, src, nrows * b.nxp * sizeof(double), cudaMemcpyHostToDevice, h->st));
-    if (h->mixed) k_rows_in<float><<<296, 256, 0, h->st>>>(h->hrow, (float *)field, b.nxp, b.px, nrows);
-    else k_rows_in<double><<<296, 256, 0, h->st>>>(h->hrow, (double *)field, b.nxp, b.px, nrows);
-    CK(cudaGetLastError());
-    return OQG_OK;
-}
 // Field -> host rows: packed on the device, then one contiguous copy.
 static int download_rows(oqg_handle *h, const void *field, double *dst, int nlay) {
     const BasinDev &b = h->hb;
