@@ -361,6 +361,7 @@ typedef struct oqg_aml_params {
     double at2d, at4d;      /* temperature diffusivities                     */
     double ahmd;            /* height diffusivity                            */
     double bface, dface;    /* entrainment coefficients (init_entrain_coeff) */
+    double cdat;            /* drag coefficient of the stress (windstress.F90) */
     double aface[OQG_MAX_NL];   /* of eta(1..nl-1)                           */
 } oqg_aml_params;
 
@@ -381,7 +382,10 @@ int oqg_aml_get_state(oqg_aml *m, double *ast, double *astm, double *hmixa,
  * with the handle's current p(:,:,1), eta from its lagged pressure
  * (pm_k - pm_{k+1}) / gp_k, and the net heat flux fnetat (nxt, nyt).  The
  * handle's wekp, txis, txin become the Ekman forcing; when compute_ent, its
- * ent becomes the layer 1/2 entrainment (other layers zero). */
+ * ent becomes the layer 1/2 entrainment (other layers zero).  With taux and
+ * tauy both NULL the stress is the atmosphere's own, from its lagged layer-1
+ * pressure by the quadratic drag law of xforc (windstress.F90:102-148, the
+ * case without the ocean-velocity dependence), computed on the device. */
 int oqg_atmos_forcing(oqg_aml *m, const double *taux, const double *tauy,
                       const double *fnetat, int compute_ent, double tdta);
 

@@ -485,14 +485,14 @@ class AtmosMixedLayer:
     fields (nyt, nxt)."""
 
     def __init__(self, qg: QG, xc1ast, dtop=None, *, hm, rho_cp, t1_rel, dt_12, hmamin, hmadmp, xcexp,
-                 at2d, at4d, ahmd, aface, bface, dface):
+                 at2d, at4d, ahmd, aface, bface, dface, cdat=1.3e-3):
         from .params import OQG_MAX_NL
         self.qg = qg
         b = qg.b
         self.tshape = (b.nyp - 1, b.nxp - 1)
         af = (ctypes.c_double * OQG_MAX_NL)(*([float(a) for a in aface] + [0.0] * (OQG_MAX_NL - len(aface))))
         self._prm = OqgAmlParams(hm, rho_cp, t1_rel, dt_12, hmamin, hmadmp, xcexp, at2d, at4d, ahmd, bface, dface,
-                                 af)
+                                 cdat, af)
         xc = _f64(xc1ast, self.tshape)
         dt = _f64(dtop, b.shape2) if dtop is not None else None
         h = ctypes.c_void_p()
@@ -522,8 +522,14 @@ class AtmosMixedLayer:
         return a
 
     def forcing(self, taux, tauy, fnetat, compute_ent: bool, tdta: float):
+        """taux = tauy = None: the stress from the atmosphere's own lagged
+        pressure (xforc's drag law, computed on the device)."""
         b = self.qg.b
-        tx, ty = _f64(taux, b.shape2), _f64(tauy, b.shape2)
+        if taux is None and tauy is None:
+            tx = ty = None
+        else:
+            tx, ty = _f64(taux, b.shape2), _f64(tauy, b.shape2)
         fn = _f64(fnetat, self.tshape)
-        _check(lib().oqg_atmos_forcing(self.h, tx.ctypes.data, ty.ctypes.data, fn.ctypes.data, int(compute_ent),
+        _check(lib().oqg_atmos_forcing(self.h, None if tx is None else tx.ctypes.data,
+                                       None if ty is None else ty.ctypes.data, fn.ctypes.data, int(compute_ent),
                                        float(tdta)), "oqg_atmos_forcing")

@@ -2224,6 +2224,7 @@ int oqg_aml_create(oqg_handle *h, const oqg_aml_params *prm, const double *xc1as
     o.dx = b.dx; o.dy = b.dy; o.fnot = b.fnot; o.hm = prm->hm; o.rho_cp = prm->rho_cp; o.t1_rel = prm->t1_rel;
     o.dt_12 = prm->dt_12; o.hmamin = prm->hmamin; o.hmadmp = prm->hmadmp; o.xcexp = prm->xcexp;
     o.at2d = prm->at2d; o.at4d = prm->at4d; o.ahmd = prm->ahmd; o.bface = prm->bface; o.dface = prm->dface;
+    o.cdat = prm->cdat;
     for (int k = 0; k < OQG_NLMAX; ++k) {
         o.aface[k] = k < b.nl - 1 ? prm->aface[k] : 0.0;
         o.gp[k] = k < b.nl - 1 ? b.gp[k] : 1.0;
@@ -2294,7 +2295,7 @@ int oqg_aml_get_state(oqg_aml *m, double *ast, double *astm, double *hmixa, doub
 
 int oqg_atmos_forcing(oqg_aml *m, const double *taux, const double *tauy, const double *fnetat, int compute_ent,
                       double tdta) {
-    if (!m || !taux || !tauy || !fnetat) return fail(OQG_EINVAL, "null argument");
+    if (!m || !fnetat || (!taux) != (!tauy)) return fail(OQG_EINVAL, "null argument");
     if (!(tdta > 0.0)) return fail(OQG_EINVAL, "tdta must be > 0");
     oqg_handle *h = m->h;
     BasinDev &b = h->hb;
@@ -2306,11 +2307,22 @@ int oqg_atmos_forcing(oqg_aml *m, const double *taux, const double *tauy, const 
     }
     if (!h->up_ev && cudaEventCreateWithFlags(&h->up_ev, cudaEventDisableTiming) != cudaSuccess)
         return fail(OQG_ECUDA, "cudaEventCreate failed");
-    CK(cudaMemcpyAsync(const_cast<double *>(o.taux), taux, np * sizeof(double), cudaMemcpyDefault, h->st));
-    CK(cudaMemcpyAsync(const_cast<double *>(o.tauy), tauy, np * sizeof(double), cudaMemcpyDefault, h->st));
+    const void *p1 = b.F[h->par], *pm = b.F[1 - h->par];   // driver.F90:127-135
+    if (taux) {
+        CK(cudaMemcpyAsync(const_cast<double *>(o.taux), taux, np * sizeof(double), cudaMemcpyDefault, h->st));
+        CK(cudaMemcpyAsync(const_cast<double *>(o.tauy), tauy, np * sizeof(double), cudaMemcpyDefault, h->st));
+    }
     CK(cudaMemcpyAsync(const_cast<double *>(o.fnet), fnetat, nt * sizeof(double), cudaMemcpyDefault, h->st));
     CK(cudaEventRecord(h->up_ev, h->st));
-    const void *p1 = b.F[h->par], *pm = b.F[1 - h->par];   // driver.F90:127-135
+    if (!taux) {   // the stress from the atmosphere's own lagged pressure (xforc)
+        const int gp = std::min((int)((np + 255) / 256), 148 * 8);
+        if (h->mixed)
+            k_aml_tau<float><<<gp, 256, 0, h->st>>>(h->d_bas, o, (const float *)pm, const_cast<double *>(o.taux),
+                                                    const_cast<double *>(o.tauy));
+        else
+            k_aml_tau<double><<<gp, 256, 0, h->st>>>(h->d_bas, o, (const double *)pm, const_cast<double *>(o.taux),
+                                                     const_cast<double *>(o.tauy));
+    }
     const int grid = std::min((int)((nt + 255) / 256), 148 * 8);
     if (h->mixed) {
         k_aml_step<float><<<grid, 256, 0, h->st>>>(o, (const float *)p1, b.px, tdta, compute_ent);

@@ -187,7 +187,7 @@ __global__ void __launch_bounds__(128) k_oml_post(OmlDev o, T *wekp, T *ent, dou
 // diffused like the ocean's sst with the cyclic branches of the numerics.
 struct AmlDev {
     int nxp, nyp, nxt, nyt, nl, tau_sign;
-    double dx, dy, fnot, hm, rho_cp, t1_rel, dt_12, hmamin, hmadmp, xcexp, at2d, at4d, ahmd, bface, dface;
+    double dx, dy, fnot, hm, rho_cp, t1_rel, dt_12, hmamin, hmadmp, xcexp, at2d, at4d, ahmd, bface, dface, cdat;
     double aface[OQG_NLMAX], gp[OQG_NLMAX];
     const double *taux, *tauy;       // [nyp][nxp]
     const double *fnet;              // [nyt][nxt] net heat flux into the mixed layer (fnetat)
@@ -350,6 +350,30 @@ __global__ void __launch_bounds__(128) k_aml_post(AmlDev o, const T *__restrict_
     if (compute_ent) {
         rs = block_sum(rs, red);
         if (threadIdx.x == 0) ent_rows[j] = rs;
+    }
+}
+
+// The atmosphere's wind stress from its lagged layer-1 pressure (xforc,
+// windstress.F90:102-148, without the ocean-velocity dependence): the
+// geostrophic velocity by dPdx_2bc / dPdy_2bc and the quadratic drag law
+// with the Ekman-layer turning, at every p point of the channel.
+template <class T>
+__global__ void __launch_bounds__(256) k_aml_tau(const BasinDev *__restrict__ bas, AmlDev o, const T *__restrict__ PM1,
+                                                  double *taux, double *tauy) {
+    const BasinDev &b = bas[0];
+    const double cdhfaa = (o.cdat / o.fnot) / o.hm;
+    const double qpreaa = 1.0 / (fabs(cdhfaa) * sqrt(2.0));
+    for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < o.nxp * o.nyp; idx += gridDim.x * blockDim.x) {
+        const int j = idx / o.nxp, i = idx - j * o.nxp;
+        double dpdx, dpdy;
+        dpdxy_bc(PM1, b, i, j, dpdx, dpdy);
+        const double u = -dpdy / o.fnot, v = dpdx / o.fnot;
+        const double u2 = 4.0 * cdhfaa * cdhfaa * (u * u + v * v);
+        const double shrmag = qpreaa * sqrt(-1.0 + sqrt(1.0 + u2));
+        const double cuohf = cdhfaa * shrmag;
+        const double cdochi = o.cdat * shrmag / (1.0 + cuohf * cuohf);
+        taux[idx] = cdochi * (u - cuohf * v);
+        tauy[idx] = cdochi * (v + cuohf * u);
     }
 }
 

@@ -55,7 +55,7 @@ class OqgAmlParams(ctypes.Structure):
     """ctypes mirror of `oqg_aml_params` (include/oqg.h): the atmospheric
     mixed layer's parameters (init_atmos_ml, amlsubs.F90:61-131)."""
     _fields_ = [(n, ctypes.c_double) for n in ("hm", "rho_cp", "t1_rel", "dt_12", "hmamin", "hmadmp", "xcexp",
-                                               "at2d", "at4d", "ahmd", "bface", "dface")] + \
+                                               "at2d", "at4d", "ahmd", "bface", "dface", "cdat")] + \
         [("aface", ctypes.c_double * OQG_MAX_NL)]
 
 

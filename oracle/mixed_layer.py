@@ -281,3 +281,29 @@ class AmlOracle:
             ent[0] = e1 + m.bface * self.dtop
         self.astm, self.ast = self.ast, astnew
         self.hmxm, self.hmx = self.hmx, hnew
+
+
+def atmos_stress(pm1, basin, cdat, hm):
+    """The atmosphere's wind stress from its lagged layer-1 pressure (xforc,
+    windstress.F90:102-148, without the ocean-velocity dependence), with
+    dPdx_2bc / dPdy_2bc (numerics.F90:470-513) of a channel; pm1 (nyp, nxp)."""
+    b = basin
+    ah = 0.5 * b.bcco + 1.0
+    dpdx = np.zeros_like(pm1)
+    dpdx[:, 1:-1] = (pm1[:, 2:] - pm1[:, :-2]) / (2.0 * b.dx)
+    dpdx[:, 0] = (pm1[:, 1] - pm1[:, -2]) / (2.0 * b.dx)
+    dpdx[:, -1] = dpdx[:, 0]
+    dpdx[0] = 0.0
+    dpdx[-1] = 0.0
+    dpdy = np.empty_like(pm1)
+    dpdy[1:-1] = (pm1[2:] - pm1[:-2]) / (2.0 * b.dy)
+    dpdy[0] = (pm1[1] - pm1[0]) / (b.dy * ah)
+    dpdy[-1] = (pm1[-1] - pm1[-2]) / (b.dy * ah)
+    u, v = -dpdy / b.fnot, dpdx / b.fnot
+    cdhfaa = (cdat / b.fnot) / hm
+    qpreaa = 1.0 / (abs(cdhfaa) * np.sqrt(2.0))
+    u2 = 4.0 * cdhfaa * cdhfaa * (u * u + v * v)
+    shrmag = qpreaa * np.sqrt(-1.0 + np.sqrt(1.0 + u2))
+    cuohf = cdhfaa * shrmag
+    cdochi = cdat * shrmag / (1.0 + cuohf * cuohf)
+    return cdochi * (u - cuohf * v), cdochi * (v + cuohf * u)

@@ -134,5 +134,5 @@ def test_added_entry_points_reject_null_arguments(liboqg):
 
 def test_aml_params_struct_layout_matches_header():
     from openqg_b200.params import OqgAmlParams
-    assert OqgAmlParams.aface.offset == 12 * 8
-    assert ctypes.sizeof(OqgAmlParams) == 12 * 8 + 8 * 8
+    assert OqgAmlParams.aface.offset == 13 * 8
+    assert ctypes.sizeof(OqgAmlParams) == 13 * 8 + 8 * 8

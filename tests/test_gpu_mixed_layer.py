@@ -129,7 +129,7 @@ def test_rejected_setups():
 
 
 # ---------------------------------------------------------------- atmosphere
-from oracle.mixed_layer import AmlOracle, AmlParams, ekman_cyclic  # noqa: E402
+from oracle.mixed_layer import AmlOracle, AmlParams, atmos_stress, ekman_cyclic  # noqa: E402
 from openqg_b200.core import AtmosMixedLayer  # noqa: E402
 
 TDTA = 360.0
@@ -217,4 +217,25 @@ def test_atmos_rejects_a_box():
     with pytest.raises(OqgError):
         AtmosMixedLayer(g, np.zeros((32, 32)), None, hm=1000.0, rho_cp=1e3, t1_rel=-5.0, dt_12=20.0, hmamin=100.0,
                         hmadmp=0.5, xcexp=1.0, at2d=0.0, at4d=0.0, ahmd=0.0, aface=(0.0, 0.0), bface=0.0, dface=0.0)
+    g.close()
+
+
+def test_atmos_forcing_with_its_own_stress():
+    """taux = tauy = None: the stress comes from the atmosphere's lagged
+    layer-1 pressure by xforc's drag law, on the device."""
+    b, prm, g, m, o, _, _, fnet, _ = _atmos_setup(seed=8)
+    ent = np.zeros((b.nl - 1,) + b.shape2)
+    g.step(TDTA, 2)                          # a lagged pressure unlike the current one
+    for ce in (True, True):
+        p, pm, _, _ = g.get_state()
+        taux, tauy = atmos_stress(pm[0], b, 1.3e-3, prm.hm)
+        uek, vek, wekt, wekp, _, _ = ekman_cyclic(taux, tauy, b.dx, b.dy, b.fnot, prm.hm)
+        m.forcing(None, None, fnet, ce, TDTA)
+        o.step(p[0], uek, vek, wekt, _eta(b, pm), fnet, ce, TDTA, ent)
+        assert rel_l2(m.get_state()[0], o.ast) <= 1e-12
+        w, e = get_forcing(g)
+        assert rel_l2(w, wekp) <= 1e-12
+        assert rel_l2(e, ent) <= 1e-12
+        g.step(TDTA, 1)
+    m.close()
     g.close()
