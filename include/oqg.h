@@ -332,7 +332,8 @@ int oqg_oml_get_sst(oqg_oml *m, double *sst, double *sstm);
  * current p(:,:,1) and the net heat flux fnetoc (nxt, nyt).  The handle's
  * wekp becomes map_T_to_P(wekt); when compute_ent, its ent becomes the
  * layer 1/2 entrainment (other layers zero), otherwise ent is kept.
- * Arrays in host or device memory. */
+ * Arrays in host or device memory.  taux = tauy = NULL: the stress of the
+ * coupled atmosphere (oqg_oml_couple). */
 int oqg_ocean_forcing(oqg_oml *m, const double *taux, const double *tauy,
                       const double *fnetoc, int compute_ent, double tdto);
 /* The handle's forcing, wekp (nxp, nyp) and ent (nxp, nyp, nl-1), copied
@@ -388,6 +389,19 @@ int oqg_aml_get_state(oqg_aml *m, double *ast, double *astm, double *hmixa,
  * case without the ocean-velocity dependence), computed on the device. */
 int oqg_atmos_forcing(oqg_aml *m, const double *taux, const double *tauy,
                       const double *fnetat, int compute_ent, double tdta);
+
+/* Couples an ocean mixed layer to an atmospheric one (NULL unlinks): from
+ * then on oqg_ocean_forcing with taux and tauy both NULL takes the ocean's
+ * stress from the atmosphere's lagged layer-1 pressure, on the device
+ * (compute_windstress, atmos_geos_vel, atmos_windstress; windstress.F90:
+ * 150-314, the case without the ocean-velocity dependence): the atmospheric
+ * geostrophic velocity and its derivatives over the ocean, interpolated
+ * bicubically to the ocean's p points (bicubic.F90), the drag law with the
+ * atmosphere's cdat and hm, times raoro = rho_atmosphere / rho_ocean.  The
+ * ocean grid must hold whole atmospheric cells (load_grid, grid.F90:36-59);
+ * the ocean sits at the channel's western end, centred in y.  The two
+ * handles' streams are ordered around the read of the pressure. */
+int oqg_oml_couple(oqg_oml *m, oqg_aml *a, double raoro);
 
 /* ---------------------------------------------------------------------
  * State slots and the adjoint step.  The reference has no adjoint (its model

@@ -93,6 +93,7 @@ def lib():
     L.oqg_oml_get_sst.argtypes = [vp, vp, vp]
     L.oqg_ocean_forcing.argtypes = [vp, vp, vp, vp, ctypes.c_int, ctypes.c_double]
     L.oqg_get_forcing.argtypes = [vp, _dp, _dp]
+    L.oqg_oml_couple.argtypes = [vp, vp, ctypes.c_double]
     L.oqg_aml_create.argtypes = [vp, ctypes.POINTER(OqgAmlParams), vp, vp, ctypes.POINTER(vp)]
     L.oqg_aml_destroy.argtypes = [vp]
     L.oqg_aml_set_state.argtypes = [vp, vp, vp, vp, vp]
@@ -459,11 +460,22 @@ class OceanMixedLayer:
         _check(lib().oqg_oml_get_sst(self.h, a.ctypes.data, am.ctypes.data), "oqg_oml_get_sst")
         return a, am
 
+    def couple(self, aml, raoro: float):
+        """Takes the ocean's stress from the atmospheric mixed layer's handle
+        when forcing() gets no stress (oqg_oml_couple); aml None unlinks."""
+        _check(lib().oqg_oml_couple(self.h, None if aml is None else aml.h, float(raoro)), "oqg_oml_couple")
+        self._aml = aml          # keeps the atmosphere alive while coupled
+
     def forcing(self, taux, tauy, fnetoc, compute_ent: bool, tdto: float):
+        """taux = tauy = None: the stress from the coupled atmosphere."""
         b = self.qg.b
-        tx, ty = _f64(taux, b.shape2), _f64(tauy, b.shape2)
+        if taux is None and tauy is None:
+            tx = ty = None
+        else:
+            tx, ty = _f64(taux, b.shape2), _f64(tauy, b.shape2)
         fn = _f64(fnetoc, self.tshape)
-        _check(lib().oqg_ocean_forcing(self.h, tx.ctypes.data, ty.ctypes.data, fn.ctypes.data, int(compute_ent),
+        _check(lib().oqg_ocean_forcing(self.h, None if tx is None else tx.ctypes.data,
+                                       None if ty is None else ty.ctypes.data, fn.ctypes.data, int(compute_ent),
                                        float(tdto)), "oqg_ocean_forcing")
 
 

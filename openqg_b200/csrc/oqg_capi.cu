@@ -1884,6 +1884,9 @@ struct oqg_oml {
     oqg_oml_params prm{};
     std::vector<void *> allocs;
     OmlDev o{};
+    oqg_handle *ha = nullptr;             // the coupled atmosphere's handle (oqg_oml_couple)
+    TauCpl cpl{};
+    cudaEvent_t ev_a = nullptr, ev_o = nullptr;
 };
 
 extern "C" {
@@ -1938,6 +1941,8 @@ int oqg_oml_destroy(oqg_oml *m) {
     if (!m) return OQG_OK;
     // the handle may be gone already: cudaFree waits for the device by itself
     for (void *p : m->allocs) cudaFree(p);
+    if (m->ev_a) cudaEventDestroy(m->ev_a);
+    if (m->ev_o) cudaEventDestroy(m->ev_o);
     delete m;
     return OQG_OK;
 }
@@ -1962,8 +1967,9 @@ int oqg_oml_get_sst(oqg_oml *m, double *sst, double *sstm) {
 
 int oqg_ocean_forcing(oqg_oml *m, const double *taux, const double *tauy, const double *fnetoc, int compute_ent,
                       double tdto) {
-    if (!m || !taux || !tauy || !fnetoc) return fail(OQG_EINVAL, "null argument");
+    if (!m || !fnetoc || (!taux) != (!tauy)) return fail(OQG_EINVAL, "null argument");
     if (!(tdto > 0.0)) return fail(OQG_EINVAL, "tdto must be > 0");
+    if (!taux && !m->ha) return fail(OQG_EINVAL, "no stress given and no atmosphere coupled (oqg_oml_couple)");
     oqg_handle *h = m->h;
     BasinDev &b = h->hb;
     OmlDev &o = m->o;
@@ -1974,10 +1980,29 @@ int oqg_ocean_forcing(oqg_oml *m, const double *taux, const double *tauy, const 
     }
     if (!h->up_ev && cudaEventCreateWithFlags(&h->up_ev, cudaEventDisableTiming) != cudaSuccess)
         return fail(OQG_ECUDA, "cudaEventCreate failed");
-    CK(cudaMemcpyAsync(const_cast<double *>(o.taux), taux, np * sizeof(double), cudaMemcpyDefault, h->st));
-    CK(cudaMemcpyAsync(const_cast<double *>(o.tauy), tauy, np * sizeof(double), cudaMemcpyDefault, h->st));
+    if (taux) {
+        CK(cudaMemcpyAsync(const_cast<double *>(o.taux), taux, np * sizeof(double), cudaMemcpyDefault, h->st));
+        CK(cudaMemcpyAsync(const_cast<double *>(o.tauy), tauy, np * sizeof(double), cudaMemcpyDefault, h->st));
+    }
     CK(cudaMemcpyAsync(const_cast<double *>(o.fnet), fnetoc, nt * sizeof(double), cudaMemcpyDefault, h->st));
     CK(cudaEventRecord(h->up_ev, h->st));
+    if (!taux) {
+        // the stress from the coupled atmosphere's lagged layer-1 pressure: this
+        // stream waits for the atmosphere's queued work, and the atmosphere's
+        // stream waits until the pressure has been read
+        oqg_handle *ha = m->ha;
+        CK(cudaEventRecord(m->ev_a, ha->st));
+        CK(cudaStreamWaitEvent(h->st, m->ev_a, 0));
+        const void *pma = ha->hb.F[1 - ha->par];
+        const int nsub = (m->cpl.nxtoar + 1) * (m->cpl.nytoar + 1);
+        const int gs = std::min((nsub + 255) / 256, 148 * 4);
+        if (ha->mixed) k_cpl_derivs<float><<<gs, 256, 0, h->st>>>(m->cpl, (const float *)pma);
+        else k_cpl_derivs<double><<<gs, 256, 0, h->st>>>(m->cpl, (const double *)pma);
+        CK(cudaEventRecord(m->ev_o, h->st));
+        CK(cudaStreamWaitEvent(ha->st, m->ev_o, 0));
+        const int gt = std::min((int)((np + 255) / 256), 148 * 8);
+        k_cpl_tau<<<gt, 256, 0, h->st>>>(m->cpl, o);
+    }
     const void *p1 = b.F[h->par];   // layer 1 of the current p (driver.F90:96-103)
     if (h->mixed) k_oml_step<float><<<OQG_OML_CTAS, 256, 0, h->st>>>(o, (const float *)p1, b.px, tdto, compute_ent);
     else k_oml_step<double><<<OQG_OML_CTAS, 256, 0, h->st>>>(o, (const double *)p1, b.px, tdto, compute_ent);
@@ -2350,6 +2375,46 @@ int oqg_atmos_forcing(oqg_aml *m, const double *taux, const double *tauy, const 
     else k_forcing_integrals<double><<<1, 512, 0, h->st>>>(h->d_bas, 0);
     CK(cudaGetLastError());
     CK(cudaEventSynchronize(h->up_ev));
+    return OQG_OK;
+}
+
+}  // extern "C"
+
+// ================================================== atmosphere -> ocean stress
+extern "C" {
+
+int oqg_oml_couple(oqg_oml *m, oqg_aml *a, double raoro) {
+    if (!m) return fail(OQG_EINVAL, "null argument");
+    if (!a) {
+        m->ha = nullptr;
+        return OQG_OK;
+    }
+    const BasinDev &bo = m->h->hb, &ba = a->h->hb;
+    const int ndxr = (int)std::lround(ba.dx / bo.dx);
+    if (ndxr < 1 || (bo.nxp - 1) % ndxr || (bo.nyp - 1) % ndxr)
+        return fail(OQG_EINVAL, "the ocean grid must hold whole atmospheric cells (nxt, nyt multiples of dxa/dxo)");
+    TauCpl &c = m->cpl;
+    const int nxtoar = (bo.nxp - 1) / ndxr, nytoar = (bo.nyp - 1) / ndxr;
+    const int r0 = (ba.nyp - 1 - nytoar) / 2;   // load_grid (grid.F90:56-57), 0-based
+    if (nxtoar + 1 > ba.nxp || r0 < 0 || r0 + nytoar + 1 > ba.nyp)
+        return fail(OQG_EINVAL, "the ocean does not fit inside the atmosphere's channel");
+    if (!c.d || c.nxtoar != nxtoar || c.nytoar != nytoar) {
+        void *d = nullptr;
+        if (cudaMalloc(&d, (size_t)8 * (nxtoar + 1) * (nytoar + 1) * sizeof(double)) != cudaSuccess)
+            return fail(OQG_ECUDA, "cudaMalloc of the coupling buffer failed");
+        m->allocs.push_back(d);
+        c.d = (double *)d;
+    }
+    if (!m->ev_a && cudaEventCreateWithFlags(&m->ev_a, cudaEventDisableTiming) != cudaSuccess)
+        return fail(OQG_ECUDA, "cudaEventCreate failed");
+    if (!m->ev_o && cudaEventCreateWithFlags(&m->ev_o, cudaEventDisableTiming) != cudaSuccess)
+        return fail(OQG_ECUDA, "cudaEventCreate failed");
+    c.ndxr = ndxr; c.nxtoar = nxtoar; c.nytoar = nytoar; c.c0 = 0; c.r0 = r0;
+    c.nxp_a = ba.nxp; c.nyp_a = ba.nyp; c.px_a = ba.px;
+    c.dxa = ba.dx; c.dya = ba.dy; c.f0a = ba.fnot; c.ah = ba.bc_half1;
+    c.fxa = ba.fx; c.fya = ba.fy; c.fyb = ba.fy_bc;
+    c.cdat = a->o.cdat; c.hma = a->o.hm; c.raoro = raoro;
+    m->ha = a->h;
     return OQG_OK;
 }
 

@@ -181,6 +181,108 @@ __global__ void __launch_bounds__(128) k_oml_post(OmlDev o, T *wekp, T *ent, dou
 }
 
 
+// ------------------------------------------------- stress on the ocean
+// The ocean's wind stress from the atmosphere's lagged layer-1 pressure
+// (compute_windstress, atmos_geos_vel, atmos_windstress; windstress.F90:
+// 150-314, without the ocean-velocity dependence).
+struct TauCpl {
+    int ndxr, nxtoar, nytoar, c0, r0;   // load_grid (grid.F90:36-59), 0-based origin
+    int nxp_a, nyp_a, px_a;
+    double dxa, dya, f0a, ah, fxa, fya, fyb;   // the atmosphere's spacing and BC factors
+    double cdat, hma, raoro;
+    double *d;                          // [8][nytoar+1][nxtoar+1]: u, ux, uy, uxy, v, vx, vy, vxy
+};
+
+// The atmospheric geostrophic velocity and its scaled derivatives at the
+// atmospheric p points over the ocean (atmos_geos_vel, :199-259), from the
+// channel's dPdx_2bc, dPdy_2bc, dP2dx2_bc, dP2dy2_bc (numerics.F90:410-513)
+// applied as there (dp2_dxy = Dx Dy p, dp3_dxxy = Dx Dx Dy p, dp3_dxyy =
+// Dx Dyy p), each nested value taken at the points the outer one reads.
+template <class T>
+__global__ void k_cpl_derivs(TauCpl c, const T *__restrict__ PM1) {
+    const int nx = c.nxtoar + 1, ny = c.nytoar + 1, nxp = c.nxp_a, nyp = c.nyp_a;
+    auto P = [&](int i, int j) { return (double)PM1[(size_t)j * c.px_a + i]; };
+    auto Dy = [&](int i, int j) {
+        if (j == 0) return (P(i, 1) - P(i, 0)) / (c.dya * c.ah);
+        if (j == nyp - 1) return (P(i, nyp - 1) - P(i, nyp - 2)) / (c.dya * c.ah);
+        return (P(i, j + 1) - P(i, j - 1)) / (2.0 * c.dya);
+    };
+    auto Dyy = [&](int i, int j) {
+        if (j == 0) return c.fyb * (P(i, 1) - P(i, 0));
+        if (j == nyp - 1) return -c.fyb * (P(i, nyp - 1) - P(i, nyp - 2));
+        return c.fya * (P(i, j - 1) + P(i, j + 1) - 2.0 * P(i, j));
+    };
+    // dPdx_2bc of a field given by F at (i, j), cyclic
+    auto Dx = [&](auto F, int i, int j) {
+        if (j == 0 || j == nyp - 1) return 0.0;
+        if (i == 0 || i == nxp - 1) return (F(1, j) - F(nxp - 2, j)) / (2.0 * c.dxa);
+        return (F(i + 1, j) - F(i - 1, j)) / (2.0 * c.dxa);
+    };
+    auto Dxx = [&](int i, int j) {
+        if (j == 0 || j == nyp - 1) return 0.0;
+        if (i == 0 || i == nxp - 1) return c.fxa * (P(nxp - 2, j) + P(1, j) - 2.0 * P(0, j));
+        return c.fxa * (P(i - 1, j) + P(i + 1, j) - 2.0 * P(i, j));
+    };
+    auto DxDy = [&](int i, int j) { return Dx(Dy, i, j); };
+    for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < nx * ny; idx += gridDim.x * blockDim.x) {
+        const int r = idx / nx, col = idx - r * nx;
+        const int i = c.c0 + col, j = c.r0 + r;
+        const double f0 = c.f0a, dx = c.dxa, dy = c.dya;
+        const size_t n = (size_t)nx * ny;
+        double *d = c.d + idx;
+        d[0] = -Dy(i, j) / f0;
+        d[n] = -(dx / f0) * DxDy(i, j);
+        d[2 * n] = -(dy / f0) * Dyy(i, j);
+        d[3 * n] = -(dx * dy / f0) * Dx(Dyy, i, j);
+        d[4 * n] = Dx(P, i, j) / f0;
+        d[5 * n] = (dx / f0) * Dxx(i, j);
+        d[6 * n] = (dy / f0) * DxDy(i, j);
+        d[7 * n] = (dx * dy / f0) * Dx(DxDy, i, j);
+    }
+}
+
+// The bicubic interpolation of the atmospheric velocity to the ocean's p
+// points (the unique bicubic matching each cell's nodal values and scaled
+// derivatives, as new_bicubic, bicubic.F90:24-85; a shared cell edge takes
+// the later cell) and the drag law there (atmos_windstress, :278-314), times
+// the density ratio: the ocean's taux, tauy (compute_windstress, :187-195).
+__global__ void k_cpl_tau(TauCpl c, OmlDev o) {
+    const int nx = c.nxtoar + 1, nd = c.ndxr;
+    const size_t n = (size_t)nx * (c.nytoar + 1);
+    const double cdhfaa = (c.cdat / c.f0a) / c.hma;
+    const double qpreaa = 1.0 / (fabs(cdhfaa) * sqrt(2.0));
+    for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < o.nxp * o.nyp; idx += gridDim.x * blockDim.x) {
+        const int jo = idx / o.nxp, io = idx - jo * o.nxp;
+        const int ci = min(io / nd, c.nxtoar - 1), cj = min(jo / nd, c.nytoar - 1);
+        const double s = (double)(io - ci * nd) / nd, t = (double)(jo - cj * nd) / nd;
+        const double hs[2] = {1.0 - 3.0 * s * s + 2.0 * s * s * s, 3.0 * s * s - 2.0 * s * s * s};
+        const double ks[2] = {s - 2.0 * s * s + s * s * s, -s * s + s * s * s};
+        const double ht[2] = {1.0 - 3.0 * t * t + 2.0 * t * t * t, 3.0 * t * t - 2.0 * t * t * t};
+        const double kt[2] = {t - 2.0 * t * t + t * t * t, -t * t + t * t * t};
+        double uv[2] = {0.0, 0.0};
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            const double *f = c.d + 4 * q * n;
+            double acc = 0.0;
+#pragma unroll
+            for (int a = 0; a < 2; ++a)
+#pragma unroll
+                for (int b2 = 0; b2 < 2; ++b2) {
+                    const size_t k = (size_t)(cj + b2) * nx + ci + a;
+                    acc = acc + (f[k] * hs[a] * ht[b2] + f[n + k] * ks[a] * ht[b2] + f[2 * n + k] * hs[a] * kt[b2] +
+                                 f[3 * n + k] * ks[a] * kt[b2]);
+                }
+            uv[q] = acc;
+        }
+        const double u = uv[0], v = uv[1];
+        const double shrmag = sqrt(-1.0 + sqrt(1.0 + 4.0 * cdhfaa * cdhfaa * (u * u + v * v)));
+        const double cuohf = (qpreaa * cdhfaa) * shrmag;
+        const double cdchi = (qpreaa * c.cdat) * shrmag / (1.0 + cuohf * cuohf);
+        const_cast<double *>(o.taux)[idx] = c.raoro * (cdchi * (u - cuohf * v));
+        const_cast<double *>(o.tauy)[idx] = c.raoro * (cdchi * (v + cuohf * u));
+    }
+}
+
 // ---------------------------------------------------------------- atmosphere
 // The atmospheric mixed layer of a zonally periodic channel (step_aml,
 // amlsubs.F90:184-326): temperature ast and height hmixa, advected and

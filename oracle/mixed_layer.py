@@ -307,3 +307,112 @@ def atmos_stress(pm1, basin, cdat, hm):
     cuohf = cdhfaa * shrmag
     cdochi = cdat * shrmag / (1.0 + cuohf * cuohf)
     return cdochi * (u - cuohf * v), cdochi * (v + cuohf * u)
+
+
+# ------------------------------------------------------- stress on the ocean
+def _dx_bc_c(f, dx):
+    """dPdx_2bc of a channel field (numerics.F90:470-492)."""
+    o = np.zeros_like(f)
+    o[:, 1:-1] = (f[:, 2:] - f[:, :-2]) / (2.0 * dx)
+    o[:, 0] = (f[:, 1] - f[:, -2]) / (2.0 * dx)
+    o[:, -1] = o[:, 0]
+    o[0] = 0.0
+    o[-1] = 0.0
+    return o
+
+
+def _dy_bc_c(f, dy, ah):
+    """dPdy_2bc of a channel field (numerics.F90:494-513)."""
+    o = np.empty_like(f)
+    o[1:-1] = (f[2:] - f[:-2]) / (2.0 * dy)
+    o[0] = (f[1] - f[0]) / (dy * ah)
+    o[-1] = (f[-1] - f[-2]) / (dy * ah)
+    return o
+
+
+def _dxx_bc_c(f, dx):
+    """dP2dx2_bc of a channel field (numerics.F90:427-448)."""
+    fac = 1.0 / (dx * dx)
+    o = np.zeros_like(f)
+    o[:, 1:-1] = fac * (f[:, :-2] + f[:, 2:] - 2.0 * f[:, 1:-1])
+    o[:, 0] = fac * (f[:, -2] + f[:, 1] - 2.0 * f[:, 0])
+    o[:, -1] = o[:, 0]
+    o[0] = 0.0
+    o[-1] = 0.0
+    return o
+
+
+def _dyy_bc_c(f, dy, alpha):
+    """dP2dy2_bc of a channel field (numerics.F90:450-468)."""
+    fac = 1.0 / (dy * dy)
+    o = np.empty_like(f)
+    o[1:-1] = fac * (f[:-2] + f[2:] - 2.0 * f[1:-1])
+    o[0] = fac * alpha / (0.5 * alpha + 1.0) * (f[1] - f[0])
+    o[-1] = -fac * alpha / (0.5 * alpha + 1.0) * (f[-1] - f[-2])
+    return o
+
+
+def coupling_grid(bo, ba):
+    """load_grid (grid.F90:36-59): the atmosphere/ocean resolution ratio
+    ndxr, the ocean's cells at atmospheric resolution and the 0-based first
+    atmospheric p row and column of the ocean."""
+    ndxr = int(round(ba.dx / bo.dx))
+    nxtoar, nytoar = (bo.nxp - 1) // ndxr, (bo.nyp - 1) // ndxr
+    ny1 = (ba.nyp - 1 - nytoar) // 2
+    return ndxr, nxtoar, nytoar, 0, ny1
+
+
+def hermite_bicubic(f, fx, fy, fxy, ndxr):
+    """Bicubic interpolation of nodal values and scaled derivatives (per unit
+    cell: fx = dx df/dx, ...) on (n+1, m+1) nodes to the ndxr-times finer
+    grid; the interpolant is the tensor product of the cubic Hermite bases,
+    the unique bicubic matching the 16 values of each cell (the role of
+    new_bicubic, bicubic.F90:24-85).  Shared cell edges take the later cell,
+    as bc3 writes them."""
+    ny, nx = f.shape[0] - 1, f.shape[1] - 1
+    io = np.arange(nx * ndxr + 1)
+    jo = np.arange(ny * ndxr + 1)
+    ci = np.minimum(io // ndxr, nx - 1)
+    cj = np.minimum(jo // ndxr, ny - 1)
+    s = (io - ci * ndxr) / ndxr
+    t = (jo - cj * ndxr) / ndxr
+    H0 = lambda x: 1.0 - 3.0 * x * x + 2.0 * x * x * x
+    H1 = lambda x: 3.0 * x * x - 2.0 * x * x * x
+    K0 = lambda x: x - 2.0 * x * x + x * x * x
+    K1 = lambda x: -x * x + x * x * x
+    out = np.zeros((jo.size, io.size))
+    S, T = s[None, :], t[:, None]
+    for a, (Ha, Ka) in enumerate(((H0, K0), (H1, K1))):
+        for c, (Hc, Kc) in enumerate(((H0, K0), (H1, K1))):
+            J, I = (cj + c)[:, None], (ci + a)[None, :]
+            out = out + (f[J, I] * Ha(S) * Hc(T) + fx[J, I] * Ka(S) * Hc(T)
+                         + fy[J, I] * Ha(S) * Kc(T) + fxy[J, I] * Ka(S) * Kc(T))
+    return out
+
+
+def ocean_stress(pma1, ba, bo, cdat, hma, raoro):
+    """The ocean's wind stress from the atmosphere's lagged layer-1 pressure
+    (compute_windstress, atmos_geos_vel, atmos_windstress; windstress.F90:
+    150-314, without the ocean-velocity dependence): the atmospheric
+    geostrophic velocity and its derivatives on the atmospheric p points over
+    the ocean, interpolated bicubically to the ocean's p points, the drag
+    law there, times the density ratio raoro.  Returns taux, tauy (nyp, nxp)."""
+    ndxr, nxtoar, nytoar, c0, r0 = coupling_grid(bo, ba)
+    ah = 0.5 * ba.bcco + 1.0
+    p = pma1
+    dpdx, dpdy = _dx_bc_c(p, ba.dx), _dy_bc_c(p, ba.dy, ah)
+    d2x, d2y = _dxx_bc_c(p, ba.dx), _dyy_bc_c(p, ba.dy, ba.bcco)
+    dxy = _dx_bc_c(dpdy, ba.dx)
+    dxxy, dxyy = _dx_bc_c(dxy, ba.dx), _dx_bc_c(d2y, ba.dx)
+    sub = (slice(r0, r0 + nytoar + 1), slice(c0, c0 + nxtoar + 1))
+    f0, dx, dy = ba.fnot, ba.dx, ba.dy
+    u = hermite_bicubic(-dpdy[sub] / f0, -(dx / f0) * dxy[sub], -(dy / f0) * d2y[sub],
+                        -(dx * dy / f0) * dxyy[sub], ndxr)
+    v = hermite_bicubic(dpdx[sub] / f0, (dx / f0) * d2x[sub], (dy / f0) * dxy[sub],
+                        (dx * dy / f0) * dxxy[sub], ndxr)
+    cdhfaa = (cdat / f0) / hma
+    qpreaa = 1.0 / (abs(cdhfaa) * np.sqrt(2.0))
+    shrmag = np.sqrt(-1.0 + np.sqrt(1.0 + 4.0 * cdhfaa * cdhfaa * (u * u + v * v)))
+    cuohf = (qpreaa * cdhfaa) * shrmag
+    cdchi = (qpreaa * cdat) * shrmag / (1.0 + cuohf * cuohf)
+    return raoro * (cdchi * (u - cuohf * v)), raoro * (cdchi * (v + cuohf * u))

@@ -129,7 +129,7 @@ def test_rejected_setups():
 
 
 # ---------------------------------------------------------------- atmosphere
-from oracle.mixed_layer import AmlOracle, AmlParams, atmos_stress, ekman_cyclic  # noqa: E402
+from oracle.mixed_layer import AmlOracle, AmlParams, atmos_stress, ekman_cyclic, ocean_stress  # noqa: E402
 from openqg_b200.core import AtmosMixedLayer  # noqa: E402
 
 TDTA = 360.0
@@ -239,3 +239,54 @@ def test_atmos_forcing_with_its_own_stress():
         g.step(TDTA, 1)
     m.close()
     g.close()
+
+
+def test_ocean_stress_from_the_coupled_atmosphere():
+    """The ocean (129x129 at 10 km) coupled to an atmosphere channel (49x25 at
+    80 km): with no stress given, the ocean's stress comes from the
+    atmosphere's lagged layer-1 pressure through the bicubic interpolation
+    and the drag law, on the device."""
+    ba = atmos_channel(49, 25, dx=80e3)
+    ga = QG(ba)
+    pa = ba.fnot * 30.0 * initial_psi(ba, seed=3)
+    ga.set_state(pa, pa)
+    y = np.arange(ba.nyp) * ba.dy
+    txa = np.repeat((0.05 * np.sin(np.pi * y / y[-1]))[:, None], ba.nxp, axis=1)
+    w, ts, tn = oracle.ekman_from_tau(ba, txa, np.zeros_like(txa))
+    ga.set_forcing(w, None, ts, tn)
+    ga.step(TDTA, 3)                           # p and pm differ
+    aprm = AmlParams(aface=(1e-7, -1e-7), bface=1e-7, dface=1e-6)
+    aml = AtmosMixedLayer(ga, np.zeros((ba.nyp - 1, ba.nxp - 1)), None, hm=aprm.hm, rho_cp=aprm.rho_cp,
+                          t1_rel=aprm.t1_rel, dt_12=aprm.dt_12, hmamin=aprm.hmamin, hmadmp=aprm.hmadmp,
+                          xcexp=aprm.xcexp, at2d=aprm.at2d, at4d=aprm.at4d, ahmd=aprm.ahmd, aface=aprm.aface,
+                          bface=aprm.bface, dface=aprm.dface, cdat=1.3e-3)
+    prm = OmlParams(hm=100.0, rho_cp=4.0e6, t1_rel=10.0, dt_12=5.0, st2d=2.0e3, st4d=1.0e11, ycexp=1.0)
+    b = ocean_double_gyre(129, dx=10.0e3)
+    g = QG(b)
+    p = b.fnot * initial_psi(b, seed=9)
+    g.set_state(p, p)
+    m = OceanMixedLayer(g, prm.hm, prm.rho_cp, prm.t1_rel, prm.dt_12, prm.st2d, prm.st4d, prm.ycexp,
+                        prm.fluxn, prm.fluxs, prm.nval, prm.sval)
+    sst = prm.t1_rel + 2.0 + np.zeros((b.nyp - 1, b.nxp - 1))
+    m.set_sst(sst, sst)
+    o = OmlOracle(b, prm)
+    o.data, o.datam = sst.copy(), sst.copy()
+    fnet = np.zeros((b.nyp - 1, b.nxp - 1))
+    m.couple(aml, 1.2e-3)
+    ent = np.zeros((b.nl - 1,) + b.shape2)
+    for _ in range(2):
+        pma = ga.get_state()[1][0]
+        taux, tauy = ocean_stress(pma, ba, b, 1.3e-3, aprm.hm, 1.2e-3)
+        uek, vek, wekt, wekp = ekman(taux, tauy, b.dx, b.dy, b.fnot, prm.hm)
+        p1 = g.get_state()[0][0]
+        m.forcing(None, None, fnet, True, TDT)
+        o.step(p1, uek, vek, wekt, fnet, True, TDT, ent)
+        w, e = get_forcing(g)
+        assert rel_l2(w, wekp) <= 1e-12
+        assert rel_l2(e, ent) <= 1e-12
+        assert rel_l2(m.get_sst()[0], o.data) <= 1e-12
+        g.step(TDT, 1)
+        aml.forcing(None, None, np.zeros((ba.nyp - 1, ba.nxp - 1)), True, TDTA)
+        ga.step(TDTA, 1)
+    for x in (m, aml, g, ga):
+        x.close()

@@ -120,3 +120,22 @@ def test_atmos_step_bounds():
     assert np.all(o.ast <= prm.t1_rel)
     assert np.all(o.hmx >= prm.hmamin)
     assert np.array_equal(ent[0][:, -1], ent[0][:, 0]) and np.all(ent[1:] == 0.0)
+
+
+def test_hermite_bicubic_reproduces_bicubics_and_nodes():
+    """The interpolant is exact for a bicubic polynomial given exact scaled
+    derivatives, and equals the nodal values at the coarse nodes."""
+    from oracle.mixed_layer import hermite_bicubic
+    rng = np.random.default_rng(5)
+    C = rng.standard_normal((4, 4))
+    P = lambda x, y: sum(C[a, c] * x ** a * y ** c for a in range(4) for c in range(4))
+    Px = lambda x, y: sum(a * C[a, c] * x ** (a - 1) * y ** c for a in range(1, 4) for c in range(4))
+    Py = lambda x, y: sum(c * C[a, c] * x ** a * y ** (c - 1) for a in range(4) for c in range(1, 4))
+    Pxy = lambda x, y: sum(a * c * C[a, c] * x ** (a - 1) * y ** (c - 1) for a in range(1, 4) for c in range(1, 4))
+    h, nd = 0.3, 6
+    X, Y = np.meshgrid(np.arange(5) * h, np.arange(4) * h)
+    out = hermite_bicubic(P(X, Y), h * Px(X, Y), h * Py(X, Y), h * h * Pxy(X, Y), nd)
+    Xf, Yf = np.meshgrid(np.arange(4 * nd + 1) * h / nd, np.arange(3 * nd + 1) * h / nd)
+    ref = P(Xf, Yf)
+    assert np.max(np.abs(out - ref)) <= 1e-12 * np.max(np.abs(ref))
+    assert np.array_equal(out[::nd, ::nd], P(X, Y))
