@@ -130,6 +130,7 @@ def test_added_entry_points_reject_null_arguments(liboqg):
     assert L.oqg_aml_set_state(None, None, None, None, None) == 1
     assert L.oqg_aml_get_state(None, None, None, None, None) == 1
     assert L.oqg_atmos_forcing(None, None, None, None, 1, ctypes.c_double(1.0)) == 1
+    assert L.oqg_oml_couple(None, None, ctypes.c_double(1.2e-3)) == 1
 
 
 def test_aml_params_struct_layout_matches_header():
