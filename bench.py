@@ -248,14 +248,16 @@ def coupled_config(nrep=3, nocean=10, nstr=10):
     """The coupled configuration's step loop on the device: per ocean step
     nstr atmosphere steps (193x97x3 channel, dx 80 km, tdt 360 s) each after
     oqg_atmos_forcing, then one ocean step (513x513x3 box, dx 10 km, tdt
-    3600 s) after oqg_ocean_forcing (driver.F90:95-143).  The radiation
-    scheme's and the stress interpolation's outputs (wind stress, net heat
-    fluxes) cross from pinned host memory each step, fixed synthetic fields;
-    the mixed layers, Ekman fields, entrainment and QG steps run on the
-    device.  Host clock over nocean coupled ocean steps, median of nrep."""
+    3600 s) after oqg_ocean_forcing (driver.F90:95-143).  Both basins' wind
+    stress comes from the atmosphere's lagged pressure on the device (xforc;
+    the ocean's through the bicubic interpolation, oqg_oml_couple); the
+    radiation scheme's outputs (net heat fluxes) cross from pinned host
+    memory each step, fixed synthetic fields; the mixed layers, Ekman fields,
+    entrainment and QG steps run on the device.  Host clock over nocean
+    coupled ocean steps, median of nrep."""
     import torch
     from openqg_b200.core import QG, AtmosMixedLayer, OceanMixedLayer, lib
-    from openqg_b200.params import atmos_channel, double_gyre_tau, ocean_double_gyre
+    from openqg_b200.params import atmos_channel, ocean_double_gyre
     L = lib()
     bo, ba = ocean_double_gyre(513, dx=10e3), atmos_channel(193, 97, dx=80e3)
     go, ga = QG(bo), QG(ba)
@@ -264,29 +266,27 @@ def coupled_config(nrep=3, nocean=10, nstr=10):
     go.set_state(po, po)
     ga.set_state(pa, pa)
     pin = lambda a: torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64)).pin_memory()
-    txo, tyo = double_gyre_tau(bo)
     yo = np.linspace(0.0, 1.0, bo.nyp - 1)[:, None] * np.ones((1, bo.nxp - 1))
     oml = OceanMixedLayer(go, hm=100.0, rho_cp=4.0e6, t1_rel=10.0, dt_12=5.0, st2d=2.0e3, st4d=0.0, ycexp=1.0)
     sst = 12.0 + 3.0 * np.cos(np.pi * yo)
     oml.set_sst(sst, sst)
-    ya = np.arange(ba.nyp) * ba.dy
-    txa = np.repeat((0.1 * np.sin(np.pi * ya / ya[-1]))[:, None], ba.nxp, axis=1)
     yt = np.linspace(0.0, 1.0, ba.nyp - 1)[:, None] * np.ones((1, ba.nxp - 1))
     aml = AtmosMixedLayer(ga, np.zeros_like(yt), None, hm=1000.0, rho_cp=1.0e3, t1_rel=-5.0, dt_12=20.0,
                           hmamin=100.0, hmadmp=0.5, xcexp=1.0, at2d=2.5e4, at4d=0.0, ahmd=2.0e4,
-                          aface=(1e-7, -1e-7), bface=1e-7, dface=1e-6)
+                          aface=(1e-7, -1e-7), bface=1e-7, dface=1e-6, cdat=1.3e-3)
     aml.set_state(-8.0 + 2.0 * np.cos(np.pi * yt), -8.0 + 2.0 * np.cos(np.pi * yt),
                   np.full(yt.shape, 1000.0), np.full(yt.shape, 1000.0))
-    bufs = [pin(a) for a in (txo, tyo, 20.0 * np.cos(np.pi * yo), txa, np.zeros_like(txa), 10.0 * np.cos(np.pi * yt))]
+    oml.couple(aml, 1.2e-3)     # rho_a / rho_o
+    bufs = [pin(a) for a in (20.0 * np.cos(np.pi * yo), 10.0 * np.cos(np.pi * yt))]
     ptr = [ctypes.c_void_p(t.data_ptr()) for t in bufs]
 
     def coupled_step():
         for _ in range(nstr):
-            rc = L.oqg_atmos_forcing(aml.h, ptr[3], ptr[4], ptr[5], 1, ctypes.c_double(360.0))
+            rc = L.oqg_atmos_forcing(aml.h, None, None, ptr[1], 1, ctypes.c_double(360.0))
             rc |= L.oqg_step(ga.h, ctypes.c_double(360.0), 1)
             if rc:
                 raise RuntimeError(L.oqg_last_error().decode())
-        rc = L.oqg_ocean_forcing(oml.h, ptr[0], ptr[1], ptr[2], 1, ctypes.c_double(3600.0))
+        rc = L.oqg_ocean_forcing(oml.h, None, None, ptr[0], 1, ctypes.c_double(3600.0))
         rc |= L.oqg_step(go.h, ctypes.c_double(3600.0), 1)
         if rc:
             raise RuntimeError(L.oqg_last_error().decode())
@@ -311,8 +311,9 @@ def coupled_config(nrep=3, nocean=10, nstr=10):
     ms = statistics.median(times) / nocean
     cells = bo.nxp * bo.nyp * bo.nl + nstr * ba.nxp * ba.nyp * ba.nl
     return {"workload": "ocean 513x513x3 box (dx 10 km, tdt 3600 s) + atmosphere 193x97x3 channel (dx 80 km, "
-                        "tdt 360 s, %d steps per ocean step), both mixed layers and Ekman fields on the device; "
-                        "wind stress and net heat fluxes from pinned host memory every step" % nstr,
+                        "tdt 360 s, %d steps per ocean step), both mixed layers, Ekman fields and both wind "
+                        "stresses (bicubic onto the ocean) on the device; net heat fluxes from pinned host "
+                        "memory every step" % nstr,
             "ms_per_coupled_ocean_step": ms, "value": cells / (ms / 1e3) / 1e6, "unit": "Mcell-layer-steps/s",
             "timer": "host clock, median of %d runs of %d coupled ocean steps" % (nrep, nocean)}
 
