@@ -245,19 +245,19 @@ def coupled_e2e(g, b, tdt, msteps, nbatch):
 
 
 def coupled_config(nrep=3, nocean=10, nstr=10):
-    """The coupled configuration's step loop on the device: per ocean step
-    nstr atmosphere steps (193x97x3 channel, dx 80 km, tdt 360 s) each after
-    oqg_atmos_forcing, then one ocean step (513x513x3 box, dx 10 km, tdt
-    3600 s) after oqg_ocean_forcing (driver.F90:95-143).  Both basins' wind
-    stress comes from the atmosphere's lagged pressure on the device (xforc;
-    the ocean's through the bicubic interpolation, oqg_oml_couple); the
-    radiation scheme's outputs (net heat fluxes) cross from pinned host
-    memory each step, fixed synthetic fields; the mixed layers, Ekman fields,
-    entrainment and QG steps run on the device.  Host clock over nocean
-    coupled ocean steps, median of nrep."""
-    import torch
+    """The coupled configuration's step loop on the device (dynamic_step,
+    driver.F90:33-143): per ocean step, xforc (both basins' wind stress from
+    the atmosphere's lagged pressure, the ocean's through the bicubic
+    interpolation) and compute_forcing (both mixed layers' net heat fluxes),
+    then nstr atmosphere steps (193x97x3 channel, dx 80 km, tdt 360 s) each
+    after oqg_atmos_forcing, the first followed by one ocean step (513x513x3
+    box, dx 10 km, tdt 3600 s) after oqg_ocean_forcing.  Every exchange runs
+    on the device; nothing crosses from the host inside the loop.  The
+    radiation coefficients are fixed synthetic values of the reference's
+    magnitudes.  Host clock over nocean coupled ocean steps, median of
+    nrep."""
     from openqg_b200.core import QG, AtmosMixedLayer, OceanMixedLayer, lib
-    from openqg_b200.params import atmos_channel, ocean_double_gyre
+    from openqg_b200.params import OqgRadCoeffs, atmos_channel, ocean_double_gyre
     L = lib()
     bo, ba = ocean_double_gyre(513, dx=10e3), atmos_channel(193, 97, dx=80e3)
     go, ga = QG(bo), QG(ba)
@@ -265,7 +265,6 @@ def coupled_config(nrep=3, nocean=10, nstr=10):
     pa, _, _, _ = initial_inputs(ba, seed=4)
     go.set_state(po, po)
     ga.set_state(pa, pa)
-    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64)).pin_memory()
     yo = np.linspace(0.0, 1.0, bo.nyp - 1)[:, None] * np.ones((1, bo.nxp - 1))
     oml = OceanMixedLayer(go, hm=100.0, rho_cp=4.0e6, t1_rel=10.0, dt_12=5.0, st2d=2.0e3, st4d=0.0, ycexp=1.0)
     sst = 12.0 + 3.0 * np.cos(np.pi * yo)
@@ -277,19 +276,20 @@ def coupled_config(nrep=3, nocean=10, nstr=10):
     aml.set_state(-8.0 + 2.0 * np.cos(np.pi * yt), -8.0 + 2.0 * np.cos(np.pi * yt),
                   np.full(yt.shape, 1000.0), np.full(yt.shape, 1000.0))
     oml.couple(aml, 1.2e-3)     # rho_a / rho_o
-    bufs = [pin(a) for a in (20.0 * np.cos(np.pi * yo), 10.0 * np.cos(np.pi * yt))]
-    ptr = [ctypes.c_void_p(t.data_ptr()) for t in bufs]
+    rad = OqgRadCoeffs(fspco=80.0, xlamda=35.0, d0up=5.5, dmdown=3.5, dup0=2.5, aup00=-0.03, adown10=0.02,
+                       adown11=0.01)
 
     def coupled_step():
-        for _ in range(nstr):
-            rc = L.oqg_atmos_forcing(aml.h, None, None, ptr[1], 1, ctypes.c_double(360.0))
+        rc = L.oqg_xforc(aml.h, oml.h)
+        rc |= L.oqg_compute_forcing(oml.h, ctypes.byref(rad))
+        for s in range(nstr):
+            rc |= L.oqg_atmos_forcing(aml.h, None, None, None, 1, ctypes.c_double(360.0))
             rc |= L.oqg_step(ga.h, ctypes.c_double(360.0), 1)
+            if s == 0:
+                rc |= L.oqg_ocean_forcing(oml.h, None, None, None, 1, ctypes.c_double(3600.0))
+                rc |= L.oqg_step(go.h, ctypes.c_double(3600.0), 1)
             if rc:
                 raise RuntimeError(L.oqg_last_error().decode())
-        rc = L.oqg_ocean_forcing(oml.h, None, None, ptr[0], 1, ctypes.c_double(3600.0))
-        rc |= L.oqg_step(go.h, ctypes.c_double(3600.0), 1)
-        if rc:
-            raise RuntimeError(L.oqg_last_error().decode())
 
     coupled_step()
     go.sync()
@@ -311,9 +311,9 @@ def coupled_config(nrep=3, nocean=10, nstr=10):
     ms = statistics.median(times) / nocean
     cells = bo.nxp * bo.nyp * bo.nl + nstr * ba.nxp * ba.nyp * ba.nl
     return {"workload": "ocean 513x513x3 box (dx 10 km, tdt 3600 s) + atmosphere 193x97x3 channel (dx 80 km, "
-                        "tdt 360 s, %d steps per ocean step), both mixed layers, Ekman fields and both wind "
-                        "stresses (bicubic onto the ocean) on the device; net heat fluxes from pinned host "
-                        "memory every step" % nstr,
+                        "tdt 360 s, %d steps per ocean step); xforc (both stresses, bicubic onto the ocean), "
+                        "compute_forcing (both heat fluxes), both mixed layers and Ekman fields on the device, "
+                        "nothing from the host in the loop" % nstr,
             "ms_per_coupled_ocean_step": ms, "value": cells / (ms / 1e3) / 1e6, "unit": "Mcell-layer-steps/s",
             "timer": "host clock, median of %d runs of %d coupled ocean steps" % (nrep, nocean)}
 

@@ -332,8 +332,9 @@ int oqg_oml_get_sst(oqg_oml *m, double *sst, double *sstm);
  * current p(:,:,1) and the net heat flux fnetoc (nxt, nyt).  The handle's
  * wekp becomes map_T_to_P(wekt); when compute_ent, its ent becomes the
  * layer 1/2 entrainment (other layers zero), otherwise ent is kept.
- * Arrays in host or device memory.  taux = tauy = NULL: the stress of the
- * coupled atmosphere (oqg_oml_couple). */
+ * Arrays in host or device memory.  taux = tauy = NULL: the stress that
+ * oqg_xforc last computed on the device; fnetoc = NULL: the flux that
+ * oqg_compute_forcing last computed on the device (zero before the first). */
 int oqg_ocean_forcing(oqg_oml *m, const double *taux, const double *tauy,
                       const double *fnetoc, int compute_ent, double tdto);
 /* The handle's forcing, wekp (nxp, nyp) and ent (nxp, nyp, nl-1), copied
@@ -347,9 +348,10 @@ int oqg_get_forcing(oqg_handle *h, double *wekp, double *ent);
  *   step_aml, compute_new_aml,
  *   compute_atmos_entrainment               src/mixed/amlsubs.F90:184-326
  *   the atmosphere step's exchange          src/driver.F90:113-143
- * The radiation scheme that supplies fnetat (compute_forcing) and the
- * entrainment coefficients (init_entrain_coeff, set_xc1ast) stays with the
- * caller: its results are passed in. */
+ * The radiation scheme's start-up (radiat, radsubs.F90:116-157) and the
+ * entrainment coefficients (init_entrain_coeff, set_xc1ast) stay with the
+ * caller: their results are passed in.  The per-step fluxes (compute_forcing)
+ * and both basins' stress (xforc) run on the device, below. */
 typedef struct oqg_aml oqg_aml;
 
 /* init_atmos_ml (amlsubs.F90:61-98) and the coefficients it derives. */
@@ -383,25 +385,58 @@ int oqg_aml_get_state(oqg_aml *m, double *ast, double *astm, double *hmixa,
  * with the handle's current p(:,:,1), eta from its lagged pressure
  * (pm_k - pm_{k+1}) / gp_k, and the net heat flux fnetat (nxt, nyt).  The
  * handle's wekp, txis, txin become the Ekman forcing; when compute_ent, its
- * ent becomes the layer 1/2 entrainment (other layers zero).  With taux and
- * tauy both NULL the stress is the atmosphere's own, from its lagged layer-1
- * pressure by the quadratic drag law of xforc (windstress.F90:102-148, the
- * case without the ocean-velocity dependence), computed on the device. */
+ * ent becomes the layer 1/2 entrainment (other layers zero).  taux = tauy =
+ * NULL: the stress that oqg_xforc last computed on the device; fnetat = NULL:
+ * the flux that oqg_compute_forcing last computed (zero before the first). */
 int oqg_atmos_forcing(oqg_aml *m, const double *taux, const double *tauy,
                       const double *fnetat, int compute_ent, double tdta);
 
-/* Couples an ocean mixed layer to an atmospheric one (NULL unlinks): from
- * then on oqg_ocean_forcing with taux and tauy both NULL takes the ocean's
- * stress from the atmosphere's lagged layer-1 pressure, on the device
- * (compute_windstress, atmos_geos_vel, atmos_windstress; windstress.F90:
- * 150-314, the case without the ocean-velocity dependence): the atmospheric
- * geostrophic velocity and its derivatives over the ocean, interpolated
- * bicubically to the ocean's p points (bicubic.F90), the drag law with the
- * atmosphere's cdat and hm, times raoro = rho_atmosphere / rho_ocean.  The
- * ocean grid must hold whole atmospheric cells (load_grid, grid.F90:36-59);
- * the ocean sits at the channel's western end, centred in y.  The two
- * handles' streams are ordered around the read of the pressure. */
+/* Couples an ocean mixed layer to an atmospheric one (NULL unlinks), for
+ * oqg_xforc and oqg_compute_forcing below: raoro = rho_atmosphere /
+ * rho_ocean.  The ocean grid must hold whole atmospheric cells (load_grid,
+ * grid.F90:36-59); the ocean sits at the channel's western end (nx1 = 1),
+ * centred in y.  The atmosphere must outlive the link. */
 int oqg_oml_couple(oqg_oml *m, oqg_aml *a, double raoro);
+
+/* Both basins' wind stress from the atmosphere's lagged layer-1 pressure, on
+ * the device, held for the forcing calls that follow with NULL stresses
+ * (xforc, windstress.F90:102-148, the case without the ocean-velocity
+ * dependence; the reference calls it at each ocean step, driver.F90:47-54):
+ * the atmosphere's by the quadratic drag law at its p points; the ocean's,
+ * when o is given (coupled to a), from the atmospheric geostrophic velocity
+ * and its derivatives over the ocean interpolated bicubically to the ocean's
+ * p points (compute_windstress, atmos_geos_vel, atmos_windstress;
+ * windstress.F90:150-314, bicubic.F90) with the atmosphere's cdat and hm,
+ * times raoro.  The two handles' streams are ordered around the read of the
+ * pressure (CUDA events). */
+int oqg_xforc(oqg_aml *a, oqg_oml *o);
+
+/* The radiation coefficients compute_forcing reads (radiate_type,
+ * radsubs.F90:15-54), the derived values radiat computes at start-up. */
+typedef struct oqg_rad_coeffs {
+    double fspco;      /* signed perturbation forcing amplitude (W m^-2)     */
+    double xlamda;     /* sensible + latent transfer coefficient (W m^-2 K^-1) */
+    double d0up;       /* D0up: ocean mixed-layer upward radiation per K     */
+    double dmdown;     /* Dmdown: atmospheric mixed-layer downward, per K    */
+    double dup0;       /* Dup(0): atmospheric mixed-layer upward, per K      */
+    double aup00;      /* Aup(0,0)                                           */
+    double adown10;    /* Adown(1,0)                                         */
+    double adown11;    /* Adown(1,1)                                         */
+} oqg_rad_coeffs;
+
+/* The net diabatic forcing of both mixed layers on the device, from the
+ * lagged sst, the atmosphere's lagged temperature and height, eta_1 of its
+ * lagged pressure and its topography (compute_forcing, forcing.F90:18-99;
+ * the reference calls it at each ocean step before step_aml, driver.F90:
+ * 133-137): the atmospheric temperature interpolated bilinearly to the
+ * ocean's T points (bilint, numerics.F90:528-589), the ocean's flux and the
+ * atmosphere's with the ocean cells' upward fluxes summed into the
+ * atmospheric cells above them.  Held for the forcing calls that follow
+ * with NULL fluxes.  o must be coupled (oqg_oml_couple). */
+int oqg_compute_forcing(oqg_oml *o, const oqg_rad_coeffs *rad);
+/* The fluxes held on the device, fnetoc (nxt, nyt) of the ocean and fnetat
+ * (nxt, nyt) of the coupled atmosphere, copied out (either may be NULL). */
+int oqg_get_fluxes(oqg_oml *o, double *fnetoc, double *fnetat);
 
 /* ---------------------------------------------------------------------
  * State slots and the adjoint step.  The reference has no adjoint (its model

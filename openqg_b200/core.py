@@ -20,7 +20,7 @@ from typing import Optional
 
 import numpy as np
 
-from .params import Basin, OqgAmlParams, OqgOmlParams, QgMonitor, STATUS
+from .params import Basin, OqgAmlParams, OqgOmlParams, OqgRadCoeffs, QgMonitor, STATUS
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "liboqg.so")
@@ -94,6 +94,9 @@ def lib():
     L.oqg_ocean_forcing.argtypes = [vp, vp, vp, vp, ctypes.c_int, ctypes.c_double]
     L.oqg_get_forcing.argtypes = [vp, _dp, _dp]
     L.oqg_oml_couple.argtypes = [vp, vp, ctypes.c_double]
+    L.oqg_xforc.argtypes = [vp, vp]
+    L.oqg_compute_forcing.argtypes = [vp, ctypes.POINTER(OqgRadCoeffs)]
+    L.oqg_get_fluxes.argtypes = [vp, vp, vp]
     L.oqg_aml_create.argtypes = [vp, ctypes.POINTER(OqgAmlParams), vp, vp, ctypes.POINTER(vp)]
     L.oqg_aml_destroy.argtypes = [vp]
     L.oqg_aml_set_state.argtypes = [vp, vp, vp, vp, vp]
@@ -461,22 +464,43 @@ class OceanMixedLayer:
         return a, am
 
     def couple(self, aml, raoro: float):
-        """Takes the ocean's stress from the atmospheric mixed layer's handle
-        when forcing() gets no stress (oqg_oml_couple); aml None unlinks."""
+        """Links the atmospheric mixed layer for xforc() and
+        compute_forcing() (oqg_oml_couple); aml None unlinks."""
         _check(lib().oqg_oml_couple(self.h, None if aml is None else aml.h, float(raoro)), "oqg_oml_couple")
         self._aml = aml          # keeps the atmosphere alive while coupled
 
+    def compute_forcing(self, rad: OqgRadCoeffs):
+        """Both mixed layers' net heat fluxes on the device (compute_forcing,
+        forcing.F90:18-99), held for forcing() calls with fnet None."""
+        _check(lib().oqg_compute_forcing(self.h, ctypes.byref(rad)), "oqg_compute_forcing")
+
+    def get_fluxes(self):
+        """The held fluxes: fnetoc (nyt, nxt) and the atmosphere's fnetat."""
+        fo = np.empty(self.tshape)
+        fa = np.empty(self._aml.tshape)
+        _check(lib().oqg_get_fluxes(self.h, fo.ctypes.data, fa.ctypes.data), "oqg_get_fluxes")
+        return fo, fa
+
     def forcing(self, taux, tauy, fnetoc, compute_ent: bool, tdto: float):
-        """taux = tauy = None: the stress from the coupled atmosphere."""
+        """taux = tauy = None: the stress xforc() last computed; fnetoc None:
+        the flux compute_forcing() last computed."""
         b = self.qg.b
         if taux is None and tauy is None:
             tx = ty = None
         else:
             tx, ty = _f64(taux, b.shape2), _f64(tauy, b.shape2)
-        fn = _f64(fnetoc, self.tshape)
+        fn = None if fnetoc is None else _f64(fnetoc, self.tshape)
         _check(lib().oqg_ocean_forcing(self.h, None if tx is None else tx.ctypes.data,
-                                       None if ty is None else ty.ctypes.data, fn.ctypes.data, int(compute_ent),
-                                       float(tdto)), "oqg_ocean_forcing")
+                                       None if ty is None else ty.ctypes.data, None if fn is None else fn.ctypes.data,
+                                       int(compute_ent), float(tdto)), "oqg_ocean_forcing")
+
+
+def xforc(aml, oml=None):
+    """Both basins' wind stress from the atmosphere's lagged layer-1 pressure
+    on the device (xforc, windstress.F90:102-148), held for the forcing()
+    calls with no stress: the atmosphere's, and the ocean's through the
+    bicubic interpolation when oml (coupled to aml) is given."""
+    _check(lib().oqg_xforc(aml.h, None if oml is None else oml.h), "oqg_xforc")
 
 
 def get_forcing(qg: QG):
@@ -534,14 +558,14 @@ class AtmosMixedLayer:
         return a
 
     def forcing(self, taux, tauy, fnetat, compute_ent: bool, tdta: float):
-        """taux = tauy = None: the stress from the atmosphere's own lagged
-        pressure (xforc's drag law, computed on the device)."""
+        """taux = tauy = None: the stress xforc() last computed on the
+        device; fnetat None: the flux compute_forcing() last computed."""
         b = self.qg.b
         if taux is None and tauy is None:
             tx = ty = None
         else:
             tx, ty = _f64(taux, b.shape2), _f64(tauy, b.shape2)
-        fn = _f64(fnetat, self.tshape)
+        fn = None if fnetat is None else _f64(fnetat, self.tshape)
         _check(lib().oqg_atmos_forcing(self.h, None if tx is None else tx.ctypes.data,
-                                       None if ty is None else ty.ctypes.data, fn.ctypes.data, int(compute_ent),
-                                       float(tdta)), "oqg_atmos_forcing")
+                                       None if ty is None else ty.ctypes.data, None if fn is None else fn.ctypes.data,
+                                       int(compute_ent), float(tdta)), "oqg_atmos_forcing")

@@ -1885,6 +1885,7 @@ struct oqg_oml {
     std::vector<void *> allocs;
     OmlDev o{};
     oqg_handle *ha = nullptr;             // the coupled atmosphere's handle (oqg_oml_couple)
+    oqg_aml *am = nullptr;                // and its mixed layer
     TauCpl cpl{};
     cudaEvent_t ev_a = nullptr, ev_o = nullptr;
 };
@@ -1967,9 +1968,8 @@ int oqg_oml_get_sst(oqg_oml *m, double *sst, double *sstm) {
 
 int oqg_ocean_forcing(oqg_oml *m, const double *taux, const double *tauy, const double *fnetoc, int compute_ent,
                       double tdto) {
-    if (!m || !fnetoc || (!taux) != (!tauy)) return fail(OQG_EINVAL, "null argument");
+    if (!m || (!taux) != (!tauy)) return fail(OQG_EINVAL, "null argument");
     if (!(tdto > 0.0)) return fail(OQG_EINVAL, "tdto must be > 0");
-    if (!taux && !m->ha) return fail(OQG_EINVAL, "no stress given and no atmosphere coupled (oqg_oml_couple)");
     oqg_handle *h = m->h;
     BasinDev &b = h->hb;
     OmlDev &o = m->o;
@@ -1984,25 +1984,9 @@ int oqg_ocean_forcing(oqg_oml *m, const double *taux, const double *tauy, const 
         CK(cudaMemcpyAsync(const_cast<double *>(o.taux), taux, np * sizeof(double), cudaMemcpyDefault, h->st));
         CK(cudaMemcpyAsync(const_cast<double *>(o.tauy), tauy, np * sizeof(double), cudaMemcpyDefault, h->st));
     }
-    CK(cudaMemcpyAsync(const_cast<double *>(o.fnet), fnetoc, nt * sizeof(double), cudaMemcpyDefault, h->st));
+    if (fnetoc)
+        CK(cudaMemcpyAsync(const_cast<double *>(o.fnet), fnetoc, nt * sizeof(double), cudaMemcpyDefault, h->st));
     CK(cudaEventRecord(h->up_ev, h->st));
-    if (!taux) {
-        // the stress from the coupled atmosphere's lagged layer-1 pressure: this
-        // stream waits for the atmosphere's queued work, and the atmosphere's
-        // stream waits until the pressure has been read
-        oqg_handle *ha = m->ha;
-        CK(cudaEventRecord(m->ev_a, ha->st));
-        CK(cudaStreamWaitEvent(h->st, m->ev_a, 0));
-        const void *pma = ha->hb.F[1 - ha->par];
-        const int nsub = (m->cpl.nxtoar + 1) * (m->cpl.nytoar + 1);
-        const int gs = std::min((nsub + 255) / 256, 148 * 4);
-        if (ha->mixed) k_cpl_derivs<float><<<gs, 256, 0, h->st>>>(m->cpl, (const float *)pma);
-        else k_cpl_derivs<double><<<gs, 256, 0, h->st>>>(m->cpl, (const double *)pma);
-        CK(cudaEventRecord(m->ev_o, h->st));
-        CK(cudaStreamWaitEvent(ha->st, m->ev_o, 0));
-        const int gt = std::min((int)((np + 255) / 256), 148 * 8);
-        k_cpl_tau<<<gt, 256, 0, h->st>>>(m->cpl, o);
-    }
     const void *p1 = b.F[h->par];   // layer 1 of the current p (driver.F90:96-103)
     if (h->mixed) k_oml_step<float><<<OQG_OML_CTAS, 256, 0, h->st>>>(o, (const float *)p1, b.px, tdto, compute_ent);
     else k_oml_step<double><<<OQG_OML_CTAS, 256, 0, h->st>>>(o, (const double *)p1, b.px, tdto, compute_ent);
@@ -2320,7 +2304,7 @@ int oqg_aml_get_state(oqg_aml *m, double *ast, double *astm, double *hmixa, doub
 
 int oqg_atmos_forcing(oqg_aml *m, const double *taux, const double *tauy, const double *fnetat, int compute_ent,
                       double tdta) {
-    if (!m || !fnetat || (!taux) != (!tauy)) return fail(OQG_EINVAL, "null argument");
+    if (!m || (!taux) != (!tauy)) return fail(OQG_EINVAL, "null argument");
     if (!(tdta > 0.0)) return fail(OQG_EINVAL, "tdta must be > 0");
     oqg_handle *h = m->h;
     BasinDev &b = h->hb;
@@ -2337,17 +2321,9 @@ int oqg_atmos_forcing(oqg_aml *m, const double *taux, const double *tauy, const 
         CK(cudaMemcpyAsync(const_cast<double *>(o.taux), taux, np * sizeof(double), cudaMemcpyDefault, h->st));
         CK(cudaMemcpyAsync(const_cast<double *>(o.tauy), tauy, np * sizeof(double), cudaMemcpyDefault, h->st));
     }
-    CK(cudaMemcpyAsync(const_cast<double *>(o.fnet), fnetat, nt * sizeof(double), cudaMemcpyDefault, h->st));
+    if (fnetat)
+        CK(cudaMemcpyAsync(const_cast<double *>(o.fnet), fnetat, nt * sizeof(double), cudaMemcpyDefault, h->st));
     CK(cudaEventRecord(h->up_ev, h->st));
-    if (!taux) {   // the stress from the atmosphere's own lagged pressure (xforc)
-        const int gp = std::min((int)((np + 255) / 256), 148 * 8);
-        if (h->mixed)
-            k_aml_tau<float><<<gp, 256, 0, h->st>>>(h->d_bas, o, (const float *)pm, const_cast<double *>(o.taux),
-                                                    const_cast<double *>(o.tauy));
-        else
-            k_aml_tau<double><<<gp, 256, 0, h->st>>>(h->d_bas, o, (const double *)pm, const_cast<double *>(o.taux),
-                                                     const_cast<double *>(o.tauy));
-    }
     const int grid = std::min((int)((nt + 255) / 256), 148 * 8);
     if (h->mixed) {
         k_aml_step<float><<<grid, 256, 0, h->st>>>(o, (const float *)p1, b.px, tdta, compute_ent);
@@ -2387,6 +2363,7 @@ int oqg_oml_couple(oqg_oml *m, oqg_aml *a, double raoro) {
     if (!m) return fail(OQG_EINVAL, "null argument");
     if (!a) {
         m->ha = nullptr;
+        m->am = nullptr;
         return OQG_OK;
     }
     const BasinDev &bo = m->h->hb, &ba = a->h->hb;
@@ -2415,6 +2392,83 @@ int oqg_oml_couple(oqg_oml *m, oqg_aml *a, double raoro) {
     c.fxa = ba.fx; c.fya = ba.fy; c.fyb = ba.fy_bc;
     c.cdat = a->o.cdat; c.hma = a->o.hm; c.raoro = raoro;
     m->ha = a->h;
+    m->am = a;
+    return OQG_OK;
+}
+
+int oqg_xforc(oqg_aml *a, oqg_oml *m) {
+    if (!a) return fail(OQG_EINVAL, "null argument");
+    if (m && m->am != a) return fail(OQG_EINVAL, "the ocean mixed layer is not coupled to this atmosphere");
+    oqg_handle *ha = a->h;
+    const AmlDev &ao = a->o;
+    const void *pma = ha->hb.F[1 - ha->par];   // the lagged pressure (driver.F90:47-54, before step_atm)
+    const int npa = ao.nxp * ao.nyp;
+    const int gp = std::min((npa + 255) / 256, 148 * 8);
+    if (ha->mixed)
+        k_aml_tau<float><<<gp, 256, 0, ha->st>>>(ha->d_bas, ao, (const float *)pma, const_cast<double *>(ao.taux),
+                                                 const_cast<double *>(ao.tauy));
+    else
+        k_aml_tau<double><<<gp, 256, 0, ha->st>>>(ha->d_bas, ao, (const double *)pma, const_cast<double *>(ao.taux),
+                                                  const_cast<double *>(ao.tauy));
+    CK(cudaGetLastError());
+    if (!m) return OQG_OK;
+    // the ocean's stress: its stream waits for the atmosphere's queued work,
+    // and the atmosphere's stream waits until the pressure has been read
+    oqg_handle *h = m->h;
+    CK(cudaEventRecord(m->ev_a, ha->st));
+    CK(cudaStreamWaitEvent(h->st, m->ev_a, 0));
+    const int nsub = (m->cpl.nxtoar + 1) * (m->cpl.nytoar + 1);
+    const int gs = std::min((nsub + 255) / 256, 148 * 4);
+    if (ha->mixed) k_cpl_derivs<float><<<gs, 256, 0, h->st>>>(m->cpl, (const float *)pma);
+    else k_cpl_derivs<double><<<gs, 256, 0, h->st>>>(m->cpl, (const double *)pma);
+    CK(cudaEventRecord(m->ev_o, h->st));
+    CK(cudaStreamWaitEvent(ha->st, m->ev_o, 0));
+    const int npo = m->o.nxp * m->o.nyp;
+    const int gt = std::min((npo + 255) / 256, 148 * 8);
+    k_cpl_tau<<<gt, 256, 0, h->st>>>(m->cpl, m->o);
+    CK(cudaGetLastError());
+    return OQG_OK;
+}
+
+int oqg_compute_forcing(oqg_oml *m, const oqg_rad_coeffs *rad) {
+    if (!m || !rad) return fail(OQG_EINVAL, "null argument");
+    if (!m->am) return fail(OQG_EINVAL, "no atmosphere coupled (oqg_oml_couple)");
+    oqg_handle *h = m->h, *ha = m->ha;
+    const AmlDev &ao = m->am->o;
+    if (ao.nl < 2) return fail(OQG_EUNSUPPORTED, "compute_forcing needs an atmosphere of two or more layers (eta_1)");
+    const RadFlux r{rad->fspco, rad->xlamda, rad->d0up, rad->dmdown, rad->dup0, rad->aup00, rad->adown10,
+                    rad->adown11};
+    // on the ocean's stream, after the atmosphere's queued work; the
+    // atmosphere's stream waits for the fluxes (its next step reads fnetat)
+    CK(cudaEventRecord(m->ev_a, ha->st));
+    CK(cudaStreamWaitEvent(h->st, m->ev_a, 0));
+    const void *pma = ha->hb.F[1 - ha->par];
+    const int n = m->o.nxt * m->o.nyt + ao.nxt * ao.nyt;
+    const int gs = std::min((n + 255) / 256, 148 * 8);
+    if (ha->mixed) k_cpl_fluxes<float><<<gs, 256, 0, h->st>>>(m->cpl, r, m->o, ao, (const float *)pma, ha->hb.px);
+    else k_cpl_fluxes<double><<<gs, 256, 0, h->st>>>(m->cpl, r, m->o, ao, (const double *)pma, ha->hb.px);
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(m->ev_o, h->st));
+    CK(cudaStreamWaitEvent(ha->st, m->ev_o, 0));
+    return OQG_OK;
+}
+
+int oqg_get_fluxes(oqg_oml *m, double *fnetoc, double *fnetat) {
+    if (!m) return fail(OQG_EINVAL, "null argument");
+    if (fnetat && !m->am) return fail(OQG_EINVAL, "no atmosphere coupled (oqg_oml_couple)");
+    oqg_handle *h = m->h;
+    if (m->am) {
+        CK(cudaEventRecord(m->ev_a, m->ha->st));
+        CK(cudaStreamWaitEvent(h->st, m->ev_a, 0));
+    }
+    if (fnetoc)
+        CK(cudaMemcpyAsync(fnetoc, m->o.fnet, (size_t)m->o.nxt * m->o.nyt * sizeof(double), cudaMemcpyDefault,
+                           h->st));
+    if (fnetat) {
+        const AmlDev &ao = m->am->o;
+        CK(cudaMemcpyAsync(fnetat, ao.fnet, (size_t)ao.nxt * ao.nyt * sizeof(double), cudaMemcpyDefault, h->st));
+    }
+    CK(cudaStreamSynchronize(h->st));
     return OQG_OK;
 }
 

@@ -498,4 +498,88 @@ __global__ void __launch_bounds__(128) k_aml_strips(AmlDev o, DevForcing *frc) {
     }
 }
 
+// ------------------------------------------------------ the coupled fluxes
+// compute_forcing's radiation coefficients (radiate_type, radsubs.F90:15-54).
+struct RadFlux {
+    double fspco, xlamda, d0up, dmdown, dup0, aup00, adown10, adown11;
+};
+
+// bilint (numerics.F90:528-589) of the atmospheric T field at at ocean T
+// point (io, jo), 0-based: the ocean's T points from its origin (c0 dxa,
+// r0 dya), the atmosphere's at ((i - 1/2) dxa, (j - 1/2) dya) for 1-based
+// (i, j); cyclic in x, the first and last T rows held beyond the channel's
+// ends.  Indexes stay 1-based and truncate like Fortran's int, as there.
+__device__ __forceinline__ double cpl_bilint(const TauCpl &c, const OmlDev &o, const AmlDev &a, const double *at,
+                                             int io, int jo) {
+    const double dxainv = 1.0 / a.dx, dyainv = 1.0 / a.dy;
+    const double xta1 = 0.5 * a.dx, yta1 = 0.5 * a.dy;
+    const double xto = (c.c0 * a.dx + io * o.dx) + 0.5 * o.dx;
+    int iam = (int)(1.0 + dxainv * (xto - xta1));
+    int iap = iam + 1;
+    const double xam = iam >= 1 ? (iam - 1) * a.dx + xta1 : xta1 - a.dx;
+    const double wpx = dxainv * (xto - xam), wmx = 1.0 - wpx;
+    iam = 1 + (iam + a.nxt - 1) % a.nxt;
+    iap = 1 + (iap + a.nxt - 1) % a.nxt;
+    const double yto = (c.r0 * a.dy + jo * o.dy) + 0.5 * o.dy;
+    int jam = (int)(1.0 + dyainv * (yto - yta1));
+    int jap = jam + 1;
+    jam = min(max(jam, 1), a.nyt);
+    jap = min(jap, a.nyt);
+    const double wpy = dyainv * (yto - ((jam - 1) * a.dy + yta1)), wmy = 1.0 - wpy;
+    const double *rm = at + (size_t)(jam - 1) * a.nxt, *rp = at + (size_t)(jap - 1) * a.nxt;
+    return wmx * wmy * rm[iam - 1] + wpx * wmy * rm[iap - 1] + wmx * wpy * rp[iam - 1] + wpx * wpy * rp[iap - 1];
+}
+
+// compute_forcing (forcing.F90:18-99): the ocean's net flux at its T points
+// and the atmosphere's at its own, one thread per cell of either grid.  An
+// atmospheric cell over the ocean sums its ndxr x ndxr ocean cells' upward
+// fluxes in the reference's order (rows, then columns), recomputing their
+// interpolated temperature.  PM is the atmosphere's lagged pressure (eta_1 =
+// (pm_1 - pm_2) / gp_1 at its p points).
+template <class T>
+__global__ void __launch_bounds__(256) k_cpl_fluxes(TauCpl c, RadFlux r, OmlDev o, AmlDev a,
+                                                    const T *__restrict__ PM, int px_a) {
+    const double pi = 3.141592653589793;
+    const int nto = o.nxt * o.nyt, nta = a.nxt * a.nyt, nd = c.ndxr;
+    const double yla = a.nyt * a.dy, ylo = o.nyt * o.dy;
+    const double ocfrac = o.dx * o.dy / (a.dx * a.dy);
+    double *fnetoc = const_cast<double *>(o.fnet), *fnetat = const_cast<double *>(a.fnet);
+    for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < nto + nta; idx += gridDim.x * blockDim.x) {
+        if (idx < nto) {
+            const int jo = idx / o.nxt, io = idx - jo * o.nxt;
+            const double asto = cpl_bilint(c, o, a, a.astm, io, jo);
+            const double sst = o.datam[idx];
+            const double fsp = r.fspco * 0.5 * sin(pi * ((-0.5 * ylo + jo * o.dy) + 0.5 * o.dy) / yla);
+            fnetoc[idx] = -fsp - r.dmdown * asto - r.d0up * sst - r.xlamda * (sst - asto);
+            continue;
+        }
+        const int k = idx - nto, ja = k / a.nxt, ia = k - ja * a.nxt;
+        const double ast = a.astm[k];
+        double f = -r.dup0 * ast - r.fspco * 0.5 * sin(pi * ((-0.5 * yla + ja * a.dy) + 0.5 * a.dy) / yla);
+        const int ci = ia - c.c0, cj = ja - c.r0;
+        if (ci >= 0 && ci < c.nxtoar && cj >= 0 && cj < c.nytoar) {
+            f = f + (r.dmdown - r.dup0) * ast;
+            for (int jo = cj * nd; jo < (cj + 1) * nd; ++jo)
+                for (int io = ci * nd; io < (ci + 1) * nd; ++io) {
+                    const double sst = o.datam[(size_t)jo * o.nxt + io];
+                    const double asto = cpl_bilint(c, o, a, a.astm, io, jo);
+                    f = f + ocfrac * (r.d0up * sst + r.xlamda * (sst - asto));
+                }
+        }
+        const size_t lay = (size_t)a.nyp * px_a;
+        auto eta = [&](int i, int j) {
+            const size_t q = (size_t)j * px_a + i;
+            return ((double)PM[q] - (double)PM[lay + q]) / a.gp[0];
+        };
+        const double me = (r.adown11 * 0.25) * (eta(ia, ja) + eta(ia + 1, ja) + eta(ia, ja + 1) + eta(ia + 1, ja + 1));
+        double mt = 0.0;
+        if (a.dtop) {
+            const double *d0 = a.dtop + (size_t)ja * a.nxp, *d1 = d0 + a.nxp;
+            mt = ((r.aup00 + r.adown10) * 0.25) * (d0[ia] + d0[ia + 1] + d1[ia] + d1[ia + 1]);
+        }
+        const double hmafac = -a.hmadmp - r.aup00 - r.adown10;
+        fnetat[k] = f - me - mt + hmafac * (a.hmxm[k] - a.hm);
+    }
+}
+
 }  // namespace oqg

@@ -59,6 +59,13 @@ class OqgAmlParams(ctypes.Structure):
         [("aface", ctypes.c_double * OQG_MAX_NL)]
 
 
+class OqgRadCoeffs(ctypes.Structure):
+    """ctypes mirror of `oqg_rad_coeffs` (include/oqg.h): the radiation
+    coefficients compute_forcing reads (radiate_type, radsubs.F90:15-54)."""
+    _fields_ = [(n, ctypes.c_double) for n in ("fspco", "xlamda", "d0up", "dmdown", "dup0", "aup00", "adown10",
+                                               "adown11")]
+
+
 class OqgParams(ctypes.Structure):
     """ctypes mirror of `oqg_params` (include/oqg.h)."""
     _fields_ = [

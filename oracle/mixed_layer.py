@@ -10,6 +10,7 @@ Follows, for a closed box (the ocean):
   map_T_to_x_face / y_face, c_grid_advection, dPdx, dPdy, map_T_to_P
                           src/glam/numerics.F90:64-107, 223-309, 392-408
   init_mixed              src/mixed/mixed.F90:73-99 (state starts at init_val)
+  compute_forcing, bilint src/mixed/forcing.F90:18-99, src/glam/numerics.F90:528-589
 
 Arrays are numpy C-order views of the Fortran ones: a Fortran (nx, ny) array
 is (ny, nx) here.  T-grid fields are (nyt, nxt) = (nyp-1, nxp-1).
@@ -416,3 +417,96 @@ def ocean_stress(pma1, ba, bo, cdat, hma, raoro):
     cuohf = (qpreaa * cdhfaa) * shrmag
     cdchi = (qpreaa * cdat) * shrmag / (1.0 + cuohf * cuohf)
     return raoro * (cdchi * (u - cuohf * v)), raoro * (cdchi * (v + cuohf * u))
+
+
+# ------------------------------------------------------------ coupled fluxes
+@dataclass
+class RadCoeffs:
+    """The radiation coefficients compute_forcing reads (radiate_type,
+    radsubs.F90:15-54), the derived values radiat computes at start-up."""
+    fspco: float
+    xlamda: float
+    d0up: float
+    dmdown: float
+    dup0: float
+    aup00: float
+    adown10: float
+    adown11: float
+
+
+def bilint(at, bo, ba):
+    """bilint (numerics.F90:528-589): the atmospheric T field at (nyt_a,
+    nxt_a) interpolated bilinearly to the ocean's T points.  The ocean's
+    origin is the atmospheric cell of coupling_grid; x is cyclic, and the
+    first and last T rows hold beyond the channel's ends.  Indexes stay
+    1-based and truncate like Fortran's int, as there."""
+    _, _, _, c0, r0 = coupling_grid(bo, ba)
+    nxta, nyta = ba.nxp - 1, ba.nyp - 1
+    nxto, nyto = bo.nxp - 1, bo.nyp - 1
+    dxainv, dyainv = 1.0 / ba.dx, 1.0 / ba.dy
+    xta1, yta1 = 0.5 * ba.dx, 0.5 * ba.dy
+    io = np.arange(nxto)
+    xto = (c0 * ba.dx + io * bo.dx) + 0.5 * bo.dx
+    iam = np.trunc(1.0 + dxainv * (xto - xta1)).astype(np.int64)
+    iap = iam + 1
+    xam = np.where(iam >= 1, (iam - 1) * ba.dx + xta1, xta1 - ba.dx)
+    wpx = dxainv * (xto - xam)
+    wmx = 1.0 - wpx
+    iam = 1 + np.mod(iam + nxta - 1, nxta)
+    iap = 1 + np.mod(iap + nxta - 1, nxta)
+    out = np.empty((nyto, nxto))
+    for jo in range(nyto):
+        yto = (r0 * ba.dy + jo * bo.dy) + 0.5 * bo.dy
+        jam = int(np.trunc(1.0 + dyainv * (yto - yta1)))
+        jap = jam + 1
+        jam = min(max(jam, 1), nyta)
+        jap = min(jap, nyta)
+        wpy = dyainv * (yto - ((jam - 1) * ba.dy + yta1))
+        wmy = 1.0 - wpy
+        rm, rp = at[jam - 1], at[jap - 1]
+        out[jo] = (wmx * wmy * rm[iam - 1] + wpx * wmy * rm[iap - 1]
+                   + wmx * wpy * rp[iam - 1] + wpx * wpy * rp[iap - 1])
+    return out
+
+
+def fsprim(fspco, yrel, yla):
+    """The perturbative radiative forcing (fsprim, radsubs.F90:97-114)."""
+    return fspco * 0.5 * np.sin(np.pi * yrel / yla)
+
+
+def compute_forcing(sstm, astm, hmxm, pma, ba, bo, rad: RadCoeffs, hma, hmadmp, dtop=None):
+    """compute_forcing (forcing.F90:18-99): the ocean's net flux fnetoc
+    (nyt_o, nxt_o) and the atmosphere's fnetat (nyt_a, nxt_a) from the lagged
+    sst, the atmosphere's lagged temperature astm and height hmxm, its lagged
+    pressure pma (nl, nyp, nxp) for eta_1 = (pm_1 - pm_2) / gp_1, and its
+    topography dtop (nyp, nxp) or None (flat)."""
+    ndxr, nxtoar, nytoar, c0, r0 = coupling_grid(bo, ba)
+    nxta, nyta = ba.nxp - 1, ba.nyp - 1
+    nxto, nyto = bo.nxp - 1, bo.nyp - 1
+    yla, ylo = nyta * ba.dy, nyto * bo.dy
+    asto = bilint(astm, bo, ba)
+    ocn_ir_up = rad.d0up * sstm
+    sense_lat = rad.xlamda * (sstm - asto)
+    aml_ir_down = rad.dmdown * asto
+    yta = (-0.5 * yla + np.arange(nyta) * ba.dy) + 0.5 * ba.dy
+    fnetat = -rad.dup0 * astm - fsprim(rad.fspco, yta, yla)[:, None]
+    over = (slice(r0, r0 + nytoar), slice(c0, c0 + nxtoar))
+    fnetat[over] = fnetat[over] + (rad.dmdown - rad.dup0) * astm[over]
+    yto = (-0.5 * ylo + np.arange(nyto) * bo.dy) + 0.5 * bo.dy
+    fsp = fsprim(rad.fspco, yto, yla)[:, None]
+    fnetoc = -fsp - aml_ir_down - ocn_ir_up - sense_lat
+    ocfrac = bo.dx * bo.dy / (ba.dx * ba.dy)
+    up = ocn_ir_up + sense_lat
+    for jo in range(nyto):
+        ja = r0 + jo // ndxr
+        for io in range(nxto):
+            ia = c0 + io // ndxr
+            fnetat[ja, ia] = fnetat[ja, ia] + ocfrac * up[jo, io]
+    eta = (pma[0] - pma[1]) / ba.gp[0]
+    p2t = lambda f, fac: (fac * 0.25) * (f[:-1, :-1] + f[:-1, 1:] + f[1:, :-1] + f[1:, 1:])
+    fmafac = rad.adown11
+    fmatop = rad.aup00 + rad.adown10
+    hmafac = -hmadmp - rad.aup00 - rad.adown10
+    top = p2t(dtop, fmatop) if dtop is not None else 0.0
+    fnetat = fnetat - p2t(eta, fmafac) - top + hmafac * (hmxm - hma)
+    return fnetoc, fnetat

@@ -131,6 +131,15 @@ def test_added_entry_points_reject_null_arguments(liboqg):
     assert L.oqg_aml_get_state(None, None, None, None, None) == 1
     assert L.oqg_atmos_forcing(None, None, None, None, 1, ctypes.c_double(1.0)) == 1
     assert L.oqg_oml_couple(None, None, ctypes.c_double(1.2e-3)) == 1
+    assert L.oqg_xforc(None, None) == 1
+    assert L.oqg_compute_forcing(None, None) == 1
+    assert L.oqg_get_fluxes(None, None, None) == 1
+
+
+def test_rad_coeffs_struct_layout_matches_header():
+    from openqg_b200.params import OqgRadCoeffs
+    assert ctypes.sizeof(OqgRadCoeffs) == 8 * 8
+    assert OqgRadCoeffs.adown11.offset == 7 * 8
 
 
 def test_aml_params_struct_layout_matches_header():

@@ -130,7 +130,9 @@ def test_rejected_setups():
 
 # ---------------------------------------------------------------- atmosphere
 from oracle.mixed_layer import AmlOracle, AmlParams, atmos_stress, ekman_cyclic, ocean_stress  # noqa: E402
-from openqg_b200.core import AtmosMixedLayer  # noqa: E402
+from oracle.mixed_layer import RadCoeffs, compute_forcing  # noqa: E402
+from openqg_b200.core import AtmosMixedLayer, xforc  # noqa: E402
+from openqg_b200.params import OqgRadCoeffs  # noqa: E402
 
 TDTA = 360.0
 
@@ -221,8 +223,8 @@ def test_atmos_rejects_a_box():
 
 
 def test_atmos_forcing_with_its_own_stress():
-    """taux = tauy = None: the stress comes from the atmosphere's lagged
-    layer-1 pressure by xforc's drag law, on the device."""
+    """taux = tauy = None: the stress that xforc computed on the device
+    from the atmosphere's lagged layer-1 pressure by the drag law."""
     b, prm, g, m, o, _, _, fnet, _ = _atmos_setup(seed=8)
     ent = np.zeros((b.nl - 1,) + b.shape2)
     g.step(TDTA, 2)                          # a lagged pressure unlike the current one
@@ -230,6 +232,7 @@ def test_atmos_forcing_with_its_own_stress():
         p, pm, _, _ = g.get_state()
         taux, tauy = atmos_stress(pm[0], b, 1.3e-3, prm.hm)
         uek, vek, wekt, wekp, _, _ = ekman_cyclic(taux, tauy, b.dx, b.dy, b.fnot, prm.hm)
+        xforc(m)
         m.forcing(None, None, fnet, ce, TDTA)
         o.step(p[0], uek, vek, wekt, _eta(b, pm), fnet, ce, TDTA, ent)
         assert rel_l2(m.get_state()[0], o.ast) <= 1e-12
@@ -243,9 +246,9 @@ def test_atmos_forcing_with_its_own_stress():
 
 def test_ocean_stress_from_the_coupled_atmosphere():
     """The ocean (129x129 at 10 km) coupled to an atmosphere channel (49x25 at
-    80 km): with no stress given, the ocean's stress comes from the
+    80 km): the ocean's stress from xforc, computed on the device from the
     atmosphere's lagged layer-1 pressure through the bicubic interpolation
-    and the drag law, on the device."""
+    and the drag law."""
     ba = atmos_channel(49, 25, dx=80e3)
     ga = QG(ba)
     pa = ba.fnot * 30.0 * initial_psi(ba, seed=3)
@@ -279,6 +282,7 @@ def test_ocean_stress_from_the_coupled_atmosphere():
         taux, tauy = ocean_stress(pma, ba, b, 1.3e-3, aprm.hm, 1.2e-3)
         uek, vek, wekt, wekp = ekman(taux, tauy, b.dx, b.dy, b.fnot, prm.hm)
         p1 = g.get_state()[0][0]
+        xforc(aml, m)
         m.forcing(None, None, fnet, True, TDT)
         o.step(p1, uek, vek, wekt, fnet, True, TDT, ent)
         w, e = get_forcing(g)
@@ -290,3 +294,146 @@ def test_ocean_stress_from_the_coupled_atmosphere():
         ga.step(TDTA, 1)
     for x in (m, aml, g, ga):
         x.close()
+
+
+RAD = RadCoeffs(fspco=80.0, xlamda=35.0, d0up=5.5, dmdown=3.5, dup0=2.5, aup00=-0.03, adown10=0.02, adown11=0.01)
+
+
+def _rad_c():
+    return OqgRadCoeffs(*[getattr(RAD, f) for f, _ in OqgRadCoeffs._fields_])
+
+
+def _coupled_pair(seed, topography=True):
+    """An ocean box (129x129 at 10 km) under an atmosphere channel (49x25 at
+    80 km), both mixed layers coupled, lagged states unlike the current
+    ones; the channel's QG state stepped three times on the device and by
+    the C++ oracle alike."""
+    rng = np.random.default_rng(seed)
+    ba = atmos_channel(49, 25, dx=80e3)
+    ga, qa = QG(ba), oracle.Oracle(ba)
+    pa = ba.fnot * 30.0 * initial_psi(ba, seed=seed)
+    ga.set_state(pa, pa)
+    qa.set_state(pa, pa)
+    y = np.arange(ba.nyp) * ba.dy
+    txa = np.repeat((0.05 * np.sin(np.pi * y / y[-1]))[:, None], ba.nxp, axis=1)
+    w, ts, tn = oracle.ekman_from_tau(ba, txa, np.zeros_like(txa))
+    ga.set_forcing(w, None, ts, tn)
+    qa.set_forcing(w, np.zeros((ba.nl - 1,) + ba.shape2), ts, tn)
+    ga.step(TDTA, 3)
+    qa.step(TDTA, 3)
+    aprm = AmlParams(aface=(1e-7, -1e-7), bface=1e-7, dface=1e-6)
+    nyta, nxta = ba.nyp - 1, ba.nxp - 1
+    dtop = None
+    if topography:
+        dtop = 50.0 * rng.standard_normal(ba.shape2)
+        dtop[:, -1] = dtop[:, 0]
+    aml = AtmosMixedLayer(ga, np.zeros((nyta, nxta)), dtop, hm=aprm.hm, rho_cp=aprm.rho_cp, t1_rel=aprm.t1_rel,
+                          dt_12=aprm.dt_12, hmamin=aprm.hmamin, hmadmp=aprm.hmadmp, xcexp=aprm.xcexp,
+                          at2d=aprm.at2d, at4d=aprm.at4d, ahmd=aprm.ahmd, aface=aprm.aface, bface=aprm.bface,
+                          dface=aprm.dface, cdat=1.3e-3)
+    ya = np.linspace(0.0, 1.0, nyta)[:, None]
+    ast = -8.0 + 2.0 * np.cos(np.pi * ya) + 0.3 * rng.standard_normal((nyta, nxta))
+    astm = ast + 0.05 * rng.standard_normal((nyta, nxta))
+    hmx = aprm.hm + 50.0 * rng.standard_normal((nyta, nxta))
+    hmxm = hmx + 5.0 * rng.standard_normal((nyta, nxta))
+    aml.set_state(ast, astm, hmx, hmxm)
+    oa = AmlOracle(ba, aprm, np.zeros((nyta, nxta)), dtop if dtop is not None else np.zeros(ba.shape2))
+    oa.ast, oa.astm, oa.hmx, oa.hmxm = ast.copy(), astm.copy(), hmx.copy(), hmxm.copy()
+    prm = OmlParams(hm=100.0, rho_cp=4.0e6, t1_rel=10.0, dt_12=5.0, st2d=2.0e3, st4d=1.0e11, ycexp=1.0)
+    b = ocean_double_gyre(129, dx=10.0e3)
+    g, qo = QG(b), oracle.Oracle(b)
+    p = b.fnot * initial_psi(b, seed=seed + 1)
+    g.set_state(p, p)
+    qo.set_state(p, p)
+    m = OceanMixedLayer(g, prm.hm, prm.rho_cp, prm.t1_rel, prm.dt_12, prm.st2d, prm.st4d, prm.ycexp,
+                        prm.fluxn, prm.fluxs, prm.nval, prm.sval)
+    nyt, nxt = b.nyp - 1, b.nxp - 1
+    yo = np.linspace(0.0, 1.0, nyt)[:, None]
+    sst = 12.0 + 3.0 * np.cos(np.pi * yo) + 0.3 * rng.standard_normal((nyt, nxt))
+    sstm = sst + 0.05 * rng.standard_normal((nyt, nxt))
+    m.set_sst(sst, sstm)
+    oo = OmlOracle(b, prm)
+    oo.data, oo.datam = sst.copy(), sstm.copy()
+    m.couple(aml, 1.2e-3)
+    return dict(ba=ba, ga=ga, qa=qa, aml=aml, oa=oa, aprm=aprm, dtop=dtop,
+                b=b, g=g, qo=qo, m=m, oo=oo, prm=prm)
+
+
+@pytest.mark.parametrize("topography", [True, False])
+def test_coupled_fluxes_match_oracle(topography):
+    """compute_forcing on the device: both mixed layers' net heat fluxes
+    against the restatement, before and after the atmosphere steps."""
+    c = _coupled_pair(seed=11, topography=topography)
+    ba, b, m, aml, ga = c["ba"], c["b"], c["m"], c["aml"], c["ga"]
+    for it in range(2):
+        m.compute_forcing(_rad_c())
+        fo, fa = m.get_fluxes()
+        _, astm, _, hmxm = aml.get_state()
+        sstm = m.get_sst()[1]
+        pma = ga.get_state()[1]
+        ro, ra = compute_forcing(sstm, astm, hmxm, pma, ba, b, RAD, c["aprm"].hm, c["aprm"].hmadmp, c["dtop"])
+        assert rel_l2(fo, ro) <= 1e-12, it
+        assert rel_l2(fa, ra) <= 1e-12, it
+        xforc(aml, m)
+        aml.forcing(None, None, None, True, TDTA)
+        ga.step(TDTA, 1)
+    for k in ("m", "aml", "g", "ga"):
+        c[k].close()
+
+
+def test_coupled_exchange_matches_oracle():
+    """Three ocean steps of the coupled driver (driver.F90:33-143) with two
+    atmosphere steps each, every exchange on the device: xforc (both
+    stresses), compute_forcing (both fluxes), the mixed layers and QG steps
+    of both basins; against the restatements and the C++ oracle's QG
+    steps."""
+    c = _coupled_pair(seed=13)
+    ba, b, aprm, prm = c["ba"], c["b"], c["aprm"], c["prm"]
+    ga, qa, aml, oa, g, qo, m, oo = (c[k] for k in ("ga", "qa", "aml", "oa", "g", "qo", "m", "oo"))
+    enta = np.zeros((ba.nl - 1,) + ba.shape2)
+    ento = np.zeros((b.nl - 1,) + b.shape2)
+    nstr = 2
+    for _ in range(3):
+        # the oracle's ocean step
+        pma = qa.get_state()[1]
+        tax, tay = atmos_stress(pma[0], ba, 1.3e-3, aprm.hm)
+        tox, toy = ocean_stress(pma[0], ba, b, 1.3e-3, aprm.hm, 1.2e-3)
+        fo, fa = compute_forcing(oo.datam, oa.astm, oa.hmxm, pma, ba, b, RAD, aprm.hm, aprm.hmadmp, c["dtop"])
+        ua, va, wta, wpa, tsa, tna = ekman_cyclic(tax, tay, ba.dx, ba.dy, ba.fnot, aprm.hm)
+        uo, vo, wto, wpo = ekman(tox, toy, b.dx, b.dy, b.fnot, prm.hm)
+        for s in range(nstr):
+            p, pm = qa.get_state()[:2]
+            oa.step(p[0], ua, va, wta, _eta(ba, pm), fa, True, TDTA, enta)
+            qa.set_forcing(wpa, enta, tsa, tna)
+            qa.step(TDTA, 1)
+            if s == 0:
+                oo.step(qo.get_state()[0][0], uo, vo, wto, fo, True, TDT, ento)
+                qo.set_forcing(wpo, ento, 0.0, 0.0)
+                qo.step(TDT, 1)
+        # the same on the device
+        xforc(aml, m)
+        m.compute_forcing(_rad_c())
+        for s in range(nstr):
+            aml.forcing(None, None, None, True, TDTA)
+            ga.step(TDTA, 1)
+            if s == 0:
+                m.forcing(None, None, None, True, TDT)
+                g.step(TDT, 1)
+    for a, r in zip(ga.get_state(), qa.get_state()):
+        assert rel_l2(a, r) <= 1e-11
+    for a, r in zip(g.get_state(), qo.get_state()):
+        assert rel_l2(a, r) <= 1e-11
+    assert rel_l2(m.get_sst()[0], oo.data) <= 1e-11
+    assert rel_l2(aml.get_state()[0], oa.ast) <= 1e-11
+    assert rel_l2(aml.get_state()[2], oa.hmx) <= 1e-11
+    for k in ("m", "aml", "g", "ga"):
+        c[k].close()
+
+
+def test_compute_forcing_needs_a_coupled_atmosphere():
+    g = QG(ocean_double_gyre(33))
+    m = OceanMixedLayer(g, 100.0, 4.0e6, 10.0, 5.0)
+    with pytest.raises(OqgError):
+        m.compute_forcing(_rad_c())
+    m.close()
+    g.close()

@@ -139,3 +139,80 @@ def test_hermite_bicubic_reproduces_bicubics_and_nodes():
     ref = P(Xf, Yf)
     assert np.max(np.abs(out - ref)) <= 1e-12 * np.max(np.abs(ref))
     assert np.array_equal(out[::nd, ::nd], P(X, Y))
+
+
+# ----------------------------------------------------------- coupled fluxes
+from oracle.mixed_layer import RadCoeffs, bilint, compute_forcing, coupling_grid  # noqa: E402
+
+
+def _pair():
+    return ocean_double_gyre(129, dx=10.0e3), atmos_channel(49, 25, dx=80e3)
+
+
+def test_bilint_reproduces_linear_fields_and_wraps_in_x():
+    """Exact for a field linear in x and y where no wrap or end row enters;
+    the westmost ocean columns interpolate across the channel's periodic
+    seam (the last T column standing half a cell west of the first)."""
+    bo, ba = _pair()
+    nxta, nyta = ba.nxp - 1, ba.nyp - 1
+    _, _, _, c0, r0 = coupling_grid(bo, ba)
+    xa = (np.arange(nxta) + 0.5) * ba.dx
+    ya = (np.arange(nyta) + 0.5) * ba.dy
+    at = 3.0 + 2e-6 * xa[None, :] - 5e-6 * ya[:, None]
+    out = bilint(at, bo, ba)
+    xo = c0 * ba.dx + (np.arange(bo.nxp - 1) + 0.5) * bo.dx
+    yo = r0 * ba.dy + (np.arange(bo.nyp - 1) + 0.5) * bo.dy
+    ref = 3.0 + 2e-6 * xo[None, :] - 5e-6 * yo[:, None]
+    east = xo >= 0.5 * ba.dx
+    assert np.max(np.abs(out[:, east] - ref[:, east])) <= 1e-12
+    # the seam: the weights of the last column (at -dx/2) and the first
+    w = (xo[~east] + 0.5 * ba.dx) / ba.dx
+    seam = (1.0 - w)[None, :] * (3.0 + 2e-6 * xa[-1]) + w[None, :] * (3.0 + 2e-6 * xa[0])
+    assert np.max(np.abs(out[:, ~east] - (seam - 5e-6 * yo[:, None]))) <= 1e-12
+
+
+def test_compute_forcing_budget():
+    """With the perturbation, eta, topography and height terms off and
+    Dmdown = Dup(0): the ocean's upward fluxes reach the atmosphere times
+    the area ratio (summed over its cells), the ocean loses them and gains
+    Dmdown times the interpolated temperature; the perturbation forcing
+    fsprim sums to zero over the channel's rows."""
+    bo, ba = _pair()
+    rng = np.random.default_rng(3)
+    nyta, nxta = ba.nyp - 1, ba.nxp - 1
+    nyto, nxto = bo.nyp - 1, bo.nxp - 1
+    astm = -8.0 + rng.standard_normal((nyta, nxta))
+    hmxm = np.full((nyta, nxta), 1000.0)
+    sstm = 12.0 + rng.standard_normal((nyto, nxto))
+    pma = np.zeros((ba.nl, ba.nyp, ba.nxp))
+    rad = RadCoeffs(fspco=0.0, xlamda=35.0, d0up=5.5, dmdown=2.5, dup0=2.5, aup00=0.0, adown10=0.0, adown11=0.0)
+    fo, fa = compute_forcing(sstm, astm, hmxm, pma, ba, bo, rad, 1000.0, 0.0)
+    asto = bilint(astm, bo, ba)
+    up = 5.5 * sstm + 35.0 * (sstm - asto)
+    assert np.allclose(fo, -2.5 * asto - up, rtol=0, atol=1e-12)
+    ocfrac = bo.dx * bo.dy / (ba.dx * ba.dy)
+    assert abs(np.sum(fa + 2.5 * astm) - ocfrac * np.sum(up)) <= 1e-9 * np.sum(np.abs(up))
+    # only the perturbation forcing: each row constant, rows sum to zero
+    rad = RadCoeffs(fspco=80.0, xlamda=0.0, d0up=0.0, dmdown=0.0, dup0=0.0, aup00=0.0, adown10=0.0, adown11=0.0)
+    _, fa = compute_forcing(sstm, astm, hmxm, pma, ba, bo, rad, 1000.0, 0.0)
+    assert np.allclose(fa, fa[:, :1], rtol=0, atol=1e-12)
+    assert abs(np.sum(fa[:, 0])) <= 1e-11 * np.sum(np.abs(fa[:, 0]))
+
+
+def test_compute_forcing_eta_topography_and_height_terms():
+    """The eta_1, topography and height terms alone: T-point averages of
+    (pm_1 - pm_2) / gp_1 and dtop scaled by their coefficients, and the
+    height damping."""
+    bo, ba = _pair()
+    rng = np.random.default_rng(4)
+    nyta, nxta = ba.nyp - 1, ba.nxp - 1
+    pma = rng.standard_normal((ba.nl, ba.nyp, ba.nxp))
+    dtop = rng.standard_normal(ba.shape2)
+    hmxm = 1000.0 + rng.standard_normal((nyta, nxta))
+    rad = RadCoeffs(fspco=0.0, xlamda=0.0, d0up=0.0, dmdown=0.0, dup0=0.0, aup00=-0.03, adown10=0.02, adown11=0.01)
+    _, fa = compute_forcing(np.zeros((bo.nyp - 1, bo.nxp - 1)), np.zeros((nyta, nxta)), hmxm, pma, ba, bo, rad,
+                            1000.0, 0.5, dtop)
+    eta = (pma[0] - pma[1]) / ba.gp[0]
+    avg = lambda f: 0.25 * (f[:-1, :-1] + f[:-1, 1:] + f[1:, :-1] + f[1:, 1:])
+    ref = -0.01 * avg(eta) - (-0.03 + 0.02) * avg(dtop) + (-0.5 + 0.03 - 0.02) * (hmxm - 1000.0)
+    assert np.allclose(fa, ref, rtol=0, atol=1e-12)
