@@ -253,31 +253,35 @@ def coupled_config(nrep=3, nocean=10, nstr=10):
     after oqg_atmos_forcing, the first followed by one ocean step (513x513x3
     box, dx 10 km, tdt 3600 s) after oqg_ocean_forcing.  Every exchange runs
     on the device; nothing crosses from the host inside the loop.  The
-    radiation coefficients are fixed synthetic values of the reference's
-    magnitudes.  Host clock over nocean coupled ocean steps, median of
-    nrep."""
+    radiation and mixed-layer parameters are the reference's coupled
+    double-gyre configuration's (data/basin/atm_dg.cdl, ocn_dg.cdl) through
+    the radiative start-up (oqg_radiat and its helpers); the mixed layers
+    start from the radiative-balance profiles.  Host clock over nocean
+    coupled ocean steps, median of nrep."""
     from openqg_b200.core import QG, AtmosMixedLayer, OceanMixedLayer, lib
-    from openqg_b200.params import OqgRadCoeffs, atmos_channel, ocean_double_gyre
+    from openqg_b200.params import atmos_channel, ocean_double_gyre
+    from openqg_b200.radiation import coupled_start
     L = lib()
     bo, ba = ocean_double_gyre(513, dx=10e3), atmos_channel(193, 97, dx=80e3)
+    rad, ak, ok = coupled_start(ba, bo, hm_a=1000.0, fsbar=-210.0, fspamp=80.0, zopt=[200.0, 3.0e4, 3.0e4, 4.0e4],
+                                gamma=1.0e-2, xlamda=35.0, tabsat=[330.0, 340.0, 350.0], rho_a=1.0, cp_a=1.0e3,
+                                t1_abs_o=278.0, t2_abs_o=268.0, rho_o=1.0e3, cp_o=4.0e3)
     go, ga = QG(bo), QG(ba)
     po, _, _, _ = initial_inputs(bo, seed=3)
     pa, _, _, _ = initial_inputs(ba, seed=4)
     go.set_state(po, po)
     ga.set_state(pa, pa)
-    yo = np.linspace(0.0, 1.0, bo.nyp - 1)[:, None] * np.ones((1, bo.nxp - 1))
-    oml = OceanMixedLayer(go, hm=100.0, rho_cp=4.0e6, t1_rel=10.0, dt_12=5.0, st2d=2.0e3, st4d=0.0, ycexp=1.0)
-    sst = 12.0 + 3.0 * np.cos(np.pi * yo)
-    oml.set_sst(sst, sst)
-    yt = np.linspace(0.0, 1.0, ba.nyp - 1)[:, None] * np.ones((1, ba.nxp - 1))
-    aml = AtmosMixedLayer(ga, np.zeros_like(yt), None, hm=1000.0, rho_cp=1.0e3, t1_rel=-5.0, dt_12=20.0,
-                          hmamin=100.0, hmadmp=0.5, xcexp=1.0, at2d=2.5e4, at4d=0.0, ahmd=2.0e4,
-                          aface=(1e-7, -1e-7), bface=1e-7, dface=1e-6, cdat=1.3e-3)
-    aml.set_state(-8.0 + 2.0 * np.cos(np.pi * yt), -8.0 + 2.0 * np.cos(np.pi * yt),
-                  np.full(yt.shape, 1000.0), np.full(yt.shape, 1000.0))
-    oml.couple(aml, 1.2e-3)     # rho_a / rho_o
-    rad = OqgRadCoeffs(fspco=80.0, xlamda=35.0, d0up=5.5, dmdown=3.5, dup0=2.5, aup00=-0.03, adown10=0.02,
-                       adown11=0.01)
+    oml = OceanMixedLayer(go, hm=100.0, rho_cp=ok["rho_cp"], t1_rel=ok["t1_rel"], dt_12=ok["dt_12"], st2d=380.0,
+                          st4d=4.0e10, ycexp=1.0, fluxs=True, sval=ok["sval"], nval=ok["nval"])
+    yo = np.linspace(ok["sval"], ok["nval"], bo.nyp - 1)[:, None] * np.ones((1, bo.nxp - 1))
+    oml.set_sst(yo, yo)
+    xc = ak["xc1ast"]
+    aml = AtmosMixedLayer(ga, xc, None, hm=1000.0, rho_cp=ak["rho_cp"], t1_rel=ak["t1_rel"], dt_12=ak["dt_12"],
+                          hmamin=100.0, hmadmp=0.15, xcexp=1.0, at2d=5.0e4, at4d=3.0e14, ahmd=2.0e5,
+                          aface=ak["aface"], bface=ak["bface"], dface=ak["dface"], cdat=1.3e-3)
+    aml.set_state(xc, xc, np.full(xc.shape, 1000.0), np.full(xc.shape, 1000.0))
+    oml.couple(aml, 1.0e-3)     # rho_a / rho_o
+    rad = rad.c
 
     def coupled_step():
         rc = L.oqg_xforc(aml.h, oml.h)

@@ -424,6 +424,63 @@ typedef struct oqg_rad_coeffs {
     double adown11;    /* Adown(1,1)                                         */
 } oqg_rad_coeffs;
 
+/* ---------------------------------------------------------------------
+ * The radiation scheme's start-up on the host: the mean radiative balance
+ * of the coupled atmosphere and the linearised coefficients that
+ * compute_forcing and the mixed layers read.  Replaces:
+ *   load_rad, radiat and its helpers      src/mixed/radsubs.F90:63-674
+ *   init_temp_from_rad, zonal_temp        src/mixed/mixed.F90:102-151
+ *   sin_lat                               src/glam/numerics.F90:516-525
+ *   init_entrain_coeff, set_xc1ast        src/mixed/amlsubs.F90:100-182
+ * Host code only; no device is touched.
+ * ------------------------------------------------------------------- */
+
+/* load_rad's inputs (radsubs.F90:63-94). */
+typedef struct oqg_rad_params {
+    double fsbar;                 /* background forcing amplitude (< 0, W m^-2)    */
+    double fspamp;                /* perturbation forcing amplitude (>= 0, W m^-2) */
+    double gamma;                 /* adiabatic lapse rate (K m^-1)                  */
+    double xlamda;                /* sensible + latent transfer (W m^-2 K^-1)       */
+    double zopt[OQG_MAX_NL + 1];  /* optical depths: mixed layer, layers 1..nl (m)  */
+    double tabsat[OQG_MAX_NL];    /* the layers' absolute temperatures T_abs (K)    */
+} oqg_rad_params;
+
+/* radiat's results (radsubs.F90:116-157). */
+typedef struct oqg_rad_state {
+    oqg_rad_coeffs c;                        /* the values compute_forcing reads      */
+    double aup[OQG_MAX_NL + 1][OQG_MAX_NL];  /* Aup(k, l), k = 0..nl, l = 0..nl-1     */
+    double adown[OQG_MAX_NL][OQG_MAX_NL];    /* Adown(k, l) at [k-1][l], k = 1..nl    */
+    double dup[OQG_MAX_NL + 1];              /* Dup(0..nl)                            */
+    double rbetat[OQG_MAX_NL];               /* rbetat(1..nl-1) at [k-1]              */
+    double rbtmat, rbtmoc;                   /* balance coefficients of Tm' (atm, ocn) */
+    double atm_tmbar, ocn_tmbar;             /* mean mixed-layer temperatures (K)     */
+} oqg_rad_state;
+
+/* load_rad + radiat for an atmosphere of nl layers of thicknesses h, mixed
+ * layer depth hm, Coriolis parameter fnot (the sign of fspco): the layers'
+ * transmissivities, the mean up- and downgoing radiation (trapezoidal rule
+ * on 10001 points), the mixed layers' mean temperatures (fixed-point
+ * iterations to 1e-13 K), the mean fluxes, the perturbation coefficients and
+ * the radiative-balance coefficients (an nl x nl LU solve).  OQG_EINVAL for
+ * fspamp < 0, as load_rad stops; OQG_ESETUP when an iteration does not
+ * converge in 200 steps or the balance matrix is singular. */
+int oqg_radiat(int nl, const double *h, double hm, double fnot, const oqg_rad_params *p, oqg_rad_state *out);
+
+/* init_entrain_coeff (amlsubs.F90:100-131): the entrainment coefficients of
+ * interface 1, aface(1..nl-1) into aface[0..nl-2], bface, dface, from the
+ * radiation coefficients, rho_cp of air and dt_12 = T(1) - T(2). */
+int oqg_entrain_coeff(int nl, double rho_cp, double dt_12, const oqg_rad_state *rad, double *aface, double *bface,
+                      double *dface);
+
+/* zonal_temp (mixed.F90:144-151, sin_lat) at the nyt T rows of a basin whose
+ * first p row is at y0 with spacing dy: -sign(dT_NS, fnot) / 2 *
+ * sin(pi / 2 (y - yc) / (yn - yc)), yc the middle and yn the northern edge of
+ * the atmosphere's y range [ya0, ya0 + yla] (init_temp_from_rad), dT_NS =
+ * |rbtm * fspco|.  set_xc1ast's field is this profile on the atmosphere's
+ * rows, repeated along x; the ocean's wall temperatures are its first and
+ * last values on the ocean's rows (omlsubs.F90:38-41). */
+int oqg_zonal_temp(int nyt, double y0, double dy, double fnot, double ya0, double yla, double dt_ns, double *out);
+
 /* The net diabatic forcing of both mixed layers on the device, from the
  * lagged sst, the atmosphere's lagged temperature and height, eta_1 of its
  * lagged pressure and its topography (compute_forcing, forcing.F90:18-99;

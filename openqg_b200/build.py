@@ -13,7 +13,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "liboqg.so")
-SOURCES = ["oqg_capi.cu", "oqg_setup.cpp"]
+SOURCES = ["oqg_capi.cu", "oqg_setup.cpp", "oqg_radiat.cpp"]
 DEPS = SOURCES + ["oqg_dev.cuh", "oqg_fft.cuh", "oqg_kernels.cuh", "oqg_tma.cuh", "oqg_setup.h",
                   "oqg_adjoint.cuh", "oqg_noalloc.cuh", "oqg_mixed.cuh",
                   os.path.join("..", "..", "include", "oqg.h")]

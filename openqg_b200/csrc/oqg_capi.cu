@@ -33,6 +33,11 @@ static int fail(int code, const std::string &msg) {
     return code;
 }
 
+// The error reporter of the library's host-only files (oqg_radiat.cpp).
+namespace oqg {
+__attribute__((visibility("hidden"))) int host_fail(int code, const char *msg) { return fail(code, msg); }
+}  // namespace oqg
+
 #define CK(x)                                                                                  \
     do {                                                                                       \
         cudaError_t e_ = (x);                                                                  \

@@ -66,6 +66,21 @@ class OqgRadCoeffs(ctypes.Structure):
                                                "adown11")]
 
 
+class OqgRadParams(ctypes.Structure):
+    """ctypes mirror of `oqg_rad_params` (include/oqg.h): load_rad's inputs."""
+    _fields_ = [("fsbar", ctypes.c_double), ("fspamp", ctypes.c_double), ("gamma", ctypes.c_double),
+                ("xlamda", ctypes.c_double), ("zopt", ctypes.c_double * (OQG_MAX_NL + 1)),
+                ("tabsat", ctypes.c_double * OQG_MAX_NL)]
+
+
+class OqgRadState(ctypes.Structure):
+    """ctypes mirror of `oqg_rad_state` (include/oqg.h): radiat's results."""
+    _fields_ = [("c", OqgRadCoeffs), ("aup", (ctypes.c_double * OQG_MAX_NL) * (OQG_MAX_NL + 1)),
+                ("adown", (ctypes.c_double * OQG_MAX_NL) * OQG_MAX_NL), ("dup", ctypes.c_double * (OQG_MAX_NL + 1)),
+                ("rbetat", ctypes.c_double * OQG_MAX_NL), ("rbtmat", ctypes.c_double), ("rbtmoc", ctypes.c_double),
+                ("atm_tmbar", ctypes.c_double), ("ocn_tmbar", ctypes.c_double)]
+
+
 class OqgParams(ctypes.Structure):
     """ctypes mirror of `oqg_params` (include/oqg.h)."""
     _fields_ = [

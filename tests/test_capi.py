@@ -134,12 +134,20 @@ def test_added_entry_points_reject_null_arguments(liboqg):
     assert L.oqg_xforc(None, None) == 1
     assert L.oqg_compute_forcing(None, None) == 1
     assert L.oqg_get_fluxes(None, None, None) == 1
+    assert L.oqg_radiat(3, None, ctypes.c_double(1.0), ctypes.c_double(1.0), None, None) == 1
+    assert L.oqg_entrain_coeff(3, ctypes.c_double(1.0), ctypes.c_double(1.0), None, None, None, None) == 1
+    assert L.oqg_zonal_temp(1, *([ctypes.c_double(1.0)] * 6), None) == 1
 
 
 def test_rad_coeffs_struct_layout_matches_header():
     from openqg_b200.params import OqgRadCoeffs
     assert ctypes.sizeof(OqgRadCoeffs) == 8 * 8
     assert OqgRadCoeffs.adown11.offset == 7 * 8
+    from openqg_b200.params import OqgRadParams, OqgRadState
+    assert ctypes.sizeof(OqgRadParams) == (4 + 9 + 8) * 8
+    assert OqgRadParams.tabsat.offset == (4 + 9) * 8
+    assert OqgRadState.dup.offset == (8 + 9 * 8 + 8 * 8) * 8
+    assert ctypes.sizeof(OqgRadState) == (8 + 9 * 8 + 8 * 8 + 9 + 8 + 4) * 8
 
 
 def test_aml_params_struct_layout_matches_header():

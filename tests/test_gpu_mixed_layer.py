@@ -359,19 +359,27 @@ def _coupled_pair(seed, topography=True):
                 b=b, g=g, qo=qo, m=m, oo=oo, prm=prm)
 
 
-@pytest.mark.parametrize("topography", [True, False])
-def test_coupled_fluxes_match_oracle(topography):
+@pytest.mark.parametrize("topography,source", [(True, "fixed"), (False, "fixed"), (True, "radiat")])
+def test_coupled_fluxes_match_oracle(topography, source):
     """compute_forcing on the device: both mixed layers' net heat fluxes
-    against the restatement, before and after the atmosphere steps."""
+    against the restatement, before and after the atmosphere steps; the
+    radiation coefficients fixed, or from the radiative start-up with the
+    reference's atmosphere parameters (data/basin/atm_dg.cdl)."""
     c = _coupled_pair(seed=11, topography=topography)
     ba, b, m, aml, ga = c["ba"], c["b"], c["m"], c["aml"], c["ga"]
+    rc, rad = _rad_c(), RAD
+    if source == "radiat":
+        from openqg_b200.radiation import radiat
+        rc = radiat(ba.h, 1000.0, ba.fnot, fsbar=-210.0, fspamp=80.0, zopt=[200.0, 3.0e4, 3.0e4, 4.0e4],
+                    gamma=1.0e-2, xlamda=35.0, tabsat=[330.0, 340.0, 350.0]).c
+        rad = RadCoeffs(*[getattr(rc, f) for f, _ in OqgRadCoeffs._fields_])
     for it in range(2):
-        m.compute_forcing(_rad_c())
+        m.compute_forcing(rc)
         fo, fa = m.get_fluxes()
         _, astm, _, hmxm = aml.get_state()
         sstm = m.get_sst()[1]
         pma = ga.get_state()[1]
-        ro, ra = compute_forcing(sstm, astm, hmxm, pma, ba, b, RAD, c["aprm"].hm, c["aprm"].hmadmp, c["dtop"])
+        ro, ra = compute_forcing(sstm, astm, hmxm, pma, ba, b, rad, c["aprm"].hm, c["aprm"].hmadmp, c["dtop"])
         assert rel_l2(fo, ro) <= 1e-12, it
         assert rel_l2(fa, ra) <= 1e-12, it
         xforc(aml, m)
