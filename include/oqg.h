@@ -410,6 +410,13 @@ int oqg_oml_couple(oqg_oml *m, oqg_aml *a, double raoro);
  * times raoro.  The two handles' streams are ordered around the read of the
  * pressure (CUDA events). */
 int oqg_xforc(oqg_aml *a, oqg_oml *o);
+/* tau_udiff (windstress.F90:24-34, 255-276) on or off for the coupled pair
+ * (off at creation): the stress then follows the difference of the
+ * atmospheric and the ocean's lagged geostrophic surface velocity, the drag
+ * factor includes both mixed layers (cdat / f0a (1 / hma + raoro / hmo)),
+ * and the atmosphere's stress at the p points the two grids share is the
+ * ocean-resolution one (before raoro), as compute_windstress writes it. */
+int oqg_oml_tau_udiff(oqg_oml *o, int on);
 
 /* The radiation coefficients compute_forcing reads (radiate_type,
  * radsubs.F90:15-54), the derived values radiat computes at start-up. */

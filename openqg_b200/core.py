@@ -95,6 +95,7 @@ def lib():
     L.oqg_get_forcing.argtypes = [vp, _dp, _dp]
     L.oqg_oml_couple.argtypes = [vp, vp, ctypes.c_double]
     L.oqg_xforc.argtypes = [vp, vp]
+    L.oqg_oml_tau_udiff.argtypes = [vp, ctypes.c_int]
     L.oqg_compute_forcing.argtypes = [vp, ctypes.POINTER(OqgRadCoeffs)]
     L.oqg_get_fluxes.argtypes = [vp, vp, vp]
     L.oqg_aml_create.argtypes = [vp, ctypes.POINTER(OqgAmlParams), vp, vp, ctypes.POINTER(vp)]
@@ -468,6 +469,11 @@ class OceanMixedLayer:
         compute_forcing() (oqg_oml_couple); aml None unlinks."""
         _check(lib().oqg_oml_couple(self.h, None if aml is None else aml.h, float(raoro)), "oqg_oml_couple")
         self._aml = aml          # keeps the atmosphere alive while coupled
+
+    def tau_udiff(self, on: bool = True):
+        """tau_udiff: the coupled stress follows the atmosphere-ocean
+        velocity difference (oqg_oml_tau_udiff)."""
+        _check(lib().oqg_oml_tau_udiff(self.h, int(bool(on))), "oqg_oml_tau_udiff")
 
     def compute_forcing(self, rad: OqgRadCoeffs):
         """Both mixed layers' net heat fluxes on the device (compute_forcing,

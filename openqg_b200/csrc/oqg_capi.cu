@@ -2396,6 +2396,7 @@ int oqg_oml_couple(oqg_oml *m, oqg_aml *a, double raoro) {
     c.dxa = ba.dx; c.dya = ba.dy; c.f0a = ba.fnot; c.ah = ba.bc_half1;
     c.fxa = ba.fx; c.fya = ba.fy; c.fyb = ba.fy_bc;
     c.cdat = a->o.cdat; c.hma = a->o.hm; c.raoro = raoro;
+    c.hmo = m->o.hm; c.f0o = bo.fnot;
     m->ha = a->h;
     m->am = a;
     return OQG_OK;
@@ -2426,12 +2427,25 @@ int oqg_xforc(oqg_aml *a, oqg_oml *m) {
     const int gs = std::min((nsub + 255) / 256, 148 * 4);
     if (ha->mixed) k_cpl_derivs<float><<<gs, 256, 0, h->st>>>(m->cpl, (const float *)pma);
     else k_cpl_derivs<double><<<gs, 256, 0, h->st>>>(m->cpl, (const double *)pma);
-    CK(cudaEventRecord(m->ev_o, h->st));
-    CK(cudaStreamWaitEvent(ha->st, m->ev_o, 0));
     const int npo = m->o.nxp * m->o.nyp;
     const int gt = std::min((npo + 255) / 256, 148 * 8);
-    k_cpl_tau<<<gt, 256, 0, h->st>>>(m->cpl, m->o);
+    TauCpl c = m->cpl;
+    c.taux_a = const_cast<double *>(ao.taux);
+    c.tauy_a = const_cast<double *>(ao.tauy);
+    const void *pmo = h->hb.F[1 - h->par];    // the ocean's lagged pressure (compute_udiff)
+    if (h->mixed) k_cpl_tau<float><<<gt, 256, 0, h->st>>>(c, m->o, h->d_bas, (const float *)pmo);
+    else k_cpl_tau<double><<<gt, 256, 0, h->st>>>(c, m->o, h->d_bas, (const double *)pmo);
     CK(cudaGetLastError());
+    // the atmosphere's stream waits for the read of its pressure and, with
+    // tau_udiff, for the stress written over the ocean
+    CK(cudaEventRecord(m->ev_o, h->st));
+    CK(cudaStreamWaitEvent(ha->st, m->ev_o, 0));
+    return OQG_OK;
+}
+
+int oqg_oml_tau_udiff(oqg_oml *m, int on) {
+    if (!m) return fail(OQG_EINVAL, "null argument");
+    m->cpl.udiff = on != 0;
     return OQG_OK;
 }
 

@@ -191,6 +191,9 @@ struct TauCpl {
     double dxa, dya, f0a, ah, fxa, fya, fyb;   // the atmosphere's spacing and BC factors
     double cdat, hma, raoro;
     double *d;                          // [8][nytoar+1][nxtoar+1]: u, ux, uy, uxy, v, vx, vy, vxy
+    int udiff;                          // tau_udiff: the stress of the velocity difference
+    double hmo, f0o;                    // the ocean's mixed-layer depth and f0
+    double *taux_a, *tauy_a;            // the atmosphere's stress [nyp_a][nxp_a] (tau_udiff writes it)
 };
 
 // The atmospheric geostrophic velocity and its scaled derivatives at the
@@ -246,10 +249,16 @@ __global__ void k_cpl_derivs(TauCpl c, const T *__restrict__ PM1) {
 // derivatives, as new_bicubic, bicubic.F90:24-85; a shared cell edge takes
 // the later cell) and the drag law there (atmos_windstress, :278-314), times
 // the density ratio: the ocean's taux, tauy (compute_windstress, :187-195).
-__global__ void k_cpl_tau(TauCpl c, OmlDev o) {
+// With tau_udiff (compute_udiff, windstress.F90:255-276) the ocean's lagged
+// geostrophic surface velocity (dPdx_2bc / dPdy_2bc of its layer-1 pm) is
+// taken from the atmosphere's, the drag coefficient includes both mixed
+// layers, and the atmosphere's stress at the p points the two grids share is
+// the ocean-resolution one (compute_windstress, :179-187).
+template <class T>
+__global__ void k_cpl_tau(TauCpl c, OmlDev o, const BasinDev *__restrict__ bo, const T *__restrict__ PMo) {
     const int nx = c.nxtoar + 1, nd = c.ndxr;
     const size_t n = (size_t)nx * (c.nytoar + 1);
-    const double cdhfaa = (c.cdat / c.f0a) / c.hma;
+    const double cdhfaa = c.udiff ? (c.cdat / c.f0a) * (1.0 / c.hma + c.raoro / c.hmo) : (c.cdat / c.f0a) / c.hma;
     const double qpreaa = 1.0 / (fabs(cdhfaa) * sqrt(2.0));
     for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < o.nxp * o.nyp; idx += gridDim.x * blockDim.x) {
         const int jo = idx / o.nxp, io = idx - jo * o.nxp;
@@ -274,12 +283,24 @@ __global__ void k_cpl_tau(TauCpl c, OmlDev o) {
                 }
             uv[q] = acc;
         }
-        const double u = uv[0], v = uv[1];
+        double u = uv[0], v = uv[1];
+        if (c.udiff) {
+            double dpx, dpy;
+            dpdxy_bc(PMo, bo[0], io, jo, dpx, dpy);
+            u = u + dpy / c.f0o;
+            v = v - dpx / c.f0o;
+        }
         const double shrmag = sqrt(-1.0 + sqrt(1.0 + 4.0 * cdhfaa * cdhfaa * (u * u + v * v)));
         const double cuohf = (qpreaa * cdhfaa) * shrmag;
         const double cdchi = (qpreaa * c.cdat) * shrmag / (1.0 + cuohf * cuohf);
-        const_cast<double *>(o.taux)[idx] = c.raoro * (cdchi * (u - cuohf * v));
-        const_cast<double *>(o.tauy)[idx] = c.raoro * (cdchi * (v + cuohf * u));
+        const double tx = cdchi * (u - cuohf * v), ty = cdchi * (v + cuohf * u);
+        const_cast<double *>(o.taux)[idx] = c.raoro * tx;
+        const_cast<double *>(o.tauy)[idx] = c.raoro * ty;
+        if (c.udiff && io % nd == 0 && jo % nd == 0) {
+            const size_t q = (size_t)(c.r0 + jo / nd) * c.nxp_a + c.c0 + io / nd;
+            c.taux_a[q] = tx;
+            c.tauy_a[q] = ty;
+        }
     }
 }
 

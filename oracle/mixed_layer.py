@@ -391,13 +391,38 @@ def hermite_bicubic(f, fx, fy, fxy, ndxr):
     return out
 
 
-def ocean_stress(pma1, ba, bo, cdat, hma, raoro):
+def _dx_bc_box(f, dx, alpha):
+    """dPdx_2bc of a closed-box field (numerics.F90:470-492)."""
+    o = np.empty_like(f)
+    o[:, 1:-1] = (f[:, 2:] - f[:, :-2]) / (2.0 * dx)
+    o[:, 0] = (f[:, 1] - f[:, 0]) / (dx * (0.5 * alpha + 1.0))
+    o[:, -1] = (f[:, -1] - f[:, -2]) / (dx * (0.5 * alpha + 1.0))
+    o[0] = 0.0
+    o[-1] = 0.0
+    return o
+
+
+def _dy_bc_box(f, dy, alpha):
+    """dPdy_2bc of a closed-box field (numerics.F90:494-513)."""
+    o = np.empty_like(f)
+    o[1:-1] = (f[2:] - f[:-2]) / (2.0 * dy)
+    o[0] = (f[1] - f[0]) / (dy * (0.5 * alpha + 1.0))
+    o[-1] = (f[-1] - f[-2]) / (dy * (0.5 * alpha + 1.0))
+    o[:, 0] = 0.0
+    o[:, -1] = 0.0
+    return o
+
+
+def ocean_stress(pma1, ba, bo, cdat, hma, raoro, pmo1=None, hmo=None, atmos_tau=None):
     """The ocean's wind stress from the atmosphere's lagged layer-1 pressure
     (compute_windstress, atmos_geos_vel, atmos_windstress; windstress.F90:
-    150-314, without the ocean-velocity dependence): the atmospheric
-    geostrophic velocity and its derivatives on the atmospheric p points over
-    the ocean, interpolated bicubically to the ocean's p points, the drag
-    law there, times the density ratio raoro.  Returns taux, tauy (nyp, nxp)."""
+    150-314): the atmospheric geostrophic velocity and its derivatives on the
+    atmospheric p points over the ocean, interpolated bicubically to the
+    ocean's p points, the drag law there, times the density ratio raoro.
+    Returns taux, tauy (nyp, nxp).  Given the ocean's lagged layer-1 pressure
+    pmo1 and mixed-layer depth hmo (tau_udiff, :255-276), the velocity is the
+    difference with the ocean's, and atmos_tau = (taux_a, tauy_a), if given,
+    takes the ocean-resolution stress at the shared p points (:179-187)."""
     ndxr, nxtoar, nytoar, c0, r0 = coupling_grid(bo, ba)
     ah = 0.5 * ba.bcco + 1.0
     p = pma1
@@ -411,12 +436,21 @@ def ocean_stress(pma1, ba, bo, cdat, hma, raoro):
                         -(dx * dy / f0) * dxyy[sub], ndxr)
     v = hermite_bicubic(dpdx[sub] / f0, (dx / f0) * d2x[sub], (dy / f0) * dxy[sub],
                         (dx * dy / f0) * dxxy[sub], ndxr)
-    cdhfaa = (cdat / f0) / hma
+    if pmo1 is not None:
+        u = u + _dy_bc_box(pmo1, bo.dy, bo.bcco) / bo.fnot
+        v = v - _dx_bc_box(pmo1, bo.dx, bo.bcco) / bo.fnot
+        cdhfaa = (cdat / f0) * (1.0 / hma + raoro / hmo)
+    else:
+        cdhfaa = (cdat / f0) / hma
     qpreaa = 1.0 / (abs(cdhfaa) * np.sqrt(2.0))
     shrmag = np.sqrt(-1.0 + np.sqrt(1.0 + 4.0 * cdhfaa * cdhfaa * (u * u + v * v)))
     cuohf = (qpreaa * cdhfaa) * shrmag
     cdchi = (qpreaa * cdat) * shrmag / (1.0 + cuohf * cuohf)
-    return raoro * (cdchi * (u - cuohf * v)), raoro * (cdchi * (v + cuohf * u))
+    tx, ty = cdchi * (u - cuohf * v), cdchi * (v + cuohf * u)
+    if pmo1 is not None and atmos_tau is not None:
+        for a, t in zip(atmos_tau, (tx, ty)):
+            a[r0:r0 + nytoar + 1, c0:c0 + nxtoar + 1] = t[::ndxr, ::ndxr]
+    return raoro * tx, raoro * ty
 
 
 # ------------------------------------------------------------ coupled fluxes

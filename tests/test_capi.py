@@ -132,6 +132,7 @@ def test_added_entry_points_reject_null_arguments(liboqg):
     assert L.oqg_atmos_forcing(None, None, None, None, 1, ctypes.c_double(1.0)) == 1
     assert L.oqg_oml_couple(None, None, ctypes.c_double(1.2e-3)) == 1
     assert L.oqg_xforc(None, None) == 1
+    assert L.oqg_oml_tau_udiff(None, 1) == 1
     assert L.oqg_compute_forcing(None, None) == 1
     assert L.oqg_get_fluxes(None, None, None) == 1
     assert L.oqg_radiat(3, None, ctypes.c_double(1.0), ctypes.c_double(1.0), None, None) == 1

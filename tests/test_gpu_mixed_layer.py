@@ -445,3 +445,30 @@ def test_compute_forcing_needs_a_coupled_atmosphere():
         m.compute_forcing(_rad_c())
     m.close()
     g.close()
+
+
+def test_tau_udiff_stresses_match_oracle():
+    """tau_udiff: the stress of the atmosphere-ocean velocity difference
+    (compute_udiff), for both basins, through each handle's Ekman pumping;
+    the atmosphere's stress over the ocean is the ocean-resolution one."""
+    c = _coupled_pair(seed=17)
+    ba, b, aprm, prm = c["ba"], c["b"], c["aprm"], c["prm"]
+    ga, aml, g, m = c["ga"], c["aml"], c["g"], c["m"]
+    g.step(TDT, 2)                         # the ocean's lagged pressure unlike its current one
+    m.tau_udiff(True)
+    for _ in range(2):
+        pma, pmo = ga.get_state()[1], g.get_state()[1]
+        tax, tay = atmos_stress(pma[0], ba, 1.3e-3, aprm.hm)
+        tox, toy = ocean_stress(pma[0], ba, b, 1.3e-3, aprm.hm, 1.2e-3, pmo1=pmo[0], hmo=prm.hm,
+                                atmos_tau=(tax, tay))
+        wpo = ekman(tox, toy, b.dx, b.dy, b.fnot, prm.hm)[3]
+        wpa = ekman_cyclic(tax, tay, ba.dx, ba.dy, ba.fnot, aprm.hm)[3]
+        xforc(aml, m)
+        m.forcing(None, None, np.zeros((b.nyp - 1, b.nxp - 1)), True, TDT)
+        aml.forcing(None, None, np.zeros((ba.nyp - 1, ba.nxp - 1)), True, TDTA)
+        assert rel_l2(get_forcing(g)[0], wpo) <= 1e-12
+        assert rel_l2(get_forcing(ga)[0], wpa) <= 1e-12
+        g.step(TDT, 1)
+        ga.step(TDTA, 1)
+    for k in ("m", "aml", "g", "ga"):
+        c[k].close()

@@ -216,3 +216,24 @@ def test_compute_forcing_eta_topography_and_height_terms():
     avg = lambda f: 0.25 * (f[:-1, :-1] + f[:-1, 1:] + f[1:, :-1] + f[1:, 1:])
     ref = -0.01 * avg(eta) - (-0.03 + 0.02) * avg(dtop) + (-0.5 + 0.03 - 0.02) * (hmxm - 1000.0)
     assert np.allclose(fa, ref, rtol=0, atol=1e-12)
+
+
+def test_tau_udiff_reduces_to_the_atmosphere_alone():
+    """With the ocean at rest and an infinitely deep ocean mixed layer the
+    velocity-difference stress is the atmosphere-only one; the atmosphere's
+    stress over the ocean becomes the ocean-resolution stress before the
+    density ratio."""
+    from oracle.mixed_layer import atmos_stress, ocean_stress
+    bo, ba = _pair()
+    rng = np.random.default_rng(6)
+    pma = ba.fnot * 1e5 * rng.standard_normal((ba.nyp, ba.nxp))
+    pma[:, -1] = pma[:, 0]
+    t0 = ocean_stress(pma, ba, bo, 1.3e-3, 1000.0, 1.2e-3)
+    t1 = ocean_stress(pma, ba, bo, 1.3e-3, 1000.0, 1.2e-3, pmo1=np.zeros((bo.nyp, bo.nxp)), hmo=np.inf)
+    assert np.array_equal(t0[0], t1[0]) and np.array_equal(t0[1], t1[1])
+    pmo = bo.fnot * 1e4 * rng.standard_normal((bo.nyp, bo.nxp))
+    tax, tay = atmos_stress(pma, ba, 1.3e-3, 1000.0)
+    tox, toy = ocean_stress(pma, ba, bo, 1.3e-3, 1000.0, 1.2e-3, pmo1=pmo, hmo=100.0, atmos_tau=(tax, tay))
+    ndxr, nxtoar, nytoar, c0, r0 = coupling_grid(bo, ba)
+    assert np.allclose(tax[r0:r0 + nytoar + 1, c0:c0 + nxtoar + 1] * 1.2e-3, tox[::ndxr, ::ndxr], rtol=1e-15, atol=0)
+    assert not np.allclose(tox, t0[0])
