@@ -256,11 +256,12 @@ def coupled_config(nrep=3, nocean=10, nstr=10):
     radiation and mixed-layer parameters are the reference's coupled
     double-gyre configuration's (data/basin/atm_dg.cdl, ocn_dg.cdl) through
     the radiative start-up (oqg_radiat and its helpers); the mixed layers
-    start from the radiative-balance profiles.  Host clock over nocean
+    start from the radiative-balance profiles (rbal), the QG states from
+    seeded noise.  Host clock over nocean
     coupled ocean steps, median of nrep."""
     from openqg_b200.core import QG, AtmosMixedLayer, OceanMixedLayer, lib
     from openqg_b200.params import atmos_channel, ocean_double_gyre
-    from openqg_b200.radiation import coupled_start
+    from openqg_b200.radiation import coupled_start, rbal_states
     L = lib()
     bo, ba = ocean_double_gyre(513, dx=10e3), atmos_channel(193, 97, dx=80e3)
     rad, ak, ok = coupled_start(ba, bo, hm_a=1000.0, fsbar=-210.0, fspamp=80.0, zopt=[200.0, 3.0e4, 3.0e4, 4.0e4],
@@ -273,13 +274,13 @@ def coupled_config(nrep=3, nocean=10, nstr=10):
     ga.set_state(pa, pa)
     oml = OceanMixedLayer(go, hm=100.0, rho_cp=ok["rho_cp"], t1_rel=ok["t1_rel"], dt_12=ok["dt_12"], st2d=380.0,
                           st4d=4.0e10, ycexp=1.0, fluxs=True, sval=ok["sval"], nval=ok["nval"])
-    yo = np.linspace(ok["sval"], ok["nval"], bo.nyp - 1)[:, None] * np.ones((1, bo.nxp - 1))
-    oml.set_sst(yo, yo)
+    _, sst, ast = rbal_states(ba, bo, rad, ak)
+    oml.set_sst(sst, sst)
     xc = ak["xc1ast"]
     aml = AtmosMixedLayer(ga, xc, None, hm=1000.0, rho_cp=ak["rho_cp"], t1_rel=ak["t1_rel"], dt_12=ak["dt_12"],
                           hmamin=100.0, hmadmp=0.15, xcexp=1.0, at2d=5.0e4, at4d=3.0e14, ahmd=2.0e5,
                           aface=ak["aface"], bface=ak["bface"], dface=ak["dface"], cdat=1.3e-3)
-    aml.set_state(xc, xc, np.full(xc.shape, 1000.0), np.full(xc.shape, 1000.0))
+    aml.set_state(ast, ast, np.full(xc.shape, 1000.0), np.full(xc.shape, 1000.0))
     oml.couple(aml, 1.0e-3)     # rho_a / rho_o
     rad = rad.c
 

@@ -67,6 +67,15 @@ def zonal_temp(nyt: int, y0: float, dy: float, fnot: float, ya0: float, yla: flo
     return out
 
 
+def _ocean_profile(ba, bo, rad: OqgRadState):
+    """zonal_temp of the ocean's temperature (init_temp_from_rad with rbtmoc)
+    on its T rows; the ocean sits centred in the channel (load_grid)."""
+    nyta, nyto = ba.nyp - 1, bo.nyp - 1
+    nytoar = nyto // int(round(ba.dx / bo.dx))
+    y0o = ((nyta - nytoar) // 2) * ba.dy
+    return zonal_temp(nyto, y0o, bo.dy, bo.fnot, 0.0, nyta * ba.dy, abs(rad.rbtmoc * rad.c.fspco))
+
+
 def coupled_start(ba, bo, *, hm_a: float, fsbar: float, fspamp: float, zopt, gamma: float, xlamda: float, tabsat,
                   rho_a: float, cp_a: float, t1_abs_o: float, t2_abs_o: float, rho_o: float, cp_o: float):
     """The coupled model's radiative start-up (openqg.F90:190-215): radiat on
@@ -86,9 +95,26 @@ def coupled_start(ba, bo, *, hm_a: float, fsbar: float, fspamp: float, zopt, gam
     xc = zonal_temp(nyta, 0.0, ba.dy, ba.fnot, 0.0, yla, abs(rad.rbtmat * rad.c.fspco))
     atm = dict(xc1ast=np.repeat(xc[:, None], ba.nxp - 1, axis=1), t1_rel=tabsat[0] - rad.atm_tmbar, dt_12=dt12_a,
                rho_cp=rho_a * cp_a, aface=tuple(aface), bface=bface, dface=dface)
-    nytoar = nyto // int(round(ba.dx / bo.dx))
-    y0o = ((nyta - nytoar) // 2) * ba.dy
-    wall = zonal_temp(nyto, y0o, bo.dy, bo.fnot, 0.0, yla, abs(rad.rbtmoc * rad.c.fspco))
+    wall = _ocean_profile(ba, bo, rad)
     ocn = dict(t1_rel=t1_abs_o - rad.ocn_tmbar, dt_12=t1_abs_o - t2_abs_o, rho_cp=rho_o * cp_o,
                nval=float(wall[-1]), sval=float(wall[0]))
     return rad, atm, ocn
+
+
+def rbal_states(ba, bo, rad: OqgRadState, atm: dict):
+    """The radiative-balance initial states (init_dynamic_state with
+    qg_state, oml_state and aml_state "rbal", openqg.F90:249-306): the
+    atmosphere's pressure (nl, nyp, nxp), p_k = plfac_k fsprim(yprel) with
+    plfac_1 = 0 and plfac_k = plfac_{k-1} - gp_{k-1} rbetat_{k-1}; the sst
+    (nyt, nxt), zonal_temp on the ocean's rows; ast, the atmosphere's
+    zonal_temp (its xc1ast, from coupled_start's atm).  p and pm, data and
+    datam start equal."""
+    nl, yla = ba.nl, (ba.nyp - 1) * ba.dy
+    plfac = np.zeros(nl)
+    for k in range(1, nl):
+        plfac[k] = plfac[k - 1] - ba.gp[k - 1] * rad.rbetat[k - 1]
+    yprel = -0.5 * yla + np.arange(ba.nyp) * ba.dy
+    fsp = rad.c.fspco * 0.5 * np.sin(np.pi * yprel / yla)          # fsprim (radsubs.F90:97-114)
+    p = plfac[:, None, None] * np.repeat(fsp[:, None], ba.nxp, axis=1)[None]
+    sst = np.repeat(_ocean_profile(ba, bo, rad)[:, None], bo.nxp - 1, axis=1)
+    return p, sst, atm["xc1ast"].copy()

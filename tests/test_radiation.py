@@ -97,3 +97,29 @@ def test_rejected_inputs():
         radiat(DG["h"], 2500.0, 1e-4, **kw)                          # mixed layer deeper than layer 1
     with pytest.raises(OqgError):
         radiat(DG["h"], DG["hm"], 1e-4, **dict(kw, zopt=[0.0, 3e4, 3e4, 4e4]))
+
+
+def test_rbal_states():
+    """The radiative-balance initial states (openqg.F90:249-306) from the
+    coupled start-up: the atmosphere's layer pressures follow fsprim with
+    the layer factors, layer 1 at rest; the mixed layers carry the zonal
+    temperature profiles, the ocean's ends its wall temperatures."""
+    from openqg_b200.params import atmos_channel, ocean_double_gyre
+    from openqg_b200.radiation import coupled_start, rbal_states
+    ba, bo = atmos_channel(49, 25, dx=80e3), ocean_double_gyre(129, dx=10e3)
+    kw = dict(hm_a=1000.0, fsbar=-210.0, fspamp=80.0, zopt=[200.0, 3.0e4, 3.0e4, 4.0e4], gamma=1.0e-2, xlamda=35.0,
+              tabsat=[330.0, 340.0, 350.0], rho_a=1.0, cp_a=1.0e3, t1_abs_o=278.0, t2_abs_o=268.0, rho_o=1.0e3,
+              cp_o=4.0e3)
+    rad, atm, ocn = coupled_start(ba, bo, **kw)
+    p, sst, ast = rbal_states(ba, bo, rad, atm)
+    o = R.radiat(ba.h, 1000.0, ba.fnot, fsbar=-210.0, fspamp=80.0, zopt=kw["zopt"], gamma=1e-2, xlamda=35.0,
+                 tabsat=kw["tabsat"])
+    yla = (ba.nyp - 1) * ba.dy
+    fsp = 80.0 * 0.5 * np.sin(np.pi * (-0.5 * yla + np.arange(ba.nyp) * ba.dy) / yla)
+    assert np.all(p[0] == 0.0)
+    plf = [0.0, -ba.gp[0] * o.rbetat[0], -ba.gp[0] * o.rbetat[0] - ba.gp[1] * o.rbetat[1]]
+    for k in range(3):
+        assert _close(p[k], plf[k] * fsp[:, None] * np.ones((1, ba.nxp)))
+    assert sst[0, 0] == ocn["sval"] and sst[-1, 0] == ocn["nval"]
+    assert np.all(sst == sst[:, :1])
+    assert np.array_equal(ast, atm["xc1ast"])
