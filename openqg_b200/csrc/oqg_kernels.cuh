@@ -498,12 +498,23 @@ k_vort(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par,
                     if (gj == nyp - 2) sq[3] += (double)(qc * (sP[(r + 1) * LPQ + c + 1] - sP[(r + 1) * LPQ + c - 1]));
                 }
             }
+            // only the row ty = 0 (warps 0 and 1) holds terms: reduce the
+            // OQG_NQ sums together in those two warps, then add warp 1's to
+            // warp 0's (the value block_sum gives, without its barriers)
             double *pt = b.part_tile + ((size_t)w.block * b.nl + k) * OQG_NQ;
+            if (ty == 0) {
 #pragma unroll
-            for (int q = 0; q < OQG_NQ; ++q) {
-                double sv = block_sum(sq[q], red);
-                if (threadIdx.x == 0) pt[q] = sv;
+                for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+                    for (int q = 0; q < OQG_NQ; ++q) sq[q] += __shfl_down_sync(0xffffffffu, sq[q], o);
+                if (threadIdx.x == 32)
+#pragma unroll
+                    for (int q = 0; q < OQG_NQ; ++q) red[q] = sq[q];
             }
+            __syncthreads();
+            if (threadIdx.x == 0)
+#pragma unroll
+                for (int q = 0; q < OQG_NQ; ++q) pt[q] = sq[q] + red[q];
         }
         __syncthreads();
     }
@@ -953,17 +964,30 @@ __device__ __noinline__ void scalar_phase(const BasinDev &b, double tdt, int par
             imode[m] = __shfl_sync(0xffffffffu, s, 0) * b.ftnorm * b.dx * b.dy;
         }
     } else {
-        // strip sums over the tiles touching rows 0, 1, nyp-2, nyp-1
+        // strip sums over the tiles touching rows 0, 1, nyp-2, nyp-1: per
+        // layer the OQG_NQ sums together, so their loads and shuffles overlap
+        // (the additions keep warp_sum's order)
         const int ntile = b.tiles_x * b.tiles_y;
 #pragma unroll 1
-        for (int kq = 0; kq < NL * OQG_NQ; ++kq) {
-            double s = 0.0;
+        for (int k = 0; k < NL; ++k) {
+            double acc[OQG_NQ];
+#pragma unroll
+            for (int q = 0; q < OQG_NQ; ++q) acc[q] = 0.0;
             for (int t = lane; t < ntile; t += 32) {
                 const int ty0 = (t / b.tiles_x) * b.vty;
-                if (ty0 <= 1 || ty0 + b.vty > b.nyp - 2) s += b.part_tile[(size_t)t * NL * OQG_NQ + kq];
+                if (ty0 <= 1 || ty0 + b.vty > b.nyp - 2) {
+                    const double *pt = b.part_tile + ((size_t)t * NL + k) * OQG_NQ;
+#pragma unroll
+                    for (int q = 0; q < OQG_NQ; ++q) acc[q] += pt[q];
+                }
             }
-            s = warp_sum(s);
-            if (lane == 0) S[kq / OQG_NQ][kq % OQG_NQ] = s;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+                for (int q = 0; q < OQG_NQ; ++q) acc[q] += __shfl_down_sync(0xffffffffu, acc[q], o);
+            if (lane == 0)
+#pragma unroll
+                for (int q = 0; q < OQG_NQ; ++q) S[k][q] = acc[q];
         }
         __syncwarp();
     }
