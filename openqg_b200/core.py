@@ -481,10 +481,13 @@ class OceanMixedLayer:
         _check(lib().oqg_compute_forcing(self.h, ctypes.byref(rad)), "oqg_compute_forcing")
 
     def get_fluxes(self):
-        """The held fluxes: fnetoc (nyt, nxt) and the atmosphere's fnetat."""
+        """The held fluxes: fnetoc (nyt, nxt) and, when coupled, the
+        atmosphere's fnetat (None otherwise)."""
         fo = np.empty(self.tshape)
-        fa = np.empty(self._aml.tshape)
-        _check(lib().oqg_get_fluxes(self.h, fo.ctypes.data, fa.ctypes.data), "oqg_get_fluxes")
+        aml = getattr(self, "_aml", None)
+        fa = np.empty(aml.tshape) if aml is not None else None
+        _check(lib().oqg_get_fluxes(self.h, fo.ctypes.data, None if fa is None else fa.ctypes.data),
+               "oqg_get_fluxes")
         return fo, fa
 
     def forcing(self, taux, tauy, fnetoc, compute_ent: bool, tdto: float):
