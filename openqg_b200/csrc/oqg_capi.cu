@@ -1893,6 +1893,7 @@ struct oqg_oml {
     oqg_aml *am = nullptr;                // and its mixed layer
     TauCpl cpl{};
     cudaEvent_t ev_a = nullptr, ev_o = nullptr;
+    unsigned *ticket = nullptr;           // k_oml_post's last-CTA counter (zero between launches)
 };
 
 extern "C" {
@@ -1919,7 +1920,7 @@ int oqg_oml_create(oqg_handle *h, const oqg_oml_params *prm, oqg_oml **out) {
     o.t1_rel = prm->t1_rel; o.dt_12 = prm->dt_12; o.st2d = prm->st2d; o.st4d = prm->st4d;
     o.ycexp = prm->ycexp; o.nval = prm->nval; o.sval = prm->sval;
     const size_t nt = (size_t)o.nxt * o.nyt, np = (size_t)o.nxp * o.nyp;
-    const size_t total = 6 * nt + 2 * np + OQG_OML_CTAS;
+    const size_t total = 6 * nt + 2 * np + OQG_OML_CTAS + 1;   // + the post kernel's ticket
     void *x = nullptr;
     if (cudaMalloc(&x, total * sizeof(double)) != cudaSuccess) {
         delete m;
@@ -1933,6 +1934,7 @@ int oqg_oml_create(oqg_handle *h, const oqg_oml_params *prm, oqg_oml **out) {
     o.taux = d + 6 * nt;
     o.tauy = d + 6 * nt + np;
     o.part = d + 6 * nt + 2 * np;
+    m->ticket = reinterpret_cast<unsigned *>(d + 6 * nt + 2 * np + OQG_OML_CTAS);
     if (cudaMemsetAsync(x, 0, total * sizeof(double), h->st) != cudaSuccess ||
         cudaStreamSynchronize(h->st) != cudaSuccess) {
         cudaFree(x);
@@ -1995,12 +1997,17 @@ int oqg_ocean_forcing(oqg_oml *m, const double *taux, const double *tauy, const 
     const void *p1 = b.F[h->par];   // layer 1 of the current p (driver.F90:96-103)
     if (h->mixed) k_oml_step<float><<<OQG_OML_CTAS, 256, 0, h->st>>>(o, (const float *)p1, b.px, tdto, compute_ent);
     else k_oml_step<double><<<OQG_OML_CTAS, 256, 0, h->st>>>(o, (const double *)p1, b.px, tdto, compute_ent);
+    // the entrainment the handle holds after this call; the last CTA of
+    // k_oml_post forms its integrals and zeroes txis, txin (a closed box)
+    const void *ent_after = compute_ent ? h->ent_buf : b.ent;
     if (h->mixed)
         k_oml_post<float><<<b.nyp, 128, 0, h->st>>>(o, (float *)b.wekp, (float *)h->ent_buf, b.ent_rows, b.px, b.nl,
-                                                    compute_ent, OQG_OML_CTAS);
+                                                    compute_ent, OQG_OML_CTAS, h->d_bas, (const float *)ent_after,
+                                                    m->ticket);
     else
         k_oml_post<double><<<b.nyp, 128, 0, h->st>>>(o, (double *)b.wekp, (double *)h->ent_buf, b.ent_rows, b.px,
-                                                     b.nl, compute_ent, OQG_OML_CTAS);
+                                                     b.nl, compute_ent, OQG_OML_CTAS, h->d_bas,
+                                                     (const double *)ent_after, m->ticket);
     CK(cudaGetLastError());
     // datam <- data, data <- the new sst; the old datam becomes the next scratch
     double *dm_old = o.datam;
@@ -2013,13 +2020,6 @@ int oqg_ocean_forcing(oqg_oml *m, const double *taux, const double *tauy, const 
         int rc = push_desc(h);
         if (rc) return rc;
     }
-    // (ent_rows came with the entrainment from k_oml_post)
-    if (h->mixed) k_forcing_integrals<float><<<1, 512, 0, h->st>>>(h->d_bas, 0);
-    else k_forcing_integrals<double><<<1, 512, 0, h->st>>>(h->d_bas, 0);
-    h->frc_host[0] = 0.0;   // txis, txin: zero for a closed box (ekman.F90:60-70)
-    h->frc_host[1] = 0.0;
-    CK(cudaMemcpyAsync(&b.frc->txis, h->frc_host, 2 * sizeof(double), cudaMemcpyHostToDevice, h->st));
-    CK(cudaGetLastError());
     CK(cudaEventSynchronize(h->up_ev));
     return OQG_OK;
 }
@@ -2219,6 +2219,7 @@ struct oqg_aml {
     oqg_handle *h = nullptr;
     std::vector<void *> allocs;
     AmlDev o{};
+    unsigned *ticket = nullptr;           // k_aml_post's last-CTA counter (zero between launches)
 };
 
 extern "C" {
@@ -2244,7 +2245,7 @@ int oqg_aml_create(oqg_handle *h, const oqg_aml_params *prm, const double *xc1as
         o.gp[k] = k < b.nl - 1 ? b.gp[k] : 1.0;
     }
     const size_t nt = (size_t)o.nxt * o.nyt, np = (size_t)o.nxp * o.nyp;
-    const size_t total = 10 * nt + 3 * np;
+    const size_t total = 10 * nt + 3 * np + 1;   // + the post kernel's ticket
     void *x = nullptr;
     if (cudaMalloc(&x, total * sizeof(double)) != cudaSuccess) {
         delete m;
@@ -2261,6 +2262,7 @@ int oqg_aml_create(oqg_handle *h, const oqg_aml_params *prm, const double *xc1as
     o.tauy = d + 10 * nt + np;
     double *dt = d + 10 * nt + 2 * np;
     o.dtop = dtop ? dt : nullptr;
+    m->ticket = reinterpret_cast<unsigned *>(d + 10 * nt + 3 * np);
     bool ok = cudaMemsetAsync(x, 0, total * sizeof(double), h->st) == cudaSuccess;
     // init_atmos_ml: ast starts at 0, hmixa at the box's hm (amlsubs.F90:88-91)
     std::vector<double> hm0(nt, prm->hm);
@@ -2330,16 +2332,20 @@ int oqg_atmos_forcing(oqg_aml *m, const double *taux, const double *tauy, const 
         CK(cudaMemcpyAsync(const_cast<double *>(o.fnet), fnetat, nt * sizeof(double), cudaMemcpyDefault, h->st));
     CK(cudaEventRecord(h->up_ev, h->st));
     const int grid = std::min((int)((nt + 255) / 256), 148 * 8);
+    // the entrainment the handle holds after this call; the last CTA of
+    // k_aml_post forms txis, txin and the forcing integrals
+    const void *ent_after = compute_ent ? h->ent_buf : b.ent;
     if (h->mixed) {
         k_aml_step<float><<<grid, 256, 0, h->st>>>(o, (const float *)p1, b.px, tdta, compute_ent);
         k_aml_post<float><<<b.nyp, 128, 0, h->st>>>(o, (const float *)pm, (float *)b.wekp, (float *)h->ent_buf,
-                                                    b.ent_rows, b.px, compute_ent);
+                                                    b.ent_rows, b.px, compute_ent, h->d_bas,
+                                                    (const float *)ent_after, m->ticket);
     } else {
         k_aml_step<double><<<grid, 256, 0, h->st>>>(o, (const double *)p1, b.px, tdta, compute_ent);
         k_aml_post<double><<<b.nyp, 128, 0, h->st>>>(o, (const double *)pm, (double *)b.wekp,
-                                                     (double *)h->ent_buf, b.ent_rows, b.px, compute_ent);
+                                                     (double *)h->ent_buf, b.ent_rows, b.px, compute_ent, h->d_bas,
+                                                     (const double *)ent_after, m->ticket);
     }
-    k_aml_strips<<<1, 128, 0, h->st>>>(o, b.frc);
     CK(cudaGetLastError());
     // lagged <- current, current <- new; the old lagged buffers become scratch
     double *a_old = o.astm, *h_old = o.hmxm;
@@ -2351,10 +2357,6 @@ int oqg_atmos_forcing(oqg_aml *m, const double *taux, const double *tauy, const 
         int rc = push_desc(h);
         if (rc) return rc;
     }
-    // the channel's forcing integrals (ent_xn and the ent strip integrals)
-    if (h->mixed) k_forcing_integrals<float><<<1, 512, 0, h->st>>>(h->d_bas, 0);
-    else k_forcing_integrals<double><<<1, 512, 0, h->st>>>(h->d_bas, 0);
-    CK(cudaGetLastError());
     CK(cudaEventSynchronize(h->up_ev));
     return OQG_OK;
 }

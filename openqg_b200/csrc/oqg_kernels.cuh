@@ -1573,11 +1573,8 @@ __global__ void __launch_bounds__(128) k_ent_rows(const BasinDev *__restrict__ b
 // (pressure.F90:52-54) from the row sums of k_ent_rows, in a fixed order,
 // and the channel strip integrals int_Be_s/n (vorticity.F90:122-128).  One CTA.
 template <class T>
-__global__ void k_forcing_integrals(const BasinDev *__restrict__ bas, int member) {
-    const BasinDev &b = bas[member];
-    __shared__ double red[32];
+__device__ void forcing_integrals_cta(const BasinDev &b, const T *E, double *red) {
     DevForcing *sc = b.frc;
-    const T *E = (const T *)b.ent;
     const size_t n2 = (size_t)b.nyp * b.px;
     double exn = 0.0, s1 = 0.0, s2 = 0.0, n1 = 0.0, n2v = 0.0;
     if (E) {
@@ -1602,6 +1599,30 @@ __global__ void k_forcing_integrals(const BasinDev *__restrict__ bas, int member
     sc->int_Be_s[1] = b.dz_sign * f1 * s2;
     sc->int_Be_n[0] = -b.dz_sign * f2 * n1;
     sc->int_Be_n[1] = -b.dz_sign * f2 * n2v;
+}
+
+// The forcing's integrals (ent_xn; a channel's ent strip integrals) from the
+// descriptor's entrainment, one CTA.
+template <class T>
+__global__ void k_forcing_integrals(const BasinDev *__restrict__ bas, int member) {
+    __shared__ double red[32];
+    const BasinDev &b = bas[member];
+    forcing_integrals_cta<T>(b, (const T *)b.ent, red);
+}
+
+// Whether this CTA is the last of its grid to arrive (a ticket counter that
+// the last one resets): every CTA's global writes before the call are then
+// visible to it.  No CTA waits.
+__device__ __forceinline__ bool last_cta(unsigned *ticket) {
+    __shared__ bool is_last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) is_last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!is_last) return false;
+    __threadfence();
+    if (threadIdx.x == 0) *ticket = 0u;
+    return true;
 }
 
 // Solve-only input: the same (nxp, nyp) right-hand side for every mode.

@@ -150,7 +150,8 @@ __device__ __forceinline__ double oml_t2p(const OmlDev &o, const double *t, doub
 // partial sums of xfo in the same order (deterministic mean).
 template <class T>
 __global__ void __launch_bounds__(128) k_oml_post(OmlDev o, T *wekp, T *ent, double *ent_rows, int px, int nl,
-                                                   int compute_ent, int nparts) {
+                                                   int compute_ent, int nparts, const BasinDev *__restrict__ bas,
+                                                   const T *ent_after, unsigned *ticket) {
     __shared__ double red[32];
     __shared__ double avg;
     if (threadIdx.x < 32) {
@@ -177,6 +178,15 @@ __global__ void __launch_bounds__(128) k_oml_post(OmlDev o, T *wekp, T *ent, dou
     if (compute_ent) {
         rs = block_sum(rs, red);
         if (threadIdx.x == 0) ent_rows[j] = rs;
+    }
+    // the last CTA: the forcing integrals (ent_xn) and a closed box's zero
+    // boundary stress integrals (ekman.F90:60-70)
+    if (!last_cta(ticket)) return;
+    __syncthreads();
+    forcing_integrals_cta<T>(bas[0], ent_after, red);
+    if (threadIdx.x == 0) {
+        bas[0].frc->txis = 0.0;
+        bas[0].frc->txin = 0.0;
     }
 }
 
@@ -444,6 +454,24 @@ __device__ __forceinline__ double aml_t2p(const AmlDev &o, const double *t, int 
     return 0.25 * (T_(i, j) + T_(i - 1, j) + T_(i, j - 1) + T_(i - 1, j - 1));
 }
 
+// The boundary stress integrals of a channel (ekman.F90:60-70):
+// txis = int_P_dx(taux(:,1) + taux(:,2)) / 2, txin likewise at the north.
+__device__ void aml_strips_cta(const AmlDev &o, DevForcing *frc, double *red) {
+    const int nxp = o.nxp;
+    double s = 0.0, n = 0.0;
+    for (int i = threadIdx.x; i < nxp; i += blockDim.x) {
+        const double w = (i == 0 || i == nxp - 1) ? 0.5 : 1.0;
+        s += w * (o.taux[i] + o.taux[(size_t)nxp + i]);
+        n += w * (o.taux[(size_t)(o.nyp - 2) * nxp + i] + o.taux[(size_t)(o.nyp - 1) * nxp + i]);
+    }
+    s = block_sum(s, red);
+    n = block_sum(n, red);
+    if (threadIdx.x == 0) {
+        frc->txis = 0.5 * (s * o.dx);
+        frc->txin = 0.5 * (n * o.dx);
+    }
+}
+
 // The QG forcing from the atmospheric mixed layer, one CTA of 128 threads
 // per p row: wekp = map_T_to_P(wekt) and, when computed, ent(:,:,1) =
 // map_T_to_P(xfa) + sum_k aface(k) eta(k) + bface dtop with eta(k) =
@@ -451,7 +479,9 @@ __device__ __forceinline__ double aml_t2p(const AmlDev &o, const double *t, int 
 // 128-131; amlsubs.F90:308-323), ent(:,:,2:) = 0, and its row sums.
 template <class T>
 __global__ void __launch_bounds__(128) k_aml_post(AmlDev o, const T *__restrict__ PM, T *wekp, T *ent,
-                                                   double *ent_rows, int px, int compute_ent) {
+                                                   double *ent_rows, int px, int compute_ent,
+                                                   const BasinDev *__restrict__ bas, const T *ent_after,
+                                                   unsigned *ticket) {
     __shared__ double red[32];
     const size_t n2 = (size_t)o.nyp * px;
     const int j = blockIdx.x;
@@ -474,6 +504,12 @@ __global__ void __launch_bounds__(128) k_aml_post(AmlDev o, const T *__restrict_
         rs = block_sum(rs, red);
         if (threadIdx.x == 0) ent_rows[j] = rs;
     }
+    // the last CTA: the boundary stress integrals and the forcing integrals
+    if (!last_cta(ticket)) return;
+    __syncthreads();
+    aml_strips_cta(o, bas[0].frc, red);
+    __syncthreads();
+    forcing_integrals_cta<T>(bas[0], ent_after, red);
 }
 
 // The atmosphere's wind stress from its lagged layer-1 pressure (xforc,
@@ -500,24 +536,6 @@ __global__ void __launch_bounds__(256) k_aml_tau(const BasinDev *__restrict__ ba
     }
 }
 
-// The boundary stress integrals of a channel (ekman.F90:60-70):
-// txis = int_P_dx(taux(:,1) + taux(:,2)) / 2, txin likewise at the north.
-__global__ void __launch_bounds__(128) k_aml_strips(AmlDev o, DevForcing *frc) {
-    __shared__ double red[32];
-    const int nxp = o.nxp;
-    double s = 0.0, n = 0.0;
-    for (int i = threadIdx.x; i < nxp; i += blockDim.x) {
-        const double w = (i == 0 || i == nxp - 1) ? 0.5 : 1.0;
-        s += w * (o.taux[i] + o.taux[(size_t)nxp + i]);
-        n += w * (o.taux[(size_t)(o.nyp - 2) * nxp + i] + o.taux[(size_t)(o.nyp - 1) * nxp + i]);
-    }
-    s = block_sum(s, red);
-    n = block_sum(n, red);
-    if (threadIdx.x == 0) {
-        frc->txis = 0.5 * (s * o.dx);
-        frc->txin = 0.5 * (n * o.dx);
-    }
-}
 
 // ------------------------------------------------------ the coupled fluxes
 // compute_forcing's radiation coefficients (radiate_type, radsubs.F90:15-54).
