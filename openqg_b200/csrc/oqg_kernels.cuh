@@ -1572,25 +1572,65 @@ __global__ void __launch_bounds__(128) k_ent_rows(const BasinDev *__restrict__ b
 // Forcing integrals that depend only on ent: ent_xn = int_P_dA(ent(:,:,1))
 // (pressure.F90:52-54) from the row sums of k_ent_rows, in a fixed order,
 // and the channel strip integrals int_Be_s/n (vorticity.F90:122-128).  One CTA.
+// K CTA sums in one pass: the warps' shuffles of the K values interleave and
+// three barriers serve them all.  The result is valid in every thread.
+template <int K>
+__device__ __forceinline__ void block_sum_n(double (&v)[K]) {
+    __shared__ double r[K][32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+        for (int q = 0; q < K; ++q) v[q] += __shfl_down_sync(0xffffffffu, v[q], o);
+    __syncthreads();
+    if (lane == 0)
+#pragma unroll
+        for (int q = 0; q < K; ++q) r[q][wid] = v[q];
+    __syncthreads();
+    if (wid == 0) {
+#pragma unroll
+        for (int q = 0; q < K; ++q) v[q] = lane < nw ? r[q][lane] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+            for (int q = 0; q < K; ++q) v[q] += __shfl_down_sync(0xffffffffu, v[q], o);
+        if (lane == 0)
+#pragma unroll
+            for (int q = 0; q < K; ++q) r[q][0] = v[q];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < K; ++q) v[q] = r[q][0];
+}
+
 template <class T>
 __device__ void forcing_integrals_cta(const BasinDev &b, const T *E, double *red) {
     DevForcing *sc = b.frc;
     const size_t n2 = (size_t)b.nyp * b.px;
-    double exn = 0.0, s1 = 0.0, s2 = 0.0, n1 = 0.0, n2v = 0.0;
+    // ent_rows' trapezoidal sum, and for a channel the trapezoidal x-sums of
+    // ent's rows 0 and nyp-1 in layers 1 and 2 (row_integral), together
+    double v[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
     if (E) {
-        double s = 0.0;
         for (int j = threadIdx.x; j < b.nyp; j += blockDim.x)
-            s += ((j == 0 || j == b.nyp - 1) ? 0.5 : 1.0) * b.ent_rows[j];
-        exn = block_sum(s, red) * b.dx * b.dy;
+            v[0] += ((j == 0 || j == b.nyp - 1) ? 0.5 : 1.0) * b.ent_rows[j];
         if (b.cyclic) {
-            s1 = row_integral(b, E, 0, -1, red);
-            n1 = row_integral(b, E, b.nyp - 1, -1, red);
-            if (b.nl - 1 >= 2) {
-                s2 = row_integral(b, E + n2, 0, -1, red);
-                n2v = row_integral(b, E + n2, b.nyp - 1, -1, red);
+            const size_t last = (size_t)(b.nyp - 1) * b.px;
+            const bool two = b.nl - 1 >= 2;
+            for (int i = threadIdx.x; i < b.nxp; i += blockDim.x) {
+                const double t = trap_x(b, i);
+                v[1] += t * (double)E[i];
+                v[2] += t * (double)E[last + i];
+                if (two) {
+                    v[3] += t * (double)E[n2 + i];
+                    v[4] += t * (double)E[n2 + last + i];
+                }
             }
         }
     }
+    block_sum_n<5>(v);
+    (void)red;
+    const double exn = v[0] * b.dx * b.dy;
+    const double s1 = v[1] * b.dx, n1 = v[2] * b.dx, s2 = v[3] * b.dx, n2v = v[4] * b.dx;
     if (threadIdx.x != 0) return;
     sc->ent_xn = exn;
     for (int k = 0; k < OQG_NLMAX; ++k) { sc->int_Be_s[k] = 0.0; sc->int_Be_n[k] = 0.0; }

@@ -464,11 +464,12 @@ __device__ void aml_strips_cta(const AmlDev &o, DevForcing *frc, double *red) {
         s += w * (o.taux[i] + o.taux[(size_t)nxp + i]);
         n += w * (o.taux[(size_t)(o.nyp - 2) * nxp + i] + o.taux[(size_t)(o.nyp - 1) * nxp + i]);
     }
-    s = block_sum(s, red);
-    n = block_sum(n, red);
+    double v[2] = {s, n};
+    block_sum_n<2>(v);
+    (void)red;
     if (threadIdx.x == 0) {
-        frc->txis = 0.5 * (s * o.dx);
-        frc->txin = 0.5 * (n * o.dx);
+        frc->txis = 0.5 * (v[0] * o.dx);
+        frc->txin = 0.5 * (v[1] * o.dx);
     }
 }
 
