@@ -334,7 +334,9 @@ int oqg_oml_get_sst(oqg_oml *m, double *sst, double *sstm);
  * layer 1/2 entrainment (other layers zero), otherwise ent is kept.
  * Arrays in host or device memory.  taux = tauy = NULL: the stress that
  * oqg_xforc last computed on the device; fnetoc = NULL: the flux that
- * oqg_compute_forcing last computed on the device (zero before the first). */
+ * oqg_compute_forcing last computed on the device (zero before the first).
+ * The call returns once its copies are done; with nothing to copy it returns
+ * without waiting for the device (the work stays queued on the stream). */
 int oqg_ocean_forcing(oqg_oml *m, const double *taux, const double *tauy,
                       const double *fnetoc, int compute_ent, double tdto);
 /* The handle's forcing, wekp (nxp, nyp) and ent (nxp, nyp, nl-1), copied

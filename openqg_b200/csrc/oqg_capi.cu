@@ -1993,7 +1993,10 @@ int oqg_ocean_forcing(oqg_oml *m, const double *taux, const double *tauy, const 
     }
     if (fnetoc)
         CK(cudaMemcpyAsync(const_cast<double *>(o.fnet), fnetoc, nt * sizeof(double), cudaMemcpyDefault, h->st));
-    CK(cudaEventRecord(h->up_ev, h->st));
+    // the caller may reuse its arrays once their copies are done; with
+    // nothing copied the call returns without waiting for the device
+    const bool copies = taux || fnetoc;
+    if (copies) CK(cudaEventRecord(h->up_ev, h->st));
     const void *p1 = b.F[h->par];   // layer 1 of the current p (driver.F90:96-103)
     if (h->mixed) k_oml_step<float><<<OQG_OML_CTAS, 256, 0, h->st>>>(o, (const float *)p1, b.px, tdto, compute_ent);
     else k_oml_step<double><<<OQG_OML_CTAS, 256, 0, h->st>>>(o, (const double *)p1, b.px, tdto, compute_ent);
@@ -2020,7 +2023,7 @@ int oqg_ocean_forcing(oqg_oml *m, const double *taux, const double *tauy, const 
         int rc = push_desc(h);
         if (rc) return rc;
     }
-    CK(cudaEventSynchronize(h->up_ev));
+    if (copies) CK(cudaEventSynchronize(h->up_ev));
     return OQG_OK;
 }
 
@@ -2330,7 +2333,10 @@ int oqg_atmos_forcing(oqg_aml *m, const double *taux, const double *tauy, const 
     }
     if (fnetat)
         CK(cudaMemcpyAsync(const_cast<double *>(o.fnet), fnetat, nt * sizeof(double), cudaMemcpyDefault, h->st));
-    CK(cudaEventRecord(h->up_ev, h->st));
+    // the caller may reuse its arrays once their copies are done; with
+    // nothing copied the call returns without waiting for the device
+    const bool copies = taux || fnetat;
+    if (copies) CK(cudaEventRecord(h->up_ev, h->st));
     const int grid = std::min((int)((nt + 255) / 256), 148 * 8);
     // the entrainment the handle holds after this call; the last CTA of
     // k_aml_post forms txis, txin and the forcing integrals
@@ -2357,7 +2363,7 @@ int oqg_atmos_forcing(oqg_aml *m, const double *taux, const double *tauy, const 
         int rc = push_desc(h);
         if (rc) return rc;
     }
-    CK(cudaEventSynchronize(h->up_ev));
+    if (copies) CK(cudaEventSynchronize(h->up_ev));
     return OQG_OK;
 }
 
