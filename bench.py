@@ -244,7 +244,7 @@ def coupled_e2e(g, b, tdt, msteps, nbatch):
             "timer": "host clock, median of %d steps" % nbatch}
 
 
-def coupled_config(nrep=3, nocean=10, nstr=10):
+def coupled_config(nrep=3, nocean=10, nstr=10, precision=None):
     """The coupled configuration's step loop on the device (dynamic_step,
     driver.F90:33-143): per ocean step, xforc (both basins' wind stress from
     the atmosphere's lagged pressure, the ocean's through the bicubic
@@ -256,14 +256,16 @@ def coupled_config(nrep=3, nocean=10, nstr=10):
     radiation and mixed-layer parameters are the reference's coupled
     double-gyre configuration's (data/basin/atm_dg.cdl, ocn_dg.cdl) through
     the radiative start-up (oqg_radiat and its helpers); the mixed layers
-    start from the radiative-balance profiles (rbal), the QG states from
-    seeded noise.  Host clock over nocean
+    start from the radiative-balance profiles (rbal) with seeded SST noise
+    (std 0.5 K), the QG states from seeded noise.  precision OQG_MIXED: both
+    handles store their state in FP32 (the configuration's FP32-bulk form).  Host clock over nocean
     coupled ocean steps, median of nrep."""
     from openqg_b200.core import QG, AtmosMixedLayer, OceanMixedLayer, lib
-    from openqg_b200.params import atmos_channel, ocean_double_gyre
+    from openqg_b200.params import OQG_FP64, atmos_channel, ocean_double_gyre
     from openqg_b200.radiation import coupled_start, rbal_states
     L = lib()
-    bo, ba = ocean_double_gyre(513, dx=10e3), atmos_channel(193, 97, dx=80e3)
+    prec = OQG_FP64 if precision is None else precision
+    bo, ba = ocean_double_gyre(513, dx=10e3, precision=prec), atmos_channel(193, 97, dx=80e3, precision=prec)
     rad, ak, ok = coupled_start(ba, bo, hm_a=1000.0, fsbar=-210.0, fspamp=80.0, zopt=[200.0, 3.0e4, 3.0e4, 4.0e4],
                                 gamma=1.0e-2, xlamda=35.0, tabsat=[330.0, 340.0, 350.0], rho_a=1.0, cp_a=1.0e3,
                                 t1_abs_o=278.0, t2_abs_o=268.0, rho_o=1.0e3, cp_o=4.0e3)
@@ -275,6 +277,7 @@ def coupled_config(nrep=3, nocean=10, nstr=10):
     oml = OceanMixedLayer(go, hm=100.0, rho_cp=ok["rho_cp"], t1_rel=ok["t1_rel"], dt_12=ok["dt_12"], st2d=380.0,
                           st4d=4.0e10, ycexp=1.0, fluxs=True, sval=ok["sval"], nval=ok["nval"])
     _, sst, ast = rbal_states(ba, bo, rad, ak)
+    sst = sst + 0.5 * np.random.default_rng(5).standard_normal(sst.shape)
     oml.set_sst(sst, sst)
     xc = ak["xc1ast"]
     aml = AtmosMixedLayer(ga, xc, None, hm=1000.0, rho_cp=ak["rho_cp"], t1_rel=ak["t1_rel"], dt_12=ak["dt_12"],
@@ -319,6 +322,7 @@ def coupled_config(nrep=3, nocean=10, nstr=10):
                         "tdt 360 s, %d steps per ocean step); xforc (both stresses, bicubic onto the ocean), "
                         "compute_forcing (both heat fluxes), both mixed layers and Ekman fields on the device, "
                         "nothing from the host in the loop" % nstr,
+            "state_storage": "fp32" if prec != OQG_FP64 else "fp64",
             "ms_per_coupled_ocean_step": ms, "value": cells / (ms / 1e3) / 1e6, "unit": "Mcell-layer-steps/s",
             "timer": "host clock, median of %d runs of %d coupled ocean steps" % (nrep, nocean)}
 
@@ -667,6 +671,7 @@ def run_ours(args):
                                        "cell-layers per step" % (list(ENSEMBLE_SIZES), cells_e))
         # the coupled configuration's step loop with both mixed layers on the device
         variants["coupled_config"] = coupled_config()
+        variants["coupled_config_fp32_bulk"] = coupled_config(precision=OQG_MIXED)
         # the adjoint: reverse pass and adjoint step against the forward step
         variants["adjoint257"] = run_adjoint()
         # the eddy-resolving box: forward + adjoint over 100 steps, checkpoint every 10
