@@ -800,8 +800,11 @@ static int create_impl(const oqg_params *prm, oqg_handle **out, bool batched) {
     const size_t t2 = 2 * h->esz;
     const int npm = (b.ny + 1) / 2;
     h->nv = b.tiles_x * b.tiles_y;
-    // forward transform: one row pair per group, CTAs of >= 256 threads
-    const int GX = std::max(1, 256 / TT);
+    // forward transform: one row pair per group, CTAs of >= 256 threads; a
+    // grid whose row pairs would not fill the SMs that way spreads them over
+    // more, smaller CTAs (each transform is a latency chain of FFT stages)
+    int GX = std::max(1, 256 / TT);
+    if ((b.nl * npm + GX - 1) / GX < 148) GX = std::max(1, std::min(GX, b.nl * npm / 148));
     h->xthreads = GX * TT;
     h->nx = (b.nl * npm + GX - 1) / GX;
     const size_t vsz = (size_t)(b.cyclic ? 16 : 8);
