@@ -123,3 +123,21 @@ def test_rbal_states():
     assert sst[0, 0] == ocn["sval"] and sst[-1, 0] == ocn["nval"]
     assert np.all(sst == sst[:, :1])
     assert np.array_equal(ast, atm["xc1ast"])
+
+
+def test_coupled_start_keywords_fit_the_mixed_layers():
+    """coupled_start's keyword dictionaries are arguments the mixed-layer
+    classes take (checked by signature; no device)."""
+    import inspect
+    from openqg_b200.core import AtmosMixedLayer, OceanMixedLayer
+    from openqg_b200.params import atmos_channel, ocean_double_gyre
+    from openqg_b200.radiation import coupled_start
+    ba, bo = atmos_channel(49, 25, dx=80e3), ocean_double_gyre(129, dx=10e3)
+    _, atm, ocn = coupled_start(ba, bo, hm_a=1000.0, fsbar=-210.0, fspamp=80.0, zopt=[200.0, 3.0e4, 3.0e4, 4.0e4],
+                                gamma=1.0e-2, xlamda=35.0, tabsat=[330.0, 340.0, 350.0], rho_a=1.0, cp_a=1.0e3,
+                                t1_abs_o=278.0, t2_abs_o=268.0, rho_o=1.0e3, cp_o=4.0e3)
+    for cls, kw in ((AtmosMixedLayer, atm), (OceanMixedLayer, ocn)):
+        params = inspect.signature(cls.__init__).parameters
+        assert set(kw) <= set(params), (cls.__name__, set(kw) - set(params))
+    assert atm["xc1ast"].shape == (ba.nyp - 1, ba.nxp - 1)
+    assert len(atm["aface"]) == ba.nl - 1
