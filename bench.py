@@ -91,11 +91,23 @@ def make_ensemble(precision, members=256, seed=0):
     return basins, inputs
 
 
-def run_ensemble(precision, steps, warmup, msteps, flush, tdt=3600.0):
-    """Whole-ensemble Mcell-layer-steps/s (all members, one launch per phase)."""
+def ensemble_shard(n, rank, ws):
+    """The members rank steps when ws ranks share an ensemble of n: every
+    ws-th member from rank (the sizes are drawn independently, so each rank
+    gets a like mix)."""
+    return list(range(rank, n, ws))
+
+
+def run_ensemble(precision, steps, warmup, msteps, flush, tdt=3600.0, rank=0, ws=1):
+    """The ensemble's steps on this rank, one launch per phase: its shard of
+    the members (ensemble_shard), so ws ranks together step the whole
+    ensemble once.  Returns the cell-layers of the whole ensemble, this
+    rank's time and the tile height."""
     import torch
     from openqg_b200.core import Ensemble
-    basins, inputs = make_ensemble(precision)
+    all_basins, all_inputs = make_ensemble(precision)
+    mine = ensemble_shard(len(all_basins), rank, ws)
+    basins, inputs = [all_basins[i] for i in mine], [all_inputs[i] for i in mine]
     e = Ensemble(basins)
     for i, (p, w, ts, tn) in enumerate(inputs):
         e.set_state(i, p, p)
@@ -117,7 +129,7 @@ def run_ensemble(precision, steps, warmup, msteps, flush, tdt=3600.0):
         e1.synchronize()
         total += e0.elapsed_time(e1)
     e.sync()
-    cells = sum(b.nxp * b.nyp * b.nl for b in basins)
+    cells = sum(b.nxp * b.nyp * b.nl for b in all_basins)
     e.close()
     return cells, total, tile_rows
 
@@ -660,15 +672,18 @@ def run_ours(args):
         tm = max_over_ranks(time_batches(gm, tdt, msteps, args.steps, flush), pg, "cuda")
         variants["mixed_fp32_bulk"] = replica_value(tm, ws, cells, msteps, args.steps)
         gm.close()
-        # the batched ensemble: 256 basins of uneven size, one launch per phase
+        # the batched ensemble: 256 basins of uneven size, one launch per phase;
+        # with N ranks each steps every N-th member (no collective), so the
+        # whole ensemble is stepped once per step across the ranks
         for vprec, vname in ((OQG_MIXED, "ensemble256_mixed"), (OQG_FP64, "ensemble256_fp64")):
-            cells_e, te, rows_e = run_ensemble(vprec, args.steps, args.warmup, msteps, flush)
+            cells_e, te, rows_e = run_ensemble(vprec, args.steps, args.warmup, msteps, flush, rank=rank, ws=ws)
             te = max_over_ranks(te, pg, "cuda")
-            variants[vname] = replica_value(te, ws, cells_e, msteps, args.steps)
+            variants[vname] = replica_value(te, 1, cells_e, msteps, args.steps)
             variants[vname + "_tile_rows"] = rows_e
         variants["ensemble_config"] = ("256 ocean 3-layer boxes, sizes uniform in %s, dx 20 km, "
                                        "per-member wind 0.05-0.15 N/m^2 and ah4 1e10-4e10; %d "
-                                       "cell-layers per step" % (list(ENSEMBLE_SIZES), cells_e))
+                                       "cell-layers per step, sharded by member over %d rank(s) "
+                                       "(strong scaling, no collective)" % (list(ENSEMBLE_SIZES), cells_e, ws))
         # the coupled configuration's step loop with both mixed layers on the device
         variants["coupled_config"] = coupled_config()
         variants["coupled_config_fp32_bulk"] = coupled_config(precision=OQG_MIXED)

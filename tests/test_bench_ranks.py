@@ -59,3 +59,16 @@ def test_replica_value_single_rank():
     assert bench.max_over_ranks(3.0, None, "cpu") == 3.0
     assert bench.replica_value(1000.0, 1, 513 * 513 * 3, 10, 5) == pytest.approx(
         513 * 513 * 3 * 50 / 1.0 / 1e6)
+
+
+@pytest.mark.parametrize("ws", [1, 2, 3, 8])
+def test_ensemble_shards_partition_the_members(ws):
+    """N ranks step disjoint shards of the 256-member ensemble whose union is
+    every member, each within one member of the others' counts; the
+    whole-job rate counts the ensemble once (no replica factor)."""
+    import bench
+    shards = [bench.ensemble_shard(256, r, ws) for r in range(ws)]
+    flat = sorted(i for s in shards for i in s)
+    assert flat == list(range(256))
+    assert max(map(len, shards)) - min(map(len, shards)) <= 1
+    assert bench.replica_value(2000.0, 1, 10 ** 6, 10, 4) == pytest.approx(10 ** 6 * 40 / 2.0 / 1e6)
