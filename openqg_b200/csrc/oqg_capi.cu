@@ -2340,17 +2340,18 @@ int oqg_atmos_forcing(oqg_aml *m, const double *taux, const double *tauy, const 
     // nothing copied the call returns without waiting for the device
     const bool copies = taux || fnetat;
     if (copies) CK(cudaEventRecord(h->up_ev, h->st));
-    const int grid = std::min((int)((nt + 255) / 256), 148 * 8);
+    // 128-thread CTAs: a channel's T cells then reach every SM
+    const int grid = std::min((int)((nt + 127) / 128), 148 * 8);
     // the entrainment the handle holds after this call; the last CTA of
     // k_aml_post forms txis, txin and the forcing integrals
     const void *ent_after = compute_ent ? h->ent_buf : b.ent;
     if (h->mixed) {
-        k_aml_step<float><<<grid, 256, 0, h->st>>>(o, (const float *)p1, b.px, tdta, compute_ent);
+        k_aml_step<float><<<grid, 128, 0, h->st>>>(o, (const float *)p1, b.px, tdta, compute_ent);
         k_aml_post<float><<<b.nyp, 128, 0, h->st>>>(o, (const float *)pm, (float *)b.wekp, (float *)h->ent_buf,
                                                     b.ent_rows, b.px, compute_ent, h->d_bas,
                                                     (const float *)ent_after, m->ticket);
     } else {
-        k_aml_step<double><<<grid, 256, 0, h->st>>>(o, (const double *)p1, b.px, tdta, compute_ent);
+        k_aml_step<double><<<grid, 128, 0, h->st>>>(o, (const double *)p1, b.px, tdta, compute_ent);
         k_aml_post<double><<<b.nyp, 128, 0, h->st>>>(o, (const double *)pm, (double *)b.wekp,
                                                      (double *)h->ent_buf, b.ent_rows, b.px, compute_ent, h->d_bas,
                                                      (const double *)ent_after, m->ticket);
