@@ -469,41 +469,61 @@ def dist():
 
 
 def run_reference(args):
-    ws, rank, _ = dist()
+    """The reference arm: the CPU restatement of step_qg (the oracle, FP64,
+    OpenMP on the leapfrog region only, as the reference parallelises it)
+    on the host cores local to the GPU.  It is timed with one thread and
+    with every bound thread; the faster is the line's value, with its thread
+    count (the reference's only parallel region is a small share of the
+    step, so more threads can be slower)."""
+    ws, rank, local = dist()
     if rank != 0:
         return 0
+    numa_cpus = None
+    try:
+        import torch
+        if torch.cuda.is_available():
+            numa_cpus = bind_to_gpu_numa(local)
+    except Exception:
+        pass
     from openqg_b200.params import OQG_FP64
     b, tdt, label = make_basin(args.workload, OQG_FP64)
     p, w, ts, tn = initial_inputs(b, seed=1, reference=True)
     import oracle
     gomp = ctypes.CDLL("libgomp.so.1")
     oracle.lib()
-    threads = os.cpu_count() or 1
-    gomp.omp_set_num_threads(threads)
-    o = oracle.Oracle(b)
-    o.set_state(p, p)
-    o.set_forcing(w, None, ts, tn)
+    allt = len(os.sched_getaffinity(0)) or (os.cpu_count() or 1)
     msteps = args.ref_model_steps
-    for _ in range(args.warmup):
-        o.step(tdt, msteps)
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        o.step(tdt, msteps)
-    el = time.perf_counter() - t0
     cells = b.nxp * b.nyp * b.nl
-    value = cells * msteps * args.steps / el / 1e6
+    runs = {}
+    for threads in sorted({1, allt}):
+        gomp.omp_set_num_threads(threads)
+        o = oracle.Oracle(b)
+        o.set_state(p, p)
+        o.set_forcing(w, None, ts, tn)
+        for _ in range(args.warmup):
+            o.step(tdt, msteps)
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            o.step(tdt, msteps)
+        el = time.perf_counter() - t0
+        o.close()
+        runs[threads] = (cells * msteps * args.steps / el / 1e6, el)
+    threads = max(runs, key=lambda t: runs[t][0])
+    value, el = runs[threads]
     line = {
         "impl": "reference", "metric": "Mcell-layer-steps/s", "value": value,
         "unit": "Mcell-layer-steps/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": el * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": label, "nxp": b.nxp, "nyp": b.nyp, "nl": b.nl,
-                   "model_steps_per_step": msteps, "parallelism": "single process"},
+                   "model_steps_per_step": msteps, "tdt_s": tdt, "parallelism": "single process"},
         "cpu_baseline": {"value": value, "unit": "Mcell-layer-steps/s", "cores": threads,
                          "kind": "port",
                          "sample": "%d x %d model steps of the %s basin (FP64 C++ restatement of the "
-                                   "Fortran step_qg, OpenMP on the leapfrog region only)"
-                                   % (args.steps, msteps, args.workload)},
+                                   "Fortran step_qg, OpenMP on the leapfrog region only), the faster of "
+                                   "1 and %d threads" % (args.steps, msteps, args.workload, allt),
+                         "by_threads": {str(t): v[0] for t, v in sorted(runs.items())},
+                         "host_cpus_bound": numa_cpus},
         "e2e": {"value": value, "unit": "Mcell-layer-steps/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -571,6 +591,114 @@ def time_batches(g, tdt, msteps, steps, flush):
     return total
 
 
+PHASES = ["k_vort", "k_xfwd", "k_ysolve", "k_xinv"]
+
+
+def phase_alg_bytes(s, nl):
+    """Algorithmic bytes per cell-layer of each step phase (s: bytes per
+    state word)."""
+    return {
+        # reads p, q, pm, qm (+ wekp once per column of layers); writes q, modal rhs
+        "k_vort": 6 * s + s / nl,
+        # reads the modal rhs, writes its transform
+        "k_xfwd": 2 * s,
+        # reads and writes the spectral field (+ FP64 pivots, not counted)
+        "k_ysolve": 2 * s,
+        # reads the spectral field, p (old) and the homogeneous solutions, writes p
+        "k_xinv": 3 * s + s * (nl - 1) / nl,
+    }
+
+
+def roofline_of(g, b, workload, precision, tdt, ms_per_model_step):
+    """The dominant phase timed alone (oqg_profile_phases: CUDA events around
+    each kernel of 20 steps) against the HBM roofline, and the whole step's
+    algorithmic bytes over its timed duration."""
+    from openqg_b200.params import OQG_FP64
+    ms = g.profile_phases(tdt, 20)
+    dom = int(np.argmax(ms))
+    s = 8 if b.precision == OQG_FP64 else 4
+    cells = b.nxp * b.nyp * b.nl
+    alg = phase_alg_bytes(s, b.nl)
+    peak, peak_kind = peaks()
+    dname = PHASES[dom]
+    achieved = alg[dname] * cells / (ms[dom] / 1e3) / 1e9
+    step_alg = (6 * s + s / b.nl) * cells
+    tt = traffic_table().get((workload, precision, dname))
+    return {"bound": "hbm", "kernel": dname, "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "peak_kind": peak_kind,
+            "traffic": tt, "alg_bytes_per_launch": alg[dname] * cells,
+            "phase_ms": dict(zip(PHASES, [float(x) for x in ms])),
+            "step_alg_bytes": step_alg,
+            # the whole step: algorithmic bytes over the timed model step
+            "step_frac": step_alg / (ms_per_model_step / 1e3) / 1e9 / peak,
+            # the phases timed one by one, summed
+            "phases_frac": step_alg / (sum(ms) / 1e3) / 1e9 / peak}
+
+
+def measure_basin(workload, prec, steps, warmup, msteps, flush, rank, pg, seed=None):
+    """Device throughput of one basin: autotuned tiles, `warmup` untimed
+    batches, then `steps` batches of msteps model steps, each after an L2
+    flush; the time is the max over ranks.  Returns the handle (open), the
+    basin, its inputs and the figures."""
+    from openqg_b200.core import QG
+    b, tdt, label = make_basin(workload, prec)
+    p, w, ts, tn = initial_inputs(b, seed=(1 + rank) if seed is None else seed)
+    g = QG(b)
+    g.set_state(p, p)
+    g.set_forcing(w, None, ts, tn)
+    # the vorticity tile height, measured on this GPU (oqg_autotune)
+    tile_rows, tune_ms = g.autotune(tdt, 20)
+    for _ in range(warmup):
+        g.step(tdt, msteps)
+    g.sync()
+    if g.check_finite() != 0:
+        raise RuntimeError("non-finite state after warm-up (%s)" % workload)
+    if pg:
+        pg.barrier()
+    total_ms = max_over_ranks(time_batches(g, tdt, msteps, steps, flush), pg, "cuda")
+    cells = b.nxp * b.nyp * b.nl
+    return g, b, (p, w, ts, tn), {
+        "workload": label, "tdt_s": tdt, "label": label, "total_ms": total_ms,
+        "ms_per_model_step": total_ms / (steps * msteps), "cells": cells,
+        "tile_rows": tile_rows, "autotune_ms_per_step": {str(k): round(v, 5) for k, v in tune_ms.items()},
+    }
+
+
+def config_line(workload, prec, steps, warmup, msteps, flush, rank, ws, pg, note=""):
+    """A whole-configuration figure with its own roofline (a variant of the
+    bench line)."""
+    from openqg_b200.params import OQG_FP64
+    g, b, _, m = measure_basin(workload, prec, steps, warmup, msteps, flush, rank, pg)
+    pname = "fp64" if prec == OQG_FP64 else "mixed"
+    roof = roofline_of(g, b, workload, pname, m["tdt_s"], m["ms_per_model_step"])
+    g.close()
+    return {"workload": m["label"] + note, "precision": pname, "tdt_s": m["tdt_s"],
+            "model_steps_per_step": msteps, "steps": steps,
+            "value": replica_value(m["total_ms"], ws, m["cells"], msteps, steps),
+            "unit": "Mcell-layer-steps/s", "ms_per_model_step": m["ms_per_model_step"],
+            "tile_rows": m["tile_rows"], "roofline": roof,
+            "l2": "flushed (256 MiB write) before every timed step of %d model steps" % msteps}
+
+
+def e2e_breakdown(g, b, L, wk_p, ent_p, p1_p, ts, tn, tdt, reps=20):
+    """Host-clock medians of the three parts of an exchanged model step:
+    the forcing upload (oqg_set_forcing, which returns once the copies have
+    read the host arrays), the step alone, and the read-back of p(:,:,1)."""
+    def med(fn):
+        ts_ = []
+        for _ in range(reps):
+            g.sync()
+            t0 = time.perf_counter()
+            fn()
+            g.sync()
+            ts_.append((time.perf_counter() - t0) * 1e3)
+        return statistics.median(ts_)
+    up = med(lambda: L.oqg_set_forcing(g.h, wk_p, ent_p, ts, tn))
+    st = med(lambda: L.oqg_step(g.h, tdt, 1))
+    rd = med(lambda: L.oqg_get_p_layer(g.h, 0, p1_p))
+    return {"upload_ms": up, "step_ms": st, "readback_ms": rd}
+
+
 def run_ours(args):
     import torch
     ws, rank, local = dist()
@@ -583,24 +711,11 @@ def run_ours(args):
         td.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                               device_id=torch.device("cuda", local))
         pg = td
-    from openqg_b200.core import QG, lib
+    from openqg_b200.core import lib
     from openqg_b200.params import OQG_FP64, OQG_MIXED
     prec = OQG_MIXED if args.precision == "mixed" else OQG_FP64
-    b, tdt, label = make_basin(args.workload, prec)
-    p, w, ts, tn = initial_inputs(b, seed=1 + rank)
     msteps = args.model_steps
-    cells = b.nxp * b.nyp * b.nl
-    g = QG(b)
-    g.set_state(p, p)
-    g.set_forcing(w, None, ts, tn)
-    # the vorticity tile height, measured on this GPU (oqg_autotune)
-    tile_rows, tune_ms = g.autotune(tdt, 20)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")   # 256 MiB > L2
-    for _ in range(args.warmup):
-        g.step(tdt, msteps)
-    g.sync()
-    if g.check_finite() != 0:
-        raise RuntimeError("non-finite state after warm-up")
 
     def barrier():
         if pg:
@@ -614,9 +729,11 @@ def run_ours(args):
         pass
     barrier()
     with Clocks(uuid) as clk:
-        total_ms = time_batches(g, tdt, msteps, args.steps, flush)
+        g, b, (p, w, ts, tn), m = measure_basin(args.workload, prec, args.steps, args.warmup, msteps, flush,
+                                                rank, pg)
         barrier()
-    total_ms = max_over_ranks(total_ms, pg, "cuda")
+    tdt, label, cells = m["tdt_s"], m["label"], m["cells"]
+    total_ms = m["total_ms"]
     value = replica_value(total_ms, ws, cells, msteps, args.steps)
 
     # e2e through the C ABI with pinned host buffers
@@ -652,26 +769,30 @@ def run_ours(args):
         e2e_times.append((time.perf_counter() - t0) * 1e3)
     e2e_ms = max_over_ranks(statistics.median(e2e_times) * e2e_steps, pg, "cuda")
     e2e_value = replica_value(e2e_ms, ws, cells, msteps, e2e_steps)
+    e2e_parts = e2e_breakdown(g, b, L, wk_p, ent_p, p1_p, ts, tn, tdt)
     h2d = msteps * (b.nxp * b.nyp * 8) * b.nl        # wekp + (nl-1) ent layers
     d2h = msteps * b.nxp * b.nyp * 8
     coupled = None
     if prec == OQG_FP64 and not b.cyclic:
         coupled = coupled_e2e(g, b, tdt, msteps, e2e_steps)
 
-    # variant: the same basin with FP32 bulk arithmetic
+    # the dominant kernel, timed alone, against the HBM roofline
+    g.set_forcing(w, None, ts, tn)
+    roof = roofline_of(g, b, args.workload, args.precision, tdt, m["ms_per_model_step"])
+
     variants = {}
     if args.variants and prec == OQG_FP64:
-        bm, _, _ = make_basin(args.workload, OQG_MIXED)
-        gm = QG(bm)
-        gm.set_state(p, p)
-        gm.set_forcing(w, None, ts, tn)
-        gm.autotune(tdt, 20)
-        for _ in range(args.warmup):
-            gm.step(tdt, msteps)
-        barrier()
-        tm = max_over_ranks(time_batches(gm, tdt, msteps, args.steps, flush), pg, "cuda")
-        variants["mixed_fp32_bulk"] = replica_value(tm, ws, cells, msteps, args.steps)
-        gm.close()
+        # the same basin with FP32 bulk arithmetic
+        variants["mixed_fp32_bulk"] = config_line(args.workload, OQG_MIXED, args.steps, args.warmup, msteps,
+                                                  flush, rank, ws, pg)
+        # the plain configuration: 129x129x3, dx 20 km, 480 leapfrog steps
+        # (one bench step is the whole run)
+        variants["config0_ocean129_480steps"] = config_line("ocean129", OQG_FP64, 3, args.warmup, 480, flush,
+                                                            rank, ws, pg)
+        # the eddy-resolving box, FP64 and FP32 bulk
+        for vprec, vname in ((OQG_FP64, "ocean2049_fp64"), (OQG_MIXED, "ocean2049_mixed")):
+            variants[vname] = config_line("ocean2049", vprec, max(3, args.steps // 2), args.warmup, msteps,
+                                          flush, rank, ws, pg)
         # the batched ensemble: 256 basins of uneven size, one launch per phase;
         # with N ranks each steps every N-th member (no collective), so the
         # whole ensemble is stepped once per step across the ranks
@@ -690,36 +811,8 @@ def run_ours(args):
         # the adjoint: reverse pass and adjoint step against the forward step
         variants["adjoint257"] = run_adjoint()
         # the eddy-resolving box: forward + adjoint over 100 steps, checkpoint every 10
-        dx, ah4, tdt = ADJOINT_BOXES[2049]
-        variants["adjoint2049"] = run_adjoint(reps=1, n=2049, dx=dx, ah4=ah4, nsteps=100, every=10, tdt=tdt)
-
-    # dominant kernel, timed alone, against the HBM roofline
-    g.set_forcing(w, None, ts, tn)
-    ms = g.profile_phases(tdt, 20)
-    names = ["k_vort", "k_xfwd", "k_ysolve", "k_xinv"]
-    dom = int(np.argmax(ms))
-    s = 8 if prec == OQG_FP64 else 4
-    # algorithmic bytes per cell-layer of each phase
-    alg = {
-        # reads p, q, pm, qm (+ wekp once per column of layers); writes q, modal rhs
-        "k_vort": 6 * s + s / b.nl,
-        # reads the modal rhs, writes its transform
-        "k_xfwd": 2 * s,
-        # reads and writes the spectral field (+ FP64 pivots, not counted)
-        "k_ysolve": 2 * s,
-        # reads the spectral field, p (old) and the homogeneous solutions, writes p
-        "k_xinv": 3 * s + s * (b.nl - 1) / b.nl,
-    }
-    peak, peak_kind = peaks()
-    dname = names[dom]
-    achieved = alg[dname] * cells / (ms[dom] / 1e3) / 1e9
-    step_alg = (6 * s + s / b.nl) * cells
-    tt = traffic_table().get((args.workload, args.precision, dname))
-    roof = {"bound": "hbm", "kernel": dname, "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": achieved / peak, "peak_kind": peak_kind,
-            "traffic": tt, "alg_bytes_per_launch": alg[dname] * cells,
-            "phase_ms": dict(zip(names, [float(x) for x in ms])),
-            "step_frac": step_alg / (sum(ms) / 1e3) / 1e9 / peak}
+        adx, aah4, atdt = ADJOINT_BOXES[2049]
+        variants["adjoint2049"] = run_adjoint(reps=1, n=2049, dx=adx, ah4=aah4, nsteps=100, every=10, tdt=atdt)
 
     line = {
         "metric": "Mcell-layer-steps/s", "value": value, "unit": "Mcell-layer-steps/s",
@@ -729,16 +822,17 @@ def run_ours(args):
         "data": "synthetic",
         "config": {"workload": label, "nxp": b.nxp, "nyp": b.nyp, "nl": b.nl,
                    "model_steps_per_step": msteps, "tdt_s": tdt,
-                   "tile_rows": tile_rows,
-                   "autotune_ms_per_step": {str(k): round(v, 5) for k, v in tune_ms.items()},
-                   "l2": "flushed (256 MiB write) before every timed step",
+                   "tile_rows": m["tile_rows"],
+                   "autotune_ms_per_step": m["autotune_ms_per_step"],
+                   "l2": "flushed (256 MiB write) before every timed step of %d model steps" % msteps,
                    "parallelism": "replicas" if ws > 1 else "single basin"},
         "roofline": roof,
         "e2e": {"value": e2e_value, "unit": "Mcell-layer-steps/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "timer": "host clock, median of %d steps" % e2e_steps,
-                "pattern": "per model step: upload wekp+ent, step, read p(:,:,1)"},
+                "pattern": "per model step: upload wekp+ent, step, read p(:,:,1)",
+                "parts_ms_per_model_step": e2e_parts},
         "e2e_coupled_ocean": coupled,
-        "gpu_launches": args.steps * msteps * 4,
+        "gpu_launches": args.steps * msteps * launches_per_step(g),
         "host_cpus_bound": numa_cpus,
         "clocks": clk.summary(),
         "variants": variants,
@@ -757,6 +851,11 @@ def run_ours(args):
         pg.barrier()
         pg.destroy_process_group()
     return 0
+
+
+def launches_per_step(g):
+    """Kernel launches of one model step of the handle's step path."""
+    return 4
 
 
 def main():

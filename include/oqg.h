@@ -138,8 +138,19 @@ int oqg_get_step_index(oqg_handle *h, long long *steps_done);
 /* suppress_comp_mode (driver.F90:174-189) applied once, now. */
 int oqg_suppress(oqg_handle *h);
 
-/* Waits for the handle's stream; reports a deferred device error. */
+/* Waits for the handle's stream; reports a deferred device error and clears
+ * it: OQG_ETIMEOUT when a bounded device wait ran out (that step's results
+ * are invalid; set the state again before stepping on), OQG_ECUDA for any
+ * other device error.  No counterpart in the reference (its step cannot
+ * fail: errors abort with stop 1, util/linalg.F90:130-134). */
 int oqg_sync(oqg_handle *h);
+
+/* Test hook of the failure detection (no counterpart in the reference): the
+ * number of polls a kernel's first wait for a tile load makes before it
+ * reports a timeout.  polls = 0 makes every such wait run out at once (the
+ * kernel then drains its copies in flight with the full limit, sets the
+ * error word and returns); polls < 0 restores the default, 2^22. */
+int oqg_set_wait_limit(oqg_handle *h, long long polls);
 
 /* Device validity scan of p and q (the role of valids, valsubs.F90:46-139):
  * *bad = number of non-finite values found. */

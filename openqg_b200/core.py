@@ -58,6 +58,7 @@ def lib():
     L.oqg_get_step_index.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
     L.oqg_suppress.argtypes = [vp]
     L.oqg_sync.argtypes = [vp]
+    L.oqg_set_wait_limit.argtypes = [vp, ctypes.c_longlong]
     L.oqg_check_finite.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
     L.oqg_diag.argtypes = [vp, _dp, _dp, _dp, _dp]
     L.oqg_diag_noalloc.argtypes = [vp, _dp, _dp, _dp, _dp]

@@ -695,6 +695,7 @@ static int create_impl(const oqg_params *prm, oqg_handle **out, bool batched) {
         b.tiles_y = (P.nyp + b.vty - 1) / b.vty;
     }
     b.kt = P.k_topo - 1;
+    b.wait_limit = OQG_WAIT_LIMIT;
     b.dz_sign = P.dz_sign; b.tau_sign = P.tau_sign;
     b.suppress_period = P.suppress_period;
     b.dx = P.dx; b.dy = P.dy; b.fnot = P.fnot; b.beta = P.beta;
@@ -1097,12 +1098,33 @@ int oqg_suppress(oqg_handle *h) {
     return OQG_OK;
 }
 
+// Reads and clears the device error word of a basin after its stream has
+// drained: a timeout of a bounded wait is OQG_ETIMEOUT, any other bit
+// OQG_ECUDA.  `who` names the basin in the message.
+static int take_device_error(const BasinDev &b, const std::string &who) {
+    int err = 0;
+    CK(cudaMemcpy(&err, b.err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (!err) return OQG_OK;
+    CK(cudaMemset(b.err, 0, sizeof(int)));
+    if (err & OQG_DERR_TIMEOUT)
+        return fail(OQG_ETIMEOUT, "a bounded device wait ran out" + who + "; the step's results are invalid");
+    return fail(OQG_ECUDA, "device error flag set" + who);
+}
+
 int oqg_sync(oqg_handle *h) {
     if (!h) return fail(OQG_EINVAL, "null handle");
     CK(cudaStreamSynchronize(h->st));
-    int err = 0;
-    CK(cudaMemcpy(&err, h->hb.err, sizeof(int), cudaMemcpyDeviceToHost));
-    if (err) return fail(OQG_ECUDA, "device error flag set");
+    return take_device_error(h->hb, "");
+}
+
+int oqg_set_wait_limit(oqg_handle *h, long long polls) {
+    if (!h) return fail(OQG_EINVAL, "null handle");
+    const unsigned v = polls < 0 ? OQG_WAIT_LIMIT : (unsigned)std::min<long long>(polls, OQG_WAIT_LIMIT);
+    h->hb.wait_limit = v;
+    h->hb64.wait_limit = v;
+    int rc = push_desc(h);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(h->st));
     return OQG_OK;
 }
 
@@ -1658,9 +1680,8 @@ int oqg_ensemble_sync(oqg_ensemble *e) {
     if (!e) return fail(OQG_EINVAL, "null ensemble");
     CK(cudaStreamSynchronize(e->st));
     for (size_t i = 0; i < e->m.size(); ++i) {
-        int err = 0;
-        CK(cudaMemcpy(&err, e->m[i]->hb.err, sizeof(int), cudaMemcpyDeviceToHost));
-        if (err) return fail(OQG_ECUDA, "device error flag set in member " + std::to_string(i));
+        int rc = take_device_error(e->m[i]->hb, " in member " + std::to_string(i));
+        if (rc) return rc;
     }
     return OQG_OK;
 }

@@ -102,6 +102,8 @@ struct BasinDev {
     int k4_rows;                // interior rows per CTA of the assembly launch
     double tdt_m;               // leapfrog step of this member when a launch
                                 // passes tdt = 0 (ensembles: one per member)
+    unsigned wait_limit;        // polls of a first wait for a tile load before
+                                // it reports a timeout (drains use the full limit)
 };
 
 // Division of ints in [0, 2^31) by a divisor d >= 1 fixed for a loop, by a

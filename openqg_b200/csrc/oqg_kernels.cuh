@@ -316,7 +316,7 @@ k_vort(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par,
             // one thread polls the barrier; the CTA barrier then publishes
             // the tile to the others without spinning warps taking issue slots
             bool ok = true;
-            if (threadIdx.x == 0) ok = mbar_wait_bounded(&bars[k & 1], (k >> 1) & 1, OQG_WAIT_LIMIT);
+            if (threadIdx.x == 0) ok = mbar_wait_bounded(&bars[k & 1], (k >> 1) & 1, b.wait_limit);
             if (__syncthreads_or(!ok)) {
                 // a tile never arrived: report, drain what is in flight, stop
                 if (threadIdx.x == 0) {

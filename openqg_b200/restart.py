@@ -9,6 +9,12 @@ attribute, and a restart sets p and pm only: q, qm and the constraints are
 recomputed from them (init_pv and init_mass_constr / init_constraint, as
 init_dynamic_state does, openqg.F90:233-243).
 
+`save_oml` / `restart_oml` and `save_aml` / `restart_aml` are the mixed
+layers' restart files (state.F90:46-80, 114-178): dimensions nxt, nyt, the
+T-point coordinates x, y in km, and sst, sstm (ocean) or ast, astm, hmixa,
+hmixam (atmosphere), each (nyt, nxt) in netCDF order.  `restart_*_into`
+loads one into a device mixed layer.
+
 `save_state` / `restore_state` go further: every field of the device state
 (p, pm, q, qm, the mass and momentum constraints and the step index), so a
 restored handle continues bit for bit.  They use numpy's .npz format.
@@ -72,6 +78,82 @@ def restart_into(path: str, qg) -> None:
     """Reads a reference restart file into a device handle: set_state(p, pm)."""
     p, pm = restart_qg(path, qg.b)
     qg.set_state(p, pm)
+
+
+def _tcoords(b: Basin, x0: float = 0.0, y0: float = 0.0):
+    """T-point coordinates in km: xt(i) = xp(i) + dx/2 (box.F90:145-160)."""
+    xt = x0 + (np.arange(b.nxp - 1) + 0.5) * b.dx
+    yt = y0 + (np.arange(b.nyp - 1) + 0.5) * b.dy
+    return xt * 1.0e-3, yt * 1.0e-3
+
+
+def _save_t_fields(path: str, b: Basin, fields, x0: float, y0: float) -> None:
+    tshape = (b.nyp - 1, b.nxp - 1)
+    x, y = _tcoords(b, x0, y0)
+    f = netcdf_file(path, "w", version=1)
+    try:
+        f.createDimension("nxt", tshape[1])
+        f.createDimension("nyt", tshape[0])
+        vx = f.createVariable("x", "d", ("nxt",))
+        vx.units = "km"
+        vy = f.createVariable("y", "d", ("nyt",))
+        vy.units = "km"
+        vx[:] = x
+        vy[:] = y
+        for name, desc, a in fields:
+            v = f.createVariable(name, "d", ("nyt", "nxt"))
+            v.units = desc
+            v[:] = np.asarray(a, dtype=np.float64).reshape(tshape)
+    finally:
+        f.close()
+
+
+def _read_t_fields(path: str, b: Basin, names):
+    tshape = (b.nyp - 1, b.nxp - 1)
+    f = netcdf_file(path, "r", mmap=False)
+    try:
+        shape = (f.dimensions["nyt"], f.dimensions["nxt"])
+        if tuple(shape) != tshape:
+            raise ValueError("restart T grid %s does not match the basin's %s" % (shape, tshape))
+        return [np.array(f.variables[n][:], dtype=np.float64) for n in names]
+    finally:
+        f.close()
+
+
+def save_oml(path: str, b: Basin, sst, sstm, x0: float = 0.0, y0: float = 0.0) -> None:
+    """save_oml (state.F90:114-143): the ocean mixed layer's temperature at
+    the current and previous level, T grid (nyt, nxt)."""
+    _save_t_fields(path, b, [("sst", "Current mixed layer temp", sst),
+                             ("sstm", "Previous mixed layer temp", sstm)], x0, y0)
+
+
+def restart_oml(path: str, b: Basin):
+    """restart_oml (state.F90:46-61): returns (sst, sstm)."""
+    return tuple(_read_t_fields(path, b, ("sst", "sstm")))
+
+
+def save_aml(path: str, b: Basin, ast, astm, hmixa, hmixam, x0: float = 0.0, y0: float = 0.0) -> None:
+    """save_aml (state.F90:145-178): the atmospheric mixed layer's
+    temperature and height at the current and previous level."""
+    _save_t_fields(path, b, [("ast", "Current mixed layer temp", ast),
+                             ("astm", "Previous mixed layer temp", astm),
+                             ("hmixa", "Current mixed layer height", hmixa),
+                             ("hmixam", "Previous mixed layer height", hmixam)], x0, y0)
+
+
+def restart_aml(path: str, b: Basin):
+    """restart_aml (state.F90:63-80): returns (ast, astm, hmixa, hmixam)."""
+    return tuple(_read_t_fields(path, b, ("ast", "astm", "hmixa", "hmixam")))
+
+
+def restart_oml_into(path: str, oml) -> None:
+    """Reads an ocean mixed-layer restart file into a device mixed layer."""
+    oml.set_sst(*restart_oml(path, oml.qg.b))
+
+
+def restart_aml_into(path: str, aml) -> None:
+    """Reads an atmospheric mixed-layer restart file into a device mixed layer."""
+    aml.set_state(*restart_aml(path, aml.qg.b))
 
 
 def save_state(path: str, qg) -> None:

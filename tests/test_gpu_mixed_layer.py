@@ -389,21 +389,23 @@ def test_coupled_fluxes_match_oracle(topography, source):
         c[k].close()
 
 
-@pytest.mark.parametrize("precision,tol", [(0, 1e-11), (OQG_MIXED, 1e-5)])
-def test_coupled_exchange_matches_oracle(precision, tol):
-    """Three ocean steps of the coupled driver (driver.F90:33-143) with two
+@pytest.mark.parametrize("precision,tol,nocean", [(0, 1e-11, 3), (OQG_MIXED, 1e-5, 3), (OQG_MIXED, 1e-5, 10)],
+                         ids=["fp64_3", "mixed_3", "mixed_10"])
+def test_coupled_exchange_matches_oracle(precision, tol, nocean):
+    """Ocean steps of the coupled driver (driver.F90:33-143) with two
     atmosphere steps each, every exchange on the device: xforc (both
     stresses), compute_forcing (both fluxes), the mixed layers and QG steps
     of both basins; against the restatements and the C++ oracle's FP64 QG
-    steps.  FP64 handles within 1e-11; FP32 state storage (OQG_MIXED, the
-    coupled configuration's FP32-bulk form) within 1e-5."""
+    steps.  FP64 handles within 1e-11 after 3 ocean steps; FP32 state
+    storage (OQG_MIXED, the coupled configuration's FP32-bulk form) within
+    1e-5 after 3 and after the configuration's 10 coupled ocean steps."""
     c = _coupled_pair(seed=13, precision=precision)
     ba, b, aprm, prm = c["ba"], c["b"], c["aprm"], c["prm"]
     ga, qa, aml, oa, g, qo, m, oo = (c[k] for k in ("ga", "qa", "aml", "oa", "g", "qo", "m", "oo"))
     enta = np.zeros((ba.nl - 1,) + ba.shape2)
     ento = np.zeros((b.nl - 1,) + b.shape2)
     nstr = 2
-    for _ in range(3):
+    for _ in range(nocean):
         # the oracle's ocean step
         pma = qa.get_state()[1]
         tax, tay = atmos_stress(pma[0], ba, 1.3e-3, aprm.hm)

@@ -7,7 +7,7 @@ import pytest
 from scipy.io import netcdf_file
 
 from openqg_b200.params import atmos_channel, double_gyre_tau, initial_psi, ocean_double_gyre
-from openqg_b200.restart import restart_qg, save_qg
+from openqg_b200.restart import restart_aml, restart_oml, restart_qg, save_aml, save_oml, save_qg
 
 
 def test_save_qg_writes_the_reference_layout(tmp_path):
@@ -35,6 +35,37 @@ def test_restart_rejects_another_grid(tmp_path):
     save_qg(path, b, np.zeros(b.shape3), np.zeros(b.shape3))
     with pytest.raises(ValueError):
         restart_qg(path, atmos_channel(97, 65))
+
+
+def test_mixed_layer_restarts_round_trip(tmp_path):
+    """save_oml / restart_oml and save_aml / restart_aml (state.F90:46-80,
+    114-178): T-grid dimensions nxt, nyt, the reference's variable names and
+    descriptions, exact round trips."""
+    rng = np.random.default_rng(3)
+    bo, ba = ocean_double_gyre(33), atmos_channel(49, 25)
+    to, ta = (bo.nyp - 1, bo.nxp - 1), (ba.nyp - 1, ba.nxp - 1)
+    sst, sstm = rng.standard_normal(to), rng.standard_normal(to)
+    po = os.path.join(tmp_path, "oml.nc")
+    save_oml(po, bo, sst, sstm)
+    f = netcdf_file(po, "r", mmap=False)
+    assert f.dimensions == {"nxt": 32, "nyt": 32}
+    assert f.variables["sst"].dimensions == ("nyt", "nxt")
+    assert f.variables["sstm"].units == b"Previous mixed layer temp"
+    assert np.allclose(f.variables["x"][:], (np.arange(32) + 0.5) * bo.dx * 1e-3)
+    f.close()
+    a, am = restart_oml(po, bo)
+    assert np.array_equal(a, sst) and np.array_equal(am, sstm)
+    fa = [rng.standard_normal(ta) for _ in range(4)]
+    pa = os.path.join(tmp_path, "aml.nc")
+    save_aml(pa, ba, *fa)
+    f = netcdf_file(pa, "r", mmap=False)
+    assert sorted(f.variables) == ["ast", "astm", "hmixa", "hmixam", "x", "y"]
+    assert f.variables["hmixa"].units == b"Current mixed layer height"
+    f.close()
+    for got, want in zip(restart_aml(pa, ba), fa):
+        assert np.array_equal(got, want)
+    with pytest.raises(ValueError):
+        restart_oml(po, ocean_double_gyre(65))
 
 
 @pytest.mark.gpu
