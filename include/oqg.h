@@ -228,6 +228,11 @@ int oqg_diagno(oqg_handle *h, const double *taux, const double *tauy, double tse
 int oqg_valids(oqg_handle *h, double pext, double qext, double wext, double *ext,
                long long *nonfinite, int *ok);
 
+/* int_P_dA (numerics.F90:165-204): the trapezoid-rule area integral of a
+ * field (nxp, nyp) on the basin's grid, computed on the device with the
+ * compensated summation the step's mass-constraint and area integrals use. */
+int oqg_int_P_dA(oqg_handle *h, const double *field, double *out);
+
 /* solve_inhomog_eqn (inhomog.F90:156-168): (Del^2 - rdm2(m)) out = rhs with
  * out = 0 on solid boundaries; m is the 1-based mode; rhs, out (nxp, nyp). */
 int oqg_solve_inhomog(oqg_handle *h, int m, const double *rhs, double *out);

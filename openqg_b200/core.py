@@ -66,6 +66,7 @@ def lib():
                              ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_int)]
     L.oqg_diagno.argtypes = [vp, _dp, _dp, ctypes.c_double, ctypes.c_double, ctypes.POINTER(QgMonitor)]
     L.oqg_solve_inhomog.argtypes = [vp, ctypes.c_int, _dp, _dp]
+    L.oqg_int_P_dA.argtypes = [vp, _dp, _dp]
     L.oqg_generate_homog_soln.argtypes = [vp, ctypes.c_int, _dp, _dp]
     L.oqg_get_modes.argtypes = [vp, _dp, _dp, _dp, _dp]
     L.oqg_ekman_from_tau.argtypes = [vp, _dp, _dp, _dp, _dp, _dp]
@@ -276,6 +277,14 @@ class QG:
         out = np.empty(self.b.shape2)
         _check(lib().oqg_solve_inhomog(self.h, int(m), _p(rhs), _p(out)), "oqg_solve_inhomog")
         return out
+
+    def int_P_dA(self, f) -> float:
+        """int_P_dA (numerics.F90:165-204) of a (nyp, nxp) field, on the
+        device with compensated summation."""
+        f = _f64(f, self.b.shape2)
+        out = np.empty(1)
+        _check(lib().oqg_int_P_dA(self.h, _p(f), _p(out)), "oqg_int_P_dA")
+        return float(out[0])
 
     def generate_homog_soln(self, m: int, L):
         L = _f64(L, self.b.shape2)

@@ -782,10 +782,10 @@ static int create_impl(const oqg_params *prm, oqg_handle **out, bool batched) {
     }
     // sized for the shortest tiles (8 rows), so oqg_autotune can retile in place
     b.part_tile = dalloc<double>(h, (size_t)b.tiles_x * ((P.nyp + 7) / 8) * b.nl * OQG_NQ);
-    b.part_col = dalloc<double>(h, (size_t)b.nl * b.nk);
+    b.part_col = dalloc<double>(h, 2 * (size_t)b.nl * b.nk);
     b.st = dalloc<DevState>(h, 2);
     b.frc = dalloc<DevForcing>(h, 1);
-    b.ent_rows = dalloc<double>(h, b.nyp);
+    b.ent_rows = dalloc<double>(h, 2 * (size_t)b.nyp);
     b.err = dalloc<int>(h, 1);
     h->stage[0] = dalloc<double>(h, n3);
     h->stage[1] = dalloc<double>(h, n3);
@@ -1301,6 +1301,17 @@ int oqg_solve_inhomog(oqg_handle *h, int m, const double *rhs, double *out) {
     if ((rc = solve_all_modes(h))) return rc;
     rc = download3(h, h->stage[1] + (m - 1) * n2, out, 1);
     if (rc) return rc;
+    CK(cudaStreamSynchronize(h->st));
+    return OQG_OK;
+}
+
+int oqg_int_P_dA(oqg_handle *h, const double *field, double *out) {
+    if (!h || !field || !out) return fail(OQG_EINVAL, "bad argument");
+    int rc = upload3(h, field, h->stage[0], 1);
+    if (rc) return rc;
+    k_area_integral<<<1, 512, 0, h->st>>>(h->d_bas64, 0, h->stage[0], h->d_diag);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(out, h->d_diag, sizeof(double), cudaMemcpyDeviceToHost, h->st));
     CK(cudaStreamSynchronize(h->st));
     return OQG_OK;
 }

@@ -92,10 +92,12 @@ struct BasinDev {
     const double *hbt;          // channel: [nyp] barotropic homogeneous solution
     const double *hbc1, *hbc2;  // channel: [nl][nyp]
     double *part_tile;          // [tiles][nl][OQG_NQ]
-    double *part_col;           // [y-solve CTAs]: dst_w-weighted column sums
+    double *part_col;           // [y-solve CTAs][2]: dst_w-weighted column sums and
+                                // their compensations
     DevState *st;               // [2] by step parity
     DevForcing *frc;
-    double *ent_rows;           // [nyp] row sums of the ent area integral
+    double *ent_rows;           // [nyp][2] row sums of the ent area integral and their
+                                // compensations
     void *inh_g;                // wide grids: modal rows of k_xinv, [nl][nyp][px] (8-byte slots)
     int *err;                   // device error bits
     // launch bookkeeping

@@ -64,6 +64,74 @@ __device__ __forceinline__ double block_sum(double v, double *red) {
     return s;
 }
 
+// ------------------------------------------------------------------ compensated sums
+// The mass-constraint and area integrals (int_P_dA, numerics.F90:165-204;
+// box_homog's modal integrals, homog.F90:331-366) are summed with a running
+// compensation: every addition is Knuth's error-free TwoSum, s + e = a + b
+// exactly, and the rounding errors are summed beside the sum (Neumaier's
+// scheme), so the result is correct to about one rounding of the total
+// whatever the cancellation among the terms.  Nothing here is contracted
+// into FMAs (no products).
+__device__ __forceinline__ void two_sum(double a, double b, double &s, double &e) {
+    s = a + b;
+    const double bb = s - a;
+    e = (a - (s - bb)) + (b - bb);
+}
+struct CSum {
+    double s = 0.0, c = 0.0;
+    __device__ __forceinline__ void add(double x) {
+        double t, e;
+        two_sum(s, x, t, e);
+        s = t;
+        c += e;
+    }
+    // another compensated sum (its sum and its compensation)
+    __device__ __forceinline__ void merge(double os, double oc) {
+        add(os);
+        c += oc;
+    }
+    // the exact product w * x of a weight and a term, added (the product's
+    // rounding error comes from an FMA)
+    __device__ __forceinline__ void add_prod(double w, double x) {
+        const double p = w * x;
+        add(p);
+        c += fma(w, x, -p);
+    }
+    __device__ __forceinline__ double value() const { return s + c; }
+};
+// Warp reduction of compensated sums; the total is in lane 0 (all lanes
+// with full=true).
+__device__ __forceinline__ CSum csum_warp(CSum v, bool full = false) {
+    for (int o = 16; o > 0; o >>= 1) {
+        const double os = full ? __shfl_xor_sync(0xffffffffu, v.s, o) : __shfl_down_sync(0xffffffffu, v.s, o);
+        const double oc = full ? __shfl_xor_sync(0xffffffffu, v.c, o) : __shfl_down_sync(0xffffffffu, v.c, o);
+        v.merge(os, oc);
+    }
+    return v;
+}
+// CTA reduction of compensated sums: the total as a compensated pair, valid
+// in every thread.  red: >= 64 doubles of shared memory.
+__device__ __forceinline__ CSum csum_block_pair(CSum v, double *red) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+    v = csum_warp(v);
+    __syncthreads();
+    if (lane == 0) { red[wid] = v.s; red[32 + wid] = v.c; }
+    __syncthreads();
+    if (wid == 0) {
+        CSum t;
+        if (lane < nw) { t.s = red[lane]; t.c = red[32 + lane]; }
+        t = csum_warp(t);
+        if (lane == 0) { red[0] = t.s; red[1] = t.c; }
+    }
+    __syncthreads();
+    CSum r;
+    r.s = red[0];
+    r.c = red[1];
+    __syncthreads();
+    return r;
+}
+__device__ __forceinline__ double csum_block(CSum v, double *red) { return csum_block_pair(v, red).value(); }
+
 // ------------------------------------------------------------------ k_vort
 #define VTX 60          // output columns of a vorticity tile
 #define VTYMAX 17       // output rows of a vorticity tile (at most)
@@ -670,7 +738,7 @@ __device__ __forceinline__ double yt_re(double2 v) { return v.x; }
 template <class V, int SM>
 __device__ __forceinline__ void ysolve_chunk_regs(V *col, const double *__restrict__ piv, int plen, double a,
                                                   int lane, int s, int n,
-                                                  int o, int ny, double &colsum) {
+                                                  int o, int ny, CSum &colsum) {
     V x[SM];
     double bt[SM];
 #pragma unroll
@@ -723,7 +791,7 @@ __device__ __forceinline__ void ysolve_chunk_regs(V *col, const double *__restri
             const double ej = (s + t == ny - 1) ? 0.0 : -a * bt[t];
             uu = yt_axpy(x[t], ej, uu);
             x[t] = uu;
-            colsum += yt_re(uu);
+            colsum.add(yt_re(uu));
         }
 #pragma unroll
     for (int t = 0; t < SM; ++t)
@@ -779,14 +847,14 @@ k_ysolve(const BasinDev *__restrict__ bas, const Work *__restrict__ work) {
     }
     __syncthreads();
 
-    double wsum = 0.0;                          // dst_w-weighted column sum (box)
+    CSum wsum;                                  // dst_w-weighted column sum (box)
     if (live) {
         const double a = b.a_tri;
         V *col = tile + c * LD;
         const int s = lane * S_, e = min(s + S_, ny);
         const int o = lane * (S_ + 1);          // padded offset of row s
         const int n = max(e - s, 0);
-        double colsum = 0.0;
+        CSum colsum;
         if (S_ <= YREG) ysolve_chunk_regs<V, YREG>(col, piv, plen, a, lane, s, n, o, ny, colsum);
         else {
             // forward elimination: u_j = f_j beta_j - a beta_j u_{j-1}
@@ -832,10 +900,15 @@ k_ysolve(const BasinDev *__restrict__ bas, const Work *__restrict__ work) {
                 const double ej = (s + t == ny - 1) ? 0.0 : -a * __ldg(piv + min(s + t, plen - 1));
                 uu = yt_axpy(col[o + t], ej, uu);
                 col[o + t] = uu;
-                colsum += yt_re(uu);
+                colsum.add(yt_re(uu));
             }
         }
-        if (!CPLX) wsum = b.dst_w[k] * warp_sum(colsum);
+        if (!CPLX) {
+            const CSum cw = csum_warp(colsum);
+            const double wk = b.dst_w[k];
+            wsum.add_prod(wk, cw.s);
+            wsum.add_prod(wk, cw.c);
+        }
     }
     __syncthreads();
     for (int i0 = threadIdx.x; i0 < ny * KB; i0 += 128 * CH) {
@@ -850,15 +923,17 @@ k_ysolve(const BasinDev *__restrict__ bas, const Work *__restrict__ work) {
         }
     }
     if (!CPLX) {
-        // one dst_w-weighted partial per CTA, summed in a fixed order
-        __shared__ double wpart[KB];
-        if (lane == 0) wpart[c] = wsum;
+        // one dst_w-weighted compensated partial (sum, compensation) per
+        // CTA, summed in a fixed order
+        __shared__ double wpart[2 * KB];
+        if (lane == 0) { wpart[c] = wsum.s; wpart[KB + c] = wsum.c; }
         __syncthreads();
         if (threadIdx.x == 0) {
-            double t = 0.0;
+            CSum t;
 #pragma unroll
-            for (int x = 0; x < KB; ++x) t += wpart[x];
-            b.part_col[w.block] = t;
+            for (int x = 0; x < KB; ++x) t.merge(wpart[x], wpart[KB + x]);
+            b.part_col[2 * w.block] = t.s;
+            b.part_col[2 * w.block + 1] = t.c;
         }
     }
 }
@@ -957,11 +1032,11 @@ __device__ __noinline__ void scalar_phase(const BasinDev &b, double tdt, int par
         const int nkb = (b.nk + 3) / 4;       // y-solve CTAs per mode (4 columns each)
 #pragma unroll
         for (int m = 0; m < NL; ++m) {
-            double s = 0.0;
+            CSum s;
 #pragma unroll 4
-            for (int x = lane; x < nkb; x += 32) s += b.part_col[m * nkb + x];
-            s = warp_sum(s);
-            imode[m] = __shfl_sync(0xffffffffu, s, 0) * b.ftnorm * b.dx * b.dy;
+            for (int x = lane; x < nkb; x += 32) s.merge(b.part_col[2 * (m * nkb + x)], b.part_col[2 * (m * nkb + x) + 1]);
+            s = csum_warp(s, true);
+            imode[m] = s.value() * b.ftnorm * b.dx * b.dy;
         }
     } else {
         // strip sums over the tiles touching rows 0, 1, nyp-2, nyp-1: per
@@ -1480,25 +1555,34 @@ __device__ __forceinline__ double trap_x(const BasinDev &b, int i) {
     return (i == 0 || i == b.nxp - 1) ? 0.5 : 1.0;
 }
 
+// int_P_dA (numerics.F90:165-204), compensated; red: >= 64 doubles.
 template <class T>
 __device__ double area_integral(const BasinDev &b, const T *f, double *red) {
-    double s = 0.0;
+    CSum s;
     for (int idx = threadIdx.x; idx < b.nyp * b.nxp; idx += blockDim.x) {
         int j = idx / b.nxp, i = idx - j * b.nxp;
-        s += trap_w(b, i, j) * (double)f[(size_t)j * b.px + i];
+        s.add(trap_w(b, i, j) * (double)f[(size_t)j * b.px + i]);
     }
-    return block_sum(s, red) * b.dx * b.dy;
+    return csum_block(s, red) * b.dx * b.dy;
 }
-// int_P_dx of row ja of f minus row jb (jb < 0: no subtraction)
+// int_P_dx of row ja of f minus row jb (jb < 0: no subtraction), compensated
 template <class T>
 __device__ double row_integral(const BasinDev &b, const T *f, int ja, int jb, double *red) {
-    double s = 0.0;
+    CSum s;
     for (int i = threadIdx.x; i < b.nxp; i += blockDim.x) {
         double v = (double)f[(size_t)ja * b.px + i];
         if (jb >= 0) v -= (double)f[(size_t)jb * b.px + i];
-        s += trap_x(b, i) * v;
+        s.add(trap_x(b, i) * v);
     }
-    return block_sum(s, red) * b.dx;
+    return csum_block(s, red) * b.dx;
+}
+
+// int_P_dA of one FP64 field [nyp][px] into out[0] (one CTA): the integral
+// the mass constraint uses, exposed for tests of its compensation.
+__global__ void k_area_integral(const BasinDev *__restrict__ bas, int member, const double *f, double *out) {
+    __shared__ double red[64];
+    const double v = area_integral(bas[member], f, red);
+    if (threadIdx.x == 0) out[0] = v;
 }
 
 // init_mass_constr (constraint.F90:145-165) and, for a channel,
@@ -1506,7 +1590,7 @@ __device__ double row_integral(const BasinDev &b, const T *f, int ja, int jb, do
 template <class T, int NL>
 __global__ void k_init_constraints(const BasinDev *__restrict__ bas, int member, int par) {
     const BasinDev &b = bas[member];
-    __shared__ double red[32];
+    __shared__ double red[64];
     __shared__ double ip[OQG_NLMAX], ipm[OQG_NLMAX], pins[OQG_NLMAX], pinn[OQG_NLMAX],
         pinsp[OQG_NLMAX], pinnp[OQG_NLMAX], cs[OQG_NLMAX], cn[OQG_NLMAX], csp[OQG_NLMAX],
         cnp[OQG_NLMAX];
@@ -1557,16 +1641,17 @@ __global__ void k_init_constraints(const BasinDev *__restrict__ bas, int member,
 }
 
 // Row sums of the ent area integral (int_P_dA, numerics.F90:165-204): one
-// CTA per row j writes sum_i trap_x(i) ent(i, j, 1) to ent_rows[j].
+// CTA per row j writes sum_i trap_x(i) ent(i, j, 1) to ent_rows[2j] with its
+// compensation in ent_rows[2j+1].
 template <class T>
 __global__ void __launch_bounds__(128) k_ent_rows(const BasinDev *__restrict__ bas, int member) {
     const BasinDev &b = bas[member];
-    __shared__ double red[32];
+    __shared__ double red[64];
     const T *E = (const T *)b.ent + (size_t)blockIdx.x * b.px;
-    double s = 0.0;
-    for (int i = threadIdx.x; i < b.nxp; i += blockDim.x) s += trap_x(b, i) * (double)E[i];
-    s = block_sum(s, red);
-    if (threadIdx.x == 0) b.ent_rows[blockIdx.x] = s;
+    CSum s;
+    for (int i = threadIdx.x; i < b.nxp; i += blockDim.x) s.add(trap_x(b, i) * (double)E[i]);
+    const CSum t = csum_block_pair(s, red);
+    if (threadIdx.x == 0) { b.ent_rows[2 * blockIdx.x] = t.s; b.ent_rows[2 * blockIdx.x + 1] = t.c; }
 }
 
 // Forcing integrals that depend only on ent: ent_xn = int_P_dA(ent(:,:,1))
@@ -1609,26 +1694,30 @@ __device__ void forcing_integrals_cta(const BasinDev &b, const T *E, double *red
     const size_t n2 = (size_t)b.nyp * b.px;
     // ent_rows' trapezoidal sum, and for a channel the trapezoidal x-sums of
     // ent's rows 0 and nyp-1 in layers 1 and 2 (row_integral), together
-    double v[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    // (compensated: the mass constraint's area integral, numerics.F90:165-204)
+    CSum cv[5];
     if (E) {
-        for (int j = threadIdx.x; j < b.nyp; j += blockDim.x)
-            v[0] += ((j == 0 || j == b.nyp - 1) ? 0.5 : 1.0) * b.ent_rows[j];
+        for (int j = threadIdx.x; j < b.nyp; j += blockDim.x) {
+            const double wj = (j == 0 || j == b.nyp - 1) ? 0.5 : 1.0;   // exact scaling
+            cv[0].merge(wj * b.ent_rows[2 * j], wj * b.ent_rows[2 * j + 1]);
+        }
         if (b.cyclic) {
             const size_t last = (size_t)(b.nyp - 1) * b.px;
             const bool two = b.nl - 1 >= 2;
             for (int i = threadIdx.x; i < b.nxp; i += blockDim.x) {
                 const double t = trap_x(b, i);
-                v[1] += t * (double)E[i];
-                v[2] += t * (double)E[last + i];
+                cv[1].add(t * (double)E[i]);
+                cv[2].add(t * (double)E[last + i]);
                 if (two) {
-                    v[3] += t * (double)E[n2 + i];
-                    v[4] += t * (double)E[n2 + last + i];
+                    cv[3].add(t * (double)E[n2 + i]);
+                    cv[4].add(t * (double)E[n2 + last + i]);
                 }
             }
         }
     }
-    block_sum_n<5>(v);
-    (void)red;
+    double v[5];
+#pragma unroll
+    for (int q = 0; q < 5; ++q) v[q] = csum_block(cv[q], red);
     const double exn = v[0] * b.dx * b.dy;
     const double s1 = v[1] * b.dx, n1 = v[2] * b.dx, s2 = v[3] * b.dx, n2v = v[4] * b.dx;
     if (threadIdx.x != 0) return;
@@ -1645,7 +1734,7 @@ __device__ void forcing_integrals_cta(const BasinDev &b, const T *E, double *red
 // descriptor's entrainment, one CTA.
 template <class T>
 __global__ void k_forcing_integrals(const BasinDev *__restrict__ bas, int member) {
-    __shared__ double red[32];
+    __shared__ double red[64];
     const BasinDev &b = bas[member];
     forcing_integrals_cta<T>(b, (const T *)b.ent, red);
 }

@@ -152,7 +152,7 @@ template <class T>
 __global__ void __launch_bounds__(128) k_oml_post(OmlDev o, T *wekp, T *ent, double *ent_rows, int px, int nl,
                                                    int compute_ent, int nparts, const BasinDev *__restrict__ bas,
                                                    const T *ent_after, unsigned *ticket) {
-    __shared__ double red[32];
+    __shared__ double red[64];
     __shared__ double avg;
     if (threadIdx.x < 32) {
         double s = 0.0;
@@ -164,20 +164,20 @@ __global__ void __launch_bounds__(128) k_oml_post(OmlDev o, T *wekp, T *ent, dou
     __syncthreads();
     const size_t n2 = (size_t)o.nyp * px;
     const int j = blockIdx.x;
-    double rs = 0.0;
+    CSum rs;
     for (int i = threadIdx.x; i < o.nxp; i += blockDim.x) {
         const size_t op = (size_t)j * px + i;
         wekp[op] = (T)oml_t2p(o, o.wekt, 0.0, i, j);
         if (compute_ent) {
             const T v = (T)oml_t2p(o, o.xfo, avg, i, j);
             ent[op] = v;
-            rs += ((i == 0 || i == o.nxp - 1) ? 0.5 : 1.0) * (double)v;
+            rs.add(((i == 0 || i == o.nxp - 1) ? 0.5 : 1.0) * (double)v);
             for (int k = 1; k < nl - 1; ++k) ent[k * n2 + op] = (T)0;
         }
     }
     if (compute_ent) {
-        rs = block_sum(rs, red);
-        if (threadIdx.x == 0) ent_rows[j] = rs;
+        const CSum t = csum_block_pair(rs, red);
+        if (threadIdx.x == 0) { ent_rows[2 * j] = t.s; ent_rows[2 * j + 1] = t.c; }
     }
     // the last CTA: the forcing integrals (ent_xn) and a closed box's zero
     // boundary stress integrals (ekman.F90:60-70)
@@ -483,10 +483,10 @@ __global__ void __launch_bounds__(128) k_aml_post(AmlDev o, const T *__restrict_
                                                    double *ent_rows, int px, int compute_ent,
                                                    const BasinDev *__restrict__ bas, const T *ent_after,
                                                    unsigned *ticket) {
-    __shared__ double red[32];
+    __shared__ double red[64];
     const size_t n2 = (size_t)o.nyp * px;
     const int j = blockIdx.x;
-    double rs = 0.0;
+    CSum rs;
     for (int i = threadIdx.x; i < o.nxp; i += blockDim.x) {
         const size_t op = (size_t)j * px + i;
         wekp[op] = (T)aml_t2p(o, o.wekt, i, j);
@@ -497,13 +497,13 @@ __global__ void __launch_bounds__(128) k_aml_post(AmlDev o, const T *__restrict_
             e1 = e1 + o.bface * (o.dtop ? o.dtop[(size_t)j * o.nxp + i] : 0.0);
             const T v = (T)e1;
             ent[op] = v;
-            rs += ((i == 0 || i == o.nxp - 1) ? 0.5 : 1.0) * (double)v;
+            rs.add(((i == 0 || i == o.nxp - 1) ? 0.5 : 1.0) * (double)v);
             for (int k = 1; k < o.nl - 1; ++k) ent[k * n2 + op] = (T)0;
         }
     }
     if (compute_ent) {
-        rs = block_sum(rs, red);
-        if (threadIdx.x == 0) ent_rows[j] = rs;
+        const CSum t = csum_block_pair(rs, red);
+        if (threadIdx.x == 0) { ent_rows[2 * j] = t.s; ent_rows[2 * j + 1] = t.c; }
     }
     // the last CTA: the boundary stress integrals and the forcing integrals
     if (!last_cta(ticket)) return;
