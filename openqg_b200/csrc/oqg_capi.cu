@@ -796,15 +796,16 @@ static int create_impl(const oqg_params *prm, oqg_handle **out, bool batched) {
     CK(cudaMemcpy(d_yp, yp.data(), yp.size() * sizeof(double), cudaMemcpyHostToDevice));
 
     // ---- launch geometry
-    h->E = b.M <= 2048 ? 8 : 16;
+    // 16 values per transform thread: one radix-16 butterfly per stage
+    h->E = 16;
     const int TT = (b.M + h->E - 1) / h->E;
     const size_t t2 = 2 * h->esz;
     const int npm = (b.ny + 1) / 2;
     h->nv = b.tiles_x * b.tiles_y;
-    // forward transform: one row pair per group, CTAs of >= 256 threads; a
+    // forward transform: one row pair per group, CTAs of >= 128 threads; a
     // grid whose row pairs would not fill the SMs that way spreads them over
     // more, smaller CTAs (each transform is a latency chain of FFT stages)
-    int GX = std::max(1, 256 / TT);
+    int GX = std::max(1, 128 / TT);
     if ((b.nl * npm + GX - 1) / GX < 148) GX = std::max(1, std::min(GX, b.nl * npm / 148));
     h->xthreads = GX * TT;
     h->nx = (b.nl * npm + GX - 1) / GX;

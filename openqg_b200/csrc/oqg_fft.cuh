@@ -4,9 +4,10 @@
 // FFTW RODFT00 for the closed box, r2c/c2r for the channel) run as complex
 // FFTs of length M over rows staged in shared memory.  Two real rows share one
 // complex transform (real and imaginary parts).  The algorithm is the Stockham
-// autosort FFT (decimation in time, e^{-2 pi i jk/M}), radices 8, 4, 2, 3 and
-// 5, ping-ponging between two shared buffers of M complex values per
-// transform.  A CTA holds G transforms; TT threads serve one transform.
+// autosort FFT (decimation in time, e^{-2 pi i jk/M}), radices 16, 8, 4, 2, 3
+// and 5, ping-ponging between two shared buffers of M complex values per
+// transform.  A CTA holds G transforms; TT threads serve one transform.  The
+// lengths of the configurations' grids run compile-time plans (fft_run).
 #pragma once
 
 #include "oqg_dev.cuh"
@@ -36,6 +37,8 @@ template <> struct FftConst<double> {
     static __device__ __forceinline__ double c52() { return -0.80901699437494742410; }
     static __device__ __forceinline__ double s51() { return 0.95105651629515357212; }
     static __device__ __forceinline__ double s52() { return 0.58778525229247312917; }
+    static __device__ __forceinline__ double c16() { return 0.92387953251128675613; }
+    static __device__ __forceinline__ double s16() { return 0.38268343236508977173; }
 };
 template <> struct FftConst<float> {
     static __device__ __forceinline__ float s3() { return 0.86602540378443864676f; }
@@ -44,6 +47,8 @@ template <> struct FftConst<float> {
     static __device__ __forceinline__ float c52() { return -0.80901699437494742410f; }
     static __device__ __forceinline__ float s51() { return 0.95105651629515357212f; }
     static __device__ __forceinline__ float s52() { return 0.58778525229247312917f; }
+    static __device__ __forceinline__ float c16() { return 0.92387953251128675613f; }
+    static __device__ __forceinline__ float s16() { return 0.38268343236508977173f; }
 };
 
 // In-register forward DFT of size R.
@@ -138,6 +143,49 @@ template <class T> struct Dft<T, 5> {
     }
 };
 
+// 16-point DFT as 4 x 4 (decimation in time, n = 4 n1 + n2, k = k1 + 4 k2):
+// length-4 DFTs over n1, the twiddles W16^(n2 k1), length-4 DFTs over n2.
+template <class T> struct Dft<T, 16> {
+    typedef typename C2<T>::t T2;
+    // z * W16^e for the e the 4 x 4 split needs: W16^e = exp(-2 pi i e / 16)
+    template <int E> static __device__ __forceinline__ T2 w16(T2 z) {
+        const T c = FftConst<T>::c16(), s = FftConst<T>::s16(), h = FftConst<T>::h2();
+        T2 r;
+        if (E == 1) { r.x = c * z.x + s * z.y; r.y = c * z.y - s * z.x; }          // (c - i s)
+        else if (E == 2) { r.x = h * (z.x + z.y); r.y = h * (z.y - z.x); }          // (h - i h)
+        else if (E == 3) { r.x = s * z.x + c * z.y; r.y = s * z.y - c * z.x; }      // (s - i c)
+        else if (E == 6) { r.x = h * (z.y - z.x); r.y = -h * (z.x + z.y); }         // (-h - i h)
+        else { r.x = -(c * z.x + s * z.y); r.y = s * z.x - c * z.y; }               // E == 9: (-c + i s)
+        return r;
+    }
+    static __device__ __forceinline__ void run(T2 *v) {
+        T2 a[4][4];
+#pragma unroll
+        for (int n2 = 0; n2 < 4; ++n2) {
+            T2 t[4] = {v[n2], v[4 + n2], v[8 + n2], v[12 + n2]};
+            Dft<T, 4>::run(t);
+#pragma unroll
+            for (int k1 = 0; k1 < 4; ++k1) a[n2][k1] = t[k1];
+        }
+        a[1][1] = w16<1>(a[1][1]);
+        a[1][2] = w16<2>(a[1][2]);
+        a[1][3] = w16<3>(a[1][3]);
+        a[2][1] = w16<2>(a[2][1]);
+        a[2][2] = c_mi(a[2][2]);
+        a[2][3] = w16<6>(a[2][3]);
+        a[3][1] = w16<3>(a[3][1]);
+        a[3][2] = w16<6>(a[3][2]);
+        a[3][3] = w16<9>(a[3][3]);
+#pragma unroll
+        for (int k1 = 0; k1 < 4; ++k1) {
+            T2 t[4] = {a[0][k1], a[1][k1], a[2][k1], a[3][k1]};
+            Dft<T, 4>::run(t);
+#pragma unroll
+            for (int k2 = 0; k2 < 4; ++k2) v[k1 + 4 * k2] = t[k2];
+        }
+    }
+};
+
 // Shared work buffers hold element i at fpad(i) = i + i/8: with one pad per 8
 // complex values the stride-R stores of the early Stockham stages and the
 // unit-stride loads both spread over all banks.
@@ -212,6 +260,7 @@ __device__ typename C2<T>::t *fft_smem(typename C2<T>::t *a, typename C2<T>::t *
         FastDiv fd;
         if (lg < 0) fd = FastDiv(Ns);
         switch (R) {
+            case 16: fft_stage<T, 16>(src, dst, M, Ns, lg, fd, tws, t, TT); break;
             case 8: fft_stage<T, 8>(src, dst, M, Ns, lg, fd, tws, t, TT); break;
             case 4: fft_stage<T, 4>(src, dst, M, Ns, lg, fd, tws, t, TT); break;
             case 2: fft_stage<T, 2>(src, dst, M, Ns, lg, fd, tws, t, TT); break;
@@ -224,6 +273,89 @@ __device__ typename C2<T>::t *fft_smem(typename C2<T>::t *a, typename C2<T>::t *
     }
     return src;
 }
+
+// ---- compile-time plans for the common transform lengths.  The radix after
+// span Ns of a length-M transform follows the host's fft_radices rule
+// (16 while it divides, then 8, 4, 2, then 3 and 5), so the per-stage
+// twiddle tables are the same for both paths.
+__host__ __device__ constexpr int fft_next_radix(int rem) {
+    return rem % 16 == 0 ? 16 : rem % 8 == 0 ? 8 : rem % 4 == 0 ? 4 : rem % 2 == 0 ? 2
+         : rem % 3 == 0 ? 3 : rem % 5 == 0 ? 5 : 0;
+}
+
+// One Stockham stage with every size known at compile time: the loop over
+// a thread's butterflies unrolls and the index arithmetic folds to shifts
+// and constants.
+template <class T, int R, int Ns, int M, int TT>
+__device__ __forceinline__ void fft_stage_ct(const typename C2<T>::t *__restrict__ src,
+                                             typename C2<T>::t *__restrict__ dst,
+                                             const typename C2<T>::t *__restrict__ tws, int t) {
+    typedef typename C2<T>::t T2;
+    constexpr int nb = M / R;
+#pragma unroll
+    for (int j0 = 0; j0 < nb; j0 += TT) {
+        const int j = j0 + t;
+        if (nb % TT == 0 || j < nb) {
+            const int q = j / Ns, jm = j - q * Ns;
+            T2 v[R];
+#pragma unroll
+            for (int r = 0; r < R; ++r) v[r] = src[fpad(j + r * nb)];
+            if (Ns > 1 && jm != 0) {
+                const T2 *w = tws + jm * (R - 1);
+#pragma unroll
+                for (int r = 1; r < R; ++r) v[r] = c_mul(v[r], __ldg(w + r - 1));
+            }
+            Dft<T, R>::run(v);
+            const int d = q * Ns * R + jm;
+#pragma unroll
+            for (int r = 0; r < R; ++r) dst[fpad(d + r * Ns)] = v[r];
+        }
+    }
+}
+
+// The stages from span Ns on; returns the buffer holding the result.  Threads
+// with live = false only take part in the barriers.
+template <class T, int M, int TT, int Ns>
+__device__ __forceinline__ typename C2<T>::t *fft_ct_from(typename C2<T>::t *src, typename C2<T>::t *dst,
+                                                         const typename C2<T>::t *__restrict__ tw, int t,
+                                                         bool live, int bar_id, int nbar) {
+    if constexpr (Ns >= M) {
+        return src;
+    } else {
+        constexpr int R = fft_next_radix(M / Ns);
+        static_assert(R > 1, "transform length must factor into 2, 3 and 5");
+        if (live) fft_stage_ct<T, R, Ns, M, TT>(src, dst, tw + (Ns - 1), t);
+        bar_sync(bar_id, nbar);
+        return fft_ct_from<T, M, TT, Ns * R>(dst, src, tw, t, live, bar_id, nbar);
+    }
+}
+
+// Forward FFT of length M by groups of TT = M / E threads: the compile-time
+// stages for the lengths of the configurations' grids, the general stages
+// otherwise.  Same contract as fft_smem (t >= TT: barriers only).
+#define OQG_FFT_CT(MM)                                                                                      \
+    case MM:                                                                                                \
+        if constexpr ((MM) % E == 0) return fft_ct_from<T, MM, (MM) / E, 1>(a, b, tw, t, t < TT, bar_id, nbar); \
+        break;
+template <class T, int E>
+__device__ __forceinline__ typename C2<T>::t *fft_run(typename C2<T>::t *a, typename C2<T>::t *b, int M,
+                                                      const int *rad, int nrad,
+                                                      const typename C2<T>::t *__restrict__ tw, int t, int TT,
+                                                      int bar_id, int nbar) {
+    switch (M) {
+        OQG_FFT_CT(128)
+        OQG_FFT_CT(192)
+        OQG_FFT_CT(256)
+        OQG_FFT_CT(384)
+        OQG_FFT_CT(512)
+        OQG_FFT_CT(1024)
+        OQG_FFT_CT(2048)
+        OQG_FFT_CT(4096)
+        default: break;
+    }
+    return fft_smem<T>(a, b, M, rad, nrad, tw, t, TT, bar_id, nbar);
+}
+#undef OQG_FFT_CT
 
 // 16-byte cp.async of n bytes (n a multiple of 16, both addresses 16-byte
 // aligned) by threads t < TT.

@@ -614,7 +614,7 @@ k_vort(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par,
 __host__ __device__ __forceinline__ int round16(int bytes) { return (bytes + 15) & ~15; }
 
 template <class T, int E>
-__global__ void __launch_bounds__(256, 3)
+__global__ void __launch_bounds__(256, 2)
 k_xfwd(const BasinDev *__restrict__ bas, const Work *__restrict__ work, const void *rhs_override) {
     typedef typename C2<T>::t T2;
     const Work w = work[blockIdx.x];
@@ -665,7 +665,7 @@ k_xfwd(const BasinDev *__restrict__ bas, const Work *__restrict__ work, const vo
         }
     }
     __syncthreads();
-    T2 *z = fft_smem<T>(za, zb, M, b.rad, b.nrad, (const T2 *)b.tw, live ? t : TT, TT, 0, 0);
+    T2 *z = fft_run<T, E>(za, zb, M, b.rad, b.nrad, (const T2 *)b.tw, live ? t : TT, TT, 0, 0);
     if (!live) return;
     if (!b.cyclic) {
         T *S = (T *)b.spec;
@@ -1204,7 +1204,7 @@ __device__ __forceinline__ void xinv_rows(const BasinDev &b, int rb, int &jlo, i
 // (FP64, [nl][nyp][px]) and nothing else (no scalar phase).
 // tdt = 0: each member steps with its own b.tdt_m (ensemble launches).
 template <class T, int NL>
-__global__ void __maxnreg__(96)
+__global__ void __maxnreg__(112)
 k_xinv(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par, double tdt, double *out) {
     typedef typename C2<T>::t T2;
     const Work w = work[blockIdx.x];
@@ -1305,7 +1305,7 @@ k_xinv(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par,
             }
         }
         bar_sync(1, nfft);
-        T2 *z = fft_smem<T>(za, zb, M, b.rad, b.nrad, (const T2 *)b.tw, live ? t : TT, TT, 1, nfft);
+        T2 *z = fft_run<T, XINV_E>(za, zb, M, b.rad, b.nrad, (const T2 *)b.tw, live ? t : TT, TT, 1, nfft);
         if (alias) {
             // set B is free now: clear it for the modal rows
             for (int idx = threadIdx.x; idx < NL * nra * nxp; idx += nfft) inh[idx] = (T)0;

@@ -162,6 +162,7 @@ void setup_pivots(bool cyclic, int nxp, int nyp, double dx, double dy,
 bool fft_radices(int M, std::vector<int> &rad) {
     rad.clear();
     int m = M;
+    while (m % 16 == 0) { rad.push_back(16); m /= 16; }
     while (m % 8 == 0) { rad.push_back(8); m /= 8; }
     while (m % 4 == 0) { rad.push_back(4); m /= 4; }
     while (m % 2 == 0) { rad.push_back(2); m /= 2; }

@@ -28,7 +28,8 @@ struct PivotTable {
 void setup_pivots(bool cyclic, int nxp, int nyp, double dx, double dy,
                   const std::vector<double> &rdm2, PivotTable &out, double &a_tri);
 
-// Radices (8, 4, 2, 3, 5) of a transform length; false if another prime remains.
+// Radices (16, 8, 4, 2, 3, 5) of a transform length, in the order the
+// device's compile-time plans take them; false if another prime remains.
 bool fft_radices(int M, std::vector<int> &rad);
 
 // Twiddles of every Stockham stage of a length-M transform with radices rad,
