@@ -3,8 +3,8 @@
 int_P_dA (numerics.F90:165-204) on the device sums with a running
 compensation (TwoSum), so a field whose terms cancel to ten orders of
 magnitude still integrates to within a few roundings of the exact sum of its
-FP64 values (math.fsum), where a plain FP64 sum of the same terms is off by
-about 1e-5 of the result.  The step's modal area integrals (box_homog) and
+FP64 values (math.fsum), where a running FP64 sum of the same terms is off
+by more than 1e-9 of the result.  The step's modal area integrals (box_homog) and
 the entrainment integral use the same accumulation.
 """
 import math
@@ -53,10 +53,11 @@ def test_area_integral_is_compensated(n, prec):
         exact = _exact_int(b, f)
         got = g.int_P_dA(f)
         assert abs(got - exact) <= 1e-15 * abs(exact), (got, exact)
-        # the same terms summed plainly in a fixed order miss by far more
+        # the same terms added one after another in FP64 (a running sum, as
+        # an uncompensated loop forms it) miss by far more
         w = np.ones(b.shape2)
         w[[0, -1], :] *= 0.5
         w[:, [0, -1]] *= 0.5
-        plain = float(np.sum((w * f).ravel(), dtype=np.float64)) * b.dx * b.dy
-        assert abs(plain - exact) > 1e3 * abs(got - exact)
+        plain = float(np.cumsum((w * f).ravel(), dtype=np.float64)[-1]) * b.dx * b.dy
+        assert abs(plain - exact) > 1e-9 * abs(exact)
     g.close()
