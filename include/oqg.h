@@ -254,7 +254,9 @@ int oqg_ekman_from_tau(const oqg_params *prm, const double *taux,
 
 /* Device pointers of the state, for zero-copy use by the PyTorch extension:
  * p, pm, q, qm as (nl, nyp, pitch) arrays of the handle's storage type
- * (FP64 or, in OQG_MIXED, FP32); *pitch is the row pitch in elements. */
+ * (FP64 or, in OQG_MIXED, FP32); *pitch is the row pitch in elements.  In
+ * OQG_MIXED q and qm hold q - beta*yprel(j) (the planetary vorticity is kept
+ * out of the FP32 values; oqg_get_state adds it back). */
 int oqg_device_state(oqg_handle *h, void **p, void **pm, void **q, void **qm,
                      int *pitch, int *elem_bytes);
 

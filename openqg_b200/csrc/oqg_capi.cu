@@ -91,7 +91,6 @@ static X *dalloc(oqg_handle *h, size_t count) {
 }
 
 // ----------------------------------------------------------- launch helpers
-static const int XTHREADS = 256;   // forward-transform CTA size (ensembles)
 
 // Launch with programmatic stream serialisation: the kernel may be scheduled
 // while its predecessor drains and waits in griddepcontrol.wait for its data.
@@ -276,6 +275,15 @@ static void stage_to_field(oqg_handle *h, const double *s, void *f, size_t n) {
 }
 static void field_to_stage(oqg_handle *h, const void *f, double *s, size_t n) {
     if (h->mixed) k_cvt_out<float><<<296, 256, 0, h->st>>>((const float *)f, s, n);
+    else cudaMemcpyAsync(s, f, n * sizeof(double), cudaMemcpyDeviceToDevice, h->st);
+}
+// The same for q fields, whose FP32 storage holds q - beta yprel.
+static void stage_to_qfield(oqg_handle *h, const double *s, void *f, size_t n) {
+    if (h->mixed) k_q_in<float><<<296, 256, 0, h->st>>>(h->d_bas64, 0, s, (float *)f, n);
+    else cudaMemcpyAsync(f, s, n * sizeof(double), cudaMemcpyDeviceToDevice, h->st);
+}
+static void qfield_to_stage(oqg_handle *h, const void *f, double *s, size_t n) {
+    if (h->mixed) k_q_out<float><<<296, 256, 0, h->st>>>(h->d_bas64, 0, (const float *)f, s, n);
     else cudaMemcpyAsync(s, f, n * sizeof(double), cudaMemcpyDeviceToDevice, h->st);
 }
 
@@ -522,7 +530,7 @@ struct oqg_ensemble {
     Work *d_wv = nullptr, *d_wx = nullptr, *d_wy = nullptr, *d_wi = nullptr;
     int nv = 0, nx = 0, nys = 0, ni = 0;
     size_t smem_v = 0, smem_x = 0, smem_y = 0, smem_i = 0;
-    int xi_threads = 64;
+    int xi_threads = 64, xthreads = 128;
     int par = 0;
     cudaGraphExec_t gexec[2] = {nullptr, nullptr};
     std::vector<void *> allocs;
@@ -548,7 +556,7 @@ struct oqg_ensemble {
 template <class T, int NL, int E>
 static void launch_ens_step_t(oqg_ensemble *e, int par) {
     launch_pdl(k_vort<T, NL>, e->nv, VTHREADS, e->smem_v, e->st, e->d_bas, e->d_wv, par, 0.0);
-    launch_pdl(k_xfwd<T, E>, e->nx, XTHREADS, e->smem_x, e->st, e->d_bas, e->d_wx, (const void *)nullptr);
+    launch_pdl(k_xfwd<T, E>, e->nx, e->xthreads, e->smem_x, e->st, e->d_bas, e->d_wx, (const void *)nullptr);
     if (e->cyclic)
         launch_pdl(k_ysolve<T, true, NL>, e->nys, 128, e->smem_y, e->st, e->d_bas, e->d_wy);
     else
@@ -915,7 +923,8 @@ int oqg_set_state_full(oqg_handle *h, const double *p, const double *pm, const d
     for (int f = 0; f < 4; ++f) {
         int rc = upload3(h, src[f], h->stage[0], b.nl);
         if (rc) return rc;
-        stage_to_field(h, h->stage[0], b.F[dst[f]], n3);
+        if (f < 2) stage_to_field(h, h->stage[0], b.F[dst[f]], n3);
+        else stage_to_qfield(h, h->stage[0], b.F[dst[f]], n3);
         CK(cudaStreamSynchronize(h->st));
     }
     DevState sc;
@@ -940,7 +949,8 @@ int oqg_get_state(oqg_handle *h, double *p, double *pm, double *q, double *qm) {
     const int src[4] = {par, 1 - par, 2 + par, 3 - par};
     for (int f = 0; f < 4; ++f) {
         if (!dst[f]) continue;
-        field_to_stage(h, b.F[src[f]], h->stage[0], n3);
+        if (f < 2) field_to_stage(h, b.F[src[f]], h->stage[0], n3);
+        else qfield_to_stage(h, b.F[src[f]], h->stage[0], n3);
         int rc = download3(h, h->stage[0], dst[f], b.nl);
         if (rc) return rc;
         CK(cudaStreamSynchronize(h->st));
@@ -1528,9 +1538,12 @@ int oqg_ensemble_create(const oqg_params *members, int nmembers, oqg_ensemble **
     e->mixed = e->m[0]->mixed;
     e->nl = e->m[0]->hb.nl;
     e->cyclic = e->m[0]->hb.cyclic;
-    e->E = 8;
-    for (oqg_handle *h : e->m)
-        if (h->hb.M > 2048) e->E = 16;
+    // 16 values per transform thread, as single handles take them; the
+    // forward-transform CTAs hold 128 threads, or one transform of the
+    // longest member if that is longer
+    e->E = 16;
+    e->xthreads = 128;
+    for (oqg_handle *h : e->m) e->xthreads = std::max(e->xthreads, rup((h->hb.M + e->E - 1) / e->E, 32));
     const size_t esz = e->m[0]->esz, t2 = 2 * esz, vsz = e->cyclic ? 16 : 8;
     // launch sizes per member, with the ensemble's E and fixed block sizes
     std::vector<int> order(nmembers);
@@ -1545,7 +1558,7 @@ int oqg_ensemble_create(const oqg_params *members, int nmembers, oqg_ensemble **
     for (int i : order) {
         const BasinDev &b = e->m[i]->hb;
         const int TT = (b.M + e->E - 1) / e->E;
-        const int G = std::max(1, XTHREADS / TT);
+        const int G = std::max(1, e->xthreads / TT);
         const int LB = fft_buf_len(b.M);
         const int npm = (b.ny + 1) / 2;
         const int nvb = b.tiles_x * b.tiles_y;

@@ -139,6 +139,14 @@ __device__ __forceinline__ double csum_block(CSum v, double *red) { return csum_
 #define XINV_E 16           // complex values per transform thread in k_xinv
 #define XINV_FFT_MAX 512    // at most this many transform threads per k_xinv CTA
 
+// Storage of q: FP64 handles keep q itself; FP32 handles keep the anomaly
+// q - beta yprel (the planetary vorticity is most of q, and in FP32 its
+// rounding would swamp the relative and stretching vorticity that the
+// Helmholtz inversion recovers from q - beta y).  Every kernel that reads or
+// writes q applies this; the host converts at the boundary (oqg_get_state,
+// oqg_set_state_full).
+template <class T> __host__ __device__ constexpr bool q_anom_stored() { return sizeof(T) == 4; }
+
 // Geometry of a basin for the stencils; the coefficients sit in a shared
 // table (K = fx, fy, fxb, fyb, jac) that the kernel fills once.
 template <class T> struct GeoS {
@@ -281,8 +289,13 @@ k_vort(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par,
     const BasinDev &b = bas[w.member];
     // uniform constants in shared memory: fx fy fxb fyb jac | c_ent1 c_wind
     // c_ent2 c_drag tdt | c2[k] | c4[k]; FP64 ctl2m
-    __shared__ T sK[10 + 2 * OQG_NLMAX];
+    __shared__ T sK[11 + 2 * OQG_NLMAX];
     __shared__ double sCtl[NL * NL];
+    // FP32 storage keeps q as its anomaly q - beta yprel (q_anom_stored): the
+    // planetary term's Jacobian then comes from p alone (its coefficient,
+    // jac_fac beta dy, is sK[10 + 2 NL])
+    constexpr bool QA = q_anom_stored<T>();
+    if (QA && threadIdx.x == 10 + 2 * NL) sK[10 + 2 * NL] = (T)(b.jac_fac * b.beta * b.dy);
     if (threadIdx.x < 10 + 2 * NL) {
         const int i = threadIdx.x;
         T v;
@@ -509,7 +522,13 @@ k_vort(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par,
                             const T Dd = pw[1][2] * (qw[2][2] - qw[0][2]) - pw[1][0] * (qw[2][0] - qw[0][0]);
                             const T Bv = qw[2][1] * (pw[2][2] - pw[2][0]) - qw[0][1] * (pw[0][2] - pw[0][0]);
                             const T Cc = pw[2][1] * (qw[2][2] - qw[2][0]) - pw[0][1] * (qw[0][2] - qw[0][0]);
-                            const T jac = gjac(g) * (qxc * pyc - qyc * pxc + A - Bv + Cc - Dd);
+                            T jac = gjac(g) * (qxc * pyc - qyc * pxc + A - Bv + Cc - Dd);
+                            if (QA) {
+                                // + J(beta y, p): the Arakawa sum of a field linear in y is
+                                // -dy (4 (pE - pW) + (pNE - pNW) + (pSE - pSW))
+                                const T py = (T)4 * pxc + (pw[2][2] - pw[2][0]) + (pw[0][2] - pw[0][0]);
+                                jac = jac - sK[10 + 2 * NL] * py;
+                            }
                             T dq = jac + sK[10 + k] * d4c - sK[10 + NL + k] * d6;
                             const size_t o2 = (size_t)gj * px + gi;
                             if (k == 0) {
@@ -521,7 +540,7 @@ k_vort(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par,
                             const T qn = sQM[r * LO + tx] + sK[9] * dq;
                             QM[((size_t)k * nyp + gj) * px + gi] = qn;
                             // modal right-hand side, FP64 (p_modes_rhs)
-                            double ql = (double)qn - sBY[r];
+                            double ql = QA ? (double)qn : (double)qn - sBY[r];
                             if (k == kt && topo) ql -= DD[o2];
     #pragma unroll
                             for (int m = 0; m < NL; ++m) acc[u][m] += ql * sCtl[k + NL * m];
@@ -546,24 +565,25 @@ k_vort(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par,
                     const int gj = j0 + r;
                     if (!(gj == 0 || gj == 1 || gj == nyp - 2 || gj == nyp - 1)) continue;
                     const int c = tx + 4;                   // p/q tile column
-                    const T qc = sQ[(r + 1) * LPQ + c];
+                    // q itself (FP32 storage holds q - beta y), in FP64
+                    const double qc = QA ? (double)sQ[(r + 1) * LPQ + c] + sBY[r] : (double)sQ[(r + 1) * LPQ + c];
                     const T d2 = sD2[(r + 2) * L2 + tx + 2], d4 = sD4[(r + 1) * L1 + tx + 1];
                     if (gj == 0) {
-                        sq[0] += (double)(qc * (sP[(r + 2) * LPQ + c + 1] - sP[(r + 2) * LPQ + c - 1]));
+                        sq[0] += qc * (double)(sP[(r + 2) * LPQ + c + 1] - sP[(r + 2) * LPQ + c - 1]);
                         sq[4] += (double)(sD2[(r + 3) * L2 + tx + 2] - d2);
                         sq[6] += (double)(sD4[(r + 2) * L1 + tx + 1] - d4);
                         if (k == kt)
                             sq[8] += (double)(sPM[(r + 4) * LPQ + tx + 4] - sPM[(r + 3) * LPQ + tx + 4]);
                     }
-                    if (gj == 1) sq[1] += (double)(qc * (sP[(r + 1) * LPQ + c + 1] - sP[(r + 1) * LPQ + c - 1]));
+                    if (gj == 1) sq[1] += qc * (double)(sP[(r + 1) * LPQ + c + 1] - sP[(r + 1) * LPQ + c - 1]);
                     if (gj == nyp - 1) {
-                        sq[2] += (double)(qc * (sP[r * LPQ + c + 1] - sP[r * LPQ + c - 1]));
+                        sq[2] += qc * (double)(sP[r * LPQ + c + 1] - sP[r * LPQ + c - 1]);
                         sq[5] += (double)(d2 - sD2[(r + 1) * L2 + tx + 2]);
                         sq[7] += (double)(d4 - sD4[r * L1 + tx + 1]);
                         if (k == kt)
                             sq[9] += (double)(sPM[(r + 3) * LPQ + tx + 4] - sPM[(r + 2) * LPQ + tx + 4]);
                     }
-                    if (gj == nyp - 2) sq[3] += (double)(qc * (sP[(r + 1) * LPQ + c + 1] - sP[(r + 1) * LPQ + c - 1]));
+                    if (gj == nyp - 2) sq[3] += qc * (double)(sP[(r + 1) * LPQ + c + 1] - sP[(r + 1) * LPQ + c - 1]);
                 }
             }
             // only the row ty = 0 (warps 0 and 1) holds terms: reduce the
@@ -1450,7 +1470,8 @@ k_xinv(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par,
             const T fmv = (T)(b.fnot * mv);
             const T by = (T)(b.beta * b.yprel[j]);
             for (int c = 0; c < cnt; ++c) qv = qv - fmv;
-            for (int c = 0; c < cnt; ++c) qv = qv + by;
+            // (FP32 storage holds q - beta y: one beta y fewer)
+            for (int c = q_anom_stored<T>() ? 1 : 0; c < cnt; ++c) qv = qv + by;
             if (k == b.kt && b.topo_active) {
                 const T dd = (T)b.ddyn[(size_t)j * px + i];
                 for (int c = 0; c < cnt; ++c) qv = qv + dd;
@@ -1503,7 +1524,7 @@ __global__ void k_qcomp(const BasinDev *__restrict__ bas, int member, const doub
         for (int k = 0; k < NL; ++k) {
             double v = lap_bc_g(p + k * n2, b, i, j, afac) / b.fnot;
             if (k == b.kt && b.topo_active) v += b.ddyn[o2];
-            v += b.beta * b.yprel[j];
+            if (!q_anom_stored<T>()) v += b.beta * b.yprel[j];
             double mv = 0.0;
 #pragma unroll
             for (int l = 0; l < NL; ++l) mv += b.amat[k + NL * l] * pv[l];
@@ -1522,6 +1543,25 @@ template <class T>
 __global__ void k_cvt_out(const T *src, double *dst, size_t n) {
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
         dst[i] = (double)src[i];
+}
+
+// q fields [nl][nyp][px] <-> FP64 staging, with the storage's anomaly
+// (q_anom_stored) removed on the way out and applied on the way in.
+template <class T>
+__global__ void k_q_out(const BasinDev *__restrict__ bas, int member, const T *src, double *dst, size_t n) {
+    const BasinDev &b = bas[member];
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const int j = (int)((i / b.px) % b.nyp);
+        dst[i] = (double)src[i] + (q_anom_stored<T>() ? b.beta * b.yprel[j] : 0.0);
+    }
+}
+template <class T>
+__global__ void k_q_in(const BasinDev *__restrict__ bas, int member, const double *src, T *dst, size_t n) {
+    const BasinDev &b = bas[member];
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const int j = (int)((i / b.px) % b.nyp);
+        dst[i] = (T)(q_anom_stored<T>() ? src[i] - b.beta * b.yprel[j] : src[i]);
+    }
 }
 
 // Host-order rows (nxp contiguous FP64 values per row) <-> pitched field rows
@@ -1882,7 +1922,7 @@ __global__ void __launch_bounds__(256) k_valids(const BasinDev *__restrict__ bas
         const size_t k = idx / ((size_t)b.nyp * b.nxp), rem = idx - k * b.nyp * b.nxp;
         const size_t j = rem / b.nxp, i = rem - j * b.nxp;
         const size_t o = k * n2 + j * b.px + i;
-        const double pv = (double)P[o], qv = (double)Q[o];
+        const double pv = (double)P[o], qv = (double)Q[o] + (q_anom_stored<T>() ? b.beta * b.yprel[j] : 0.0);
         if (!isfinite(pv)) bad += 1.0; else { v[0] = fmin(v[0], pv); v[1] = fmax(v[1], pv); }
         if (!isfinite(qv)) bad += 1.0; else { v[2] = fmin(v[2], qv); v[3] = fmax(v[3], qv); }
         if (k == 0) {
@@ -1996,7 +2036,7 @@ __global__ void __launch_bounds__(128) k_dg_rows(const BasinDev *__restrict__ ba
         const double pv = (double)P[o];
         const double ug = V[o], vg = V[n3 + o], uc = V[2 * n3 + o], vc = V[3 * n3 + o];
         s[0] += w * pv;
-        s[1] += w * (double)Q[o];
+        s[1] += w * ((double)Q[o] + (q_anom_stored<T>() ? b.beta * b.yprel[j] : 0.0));
         s[2] += w * (uc * V[4 * n3 + o]);
         s[3] += w * (vc * V[6 * n3 + o]);
         s[4] += w * (uc * V[5 * n3 + o]);
