@@ -525,9 +525,10 @@ k_vort(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par,
                             T jac = gjac(g) * (qxc * pyc - qyc * pxc + A - Bv + Cc - Dd);
                             if (QA) {
                                 // + J(beta y, p): the Arakawa sum of a field linear in y is
-                                // -dy (4 (pE - pW) + (pNE - pNW) + (pSE - pSW))
-                                const T py = (T)4 * pxc + (pw[2][2] - pw[2][0]) + (pw[0][2] - pw[0][0]);
-                                jac = jac - sK[10 + 2 * NL] * py;
+                                // -dy (4 (pE - pW) + (pNE - pNW) + (pSE - pSW)); explicit FMAs
+                                // keep the rounding the same in every tile instance
+                                const T py = fma((T)4, pxc, (pw[2][2] - pw[2][0]) + (pw[0][2] - pw[0][0]));
+                                jac = fma(-sK[10 + 2 * NL], py, jac);
                             }
                             T dq = jac + sK[10 + k] * d4c - sK[10 + NL + k] * d6;
                             const size_t o2 = (size_t)gj * px + gi;

@@ -52,13 +52,14 @@ def _run_pair(members, tdts, nsteps):
     return e, singles
 
 
-def _assert_same(e, singles):
+def _assert_same(e, singles, tol=1e-13):
     # members tile the vorticity kernel with the tallest (or a tuned) height, single handles
     # with tiles fitted to whole waves; the channel strip sums and the wall
     # rows then round differently, so the match is to rounding, not bits
+    # (FP64 rounding; FP32 storage rounds at about 1e-7)
     for i, g in enumerate(singles):
         for name, a, c in zip(("p", "pm", "q", "qm"), e.get_state(i), g.get_state()):
-            assert rel_l2(a, c) <= 1e-13, "member %d %s rel L2 %.3e" % (i, name, rel_l2(a, c))
+            assert rel_l2(a, c) <= tol, "member %d %s rel L2 %.3e" % (i, name, rel_l2(a, c))
 
 
 def test_box_ensemble_equals_single_handles():
@@ -102,7 +103,7 @@ def test_per_member_step_and_mixed_precision():
     members = [ocean_double_gyre(n, precision=OQG_MIXED) for n in (129, 65, 97)]
     tdts = np.array([3600.0, 1800.0, 2400.0])
     e, singles = _run_pair(members, tdts, 4)
-    _assert_same(e, singles)
+    _assert_same(e, singles, tol=1e-6)
 
 
 def test_ensemble_rejects_bad_members():
