@@ -57,8 +57,8 @@ struct oqg_handle {
     std::vector<void *> allocs;
     Work *d_wv = nullptr, *d_wx = nullptr, *d_wy = nullptr, *d_wi = nullptr;
     int nv = 0, nx = 0, nys = 0, ni = 0;
-    int E = 8, KB = 16, xthreads = 128, xi_threads = 64, xa_threads = 64;
-    size_t smem_v = 0, smem_x = 0, smem_x64 = 0, smem_y = 0, smem_i = 0, smem_i64 = 0, smem_a = 0;
+    int E = 8, KB = 16, xthreads = 128, xi_threads = 64;
+    size_t smem_v = 0, smem_x = 0, smem_x64 = 0, smem_y = 0, smem_i = 0, smem_i64 = 0;
     double *stage[2] = {nullptr, nullptr};
     double *hrow = nullptr;     // contiguous host-order copy buffer [nl][nyp][nxp]
     double *dg = nullptr;       // qg_diagno scratch, made on its first call
@@ -136,7 +136,8 @@ static void launch_step_t(oqg_handle *h, int par, double tdt) {
         launch_pdl(k_ysolve<T, true, NL>, h->nys, 32 * h->KB, h->smem_y, h->st, h->d_bas, h->d_wy);
     else
         launch_pdl(k_ysolve<T, false, NL>, h->nys, 32 * h->KB, h->smem_y, h->st, h->d_bas, h->d_wy);
-    launch_pdl(k_xasm<T, NL>, h->ni, h->xa_threads, h->smem_a, h->st, h->d_bas, h->d_wi, par, tdt);
+    launch_pdl(k_xinv<T, NL>, h->ni, h->xi_threads, h->smem_i, h->st, h->d_bas, h->d_wi, par, tdt,
+               (double *)nullptr);
 }
 
 // FP64 solve of the modal Helmholtz problems with the rhs buffer as input;
@@ -192,15 +193,10 @@ static void raise_step_smem(size_t v, size_t x, size_t y, size_t i) {
     raise_smem((const void *)k_ysolve<T, false, NL>, y);
     raise_smem((const void *)k_xinv<T, NL>, i);
 }
-template <class T, int NL>
-static void raise_xasm_smem(size_t a) {
-    raise_smem((const void *)k_xasm<T, NL>, a);
-}
 
 template <class T, int NL, int E>
 static void set_attrs_t(oqg_handle *h) {
     raise_step_smem<T, NL, E>(h->smem_v, h->smem_x, h->smem_y, h->smem_i);
-    raise_xasm_smem<T, NL>(h->smem_a);
     raise_smem((const void *)k_xfwd<double, E>, h->smem_x64);
     raise_smem((const void *)k_ysolve<double, true, NL>, h->smem_y);
     raise_smem((const void *)k_ysolve<double, false, NL>, h->smem_y);
@@ -510,7 +506,7 @@ static void launch_phase_t(oqg_handle *h, int phase, int par, double tdt) {
             else
                 k_ysolve<T, false, NL><<<h->nys, 32 * h->KB, h->smem_y, h->st>>>(h->d_bas, h->d_wy);
             break;
-        default: k_xasm<T, NL><<<h->ni, h->xa_threads, h->smem_a, h->st>>>(h->d_bas, h->d_wi, par, tdt); break;
+        default: k_xinv<T, NL><<<h->ni, h->xi_threads, h->smem_i, h->st>>>(h->d_bas, h->d_wi, par, tdt, nullptr); break;
     }
 }
 static void launch_phase(oqg_handle *h, int phase, int par, double tdt) {
@@ -533,8 +529,8 @@ struct oqg_ensemble {
     BasinDev *d_bas = nullptr;
     Work *d_wv = nullptr, *d_wx = nullptr, *d_wy = nullptr, *d_wi = nullptr;
     int nv = 0, nx = 0, nys = 0, ni = 0;
-    size_t smem_v = 0, smem_x = 0, smem_y = 0, smem_i = 0, smem_a = 0;
-    int xi_threads = 64, xthreads = 128, xa_threads = 64;
+    size_t smem_v = 0, smem_x = 0, smem_y = 0, smem_i = 0;
+    int xi_threads = 64, xthreads = 128;
     int par = 0;
     cudaGraphExec_t gexec[2] = {nullptr, nullptr};
     std::vector<void *> allocs;
@@ -565,12 +561,12 @@ static void launch_ens_step_t(oqg_ensemble *e, int par) {
         launch_pdl(k_ysolve<T, true, NL>, e->nys, 128, e->smem_y, e->st, e->d_bas, e->d_wy);
     else
         launch_pdl(k_ysolve<T, false, NL>, e->nys, 128, e->smem_y, e->st, e->d_bas, e->d_wy);
-    launch_pdl(k_xasm<T, NL>, e->ni, e->xa_threads, e->smem_a, e->st, e->d_bas, e->d_wi, par, 0.0);
+    launch_pdl(k_xinv<T, NL>, e->ni, e->xi_threads, e->smem_i, e->st, e->d_bas, e->d_wi, par, 0.0,
+               (double *)nullptr);
 }
 template <class T, int NL, int E>
 static void raise_ens_smem_t(oqg_ensemble *e) {
     raise_step_smem<T, NL, E>(e->smem_v, e->smem_x, e->smem_y, e->smem_i);
-    raise_xasm_smem<T, NL>(e->smem_a);
 }
 static void launch_ens_step(oqg_ensemble *e, int par) { OQG_DISPATCH_E(launch_ens_step_t, e, e, par); }
 
@@ -832,8 +828,10 @@ static int create_impl(const oqg_params *prm, oqg_handle **out, bool batched) {
     h->ni = (b.ny + b.k4_rows - 1) / b.k4_rows;
     h->smem_v = vort_smem_bytes(b.vty, (int)h->esz);
     const int LB = fft_buf_len(b.M);
-    h->smem_x = (size_t)GX * 2 * LB * t2;
-    h->smem_x64 = (size_t)GX * 2 * LB * 16;
+    // the long lengths transform in place: one buffer plus two staged rows per group
+    const size_t xrow = (size_t)((b.nxin + 3) & ~3);
+    h->smem_x = fft_inplace_len(b.M) ? (size_t)GX * (LB * t2 + 2 * xrow * h->esz) : (size_t)GX * 2 * LB * t2;
+    h->smem_x64 = fft_inplace_len(b.M) ? (size_t)GX * (LB * 16 + 2 * xrow * 8) : (size_t)GX * 2 * LB * 16;
     h->smem_y = (size_t)LDy * h->KB * vsz;
     // rows of an assembly CTA: k4_rows interior rows plus at most one wall row
     const int nra = (b.ny > b.k4_rows) ? b.k4_rows + 1 : b.ny + 2;
@@ -854,13 +852,8 @@ static int create_impl(const oqg_params *prm, oqg_handle **out, bool batched) {
     }
     h->xi_threads = nfft_i + 32;
     h->smem_i = xinv_smem(b.M, b.nl, nra, b.nxp, nfft_i, h->esz, split);
-    // the step's inverse transforms and assembly (k_xasm)
-    h->xa_threads = xasm_threads(b.M, b.nl);
-    h->smem_a = xasm_smem(b.M, b.nl, h->esz);
-    b.wall_adj = dalloc<char>(h, 2 * (size_t)b.nl * b.px * h->esz);
-    if (!b.wall_adj) return bail(OQG_ECUDA, "out of device memory");
     h->smem_i64 = xinv_smem(b.M, b.nl, nra, b.nxp, nfft_i, 8, split);
-    if (h->smem_i64 > 227 * 1024 || h->smem_x64 > 227 * 1024 || h->smem_y > 227 * 1024 || h->smem_a > 227 * 1024)
+    if (h->smem_i64 > 227 * 1024 || h->smem_x64 > 227 * 1024 || h->smem_y > 227 * 1024)
         return bail(OQG_EUNSUPPORTED, "grid too large for this build's shared-memory tiling");
     std::vector<Work> wv(h->nv), wx(h->nx), wy(h->nys), wi(h->ni);
     for (int i = 0; i < h->nv; ++i) wv[i] = Work{0, i};
@@ -1580,13 +1573,13 @@ int oqg_ensemble_create(const oqg_params *members, int nmembers, oqg_ensemble **
         for (int k = 0; k < nib; ++k) wi.push_back(Work{i, k});
         const int nra = (b.ny > b.k4_rows) ? b.k4_rows + 1 : b.ny + 2;
         e->smem_v = std::max(e->smem_v, vort_smem_bytes(b.vty, (int)esz));
-        e->smem_x = std::max(e->smem_x, (size_t)G * 2 * LB * t2);
+        const size_t xrow = (size_t)((b.nxin + 3) & ~3);
+        e->smem_x = std::max(e->smem_x, fft_inplace_len(b.M) ? (size_t)G * (LB * t2 + 2 * xrow * esz)
+                                                               : (size_t)G * 2 * LB * t2);
         e->smem_y = std::max(e->smem_y, (size_t)((b.ny + 32) | 1) * 4 * vsz);
         e->smem_i = std::max(e->smem_i, xinv_smem(b.M, b.nl, nra, b.nxp, nfft_e, esz, b.inh_g != nullptr));
-        e->smem_a = std::max(e->smem_a, xasm_smem(b.M, b.nl, esz));
-        e->xa_threads = std::max(e->xa_threads, xasm_threads(b.M, b.nl));
     }
-    if (e->smem_x > 227 * 1024 || e->smem_i > 227 * 1024 || e->smem_v > 227 * 1024 || e->smem_a > 227 * 1024) {
+    if (e->smem_x > 227 * 1024 || e->smem_i > 227 * 1024 || e->smem_v > 227 * 1024) {
         ens_free(e);
         return fail(OQG_EUNSUPPORTED, "ensemble member too large for the shared-memory tiling");
     }

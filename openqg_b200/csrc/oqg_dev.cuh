@@ -99,7 +99,6 @@ struct BasinDev {
     double *ent_rows;           // [nyp][2] row sums of the ent area integral and their
                                 // compensations
     void *inh_g;                // wide grids: modal rows of k_xinv, [nl][nyp][px] (8-byte slots)
-    void *wall_adj;             // [2][nl][px] T: unaveraged p of rows 1 and nyp-2 (k_xasm)
     int *err;                   // device error bits
     // launch bookkeeping
     int k4_rows;                // interior rows per CTA of the assembly launch

@@ -186,46 +186,6 @@ template <class T> struct Dft<T, 16> {
     }
 };
 
-// Multiplies v[r] (r = 1 .. R-1) of a butterfly by its twiddle w^r, w the
-// butterfly's stage twiddle.  w: the stage table's entries (w^1 .. w^(R-1)).
-// For power-of-two radices only w, w^2, w^4 and w^8 are read and the others
-// formed by at most three products (each correctly rounded table entry is
-// within half an ulp; a product adds about one ulp), so few twiddles are live
-// in registers at once; radices 3 and 5 read all theirs.
-template <class T, int R>
-__device__ __forceinline__ void twiddle_mul(typename C2<T>::t *v, const typename C2<T>::t *__restrict__ w) {
-    typedef typename C2<T>::t T2;
-    if constexpr (R == 2 || R == 3 || R == 5) {
-#pragma unroll
-        for (int r = 1; r < R; ++r) v[r] = c_mul(v[r], __ldg(w + r - 1));
-    } else {
-        const T2 w1 = __ldg(w), w2 = __ldg(w + 1);
-        v[1] = c_mul(v[1], w1);
-        v[2] = c_mul(v[2], w2);
-        const T2 w3 = c_mul(w1, w2);
-        v[3] = c_mul(v[3], w3);
-        if constexpr (R >= 8) {
-            const T2 w4 = __ldg(w + 3);
-            v[4] = c_mul(v[4], w4);
-            v[5] = c_mul(v[5], c_mul(w1, w4));
-            v[6] = c_mul(v[6], c_mul(w2, w4));
-            v[7] = c_mul(v[7], c_mul(w3, w4));
-            if constexpr (R == 16) {
-                const T2 w8 = __ldg(w + 7);
-                v[8] = c_mul(v[8], w8);
-                v[9] = c_mul(v[9], c_mul(w1, w8));
-                v[10] = c_mul(v[10], c_mul(w2, w8));
-                v[11] = c_mul(v[11], c_mul(w3, w8));
-                const T2 w12 = c_mul(w4, w8);
-                v[12] = c_mul(v[12], w12);
-                v[13] = c_mul(v[13], c_mul(w1, w12));
-                v[14] = c_mul(v[14], c_mul(w2, w12));
-                v[15] = c_mul(v[15], c_mul(w3, w12));
-            }
-        }
-    }
-}
-
 // Shared work buffers hold element i at fpad(i) = i + i/8: with one pad per 8
 // complex values the stride-R stores of the early Stockham stages and the
 // unit-stride loads both spread over all banks.
@@ -340,7 +300,11 @@ __device__ __forceinline__ void fft_stage_ct(const typename C2<T>::t *__restrict
             T2 v[R];
 #pragma unroll
             for (int r = 0; r < R; ++r) v[r] = src[fpad(j + r * nb)];
-            if (Ns > 1 && jm != 0) twiddle_mul<T, R>(v, tws + jm * (R - 1));
+            if (Ns > 1 && jm != 0) {
+                const T2 *w = tws + jm * (R - 1);
+#pragma unroll
+                for (int r = 1; r < R; ++r) v[r] = c_mul(v[r], __ldg(w + r - 1));
+            }
             Dft<T, R>::run(v);
             const int d = q * Ns * R + jm;
 #pragma unroll
@@ -366,10 +330,11 @@ __device__ __forceinline__ typename C2<T>::t *fft_ct_from(typename C2<T>::t *src
     }
 }
 
-// ---- in-place stages for power-of-two lengths: one padded buffer per
-// transform.  Each thread holds the inputs of all its butterflies in
-// registers (E = M / TT values, E a multiple of every radix of the plan),
-// the group synchronises, then the thread computes and stores them.
+// ---- in-place stages for the long power-of-two lengths: one padded buffer
+// per transform, so two transforms of 4096 FP64 values fit where the
+// ping-pong pair fits one.  Each thread holds the inputs of all its
+// butterflies in registers (E = M / TT values, E a multiple of every radix of
+// the plan), the group synchronises, then the thread computes and stores.
 template <class T, int R, int Ns, int M, int TT>
 __device__ __forceinline__ void fft_stage_ip(typename C2<T>::t *buf, const typename C2<T>::t *__restrict__ tws,
                                              int t, bool live, int bar_id, int nbar) {
@@ -389,7 +354,11 @@ __device__ __forceinline__ void fft_stage_ip(typename C2<T>::t *buf, const typen
         for (int u = 0; u < NB; ++u) {
             const int j = t + u * TT;
             const int q = j / Ns, jm = j - q * Ns;
-            if (Ns > 1 && jm != 0) twiddle_mul<T, R>(v[u], tws + jm * (R - 1));
+            if (Ns > 1 && jm != 0) {
+                const T2 *w = tws + jm * (R - 1);
+#pragma unroll
+                for (int r = 1; r < R; ++r) v[u][r] = c_mul(v[u][r], __ldg(w + r - 1));
+            }
             Dft<T, R>::run(v[u]);
             const int d = q * Ns * R + jm;
 #pragma unroll
@@ -407,30 +376,17 @@ __device__ __forceinline__ void fft_ip_from(typename C2<T>::t *buf, const typena
         fft_ip_from<T, M, TT, Ns * R>(buf, tw, t, live, bar_id, nbar);
     }
 }
-// Whether length M runs in place with 16 values per thread.
-__host__ __device__ constexpr bool fft_inplace_len(int M) {
-    return M == 128 || M == 256 || M == 512 || M == 1024 || M == 2048 || M == 4096;
-}
-// In-place forward FFT of length M (fft_inplace_len) by groups of TT = M/16
-// threads; the caller has written the input to buf and synchronised.
-#define OQG_FFT_IP(MM)                                                                 \
-    case MM:                                                                           \
-        fft_ip_from<T, MM, (MM) / 16, 1>(buf, tw, t, t < (MM) / 16, bar_id, nbar);   \
-        return;
+// The lengths that transform in place (16 values per thread).
+__host__ __device__ constexpr bool fft_inplace_len(int M) { return M == 2048 || M == 4096; }
+// In-place forward FFT of length M (fft_inplace_len) by groups of TT = M / 16
+// threads (t >= TT: barriers only); the input is in buf, the barrier after
+// its writes taken.
 template <class T>
 __device__ __forceinline__ void fft_inplace(typename C2<T>::t *buf, int M, const typename C2<T>::t *__restrict__ tw,
                                             int t, int bar_id, int nbar) {
-    switch (M) {
-        OQG_FFT_IP(128)
-        OQG_FFT_IP(256)
-        OQG_FFT_IP(512)
-        OQG_FFT_IP(1024)
-        OQG_FFT_IP(2048)
-        OQG_FFT_IP(4096)
-        default: break;
-    }
+    if (M == 2048) fft_ip_from<T, 2048, 128, 1>(buf, tw, t, t < 128, bar_id, nbar);
+    else if (M == 4096) fft_ip_from<T, 4096, 256, 1>(buf, tw, t, t < 256, bar_id, nbar);
 }
-#undef OQG_FFT_IP
 
 // Forward FFT of length M by groups of TT = M / E threads: the compile-time
 // stages for the lengths of the configurations' grids, the general stages

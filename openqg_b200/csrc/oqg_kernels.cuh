@@ -651,11 +651,15 @@ k_xfwd(const BasinDev *__restrict__ bas, const Work *__restrict__ work, const vo
     const int m = live ? pair / npm : 0;
     const int j = live ? 2 * (pair - m * npm) : 0;
     const bool two = live && (j + 1 < b.ny);
-    T2 *za = zs + (size_t)(g < G ? g : 0) * 2 * LB;
-    T2 *zb = za + LB;
-    T *raw = reinterpret_cast<T *>(zb);
     const int n = b.nxin;
     const int RO = (n + 3) & ~3;              // offset of the second row (16-byte aligned)
+    // the long lengths transform in place: one buffer per group, the input
+    // rows staged after all the groups' buffers
+    const bool ip = E == 16 && fft_inplace_len(M);
+    T2 *za = zs + (size_t)(g < G ? g : 0) * (ip ? LB : 2 * LB);
+    T2 *zb = za + LB;
+    T *raw = ip ? reinterpret_cast<T *>(zs + (size_t)G * LB) + (size_t)(g < G ? g : 0) * 2 * RO
+                : reinterpret_cast<T *>(zb);
     const T *R = (const T *)(rhs_override ? rhs_override : b.rhs);
     const T *x = R + ((size_t)m * b.ny + j) * b.pr;
     pdl_trigger();
@@ -686,7 +690,9 @@ k_xfwd(const BasinDev *__restrict__ bas, const Work *__restrict__ work, const vo
         }
     }
     __syncthreads();
-    T2 *z = fft_run<T, E>(za, zb, M, b.rad, b.nrad, (const T2 *)b.tw, live ? t : TT, TT, 0, 0);
+    T2 *z = za;
+    if (ip) fft_inplace<T>(za, M, (const T2 *)b.tw, live ? t : M, 0, 0);
+    else z = fft_run<T, E>(za, zb, M, b.rad, b.nrad, (const T2 *)b.tw, live ? t : TT, TT, 0, 0);
     if (!live) return;
     if (!b.cyclic) {
         T *S = (T *)b.spec;
@@ -1254,6 +1260,9 @@ k_xinv(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par,
     T2 *set_in = (b.nrad & 1) ? setB : setA, *set_st = (b.nrad & 1) ? setA : setB;
     const bool split = b.inh_g != nullptr;
     const bool alias = one_round && !split;
+    // a row of the spectral buffer: n reals (box) or nk complex (channel)
+    const int rowbytes = b.cyclic ? b.nk * (int)sizeof(T2) : n * (int)sizeof(T);
+    const int RO = round16(rowbytes) / (int)sizeof(T);   // second row offset (T units)
     T *inh;
     size_t ms, rs;                               // mode and row strides of inh
     if (split) { inh = (T *)b.inh_g + (size_t)jfirst * px; ms = (size_t)nyp * px; rs = px; }
@@ -1276,9 +1285,6 @@ k_xinv(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par,
                 for (int i = threadIdx.x; i < nxp; i += nfft) inh[m * ms + lr * rs + i] = (T)0;
     pdl_wait();
 
-    // a row of the spectral buffer: n reals (box) or nk complex (channel)
-    const int rowbytes = b.cyclic ? b.nk * (int)sizeof(T2) : n * (int)sizeof(T);
-    const int RO = round16(rowbytes) / (int)sizeof(T);   // second row offset (T units)
     for (int base = 0; base < npairs; base += G) {
         const int pair = base + g;
         const bool live = g < G && pair < npairs;
@@ -1484,269 +1490,6 @@ k_xinv(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par,
     }
 }
 
-// ------------------------------------------------------------------ k_xasm
-// The inverse x-transforms and the assembly of the step, in layer space.
-// modes_to_layers (modes.F90:268-284) and the inverse transform are both
-// linear, so each layer's spectral rows  sum_m ctm2l(m,k) s_m  are formed
-// first (in FP64) and transformed once, and the homogeneous correction
-// sum_m ctm2l(m,k) c_m h_m (box_homog, homog.F90:331-366; cyclic_homog,
-// homog.F90:280-329) is added in physical space: no modal rows are kept.
-// One group of TT = ceil(M/16) threads transforms one layer's row pair
-// (power-of-two lengths in place, in one padded buffer); G groups per CTA,
-// rounds over the layers.  The last warp runs the scalar phase meanwhile.
-// The unaveraged p that ocqbdy (vorsubs.F90:58-114) needs is kept beside:
-// the four points next to the meridional walls in shared memory, the rows
-// next to the zonal walls (1 and nyp-2) in the global rows b.wall_adj.
-#define XASM_ROWS 2      // interior rows per CTA (k4_rows)
-// Threads (transform groups + the scalar warp) and dynamic shared bytes of
-// k_xasm for a transform length M, nl layers, element size esz.
-__host__ __device__ __forceinline__ int xasm_groups(int M, int nl) {
-    const int tt = (M + 15) / 16;
-    int G = 256 / tt;
-    if (G < 1) G = 1;
-    if (G > nl) G = nl;
-    return G;
-}
-__host__ __device__ __forceinline__ int xasm_threads(int M, int nl) {
-    const int tt = (M + 15) / 16;
-    const int f = xasm_groups(M, nl) * tt;
-    return (f + 31) / 32 * 32 + 32;
-}
-__host__ __device__ __forceinline__ size_t xasm_smem(int M, int nl, size_t esz) {
-    return (size_t)xasm_groups(M, nl) * (fft_inplace_len(M) ? 1 : 2) * fft_buf_len(M) * 2 * esz;
-}
-
-template <class T, int NL>
-__global__ void __maxnreg__(168)
-k_xasm(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par, double tdt) {
-    typedef typename C2<T>::t T2;
-    const Work w = work[blockIdx.x];
-    const BasinDev &b = bas[w.member];
-    const int nfft = blockDim.x - 32;
-    const bool fft_thread = (int)threadIdx.x < nfft;
-    const int M = b.M, TT = (M + 15) >> 4;
-    const bool ip = fft_inplace_len(M);
-    const int G = xasm_groups(M, NL);
-    const int g = threadIdx.x / TT, t = threadIdx.x - g * TT;
-    int jlo, jhi, jfirst, nra;
-    xinv_rows(b, w.block, jlo, jhi, jfirst, nra);
-    const int nr = jhi - jlo;                    // interior rows (1 or 2)
-    const int nxp = b.nxp, n = b.nxin, nyp = b.nyp, px = b.px, ny = b.ny;
-    const size_t n2 = (size_t)nyp * px;
-    const int LB = fft_buf_len(M);
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    T2 *bufs = reinterpret_cast<T2 *>(smem_raw);
-    __shared__ XinvScal sS;
-    __shared__ T stash[NL][XASM_ROWS][4];        // unaveraged p at i = 0, 1, nxp-2, nxp-1
-    const double ftn = b.ftnorm;
-    const T *__restrict__ Pold = (const T *)b.F[par];
-    T *__restrict__ Pnew = (T *)b.F[1 - par];
-    T *__restrict__ wadj = (T *)b.wall_adj;
-    const T *__restrict__ H = (const T *)b.hsb;
-    pdl_trigger();
-    if (!fft_thread) {
-        pdl_wait();
-        scalar_phase<T, NL>(b, tdt != 0.0 ? tdt : b.tdt_m, par, w.block == 0, &sS);
-        __syncthreads();                         // sS is ready
-    } else {
-        pdl_wait();
-        const int sj = jlo - 1;                  // spectral row of the first interior row
-        const bool two = nr == 2;
-        for (int base = 0; base < NL; base += G) {
-            const int k = base + g;
-            const bool live = g < G && k < NL;
-            T2 *za = bufs + (size_t)(g < G ? g : 0) * (ip ? LB : 2 * LB);
-            double ck[NL];                       // ctm2l(m, k) of this group's layer
-#pragma unroll
-            for (int m = 0; m < NL; ++m) ck[m] = live ? b.ctm2l[m + NL * k] : 0.0;
-            if (live) {
-                if (!b.cyclic) {
-                    // odd extension of the two rows of layer k: z_0 = z_{n+1} = 0,
-                    // z_{M-jj} = -z_jj, values ftnorm * sum_m ctm2l(m,k) s_m
-                    const T *S = (const T *)b.spec;
-#pragma unroll 1
-                    for (int jj = t; jj <= (M >> 1); jj += TT) {
-                        T2 v;
-                        if (jj == 0 || jj == n + 1) { v.x = (T)0; v.y = (T)0; }
-                        else {
-                            double xs = 0.0, ys = 0.0;
-#pragma unroll
-                            for (int m = 0; m < NL; ++m) {
-                                const T *row = S + ((size_t)m * ny + sj) * b.pk + (jj - 1);
-                                xs += ck[m] * (double)__ldg(row);
-                                if (two) ys += ck[m] * (double)__ldg(row + b.pk);
-                            }
-                            v.x = (T)(ftn * xs);
-                            v.y = (T)(ftn * ys);
-                        }
-                        za[fpad(jj)] = v;
-                        if (jj != 0 && 2 * jj != M) {
-                            T2 vm;
-                            vm.x = -v.x;
-                            vm.y = -v.y;
-                            za[fpad(M - jj)] = vm;
-                        }
-                    }
-                } else {
-                    // the rows' half spectra as one complex transform (c2r of two rows)
-                    const T2 *S = (const T2 *)b.spec;
-#pragma unroll 1
-                    for (int kk = t; kk < M; kk += TT) {
-                        const bool lo = kk <= M / 2;
-                        const int ks = lo ? kk : M - kk;
-                        double Xr = 0.0, Xi = 0.0, Yr = 0.0, Yi = 0.0;
-#pragma unroll
-                        for (int m = 0; m < NL; ++m) {
-                            const T2 *row = S + ((size_t)m * ny + sj) * b.pk + ks;
-                            const T2 x = row[0];
-                            Xr += ck[m] * (double)x.x;
-                            Xi += ck[m] * (double)x.y;
-                            if (two) {
-                                const T2 y = row[b.pk];
-                                Yr += ck[m] * (double)y.x;
-                                Yi += ck[m] * (double)y.y;
-                            }
-                        }
-                        if (!lo) { Xi = -Xi; Yi = -Yi; }
-                        if (kk == 0 || 2 * kk == M) { Xi = 0.0; Yi = 0.0; }
-                        // conj(ftnorm (X + iY))
-                        T2 v;
-                        v.x = (T)(ftn * Xr - ftn * Yi);
-                        v.y = (T)(-(ftn * Xi + ftn * Yr));
-                        za[fpad(kk)] = v;
-                    }
-                }
-            }
-            bar_sync(1, nfft);
-            T2 *z = za;
-            if (ip) fft_inplace<T>(za, M, (const T2 *)b.tw, live ? t : M, 1, nfft);
-            else z = fft_run<T, 16>(za, za + LB, M, b.rad, b.nrad, (const T2 *)b.tw, live ? t : TT, TT, 1, nfft);
-            if (base == 0) __syncthreads();      // the scalar phase's results
-            if (live) {
-                const int supp = sS.supp;
-                for (int lr = 0; lr < nr; ++lr) {
-                    const int j = jlo + lr;
-                    double homy = 0.0;           // channel: the y-only correction of row j
-                    if (b.cyclic) {
-                        homy = ck[0] * (sS.c_bt * b.hbt[j]);
-#pragma unroll
-                        for (int m = 1; m < NL; ++m)
-                            homy += ck[m] * (sS.c_bc1[m] * b.hbc1[m * nyp + j] + sS.c_bc2[m] * b.hbc2[m * nyp + j]);
-                    }
-#pragma unroll 1
-                    for (int i = t; i < nxp; i += TT) {
-                        double pv;
-                        if (!b.cyclic) {
-                            double hom = 0.0;
-#pragma unroll
-                            for (int m = 1; m < NL; ++m)
-                                hom += ck[m] * (sS.alpha[m - 1] * (double)H[((size_t)(m - 1) * nyp + j) * px + i]);
-                            double zv = 0.0;
-                            if (i >= 1 && i <= n) {
-                                const T2 zz = z[fpad(i)];
-                                zv = lr == 0 ? -(double)zz.y : (double)zz.x;
-                            }
-                            pv = zv + hom;
-                        } else {
-                            const T2 zz = z[fpad(i == nxp - 1 ? 0 : i)];
-                            pv = (lr == 0 ? (double)zz.x : -(double)zz.y) + homy;
-                        }
-                        const T pn = (T)pv;
-                        const size_t o = (size_t)k * n2 + (size_t)j * px + i;
-                        Pnew[o] = supp ? (T)((T)0.5 * (pn + Pold[o])) : pn;
-                        if (!b.cyclic) {
-                            const int slot = i == 0 ? 0 : i == 1 ? 1 : i == nxp - 2 ? 2 : i == nxp - 1 ? 3 : -1;
-                            if (slot >= 0) stash[k][lr][slot] = pn;
-                        }
-                        if (j == 1) wadj[(size_t)k * px + i] = pn;
-                        if (j == nyp - 2) wadj[((size_t)NL + k) * px + i] = pn;
-                    }
-                }
-            }
-            bar_sync(1, nfft);                   // the buffers are free for the next round
-        }
-    }
-    __syncthreads();
-
-    // the wall rows' p (the homogeneous part alone: the modal solutions are
-    // zero there), ocqbdy on the walls of these rows, and the
-    // suppress_comp_mode average of q (driver.F90:180)
-    const int supp = sS.supp;
-    double ctm[NL * NL];
-#pragma unroll
-    for (int x = 0; x < NL * NL; ++x) ctm[x] = b.ctm2l[x];
-    auto p_wall_row = [&](int k, int j, int i) -> T {
-        double s2 = 0.0;
-        if (!b.cyclic) {
-#pragma unroll
-            for (int m = 1; m < NL; ++m)
-                s2 += ctm[m + NL * k] * (sS.alpha[m - 1] * (double)H[((size_t)(m - 1) * nyp + j) * px + i]);
-        } else {
-            s2 = ctm[NL * k] * (sS.c_bt * b.hbt[j]);
-#pragma unroll
-            for (int m = 1; m < NL; ++m)
-                s2 += ctm[m + NL * k] * (sS.c_bc1[m] * b.hbc1[m * nyp + j] + sS.c_bc2[m] * b.hbc2[m * nyp + j]);
-        }
-        return (T)s2;
-    };
-    // unaveraged p at (i, j) of these rows or of the rows next to the walls
-    auto p_at = [&](int k, int j, int i) -> T {
-        if (j == 0 || j == nyp - 1) return p_wall_row(k, j, i);
-        if (!b.cyclic && j >= jlo && j < jhi && (i <= 1 || i >= nxp - 2))
-            return stash[k][j - jlo][i == 0 ? 0 : i == 1 ? 1 : i == nxp - 2 ? 2 : 3];
-        return j == 1 ? wadj[(size_t)k * px + i] : wadj[((size_t)NL + k) * px + i];
-    };
-    T *Qc = (T *)b.F[3 - par];        // q after this step
-    const T *Qm = (const T *)b.F[2 + par];
-    const T fac = (T)b.qb_fac;
-    const FastDiv fdx(nxp);
-    for (int idx = threadIdx.x; idx < nra * nxp; idx += blockDim.x) {
-        const int lr = fdx.div(idx), i = idx - lr * nxp;
-        const int j = jfirst + lr;
-        const bool zon = (j == 0 || j == nyp - 1);
-        const bool mer = !b.cyclic && (i == 0 || i == nxp - 1);
-        if (zon) {
-#pragma unroll
-            for (int k = 0; k < NL; ++k) {
-                const size_t o = (size_t)k * n2 + (size_t)j * px + i;
-                const T pn = p_wall_row(k, j, i);
-                Pnew[o] = supp ? (T)((T)0.5 * (pn + Pold[o])) : pn;
-            }
-        }
-        if (!zon && !mer) {
-            if (supp)
-                for (int k = 0; k < NL; ++k) {
-                    const size_t o3 = ((size_t)k * nyp + j) * px + i;
-                    Qc[o3] = (T)0.5 * (Qc[o3] + Qm[o3]);
-                }
-            continue;
-        }
-        const int cnt = (zon ? 1 : 0) + (mer ? 1 : 0);
-        T pv[NL];
-#pragma unroll
-        for (int k = 0; k < NL; ++k) pv[k] = p_at(k, j, i);
-#pragma unroll
-        for (int k = 0; k < NL; ++k) {
-            T qv;
-            if (mer) qv = (i == 0) ? fac * (p_at(k, j, 1) - pv[k]) : fac * (p_at(k, j, nxp - 2) - pv[k]);
-            else qv = (j == 0) ? fac * (p_at(k, 1, i) - pv[k]) : fac * (p_at(k, nyp - 2, i) - pv[k]);
-            double mv = 0.0;
-#pragma unroll
-            for (int l = 0; l < NL; ++l) mv += b.amat[k + NL * l] * (double)pv[l];
-            const T fmv = (T)(b.fnot * mv);
-            const T by = (T)(b.beta * b.yprel[j]);
-            for (int c = 0; c < cnt; ++c) qv = qv - fmv;
-            // (FP32 storage holds q - beta y: one beta y fewer)
-            for (int c = q_anom_stored<T>() ? 1 : 0; c < cnt; ++c) qv = qv + by;
-            if (k == b.kt && b.topo_active) {
-                const T dd = (T)b.ddyn[(size_t)j * px + i];
-                for (int c = 0; c < cnt; ++c) qv = qv + dd;
-            }
-            const size_t o3 = ((size_t)k * nyp + j) * px + i;
-            Qc[o3] = supp ? (T)((T)0.5 * (qv + Qm[o3])) : qv;
-        }
-    }
-}
 // ------------------------------------------------------------------ init / aux
 // Laplacian with the wall condition on a global FP64 field (one layer),
 // numerics.F90:410-468; the channel's column nxp-1 repeats column 0.
