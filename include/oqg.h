@@ -270,7 +270,7 @@ int oqg_profile_phases(oqg_handle *h, double tdt, int nsteps, double *ms);
 /* CUDA stream of the handle (a cudaStream_t). */
 int oqg_stream(oqg_handle *h, void **stream);
 
-/* Measures the vorticity kernel's tile heights (8..17 rows of 60 columns)
+/* Measures the vorticity kernel's tile heights (8, 12 and 16 rows of 60 columns)
  * on the device: for each, nsteps (>= 2) steps of tdt from the handle's
  * current state, timed with CUDA events; keeps the fastest, restores the
  * state, and records the height for the basin's shape and precision, so

@@ -127,10 +127,21 @@ static void launch_pdl(void (*kern)(KArgs...), int grid, int block, size_t smem,
     cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...);
 }
 
+// The vorticity kernel instance of a tile height (vort_tile_ok).
+typedef void (*VortFn)(const BasinDev *, const Work *, int, double);
+template <class T, int NL>
+static VortFn vort_kernel(int vt) {
+    switch (vt) {
+        case 8: return k_vort<T, NL, 8>;
+        case 12: return k_vort<T, NL, 12>;
+        default: return k_vort<T, NL, 16>;
+    }
+}
+
 template <class T, int NL, int E>
 static void launch_step_t(oqg_handle *h, int par, double tdt) {
     const BasinDev &b = h->hb;
-    launch_pdl(k_vort<T, NL>, h->nv, VTHREADS, h->smem_v, h->st, h->d_bas, h->d_wv, par, tdt);
+    launch_pdl(vort_kernel<T, NL>(h->hb.vty), h->nv, VTHREADS, h->smem_v, h->st, h->d_bas, h->d_wv, par, tdt);
     launch_pdl(k_xfwd<T, E>, h->nx, h->xthreads, h->smem_x, h->st, h->d_bas, h->d_wx, (const void *)nullptr);
     if (b.cyclic)
         launch_pdl(k_ysolve<T, true, NL>, h->nys, 32 * h->KB, h->smem_y, h->st, h->d_bas, h->d_wy);
@@ -187,7 +198,7 @@ static void raise_smem(const void *fn, size_t bytes) {
 
 template <class T, int NL, int E>
 static void raise_step_smem(size_t v, size_t x, size_t y, size_t i) {
-    raise_smem((const void *)k_vort<T, NL>, v);
+    for (int vt : {8, 12, 16}) raise_smem((const void *)vort_kernel<T, NL>(vt), v);
     raise_smem((const void *)k_xfwd<T, E>, x);
     raise_smem((const void *)k_ysolve<T, true, NL>, y);
     raise_smem((const void *)k_ysolve<T, false, NL>, y);
@@ -498,7 +509,7 @@ template <class T, int NL, int E>
 static void launch_phase_t(oqg_handle *h, int phase, int par, double tdt) {
     const BasinDev &b = h->hb;
     switch (phase) {
-        case 0: k_vort<T, NL><<<h->nv, VTHREADS, h->smem_v, h->st>>>(h->d_bas, h->d_wv, par, tdt); break;
+        case 0: vort_kernel<T, NL>(b.vty)<<<h->nv, VTHREADS, h->smem_v, h->st>>>(h->d_bas, h->d_wv, par, tdt); break;
         case 1: k_xfwd<T, E><<<h->nx, h->xthreads, h->smem_x, h->st>>>(h->d_bas, h->d_wx, nullptr); break;
         case 2:
             if (b.cyclic)
@@ -555,7 +566,7 @@ struct oqg_ensemble {
 // descriptor (tdt = 0).
 template <class T, int NL, int E>
 static void launch_ens_step_t(oqg_ensemble *e, int par) {
-    launch_pdl(k_vort<T, NL>, e->nv, VTHREADS, e->smem_v, e->st, e->d_bas, e->d_wv, par, 0.0);
+    launch_pdl(vort_kernel<T, NL>(e->hb[0].vty), e->nv, VTHREADS, e->smem_v, e->st, e->d_bas, e->d_wv, par, 0.0);
     launch_pdl(k_xfwd<T, E>, e->nx, e->xthreads, e->smem_x, e->st, e->d_bas, e->d_wx, (const void *)nullptr);
     if (e->cyclic)
         launch_pdl(k_ysolve<T, true, NL>, e->nys, 128, e->smem_y, e->st, e->d_bas, e->d_wy);
@@ -689,9 +700,9 @@ static int create_impl(const oqg_params *prm, oqg_handle **out, bool batched) {
         cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, 0);
         const int slots = 2 * nsm;
         b.tiles_x = (P.nxp + VTX - 1) / VTX;
-        int best = VTYMAX;
+        int best = 16;
         long best_cost = -1;
-        for (int vt = VTYMAX; vt >= 8 && !batched; --vt) {
+        for (int vt = 16; vt >= 8 && !batched; vt -= 4) {          // the compiled heights
             const int ty = (P.nyp + vt - 1) / vt;
             const long waves = ((long)b.tiles_x * ty + slots - 1) / slots;
             const long cost = waves * (vt + 6);
@@ -2139,7 +2150,7 @@ int oqg_autotune(oqg_handle *h, double tdt, int nsteps, int *best_vty, double *m
     int rc = oqg_state_save(h, save);
     int best = h->hb.vty;
     float best_ms = -1.0f;
-    for (int vt = 8; vt <= VTYMAX && rc == OQG_OK; ++vt) {
+    for (int vt = 8; vt <= 16 && rc == OQG_OK; vt += 4) {           // the compiled heights
         if ((rc = set_vty(h, vt))) break;
         // warm up (captures the graphs), then time nsteps from the saved state
         if ((rc = oqg_state_load(h, save)) || (rc = oqg_step(h, tdt, nsteps))) break;
@@ -2246,7 +2257,7 @@ int oqg_ensemble_autotune(oqg_ensemble *e, const double *tdt, int nsteps, int *b
     int rc = each(false);
     int best = e->hb[0].vty;
     float best_ms = -1.0f;
-    for (int vt = 8; vt <= VTYMAX && rc == OQG_OK; ++vt) {
+    for (int vt = 8; vt <= 16 && rc == OQG_OK; vt += 4) {           // the compiled heights
         if ((rc = ens_set_vty(e, vt)) || (rc = each(true)) || (rc = oqg_ensemble_step(e, tdt, nsteps))) break;
         if ((rc = oqg_ensemble_sync(e)) || (rc = each(true))) break;
         cudaEventRecord(e0, e->st);

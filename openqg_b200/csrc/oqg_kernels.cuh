@@ -279,12 +279,18 @@ __host__ __device__ __forceinline__ size_t vort_smem_bytes(int vt, int esz) {
 #define OQG_TMAP_BYTES 128
 
 // tdt = 0: each member steps with its own b.tdt_m (ensemble launches).
-template <class T, int NL>
+// VT: the tile's rows (b.vty), a compile-time multiple of 4 (vort_tile_rows),
+// so every strip's row loop has a fixed trip count: the loops unroll with no
+// predicates and the rolling windows live in renamed registers.
+template <class T, int NL, int VT>
 __global__ void __launch_bounds__(VTHREADS, 2)
 k_vort(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par, double tdt) {
+    static_assert(VT % 4 == 0 && VT >= 8 && VT <= VTYMAX, "tile rows: a multiple of 4 in [8, VTYMAX]");
     constexpr int LPQ = VTX + 8, L2 = VTX + 4, L1 = VTX + 2, LO = VTX;
-    constexpr int RMAX = (VTYMAX + 3) / 4;     // output rows per strip
-    constexpr int R2MAX = (VTYMAX + 4 + 3) / 4, R1MAX = (VTYMAX + 2 + 3) / 4;
+    constexpr int HPM = VT + 6, H2 = VT + 4, H1 = VT + 2;
+    // rows per strip of each phase (4 strips); the last d4 strip starts
+    // early and recomputes a row or two of its neighbour (the same values)
+    constexpr int RMAX = VT / 4, R2MAX = H2 / 4, R1MAX = (H1 + 3) / 4;
     const Work w = work[blockIdx.x];
     const BasinDev &b = bas[w.member];
     // uniform constants in shared memory: fx fy fxb fyb jac | c_ent1 c_wind
@@ -308,9 +314,7 @@ k_vort(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par,
     if (threadIdx.x < NL * NL) sCtl[threadIdx.x] = b.ctl2m[threadIdx.x];
     GeoS<T> g;
     g.nxp = b.nxp; g.nyp = b.nyp; g.cyclic = b.cyclic; g.K = sK;
-    const int VT = b.vty;
     const VortLayout LY = vort_layout(VT, (int)sizeof(T));
-    const int HPM = LY.HPM, H2 = LY.H2, H1 = LY.H1;
     const int tile_x = w.block % b.tiles_x, tile_y = w.block / b.tiles_x;
     const int i0 = tile_x * VTX, j0 = tile_y * VT;
 
@@ -373,7 +377,7 @@ k_vort(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par,
     issue(0);
 
     // strips of rows: [ty*R, ty*R + R) of each region
-    const int R2 = (H2 + 3) >> 2, R1 = (H1 + 3) >> 2, R0 = (VT + 3) >> 2;
+    constexpr int R2 = R2MAX, R1 = R1MAX, R0 = RMAX;
     const int r0 = ty * R0;
     double acc[RMAX][NL];
 #pragma unroll
@@ -427,13 +431,13 @@ k_vort(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par,
                 const int gi = i0 - 2 + tx, cs = tx + 2;          // column in the pm tile
                 const bool cv = colok(gi);
                 const bool wl = !g.cyclic && gi == 0, wr = !g.cyclic && gi == nxp - 1;
-                const int rb = ty * R2;
+                const int rb = ty * R2;          // H2 = 4 R2: the strips tile exactly
                 const T *col = sPM + rb * LPQ + cs;
                 T sv = col[0], cv_ = col[LPQ];
     #pragma unroll
                 for (int u = 0; u < R2MAX; ++u) {
                     const int r = rb + u;
-                    if (u < R2 && r < H2) {
+                    {
                         const T nv = col[(u + 2) * LPQ];
                         const T wv = col[(u + 1) * LPQ - 1], ev = col[(u + 1) * LPQ + 1];
                         const int gj = j0 - 2 + r;
@@ -454,13 +458,13 @@ k_vort(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par,
                 const int gi = i0 - 1 + tx, cs = tx + 1;          // column in the d2 tile
                 const bool cv = colok(gi);
                 const bool wl = !g.cyclic && gi == 0, wr = !g.cyclic && gi == nxp - 1;
-                const int rb = ty * R1;
+                const int rb = min(ty * R1, H1 - R1);
                 const T *col = sD2 + rb * L2 + cs;
                 T sv = col[0], cv_ = col[L2];
     #pragma unroll
                 for (int u = 0; u < R1MAX; ++u) {
                     const int r = rb + u;
-                    if (u < R1 && r < H1) {
+                    {
                         const T nv = col[(u + 2) * L2];
                         const T wv = col[(u + 1) * L2 - 1], ev = col[(u + 1) * L2 + 1];
                         const int gj = j0 - 1 + r;
@@ -502,7 +506,7 @@ k_vort(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par,
                 for (int u = 0; u < RMAX; ++u) {
                     const int r = r0 + u;
                     const int gj = j0 + r;
-                    if (u < R0 && r < VT) {
+                    {
                         // shift the windows down one row and load the new bottom row
                         const T d4n = d4col[(u + 2) * L1];
                         const T d4w = d4col[(u + 1) * L1 - 1], d4e = d4col[(u + 1) * L1 + 1];
@@ -617,7 +621,7 @@ k_vort(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par,
         for (int u = 0; u < RMAX; ++u) {
             const int r = r0 + u;
             const int gj = j0 + r, gi = i0 + tx;
-            if (u >= R0 || r >= VT || gj < 1 || gj > nyp - 2) continue;
+            if (gj < 1 || gj > nyp - 2) continue;
             const int xi = gi - ioff;
             if (xi < 0 || xi >= b.nxin) continue;
 #pragma unroll

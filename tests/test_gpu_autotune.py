@@ -46,8 +46,8 @@ def test_autotune_keeps_state_and_results(precision, channel):
     ref.step(tdt, 3)
     before = g.get_state()
     best, ms = g.autotune(tdt, 6)
-    assert 8 <= best <= 17 and g.tile_rows() == best
-    assert sorted(ms) == list(range(8, 18)) and all(v > 0 for v in ms.values())
+    assert best in (8, 12, 16) and g.tile_rows() == best
+    assert sorted(ms) == [8, 12, 16] and all(v > 0 for v in ms.values())
     for a, r in zip(g.get_state(), before):
         assert np.array_equal(a, r)
     assert g.step_index() == 3

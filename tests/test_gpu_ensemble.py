@@ -119,8 +119,8 @@ def test_ensemble_autotune_keeps_states_and_results():
     e, singles = _run_pair(members, 3600.0, 2)
     before = [e.get_state(i) for i in range(len(members))]
     best, ms = e.autotune(3600.0, 4)
-    assert 8 <= best <= 17
-    assert sorted(ms) == list(range(8, 18))
+    assert best in (8, 12, 16)
+    assert sorted(ms) == [8, 12, 16]
     for i in range(len(members)):
         for a, r in zip(e.get_state(i), before[i]):
             assert np.array_equal(a, r)
