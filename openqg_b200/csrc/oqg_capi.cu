@@ -832,7 +832,7 @@ static int create_impl(const oqg_params *prm, oqg_handle **out, bool batched) {
     // y-solve: 4 columns (warps) per CTA; the padded column tile (pivots come through L1)
     h->KB = 4;
     const int S_ = (b.ny + 31) / 32;
-    const int LDy = (b.ny + 32) | 1;
+    const int LDy = ysolve_ld(b.ny);
     (void)S_;
     h->nys = b.nl * ((b.nk + h->KB - 1) / h->KB);
     b.k4_rows = 2;
@@ -1587,7 +1587,7 @@ int oqg_ensemble_create(const oqg_params *members, int nmembers, oqg_ensemble **
         const size_t xrow = (size_t)((b.nxin + 3) & ~3);
         e->smem_x = std::max(e->smem_x, fft_inplace_len(b.M) ? (size_t)G * (LB * t2 + 2 * xrow * esz)
                                                                : (size_t)G * 2 * LB * t2);
-        e->smem_y = std::max(e->smem_y, (size_t)((b.ny + 32) | 1) * 4 * vsz);
+        e->smem_y = std::max(e->smem_y, (size_t)ysolve_ld(b.ny) * 4 * vsz);
         e->smem_i = std::max(e->smem_i, xinv_smem(b.M, b.nl, nra, b.nxp, nfft_e, esz, b.inh_g != nullptr));
     }
     if (e->smem_x > 227 * 1024 || e->smem_i > 227 * 1024 || e->smem_v > 227 * 1024) {

@@ -191,6 +191,13 @@ template <class T> struct Dft<T, 16> {
 // unit-stride loads both spread over all banks.
 __device__ __forceinline__ int fpad(int i) { return i + (i >> 3); }
 __host__ __device__ __forceinline__ int fft_buf_len(int M) { return M + (M >> 3) + 4; }
+// fpad(i + r S) for a compile-time stride S: when S is a multiple of 8 the
+// pad of i + r S is the pad of i plus r S / 8, so the index is affine in r
+// (one address per butterfly, constant offsets for its R values).
+template <int S> __device__ __forceinline__ int fpad_step(int i, int r) {
+    if constexpr (S % 8 == 0) return fpad(i) + r * (S + S / 8);
+    else return fpad(i + r * S);
+}
 
 // One Stockham stage of radix R: src -> dst (both shared, padded, length M).
 // Threads t < TT of the transform's group each take butterflies t, t+TT, ...
@@ -299,7 +306,7 @@ __device__ __forceinline__ void fft_stage_ct(const typename C2<T>::t *__restrict
             const int q = j / Ns, jm = j - q * Ns;
             T2 v[R];
 #pragma unroll
-            for (int r = 0; r < R; ++r) v[r] = src[fpad(j + r * nb)];
+            for (int r = 0; r < R; ++r) v[r] = src[fpad_step<nb>(j, r)];
             if (Ns > 1 && jm != 0) {
                 const T2 *w = tws + jm * (R - 1);
 #pragma unroll
@@ -308,7 +315,7 @@ __device__ __forceinline__ void fft_stage_ct(const typename C2<T>::t *__restrict
             Dft<T, R>::run(v);
             const int d = q * Ns * R + jm;
 #pragma unroll
-            for (int r = 0; r < R; ++r) dst[fpad(d + r * Ns)] = v[r];
+            for (int r = 0; r < R; ++r) dst[fpad_step<Ns>(d, r)] = v[r];
         }
     }
 }
@@ -346,7 +353,7 @@ __device__ __forceinline__ void fft_stage_ip(typename C2<T>::t *buf, const typen
 #pragma unroll
         for (int u = 0; u < NB; ++u)
 #pragma unroll
-            for (int r = 0; r < R; ++r) v[u][r] = buf[fpad(t + u * TT + r * nb)];
+            for (int r = 0; r < R; ++r) v[u][r] = buf[fpad_step<nb>(t + u * TT, r)];
     }
     bar_sync(bar_id, nbar);
     if (live) {
@@ -362,7 +369,7 @@ __device__ __forceinline__ void fft_stage_ip(typename C2<T>::t *buf, const typen
             Dft<T, R>::run(v[u]);
             const int d = q * Ns * R + jm;
 #pragma unroll
-            for (int r = 0; r < R; ++r) buf[fpad(d + r * Ns)] = v[u][r];
+            for (int r = 0; r < R; ++r) buf[fpad_step<Ns>(d, r)] = v[u][r];
         }
     }
     bar_sync(bar_id, nbar);

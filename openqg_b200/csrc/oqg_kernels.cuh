@@ -760,32 +760,34 @@ template <> __device__ __forceinline__ float2 yt_store2<float2>(double2 v) { ret
 __device__ __forceinline__ double yt_re(double v) { return v; }
 __device__ __forceinline__ double yt_re(double2 v) { return v.x; }
 
-// The column solve of one warp with each lane's rows [s, s+n) (n <= SM)
-// held in registers through all four passes: forward elimination as an
-// affine scan (chunk pass, warp scan of the chunk maps, chunk pass), then back
-// substitution the same way from the bottom.  col: the column in shared
+// The column solve of one warp with each lane's rows [s, s+SM) held in
+// registers through all four passes: forward elimination as an affine scan
+// (chunk pass, warp scan of the chunk maps, chunk pass), then back
+// substitution the same way from the bottom.  Rows at or beyond ny are
+// padding: their value and pivot are zero, so they map everything to zero in
+// both sweeps and the last row's zero neighbour below needs no special case;
+// the passes then run without per-row predicates.  col: the column in shared
 // memory at padded offset o; piv: its pivots (global, plen stored).
 #define YREG 16
 template <class V, int SM>
 __device__ __forceinline__ void ysolve_chunk_regs(V *col, const double *__restrict__ piv, int plen, double a,
-                                                  int lane, int s, int n,
-                                                  int o, int ny, CSum &colsum) {
+                                                  int lane, int s, int o, int ny, CSum &colsum) {
     V x[SM];
     double bt[SM];
 #pragma unroll
     for (int t = 0; t < SM; ++t) {
-        x[t] = t < n ? col[o + t] : yt_zero(V());
-        bt[t] = t < n ? __ldg(piv + min(s + t, plen - 1)) : 0.0;
+        const bool in = s + t < ny;
+        x[t] = in ? col[o + t] : yt_zero(V());
+        bt[t] = in ? __ldg(piv + min(s + t, plen - 1)) : 0.0;
     }
     // forward elimination: u_j = f_j beta_j - a beta_j u_{j-1}
     V C = yt_zero(V());
     double D = 1.0;
 #pragma unroll
-    for (int t = 0; t < SM; ++t)
-        if (t < n) {
-            C = yt_axpy(yt_scale(x[t], bt[t]), -a * bt[t], C);
-            D = -a * bt[t] * D;
-        }
+    for (int t = 0; t < SM; ++t) {
+        C = yt_axpy(yt_scale(x[t], bt[t]), -a * bt[t], C);
+        D = -a * bt[t] * D;
+    }
     for (int q = 1; q < 32; q <<= 1) {
         V Co = yt_up(C, q);
         double Do = shfl_up_d(D, q);
@@ -794,21 +796,19 @@ __device__ __forceinline__ void ysolve_chunk_regs(V *col, const double *__restri
     V uu = yt_up(C, 1);
     if (lane == 0) uu = yt_zero(V());
 #pragma unroll
-    for (int t = 0; t < SM; ++t)
-        if (t < n) {
-            uu = yt_axpy(yt_scale(x[t], bt[t]), -a * bt[t], uu);
-            x[t] = uu;
-        }
+    for (int t = 0; t < SM; ++t) {
+        uu = yt_axpy(yt_scale(x[t], bt[t]), -a * bt[t], uu);
+        x[t] = uu;
+    }
     // back substitution: u_j = u'_j - a beta_j u_{j+1}
     C = yt_zero(V());
     D = 1.0;
 #pragma unroll
-    for (int t = SM - 1; t >= 0; --t)
-        if (t < n) {
-            const double ej = (s + t == ny - 1) ? 0.0 : -a * bt[t];
-            C = yt_axpy(x[t], ej, C);
-            D = ej * D;
-        }
+    for (int t = SM - 1; t >= 0; --t) {
+        const double ej = -a * bt[t];
+        C = yt_axpy(x[t], ej, C);
+        D = ej * D;
+    }
     for (int q = 1; q < 32; q <<= 1) {
         V Co = yt_dn(C, q);
         double Do = shfl_dn_d(D, q);
@@ -817,16 +817,28 @@ __device__ __forceinline__ void ysolve_chunk_regs(V *col, const double *__restri
     uu = yt_dn(C, 1);
     if (lane == 31) uu = yt_zero(V());
 #pragma unroll
-    for (int t = SM - 1; t >= 0; --t)
-        if (t < n) {
-            const double ej = (s + t == ny - 1) ? 0.0 : -a * bt[t];
-            uu = yt_axpy(x[t], ej, uu);
-            x[t] = uu;
-            colsum.add(yt_re(uu));
-        }
+    for (int t = SM - 1; t >= 0; --t) {
+        const double ej = -a * bt[t];
+        uu = yt_axpy(x[t], ej, uu);
+        x[t] = uu;
+        colsum.add(yt_re(uu));
+    }
 #pragma unroll
     for (int t = 0; t < SM; ++t)
-        if (t < n) col[o + t] = x[t];
+        if (s + t < ny) col[o + t] = x[t];
+}
+
+// Rows per lane of the y-solve and the padded column length of its tile:
+// grids of up to 32 YREG rows take YREG rows per lane (the register path),
+// wider ones ceil(ny/32).
+__host__ __device__ __forceinline__ int ysolve_rows_per_lane(int ny) {
+    return ny <= 32 * YREG ? YREG : (ny + 31) >> 5;
+}
+__host__ __device__ __forceinline__ int ysolve_ld(int ny) {
+    const int s = ysolve_rows_per_lane(ny);
+    const int need = 32 * (s + 1) + 1;                 // 32 lanes of s rows, one pad each
+    const int ld = (ny + 32) | 1;
+    return ld > need ? ld : (need | 1);
 }
 
 template <class T, bool CPLX, int NL>
@@ -845,8 +857,8 @@ k_ysolve(const BasinDev *__restrict__ bas, const Work *__restrict__ work) {
     // Lane `l` owns rows [l S, l S + S).  Columns are stored with one pad word
     // per S rows (row j at j + j / S), so the 32 lanes of a warp reading their
     // chunks hit distinct banks.
-    const int S_ = (ny + 31) >> 5;
-    const int LD = (ny + 32) | 1;            // > (ny-1) + (ny-1)/S, odd
+    const int S_ = ysolve_rows_per_lane(ny);
+    const int LD = ysolve_ld(ny);            // > 32 S + 31 pads, odd
     const FastDiv fdS(S_);
     extern __shared__ __align__(16) unsigned char smem_raw[];
     V *tile = reinterpret_cast<V *>(smem_raw);                 // [KB][LD]
@@ -886,7 +898,7 @@ k_ysolve(const BasinDev *__restrict__ bas, const Work *__restrict__ work) {
         const int o = lane * (S_ + 1);          // padded offset of row s
         const int n = max(e - s, 0);
         CSum colsum;
-        if (S_ <= YREG) ysolve_chunk_regs<V, YREG>(col, piv, plen, a, lane, s, n, o, ny, colsum);
+        if (S_ == YREG) ysolve_chunk_regs<V, YREG>(col, piv, plen, a, lane, s, o, ny, colsum);
         else {
             // forward elimination: u_j = f_j beta_j - a beta_j u_{j-1}
             V C = yt_zero(V());
@@ -1449,8 +1461,9 @@ k_xinv(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par,
     T *Qc = (T *)b.F[3 - par];        // q after this step (qm buffer of K1)
     const T *Qm = (const T *)b.F[2 + par];
     const T fac = (T)b.qb_fac;
-    for (int idx = threadIdx.x; idx < nra * nxp; idx += blockDim.x) {
-        const int lr = fdx.div(idx), i = idx - lr * nxp;
+    // the point (lr, i) of these rows: q's average on a suppression step,
+    // ocqbdy's value on a wall
+    auto wall_point = [&](int lr, int i) {
         const int j = jfirst + lr;
         const bool zon = (j == 0 || j == nyp - 1);
         const bool mer = !b.cyclic && (i == 0 || i == nxp - 1);
@@ -1460,7 +1473,7 @@ k_xinv(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par,
                     const size_t o3 = ((size_t)k * nyp + j) * px + i;
                     Qc[o3] = (T)0.5 * (Qc[o3] + Qm[o3]);
                 }
-            continue;
+            return;
         }
         const int cnt = (zon ? 1 : 0) + (mer ? 1 : 0);
 #define PN(kk, rr, ii) inh[(kk) * ms + (rr) * rs + (ii)]
@@ -1491,6 +1504,16 @@ k_xinv(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par,
             Qc[o3] = supp ? (T)((T)0.5 * (qv + Qm[o3])) : qv;
         }
 #undef PN
+    };
+    // every point on a suppression step and along the zonal walls; else the
+    // two meridional wall points of each row
+    for (int lr = 0; lr < nra; ++lr) {
+        const int j = jfirst + lr;
+        if (supp || j == 0 || j == nyp - 1) {
+            for (int i = threadIdx.x; i < nxp; i += blockDim.x) wall_point(lr, i);
+        } else if (!b.cyclic && threadIdx.x < 2) {
+            wall_point(lr, threadIdx.x == 0 ? 0 : nxp - 1);
+        }
     }
 }
 
