@@ -677,12 +677,21 @@ k_xfwd(const BasinDev *__restrict__ bas, const Work *__restrict__ work, const vo
     if (live) {
         if (!b.cyclic) {
             // odd extension of two rows: z_0 = z_{n+1} = 0, z_{M-jj} = -z_jj
-            for (int jj = t; jj < M; jj += TT) {
-                T2 v;
-                if (jj == 0 || jj == n + 1) { v.x = (T)0; v.y = (T)0; }
-                else if (jj <= n) { v.x = raw[jj - 1]; v.y = two ? raw[RO + jj - 1] : (T)0; }
-                else { const int s2 = M - jj; v.x = -raw[s2 - 1]; v.y = two ? -raw[RO + s2 - 1] : (T)0; }
+            if (t == 0) {
+                T2 zero;
+                zero.x = (T)0;
+                zero.y = (T)0;
+                za[fpad(0)] = zero;
+                za[fpad(n + 1)] = zero;
+            }
+            for (int jj = 1 + t; jj <= n; jj += TT) {
+                T2 v, vm;
+                v.x = raw[jj - 1];
+                v.y = two ? raw[RO + jj - 1] : (T)0;
+                vm.x = -v.x;
+                vm.y = -v.y;
                 za[fpad(jj)] = v;
+                za[fpad(M - jj)] = vm;
             }
         } else {
             for (int jj = t; jj < M; jj += TT) {
@@ -1322,12 +1331,22 @@ k_xinv(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par,
         if (live) {
             if (!b.cyclic) {
                 const T *x = raw, *y = raw + RO;
-                for (int jj = t; jj < M; jj += TT) {
-                    T2 v;
-                    if (jj == 0 || jj == n + 1) { v.x = (T)0; v.y = (T)0; }
-                    else if (jj <= n) { v.x = ftn * x[jj - 1]; v.y = two ? ftn * y[jj - 1] : (T)0; }
-                    else { const int s2 = M - jj; v.x = -(ftn * x[s2 - 1]); v.y = two ? -(ftn * y[s2 - 1]) : (T)0; }
+                // odd extension: z_0 = z_{n+1} = 0, z_{M-jj} = -z_jj
+                if (t == 0) {
+                    T2 zero;
+                    zero.x = (T)0;
+                    zero.y = (T)0;
+                    za[fpad(0)] = zero;
+                    za[fpad(n + 1)] = zero;
+                }
+                for (int jj = 1 + t; jj <= n; jj += TT) {
+                    T2 v, vm;
+                    v.x = ftn * x[jj - 1];
+                    v.y = two ? ftn * y[jj - 1] : (T)0;
+                    vm.x = -v.x;
+                    vm.y = -v.y;
                     za[fpad(jj)] = v;
+                    za[fpad(M - jj)] = vm;
                 }
             } else {
                 const T2 *x = reinterpret_cast<const T2 *>(raw), *y = reinterpret_cast<const T2 *>(raw + RO);
