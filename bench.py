@@ -770,7 +770,8 @@ def run_ours(args):
     e2e_ms = max_over_ranks(statistics.median(e2e_times) * e2e_steps, pg, "cuda")
     e2e_value = replica_value(e2e_ms, ws, cells, msteps, e2e_steps)
     e2e_parts = e2e_breakdown(g, b, L, wk_p, ent_p, p1_p, ts, tn, tdt)
-    h2d = msteps * (b.nxp * b.nyp * 8) * b.nl        # wekp + (nl-1) ent layers
+    # wekp + the ent layers the step reads (a box: ent(:,:,1); a channel: all nl-1)
+    h2d = msteps * (b.nxp * b.nyp * 8) * (b.nl if b.cyclic else 2)
     d2h = msteps * b.nxp * b.nyp * 8
     coupled = None
     if prec == OQG_FP64 and not b.cyclic:
@@ -829,7 +830,7 @@ def run_ours(args):
         "roofline": roof,
         "e2e": {"value": e2e_value, "unit": "Mcell-layer-steps/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "timer": "host clock, median of %d steps" % e2e_steps,
-                "pattern": "per model step: upload wekp+ent, step, read p(:,:,1)",
+                "pattern": "per model step: upload wekp+ent (the layers the step reads), step, read p(:,:,1)",
                 "parts_ms_per_model_step": e2e_parts},
         "e2e_coupled_ocean": coupled,
         "gpu_launches": args.steps * msteps * launches_per_step(g),

@@ -120,7 +120,11 @@ int oqg_get_p_layer(oqg_handle *h, int k, double *out);
 
 /* Forcing of step_qg: wekp (nxp,nyp), ent (nxp,nyp,nl-1) or NULL for zero
  * entrainment, and the channel wind-stress integrals txis, txin.  Stored on
- * the device and reused by every step until set again. */
+ * the device and reused by every step until set again.  A closed box's step
+ * reads ent(:,:,1) alone (vorticity.F90:71-72, pressure.F90:52-53), so for a
+ * box only that layer is copied (the device keeps zeros in the others); a
+ * channel copies every layer (its momentum constraints read layer 2's wall
+ * rows, vorticity.F90:88-93). */
 int oqg_set_forcing(oqg_handle *h, const double *wekp, const double *ent,
                     double txis, double txin);
 
@@ -358,7 +362,8 @@ int oqg_oml_get_sst(oqg_oml *m, double *sst, double *sstm);
 int oqg_ocean_forcing(oqg_oml *m, const double *taux, const double *tauy,
                       const double *fnetoc, int compute_ent, double tdto);
 /* The handle's forcing, wekp (nxp, nyp) and ent (nxp, nyp, nl-1), copied
- * to host arrays (either may be NULL). */
+ * to host arrays (either may be NULL); for a box the layers after the first
+ * are the zeros the step reads in their place. */
 int oqg_get_forcing(oqg_handle *h, double *wekp, double *ent);
 
 /* The atmosphere half: the Ekman fields of a channel and the atmospheric

@@ -1018,8 +1018,12 @@ int oqg_set_forcing(oqg_handle *h, const double *wekp, const double *ent, double
     // and integral kernels run on the stream after it returns
     if (wekp)
         CK(cudaMemcpyAsync(h->hrow, wekp, plane * sizeof(double), cudaMemcpyHostToDevice, h->st));
+    // a closed box's step reads ent(:,:,1) alone (vorticity.F90:71-72,
+    // pressure.F90:52-53): only that layer crosses; a channel's momentum
+    // constraints also read layer 2's wall rows (vorticity.F90:88-93)
+    const int ent_layers = b.cyclic ? b.nl - 1 : 1;
     if (ent)
-        CK(cudaMemcpyAsync(h->hrow + plane, ent, (b.nl - 1) * plane * sizeof(double), cudaMemcpyHostToDevice,
+        CK(cudaMemcpyAsync(h->hrow + plane, ent, ent_layers * plane * sizeof(double), cudaMemcpyHostToDevice,
                            h->st));
     CK(cudaEventRecord(h->up_ev, h->st));
     if (wekp) {
@@ -1030,7 +1034,7 @@ int oqg_set_forcing(oqg_handle *h, const double *wekp, const double *ent, double
     }
     const void *old_ent = b.ent;
     if (ent) {
-        const size_t nr = (size_t)(b.nl - 1) * b.nyp;
+        const size_t nr = (size_t)ent_layers * b.nyp;
         if (h->mixed) k_rows_in<float><<<296, 256, 0, h->st>>>(h->hrow + plane, (float *)h->ent_buf, b.nxp, b.px, nr);
         else k_rows_in<double><<<296, 256, 0, h->st>>>(h->hrow + plane, (double *)h->ent_buf, b.nxp, b.px, nr);
         b.ent = h->ent_buf;

@@ -838,10 +838,11 @@ __device__ __forceinline__ void ysolve_chunk_regs(V *col, const double *__restri
 }
 
 // Rows per lane of the y-solve and the padded column length of its tile:
-// grids of up to 32 YREG rows take YREG rows per lane (the register path),
-// wider ones ceil(ny/32).
+// grids of up to 32 YREG rows take the smallest of 4, 8 and 16 rows per lane
+// that covers them (the register path, one instance each), wider ones
+// ceil(ny/32).
 __host__ __device__ __forceinline__ int ysolve_rows_per_lane(int ny) {
-    return ny <= 32 * YREG ? YREG : (ny + 31) >> 5;
+    return ny <= 128 ? 4 : ny <= 256 ? 8 : ny <= 32 * YREG ? YREG : (ny + 31) >> 5;
 }
 __host__ __device__ __forceinline__ int ysolve_ld(int ny) {
     const int s = ysolve_rows_per_lane(ny);
@@ -907,7 +908,9 @@ k_ysolve(const BasinDev *__restrict__ bas, const Work *__restrict__ work) {
         const int o = lane * (S_ + 1);          // padded offset of row s
         const int n = max(e - s, 0);
         CSum colsum;
-        if (S_ == YREG) ysolve_chunk_regs<V, YREG>(col, piv, plen, a, lane, s, o, ny, colsum);
+        if (S_ == 4) ysolve_chunk_regs<V, 4>(col, piv, plen, a, lane, s, o, ny, colsum);
+        else if (S_ == 8) ysolve_chunk_regs<V, 8>(col, piv, plen, a, lane, s, o, ny, colsum);
+        else if (S_ == YREG) ysolve_chunk_regs<V, YREG>(col, piv, plen, a, lane, s, o, ny, colsum);
         else {
             // forward elimination: u_j = f_j beta_j - a beta_j u_{j-1}
             V C = yt_zero(V());
