@@ -632,7 +632,11 @@ def roofline_of(g, b, workload, precision, tdt, ms_per_model_step):
             # the whole step: algorithmic bytes over the timed model step
             "step_frac": step_alg / (ms_per_model_step / 1e3) / 1e9 / peak,
             # the phases timed one by one, summed
-            "phases_frac": step_alg / (sum(ms) / 1e3) / 1e9 / peak}
+            "phases_frac": step_alg / (sum(ms) / 1e3) / 1e9 / peak,
+            # the step chain's launches with no work (oqg_launch_floor): the
+            # most a single persistent launch could take off a step
+            "launch_floor_us_per_step": g.launch_floor(16),
+            "launches_per_step": g.step_launches()}
 
 
 def measure_basin(workload, prec, steps, warmup, msteps, flush, rank, pg, seed=None):
@@ -856,7 +860,7 @@ def run_ours(args):
 
 def launches_per_step(g):
     """Kernel launches of one model step of the handle's step path."""
-    return 4
+    return g.step_launches()
 
 
 def main():

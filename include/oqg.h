@@ -274,6 +274,18 @@ int oqg_profile_phases(oqg_handle *h, double tdt, int nsteps, double *ms);
 /* CUDA stream of the handle (a cudaStream_t). */
 int oqg_stream(oqg_handle *h, void **stream);
 
+/* Kernel launches of one model step: 4 (vorticity, forward transform,
+ * y-solve, inverse transform with the assembly), 5 for boxes wide enough
+ * that the inverse transforms run as a launch of their own. */
+int oqg_step_launches(oqg_handle *h, int *launches);
+
+/* The launch floor of the step chain: nsteps steps of launches with the
+ * step kernels' grids, blocks, shared-memory sizes and dependent-launch
+ * chaining but no work, replayed from a CUDA graph on the handle's stream;
+ * the device time per step in microseconds.  For measurement: it tells how
+ * much of a step a single persistent launch could save at most. */
+int oqg_launch_floor(oqg_handle *h, int nsteps, double *us_per_step);
+
 /* Measures the vorticity kernel's tile heights (8, 12 and 16 rows of 60 columns)
  * on the device: for each, nsteps (>= 2) steps of tdt from the handle's
  * current state, timed with CUDA events; keeps the fastest, restores the

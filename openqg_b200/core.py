@@ -72,6 +72,8 @@ def lib():
     L.oqg_ekman_from_tau.argtypes = [vp, _dp, _dp, _dp, _dp, _dp]
     L.oqg_device_state.argtypes = [vp] + [ctypes.POINTER(vp)] * 4 + [ctypes.POINTER(ctypes.c_int)] * 2
     L.oqg_stream.argtypes = [vp, ctypes.POINTER(vp)]
+    L.oqg_step_launches.argtypes = [vp, ctypes.POINTER(ctypes.c_int)]
+    L.oqg_launch_floor.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
     L.oqg_profile_phases.argtypes = [vp, ctypes.c_double, ctypes.c_int, _dp]
     L.oqg_ensemble_create.argtypes = [vp, ctypes.c_int, ctypes.POINTER(vp)]
     L.oqg_ensemble_destroy.argtypes = [vp]
@@ -331,6 +333,18 @@ class QG:
         s = ctypes.c_void_p()
         _check(lib().oqg_stream(self.h, ctypes.byref(s)), "oqg_stream")
         return s.value or 0
+
+    def launch_floor(self, nsteps: int = 16) -> float:
+        """Device microseconds per step of the step chain's launches with no work."""
+        v = ctypes.c_double()
+        _check(lib().oqg_launch_floor(self.h, int(nsteps), ctypes.byref(v)), "oqg_launch_floor")
+        return v.value
+
+    def step_launches(self) -> int:
+        """Kernel launches of one model step (4, or 5 for wide boxes)."""
+        v = ctypes.c_int()
+        _check(lib().oqg_step_launches(self.h, ctypes.byref(v)), "oqg_step_launches")
+        return v.value
 
 
 def init_qg(basin: Basin) -> QG:

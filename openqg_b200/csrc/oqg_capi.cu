@@ -58,6 +58,7 @@ struct oqg_handle {
     Work *d_wv = nullptr, *d_wx = nullptr, *d_wy = nullptr, *d_wi = nullptr;
     int nv = 0, nx = 0, nys = 0, ni = 0;
     int E = 8, KB = 16, xthreads = 128, xi_threads = 64;
+    int yW = 1;                          // warps per y-solve column
     size_t smem_v = 0, smem_x = 0, smem_x64 = 0, smem_y = 0, smem_i = 0, smem_i64 = 0;
     double *stage[2] = {nullptr, nullptr};
     double *hrow = nullptr;     // contiguous host-order copy buffer [nl][nyp][nxp]
@@ -127,6 +128,40 @@ static void launch_pdl(void (*kern)(KArgs...), int grid, int block, size_t smem,
     cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...);
 }
 
+// The y-solve instance for a column spread over W warps (1, 2 or 4) in the
+// box (real) or channel (complex) form.
+template <class T, bool CPLX, int W>
+static void ysolve_w(int grid, size_t smem, cudaStream_t st, const BasinDev *bas, const Work *wy, bool pdl) {
+    if (pdl) launch_pdl(k_ysolve<T, CPLX, W>, grid, 128 * W, smem, st, bas, wy);
+    else k_ysolve<T, CPLX, W><<<grid, 128 * W, smem, st>>>(bas, wy);
+}
+template <class T>
+static void launch_ysolve(bool cplx, int W, int grid, size_t smem, cudaStream_t st, const BasinDev *bas,
+                          const Work *wy, bool pdl) {
+    if (cplx) {
+        if (W == 4) ysolve_w<T, true, 4>(grid, smem, st, bas, wy, pdl);
+        else if (W == 2) ysolve_w<T, true, 2>(grid, smem, st, bas, wy, pdl);
+        else ysolve_w<T, true, 1>(grid, smem, st, bas, wy, pdl);
+    } else {
+        if (W == 4) ysolve_w<T, false, 4>(grid, smem, st, bas, wy, pdl);
+        else if (W == 2) ysolve_w<T, false, 2>(grid, smem, st, bas, wy, pdl);
+        else ysolve_w<T, false, 1>(grid, smem, st, bas, wy, pdl);
+    }
+}
+// Warps per y-solve column for ncols columns of ny rows: enough that the
+// columns put about 20 warps on each of the 148 SMs, as long as every warp
+// keeps 4 or more rows per lane and no lane more than 8 (the register path
+// within the instance's register budget).
+static int ysolve_warps(int ny, long long ncols) {
+    int W = 1;
+    while (W < 4 && ncols * W < 148LL * 20) {
+        const int W2 = 2 * W;
+        if (ny <= 32 * W * 4 || ny > 32 * W2 * 8) break;
+        W = W2;
+    }
+    return W;
+}
+
 // The vorticity kernel instance of a tile height (vort_tile_ok).
 typedef void (*VortFn)(const BasinDev *, const Work *, int, double);
 template <class T, int NL>
@@ -143,10 +178,9 @@ static void launch_step_t(oqg_handle *h, int par, double tdt) {
     const BasinDev &b = h->hb;
     launch_pdl(vort_kernel<T, NL>(h->hb.vty), h->nv, VTHREADS, h->smem_v, h->st, h->d_bas, h->d_wv, par, tdt);
     launch_pdl(k_xfwd<T, E>, h->nx, h->xthreads, h->smem_x, h->st, h->d_bas, h->d_wx, (const void *)nullptr);
-    if (b.cyclic)
-        launch_pdl(k_ysolve<T, true, NL>, h->nys, 32 * h->KB, h->smem_y, h->st, h->d_bas, h->d_wy);
-    else
-        launch_pdl(k_ysolve<T, false, NL>, h->nys, 32 * h->KB, h->smem_y, h->st, h->d_bas, h->d_wy);
+    launch_ysolve<T>(b.cyclic, h->yW, h->nys, h->smem_y, h->st, h->d_bas, h->d_wy, true);
+    if (b.xinv_sep)
+        launch_pdl(k_xinv_rows<T, NL, E>, h->nx + 1, h->xthreads, h->smem_x, h->st, h->d_bas, h->d_wx, 1, par, tdt);
     launch_pdl(k_xinv<T, NL>, h->ni, h->xi_threads, h->smem_i, h->st, h->d_bas, h->d_wi, par, tdt,
                (double *)nullptr);
 }
@@ -160,18 +194,17 @@ static void launch_solve_t(oqg_handle *h, double *out, bool pdl) {
     if (pdl) {
         launch_pdl(k_xfwd<double, E>, h->nx, h->xthreads, h->smem_x64, h->st, h->d_bas64, h->d_wx,
                    (const void *)nullptr);
-        if (h->hb.cyclic)
-            launch_pdl(k_ysolve<double, true, NL>, h->nys, 32 * h->KB, h->smem_y, h->st, h->d_bas64, h->d_wy);
-        else
-            launch_pdl(k_ysolve<double, false, NL>, h->nys, 32 * h->KB, h->smem_y, h->st, h->d_bas64, h->d_wy);
+        launch_ysolve<double>(h->hb.cyclic, h->yW, h->nys, h->smem_y, h->st, h->d_bas64, h->d_wy, true);
+        if (h->hb.xinv_sep)
+            launch_pdl(k_xinv_rows<double, NL, E>, h->nx, h->xthreads, h->smem_x64, h->st, h->d_bas64, h->d_wx, 0, 0,
+                       0.0);
         launch_pdl(k_xinv<double, NL>, h->ni, h->xi_threads, h->smem_i64, h->st, h->d_bas64, h->d_wi, 0, 0.0, out);
         return;
     }
     k_xfwd<double, E><<<h->nx, h->xthreads, h->smem_x64, h->st>>>(h->d_bas64, h->d_wx, nullptr);
-    if (h->hb.cyclic)
-        k_ysolve<double, true, NL><<<h->nys, 32 * h->KB, h->smem_y, h->st>>>(h->d_bas64, h->d_wy);
-    else
-        k_ysolve<double, false, NL><<<h->nys, 32 * h->KB, h->smem_y, h->st>>>(h->d_bas64, h->d_wy);
+    launch_ysolve<double>(h->hb.cyclic, h->yW, h->nys, h->smem_y, h->st, h->d_bas64, h->d_wy, false);
+    if (h->hb.xinv_sep)
+        k_xinv_rows<double, NL, E><<<h->nx, h->xthreads, h->smem_x64, h->st>>>(h->d_bas64, h->d_wx, 0, 0, 0.0);
     k_xinv<double, NL><<<h->ni, h->xi_threads, h->smem_i64, h->st>>>(h->d_bas64, h->d_wi, 0, 0.0, out);
 }
 
@@ -196,12 +229,22 @@ static void raise_smem(const void *fn, size_t bytes) {
         g_smem_set.push_back({{dev, fn}, (int)bytes});
 }
 
+template <class T>
+static void raise_ysolve_smem(size_t y) {
+    raise_smem((const void *)k_ysolve<T, true, 1>, y);
+    raise_smem((const void *)k_ysolve<T, true, 2>, y);
+    raise_smem((const void *)k_ysolve<T, true, 4>, y);
+    raise_smem((const void *)k_ysolve<T, false, 1>, y);
+    raise_smem((const void *)k_ysolve<T, false, 2>, y);
+    raise_smem((const void *)k_ysolve<T, false, 4>, y);
+}
+
 template <class T, int NL, int E>
 static void raise_step_smem(size_t v, size_t x, size_t y, size_t i) {
     for (int vt : {8, 12, 16}) raise_smem((const void *)vort_kernel<T, NL>(vt), v);
     raise_smem((const void *)k_xfwd<T, E>, x);
-    raise_smem((const void *)k_ysolve<T, true, NL>, y);
-    raise_smem((const void *)k_ysolve<T, false, NL>, y);
+    raise_smem((const void *)k_xinv_rows<T, NL, E>, x);
+    raise_ysolve_smem<T>(y);
     raise_smem((const void *)k_xinv<T, NL>, i);
 }
 
@@ -209,8 +252,8 @@ template <class T, int NL, int E>
 static void set_attrs_t(oqg_handle *h) {
     raise_step_smem<T, NL, E>(h->smem_v, h->smem_x, h->smem_y, h->smem_i);
     raise_smem((const void *)k_xfwd<double, E>, h->smem_x64);
-    raise_smem((const void *)k_ysolve<double, true, NL>, h->smem_y);
-    raise_smem((const void *)k_ysolve<double, false, NL>, h->smem_y);
+    raise_smem((const void *)k_xinv_rows<double, NL, E>, h->smem_x64);
+    raise_ysolve_smem<double>(h->smem_y);
     raise_smem((const void *)k_xinv<double, NL>, h->smem_i64);
 }
 
@@ -511,13 +554,12 @@ static void launch_phase_t(oqg_handle *h, int phase, int par, double tdt) {
     switch (phase) {
         case 0: vort_kernel<T, NL>(b.vty)<<<h->nv, VTHREADS, h->smem_v, h->st>>>(h->d_bas, h->d_wv, par, tdt); break;
         case 1: k_xfwd<T, E><<<h->nx, h->xthreads, h->smem_x, h->st>>>(h->d_bas, h->d_wx, nullptr); break;
-        case 2:
-            if (b.cyclic)
-                k_ysolve<T, true, NL><<<h->nys, 32 * h->KB, h->smem_y, h->st>>>(h->d_bas, h->d_wy);
-            else
-                k_ysolve<T, false, NL><<<h->nys, 32 * h->KB, h->smem_y, h->st>>>(h->d_bas, h->d_wy);
+        case 2: launch_ysolve<T>(b.cyclic, h->yW, h->nys, h->smem_y, h->st, h->d_bas, h->d_wy, false); break;
+        default:
+            if (b.xinv_sep)
+                k_xinv_rows<T, NL, E><<<h->nx + 1, h->xthreads, h->smem_x, h->st>>>(h->d_bas, h->d_wx, 1, par, tdt);
+            k_xinv<T, NL><<<h->ni, h->xi_threads, h->smem_i, h->st>>>(h->d_bas, h->d_wi, par, tdt, nullptr);
             break;
-        default: k_xinv<T, NL><<<h->ni, h->xi_threads, h->smem_i, h->st>>>(h->d_bas, h->d_wi, par, tdt, nullptr); break;
     }
 }
 static void launch_phase(oqg_handle *h, int phase, int par, double tdt) {
@@ -542,6 +584,7 @@ struct oqg_ensemble {
     int nv = 0, nx = 0, nys = 0, ni = 0;
     size_t smem_v = 0, smem_x = 0, smem_y = 0, smem_i = 0;
     int xi_threads = 64, xthreads = 128;
+    int yW = 1;                        // warps per y-solve column, one for every member
     int par = 0;
     cudaGraphExec_t gexec[2] = {nullptr, nullptr};
     std::vector<void *> allocs;
@@ -568,10 +611,7 @@ template <class T, int NL, int E>
 static void launch_ens_step_t(oqg_ensemble *e, int par) {
     launch_pdl(vort_kernel<T, NL>(e->hb[0].vty), e->nv, VTHREADS, e->smem_v, e->st, e->d_bas, e->d_wv, par, 0.0);
     launch_pdl(k_xfwd<T, E>, e->nx, e->xthreads, e->smem_x, e->st, e->d_bas, e->d_wx, (const void *)nullptr);
-    if (e->cyclic)
-        launch_pdl(k_ysolve<T, true, NL>, e->nys, 128, e->smem_y, e->st, e->d_bas, e->d_wy);
-    else
-        launch_pdl(k_ysolve<T, false, NL>, e->nys, 128, e->smem_y, e->st, e->d_bas, e->d_wy);
+    launch_ysolve<T>(e->cyclic, e->yW, e->nys, e->smem_y, e->st, e->d_bas, e->d_wy, true);
     launch_pdl(k_xinv<T, NL>, e->ni, e->xi_threads, e->smem_i, e->st, e->d_bas, e->d_wi, par, 0.0,
                (double *)nullptr);
 }
@@ -831,9 +871,8 @@ static int create_impl(const oqg_params *prm, oqg_handle **out, bool batched) {
     const size_t vsz = (size_t)(b.cyclic ? 16 : 8);
     // y-solve: 4 columns (warps) per CTA; the padded column tile (pivots come through L1)
     h->KB = 4;
-    const int S_ = (b.ny + 31) / 32;
-    const int LDy = ysolve_ld(b.ny);
-    (void)S_;
+    h->yW = ysolve_warps(b.ny, (long long)b.nl * b.nk);
+    const int LDy = ysolve_ld(b.ny, h->yW);
     h->nys = b.nl * ((b.nk + h->KB - 1) / h->KB);
     b.k4_rows = 2;
     h->ni = (b.ny + b.k4_rows - 1) / b.k4_rows;
@@ -864,6 +903,15 @@ static int create_impl(const oqg_params *prm, oqg_handle **out, bool batched) {
     h->xi_threads = nfft_i + 32;
     h->smem_i = xinv_smem(b.M, b.nl, nra, b.nxp, nfft_i, h->esz, split);
     h->smem_i64 = xinv_smem(b.M, b.nl, nra, b.nxp, nfft_i, 8, split);
+    // wide boxes: the inverse transforms run as a launch of their own, shaped
+    // like the forward one, and the assembly kernel needs no shared buffers
+    b.xinv_sep = (split && !b.cyclic) ? 1 : 0;
+    b.scal_g = nullptr;
+    if (b.xinv_sep) {
+        h->smem_i = h->smem_i64 = 0;
+        b.scal_g = dalloc<char>(h, sizeof(XinvScal));
+        if (!b.scal_g) return bail(OQG_ECUDA, "out of device memory");
+    }
     if (h->smem_i64 > 227 * 1024 || h->smem_x64 > 227 * 1024 || h->smem_y > 227 * 1024)
         return bail(OQG_EUNSUPPORTED, "grid too large for this build's shared-memory tiling");
     std::vector<Work> wv(h->nv), wx(h->nx), wy(h->nys), wi(h->ni);
@@ -1468,6 +1516,59 @@ int oqg_stream(oqg_handle *h, void **stream) {
     return OQG_OK;
 }
 
+int oqg_step_launches(oqg_handle *h, int *launches) {
+    if (!h || !launches) return fail(OQG_EINVAL, "bad argument");
+    *launches = h->hb.xinv_sep ? 5 : 4;
+    return OQG_OK;
+}
+
+// A launch of the step chain with no work: it triggers its dependent and
+// waits for its predecessor like the step kernels, and nothing else.
+__global__ void k_chain_empty() {
+    pdl_trigger();
+    pdl_wait();
+}
+
+int oqg_launch_floor(oqg_handle *h, int nsteps, double *us_per_step) {
+    if (!h || !us_per_step || nsteps < 1) return fail(OQG_EINVAL, "bad argument");
+    struct Shape { int grid, block; size_t smem; };
+    std::vector<Shape> sh = {{h->nv, VTHREADS, h->smem_v}, {h->nx, h->xthreads, h->smem_x},
+                             {h->nys, 128 * h->yW, h->smem_y}};
+    if (h->hb.xinv_sep) sh.push_back({h->nx + 1, h->xthreads, h->smem_x});
+    sh.push_back({h->ni, h->xi_threads, h->smem_i});
+    size_t mx = 0;
+    for (const Shape &x : sh) mx = std::max(mx, x.smem);
+    raise_smem((const void *)k_chain_empty, mx);
+    cudaGraph_t g = nullptr;
+    cudaGraphExec_t ge = nullptr;
+    CK(cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
+    for (int s = 0; s < nsteps; ++s)
+        for (const Shape &x : sh) launch_pdl(k_chain_empty, x.grid, x.block, x.smem, h->st);
+    CK(cudaStreamEndCapture(h->st, &g));
+    if (cudaGraphInstantiate(&ge, g, 0) != cudaSuccess) {
+        cudaGraphDestroy(g);
+        return fail(OQG_ECUDA, "graph instantiation failed");
+    }
+    cudaEvent_t a, b;
+    CK(cudaEventCreate(&a));
+    CK(cudaEventCreate(&b));
+    for (int i = 0; i < 3; ++i) CK(cudaGraphLaunch(ge, h->st));
+    constexpr int REP = 10;
+    CK(cudaEventRecord(a, h->st));
+    for (int i = 0; i < REP; ++i) CK(cudaGraphLaunch(ge, h->st));
+    CK(cudaEventRecord(b, h->st));
+    CK(cudaEventSynchronize(b));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, a, b));
+    *us_per_step = 1000.0 * ms / ((double)REP * nsteps);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaGraphExecDestroy(ge);
+    cudaGraphDestroy(g);
+    CK(cudaGetLastError());
+    return OQG_OK;
+}
+
 // Scratch of oqg_diag_noalloc (layout in oqg_noalloc.cuh).  Every GPU that
 // loads the library holds these 256 KiB until the process exits.  Host code
 // must not pass the name itself to a kernel: on the host it is only a
@@ -1572,6 +1673,12 @@ int oqg_ensemble_create(const oqg_params *members, int nmembers, oqg_ensemble **
     int nfft_e = 32;
     for (oqg_handle *h : e->m) nfft_e = std::max(nfft_e, xinv_fft_threads(h->hb.M, h->hb.nl));
     e->xi_threads = nfft_e + 32;
+    {
+        long long cols = 0;
+        int ny_max = 0;
+        for (oqg_handle *h : e->m) { cols += (long long)h->hb.nl * h->hb.nk; ny_max = std::max(ny_max, h->hb.ny); }
+        e->yW = ysolve_warps(ny_max, cols);
+    }
     for (int i : order) {
         const BasinDev &b = e->m[i]->hb;
         const int TT = (b.M + e->E - 1) / e->E;
@@ -1591,7 +1698,7 @@ int oqg_ensemble_create(const oqg_params *members, int nmembers, oqg_ensemble **
         const size_t xrow = (size_t)((b.nxin + 3) & ~3);
         e->smem_x = std::max(e->smem_x, fft_inplace_len(b.M) ? (size_t)G * (LB * t2 + 2 * xrow * esz)
                                                                : (size_t)G * 2 * LB * t2);
-        e->smem_y = std::max(e->smem_y, (size_t)ysolve_ld(b.ny) * 4 * vsz);
+        e->smem_y = std::max(e->smem_y, (size_t)ysolve_ld(b.ny, e->yW) * 4 * vsz);
         e->smem_i = std::max(e->smem_i, xinv_smem(b.M, b.nl, nra, b.nxp, nfft_e, esz, b.inh_g != nullptr));
     }
     if (e->smem_x > 227 * 1024 || e->smem_i > 227 * 1024 || e->smem_v > 227 * 1024) {
@@ -1608,7 +1715,8 @@ int oqg_ensemble_create(const oqg_params *members, int nmembers, oqg_ensemble **
         return d;
     };
     e->hb.resize(nmembers);
-    for (int i = 0; i < nmembers; ++i) e->hb[i] = e->m[i]->hb;
+    // the ensemble's assembly launches transform in k_xinv for every member
+    for (int i = 0; i < nmembers; ++i) { e->hb[i] = e->m[i]->hb; e->hb[i].xinv_sep = 0; }
     e->d_bas = (BasinDev *)up(e->hb.data(), e->hb.size() * sizeof(BasinDev));
     e->d_wv = (Work *)up(wv.data(), wv.size() * sizeof(Work));
     e->d_wx = (Work *)up(wx.data(), wx.size() * sizeof(Work));
@@ -1642,6 +1750,7 @@ static int ens_member(oqg_ensemble *e, int member, oqg_handle **h) {
 static int ens_refresh(oqg_ensemble *e, int member) {
     const double tdt = e->hb[member].tdt_m;
     e->hb[member] = e->m[member]->hb;
+    e->hb[member].xinv_sep = 0;
     e->hb[member].tdt_m = tdt;
     CK(cudaMemcpyAsync(e->d_bas + member, &e->hb[member], sizeof(BasinDev), cudaMemcpyHostToDevice, e->st));
     CK(cudaStreamSynchronize(e->st));

@@ -102,6 +102,10 @@ struct BasinDev {
     int *err;                   // device error bits
     // launch bookkeeping
     int k4_rows;                // interior rows per CTA of the assembly launch
+    int xinv_sep;               // the inverse transforms run as k_xinv_rows (wide boxes;
+                                // modal rows in inh_g) and k_xinv only assembles
+    void *scal_g;               // with xinv_sep: the step's scalar phase results,
+                                // written once per step by k_xinv_rows
     double tdt_m;               // leapfrog step of this member when a launch
                                 // passes tdt = 0 (ensembles: one per member)
     unsigned wait_limit;        // polls of a first wait for a tile load before

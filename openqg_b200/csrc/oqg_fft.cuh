@@ -202,7 +202,7 @@ template <int S> __device__ __forceinline__ int fpad_step(int i, int r) {
 // One Stockham stage of radix R: src -> dst (both shared, padded, length M).
 // Threads t < TT of the transform's group each take butterflies t, t+TT, ...
 // tws: this stage's twiddles in global memory (read through L1), entry
-// jm (R-1) + r - 1 = exp(-2 pi i r jm / (Ns R)).  lg = log2(Ns) when Ns is a
+// (r - 1) Ns + jm = exp(-2 pi i r jm / (Ns R)).  lg = log2(Ns) when Ns is a
 // power of two (a shift), else -1 (fd divides by Ns).
 template <class T, int R>
 __device__ __forceinline__ void fft_stage(const typename C2<T>::t *__restrict__ src,
@@ -217,9 +217,8 @@ __device__ __forceinline__ void fft_stage(const typename C2<T>::t *__restrict__ 
 #pragma unroll
         for (int r = 0; r < R; ++r) v[r] = src[fpad(j + r * nb)];
         if (jm != 0) {
-            const T2 *w = tws + jm * (R - 1);
 #pragma unroll
-            for (int r = 1; r < R; ++r) v[r] = c_mul(v[r], __ldg(w + r - 1));
+            for (int r = 1; r < R; ++r) v[r] = c_mul(v[r], __ldg(tws + (r - 1) * Ns + jm));
         }
         Dft<T, R>::run(v);
         const int d = q * Ns * R + jm;
@@ -308,9 +307,8 @@ __device__ __forceinline__ void fft_stage_ct(const typename C2<T>::t *__restrict
 #pragma unroll
             for (int r = 0; r < R; ++r) v[r] = src[fpad_step<nb>(j, r)];
             if (Ns > 1 && jm != 0) {
-                const T2 *w = tws + jm * (R - 1);
 #pragma unroll
-                for (int r = 1; r < R; ++r) v[r] = c_mul(v[r], __ldg(w + r - 1));
+                for (int r = 1; r < R; ++r) v[r] = c_mul(v[r], __ldg(tws + (r - 1) * Ns + jm));
             }
             Dft<T, R>::run(v);
             const int d = q * Ns * R + jm;
@@ -362,9 +360,8 @@ __device__ __forceinline__ void fft_stage_ip(typename C2<T>::t *buf, const typen
             const int j = t + u * TT;
             const int q = j / Ns, jm = j - q * Ns;
             if (Ns > 1 && jm != 0) {
-                const T2 *w = tws + jm * (R - 1);
 #pragma unroll
-                for (int r = 1; r < R; ++r) v[u][r] = c_mul(v[u][r], __ldg(w + r - 1));
+                for (int r = 1; r < R; ++r) v[u][r] = c_mul(v[u][r], __ldg(tws + (r - 1) * Ns + jm));
             }
             Dft<T, R>::run(v[u]);
             const int d = q * Ns * R + jm;

@@ -769,18 +769,50 @@ template <> __device__ __forceinline__ float2 yt_store2<float2>(double2 v) { ret
 __device__ __forceinline__ double yt_re(double v) { return v; }
 __device__ __forceinline__ double yt_re(double2 v) { return v.x; }
 
-// The column solve of one warp with each lane's rows [s, s+SM) held in
-// registers through all four passes: forward elimination as an affine scan
-// (chunk pass, warp scan of the chunk maps, chunk pass), then back
-// substitution the same way from the bottom.  Rows at or beyond ny are
-// padding: their value and pivot are zero, so they map everything to zero in
-// both sweeps and the last row's zero neighbour below needs no special case;
-// the passes then run without per-row predicates.  col: the column in shared
-// memory at padded offset o; piv: its pivots (global, plen stored).
+// The maps of the two sweeps compose across the lanes of a column: lane l's
+// rows give an affine map u_out = C + D u_in, and the lanes' maps are scanned
+// in sweep order.  A column spread over W warps also composes across them:
+// each warp publishes its aggregate map (lane 31 going down the rows, lane 0
+// going up) and a warp's carry-in is the composition of the warps before it.
+// Returns this lane's input value: its exclusive prefix applied to the carry.
+// Every thread of the CTA calls it (a CTA barrier when W > 1).
+template <class V, int W, bool DOWN>
+__device__ __forceinline__ V ysolve_scan(V C, double D, int lane, int wc, V *sC, double *sD) {
+    for (int q = 1; q < 32; q <<= 1) {
+        const V Co = DOWN ? yt_up(C, q) : yt_dn(C, q);
+        const double Do = DOWN ? shfl_up_d(D, q) : shfl_dn_d(D, q);
+        if (DOWN ? lane >= q : lane + q < 32) { C = yt_axpy(C, D, Co); D = D * Do; }
+    }
+    V Ce = DOWN ? yt_up(C, 1) : yt_dn(C, 1);
+    if constexpr (W == 1) {
+        if (lane == (DOWN ? 0 : 31)) Ce = yt_zero(V());
+        return Ce;
+    } else {
+        double De = DOWN ? shfl_up_d(D, 1) : shfl_dn_d(D, 1);
+        if (lane == (DOWN ? 0 : 31)) { Ce = yt_zero(V()); De = 1.0; }
+        if (lane == (DOWN ? 31 : 0)) { sC[wc] = C; sD[wc] = D; }
+        __syncthreads();
+        V u = yt_zero(V());
+        if (DOWN) { for (int v = 0; v < wc; ++v) u = yt_axpy(sC[v], sD[v], u); }
+        else { for (int v = W - 1; v > wc; --v) u = yt_axpy(sC[v], sD[v], u); }
+        return yt_axpy(Ce, De, u);
+    }
+}
+
+// The column solve with each lane's rows [s, s+SM) held in registers through
+// all four passes: forward elimination as an affine scan (chunk pass, scan
+// of the chunk maps, chunk pass), then back substitution the same way from
+// the bottom.  Rows at or beyond ny are padding: their value and pivot are
+// zero, so they map everything to zero in both sweeps and the last row's
+// zero neighbour below needs no special case; the passes then run without
+// per-row predicates.  col: the column in shared memory at padded offset o;
+// piv: its pivots (global, plen stored); sC/sD: the column's W carry slots
+// of each sweep.
 #define YREG 16
-template <class V, int SM>
+template <class V, int W, int SM>
 __device__ __forceinline__ void ysolve_chunk_regs(V *col, const double *__restrict__ piv, int plen, double a,
-                                                  int lane, int s, int o, int ny, CSum &colsum) {
+                                                  int lane, int wc, int s, int o, int ny, V *sC, double *sD,
+                                                  CSum &colsum) {
     V x[SM];
     double bt[SM];
 #pragma unroll
@@ -797,13 +829,7 @@ __device__ __forceinline__ void ysolve_chunk_regs(V *col, const double *__restri
         C = yt_axpy(yt_scale(x[t], bt[t]), -a * bt[t], C);
         D = -a * bt[t] * D;
     }
-    for (int q = 1; q < 32; q <<= 1) {
-        V Co = yt_up(C, q);
-        double Do = shfl_up_d(D, q);
-        if (lane >= q) { C = yt_axpy(C, D, Co); D = D * Do; }
-    }
-    V uu = yt_up(C, 1);
-    if (lane == 0) uu = yt_zero(V());
+    V uu = ysolve_scan<V, W, true>(C, D, lane, wc, sC, sD);
 #pragma unroll
     for (int t = 0; t < SM; ++t) {
         uu = yt_axpy(yt_scale(x[t], bt[t]), -a * bt[t], uu);
@@ -818,13 +844,7 @@ __device__ __forceinline__ void ysolve_chunk_regs(V *col, const double *__restri
         C = yt_axpy(x[t], ej, C);
         D = ej * D;
     }
-    for (int q = 1; q < 32; q <<= 1) {
-        V Co = yt_dn(C, q);
-        double Do = shfl_dn_d(D, q);
-        if (lane + q < 32) { C = yt_axpy(C, D, Co); D = D * Do; }
-    }
-    uu = yt_dn(C, 1);
-    if (lane == 31) uu = yt_zero(V());
+    uu = ysolve_scan<V, W, false>(C, D, lane, wc, sC + W, sD + W);
 #pragma unroll
     for (int t = SM - 1; t >= 0; --t) {
         const double ej = -a * bt[t];
@@ -837,139 +857,142 @@ __device__ __forceinline__ void ysolve_chunk_regs(V *col, const double *__restri
         if (s + t < ny) col[o + t] = x[t];
 }
 
-// Rows per lane of the y-solve and the padded column length of its tile:
-// grids of up to 32 YREG rows take the smallest of 4, 8 and 16 rows per lane
-// that covers them (the register path, one instance each), wider ones
-// ceil(ny/32).
-__host__ __device__ __forceinline__ int ysolve_rows_per_lane(int ny) {
-    return ny <= 128 ? 4 : ny <= 256 ? 8 : ny <= 32 * YREG ? YREG : (ny + 31) >> 5;
+// Rows per lane of a column spread over W warps and the padded column
+// length of its tile: up to 32 W YREG rows the smallest of 4, 8 and 16 rows
+// per lane that covers them (the register path, one instance each), beyond
+// that ceil(ny / 32 W) rows per lane through shared memory.
+__host__ __device__ __forceinline__ int ysolve_rows_per_lane(int ny, int W) {
+    const int L = 32 * W;
+    return ny <= 4 * L ? 4 : ny <= 8 * L ? 8 : ny <= YREG * L ? YREG : (ny + L - 1) / L;
 }
-__host__ __device__ __forceinline__ int ysolve_ld(int ny) {
-    const int s = ysolve_rows_per_lane(ny);
-    const int need = 32 * (s + 1) + 1;                 // 32 lanes of s rows, one pad each
+__host__ __device__ __forceinline__ int ysolve_ld(int ny, int W) {
+    const int s = ysolve_rows_per_lane(ny, W);
+    const int need = 32 * W * (s + 1) + 1;             // 32 W lanes of s rows, one pad each
     const int ld = (ny + 32) | 1;
     return ld > need ? ld : (need | 1);
 }
 
-template <class T, bool CPLX, int NL>
-__global__ void __launch_bounds__(128)
+// One column per W warps, 4 columns per CTA (blockDim = 128 W).  More warps
+// per column cut the rows each lane carries through the sweeps and put more
+// warps on the SMs when the grid has few columns.
+template <class T, bool CPLX, int W>
+__global__ void __launch_bounds__(128 * W, W == 1 ? 1 : W == 2 ? 3 : 1)
 k_ysolve(const BasinDev *__restrict__ bas, const Work *__restrict__ work) {
     typedef typename YT<T, CPLX>::v V;
     typedef typename YT<T, CPLX>::g Gm;
-    constexpr int KB = 4;                       // columns (warps) per CTA
-    constexpr int CH = 16;                      // rows per unrolled chunk
+    constexpr int KB = 4;                       // columns per CTA
+    constexpr int NT = 128 * W;                 // threads
+    constexpr int CH = 16 / W;                  // loads in flight per thread and pass
     const Work w = work[blockIdx.x];
     const BasinDev &b = bas[w.member];
-    const int lane = threadIdx.x & 31, c = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int c = wid / W, wc = wid - c * W;    // column of the CTA, warp within it
     const int nk = b.nk, ny = b.ny, pk = b.pk;
     const int nkb = (nk + KB - 1) / KB;
     const int m = w.block / nkb, k0 = (w.block - m * nkb) * KB;
-    // Lane `l` owns rows [l S, l S + S).  Columns are stored with one pad word
-    // per S rows (row j at j + j / S), so the 32 lanes of a warp reading their
-    // chunks hit distinct banks.
-    const int S_ = ysolve_rows_per_lane(ny);
-    const int LD = ysolve_ld(ny);            // > 32 S + 31 pads, odd
+    // Lane l of warp wc owns rows [(32 wc + l) S, +S).  Columns are stored
+    // with one pad word per S rows (row j at j + j / S), so the 32 lanes of a
+    // warp reading their chunks hit distinct banks.
+    const int S_ = ysolve_rows_per_lane(ny, W);
+    const int LD = ysolve_ld(ny, W);            // > 32 W (S + 1), odd
     const FastDiv fdS(S_);
     extern __shared__ __align__(16) unsigned char smem_raw[];
     V *tile = reinterpret_cast<V *>(smem_raw);                 // [KB][LD]
+    __shared__ V sC[KB][2 * W];                 // carries of the two sweeps
+    __shared__ double sD[KB][2 * W];
     const int k = k0 + c;
     const bool live = k < nk;
     const int pidx = m * nk + (live ? k : 0);
-    // this warp's pivots (constant data, read through L1); beyond the stored
-    // length a pivot repeats its fixed point
+    // this column's pivots (constant data, read through L1); beyond the
+    // stored length a pivot repeats its fixed point
     const double *__restrict__ piv = b.piv_tab + b.piv_off[pidx];
     const int plen = b.piv_len[pidx];
     Gm *S = (Gm *)b.spec + (size_t)m * ny * pk;
     pdl_trigger();
     pdl_wait();
     // load the spectral columns: thread -> (row, column), coalesced along k
-    for (int i0 = threadIdx.x; i0 < ny * KB; i0 += 128 * CH) {
+    for (int i0 = threadIdx.x; i0 < ny * KB; i0 += NT * CH) {
         V v[CH];
 #pragma unroll
         for (int u = 0; u < CH; ++u) {
-            const int idx = i0 + 128 * u;
+            const int idx = i0 + NT * u;
             const int jj = idx >> 2, cc = idx & 3, kk = k0 + cc;
             v[u] = (idx < ny * KB && kk < nk) ? yt_load(S[(size_t)jj * pk + kk]) : yt_zero(V());
         }
 #pragma unroll
         for (int u = 0; u < CH; ++u) {
-            const int idx = i0 + 128 * u;
+            const int idx = i0 + NT * u;
             const int jj = idx >> 2, cc = idx & 3;
             if (idx < ny * KB) tile[cc * LD + jj + fdS.div(jj)] = v[u];
         }
     }
     __syncthreads();
 
-    CSum wsum;                                  // dst_w-weighted column sum (box)
-    if (live) {
-        const double a = b.a_tri;
-        V *col = tile + c * LD;
-        const int s = lane * S_, e = min(s + S_, ny);
-        const int o = lane * (S_ + 1);          // padded offset of row s
-        const int n = max(e - s, 0);
-        CSum colsum;
-        if (S_ == 4) ysolve_chunk_regs<V, 4>(col, piv, plen, a, lane, s, o, ny, colsum);
-        else if (S_ == 8) ysolve_chunk_regs<V, 8>(col, piv, plen, a, lane, s, o, ny, colsum);
-        else if (S_ == YREG) ysolve_chunk_regs<V, YREG>(col, piv, plen, a, lane, s, o, ny, colsum);
-        else {
-            // forward elimination: u_j = f_j beta_j - a beta_j u_{j-1}
-            V C = yt_zero(V());
-            double D = 1.0;
+    // Every warp runs the sweeps (a column past nk solves zeros) so that the
+    // carry barriers are uniform over the CTA.
+    const double a = b.a_tri;
+    V *col = tile + c * LD;
+    const int gl = wc * 32 + lane;
+    const int s = gl * S_, e = min(s + S_, ny);
+    const int o = gl * (S_ + 1);                // padded offset of row s
+    const int n = max(e - s, 0);
+    CSum colsum;
+    if (S_ == 4) ysolve_chunk_regs<V, W, 4>(col, piv, plen, a, lane, wc, s, o, ny, sC[c], sD[c], colsum);
+    else if (S_ == 8) ysolve_chunk_regs<V, W, 8>(col, piv, plen, a, lane, wc, s, o, ny, sC[c], sD[c], colsum);
+    // (16 rows per lane only with one warp per column: the multi-warp
+    // instances run at most 8 within their register budget)
+    else if (W == 1 && S_ == YREG)
+        ysolve_chunk_regs<V, W, YREG>(col, piv, plen, a, lane, wc, s, o, ny, sC[c], sD[c], colsum);
+    else {
+        // forward elimination: u_j = f_j beta_j - a beta_j u_{j-1}
+        V C = yt_zero(V());
+        double D = 1.0;
 #pragma unroll 8
-            for (int t = 0; t < n; ++t) {
-                const double bt = __ldg(piv + min(s + t, plen - 1));
-                C = yt_axpy(yt_scale(col[o + t], bt), -a * bt, C);
-                D = -a * bt * D;
-            }
-            for (int q = 1; q < 32; q <<= 1) {
-                V Co = yt_up(C, q);
-                double Do = shfl_up_d(D, q);
-                if (lane >= q) { C = yt_axpy(C, D, Co); D = D * Do; }
-            }
-            V uu = yt_up(C, 1);
-            if (lane == 0) uu = yt_zero(V());
-#pragma unroll 8
-            for (int t = 0; t < n; ++t) {
-                const double bt = __ldg(piv + min(s + t, plen - 1));
-                uu = yt_axpy(yt_scale(col[o + t], bt), -a * bt, uu);
-                col[o + t] = uu;
-            }
-            // back substitution: u_j = u'_j - a beta_j u_{j+1}
-            C = yt_zero(V());
-            D = 1.0;
-#pragma unroll 8
-            for (int t = n - 1; t >= 0; --t) {
-                const double ej = (s + t == ny - 1) ? 0.0 : -a * __ldg(piv + min(s + t, plen - 1));
-                C = yt_axpy(col[o + t], ej, C);
-                D = ej * D;
-            }
-            for (int q = 1; q < 32; q <<= 1) {
-                V Co = yt_dn(C, q);
-                double Do = shfl_dn_d(D, q);
-                if (lane + q < 32) { C = yt_axpy(C, D, Co); D = D * Do; }
-            }
-            uu = yt_dn(C, 1);
-            if (lane == 31) uu = yt_zero(V());
-#pragma unroll 8
-            for (int t = n - 1; t >= 0; --t) {
-                const double ej = (s + t == ny - 1) ? 0.0 : -a * __ldg(piv + min(s + t, plen - 1));
-                uu = yt_axpy(col[o + t], ej, uu);
-                col[o + t] = uu;
-                colsum.add(yt_re(uu));
-            }
+        for (int t = 0; t < n; ++t) {
+            const double bt = __ldg(piv + min(s + t, plen - 1));
+            C = yt_axpy(yt_scale(col[o + t], bt), -a * bt, C);
+            D = -a * bt * D;
         }
-        if (!CPLX) {
-            const CSum cw = csum_warp(colsum);
+        V uu = ysolve_scan<V, W, true>(C, D, lane, wc, sC[c], sD[c]);
+#pragma unroll 8
+        for (int t = 0; t < n; ++t) {
+            const double bt = __ldg(piv + min(s + t, plen - 1));
+            uu = yt_axpy(yt_scale(col[o + t], bt), -a * bt, uu);
+            col[o + t] = uu;
+        }
+        // back substitution: u_j = u'_j - a beta_j u_{j+1}
+        C = yt_zero(V());
+        D = 1.0;
+#pragma unroll 8
+        for (int t = n - 1; t >= 0; --t) {
+            const double ej = (s + t == ny - 1) ? 0.0 : -a * __ldg(piv + min(s + t, plen - 1));
+            C = yt_axpy(col[o + t], ej, C);
+            D = ej * D;
+        }
+        uu = ysolve_scan<V, W, false>(C, D, lane, wc, sC[c] + W, sD[c] + W);
+#pragma unroll 8
+        for (int t = n - 1; t >= 0; --t) {
+            const double ej = (s + t == ny - 1) ? 0.0 : -a * __ldg(piv + min(s + t, plen - 1));
+            uu = yt_axpy(col[o + t], ej, uu);
+            col[o + t] = uu;
+            colsum.add(yt_re(uu));
+        }
+    }
+    // dst_w-weighted column sum (box), one compensated partial per warp
+    CSum wsum;
+    if (!CPLX) {
+        const CSum cw = csum_warp(colsum);
+        if (live) {
             const double wk = b.dst_w[k];
             wsum.add_prod(wk, cw.s);
             wsum.add_prod(wk, cw.c);
         }
     }
     __syncthreads();
-    for (int i0 = threadIdx.x; i0 < ny * KB; i0 += 128 * CH) {
+    for (int i0 = threadIdx.x; i0 < ny * KB; i0 += NT * CH) {
 #pragma unroll
         for (int u = 0; u < CH; ++u) {
-            const int idx = i0 + 128 * u;
+            const int idx = i0 + NT * u;
             const int jj = idx >> 2, cc = idx & 3, kk = k0 + cc;
             if (idx < ny * KB && kk < nk) {
                 if constexpr (CPLX) S[(size_t)jj * pk + kk] = yt_store2<Gm>(tile[cc * LD + jj + fdS.div(jj)]);
@@ -978,15 +1001,15 @@ k_ysolve(const BasinDev *__restrict__ bas, const Work *__restrict__ work) {
         }
     }
     if (!CPLX) {
-        // one dst_w-weighted compensated partial (sum, compensation) per
-        // CTA, summed in a fixed order
-        __shared__ double wpart[2 * KB];
-        if (lane == 0) { wpart[c] = wsum.s; wpart[KB + c] = wsum.c; }
+        // the CTA's partial (sum, compensation), its warps merged in a fixed
+        // order
+        __shared__ double wpart[2 * KB * W];
+        if (lane == 0) { wpart[wid] = wsum.s; wpart[KB * W + wid] = wsum.c; }
         __syncthreads();
         if (threadIdx.x == 0) {
             CSum t;
 #pragma unroll
-            for (int x = 0; x < KB; ++x) t.merge(wpart[x], wpart[KB + x]);
+            for (int x = 0; x < KB * W; ++x) t.merge(wpart[x], wpart[KB * W + x]);
             b.part_col[2 * w.block] = t.s;
             b.part_col[2 * w.block + 1] = t.c;
         }
@@ -1240,6 +1263,106 @@ __device__ __noinline__ void scalar_phase(const BasinDev &b, double tdt, int par
     nx->nt = nt + 1;
 }
 
+// ------------------------------------------------------------------ k_xinv_rows
+// Wide boxes (modal rows in the global buffer b.inh_g): the inverse DST-I of
+// the y-solved spectral rows as a launch of its own, shaped like k_xfwd (one
+// row pair per group, the 2048- and 4096-point lengths in place, two CTAs
+// per SM), so k_xinv only assembles.  The inverse is the forward transform
+// scaled by ftnorm (inhomog.F90:200-211); the modal row j + 1 of mode m gets
+// the n interior values and zeros on both walls, and the first and last row
+// pairs of a mode clear the wall rows 0 and nyp - 1.  scal != 0: one CTA
+// more, after the transforms', runs the step's scalar phase once into
+// b.scal_g (the assembly CTAs read it there) and writes the next state.
+template <class T, int NL, int E>
+__global__ void __launch_bounds__(256, 2)
+k_xinv_rows(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int scal, int par, double tdt) {
+    typedef typename C2<T>::t T2;
+    if (scal && blockIdx.x == gridDim.x - 1) {
+        pdl_trigger();
+        pdl_wait();
+        if (threadIdx.x < 32) {
+            const BasinDev &b = bas[0];
+            scalar_phase<T, NL>(b, tdt != 0.0 ? tdt : b.tdt_m, par, true, (XinvScal *)b.scal_g);
+        }
+        return;
+    }
+    const Work w = work[blockIdx.x];
+    const BasinDev &b = bas[w.member];
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int M = b.M, TT = (M + E - 1) / E, G = blockDim.x / TT;
+    const int g = threadIdx.x / TT, t = threadIdx.x - g * TT;
+    const int LB = fft_buf_len(M);
+    T2 *zs = reinterpret_cast<T2 *>(smem_raw);
+    const int npm = (b.ny + 1) >> 1;          // row pairs per mode
+    const int pair = w.block * G + g;
+    const bool live = g < G && pair < b.nl * npm;
+    const int m = live ? pair / npm : 0;
+    const int j = live ? 2 * (pair - m * npm) : 0;
+    const bool two = live && (j + 1 < b.ny);
+    const int n = b.nxin, nxp = b.nxp, px = b.px;
+    const int RO = (n + 3) & ~3;              // offset of the second row (16-byte aligned)
+    const bool ip = E == 16 && fft_inplace_len(M);
+    T2 *za = zs + (size_t)(g < G ? g : 0) * (ip ? LB : 2 * LB);
+    T2 *zb = za + LB;
+    T *raw = ip ? reinterpret_cast<T *>(zs + (size_t)G * LB) + (size_t)(g < G ? g : 0) * 2 * RO
+                : reinterpret_cast<T *>(zb);
+    const T *x = (const T *)b.spec + ((size_t)m * b.ny + j) * b.pk;
+    T *inh = (T *)b.inh_g;
+    const T ftn = (T)b.ftnorm;
+    pdl_trigger();
+    pdl_wait();
+    if (live) {
+        cp_async_16(raw, x, round16(n * (int)sizeof(T)), t, TT);
+        if (two) cp_async_16(raw + RO, x + b.pk, round16(n * (int)sizeof(T)), t, TT);
+    }
+    cp_async_commit_wait_all();
+    __syncthreads();
+    if (live) {
+        if (t == 0) {
+            T2 zero;
+            zero.x = (T)0;
+            zero.y = (T)0;
+            za[fpad(0)] = zero;
+            za[fpad(n + 1)] = zero;
+        }
+        for (int jj = 1 + t; jj <= n; jj += TT) {
+            T2 v, vm;
+            v.x = ftn * raw[jj - 1];
+            v.y = two ? ftn * raw[RO + jj - 1] : (T)0;
+            vm.x = -v.x;
+            vm.y = -v.y;
+            za[fpad(jj)] = v;
+            za[fpad(M - jj)] = vm;
+        }
+    }
+    __syncthreads();
+    T2 *z = za;
+    if (ip) fft_inplace<T>(za, M, (const T2 *)b.tw, live ? t : M, 0, 0);
+    else z = fft_run<T, E>(za, zb, M, b.rad, b.nrad, (const T2 *)b.tw, live ? t : TT, TT, 0, 0);
+    if (!live) return;
+    T *ox = inh + ((size_t)m * b.nyp + j + 1) * px;
+    T *oy = ox + px;
+    for (int kk = t; kk < n; kk += TT) {
+        const T2 v = z[fpad(kk + 1)];
+        ox[kk + 1] = -v.y;
+        if (two) oy[kk + 1] = v.x;
+    }
+    if (t == 0) {
+        ox[0] = (T)0;
+        ox[nxp - 1] = (T)0;
+        if (two) { oy[0] = (T)0; oy[nxp - 1] = (T)0; }
+    }
+    // the wall rows
+    T *wrow = nullptr;
+    if (j == 0) wrow = inh + (size_t)m * b.nyp * px;
+    if (j + 2 >= b.ny) {
+        T *last = inh + ((size_t)m * b.nyp + b.nyp - 1) * px;
+        for (int i = t; i < nxp; i += TT) last[i] = (T)0;
+    }
+    if (wrow)
+        for (int i = t; i < nxp; i += TT) wrow[i] = (T)0;
+}
+
 // ------------------------------------------------------------------ k_xinv
 // Rows of one CTA: interior rows [jlo, jhi) plus wall row 0 (first CTA) and
 // wall row nyp-1 (last CTA).
@@ -1304,7 +1427,18 @@ k_xinv(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par,
     pdl_trigger();
     if (!fft_thread) {
         pdl_wait();
-        if (!out) scalar_phase<T, NL>(b, tdt != 0.0 ? tdt : b.tdt_m, par, w.block == 0, &sS);
+        if (!out) {
+            if (split && b.xinv_sep) {
+                // computed once by k_xinv_rows
+                const double *src = (const double *)b.scal_g;
+                double *dst = reinterpret_cast<double *>(&sS);
+                for (int x = threadIdx.x & 31; x < (int)(sizeof(XinvScal) / sizeof(double)); x += 32) dst[x] = src[x];
+            } else {
+                scalar_phase<T, NL>(b, tdt != 0.0 ? tdt : b.tdt_m, par, w.block == 0, &sS);
+            }
+        }
+    } else if (split && b.xinv_sep) {
+        pdl_wait();                     // the modal rows come from k_xinv_rows
     } else {
     // zero the wall rows / columns of the modal fields
     if (!alias)
@@ -1471,7 +1605,9 @@ k_xinv(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par,
 #pragma unroll
                 for (int m = 0; m < NL; ++m) s2 += pm_[m] * ctm[m + NL * k];
                 const T pn = (T)s2;
-                inh[k * ms + lr * rs + i] = pn;
+                // ocqbdy reads the layer values on and next to the walls
+                // (in shared memory they go back everywhere)
+                if (!split || i <= 1 || i >= nxp - 2 || j <= 1 || j >= nyp - 2) inh[k * ms + lr * rs + i] = pn;
                 Pnew[k * n2 + (size_t)j * px + i] = supp ? (T)((T)0.5 * (pn + (T)po[u][k])) : pn;
             }
         }

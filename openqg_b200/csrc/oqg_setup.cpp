@@ -176,12 +176,13 @@ void fft_stage_twiddles(int M, const std::vector<int> &rad, std::vector<double> 
     const long double pi = 3.14159265358979323846264338327950288L;
     long long Ns = 1;
     for (int R : rad) {
-        // stage of radix R after Ns: entries (jm, r) at Ns-1 + jm (R-1) + r-1
+        // stage of radix R after Ns: entries (jm, r) at Ns-1 + (r-1) Ns + jm, so
+        // the butterflies of a warp (consecutive jm) read consecutive entries
         for (long long jm = 0; jm < Ns; ++jm)
             for (int r = 1; r < R; ++r) {
                 const long long k = (long long)r * jm;       // exponent k / (Ns R)
                 const long double ang = -2.0L * pi * (long double)(k % (Ns * R)) / (long double)(Ns * R);
-                const size_t e = (size_t)(Ns - 1 + jm * (R - 1) + (r - 1));
+                const size_t e = (size_t)(Ns - 1 + (r - 1) * Ns + jm);
                 tw[2 * e] = (double)cosl(ang);
                 tw[2 * e + 1] = (double)sinl(ang);
             }

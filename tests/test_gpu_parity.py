@@ -79,8 +79,11 @@ def assert_constraints_close(g, o, tol):
 # ------------------------------------------------------------------ pieces
 BOXES = [ocean_double_gyre(129), ocean_double_gyre(65), ocean_double_gyre(513, dx=10e3),
          Basin(nxp=81, nyp=101, dx=1e4, dy=1e4, h=[1000.0, 2000.0, 3000.0], gp=[0.02, 0.01]),
-         atmos_channel(193, 97), atmos_channel(101, 101, dx=1e4), atmos_channel(49, 25)]
-IDS = ["box129", "box65", "box513", "box81x101", "chan193x97", "chan101", "chan49x25"]
+         atmos_channel(193, 97), atmos_channel(101, 101, dx=1e4), atmos_channel(49, 25),
+         Basin(nxp=33, nyp=301, dx=1e4, dy=1e4, h=[1000.0, 2000.0, 3000.0], gp=[0.02, 0.01]),
+         atmos_channel(33, 301, dx=2e4)]
+IDS = ["box129", "box65", "box513", "box81x101", "chan193x97", "chan101", "chan49x25", "box33x301",
+       "chan33x301"]
 
 
 @pytest.mark.parametrize("b", BOXES, ids=IDS)
@@ -154,9 +157,14 @@ STEP_CASES = [
     (atmos_channel(193, 97), dict(amp_psi=30.0)),
     (atmos_channel(49, 25), dict(ent=True, amp_psi=30.0)),
     (atmos_channel(97, 65), dict(amp_psi=30.0)),
+    # few columns of many rows: the y-solve spreads a column over 2 (257^2)
+    # or 4 warps (the tall strips)
+    (ocean_double_gyre(257), dict()),
+    (Basin(nxp=33, nyp=301, dx=1e4, dy=1e4, h=[1000.0, 2000.0, 3000.0], gp=[0.02, 0.01]), dict(ent=True)),
+    (atmos_channel(33, 301, dx=2e4), dict(amp_psi=30.0)),
 ]
 STEP_IDS = ["box17", "box33ent", "box65", "box97", "box129", "box129ent", "box513",
-            "chan193x97", "chan49ent", "chan97x65"]
+            "chan193x97", "chan49ent", "chan97x65", "box257", "box33x301ent", "chan33x301"]
 
 
 @pytest.mark.parametrize("b,kw", STEP_CASES, ids=STEP_IDS)
