@@ -592,6 +592,8 @@ def time_batches(g, tdt, msteps, steps, flush):
 
 
 PHASES = ["k_vort", "k_xfwd", "k_ysolve", "k_xinv"]
+# a closed box runs the inverse transforms and the assembly as two launches
+PHASES_SEP = ["k_vort", "k_xfwd", "k_ysolve", "k_xinv_rows", "k_xinv_asm"]
 
 
 def phase_alg_bytes(s, nl):
@@ -606,6 +608,10 @@ def phase_alg_bytes(s, nl):
         "k_ysolve": 2 * s,
         # reads the spectral field, p (old) and the homogeneous solutions, writes p
         "k_xinv": 3 * s + s * (nl - 1) / nl,
+        # reads the spectral field, writes the modal rows
+        "k_xinv_rows": 2 * s,
+        # reads the modal rows and the homogeneous solutions, writes p
+        "k_xinv_asm": 2 * s + s * (nl - 1) / nl,
     }
 
 
@@ -614,20 +620,21 @@ def roofline_of(g, b, workload, precision, tdt, ms_per_model_step):
     each kernel of 20 steps) against the HBM roofline, and the whole step's
     algorithmic bytes over its timed duration."""
     from openqg_b200.params import OQG_FP64
-    ms = g.profile_phases(tdt, 20)
+    names = PHASES_SEP if g.xinv_sep() else PHASES
+    ms = g.profile_phases(tdt, 20)[:len(names)]
     dom = int(np.argmax(ms))
     s = 8 if b.precision == OQG_FP64 else 4
     cells = b.nxp * b.nyp * b.nl
     alg = phase_alg_bytes(s, b.nl)
     peak, peak_kind = peaks()
-    dname = PHASES[dom]
+    dname = names[dom]
     achieved = alg[dname] * cells / (ms[dom] / 1e3) / 1e9
     step_alg = (6 * s + s / b.nl) * cells
     tt = traffic_table().get((workload, precision, dname))
     return {"bound": "hbm", "kernel": dname, "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak, "peak_kind": peak_kind,
             "traffic": tt, "alg_bytes_per_launch": alg[dname] * cells,
-            "phase_ms": dict(zip(PHASES, [float(x) for x in ms])),
+            "phase_ms": dict(zip(names, [float(x) for x in ms])),
             "step_alg_bytes": step_alg,
             # the whole step: algorithmic bytes over the timed model step
             "step_frac": step_alg / (ms_per_model_step / 1e3) / 1e9 / peak,
@@ -637,6 +644,11 @@ def roofline_of(g, b, workload, precision, tdt, ms_per_model_step):
             # most a single persistent launch could take off a step
             "launch_floor_us_per_step": g.launch_floor(16),
             "launches_per_step": g.step_launches()}
+
+
+# --tile-rows / --ysolve-warps: settings fixed instead of measured (for
+# profiling runs, where a profiler's replays would distort the measurement)
+PINNED = {}
 
 
 def measure_basin(workload, prec, steps, warmup, msteps, flush, rank, pg, seed=None):
@@ -650,8 +662,20 @@ def measure_basin(workload, prec, steps, warmup, msteps, flush, rank, pg, seed=N
     g = QG(b)
     g.set_state(p, p)
     g.set_forcing(w, None, ts, tn)
-    # the vorticity tile height, measured on this GPU (oqg_autotune)
-    tile_rows, tune_ms = g.autotune(tdt, 20)
+    # the vorticity tile height and the y-solve's warps per column, measured
+    # on this GPU (oqg_autotune, oqg_autotune_ysolve), unless fixed
+    if PINNED.get("tile_rows"):
+        g.set_tile_rows(PINNED["tile_rows"])
+        tile_rows, tune_ms = PINNED["tile_rows"], {}
+    else:
+        tile_rows, tune_ms = g.autotune(tdt, 20)
+    if PINNED.get("xinv_sep") is not None and not b.cyclic:
+        g.set_xinv_sep(PINNED["xinv_sep"])
+    if PINNED.get("ysolve_warps"):
+        g.set_ysolve_warps(PINNED["ysolve_warps"])
+        ywarps, ytune_ms = PINNED["ysolve_warps"], {}
+    else:
+        ywarps, ytune_ms = g.autotune_ysolve(tdt, 20)
     for _ in range(warmup):
         g.step(tdt, msteps)
     g.sync()
@@ -665,6 +689,7 @@ def measure_basin(workload, prec, steps, warmup, msteps, flush, rank, pg, seed=N
         "workload": label, "tdt_s": tdt, "label": label, "total_ms": total_ms,
         "ms_per_model_step": total_ms / (steps * msteps), "cells": cells,
         "tile_rows": tile_rows, "autotune_ms_per_step": {str(k): round(v, 5) for k, v in tune_ms.items()},
+        "ysolve_warps": ywarps, "ysolve_autotune_ms_per_step": {str(k): round(v, 5) for k, v in ytune_ms.items()},
     }
 
 
@@ -680,7 +705,7 @@ def config_line(workload, prec, steps, warmup, msteps, flush, rank, ws, pg, note
             "model_steps_per_step": msteps, "steps": steps,
             "value": replica_value(m["total_ms"], ws, m["cells"], msteps, steps),
             "unit": "Mcell-layer-steps/s", "ms_per_model_step": m["ms_per_model_step"],
-            "tile_rows": m["tile_rows"], "roofline": roof,
+            "tile_rows": m["tile_rows"], "ysolve_warps": m["ysolve_warps"], "roofline": roof,
             "l2": "flushed (256 MiB write) before every timed step of %d model steps" % msteps}
 
 
@@ -829,6 +854,8 @@ def run_ours(args):
                    "model_steps_per_step": msteps, "tdt_s": tdt,
                    "tile_rows": m["tile_rows"],
                    "autotune_ms_per_step": m["autotune_ms_per_step"],
+                   "ysolve_warps": m["ysolve_warps"],
+                   "ysolve_autotune_ms_per_step": m["ysolve_autotune_ms_per_step"],
                    "l2": "flushed (256 MiB write) before every timed step of %d model steps" % msteps,
                    "parallelism": "replicas" if ws > 1 else "single basin"},
         "roofline": roof,
@@ -875,6 +902,13 @@ def main():
     ap.add_argument("--ref-model-steps", type=int, default=2)
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-variants", dest="variants", action="store_false")
+    ap.add_argument("--tile-rows", type=int, default=0, choices=[0, 8, 12, 16],
+                    help="fix the vorticity tile height instead of measuring it")
+    ap.add_argument("--xinv-sep", type=int, default=None, choices=[0, 1],
+                    help="closed boxes: the inverse transforms as a launch of their own (1) or inside "
+                         "the assembly kernel (0); default: the library's choice")
+    ap.add_argument("--ysolve-warps", type=int, default=0, choices=[0, 1, 2, 4],
+                    help="fix the y-solve's warps per column instead of measuring them")
     ap.add_argument("--adjoint-only", action="store_true",
                     help="time only the adjoint configuration (one repetition of 40 steps) and "
                          "print its figures; for profiling")
@@ -883,6 +917,9 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    PINNED["tile_rows"] = args.tile_rows
+    PINNED["ysolve_warps"] = args.ysolve_warps
+    PINNED["xinv_sep"] = args.xinv_sep
     if args.impl == "reference":
         return run_reference(args)
     if args.adjoint_only:

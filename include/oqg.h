@@ -264,19 +264,22 @@ int oqg_ekman_from_tau(const oqg_params *prm, const double *taux,
 int oqg_device_state(oqg_handle *h, void **p, void **pm, void **q, void **qm,
                      int *pitch, int *elem_bytes);
 
-/* Runs nsteps steps as separate launches with CUDA events between the four
+/* Runs nsteps steps as separate launches with CUDA events between the
  * kernels of each step, on the handle's stream, and returns the mean device
- * time per launch (ms) of each phase: ms[0] vorticity step + modal RHS,
- * ms[1] forward x-transform, ms[2] y-solve, ms[3] inverse x-transform +
- * scalar phase + assembly.  For measurement; the state advances normally. */
+ * time per launch (ms) of each: ms[0] vorticity step + modal RHS, ms[1]
+ * forward x-transform, ms[2] y-solve, ms[3] inverse x-transform (with the
+ * scalar phase, and with the assembly when one kernel does both), ms[4] the
+ * assembly when it runs as a launch of its own (oqg_set_xinv_sep), else 0.
+ * ms holds 5 values.  For measurement; the state advances normally. */
 int oqg_profile_phases(oqg_handle *h, double tdt, int nsteps, double *ms);
 
 /* CUDA stream of the handle (a cudaStream_t). */
 int oqg_stream(oqg_handle *h, void **stream);
 
-/* Kernel launches of one model step: 4 (vorticity, forward transform,
- * y-solve, inverse transform with the assembly), 5 for boxes wide enough
- * that the inverse transforms run as a launch of their own. */
+/* Kernel launches of one model step: 5 for a closed box (vorticity, forward
+ * transform, y-solve, inverse transform, assembly), 4 for a channel or a box
+ * after oqg_set_xinv_sep(h, 0) (the inverse transform and the assembly in
+ * one kernel). */
 int oqg_step_launches(oqg_handle *h, int *launches);
 
 /* The launch floor of the step chain: nsteps steps of launches with the
@@ -297,6 +300,29 @@ int oqg_launch_floor(oqg_handle *h, int nsteps, double *us_per_step);
 int oqg_autotune(oqg_handle *h, double tdt, int nsteps, int *best_vty, double *ms);
 /* Current tile height of the vorticity kernel. */
 int oqg_get_vty(oqg_handle *h, int *vty);
+
+/* The y-solve's warps per column (1, 2 or 4): oqg_create picks enough for
+ * about 20 warps per SM while each lane keeps 4 to 8 rows; this measures the
+ * three on the device like oqg_autotune (nsteps steps of tdt from the
+ * current state, restored) and keeps the fastest.  ms[0..2]: ms per step
+ * with 1, 2 and 4 warps.  Results agree to rounding (the scan's
+ * association changes with the split). */
+int oqg_autotune_ysolve(oqg_handle *h, double tdt, int nsteps, int *best_warps, double *ms);
+/* Current warps per y-solve column. */
+int oqg_get_ysolve_warps(oqg_handle *h, int *warps);
+/* Fix the vorticity tile height (8, 12 or 16) or the y-solve's warps per
+ * column (1, 2 or 4) without measuring, e.g. from an earlier oqg_autotune
+ * on the same GPU; OQG_EINVAL for other values. */
+int oqg_set_vty(oqg_handle *h, int vty);
+int oqg_set_ysolve_warps(oqg_handle *h, int warps);
+/* Closed boxes: the inverse transforms as a launch shaped like the forward
+ * one (k_xinv_rows, which also runs the step's scalar phase once) and a
+ * one-pass assembly (k_xinv_asm), instead of one kernel that transforms and
+ * assembles in shared memory.  On by default for boxes; it cannot be turned
+ * off where the modal rows do not fit in shared memory (1025 points wide and
+ * more: OQG_EUNSUPPORTED); channels: OQG_EUNSUPPORTED. */
+int oqg_set_xinv_sep(oqg_handle *h, int on);
+int oqg_get_xinv_sep(oqg_handle *h, int *on);
 
 /* ---------------------------------------------------------------------
  * Ensembles: many independent basins of uneven size stepped together by one

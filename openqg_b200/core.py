@@ -110,6 +110,13 @@ def lib():
     L.oqg_ensemble_autotune.argtypes = [vp, _dp, ctypes.c_int, ctypes.POINTER(ctypes.c_int), _dp]
     L.oqg_autotune.argtypes = [vp, ctypes.c_double, ctypes.c_int, ctypes.POINTER(ctypes.c_int), _dp]
     L.oqg_get_vty.argtypes = [vp, ctypes.POINTER(ctypes.c_int)]
+    L.oqg_autotune_ysolve.argtypes = [vp, ctypes.c_double, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                      ctypes.POINTER(ctypes.c_double)]
+    L.oqg_get_ysolve_warps.argtypes = [vp, ctypes.POINTER(ctypes.c_int)]
+    L.oqg_set_vty.argtypes = [vp, ctypes.c_int]
+    L.oqg_set_ysolve_warps.argtypes = [vp, ctypes.c_int]
+    L.oqg_set_xinv_sep.argtypes = [vp, ctypes.c_int]
+    L.oqg_get_xinv_sep.argtypes = [vp, ctypes.POINTER(ctypes.c_int)]
     L.oqg_adj_segment.argtypes = [vp, vp, vp, ctypes.c_size_t, ctypes.c_int, ctypes.c_double, ctypes.c_longlong]
     _lib = L
     return L
@@ -311,8 +318,10 @@ class QG:
         return [x.value for x in ptr], pitch.value, eb.value
 
     def profile_phases(self, tdt: float, nsteps: int):
-        """Mean device ms per launch of the four phases of a step."""
-        ms = np.zeros(4)
+        """Mean device ms per launch of the kernels of a step: vorticity,
+        forward transform, y-solve, inverse transform, and the assembly when
+        it runs as a launch of its own (else 0)."""
+        ms = np.zeros(5)
         _check(lib().oqg_profile_phases(self.h, float(tdt), int(nsteps), _p(ms)), "oqg_profile_phases")
         return ms
 
@@ -323,6 +332,38 @@ class QG:
         ms = np.full(18, np.nan)
         _check(lib().oqg_autotune(self.h, float(tdt), int(nsteps), ctypes.byref(best), _p(ms)), "oqg_autotune")
         return best.value, {v: float(ms[v]) for v in range(8, 18) if np.isfinite(ms[v])}
+
+    def autotune_ysolve(self, tdt: float, nsteps: int = 20):
+        """Measures the y-solve with 1, 2 and 4 warps per column and keeps the
+        fastest; returns (warps, {warps: ms per step})."""
+        best = ctypes.c_int()
+        ms = (ctypes.c_double * 3)()
+        _check(lib().oqg_autotune_ysolve(self.h, float(tdt), int(nsteps), ctypes.byref(best), ms),
+               "oqg_autotune_ysolve")
+        return best.value, {w: ms[i] for i, w in enumerate((1, 2, 4)) if ms[i] >= 0}
+
+    def set_tile_rows(self, rows: int):
+        """Fixes the vorticity tile height (8, 12 or 16) without measuring."""
+        _check(lib().oqg_set_vty(self.h, int(rows)), "oqg_set_vty")
+
+    def set_ysolve_warps(self, warps: int):
+        """Fixes the y-solve's warps per column (1, 2 or 4) without measuring."""
+        _check(lib().oqg_set_ysolve_warps(self.h, int(warps)), "oqg_set_ysolve_warps")
+
+    def set_xinv_sep(self, on: bool):
+        """Closed boxes: the inverse transforms as a launch of their own and a
+        one-pass assembly (on), or one kernel for both (off)."""
+        _check(lib().oqg_set_xinv_sep(self.h, 1 if on else 0), "oqg_set_xinv_sep")
+
+    def xinv_sep(self) -> bool:
+        v = ctypes.c_int()
+        _check(lib().oqg_get_xinv_sep(self.h, ctypes.byref(v)), "oqg_get_xinv_sep")
+        return bool(v.value)
+
+    def ysolve_warps(self) -> int:
+        v = ctypes.c_int()
+        _check(lib().oqg_get_ysolve_warps(self.h, ctypes.byref(v)), "oqg_get_ysolve_warps")
+        return v.value
 
     def tile_rows(self) -> int:
         v = ctypes.c_int()

@@ -59,6 +59,10 @@ struct oqg_handle {
     int nv = 0, nx = 0, nys = 0, ni = 0;
     int E = 8, KB = 16, xthreads = 128, xi_threads = 64;
     int yW = 1;                          // warps per y-solve column
+    bool xinv_split_needed = false;      // the modal rows do not fit in shared memory
+    size_t smem_i_full = 0, smem_i64_full = 0;   // k_xinv's shared memory when it transforms
+    int na = 0;                          // CTAs of k_xinv_asm
+    int xg = 1;                          // transforms per CTA of k_xfwd and k_xinv_rows
     size_t smem_v = 0, smem_x = 0, smem_x64 = 0, smem_y = 0, smem_i = 0, smem_i64 = 0;
     double *stage[2] = {nullptr, nullptr};
     double *hrow = nullptr;     // contiguous host-order copy buffer [nl][nyp][nxp]
@@ -173,16 +177,33 @@ static VortFn vort_kernel(int vt) {
     }
 }
 
+// The inverse transforms as k_xinv_rows and the one-pass k_xinv_asm (box),
+// or inside k_xinv; k_xinv keeps its modal rows in global memory when they
+// run separately or do not fit in shared memory.
+static void apply_xinv_sep(oqg_handle *h, bool on) {
+    BasinDev &b = h->hb;
+    b.xinv_sep = on ? 1 : 0;
+    b.xinv_split = (on || h->xinv_split_needed) ? 1 : 0;
+    h->smem_i = on ? 0 : h->smem_i_full;
+    h->smem_i64 = on ? 0 : h->smem_i64_full;
+    h->hb64.xinv_sep = b.xinv_sep;
+    h->hb64.xinv_split = b.xinv_split;
+}
+
 template <class T, int NL, int E>
 static void launch_step_t(oqg_handle *h, int par, double tdt) {
     const BasinDev &b = h->hb;
     launch_pdl(vort_kernel<T, NL>(h->hb.vty), h->nv, VTHREADS, h->smem_v, h->st, h->d_bas, h->d_wv, par, tdt);
     launch_pdl(k_xfwd<T, E>, h->nx, h->xthreads, h->smem_x, h->st, h->d_bas, h->d_wx, (const void *)nullptr);
     launch_ysolve<T>(b.cyclic, h->yW, h->nys, h->smem_y, h->st, h->d_bas, h->d_wy, true);
-    if (b.xinv_sep)
-        launch_pdl(k_xinv_rows<T, NL, E>, h->nx + 1, h->xthreads, h->smem_x, h->st, h->d_bas, h->d_wx, 1, par, tdt);
-    launch_pdl(k_xinv<T, NL>, h->ni, h->xi_threads, h->smem_i, h->st, h->d_bas, h->d_wi, par, tdt,
-               (double *)nullptr);
+    if (b.xinv_sep) {
+        launch_pdl(k_xinv_rows<T, NL, E>, h->nx + 1, rup(h->xthreads, 32), h->smem_x, h->st, h->d_bas, h->d_wx,
+                   h->xg, 1, par, tdt, (T *)nullptr);
+        launch_pdl(k_xinv_asm<T, NL>, h->na, 256, 0, h->st, h->d_bas, par);
+    } else {
+        launch_pdl(k_xinv<T, NL>, h->ni, h->xi_threads, h->smem_i, h->st, h->d_bas, h->d_wi, par, tdt,
+                   (double *)nullptr);
+    }
 }
 
 // FP64 solve of the modal Helmholtz problems with the rhs buffer as input;
@@ -196,16 +217,20 @@ static void launch_solve_t(oqg_handle *h, double *out, bool pdl) {
                    (const void *)nullptr);
         launch_ysolve<double>(h->hb.cyclic, h->yW, h->nys, h->smem_y, h->st, h->d_bas64, h->d_wy, true);
         if (h->hb.xinv_sep)
-            launch_pdl(k_xinv_rows<double, NL, E>, h->nx, h->xthreads, h->smem_x64, h->st, h->d_bas64, h->d_wx, 0, 0,
-                       0.0);
-        launch_pdl(k_xinv<double, NL>, h->ni, h->xi_threads, h->smem_i64, h->st, h->d_bas64, h->d_wi, 0, 0.0, out);
+            launch_pdl(k_xinv_rows<double, NL, E>, h->nx, rup(h->xthreads, 32), h->smem_x64, h->st, h->d_bas64,
+                       h->d_wx, h->xg, 0, 0, 0.0, out);
+        else
+            launch_pdl(k_xinv<double, NL>, h->ni, h->xi_threads, h->smem_i64, h->st, h->d_bas64, h->d_wi, 0, 0.0,
+                       out);
         return;
     }
     k_xfwd<double, E><<<h->nx, h->xthreads, h->smem_x64, h->st>>>(h->d_bas64, h->d_wx, nullptr);
     launch_ysolve<double>(h->hb.cyclic, h->yW, h->nys, h->smem_y, h->st, h->d_bas64, h->d_wy, false);
     if (h->hb.xinv_sep)
-        k_xinv_rows<double, NL, E><<<h->nx, h->xthreads, h->smem_x64, h->st>>>(h->d_bas64, h->d_wx, 0, 0, 0.0);
-    k_xinv<double, NL><<<h->ni, h->xi_threads, h->smem_i64, h->st>>>(h->d_bas64, h->d_wi, 0, 0.0, out);
+        k_xinv_rows<double, NL, E><<<h->nx, rup(h->xthreads, 32), h->smem_x64, h->st>>>(h->d_bas64, h->d_wx, h->xg,
+                                                                                        0, 0, 0.0, out);
+    else
+        k_xinv<double, NL><<<h->ni, h->xi_threads, h->smem_i64, h->st>>>(h->d_bas64, h->d_wi, 0, 0.0, out);
 }
 
 // The dynamic shared-memory limit of a kernel is a property of the function
@@ -555,11 +580,14 @@ static void launch_phase_t(oqg_handle *h, int phase, int par, double tdt) {
         case 0: vort_kernel<T, NL>(b.vty)<<<h->nv, VTHREADS, h->smem_v, h->st>>>(h->d_bas, h->d_wv, par, tdt); break;
         case 1: k_xfwd<T, E><<<h->nx, h->xthreads, h->smem_x, h->st>>>(h->d_bas, h->d_wx, nullptr); break;
         case 2: launch_ysolve<T>(b.cyclic, h->yW, h->nys, h->smem_y, h->st, h->d_bas, h->d_wy, false); break;
-        default:
+        case 3:
             if (b.xinv_sep)
-                k_xinv_rows<T, NL, E><<<h->nx + 1, h->xthreads, h->smem_x, h->st>>>(h->d_bas, h->d_wx, 1, par, tdt);
-            k_xinv<T, NL><<<h->ni, h->xi_threads, h->smem_i, h->st>>>(h->d_bas, h->d_wi, par, tdt, nullptr);
+                k_xinv_rows<T, NL, E><<<h->nx + 1, rup(h->xthreads, 32), h->smem_x, h->st>>>(h->d_bas, h->d_wx, h->xg,
+                                                                                           1, par, tdt, nullptr);
+            else
+                k_xinv<T, NL><<<h->ni, h->xi_threads, h->smem_i, h->st>>>(h->d_bas, h->d_wi, par, tdt, nullptr);
             break;
+        default: k_xinv_asm<T, NL><<<h->na, 256, 0, h->st>>>(h->d_bas, par); break;
     }
 }
 static void launch_phase(oqg_handle *h, int phase, int par, double tdt) {
@@ -743,7 +771,7 @@ static int create_impl(const oqg_params *prm, oqg_handle **out, bool batched) {
         int best = 16;
         long best_cost = -1;
         for (int vt = 16; vt >= 8 && !batched; vt -= 4) {          // the compiled heights
-            const int ty = (P.nyp + vt - 1) / vt;
+            const int ty = vort_tile_rows(P.nyp, P.cyclic, vt);
             const long waves = ((long)b.tiles_x * ty + slots - 1) / slots;
             const long cost = waves * (vt + 6);
             if (best_cost < 0 || cost < best_cost) { best_cost = cost; best = vt; }
@@ -751,7 +779,7 @@ static int create_impl(const oqg_params *prm, oqg_handle **out, bool batched) {
         const int tuned = tuned_vty(P, h->mixed);
         if (tuned > 0 && !batched) best = tuned;
         b.vty = best;
-        b.tiles_y = (P.nyp + b.vty - 1) / b.vty;
+        b.tiles_y = vort_tile_rows(P.nyp, P.cyclic, b.vty);
     }
     b.kt = P.k_topo - 1;
     b.wait_limit = OQG_WAIT_LIMIT;
@@ -867,6 +895,7 @@ static int create_impl(const oqg_params *prm, oqg_handle **out, bool batched) {
     int GX = std::max(1, 128 / TT);
     if ((b.nl * npm + GX - 1) / GX < 148) GX = std::max(1, std::min(GX, b.nl * npm / 148));
     h->xthreads = GX * TT;
+    h->xg = GX;
     h->nx = (b.nl * npm + GX - 1) / GX;
     const size_t vsz = (size_t)(b.cyclic ? 16 : 8);
     // y-solve: 4 columns (warps) per CTA; the padded column tile (pivots come through L1)
@@ -897,22 +926,28 @@ static int create_impl(const oqg_params *prm, oqg_handle **out, bool batched) {
         const int G = std::max(1, std::min(b.nl, (int)((227 * 1024) / per)));
         nfft_i = std::min(XINV_FFT_MAX, rup(G * tt, 32));
         if ((nfft_i / tt) * per > 227 * 1024) nfft_i = rup(tt, 32);
+    }
+    // a box keeps the buffers of the separate inverse transforms (the modal
+    // rows in global memory, the step's scalars) at any width
+    if (split || !b.cyclic) {
         b.inh_g = dalloc<char>(h, (size_t)b.nl * b.nyp * b.px * 8);
         if (!b.inh_g) return bail(OQG_ECUDA, "out of device memory");
     }
-    h->xi_threads = nfft_i + 32;
-    h->smem_i = xinv_smem(b.M, b.nl, nra, b.nxp, nfft_i, h->esz, split);
-    h->smem_i64 = xinv_smem(b.M, b.nl, nra, b.nxp, nfft_i, 8, split);
-    // wide boxes: the inverse transforms run as a launch of their own, shaped
-    // like the forward one, and the assembly kernel needs no shared buffers
-    b.xinv_sep = (split && !b.cyclic) ? 1 : 0;
     b.scal_g = nullptr;
-    if (b.xinv_sep) {
-        h->smem_i = h->smem_i64 = 0;
+    if (!b.cyclic) {
         b.scal_g = dalloc<char>(h, sizeof(XinvScal));
         if (!b.scal_g) return bail(OQG_ECUDA, "out of device memory");
     }
-    if (h->smem_i64 > 227 * 1024 || h->smem_x64 > 227 * 1024 || h->smem_y > 227 * 1024)
+    h->xi_threads = nfft_i + 32;
+    h->smem_i_full = xinv_smem(b.M, b.nl, nra, b.nxp, nfft_i, h->esz, split);
+    h->smem_i64_full = xinv_smem(b.M, b.nl, nra, b.nxp, nfft_i, 8, split);
+    h->xinv_split_needed = split;
+    h->na = (int)std::min<long long>(((long long)b.nxp * b.nyp + 255) / 256, 148LL * 8);
+    // boxes: the inverse transforms run as a launch of their own, shaped like
+    // the forward one, then a one-pass assembly (oqg_set_xinv_sep; faster at
+    // 513^2 and the only form once the modal rows leave shared memory)
+    apply_xinv_sep(h, !b.cyclic);
+    if (h->smem_i64_full > 227 * 1024 || h->smem_x64 > 227 * 1024 || h->smem_y > 227 * 1024)
         return bail(OQG_EUNSUPPORTED, "grid too large for this build's shared-memory tiling");
     std::vector<Work> wv(h->nv), wx(h->nx), wy(h->nys), wi(h->ni);
     for (int i = 0; i < h->nv; ++i) wv[i] = Work{0, i};
@@ -1487,25 +1522,26 @@ int oqg_device_state(oqg_handle *h, void **p, void **pm, void **q, void **qm, in
 
 int oqg_profile_phases(oqg_handle *h, double tdt, int nsteps, double *ms) {
     if (!h || !ms || nsteps < 1) return fail(OQG_EINVAL, "bad argument");
-    cudaEvent_t ev[5];
-    for (int i = 0; i < 5; ++i) CK(cudaEventCreate(&ev[i]));
-    double acc[4] = {0, 0, 0, 0};
+    const int np = h->hb.xinv_sep ? 5 : 4;
+    cudaEvent_t ev[6];
+    for (int i = 0; i <= np; ++i) CK(cudaEventCreate(&ev[i]));
+    double acc[5] = {0, 0, 0, 0, 0};
     for (int s = 0; s < nsteps; ++s) {
         CK(cudaEventRecord(ev[0], h->st));
-        for (int ph = 0; ph < 4; ++ph) {
+        for (int ph = 0; ph < np; ++ph) {
             launch_phase(h, ph, h->par, tdt);
             CK(cudaEventRecord(ev[ph + 1], h->st));
         }
         h->par ^= 1;
-        CK(cudaEventSynchronize(ev[4]));
-        for (int ph = 0; ph < 4; ++ph) {
+        CK(cudaEventSynchronize(ev[np]));
+        for (int ph = 0; ph < np; ++ph) {
             float t = 0.f;
             CK(cudaEventElapsedTime(&t, ev[ph], ev[ph + 1]));
             acc[ph] += t;
         }
     }
-    for (int i = 0; i < 5; ++i) cudaEventDestroy(ev[i]);
-    for (int ph = 0; ph < 4; ++ph) ms[ph] = acc[ph] / nsteps;
+    for (int i = 0; i <= np; ++i) cudaEventDestroy(ev[i]);
+    for (int ph = 0; ph < 5; ++ph) ms[ph] = acc[ph] / nsteps;
     CK(cudaGetLastError());
     return OQG_OK;
 }
@@ -1534,8 +1570,12 @@ int oqg_launch_floor(oqg_handle *h, int nsteps, double *us_per_step) {
     struct Shape { int grid, block; size_t smem; };
     std::vector<Shape> sh = {{h->nv, VTHREADS, h->smem_v}, {h->nx, h->xthreads, h->smem_x},
                              {h->nys, 128 * h->yW, h->smem_y}};
-    if (h->hb.xinv_sep) sh.push_back({h->nx + 1, h->xthreads, h->smem_x});
-    sh.push_back({h->ni, h->xi_threads, h->smem_i});
+    if (h->hb.xinv_sep) {
+        sh.push_back({h->nx + 1, rup(h->xthreads, 32), h->smem_x});
+        sh.push_back({h->na, 256, 0});
+    } else {
+        sh.push_back({h->ni, h->xi_threads, h->smem_i});
+    }
     size_t mx = 0;
     for (const Shape &x : sh) mx = std::max(mx, x.smem);
     raise_smem((const void *)k_chain_empty, mx);
@@ -1699,7 +1739,7 @@ int oqg_ensemble_create(const oqg_params *members, int nmembers, oqg_ensemble **
         e->smem_x = std::max(e->smem_x, fft_inplace_len(b.M) ? (size_t)G * (LB * t2 + 2 * xrow * esz)
                                                                : (size_t)G * 2 * LB * t2);
         e->smem_y = std::max(e->smem_y, (size_t)ysolve_ld(b.ny, e->yW) * 4 * vsz);
-        e->smem_i = std::max(e->smem_i, xinv_smem(b.M, b.nl, nra, b.nxp, nfft_e, esz, b.inh_g != nullptr));
+        e->smem_i = std::max(e->smem_i, xinv_smem(b.M, b.nl, nra, b.nxp, nfft_e, esz, e->m[i]->xinv_split_needed));
     }
     if (e->smem_x > 227 * 1024 || e->smem_i > 227 * 1024 || e->smem_v > 227 * 1024) {
         ens_free(e);
@@ -1716,7 +1756,11 @@ int oqg_ensemble_create(const oqg_params *members, int nmembers, oqg_ensemble **
     };
     e->hb.resize(nmembers);
     // the ensemble's assembly launches transform in k_xinv for every member
-    for (int i = 0; i < nmembers; ++i) { e->hb[i] = e->m[i]->hb; e->hb[i].xinv_sep = 0; }
+    for (int i = 0; i < nmembers; ++i) {
+        e->hb[i] = e->m[i]->hb;
+        e->hb[i].xinv_sep = 0;
+        e->hb[i].xinv_split = e->m[i]->xinv_split_needed ? 1 : 0;
+    }
     e->d_bas = (BasinDev *)up(e->hb.data(), e->hb.size() * sizeof(BasinDev));
     e->d_wv = (Work *)up(wv.data(), wv.size() * sizeof(Work));
     e->d_wx = (Work *)up(wx.data(), wx.size() * sizeof(Work));
@@ -1751,6 +1795,7 @@ static int ens_refresh(oqg_ensemble *e, int member) {
     const double tdt = e->hb[member].tdt_m;
     e->hb[member] = e->m[member]->hb;
     e->hb[member].xinv_sep = 0;
+    e->hb[member].xinv_split = e->m[member]->xinv_split_needed ? 1 : 0;
     e->hb[member].tdt_m = tdt;
     CK(cudaMemcpyAsync(e->d_bas + member, &e->hb[member], sizeof(BasinDev), cudaMemcpyHostToDevice, e->st));
     CK(cudaStreamSynchronize(e->st));
@@ -2228,7 +2273,7 @@ int oqg_get_forcing(oqg_handle *h, double *wekp, double *ent) {
 static int set_vty(oqg_handle *h, int vt) {
     BasinDev &b = h->hb;
     b.vty = vt;
-    b.tiles_y = (b.nyp + vt - 1) / vt;
+    b.tiles_y = vort_tile_rows(b.nyp, b.cyclic, vt);
     h->nv = b.tiles_x * b.tiles_y;
     std::vector<Work> wv(h->nv);
     for (int i = 0; i < h->nv; ++i) wv[i] = Work{0, i};
@@ -2243,16 +2288,24 @@ static int set_vty(oqg_handle *h, int vt) {
     return push_desc(h);
 }
 
-extern "C" {
-
-int oqg_get_vty(oqg_handle *h, int *vty) {
-    if (!h || !vty) return fail(OQG_EINVAL, "bad argument");
-    *vty = h->hb.vty;
+// The y-solve spread over W warps per column: launch shape, shared memory,
+// the graphs.
+static int set_ysolve_w(oqg_handle *h, int W) {
+    const size_t smem = (size_t)ysolve_ld(h->hb.ny, W) * h->KB * (h->hb.cyclic ? 16 : 8);
+    if (smem > 227 * 1024) return fail(OQG_EUNSUPPORTED, "y-solve tile too large");
+    h->yW = W;
+    h->smem_y = smem;
+    set_attrs(h);
+    drop_graphs(h);
     return OQG_OK;
 }
 
-int oqg_autotune(oqg_handle *h, double tdt, int nsteps, int *best_vty, double *ms) {
-    if (!h || nsteps < 2 || !(tdt > 0.0)) return fail(OQG_EINVAL, "bad argument");
+// Times nsteps steps of tdt from the handle's state under each candidate
+// setting (set(h, c)), restoring the state before each; keeps the fastest
+// setting and the state as found.  ms[i]: ms per step of cand[i].
+template <class Set>
+static int tune_setting(oqg_handle *h, double tdt, int nsteps, const std::vector<int> &cand, Set set, int *best_out,
+                        std::vector<float> &ms) {
     size_t full = 0;
     oqg_state_bytes(h, &full, nullptr);
     void *save = nullptr;
@@ -2261,10 +2314,11 @@ int oqg_autotune(oqg_handle *h, double tdt, int nsteps, int *best_vty, double *m
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     int rc = oqg_state_save(h, save);
-    int best = h->hb.vty;
+    int best = -1;
     float best_ms = -1.0f;
-    for (int vt = 8; vt <= 16 && rc == OQG_OK; vt += 4) {           // the compiled heights
-        if ((rc = set_vty(h, vt))) break;
+    ms.assign(cand.size(), -1.0f);
+    for (size_t ci = 0; ci < cand.size() && rc == OQG_OK; ++ci) {
+        if ((rc = set(h, cand[ci]))) break;
         // warm up (captures the graphs), then time nsteps from the saved state
         if ((rc = oqg_state_load(h, save)) || (rc = oqg_step(h, tdt, nsteps))) break;
         if ((rc = oqg_state_load(h, save))) break;
@@ -2275,18 +2329,93 @@ int oqg_autotune(oqg_handle *h, double tdt, int nsteps, int *best_vty, double *m
         if (cudaEventSynchronize(e1) != cudaSuccess) { rc = fail(OQG_ECUDA, "autotune timing failed"); break; }
         float t = 0.0f;
         cudaEventElapsedTime(&t, e0, e1);
-        if (ms) ms[vt] = t / nsteps;
-        if (best_ms < 0.0f || t < best_ms) { best_ms = t; best = vt; }
+        ms[ci] = t / nsteps;
+        if (best_ms < 0.0f || t < best_ms) { best_ms = t; best = cand[ci]; }
     }
-    if (rc == OQG_OK) rc = set_vty(h, best);
+    if (rc == OQG_OK && best >= 0) rc = set(h, best);
     if (rc == OQG_OK) rc = oqg_state_load(h, save);
     if (rc == OQG_OK && cudaStreamSynchronize(h->st) != cudaSuccess) rc = fail(OQG_ECUDA, "autotune restore failed");
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     cudaFree(save);
+    if (rc == OQG_OK && best_out) *best_out = best;
+    return rc;
+}
+
+extern "C" {
+
+int oqg_get_vty(oqg_handle *h, int *vty) {
+    if (!h || !vty) return fail(OQG_EINVAL, "bad argument");
+    *vty = h->hb.vty;
+    return OQG_OK;
+}
+
+int oqg_autotune(oqg_handle *h, double tdt, int nsteps, int *best_vty, double *ms) {
+    if (!h || nsteps < 2 || !(tdt > 0.0)) return fail(OQG_EINVAL, "bad argument");
+    const std::vector<int> cand = {8, 12, 16};            // the compiled heights
+    std::vector<float> t;
+    int best = h->hb.vty;
+    const int rc = tune_setting(h, tdt, nsteps, cand, set_vty, &best, t);
     if (rc) return rc;
+    if (ms)
+        for (size_t i = 0; i < cand.size(); ++i) ms[cand[i]] = t[i];
     record_vty(h->prm, h->mixed, best);
     if (best_vty) *best_vty = best;
+    return OQG_OK;
+}
+
+int oqg_set_xinv_sep(oqg_handle *h, int on) {
+    if (!h) return fail(OQG_EINVAL, "bad argument");
+    if (h->hb.cyclic) return fail(OQG_EUNSUPPORTED, "the separate inverse transforms are built for the closed box");
+    if (!on && h->xinv_split_needed)
+        return fail(OQG_EUNSUPPORTED, "this width keeps its modal rows in global memory: the transforms run separately");
+    apply_xinv_sep(h, on != 0);
+    set_attrs(h);
+    drop_graphs(h);
+    const int rc = push_desc(h);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(h->st));
+    return OQG_OK;
+}
+
+int oqg_get_xinv_sep(oqg_handle *h, int *on) {
+    if (!h || !on) return fail(OQG_EINVAL, "bad argument");
+    *on = h->hb.xinv_sep;
+    return OQG_OK;
+}
+
+int oqg_set_vty(oqg_handle *h, int vty) {
+    if (!h || (vty != 8 && vty != 12 && vty != 16)) return fail(OQG_EINVAL, "tile height must be 8, 12 or 16");
+    const int rc = set_vty(h, vty);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(h->st));
+    return OQG_OK;
+}
+
+int oqg_set_ysolve_warps(oqg_handle *h, int warps) {
+    if (!h || (warps != 1 && warps != 2 && warps != 4)) return fail(OQG_EINVAL, "warps per column must be 1, 2 or 4");
+    const int rc = set_ysolve_w(h, warps);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(h->st));
+    return OQG_OK;
+}
+
+int oqg_get_ysolve_warps(oqg_handle *h, int *warps) {
+    if (!h || !warps) return fail(OQG_EINVAL, "bad argument");
+    *warps = h->yW;
+    return OQG_OK;
+}
+
+int oqg_autotune_ysolve(oqg_handle *h, double tdt, int nsteps, int *best_warps, double *ms) {
+    if (!h || nsteps < 2 || !(tdt > 0.0)) return fail(OQG_EINVAL, "bad argument");
+    const std::vector<int> cand = {1, 2, 4};
+    std::vector<float> t;
+    int best = h->yW;
+    const int rc = tune_setting(h, tdt, nsteps, cand, set_ysolve_w, &best, t);
+    if (rc) return rc;
+    if (ms)
+        for (size_t i = 0; i < cand.size(); ++i) ms[i] = t[i];
+    if (best_warps) *best_warps = best;
     return OQG_OK;
 }
 
@@ -2308,7 +2437,7 @@ static int ens_set_vty(oqg_ensemble *e, int vt) {
         oqg_handle *h = e->m[i];
         BasinDev &b = h->hb;
         b.vty = vt;
-        b.tiles_y = (b.nyp + vt - 1) / vt;
+        b.tiles_y = vort_tile_rows(b.nyp, b.cyclic, vt);
         if (b.tmaps && !make_tmaps(h)) return fail(OQG_ECUDA, "tensor maps could not be encoded");
         h->hb64.vty = b.vty;
         h->hb64.tiles_y = b.tiles_y;

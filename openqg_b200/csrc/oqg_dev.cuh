@@ -98,12 +98,14 @@ struct BasinDev {
     DevForcing *frc;
     double *ent_rows;           // [nyp][2] row sums of the ent area integral and their
                                 // compensations
-    void *inh_g;                // wide grids: modal rows of k_xinv, [nl][nyp][px] (8-byte slots)
+    void *inh_g;                // modal rows in global memory, [nl][nyp][px] (8-byte
+                                // slots): wide grids, and every box (k_xinv_rows)
     int *err;                   // device error bits
     // launch bookkeeping
     int k4_rows;                // interior rows per CTA of the assembly launch
-    int xinv_sep;               // the inverse transforms run as k_xinv_rows (wide boxes;
-                                // modal rows in inh_g) and k_xinv only assembles
+    int xinv_sep;               // the inverse transforms run as k_xinv_rows and the
+                                // assembly as k_xinv_asm (boxes; always when wide)
+    int xinv_split;             // k_xinv keeps its modal rows in inh_g
     void *scal_g;               // with xinv_sep: the step's scalar phase results,
                                 // written once per step by k_xinv_rows
     double tdt_m;               // leapfrog step of this member when a launch

@@ -225,7 +225,7 @@ __device__ __forceinline__ void load_tile_async(T *s, const T *__restrict__ f, c
 }
 
 // Tiles are VTX columns by b.vty rows (b.vty <= VTYMAX, chosen per basin so
-// that the tiles fill whole waves).  Shared tiles per layer (origin, pitch):
+// that the tiles fill whole waves); a box's tile rows start at row 1.  Shared tiles per layer (origin, pitch):
 //   pm     rows j0-3 .. j0+vty+2, cols from i0-4   (LPQ = VTX+8 = 68)
 //   p, q   rows j0-1 .. j0+vty,   cols from i0-4   (LPQ)
 //   qm     rows j0 .. j0+vty-1,   cols from i0     (LO = VTX)
@@ -263,6 +263,10 @@ __host__ __device__ __forceinline__ VortLayout vort_layout(int vt, int esz) {
     L.by = L.wk + vort_round(vt * LO, esz);
     L.total = L.by + vort_round(vt * 8 / esz + 1, esz);   // vt doubles
     return L;
+}
+// Rows of vorticity tiles: a box tiles its interior rows, a channel all.
+__host__ __device__ __forceinline__ int vort_tile_rows(int nyp, int cyclic, int vt) {
+    return cyclic ? (nyp + vt - 1) / vt : (nyp - 2 + vt - 1) / vt;
 }
 // Dynamic shared bytes of k_vort (plus slack to align the base to 128 bytes).
 __host__ __device__ __forceinline__ size_t vort_smem_bytes(int vt, int esz) {
@@ -316,7 +320,9 @@ k_vort(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par,
     g.nxp = b.nxp; g.nyp = b.nyp; g.cyclic = b.cyclic; g.K = sK;
     const VortLayout LY = vort_layout(VT, (int)sizeof(T));
     const int tile_x = w.block % b.tiles_x, tile_y = w.block / b.tiles_x;
-    const int i0 = tile_x * VTX, j0 = tile_y * VT;
+    // a box's tiles cover its interior rows 1 .. nyp-2 (the walls are not
+    // stepped); a channel's start at row 0 (its strip integrals hold row 0)
+    const int i0 = tile_x * VTX, j0 = tile_y * VT + (g.cyclic ? 0 : 1);
 
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T *sm = reinterpret_cast<T *>(((uintptr_t)smem_raw + 127) & ~(uintptr_t)127);
@@ -939,9 +945,9 @@ k_ysolve(const BasinDev *__restrict__ bas, const Work *__restrict__ work) {
     CSum colsum;
     if (S_ == 4) ysolve_chunk_regs<V, W, 4>(col, piv, plen, a, lane, wc, s, o, ny, sC[c], sD[c], colsum);
     else if (S_ == 8) ysolve_chunk_regs<V, W, 8>(col, piv, plen, a, lane, wc, s, o, ny, sC[c], sD[c], colsum);
-    // (16 rows per lane only with one warp per column: the multi-warp
-    // instances run at most 8 within their register budget)
-    else if (W == 1 && S_ == YREG)
+    // (16 rows per lane with one warp per column, and with four for the
+    // box; the two-warp instances run at most 8 within their register budget)
+    else if ((W == 1 || (W == 4 && !CPLX)) && S_ == YREG)
         ysolve_chunk_regs<V, W, YREG>(col, piv, plen, a, lane, wc, s, o, ny, sC[c], sD[c], colsum);
     else {
         // forward elimination: u_j = f_j beta_j - a beta_j u_{j-1}
@@ -1270,12 +1276,16 @@ __device__ __noinline__ void scalar_phase(const BasinDev &b, double tdt, int par
 // per SM), so k_xinv only assembles.  The inverse is the forward transform
 // scaled by ftnorm (inhomog.F90:200-211); the modal row j + 1 of mode m gets
 // the n interior values and zeros on both walls, and the first and last row
-// pairs of a mode clear the wall rows 0 and nyp - 1.  scal != 0: one CTA
+// pairs of a mode clear the wall rows 0 and nyp - 1 (into out instead of
+// inh_g when out != null: the solve-only mode).  scal != 0: one CTA
 // more, after the transforms', runs the step's scalar phase once into
 // b.scal_g (the assembly CTAs read it there) and writes the next state.
+// G: transforms per CTA (the forward launch's), blockDim >= G TT rounded up
+// to whole warps so the scalar CTA has a full warp.
 template <class T, int NL, int E>
 __global__ void __launch_bounds__(256, 2)
-k_xinv_rows(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int scal, int par, double tdt) {
+k_xinv_rows(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int G, int scal, int par,
+            double tdt, T *out) {
     typedef typename C2<T>::t T2;
     if (scal && blockIdx.x == gridDim.x - 1) {
         pdl_trigger();
@@ -1289,7 +1299,7 @@ k_xinv_rows(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int
     const Work w = work[blockIdx.x];
     const BasinDev &b = bas[w.member];
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int M = b.M, TT = (M + E - 1) / E, G = blockDim.x / TT;
+    const int M = b.M, TT = (M + E - 1) / E;
     const int g = threadIdx.x / TT, t = threadIdx.x - g * TT;
     const int LB = fft_buf_len(M);
     T2 *zs = reinterpret_cast<T2 *>(smem_raw);
@@ -1307,7 +1317,9 @@ k_xinv_rows(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int
     T *raw = ip ? reinterpret_cast<T *>(zs + (size_t)G * LB) + (size_t)(g < G ? g : 0) * 2 * RO
                 : reinterpret_cast<T *>(zb);
     const T *x = (const T *)b.spec + ((size_t)m * b.ny + j) * b.pk;
-    T *inh = (T *)b.inh_g;
+    // out != null: solve-only mode, the modal solutions go straight to out
+    // ([nl][nyp][px], the same layout)
+    T *inh = out ? out : (T *)b.inh_g;
     const T ftn = (T)b.ftnorm;
     pdl_trigger();
     pdl_wait();
@@ -1409,7 +1421,7 @@ k_xinv(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par,
     // global buffer b.inh_g ([nl][nyp][px], rows of this CTA only).
     T2 *setA = reinterpret_cast<T2 *>(smem_raw), *setB = setA + (size_t)G * LB;
     T2 *set_in = (b.nrad & 1) ? setB : setA, *set_st = (b.nrad & 1) ? setA : setB;
-    const bool split = b.inh_g != nullptr;
+    const bool split = b.xinv_split != 0;
     const bool alias = one_round && !split;
     // a row of the spectral buffer: n reals (box) or nk complex (channel)
     const int rowbytes = b.cyclic ? b.nk * (int)sizeof(T2) : n * (int)sizeof(T);
@@ -1427,18 +1439,10 @@ k_xinv(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par,
     pdl_trigger();
     if (!fft_thread) {
         pdl_wait();
-        if (!out) {
-            if (split && b.xinv_sep) {
-                // computed once by k_xinv_rows
-                const double *src = (const double *)b.scal_g;
-                double *dst = reinterpret_cast<double *>(&sS);
-                for (int x = threadIdx.x & 31; x < (int)(sizeof(XinvScal) / sizeof(double)); x += 32) dst[x] = src[x];
-            } else {
-                scalar_phase<T, NL>(b, tdt != 0.0 ? tdt : b.tdt_m, par, w.block == 0, &sS);
-            }
-        }
+        if (!out) scalar_phase<T, NL>(b, tdt != 0.0 ? tdt : b.tdt_m, par, w.block == 0, &sS);
     } else if (split && b.xinv_sep) {
-        pdl_wait();                     // the modal rows come from k_xinv_rows
+        // (solve-only mode) the modal rows come from k_xinv_rows
+        pdl_wait();
     } else {
     // zero the wall rows / columns of the modal fields
     if (!alias)
@@ -1671,6 +1675,108 @@ k_xinv(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par,
             for (int i = threadIdx.x; i < nxp; i += blockDim.x) wall_point(lr, i);
         } else if (!b.cyclic && threadIdx.x < 2) {
             wall_point(lr, threadIdx.x == 0 ? 0 : nxp - 1);
+        }
+    }
+}
+
+// ------------------------------------------------------------------ k_xinv_asm
+// The assembly of a box whose inverse transforms ran as k_xinv_rows: the
+// homogeneous correction and modes_to_layers (modes.F90:268-284) of every
+// point from the modal rows in b.inh_g, ocqbdy (vorsubs.F90:58-114) on the
+// walls and the suppress_comp_mode averages (driver.F90:174-189), with the
+// step's scalars from b.scal_g.  One thread per point; a wall point also
+// forms the layer values of its inner neighbour (the same arithmetic as the
+// neighbour's own thread), so no point waits for another.
+template <class T, int NL>
+__device__ __forceinline__ void xinv_layers(const BasinDev &b, const T *__restrict__ inh, const T *__restrict__ H,
+                                            const double *ctm, const double *hc, size_t o2, T *pn) {
+    const size_t ms = (size_t)b.nyp * b.px;
+    double pm_[NL];
+#pragma unroll
+    for (int m = 0; m < NL; ++m) pm_[m] = (double)inh[m * ms + o2];
+#pragma unroll
+    for (int m = 1; m < NL; ++m) pm_[m] = pm_[m] + hc[m - 1] * (double)H[(m - 1) * ms + o2];
+#pragma unroll
+    for (int k = 0; k < NL; ++k) {
+        double s2 = 0.0;
+#pragma unroll
+        for (int m = 0; m < NL; ++m) s2 += pm_[m] * ctm[m + NL * k];
+        pn[k] = (T)s2;
+    }
+}
+
+template <class T, int NL>
+__global__ void __launch_bounds__(256)
+k_xinv_asm(const BasinDev *__restrict__ bas, int par) {
+    const BasinDev &b = bas[0];
+    __shared__ double sCtm[NL * NL], sAmat[NL * NL], sHc[NL > 1 ? NL - 1 : 1];
+    __shared__ int sSupp;
+    pdl_trigger();
+    pdl_wait();
+    const XinvScal *sc = (const XinvScal *)b.scal_g;
+    if (threadIdx.x < NL * NL) {
+        sCtm[threadIdx.x] = b.ctm2l[threadIdx.x];
+        sAmat[threadIdx.x] = b.amat[threadIdx.x];
+    }
+    if (threadIdx.x < NL - 1) sHc[threadIdx.x] = sc->alpha[threadIdx.x];
+    if (threadIdx.x == 0) sSupp = sc->supp;
+    __syncthreads();
+    double ctm[NL * NL], hc[NL > 1 ? NL - 1 : 1];
+#pragma unroll
+    for (int x = 0; x < NL * NL; ++x) ctm[x] = sCtm[x];
+#pragma unroll
+    for (int m = 0; m < NL - 1; ++m) hc[m] = sHc[m];
+    const bool supp = sSupp != 0;
+    const int nxp = b.nxp, nyp = b.nyp, px = b.px;
+    const size_t ms = (size_t)nyp * px;
+    const T *__restrict__ inh = (const T *)b.inh_g;
+    const T *__restrict__ H = (const T *)b.hsb;
+    const T *__restrict__ Pold = (const T *)b.F[par];
+    T *__restrict__ Pnew = (T *)b.F[1 - par];
+    T *__restrict__ Qc = (T *)b.F[3 - par];          // q after this step
+    const T *__restrict__ Qm = (const T *)b.F[2 + par];
+    const T fac = (T)b.qb_fac;
+    const FastDiv fdx(nxp);
+    const int npts = nxp * nyp;
+    for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < npts; idx += gridDim.x * blockDim.x) {
+        const int j = fdx.div(idx), i = idx - j * nxp;
+        const size_t o2 = (size_t)j * px + i;
+        T pn[NL];
+        xinv_layers<T, NL>(b, inh, H, ctm, hc, o2, pn);
+#pragma unroll
+        for (int k = 0; k < NL; ++k)
+            Pnew[k * ms + o2] = supp ? (T)((T)0.5 * (pn[k] + Pold[k * ms + o2])) : pn[k];
+        const bool zon = (j == 0 || j == nyp - 1);
+        const bool mer = (i == 0 || i == nxp - 1);
+        if (!zon && !mer) {
+            if (supp)
+#pragma unroll
+                for (int k = 0; k < NL; ++k) Qc[k * ms + o2] = (T)0.5 * (Qc[k * ms + o2] + Qm[k * ms + o2]);
+            continue;
+        }
+        // ocqbdy: the inner neighbour across the meridional wall (a corner
+        // takes that one), else across the zonal wall
+        const size_t on = mer ? (size_t)j * px + (i == 0 ? 1 : nxp - 2)
+                              : (size_t)(j == 0 ? 1 : nyp - 2) * px + i;
+        T pnb[NL];
+        xinv_layers<T, NL>(b, inh, H, ctm, hc, on, pnb);
+        const int cnt = (zon ? 1 : 0) + (mer ? 1 : 0);
+        const T by = (T)(b.beta * b.yprel[j]);
+#pragma unroll
+        for (int k = 0; k < NL; ++k) {
+            T qv = fac * (pnb[k] - pn[k]);
+            double mv = 0.0;
+#pragma unroll
+            for (int l = 0; l < NL; ++l) mv += sAmat[k + NL * l] * (double)pn[l];
+            const T fmv = (T)(b.fnot * mv);
+            for (int c = 0; c < cnt; ++c) qv = qv - fmv;
+            // (FP32 storage holds q - beta y: one beta y fewer)
+            for (int c = q_anom_stored<T>() ? 1 : 0; c < cnt; ++c) qv = qv + by;
+            if (k == b.kt && b.topo_active) {
+                const T dd = (T)b.ddyn[o2];
+                for (int c = 0; c < cnt; ++c) qv = qv + dd;
+            }
+            Qc[k * ms + o2] = supp ? (T)((T)0.5 * (qv + Qm[k * ms + o2])) : qv;
         }
     }
 }

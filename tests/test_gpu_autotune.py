@@ -8,7 +8,7 @@ import numpy as np
 import pytest
 
 import oracle
-from openqg_b200.core import QG
+from openqg_b200.core import QG, OqgError
 from openqg_b200.params import OQG_MIXED, atmos_channel, double_gyre_tau, initial_psi, ocean_double_gyre
 from tests.qg_numpy import rel_l2
 
@@ -60,4 +60,47 @@ def test_autotune_keeps_state_and_results(precision, channel):
     g2 = QG(b)
     assert g2.tile_rows() == best
     for x in (g, ref, g2):
+        x.close()
+
+
+@pytest.mark.parametrize("n,channel", [(257, False), (161, True)])
+def test_ysolve_warps_tuning_keeps_state_and_results(n, channel):
+    """The y-solve with 1, 2 and 4 warps per column: the tuner times each,
+    keeps the fastest, leaves the state as found, and stepping with the
+    chosen split matches the default one to rounding."""
+    b = atmos_channel(n, 97) if channel else ocean_double_gyre(n)
+    g, ref = _handle(b), _handle(b)
+    tdt = 360.0 if channel else 3600.0
+    g.step(tdt, 2)
+    ref.step(tdt, 2)
+    before = g.get_state()
+    w0 = g.ysolve_warps()
+    assert w0 in (1, 2, 4)
+    best, ms = g.autotune_ysolve(tdt, 4)
+    assert best in (1, 2, 4) and g.ysolve_warps() == best
+    assert sorted(ms) == [1, 2, 4] and all(v > 0 for v in ms.values())
+    for a, r in zip(g.get_state(), before):
+        assert np.array_equal(a, r)
+    g.step(tdt, 5)
+    ref.step(tdt, 5)
+    for a, r in zip(g.get_state(), ref.get_state()):
+        assert rel_l2(a, r) <= 1e-12
+    for x in (g, ref):
+        x.close()
+
+
+def test_fixed_settings_are_kept_and_checked():
+    b = ocean_double_gyre(129)
+    g, ref = _handle(b), _handle(b)
+    g.set_tile_rows(12)
+    g.set_ysolve_warps(4)
+    assert g.tile_rows() == 12 and g.ysolve_warps() == 4
+    for bad in (lambda: g.set_tile_rows(10), lambda: g.set_ysolve_warps(3)):
+        with pytest.raises(OqgError):
+            bad()
+    g.step(3600.0, 4)
+    ref.step(3600.0, 4)
+    for a, r in zip(g.get_state(), ref.get_state()):
+        assert rel_l2(a, r) <= 1e-12
+    for x in (g, ref):
         x.close()

@@ -22,7 +22,7 @@ def test_launch_floor_is_a_small_part_of_a_step():
     g.set_state(p, p)
     w, ts, tn = ekman_from_tau(b, *double_gyre_tau(b))
     g.set_forcing(w, None, ts, tn)
-    assert g.step_launches() == 4
+    assert g.step_launches() == 5
     floor = g.launch_floor(16)
     ms = g.profile_phases(3600.0, 5)
     assert 0.0 < floor < 0.5 * 1000.0 * sum(ms), (floor, ms)

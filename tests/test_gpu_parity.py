@@ -182,6 +182,37 @@ def test_step_parity(b, kw):
     assert g.step_index() == 10
 
 
+@pytest.mark.parametrize("b,kw", [STEP_CASES[i] for i in (1, 4, 6, 11)],
+                         ids=[STEP_IDS[i] for i in (1, 4, 6, 11)])
+def test_step_parity_separate_inverse(b, kw):
+    """Boxes with the inverse transforms and the assembly in one kernel (off)
+    and as two launches (on, the default for boxes), switched on one handle."""
+    g, o = make_pair(b, **kw)
+    assert g.xinv_sep() and g.step_launches() == 5
+    g.set_xinv_sep(False)
+    assert not g.xinv_sep() and g.step_launches() == 4
+    g.step(3600.0, 1)
+    o.step(3600.0, 1)
+    assert_state_close(g, o, 1e-12, "1 step")
+    assert_constraints_close(g, o, 1e-11)
+    g.step(3600.0, 29)            # through a suppression step (every 25)
+    o.step(3600.0, 29)
+    assert_state_close(g, o, 1e-10, "30 steps")
+    assert_constraints_close(g, o, 1e-9)
+    g.set_xinv_sep(True)
+    assert g.xinv_sep()
+    g.step(3600.0, 1)
+    o.step(3600.0, 1)
+    assert_state_close(g, o, 1e-10, "31 steps")
+
+
+def test_separate_inverse_is_box_only():
+    g = QG(atmos_channel(49, 25))
+    with pytest.raises(Exception):
+        g.set_xinv_sep(True)
+    g.close()
+
+
 def test_topography_and_drag_layer():
     b = ocean_double_gyre(65)
     yy, xx = np.meshgrid(np.linspace(-1, 1, b.nyp), np.linspace(-1, 1, b.nxp), indexing="ij")
