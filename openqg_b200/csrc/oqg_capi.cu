@@ -56,6 +56,7 @@ struct oqg_handle {
     BasinDev *d_bas = nullptr, *d_bas64 = nullptr;
     std::vector<void *> allocs;
     Work *d_wv = nullptr, *d_wx = nullptr, *d_wy = nullptr, *d_wi = nullptr;
+    Work *d_wa = nullptr;                // k_xinv_asm work items
     int nv = 0, nx = 0, nys = 0, ni = 0;
     int E = 8, KB = 16, xthreads = 128, xi_threads = 64;
     int yW = 1;                          // warps per y-solve column
@@ -166,6 +167,29 @@ static int ysolve_warps(int ny, long long ncols) {
     return W;
 }
 
+// The transform kernels' instance for a basin's transform length: one built
+// for each length of the configurations' boxes (only that FFT plan in its
+// code), the any-length one otherwise (and for ensembles).
+#define OQG_XLENS(X) X(256) X(512) X(1024) X(2048) X(4096)
+template <class T, int E>
+static void (*xfwd_kernel(int M))(const BasinDev *, const Work *, const void *) {
+    switch (M) {
+#define OQG_XF(MM) case MM: return k_xfwd<T, E, MM>;
+        OQG_XLENS(OQG_XF)
+#undef OQG_XF
+        default: return k_xfwd<T, E>;
+    }
+}
+template <class T, int NL, int E>
+static void (*xinv_rows_kernel(int M))(const BasinDev *, const Work *, int, int, int, double, T *) {
+    switch (M) {
+#define OQG_XI(MM) case MM: return k_xinv_rows<T, NL, E, MM>;
+        OQG_XLENS(OQG_XI)
+#undef OQG_XI
+        default: return k_xinv_rows<T, NL, E>;
+    }
+}
+
 // The vorticity kernel instance of a tile height (vort_tile_ok).
 typedef void (*VortFn)(const BasinDev *, const Work *, int, double);
 template <class T, int NL>
@@ -194,12 +218,12 @@ template <class T, int NL, int E>
 static void launch_step_t(oqg_handle *h, int par, double tdt) {
     const BasinDev &b = h->hb;
     launch_pdl(vort_kernel<T, NL>(h->hb.vty), h->nv, VTHREADS, h->smem_v, h->st, h->d_bas, h->d_wv, par, tdt);
-    launch_pdl(k_xfwd<T, E>, h->nx, h->xthreads, h->smem_x, h->st, h->d_bas, h->d_wx, (const void *)nullptr);
+    launch_pdl(xfwd_kernel<T, E>(b.M), h->nx, h->xthreads, h->smem_x, h->st, h->d_bas, h->d_wx, (const void *)nullptr);
     launch_ysolve<T>(b.cyclic, h->yW, h->nys, h->smem_y, h->st, h->d_bas, h->d_wy, true);
     if (b.xinv_sep) {
-        launch_pdl(k_xinv_rows<T, NL, E>, h->nx + 1, rup(h->xthreads, 32), h->smem_x, h->st, h->d_bas, h->d_wx,
+        launch_pdl(xinv_rows_kernel<T, NL, E>(b.M), h->nx + 1, rup(h->xthreads, 32), h->smem_x, h->st, h->d_bas, h->d_wx,
                    h->xg, 1, par, tdt, (T *)nullptr);
-        launch_pdl(k_xinv_asm<T, NL>, h->na, 256, 0, h->st, h->d_bas, par);
+        launch_pdl(k_xinv_asm<T, NL>, h->na, 256, 0, h->st, h->d_bas, (const Work *)h->d_wa, par);
     } else {
         launch_pdl(k_xinv<T, NL>, h->ni, h->xi_threads, h->smem_i, h->st, h->d_bas, h->d_wi, par, tdt,
                    (double *)nullptr);
@@ -213,21 +237,21 @@ static void launch_step_t(oqg_handle *h, int par, double tdt) {
 template <int NL, int E>
 static void launch_solve_t(oqg_handle *h, double *out, bool pdl) {
     if (pdl) {
-        launch_pdl(k_xfwd<double, E>, h->nx, h->xthreads, h->smem_x64, h->st, h->d_bas64, h->d_wx,
+        launch_pdl(xfwd_kernel<double, E>(h->hb.M), h->nx, h->xthreads, h->smem_x64, h->st, h->d_bas64, h->d_wx,
                    (const void *)nullptr);
         launch_ysolve<double>(h->hb.cyclic, h->yW, h->nys, h->smem_y, h->st, h->d_bas64, h->d_wy, true);
         if (h->hb.xinv_sep)
-            launch_pdl(k_xinv_rows<double, NL, E>, h->nx, rup(h->xthreads, 32), h->smem_x64, h->st, h->d_bas64,
+            launch_pdl(xinv_rows_kernel<double, NL, E>(h->hb.M), h->nx, rup(h->xthreads, 32), h->smem_x64, h->st, h->d_bas64,
                        h->d_wx, h->xg, 0, 0, 0.0, out);
         else
             launch_pdl(k_xinv<double, NL>, h->ni, h->xi_threads, h->smem_i64, h->st, h->d_bas64, h->d_wi, 0, 0.0,
                        out);
         return;
     }
-    k_xfwd<double, E><<<h->nx, h->xthreads, h->smem_x64, h->st>>>(h->d_bas64, h->d_wx, nullptr);
+    xfwd_kernel<double, E>(h->hb.M)<<<h->nx, h->xthreads, h->smem_x64, h->st>>>(h->d_bas64, h->d_wx, nullptr);
     launch_ysolve<double>(h->hb.cyclic, h->yW, h->nys, h->smem_y, h->st, h->d_bas64, h->d_wy, false);
     if (h->hb.xinv_sep)
-        k_xinv_rows<double, NL, E><<<h->nx, rup(h->xthreads, 32), h->smem_x64, h->st>>>(h->d_bas64, h->d_wx, h->xg,
+        xinv_rows_kernel<double, NL, E>(h->hb.M)<<<h->nx, rup(h->xthreads, 32), h->smem_x64, h->st>>>(h->d_bas64, h->d_wx, h->xg,
                                                                                         0, 0, 0.0, out);
     else
         k_xinv<double, NL><<<h->ni, h->xi_threads, h->smem_i64, h->st>>>(h->d_bas64, h->d_wi, 0, 0.0, out);
@@ -269,6 +293,9 @@ static void raise_step_smem(size_t v, size_t x, size_t y, size_t i) {
     for (int vt : {8, 12, 16}) raise_smem((const void *)vort_kernel<T, NL>(vt), v);
     raise_smem((const void *)k_xfwd<T, E>, x);
     raise_smem((const void *)k_xinv_rows<T, NL, E>, x);
+#define OQG_RX(MM) raise_smem((const void *)k_xfwd<T, E, MM>, x); raise_smem((const void *)k_xinv_rows<T, NL, E, MM>, x);
+    OQG_XLENS(OQG_RX)
+#undef OQG_RX
     raise_ysolve_smem<T>(y);
     raise_smem((const void *)k_xinv<T, NL>, i);
 }
@@ -276,24 +303,24 @@ static void raise_step_smem(size_t v, size_t x, size_t y, size_t i) {
 template <class T, int NL, int E>
 static void set_attrs_t(oqg_handle *h) {
     raise_step_smem<T, NL, E>(h->smem_v, h->smem_x, h->smem_y, h->smem_i);
-    raise_smem((const void *)k_xfwd<double, E>, h->smem_x64);
-    raise_smem((const void *)k_xinv_rows<double, NL, E>, h->smem_x64);
+    raise_smem((const void *)xfwd_kernel<double, E>(h->hb.M), h->smem_x64);
+    raise_smem((const void *)xinv_rows_kernel<double, NL, E>(h->hb.M), h->smem_x64);
     raise_ysolve_smem<double>(h->smem_y);
     raise_smem((const void *)k_xinv<double, NL>, h->smem_i64);
 }
 
-// dispatch over (T, NL, E)
+// dispatch over (T, NL); 16 values per transform thread
 #define OQG_DISPATCH(FN, h, ...)                                                      \
     do {                                                                              \
-        const int nl_ = (h)->hb.nl, e_ = (h)->E;                                      \
+        const int nl_ = (h)->hb.nl;                                                   \
         if ((h)->mixed) {                                                             \
-            if (nl_ == 2) { if (e_ == 8) FN<float, 2, 8>(__VA_ARGS__); else FN<float, 2, 16>(__VA_ARGS__); } \
-            else if (nl_ == 3) { if (e_ == 8) FN<float, 3, 8>(__VA_ARGS__); else FN<float, 3, 16>(__VA_ARGS__); } \
-            else { if (e_ == 8) FN<float, 4, 8>(__VA_ARGS__); else FN<float, 4, 16>(__VA_ARGS__); } \
+            if (nl_ == 2) FN<float, 2, 16>(__VA_ARGS__);                              \
+            else if (nl_ == 3) FN<float, 3, 16>(__VA_ARGS__);                         \
+            else FN<float, 4, 16>(__VA_ARGS__);                                       \
         } else {                                                                      \
-            if (nl_ == 2) { if (e_ == 8) FN<double, 2, 8>(__VA_ARGS__); else FN<double, 2, 16>(__VA_ARGS__); } \
-            else if (nl_ == 3) { if (e_ == 8) FN<double, 3, 8>(__VA_ARGS__); else FN<double, 3, 16>(__VA_ARGS__); } \
-            else { if (e_ == 8) FN<double, 4, 8>(__VA_ARGS__); else FN<double, 4, 16>(__VA_ARGS__); } \
+            if (nl_ == 2) FN<double, 2, 16>(__VA_ARGS__);                             \
+            else if (nl_ == 3) FN<double, 3, 16>(__VA_ARGS__);                        \
+            else FN<double, 4, 16>(__VA_ARGS__);                                      \
         }                                                                             \
     } while (0)
 
@@ -302,9 +329,9 @@ static void set_attrs(oqg_handle *h) { OQG_DISPATCH(set_attrs_t, h, h); }
 
 static void launch_solve(oqg_handle *h, double *out, bool pdl = false) {
     const int nl = h->hb.nl;
-    if (nl == 2) { if (h->E == 8) launch_solve_t<2, 8>(h, out, pdl); else launch_solve_t<2, 16>(h, out, pdl); }
-    else if (nl == 3) { if (h->E == 8) launch_solve_t<3, 8>(h, out, pdl); else launch_solve_t<3, 16>(h, out, pdl); }
-    else { if (h->E == 8) launch_solve_t<4, 8>(h, out, pdl); else launch_solve_t<4, 16>(h, out, pdl); }
+    if (nl == 2) launch_solve_t<2, 16>(h, out, pdl);
+    else if (nl == 3) launch_solve_t<3, 16>(h, out, pdl);
+    else launch_solve_t<4, 16>(h, out, pdl);
 }
 
 #define OQG_NL_T(FN, h, ...)                                                                   \
@@ -578,16 +605,16 @@ static void launch_phase_t(oqg_handle *h, int phase, int par, double tdt) {
     const BasinDev &b = h->hb;
     switch (phase) {
         case 0: vort_kernel<T, NL>(b.vty)<<<h->nv, VTHREADS, h->smem_v, h->st>>>(h->d_bas, h->d_wv, par, tdt); break;
-        case 1: k_xfwd<T, E><<<h->nx, h->xthreads, h->smem_x, h->st>>>(h->d_bas, h->d_wx, nullptr); break;
+        case 1: xfwd_kernel<T, E>(b.M)<<<h->nx, h->xthreads, h->smem_x, h->st>>>(h->d_bas, h->d_wx, nullptr); break;
         case 2: launch_ysolve<T>(b.cyclic, h->yW, h->nys, h->smem_y, h->st, h->d_bas, h->d_wy, false); break;
         case 3:
             if (b.xinv_sep)
-                k_xinv_rows<T, NL, E><<<h->nx + 1, rup(h->xthreads, 32), h->smem_x, h->st>>>(h->d_bas, h->d_wx, h->xg,
+                xinv_rows_kernel<T, NL, E>(b.M)<<<h->nx + 1, rup(h->xthreads, 32), h->smem_x, h->st>>>(h->d_bas, h->d_wx, h->xg,
                                                                                            1, par, tdt, nullptr);
             else
                 k_xinv<T, NL><<<h->ni, h->xi_threads, h->smem_i, h->st>>>(h->d_bas, h->d_wi, par, tdt, nullptr);
             break;
-        default: k_xinv_asm<T, NL><<<h->na, 256, 0, h->st>>>(h->d_bas, par); break;
+        default: k_xinv_asm<T, NL><<<h->na, 256, 0, h->st>>>(h->d_bas, h->d_wa, par); break;
     }
 }
 static void launch_phase(oqg_handle *h, int phase, int par, double tdt) {
@@ -609,6 +636,9 @@ struct oqg_ensemble {
     int nl = 3, E = 8, cyclic = 0;
     BasinDev *d_bas = nullptr;
     Work *d_wv = nullptr, *d_wx = nullptr, *d_wy = nullptr, *d_wi = nullptr;
+    Work *d_wa = nullptr;              // k_xinv_asm work items (boxes)
+    int na = 0;                        // k_xinv_asm work items
+    bool sep = false;                  // boxes: k_xinv_rows + k_xinv_asm
     int nv = 0, nx = 0, nys = 0, ni = 0;
     size_t smem_v = 0, smem_x = 0, smem_y = 0, smem_i = 0;
     int xi_threads = 64, xthreads = 128;
@@ -621,15 +651,15 @@ struct oqg_ensemble {
 
 #define OQG_DISPATCH_E(FN, e, ...)                                                    \
     do {                                                                              \
-        const int nl_ = (e)->nl, e_ = (e)->E;                                         \
+        const int nl_ = (e)->nl;                                                      \
         if ((e)->mixed) {                                                             \
-            if (nl_ == 2) { if (e_ == 8) FN<float, 2, 8>(__VA_ARGS__); else FN<float, 2, 16>(__VA_ARGS__); } \
-            else if (nl_ == 3) { if (e_ == 8) FN<float, 3, 8>(__VA_ARGS__); else FN<float, 3, 16>(__VA_ARGS__); } \
-            else { if (e_ == 8) FN<float, 4, 8>(__VA_ARGS__); else FN<float, 4, 16>(__VA_ARGS__); } \
+            if (nl_ == 2) FN<float, 2, 16>(__VA_ARGS__);                              \
+            else if (nl_ == 3) FN<float, 3, 16>(__VA_ARGS__);                         \
+            else FN<float, 4, 16>(__VA_ARGS__);                                       \
         } else {                                                                      \
-            if (nl_ == 2) { if (e_ == 8) FN<double, 2, 8>(__VA_ARGS__); else FN<double, 2, 16>(__VA_ARGS__); } \
-            else if (nl_ == 3) { if (e_ == 8) FN<double, 3, 8>(__VA_ARGS__); else FN<double, 3, 16>(__VA_ARGS__); } \
-            else { if (e_ == 8) FN<double, 4, 8>(__VA_ARGS__); else FN<double, 4, 16>(__VA_ARGS__); } \
+            if (nl_ == 2) FN<double, 2, 16>(__VA_ARGS__);                             \
+            else if (nl_ == 3) FN<double, 3, 16>(__VA_ARGS__);                        \
+            else FN<double, 4, 16>(__VA_ARGS__);                                      \
         }                                                                             \
     } while (0)
 
@@ -640,8 +670,16 @@ static void launch_ens_step_t(oqg_ensemble *e, int par) {
     launch_pdl(vort_kernel<T, NL>(e->hb[0].vty), e->nv, VTHREADS, e->smem_v, e->st, e->d_bas, e->d_wv, par, 0.0);
     launch_pdl(k_xfwd<T, E>, e->nx, e->xthreads, e->smem_x, e->st, e->d_bas, e->d_wx, (const void *)nullptr);
     launch_ysolve<T>(e->cyclic, e->yW, e->nys, e->smem_y, e->st, e->d_bas, e->d_wy, true);
-    launch_pdl(k_xinv<T, NL>, e->ni, e->xi_threads, e->smem_i, e->st, e->d_bas, e->d_wi, par, 0.0,
-               (double *)nullptr);
+    if (e->sep) {
+        // per-member transform groups (G = 0) and one scalar CTA per member
+        const int nm = (int)e->m.size();
+        launch_pdl(k_xinv_rows<T, NL, E>, e->nx + nm, e->xthreads, e->smem_x, e->st, e->d_bas, e->d_wx, 0, nm, par,
+                   0.0, (T *)nullptr);
+        launch_pdl(k_xinv_asm<T, NL>, e->na, 256, 0, e->st, e->d_bas, (const Work *)e->d_wa, par);
+    } else {
+        launch_pdl(k_xinv<T, NL>, e->ni, e->xi_threads, e->smem_i, e->st, e->d_bas, e->d_wi, par, 0.0,
+                   (double *)nullptr);
+    }
 }
 template <class T, int NL, int E>
 static void raise_ens_smem_t(oqg_ensemble *e) {
@@ -942,14 +980,15 @@ static int create_impl(const oqg_params *prm, oqg_handle **out, bool batched) {
     h->smem_i_full = xinv_smem(b.M, b.nl, nra, b.nxp, nfft_i, h->esz, split);
     h->smem_i64_full = xinv_smem(b.M, b.nl, nra, b.nxp, nfft_i, 8, split);
     h->xinv_split_needed = split;
-    h->na = (int)std::min<long long>(((long long)b.nxp * b.nyp + 255) / 256, 148LL * 8);
+    h->na = (b.nxp * b.nyp + XASM_POINTS - 1) / XASM_POINTS;
     // boxes: the inverse transforms run as a launch of their own, shaped like
     // the forward one, then a one-pass assembly (oqg_set_xinv_sep; faster at
     // 513^2 and the only form once the modal rows leave shared memory)
     apply_xinv_sep(h, !b.cyclic);
     if (h->smem_i64_full > 227 * 1024 || h->smem_x64 > 227 * 1024 || h->smem_y > 227 * 1024)
         return bail(OQG_EUNSUPPORTED, "grid too large for this build's shared-memory tiling");
-    std::vector<Work> wv(h->nv), wx(h->nx), wy(h->nys), wi(h->ni);
+    std::vector<Work> wv(h->nv), wx(h->nx), wy(h->nys), wi(h->ni), wa(h->na);
+    for (int i = 0; i < h->na; ++i) wa[i] = Work{0, i};
     for (int i = 0; i < h->nv; ++i) wv[i] = Work{0, i};
     for (int i = 0; i < h->nx; ++i) wx[i] = Work{0, i};
     for (int i = 0; i < h->nys; ++i) wy[i] = Work{0, i};
@@ -958,10 +997,12 @@ static int create_impl(const oqg_params *prm, oqg_handle **out, bool batched) {
     h->d_wx = dalloc<Work>(h, wx.size());
     h->d_wy = dalloc<Work>(h, wy.size());
     h->d_wi = dalloc<Work>(h, wi.size());
+    h->d_wa = dalloc<Work>(h, wa.size());
     CK(cudaMemcpy(h->d_wv, wv.data(), wv.size() * sizeof(Work), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(h->d_wx, wx.data(), wx.size() * sizeof(Work), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(h->d_wy, wy.data(), wy.size() * sizeof(Work), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(h->d_wi, wi.data(), wi.size() * sizeof(Work), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(h->d_wa, wa.data(), wa.size() * sizeof(Work), cudaMemcpyHostToDevice));
 
     b.tmaps = nullptr;
     make_tmaps(h);
@@ -1709,7 +1750,10 @@ int oqg_ensemble_create(const oqg_params *members, int nmembers, oqg_ensemble **
     std::stable_sort(order.begin(), order.end(), [&](int a, int c) {
         return (long)e->m[a]->hb.nxp * e->m[a]->hb.nyp > (long)e->m[c]->hb.nxp * e->m[c]->hb.nyp;
     });
-    std::vector<Work> wv, wx, wy, wi;
+    std::vector<Work> wv, wx, wy, wi, wa;
+    // boxes invert as a transform launch and a one-pass assembly, as single
+    // handles do
+    e->sep = !e->cyclic;
     int nfft_e = 32;
     for (oqg_handle *h : e->m) nfft_e = std::max(nfft_e, xinv_fft_threads(h->hb.M, h->hb.nl));
     e->xi_threads = nfft_e + 32;
@@ -1733,6 +1777,7 @@ int oqg_ensemble_create(const oqg_params *members, int nmembers, oqg_ensemble **
         for (int k = 0; k < nxb; ++k) wx.push_back(Work{i, k});
         for (int k = 0; k < nyb; ++k) wy.push_back(Work{i, k});
         for (int k = 0; k < nib; ++k) wi.push_back(Work{i, k});
+        for (int k = 0; k < (b.nxp * b.nyp + XASM_POINTS - 1) / XASM_POINTS; ++k) wa.push_back(Work{i, k});
         const int nra = (b.ny > b.k4_rows) ? b.k4_rows + 1 : b.ny + 2;
         e->smem_v = std::max(e->smem_v, vort_smem_bytes(b.vty, (int)esz));
         const size_t xrow = (size_t)((b.nxin + 3) & ~3);
@@ -1746,6 +1791,7 @@ int oqg_ensemble_create(const oqg_params *members, int nmembers, oqg_ensemble **
         return fail(OQG_EUNSUPPORTED, "ensemble member too large for the shared-memory tiling");
     }
     e->nv = (int)wv.size(); e->nx = (int)wx.size(); e->nys = (int)wy.size(); e->ni = (int)wi.size();
+    e->na = (int)wa.size();
     e->wv_cap = wv.size();
     auto up = [&](const void *src, size_t bytes) -> void * {
         void *d = nullptr;
@@ -1755,18 +1801,18 @@ int oqg_ensemble_create(const oqg_params *members, int nmembers, oqg_ensemble **
         return d;
     };
     e->hb.resize(nmembers);
-    // the ensemble's assembly launches transform in k_xinv for every member
     for (int i = 0; i < nmembers; ++i) {
         e->hb[i] = e->m[i]->hb;
-        e->hb[i].xinv_sep = 0;
-        e->hb[i].xinv_split = e->m[i]->xinv_split_needed ? 1 : 0;
+        e->hb[i].xinv_sep = e->sep ? 1 : 0;
+        e->hb[i].xinv_split = (e->sep || e->m[i]->xinv_split_needed) ? 1 : 0;
     }
     e->d_bas = (BasinDev *)up(e->hb.data(), e->hb.size() * sizeof(BasinDev));
     e->d_wv = (Work *)up(wv.data(), wv.size() * sizeof(Work));
     e->d_wx = (Work *)up(wx.data(), wx.size() * sizeof(Work));
     e->d_wy = (Work *)up(wy.data(), wy.size() * sizeof(Work));
     e->d_wi = (Work *)up(wi.data(), wi.size() * sizeof(Work));
-    if (!e->d_bas || !e->d_wv || !e->d_wx || !e->d_wy || !e->d_wi) {
+    e->d_wa = (Work *)up(wa.data(), wa.size() * sizeof(Work));
+    if (!e->d_bas || !e->d_wv || !e->d_wx || !e->d_wy || !e->d_wi || !e->d_wa) {
         ens_free(e);
         return fail(OQG_ECUDA, "out of device memory");
     }
@@ -1794,8 +1840,8 @@ static int ens_member(oqg_ensemble *e, int member, oqg_handle **h) {
 static int ens_refresh(oqg_ensemble *e, int member) {
     const double tdt = e->hb[member].tdt_m;
     e->hb[member] = e->m[member]->hb;
-    e->hb[member].xinv_sep = 0;
-    e->hb[member].xinv_split = e->m[member]->xinv_split_needed ? 1 : 0;
+    e->hb[member].xinv_sep = e->sep ? 1 : 0;
+    e->hb[member].xinv_split = (e->sep || e->m[member]->xinv_split_needed) ? 1 : 0;
     e->hb[member].tdt_m = tdt;
     CK(cudaMemcpyAsync(e->d_bas + member, &e->hb[member], sizeof(BasinDev), cudaMemcpyHostToDevice, e->st));
     CK(cudaStreamSynchronize(e->st));
@@ -2315,8 +2361,10 @@ static int tune_setting(oqg_handle *h, double tdt, int nsteps, const std::vector
     cudaEventCreate(&e1);
     int rc = oqg_state_save(h, save);
     int best = -1;
-    float best_ms = -1.0f;
     ms.assign(cand.size(), -1.0f);
+    // three rounds over the candidates, the fastest time of each kept: one
+    // timing of a few steps varies by several percent from run to run
+    for (int round = 0; round < 3 && rc == OQG_OK; ++round)
     for (size_t ci = 0; ci < cand.size() && rc == OQG_OK; ++ci) {
         if ((rc = set(h, cand[ci]))) break;
         // warm up (captures the graphs), then time nsteps from the saved state
@@ -2329,9 +2377,11 @@ static int tune_setting(oqg_handle *h, double tdt, int nsteps, const std::vector
         if (cudaEventSynchronize(e1) != cudaSuccess) { rc = fail(OQG_ECUDA, "autotune timing failed"); break; }
         float t = 0.0f;
         cudaEventElapsedTime(&t, e0, e1);
-        ms[ci] = t / nsteps;
-        if (best_ms < 0.0f || t < best_ms) { best_ms = t; best = cand[ci]; }
+        if (ms[ci] < 0.0f || t / nsteps < ms[ci]) ms[ci] = t / nsteps;
     }
+    for (size_t ci = 0; ci < cand.size(); ++ci)
+        if (ms[ci] >= 0.0f && (best < 0 || ms[ci] < ms[best])) best = (int)ci;
+    if (best >= 0) best = cand[best];
     if (rc == OQG_OK && best >= 0) rc = set(h, best);
     if (rc == OQG_OK) rc = oqg_state_load(h, save);
     if (rc == OQG_OK && cudaStreamSynchronize(h->st) != cudaSuccess) rc = fail(OQG_ECUDA, "autotune restore failed");

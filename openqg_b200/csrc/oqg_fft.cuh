@@ -385,37 +385,49 @@ __host__ __device__ constexpr bool fft_inplace_len(int M) { return M == 2048 || 
 // In-place forward FFT of length M (fft_inplace_len) by groups of TT = M / 16
 // threads (t >= TT: barriers only); the input is in buf, the barrier after
 // its writes taken.
-template <class T>
+// MC > 0: the kernel is built for that one length, and only its plan is
+// compiled.
+template <class T, int MC = 0>
 __device__ __forceinline__ void fft_inplace(typename C2<T>::t *buf, int M, const typename C2<T>::t *__restrict__ tw,
                                             int t, int bar_id, int nbar) {
-    if (M == 2048) fft_ip_from<T, 2048, 128, 1>(buf, tw, t, t < 128, bar_id, nbar);
-    else if (M == 4096) fft_ip_from<T, 4096, 256, 1>(buf, tw, t, t < 256, bar_id, nbar);
+    if constexpr (MC == 2048 || MC == 4096) {
+        fft_ip_from<T, MC, MC / 16, 1>(buf, tw, t, t < MC / 16, bar_id, nbar);
+    } else if constexpr (MC == 0) {
+        if (M == 2048) fft_ip_from<T, 2048, 128, 1>(buf, tw, t, t < 128, bar_id, nbar);
+        else if (M == 4096) fft_ip_from<T, 4096, 256, 1>(buf, tw, t, t < 256, bar_id, nbar);
+    }
 }
 
 // Forward FFT of length M by groups of TT = M / E threads: the compile-time
 // stages for the lengths of the configurations' grids, the general stages
-// otherwise.  Same contract as fft_smem (t >= TT: barriers only).
+// otherwise.  Same contract as fft_smem (t >= TT: barriers only).  MC > 0:
+// the kernel is built for that one length (M == MC), and only its plan is
+// compiled, which keeps the kernel's code within the instruction cache.
 #define OQG_FFT_CT(MM)                                                                                      \
     case MM:                                                                                                \
         if constexpr ((MM) % E == 0) return fft_ct_from<T, MM, (MM) / E, 1>(a, b, tw, t, t < TT, bar_id, nbar); \
         break;
-template <class T, int E>
+template <class T, int E, int MC = 0>
 __device__ __forceinline__ typename C2<T>::t *fft_run(typename C2<T>::t *a, typename C2<T>::t *b, int M,
                                                       const int *rad, int nrad,
                                                       const typename C2<T>::t *__restrict__ tw, int t, int TT,
                                                       int bar_id, int nbar) {
-    switch (M) {
-        OQG_FFT_CT(128)
-        OQG_FFT_CT(192)
-        OQG_FFT_CT(256)
-        OQG_FFT_CT(384)
-        OQG_FFT_CT(512)
-        OQG_FFT_CT(1024)
-        OQG_FFT_CT(2048)
-        OQG_FFT_CT(4096)
-        default: break;
+    if constexpr (MC > 0 && MC % E == 0) {
+        return fft_ct_from<T, MC, MC / E, 1>(a, b, tw, t, t < TT, bar_id, nbar);
+    } else {
+        switch (M) {
+            OQG_FFT_CT(128)
+            OQG_FFT_CT(192)
+            OQG_FFT_CT(256)
+            OQG_FFT_CT(384)
+            OQG_FFT_CT(512)
+            OQG_FFT_CT(1024)
+            OQG_FFT_CT(2048)
+            OQG_FFT_CT(4096)
+            default: break;
+        }
+        return fft_smem<T>(a, b, M, rad, nrad, tw, t, TT, bar_id, nbar);
     }
-    return fft_smem<T>(a, b, M, rad, nrad, tw, t, TT, bar_id, nbar);
 }
 #undef OQG_FFT_CT
 

@@ -644,14 +644,16 @@ k_vort(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par,
 // expanded into the first.  The stage twiddles are read from global memory.
 __host__ __device__ __forceinline__ int round16(int bytes) { return (bytes + 15) & ~15; }
 
-template <class T, int E>
+// MC > 0: an instance for transforms of length MC only (the host picks it
+// for a basin of that length); MC = 0 serves any length (ensembles).
+template <class T, int E, int MC = 0>
 __global__ void __launch_bounds__(256, 2)
 k_xfwd(const BasinDev *__restrict__ bas, const Work *__restrict__ work, const void *rhs_override) {
     typedef typename C2<T>::t T2;
     const Work w = work[blockIdx.x];
     const BasinDev &b = bas[w.member];
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int M = b.M, TT = (M + E - 1) / E, G = blockDim.x / TT;
+    const int M = MC > 0 ? MC : b.M, TT = (M + E - 1) / E, G = blockDim.x / TT;
     const int g = threadIdx.x / TT, t = threadIdx.x - g * TT;
     const int LB = fft_buf_len(M);
     T2 *zs = reinterpret_cast<T2 *>(smem_raw);
@@ -710,8 +712,8 @@ k_xfwd(const BasinDev *__restrict__ bas, const Work *__restrict__ work, const vo
     }
     __syncthreads();
     T2 *z = za;
-    if (ip) fft_inplace<T>(za, M, (const T2 *)b.tw, live ? t : M, 0, 0);
-    else z = fft_run<T, E>(za, zb, M, b.rad, b.nrad, (const T2 *)b.tw, live ? t : TT, TT, 0, 0);
+    if (ip) fft_inplace<T, MC>(za, M, (const T2 *)b.tw, live ? t : M, 0, 0);
+    else z = fft_run<T, E, MC>(za, zb, M, b.rad, b.nrad, (const T2 *)b.tw, live ? t : TT, TT, 0, 0);
     if (!live) return;
     if (!b.cyclic) {
         T *S = (T *)b.spec;
@@ -1277,21 +1279,23 @@ __device__ __noinline__ void scalar_phase(const BasinDev &b, double tdt, int par
 // scaled by ftnorm (inhomog.F90:200-211); the modal row j + 1 of mode m gets
 // the n interior values and zeros on both walls, and the first and last row
 // pairs of a mode clear the wall rows 0 and nyp - 1 (into out instead of
-// inh_g when out != null: the solve-only mode).  scal != 0: one CTA
-// more, after the transforms', runs the step's scalar phase once into
-// b.scal_g (the assembly CTAs read it there) and writes the next state.
-// G: transforms per CTA (the forward launch's), blockDim >= G TT rounded up
-// to whole warps so the scalar CTA has a full warp.
-template <class T, int NL, int E>
+// inh_g when out != null: the solve-only mode).  A scalar CTA after the
+// transforms' runs a basin's scalar phase once into b.scal_g (the assembly
+// reads it there) and writes the basin's next scalar state.
+// G: transforms per CTA (the forward launch's; <= 0: blockDim / TT, per
+// member of an ensemble), blockDim >= G TT rounded up to whole warps so the
+// scalar CTAs have a full warp.  scal: the last scal CTAs run the scalar
+// phase of member 0, 1, ... (0: none).
+template <class T, int NL, int E, int MC = 0>
 __global__ void __launch_bounds__(256, 2)
 k_xinv_rows(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int G, int scal, int par,
             double tdt, T *out) {
     typedef typename C2<T>::t T2;
-    if (scal && blockIdx.x == gridDim.x - 1) {
+    if (scal > 0 && (int)blockIdx.x >= (int)gridDim.x - scal) {
         pdl_trigger();
         pdl_wait();
         if (threadIdx.x < 32) {
-            const BasinDev &b = bas[0];
+            const BasinDev &b = bas[blockIdx.x - (gridDim.x - scal)];
             scalar_phase<T, NL>(b, tdt != 0.0 ? tdt : b.tdt_m, par, true, (XinvScal *)b.scal_g);
         }
         return;
@@ -1299,7 +1303,8 @@ k_xinv_rows(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int
     const Work w = work[blockIdx.x];
     const BasinDev &b = bas[w.member];
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int M = b.M, TT = (M + E - 1) / E;
+    const int M = MC > 0 ? MC : b.M, TT = (M + E - 1) / E;
+    if (G <= 0) G = blockDim.x / TT;            // an ensemble: per member, as k_xfwd
     const int g = threadIdx.x / TT, t = threadIdx.x - g * TT;
     const int LB = fft_buf_len(M);
     T2 *zs = reinterpret_cast<T2 *>(smem_raw);
@@ -1349,8 +1354,8 @@ k_xinv_rows(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int
     }
     __syncthreads();
     T2 *z = za;
-    if (ip) fft_inplace<T>(za, M, (const T2 *)b.tw, live ? t : M, 0, 0);
-    else z = fft_run<T, E>(za, zb, M, b.rad, b.nrad, (const T2 *)b.tw, live ? t : TT, TT, 0, 0);
+    if (ip) fft_inplace<T, MC>(za, M, (const T2 *)b.tw, live ? t : M, 0, 0);
+    else z = fft_run<T, E, MC>(za, zb, M, b.rad, b.nrad, (const T2 *)b.tw, live ? t : TT, TT, 0, 0);
     if (!live) return;
     T *ox = inh + ((size_t)m * b.nyp + j + 1) * px;
     T *oy = ox + px;
@@ -1680,11 +1685,14 @@ k_xinv(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par,
 }
 
 // ------------------------------------------------------------------ k_xinv_asm
+#define XASM_POINTS 256     // points of one assembly work item (one per thread)
 // The assembly of a box whose inverse transforms ran as k_xinv_rows: the
 // homogeneous correction and modes_to_layers (modes.F90:268-284) of every
 // point from the modal rows in b.inh_g, ocqbdy (vorsubs.F90:58-114) on the
 // walls and the suppress_comp_mode averages (driver.F90:174-189), with the
-// step's scalars from b.scal_g.  One thread per point; a wall point also
+// step's scalars from b.scal_g.  Each work item is XASM_POINTS consecutive
+// points of one basin (the work list spans an ensemble's members); one
+// thread per point; a wall point also
 // forms the layer values of its inner neighbour (the same arithmetic as the
 // neighbour's own thread), so no point waits for another.
 template <class T, int NL>
@@ -1707,8 +1715,9 @@ __device__ __forceinline__ void xinv_layers(const BasinDev &b, const T *__restri
 
 template <class T, int NL>
 __global__ void __launch_bounds__(256)
-k_xinv_asm(const BasinDev *__restrict__ bas, int par) {
-    const BasinDev &b = bas[0];
+k_xinv_asm(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par) {
+    const Work w = work[blockIdx.x];
+    const BasinDev &b = bas[w.member];
     __shared__ double sCtm[NL * NL], sAmat[NL * NL], sHc[NL > 1 ? NL - 1 : 1];
     __shared__ int sSupp;
     pdl_trigger();
@@ -1738,7 +1747,9 @@ k_xinv_asm(const BasinDev *__restrict__ bas, int par) {
     const T fac = (T)b.qb_fac;
     const FastDiv fdx(nxp);
     const int npts = nxp * nyp;
-    for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < npts; idx += gridDim.x * blockDim.x) {
+    const int first = w.block * XASM_POINTS;
+    const int last = min(first + XASM_POINTS, npts);
+    for (int idx = first + threadIdx.x; idx < last; idx += blockDim.x) {
         const int j = fdx.div(idx), i = idx - j * nxp;
         const size_t o2 = (size_t)j * px + i;
         T pn[NL];
