@@ -671,6 +671,9 @@ def measure_basin(workload, prec, steps, warmup, msteps, flush, rank, pg, seed=N
         tile_rows, tune_ms = g.autotune(tdt, 20)
     if PINNED.get("xinv_sep") is not None and not b.cyclic:
         g.set_xinv_sep(PINNED["xinv_sep"])
+        xsep, xtune_ms = bool(PINNED["xinv_sep"]), {}
+    else:
+        xsep, xtune_ms = g.autotune_xinv(tdt, 20)
     if PINNED.get("ysolve_warps"):
         g.set_ysolve_warps(PINNED["ysolve_warps"])
         ywarps, ytune_ms = PINNED["ysolve_warps"], {}
@@ -690,6 +693,9 @@ def measure_basin(workload, prec, steps, warmup, msteps, flush, rank, pg, seed=N
         "ms_per_model_step": total_ms / (steps * msteps), "cells": cells,
         "tile_rows": tile_rows, "autotune_ms_per_step": {str(k): round(v, 5) for k, v in tune_ms.items()},
         "ysolve_warps": ywarps, "ysolve_autotune_ms_per_step": {str(k): round(v, 5) for k, v in ytune_ms.items()},
+        "xinv_two_launches": xsep,
+        "xinv_autotune_ms_per_step": {("two launches" if k else "one kernel"): round(v, 5)
+                                      for k, v in xtune_ms.items()},
     }
 
 
@@ -705,7 +711,8 @@ def config_line(workload, prec, steps, warmup, msteps, flush, rank, ws, pg, note
             "model_steps_per_step": msteps, "steps": steps,
             "value": replica_value(m["total_ms"], ws, m["cells"], msteps, steps),
             "unit": "Mcell-layer-steps/s", "ms_per_model_step": m["ms_per_model_step"],
-            "tile_rows": m["tile_rows"], "ysolve_warps": m["ysolve_warps"], "roofline": roof,
+            "tile_rows": m["tile_rows"], "ysolve_warps": m["ysolve_warps"],
+            "xinv_two_launches": m["xinv_two_launches"], "roofline": roof,
             "l2": "flushed (256 MiB write) before every timed step of %d model steps" % msteps}
 
 
@@ -856,6 +863,8 @@ def run_ours(args):
                    "autotune_ms_per_step": m["autotune_ms_per_step"],
                    "ysolve_warps": m["ysolve_warps"],
                    "ysolve_autotune_ms_per_step": m["ysolve_autotune_ms_per_step"],
+                   "xinv_two_launches": m["xinv_two_launches"],
+                   "xinv_autotune_ms_per_step": m["xinv_autotune_ms_per_step"],
                    "l2": "flushed (256 MiB write) before every timed step of %d model steps" % msteps,
                    "parallelism": "replicas" if ws > 1 else "single basin"},
         "roofline": roof,

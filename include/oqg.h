@@ -323,6 +323,11 @@ int oqg_set_ysolve_warps(oqg_handle *h, int warps);
  * more: OQG_EUNSUPPORTED); channels: OQG_EUNSUPPORTED. */
 int oqg_set_xinv_sep(oqg_handle *h, int on);
 int oqg_get_xinv_sep(oqg_handle *h, int *on);
+/* Measures the box's two forms of the inverse transform and assembly (one
+ * kernel, or two launches) like oqg_autotune and keeps the faster; ms[0]:
+ * one kernel, ms[1]: two launches (ms per step; -1 where a form is not
+ * available: channels and wide boxes keep theirs and return at once). */
+int oqg_autotune_xinv(oqg_handle *h, double tdt, int nsteps, int *best_sep, double *ms);
 
 /* ---------------------------------------------------------------------
  * Ensembles: many independent basins of uneven size stepped together by one

@@ -117,6 +117,8 @@ def lib():
     L.oqg_set_ysolve_warps.argtypes = [vp, ctypes.c_int]
     L.oqg_set_xinv_sep.argtypes = [vp, ctypes.c_int]
     L.oqg_get_xinv_sep.argtypes = [vp, ctypes.POINTER(ctypes.c_int)]
+    L.oqg_autotune_xinv.argtypes = [vp, ctypes.c_double, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                    ctypes.POINTER(ctypes.c_double)]
     L.oqg_adj_segment.argtypes = [vp, vp, vp, ctypes.c_size_t, ctypes.c_int, ctypes.c_double, ctypes.c_longlong]
     _lib = L
     return L
@@ -354,6 +356,16 @@ class QG:
         """Closed boxes: the inverse transforms as a launch of their own and a
         one-pass assembly (on), or one kernel for both (off)."""
         _check(lib().oqg_set_xinv_sep(self.h, 1 if on else 0), "oqg_set_xinv_sep")
+
+    def autotune_xinv(self, tdt: float, nsteps: int = 20):
+        """Closed boxes below 1025 points: measures the inverse transform and
+        assembly as one kernel and as two launches and keeps the faster;
+        returns (two_launches, {False: ms, True: ms}) for the forms measured."""
+        best = ctypes.c_int()
+        ms = (ctypes.c_double * 2)()
+        _check(lib().oqg_autotune_xinv(self.h, float(tdt), int(nsteps), ctypes.byref(best), ms),
+               "oqg_autotune_xinv")
+        return bool(best.value), {bool(i): ms[i] for i in range(2) if ms[i] >= 0}
 
     def xinv_sep(self) -> bool:
         v = ctypes.c_int()

@@ -173,6 +173,11 @@ static int ysolve_warps(int ny, long long ncols) {
 #define OQG_XLENS(X) X(256) X(512) X(1024) X(2048) X(4096)
 template <class T, int E>
 static void (*xfwd_kernel(int M))(const BasinDev *, const Work *, const void *) {
+    // FP32 storage keeps the any-length instances: at 513^2 the step measured
+    // 44.5 us with them against 48.1 us with the per-length ones (which take
+    // 80 registers instead of 128); FP64 measured 51.0 against 53.8 us the
+    // other way round
+    if (std::is_same<T, float>::value) M = 0;
     switch (M) {
 #define OQG_XF(MM) case MM: return k_xfwd<T, E, MM>;
         OQG_XLENS(OQG_XF)
@@ -182,6 +187,7 @@ static void (*xfwd_kernel(int M))(const BasinDev *, const Work *, const void *) 
 }
 template <class T, int NL, int E>
 static void (*xinv_rows_kernel(int M))(const BasinDev *, const Work *, int, int, int, double, T *) {
+    if (std::is_same<T, float>::value) M = 0;      // as xfwd_kernel
     switch (M) {
 #define OQG_XI(MM) case MM: return k_xinv_rows<T, NL, E, MM>;
         OQG_XLENS(OQG_XI)
@@ -980,7 +986,10 @@ static int create_impl(const oqg_params *prm, oqg_handle **out, bool batched) {
     h->smem_i_full = xinv_smem(b.M, b.nl, nra, b.nxp, nfft_i, h->esz, split);
     h->smem_i64_full = xinv_smem(b.M, b.nl, nra, b.nxp, nfft_i, 8, split);
     h->xinv_split_needed = split;
-    h->na = (b.nxp * b.nyp + XASM_POINTS - 1) / XASM_POINTS;
+    // one point per thread, at most 8 work items of 256 threads per SM (the
+    // items stride over larger grids)
+    b.asm_items = std::min((b.nxp * b.nyp + 255) / 256, 148 * 8);
+    h->na = b.asm_items;
     // boxes: the inverse transforms run as a launch of their own, shaped like
     // the forward one, then a one-pass assembly (oqg_set_xinv_sep; faster at
     // 513^2 and the only form once the modal rows leave shared memory)
@@ -1777,7 +1786,7 @@ int oqg_ensemble_create(const oqg_params *members, int nmembers, oqg_ensemble **
         for (int k = 0; k < nxb; ++k) wx.push_back(Work{i, k});
         for (int k = 0; k < nyb; ++k) wy.push_back(Work{i, k});
         for (int k = 0; k < nib; ++k) wi.push_back(Work{i, k});
-        for (int k = 0; k < (b.nxp * b.nyp + XASM_POINTS - 1) / XASM_POINTS; ++k) wa.push_back(Work{i, k});
+        for (int k = 0; k < (b.nxp * b.nyp + XASM_ENS_POINTS - 1) / XASM_ENS_POINTS; ++k) wa.push_back(Work{i, k});
         const int nra = (b.ny > b.k4_rows) ? b.k4_rows + 1 : b.ny + 2;
         e->smem_v = std::max(e->smem_v, vort_smem_bytes(b.vty, (int)esz));
         const size_t xrow = (size_t)((b.nxin + 3) & ~3);
@@ -1805,6 +1814,7 @@ int oqg_ensemble_create(const oqg_params *members, int nmembers, oqg_ensemble **
         e->hb[i] = e->m[i]->hb;
         e->hb[i].xinv_sep = e->sep ? 1 : 0;
         e->hb[i].xinv_split = (e->sep || e->m[i]->xinv_split_needed) ? 1 : 0;
+        e->hb[i].asm_items = (e->hb[i].nxp * e->hb[i].nyp + XASM_ENS_POINTS - 1) / XASM_ENS_POINTS;
     }
     e->d_bas = (BasinDev *)up(e->hb.data(), e->hb.size() * sizeof(BasinDev));
     e->d_wv = (Work *)up(wv.data(), wv.size() * sizeof(Work));
@@ -1842,6 +1852,7 @@ static int ens_refresh(oqg_ensemble *e, int member) {
     e->hb[member] = e->m[member]->hb;
     e->hb[member].xinv_sep = e->sep ? 1 : 0;
     e->hb[member].xinv_split = (e->sep || e->m[member]->xinv_split_needed) ? 1 : 0;
+    e->hb[member].asm_items = (e->hb[member].nxp * e->hb[member].nyp + XASM_ENS_POINTS - 1) / XASM_ENS_POINTS;
     e->hb[member].tdt_m = tdt;
     CK(cudaMemcpyAsync(e->d_bas + member, &e->hb[member], sizeof(BasinDev), cudaMemcpyHostToDevice, e->st));
     CK(cudaStreamSynchronize(e->st));
@@ -2431,6 +2442,30 @@ int oqg_set_xinv_sep(oqg_handle *h, int on) {
 int oqg_get_xinv_sep(oqg_handle *h, int *on) {
     if (!h || !on) return fail(OQG_EINVAL, "bad argument");
     *on = h->hb.xinv_sep;
+    return OQG_OK;
+}
+
+int oqg_autotune_xinv(oqg_handle *h, double tdt, int nsteps, int *best_sep, double *ms) {
+    if (!h || nsteps < 2 || !(tdt > 0.0)) return fail(OQG_EINVAL, "bad argument");
+    if (ms) ms[0] = ms[1] = -1.0;
+    // channels have the one-kernel form only, wide boxes the two-launch one
+    if (h->hb.cyclic || h->xinv_split_needed) {
+        if (best_sep) *best_sep = h->hb.xinv_sep;
+        return OQG_OK;
+    }
+    auto set = [](oqg_handle *hh, int on) {
+        apply_xinv_sep(hh, on != 0);
+        set_attrs(hh);
+        drop_graphs(hh);
+        return push_desc(hh);
+    };
+    const std::vector<int> cand = {1, 0};
+    std::vector<float> t;
+    int best = h->hb.xinv_sep;
+    const int rc = tune_setting(h, tdt, nsteps, cand, set, &best, t);
+    if (rc) return rc;
+    if (ms) { ms[1] = t[0]; ms[0] = t[1]; }
+    if (best_sep) *best_sep = best;
     return OQG_OK;
 }
 

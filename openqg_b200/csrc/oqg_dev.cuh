@@ -106,6 +106,8 @@ struct BasinDev {
     int xinv_sep;               // the inverse transforms run as k_xinv_rows and the
                                 // assembly as k_xinv_asm (boxes; always when wide)
     int xinv_split;             // k_xinv keeps its modal rows in inh_g
+    int asm_items;              // k_xinv_asm work items of this basin (256-point runs
+                                // interleaved over them)
     void *scal_g;               // with xinv_sep: the step's scalar phase results,
                                 // written once per step by k_xinv_rows
     double tdt_m;               // leapfrog step of this member when a launch

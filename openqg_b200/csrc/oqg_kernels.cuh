@@ -1685,14 +1685,14 @@ k_xinv(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par,
 }
 
 // ------------------------------------------------------------------ k_xinv_asm
-#define XASM_POINTS 256     // points of one assembly work item (one per thread)
+#define XASM_ENS_POINTS 1024   // points per assembly work item of an ensemble's member
 // The assembly of a box whose inverse transforms ran as k_xinv_rows: the
 // homogeneous correction and modes_to_layers (modes.F90:268-284) of every
 // point from the modal rows in b.inh_g, ocqbdy (vorsubs.F90:58-114) on the
 // walls and the suppress_comp_mode averages (driver.F90:174-189), with the
-// step's scalars from b.scal_g.  Each work item is XASM_POINTS consecutive
-// points of one basin (the work list spans an ensemble's members); one
-// thread per point; a wall point also
+// step's scalars from b.scal_g.  The work items of a basin (the work list
+// spans an ensemble's members) take interleaved runs of 256 points, one
+// point per thread in each; a wall point also
 // forms the layer values of its inner neighbour (the same arithmetic as the
 // neighbour's own thread), so no point waits for another.
 template <class T, int NL>
@@ -1747,9 +1747,10 @@ k_xinv_asm(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int 
     const T fac = (T)b.qb_fac;
     const FastDiv fdx(nxp);
     const int npts = nxp * nyp;
-    const int first = w.block * XASM_POINTS;
-    const int last = min(first + XASM_POINTS, npts);
-    for (int idx = first + threadIdx.x; idx < last; idx += blockDim.x) {
+    // the basin's b.asm_items work items interleave: item w.block takes the
+    // points w.block * 256 + t, then every b.asm_items * 256 further
+    const int stride = b.asm_items * 256;
+    for (int idx = w.block * 256 + threadIdx.x; idx < npts; idx += stride) {
         const int j = fdx.div(idx), i = idx - j * nxp;
         const size_t o2 = (size_t)j * px + i;
         T pn[NL];

@@ -104,3 +104,25 @@ def test_fixed_settings_are_kept_and_checked():
         assert rel_l2(a, r) <= 1e-12
     for x in (g, ref):
         x.close()
+
+
+def test_inverse_form_tuning_keeps_state_and_results():
+    """A box below 1025 points: the tuner times the one-kernel and the
+    two-launch inverse, keeps the faster, leaves the state as found, and
+    steps match the default form's to rounding."""
+    b = ocean_double_gyre(129)
+    g, ref = _handle(b), _handle(b)
+    g.step(3600.0, 2)
+    ref.step(3600.0, 2)
+    before = g.get_state()
+    best, ms = g.autotune_xinv(3600.0, 4)
+    assert g.xinv_sep() == best
+    assert sorted(ms) == [False, True] and all(v > 0 for v in ms.values())
+    for a, r in zip(g.get_state(), before):
+        assert np.array_equal(a, r)
+    g.step(3600.0, 5)
+    ref.step(3600.0, 5)
+    for a, r in zip(g.get_state(), ref.get_state()):
+        assert rel_l2(a, r) <= 1e-12
+    for x in (g, ref):
+        x.close()
