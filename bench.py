@@ -314,6 +314,14 @@ def coupled_config(nrep=3, nocean=10, nstr=10, precision=None):
     coupled_step()
     go.sync()
     ga.sync()
+    # each basin's tunable settings, measured on its own steps after the
+    # first coupled step set its forcing (the states are restored)
+    tuned = {}
+    for name, g, tdt_g in (("ocean", go, 3600.0), ("atmosphere", ga, 360.0)):
+        rows, _ = g.autotune(tdt_g, 10)
+        yw, _ = g.autotune_ysolve(tdt_g, 10)
+        xs, _ = g.autotune_xinv(tdt_g, 10)
+        tuned[name] = {"tile_rows": rows, "ysolve_warps": yw, "xinv_two_launches": xs}
     times = []
     for _ in range(nrep):
         t0 = time.perf_counter()
@@ -336,6 +344,7 @@ def coupled_config(nrep=3, nocean=10, nstr=10, precision=None):
                         "nothing from the host in the loop" % nstr,
             "state_storage": "fp32" if prec != OQG_FP64 else "fp64",
             "ms_per_coupled_ocean_step": ms, "value": cells / (ms / 1e3) / 1e6, "unit": "Mcell-layer-steps/s",
+            "tuned": tuned,
             "timer": "host clock, median of %d runs of %d coupled ocean steps" % (nrep, nocean)}
 
 
@@ -669,7 +678,7 @@ def measure_basin(workload, prec, steps, warmup, msteps, flush, rank, pg, seed=N
         tile_rows, tune_ms = PINNED["tile_rows"], {}
     else:
         tile_rows, tune_ms = g.autotune(tdt, 20)
-    if PINNED.get("xinv_sep") is not None and not b.cyclic:
+    if PINNED.get("xinv_sep") is not None:
         g.set_xinv_sep(PINNED["xinv_sep"])
         xsep, xtune_ms = bool(PINNED["xinv_sep"]), {}
     else:
@@ -914,8 +923,8 @@ def main():
     ap.add_argument("--tile-rows", type=int, default=0, choices=[0, 8, 12, 16],
                     help="fix the vorticity tile height instead of measuring it")
     ap.add_argument("--xinv-sep", type=int, default=None, choices=[0, 1],
-                    help="closed boxes: the inverse transforms as a launch of their own (1) or inside "
-                         "the assembly kernel (0); default: the library's choice")
+                    help="the inverse transforms as a launch of their own (1) or inside the assembly "
+                         "kernel (0); default: measured")
     ap.add_argument("--ysolve-warps", type=int, default=0, choices=[0, 1, 2, 4],
                     help="fix the y-solve's warps per column instead of measuring them")
     ap.add_argument("--adjoint-only", action="store_true",

@@ -277,9 +277,9 @@ int oqg_profile_phases(oqg_handle *h, double tdt, int nsteps, double *ms);
 int oqg_stream(oqg_handle *h, void **stream);
 
 /* Kernel launches of one model step: 5 for a closed box (vorticity, forward
- * transform, y-solve, inverse transform, assembly), 4 for a channel or a box
- * after oqg_set_xinv_sep(h, 0) (the inverse transform and the assembly in
- * one kernel). */
+ * transform, y-solve, inverse transform, assembly), 4 with the inverse
+ * transform and the assembly in one kernel (a channel's default, or after
+ * oqg_set_xinv_sep(h, 0)). */
 int oqg_step_launches(oqg_handle *h, int *launches);
 
 /* The launch floor of the step chain: nsteps steps of launches with the
@@ -315,18 +315,18 @@ int oqg_get_ysolve_warps(oqg_handle *h, int *warps);
  * on the same GPU; OQG_EINVAL for other values. */
 int oqg_set_vty(oqg_handle *h, int vty);
 int oqg_set_ysolve_warps(oqg_handle *h, int warps);
-/* Closed boxes: the inverse transforms as a launch shaped like the forward
+/* The inverse transforms as a launch shaped like the forward
  * one (k_xinv_rows, which also runs the step's scalar phase once) and a
  * one-pass assembly (k_xinv_asm), instead of one kernel that transforms and
- * assembles in shared memory.  On by default for boxes; it cannot be turned
- * off where the modal rows do not fit in shared memory (1025 points wide and
- * more: OQG_EUNSUPPORTED); channels: OQG_EUNSUPPORTED. */
+ * assembles in shared memory.  On by default for boxes, off for channels;
+ * it cannot be turned off where the modal rows do not fit in shared memory
+ * (1025 points wide and more: OQG_EUNSUPPORTED). */
 int oqg_set_xinv_sep(oqg_handle *h, int on);
 int oqg_get_xinv_sep(oqg_handle *h, int *on);
-/* Measures the box's two forms of the inverse transform and assembly (one
- * kernel, or two launches) like oqg_autotune and keeps the faster; ms[0]:
- * one kernel, ms[1]: two launches (ms per step; -1 where a form is not
- * available: channels and wide boxes keep theirs and return at once). */
+/* Measures the two forms of the inverse transform and assembly (one kernel,
+ * or two launches) like oqg_autotune and keeps the faster; ms[0]: one
+ * kernel, ms[1]: two launches (ms per step; -1 where a form is not
+ * available: wide grids keep the two launches and return at once). */
 int oqg_autotune_xinv(oqg_handle *h, double tdt, int nsteps, int *best_sep, double *ms);
 
 /* ---------------------------------------------------------------------

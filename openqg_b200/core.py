@@ -353,12 +353,12 @@ class QG:
         _check(lib().oqg_set_ysolve_warps(self.h, int(warps)), "oqg_set_ysolve_warps")
 
     def set_xinv_sep(self, on: bool):
-        """Closed boxes: the inverse transforms as a launch of their own and a
-        one-pass assembly (on), or one kernel for both (off)."""
+        """The inverse transforms as a launch of their own and a one-pass
+        assembly (on), or one kernel for both (off)."""
         _check(lib().oqg_set_xinv_sep(self.h, 1 if on else 0), "oqg_set_xinv_sep")
 
     def autotune_xinv(self, tdt: float, nsteps: int = 20):
-        """Closed boxes below 1025 points: measures the inverse transform and
+        """Grids below 1025 points: measures the inverse transform and
         assembly as one kernel and as two launches and keeps the faster;
         returns (two_launches, {False: ms, True: ms}) for the forms measured."""
         best = ctypes.c_int()

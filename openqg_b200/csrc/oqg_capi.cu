@@ -971,17 +971,11 @@ static int create_impl(const oqg_params *prm, oqg_handle **out, bool batched) {
         nfft_i = std::min(XINV_FFT_MAX, rup(G * tt, 32));
         if ((nfft_i / tt) * per > 227 * 1024) nfft_i = rup(tt, 32);
     }
-    // a box keeps the buffers of the separate inverse transforms (the modal
-    // rows in global memory, the step's scalars) at any width
-    if (split || !b.cyclic) {
-        b.inh_g = dalloc<char>(h, (size_t)b.nl * b.nyp * b.px * 8);
-        if (!b.inh_g) return bail(OQG_ECUDA, "out of device memory");
-    }
-    b.scal_g = nullptr;
-    if (!b.cyclic) {
-        b.scal_g = dalloc<char>(h, sizeof(XinvScal));
-        if (!b.scal_g) return bail(OQG_ECUDA, "out of device memory");
-    }
+    // the buffers of the separate inverse transforms (the modal rows in
+    // global memory, the step's scalars), kept at any width
+    b.inh_g = dalloc<char>(h, (size_t)b.nl * b.nyp * b.px * 8);
+    b.scal_g = dalloc<char>(h, sizeof(XinvScal));
+    if (!b.inh_g || !b.scal_g) return bail(OQG_ECUDA, "out of device memory");
     h->xi_threads = nfft_i + 32;
     h->smem_i_full = xinv_smem(b.M, b.nl, nra, b.nxp, nfft_i, h->esz, split);
     h->smem_i64_full = xinv_smem(b.M, b.nl, nra, b.nxp, nfft_i, 8, split);
@@ -992,8 +986,9 @@ static int create_impl(const oqg_params *prm, oqg_handle **out, bool batched) {
     h->na = b.asm_items;
     // boxes: the inverse transforms run as a launch of their own, shaped like
     // the forward one, then a one-pass assembly (oqg_set_xinv_sep; faster at
-    // 513^2 and the only form once the modal rows leave shared memory)
-    apply_xinv_sep(h, !b.cyclic);
+    // 513^2 and the only form once the modal rows leave shared memory);
+    // channels start with the one-kernel form (oqg_autotune_xinv measures both)
+    apply_xinv_sep(h, !b.cyclic || split);
     if (h->smem_i64_full > 227 * 1024 || h->smem_x64 > 227 * 1024 || h->smem_y > 227 * 1024)
         return bail(OQG_EUNSUPPORTED, "grid too large for this build's shared-memory tiling");
     std::vector<Work> wv(h->nv), wx(h->nx), wy(h->nys), wi(h->ni), wa(h->na);
@@ -2427,7 +2422,6 @@ int oqg_autotune(oqg_handle *h, double tdt, int nsteps, int *best_vty, double *m
 
 int oqg_set_xinv_sep(oqg_handle *h, int on) {
     if (!h) return fail(OQG_EINVAL, "bad argument");
-    if (h->hb.cyclic) return fail(OQG_EUNSUPPORTED, "the separate inverse transforms are built for the closed box");
     if (!on && h->xinv_split_needed)
         return fail(OQG_EUNSUPPORTED, "this width keeps its modal rows in global memory: the transforms run separately");
     apply_xinv_sep(h, on != 0);
@@ -2448,8 +2442,8 @@ int oqg_get_xinv_sep(oqg_handle *h, int *on) {
 int oqg_autotune_xinv(oqg_handle *h, double tdt, int nsteps, int *best_sep, double *ms) {
     if (!h || nsteps < 2 || !(tdt > 0.0)) return fail(OQG_EINVAL, "bad argument");
     if (ms) ms[0] = ms[1] = -1.0;
-    // channels have the one-kernel form only, wide boxes the two-launch one
-    if (h->hb.cyclic || h->xinv_split_needed) {
+    // grids whose modal rows leave shared memory have the two-launch form only
+    if (h->xinv_split_needed) {
         if (best_sep) *best_sep = h->hb.xinv_sep;
         return OQG_OK;
     }

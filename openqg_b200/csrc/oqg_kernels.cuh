@@ -1272,12 +1272,14 @@ __device__ __noinline__ void scalar_phase(const BasinDev &b, double tdt, int par
 }
 
 // ------------------------------------------------------------------ k_xinv_rows
-// Wide boxes (modal rows in the global buffer b.inh_g): the inverse DST-I of
-// the y-solved spectral rows as a launch of its own, shaped like k_xfwd (one
-// row pair per group, the 2048- and 4096-point lengths in place, two CTAs
-// per SM), so k_xinv only assembles.  The inverse is the forward transform
-// scaled by ftnorm (inhomog.F90:200-211); the modal row j + 1 of mode m gets
-// the n interior values and zeros on both walls, and the first and last row
+// The inverse x-transforms of the y-solved spectral rows as a launch of
+// their own, shaped like k_xfwd (one row pair per group, the 2048- and
+// 4096-point box lengths in place), into the modal rows b.inh_g, which
+// k_xinv_asm assembles.  A box's inverse DST-I is the forward transform
+// scaled by ftnorm (inhomog.F90:200-211): the modal row j + 1 of mode m gets
+// the n interior values and zeros on both walls.  A channel's c2r
+// (inhomog.F90:214-255) fills every column, the last repeating the first.
+// The first and last row
 // pairs of a mode clear the wall rows 0 and nyp - 1 (into out instead of
 // inh_g when out != null: the solve-only mode).  A scalar CTA after the
 // transforms' runs a basin's scalar phase once into b.scal_g (the assembly
@@ -1315,13 +1317,18 @@ k_xinv_rows(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int
     const int j = live ? 2 * (pair - m * npm) : 0;
     const bool two = live && (j + 1 < b.ny);
     const int n = b.nxin, nxp = b.nxp, px = b.px;
-    const int RO = (n + 3) & ~3;              // offset of the second row (16-byte aligned)
-    const bool ip = E == 16 && fft_inplace_len(M);
+    // a spectral row: n reals (box) or nk complex values (channel); a channel
+    // transforms through the ping-pong pair, whose second buffer holds both
+    const bool cyc = b.cyclic != 0;
+    const int rowbytes = cyc ? b.nk * (int)sizeof(T2) : n * (int)sizeof(T);
+    const int RO = round16(rowbytes) / (int)sizeof(T);   // offset of the second row (16-byte aligned)
+    const bool ip = E == 16 && !cyc && fft_inplace_len(M);
     T2 *za = zs + (size_t)(g < G ? g : 0) * (ip ? LB : 2 * LB);
     T2 *zb = za + LB;
     T *raw = ip ? reinterpret_cast<T *>(zs + (size_t)G * LB) + (size_t)(g < G ? g : 0) * 2 * RO
                 : reinterpret_cast<T *>(zb);
-    const T *x = (const T *)b.spec + ((size_t)m * b.ny + j) * b.pk;
+    const size_t pitchb = (size_t)b.pk * (cyc ? sizeof(T2) : sizeof(T));
+    const char *x = (const char *)b.spec + ((size_t)m * b.ny + j) * pitchb;
     // out != null: solve-only mode, the modal solutions go straight to out
     // ([nl][nyp][px], the same layout)
     T *inh = out ? out : (T *)b.inh_g;
@@ -1329,12 +1336,29 @@ k_xinv_rows(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int
     pdl_trigger();
     pdl_wait();
     if (live) {
-        cp_async_16(raw, x, round16(n * (int)sizeof(T)), t, TT);
-        if (two) cp_async_16(raw + RO, x + b.pk, round16(n * (int)sizeof(T)), t, TT);
+        cp_async_16(raw, x, round16(rowbytes), t, TT);
+        if (two) cp_async_16(raw + RO, x + pitchb, round16(rowbytes), t, TT);
     }
     cp_async_commit_wait_all();
     __syncthreads();
-    if (live) {
+    if (live && cyc) {
+        // c2r by one complex transform of two rows: the Hermitian extension
+        // of X + iY, conjugated (inhomog.F90:214-255)
+        const T2 *xr = reinterpret_cast<const T2 *>(raw), *yr = reinterpret_cast<const T2 *>(raw + RO);
+        for (int kk = t; kk < M; kk += TT) {
+            T2 X, Y;
+            const bool lo = kk <= M / 2;
+            const int ks = lo ? kk : M - kk;
+            X = xr[ks];
+            if (two) Y = yr[ks]; else { Y.x = (T)0; Y.y = (T)0; }
+            if (!lo) { X.y = -X.y; Y.y = -Y.y; }
+            if (kk == 0 || 2 * kk == M) { X.y = (T)0; Y.y = (T)0; }
+            T2 v;
+            v.x = ftn * X.x - ftn * Y.y;
+            v.y = -(ftn * X.y + ftn * Y.x);
+            za[fpad(kk)] = v;
+        }
+    } else if (live) {
         if (t == 0) {
             T2 zero;
             zero.x = (T)0;
@@ -1359,17 +1383,31 @@ k_xinv_rows(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int
     if (!live) return;
     T *ox = inh + ((size_t)m * b.nyp + j + 1) * px;
     T *oy = ox + px;
-    for (int kk = t; kk < n; kk += TT) {
-        const T2 v = z[fpad(kk + 1)];
-        ox[kk + 1] = -v.y;
-        if (two) oy[kk + 1] = v.x;
+    if (cyc) {
+        // every column; column nxp-1 = M repeats column 0 (inhomog.F90:250)
+        for (int i = t; i < M; i += TT) {
+            const T2 v = z[fpad(i)];
+            ox[i] = v.x;
+            if (two) oy[i] = -v.y;
+        }
+        if (t == 0) {
+            const T2 v = z[fpad(0)];
+            ox[M] = v.x;
+            if (two) oy[M] = -v.y;
+        }
+    } else {
+        for (int kk = t; kk < n; kk += TT) {
+            const T2 v = z[fpad(kk + 1)];
+            ox[kk + 1] = -v.y;
+            if (two) oy[kk + 1] = v.x;
+        }
     }
-    if (t == 0) {
+    if (t == 0 && !cyc) {
         ox[0] = (T)0;
         ox[nxp - 1] = (T)0;
         if (two) { oy[0] = (T)0; oy[nxp - 1] = (T)0; }
     }
-    // the wall rows
+    // the wall rows (zonal walls of either geometry)
     T *wrow = nullptr;
     if (j == 0) wrow = inh + (size_t)m * b.nyp * px;
     if (j + 2 >= b.ny) {
@@ -1686,7 +1724,7 @@ k_xinv(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par,
 
 // ------------------------------------------------------------------ k_xinv_asm
 #define XASM_ENS_POINTS 1024   // points per assembly work item of an ensemble's member
-// The assembly of a box whose inverse transforms ran as k_xinv_rows: the
+// The assembly of a basin whose inverse transforms ran as k_xinv_rows: the
 // homogeneous correction and modes_to_layers (modes.F90:268-284) of every
 // point from the modal rows in b.inh_g, ocqbdy (vorsubs.F90:58-114) on the
 // walls and the suppress_comp_mode averages (driver.F90:174-189), with the
@@ -1695,15 +1733,25 @@ k_xinv(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par,
 // point per thread in each; a wall point also
 // forms the layer values of its inner neighbour (the same arithmetic as the
 // neighbour's own thread), so no point waits for another.
+// hc: the box's alpha (nl-1), or the channel's c_bt, c_bc1[1..], c_bc2[1..]
+// (homog.F90:280-366, by k_xinv_rows' scalar CTA).
 template <class T, int NL>
 __device__ __forceinline__ void xinv_layers(const BasinDev &b, const T *__restrict__ inh, const T *__restrict__ H,
-                                            const double *ctm, const double *hc, size_t o2, T *pn) {
+                                            const double *ctm, const double *hc, size_t o2, int j, T *pn) {
     const size_t ms = (size_t)b.nyp * b.px;
     double pm_[NL];
 #pragma unroll
     for (int m = 0; m < NL; ++m) pm_[m] = (double)inh[m * ms + o2];
+    if (!b.cyclic) {
 #pragma unroll
-    for (int m = 1; m < NL; ++m) pm_[m] = pm_[m] + hc[m - 1] * (double)H[(m - 1) * ms + o2];
+        for (int m = 1; m < NL; ++m) pm_[m] = pm_[m] + hc[m - 1] * (double)H[(m - 1) * ms + o2];
+    } else {
+        const int nyp = b.nyp;
+        pm_[0] = pm_[0] + hc[0] * b.hbt[j];
+#pragma unroll
+        for (int m = 1; m < NL; ++m)
+            pm_[m] = pm_[m] + (hc[m] * b.hbc1[m * nyp + j] + hc[NL + m] * b.hbc2[m * nyp + j]);
+    }
 #pragma unroll
     for (int k = 0; k < NL; ++k) {
         double s2 = 0.0;
@@ -1718,7 +1766,7 @@ __global__ void __launch_bounds__(256)
 k_xinv_asm(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int par) {
     const Work w = work[blockIdx.x];
     const BasinDev &b = bas[w.member];
-    __shared__ double sCtm[NL * NL], sAmat[NL * NL], sHc[NL > 1 ? NL - 1 : 1];
+    __shared__ double sCtm[NL * NL], sAmat[NL * NL], sHc[2 * NL];
     __shared__ int sSupp;
     pdl_trigger();
     pdl_wait();
@@ -1727,14 +1775,20 @@ k_xinv_asm(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int 
         sCtm[threadIdx.x] = b.ctm2l[threadIdx.x];
         sAmat[threadIdx.x] = b.amat[threadIdx.x];
     }
-    if (threadIdx.x < NL - 1) sHc[threadIdx.x] = sc->alpha[threadIdx.x];
+    if (!b.cyclic) {
+        if (threadIdx.x < NL - 1) sHc[threadIdx.x] = sc->alpha[threadIdx.x];
+    } else if (threadIdx.x < 2 * NL) {
+        // c_bt, c_bc1[1..NL), then c_bc2 at NL + m
+        const int x = threadIdx.x;
+        sHc[x] = x == 0 ? sc->c_bt : (x < NL ? sc->c_bc1[x] : (x == NL ? 0.0 : sc->c_bc2[x - NL]));
+    }
     if (threadIdx.x == 0) sSupp = sc->supp;
     __syncthreads();
-    double ctm[NL * NL], hc[NL > 1 ? NL - 1 : 1];
+    double ctm[NL * NL], hc[2 * NL];
 #pragma unroll
     for (int x = 0; x < NL * NL; ++x) ctm[x] = sCtm[x];
 #pragma unroll
-    for (int m = 0; m < NL - 1; ++m) hc[m] = sHc[m];
+    for (int m = 0; m < 2 * NL; ++m) hc[m] = sHc[m];
     const bool supp = sSupp != 0;
     const int nxp = b.nxp, nyp = b.nyp, px = b.px;
     const size_t ms = (size_t)nyp * px;
@@ -1754,12 +1808,12 @@ k_xinv_asm(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int 
         const int j = fdx.div(idx), i = idx - j * nxp;
         const size_t o2 = (size_t)j * px + i;
         T pn[NL];
-        xinv_layers<T, NL>(b, inh, H, ctm, hc, o2, pn);
+        xinv_layers<T, NL>(b, inh, H, ctm, hc, o2, j, pn);
 #pragma unroll
         for (int k = 0; k < NL; ++k)
             Pnew[k * ms + o2] = supp ? (T)((T)0.5 * (pn[k] + Pold[k * ms + o2])) : pn[k];
         const bool zon = (j == 0 || j == nyp - 1);
-        const bool mer = (i == 0 || i == nxp - 1);
+        const bool mer = !b.cyclic && (i == 0 || i == nxp - 1);
         if (!zon && !mer) {
             if (supp)
 #pragma unroll
@@ -1768,10 +1822,10 @@ k_xinv_asm(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int 
         }
         // ocqbdy: the inner neighbour across the meridional wall (a corner
         // takes that one), else across the zonal wall
-        const size_t on = mer ? (size_t)j * px + (i == 0 ? 1 : nxp - 2)
-                              : (size_t)(j == 0 ? 1 : nyp - 2) * px + i;
+        const int jn = mer ? j : (j == 0 ? 1 : nyp - 2);
+        const size_t on = mer ? (size_t)j * px + (i == 0 ? 1 : nxp - 2) : (size_t)jn * px + i;
         T pnb[NL];
-        xinv_layers<T, NL>(b, inh, H, ctm, hc, on, pnb);
+        xinv_layers<T, NL>(b, inh, H, ctm, hc, on, jn, pnb);
         const int cnt = (zon ? 1 : 0) + (mer ? 1 : 0);
         const T by = (T)(b.beta * b.yprel[j]);
 #pragma unroll

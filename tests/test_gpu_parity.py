@@ -206,11 +206,23 @@ def test_step_parity_separate_inverse(b, kw):
     assert_state_close(g, o, 1e-10, "31 steps")
 
 
-def test_separate_inverse_is_box_only():
-    g = QG(atmos_channel(49, 25))
-    with pytest.raises(Exception):
-        g.set_xinv_sep(True)
-    g.close()
+@pytest.mark.parametrize("b,kw", [STEP_CASES[i] for i in (7, 8, 9, 12)],
+                         ids=[STEP_IDS[i] for i in (7, 8, 9, 12)])
+def test_step_parity_channel_separate_inverse(b, kw):
+    """Channels with the inverse transforms (c2r) as a launch of their own
+    and the one-pass assembly (the one-kernel form is their default)."""
+    g, o = make_pair(b, **kw)
+    assert not g.xinv_sep() and g.step_launches() == 4
+    g.set_xinv_sep(True)
+    assert g.xinv_sep() and g.step_launches() == 5
+    g.step(360.0, 1)
+    o.step(360.0, 1)
+    assert_state_close(g, o, 1e-12, "1 step")
+    assert_constraints_close(g, o, 1e-11)
+    g.step(360.0, 9)
+    o.step(360.0, 9)
+    assert_state_close(g, o, 1e-10, "10 steps")
+    assert_constraints_close(g, o, 1e-9)
 
 
 def test_topography_and_drag_layer():
