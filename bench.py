@@ -119,6 +119,7 @@ def run_ensemble(precision, steps, warmup, msteps, flush, tdt=3600.0, rank=0, ws
     e.sync()
     s = torch.cuda.ExternalStream(e.stream())
     total = 0.0
+    torch.cuda.nvtx.range_push("ensemble_steps")
     for _ in range(steps):
         flush.zero_()
         torch.cuda.synchronize()
@@ -128,6 +129,7 @@ def run_ensemble(precision, steps, warmup, msteps, flush, tdt=3600.0, rank=0, ws
         e1.record(s)
         e1.synchronize()
         total += e0.elapsed_time(e1)
+    torch.cuda.nvtx.range_pop()
     e.sync()
     cells = sum(b.nxp * b.nyp * b.nl for b in all_basins)
     e.close()
@@ -932,6 +934,8 @@ def main():
                          "print its figures; for profiling")
     ap.add_argument("--adjoint-n", type=int, default=257, choices=sorted(ADJOINT_BOXES),
                     help="box size of --adjoint-only")
+    ap.add_argument("--ensemble-only", action="store_true",
+                    help="time only the 256-member ensemble (--precision) and print its figure; for profiling")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -946,6 +950,16 @@ def main():
         dx, ah4, tdt = ADJOINT_BOXES[args.adjoint_n]
         print(json.dumps(run_adjoint(reps=1, n=args.adjoint_n, dx=dx, ah4=ah4, nsteps=40, every=20, tdt=tdt)),
               flush=True)
+        return 0
+    if args.ensemble_only:
+        import torch
+        from openqg_b200.params import OQG_FP64, OQG_MIXED
+        torch.cuda.set_device(0)
+        flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+        prec = OQG_MIXED if args.precision == "mixed" else OQG_FP64
+        cells, te, rows = run_ensemble(prec, args.steps, args.warmup, args.model_steps, flush)
+        print(json.dumps({"ensemble256": args.precision, "value": replica_value(te, 1, cells, args.model_steps, args.steps),
+                          "unit": "Mcell-layer-steps/s", "tile_rows": rows}), flush=True)
         return 0
     return run_ours(args)
 
