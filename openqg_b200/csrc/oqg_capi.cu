@@ -1,9 +1,10 @@
 // oqg_capi.cu -- the C ABI of include/oqg.h: handles, device memory, launches.
 //
 // A handle is one basin on one device with its own stream.  oqg_step queues
-// step_qg (qg/core.F90:16-33) as four kernels per step; pairs of steps are
-// captured once into a CUDA graph (the parity of the p/q buffers returns after
-// two steps) and replayed.
+// step_qg (qg/core.F90:16-33) as five kernels per step (four when the inverse
+// transforms and the assembly share one kernel); runs of steps are captured
+// into CUDA graphs (the parity of the p/q buffers returns after two steps)
+// and replayed.
 #include "../../include/oqg.h"
 #include "oqg_dev.cuh"
 #include "oqg_kernels.cuh"

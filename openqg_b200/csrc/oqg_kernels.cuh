@@ -1,13 +1,14 @@
 // oqg_kernels.cuh -- the per-step kernels of the QG core (sm_100a).
 //
-// One step_qg (qg/core.F90:16-33) is four launches, one per dependent phase:
+// One step_qg (qg/core.F90:16-33) is a chain of launches, one per dependent
+// phase:
 //   k_vort   vort_step (qg/vorticity.F90:14-103) + p_modes_rhs (qg/modes.F90:248-266)
 //            2-D tiles staged in shared memory; the layer loop runs inside the
 //            CTA so the modal right-hand side is formed in registers.
 //   k_xfwd   forward x-transform of solve_inhomog_box / _cyclic
 //            (qg/inhomog.F90:170-255): DST-I (box) or r2c FFT (channel).
 //   k_ysolve Thomas solve in y per (mode, wavenumber) (inhomog.F90:187-199),
-//            one warp per column as a warp-parallel affine scan.
+//            one to four warps per column as a warp-parallel affine scan.
 //   k_xinv   inverse x-transform + homogeneous correction + modes_to_layers
 //            (modes.F90:268-284) + ocqbdy (vorsubs.F90:58-114) +
 //            suppress_comp_mode (driver.F90:174-189).  One warp of each CTA
@@ -16,6 +17,11 @@
 //            or step_constraints + cyclic_homog (constraint.F90:182-215,
 //            homog.F90:280-329), and the suppress_comp_mode schedule
 //            (openqg.F90:485-487).
+//   or, as two launches (the default for boxes, measured for channels):
+//   k_xinv_rows  the inverse x-transforms alone, shaped like k_xfwd, with one
+//            extra CTA per basin for the scalar phase;
+//   k_xinv_asm   the homogeneous correction, modes_to_layers, ocqbdy and the
+//            suppression averages, one thread per point.
 // Every launch takes a work list, so one launch serves one basin or an
 // ensemble of basins of uneven size.
 #pragma once
@@ -858,7 +864,8 @@ __device__ __forceinline__ void ysolve_chunk_regs(V *col, const double *__restri
         const double ej = -a * bt[t];
         uu = yt_axpy(x[t], ej, uu);
         x[t] = uu;
-        colsum.add(yt_re(uu));
+        // the box's dst_w-weighted column sum (a channel has none)
+        if constexpr (std::is_same<V, double>::value) colsum.add(yt_re(uu));
     }
 #pragma unroll
     for (int t = 0; t < SM; ++t)
@@ -992,7 +999,7 @@ k_ysolve(const BasinDev *__restrict__ bas, const Work *__restrict__ work) {
             const double ej = (s + t == ny - 1) ? 0.0 : -a * __ldg(piv + min(s + t, plen - 1));
             uu = yt_axpy(col[o + t], ej, uu);
             col[o + t] = uu;
-            colsum.add(yt_re(uu));
+            if constexpr (std::is_same<V, double>::value) colsum.add(yt_re(uu));
         }
     }
     // dst_w-weighted column sum (box), one compensated partial per warp
