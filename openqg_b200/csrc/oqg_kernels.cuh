@@ -925,29 +925,20 @@ k_ysolve(const BasinDev *__restrict__ bas, const Work *__restrict__ work) {
     Gm *S = (Gm *)b.spec + (size_t)m * ny * pk;
     pdl_trigger();
     pdl_wait();
-    // load the spectral columns: a thread keeps one column (thread % 4) and
-    // steps over rows NT/4 apart, so a warp reads 8 rows x 4 adjacent columns
-    // (whole 32-byte sectors) and the padded tile index of a row is a shift
-    // when S is a power of two
-    constexpr int RS = NT / KB;                 // rows per pass
-    const int cl = threadIdx.x & (KB - 1), jr = threadIdx.x / KB;
-    const bool colok = k0 + cl < nk;
-    const int sh = (S_ & (S_ - 1)) == 0 ? __ffs(S_) - 1 : -1;
-    auto padded = [&](int jj) { return jj + (sh >= 0 ? (jj >> sh) : fdS.div(jj)); };
-    const size_t rstep = (size_t)RS * pk;
-    const Gm *src = S + (size_t)jr * pk + (colok ? k0 + cl : 0);
-    V *dst = tile + cl * LD;
-    for (int j0 = 0; j0 < ny; j0 += RS * CH) {
+    // load the spectral columns: thread -> (row, column), coalesced along k
+    for (int i0 = threadIdx.x; i0 < ny * KB; i0 += NT * CH) {
         V v[CH];
 #pragma unroll
         for (int u = 0; u < CH; ++u) {
-            const int jj = jr + j0 + RS * u;
-            v[u] = (jj < ny && colok) ? yt_load(src[(size_t)(j0 / RS + u) * rstep]) : yt_zero(V());
+            const int idx = i0 + NT * u;
+            const int jj = idx >> 2, cc = idx & 3, kk = k0 + cc;
+            v[u] = (idx < ny * KB && kk < nk) ? yt_load(S[(size_t)jj * pk + kk]) : yt_zero(V());
         }
 #pragma unroll
         for (int u = 0; u < CH; ++u) {
-            const int jj = jr + j0 + RS * u;
-            if (jj < ny) dst[padded(jj)] = v[u];
+            const int idx = i0 + NT * u;
+            const int jj = idx >> 2, cc = idx & 3;
+            if (idx < ny * KB) tile[cc * LD + jj + fdS.div(jj)] = v[u];
         }
     }
     __syncthreads();
@@ -1013,16 +1004,14 @@ k_ysolve(const BasinDev *__restrict__ bas, const Work *__restrict__ work) {
         }
     }
     __syncthreads();
-    if (colok) {
-        Gm *out = S + (size_t)jr * pk + k0 + cl;
-        for (int j0 = 0; j0 < ny; j0 += RS * CH) {
+    for (int i0 = threadIdx.x; i0 < ny * KB; i0 += NT * CH) {
 #pragma unroll
-            for (int u = 0; u < CH; ++u) {
-                const int jj = jr + j0 + RS * u;
-                if (jj < ny) {
-                    if constexpr (CPLX) out[(size_t)(j0 / RS + u) * rstep] = yt_store2<Gm>(dst[padded(jj)]);
-                    else out[(size_t)(j0 / RS + u) * rstep] = yt_store<Gm>(dst[padded(jj)]);
-                }
+        for (int u = 0; u < CH; ++u) {
+            const int idx = i0 + NT * u;
+            const int jj = idx >> 2, cc = idx & 3, kk = k0 + cc;
+            if (idx < ny * KB && kk < nk) {
+                if constexpr (CPLX) S[(size_t)jj * pk + kk] = yt_store2<Gm>(tile[cc * LD + jj + fdS.div(jj)]);
+                else S[(size_t)jj * pk + kk] = yt_store<Gm>(tile[cc * LD + jj + fdS.div(jj)]);
             }
         }
     }
