@@ -1776,12 +1776,13 @@ k_xinv_asm(const BasinDev *__restrict__ bas, const Work *__restrict__ work, int 
     __shared__ double sCtm[NL * NL], sAmat[NL * NL], sHc[2 * NL];
     __shared__ int sSupp;
     pdl_trigger();
-    pdl_wait();
-    const XinvScal *sc = (const XinvScal *)b.scal_g;
+    // the basin's constant tables before the wait for the previous launch
     if (threadIdx.x < NL * NL) {
         sCtm[threadIdx.x] = b.ctm2l[threadIdx.x];
         sAmat[threadIdx.x] = b.amat[threadIdx.x];
     }
+    pdl_wait();
+    const XinvScal *sc = (const XinvScal *)b.scal_g;
     if (!b.cyclic) {
         if (threadIdx.x < NL - 1) sHc[threadIdx.x] = sc->alpha[threadIdx.x];
     } else if (threadIdx.x < 2 * NL) {
