@@ -174,11 +174,12 @@ static int ysolve_warps(int ny, long long ncols) {
 #define OQG_XLENS(X) X(256) X(512) X(1024) X(2048) X(4096)
 template <class T, int E>
 static void (*xfwd_kernel(int M))(const BasinDev *, const Work *, const void *) {
-    // FP32 storage keeps the any-length instances: at 513^2 the step measured
-    // 44.5 us with them against 48.1 us with the per-length ones (which take
-    // 80 registers instead of 128); FP64 measured 51.0 against 53.8 us the
-    // other way round
-    if (std::is_same<T, float>::value) M = 0;
+    // FP32 storage keeps the any-length instances below the in-place lengths:
+    // at 513^2 the step measured 44.5 us with them against 48.1 us with the
+    // per-length ones (which take 80 registers instead of 128), while at
+    // 2049^2 the per-length forward transform measured 72 against 79 us;
+    // FP64 measured 51.0 against 53.8 us at 513^2 the other way round
+    if (std::is_same<T, float>::value && !fft_inplace_len(M)) M = 0;
     switch (M) {
 #define OQG_XF(MM) case MM: return k_xfwd<T, E, MM>;
         OQG_XLENS(OQG_XF)
@@ -188,7 +189,7 @@ static void (*xfwd_kernel(int M))(const BasinDev *, const Work *, const void *) 
 }
 template <class T, int NL, int E>
 static void (*xinv_rows_kernel(int M))(const BasinDev *, const Work *, int, int, int, double, T *) {
-    if (std::is_same<T, float>::value) M = 0;      // as xfwd_kernel
+    if (std::is_same<T, float>::value && !fft_inplace_len(M)) M = 0;      // as xfwd_kernel
     switch (M) {
 #define OQG_XI(MM) case MM: return k_xinv_rows<T, NL, E, MM>;
         OQG_XLENS(OQG_XI)
