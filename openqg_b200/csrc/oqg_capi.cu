@@ -169,9 +169,10 @@ static int ysolve_warps(int ny, long long ncols) {
 }
 
 // The transform kernels' instance for a basin's transform length: one built
-// for each length of the configurations' boxes (only that FFT plan in its
-// code), the any-length one otherwise (and for ensembles).
-#define OQG_XLENS(X) X(256) X(512) X(1024) X(2048) X(4096)
+// for each length of the configurations' grids (boxes of 65 to 2049 points,
+// the 193-point channel; only that FFT plan in its code), the any-length one
+// otherwise (and for ensembles).
+#define OQG_XLENS(X) X(128) X(192) X(256) X(384) X(512) X(1024) X(2048) X(4096)
 template <class T, int E>
 static void (*xfwd_kernel(int M))(const BasinDev *, const Work *, const void *) {
     // FP32 storage keeps the any-length instances below the in-place lengths:
