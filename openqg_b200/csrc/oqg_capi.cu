@@ -648,6 +648,7 @@ struct oqg_ensemble {
     Work *d_wa = nullptr;              // k_xinv_asm work items (boxes)
     int na = 0;                        // k_xinv_asm work items
     bool sep = false;                  // boxes: k_xinv_rows + k_xinv_asm
+    int Mu = 0;                        // the members' common transform length, else 0
     int nv = 0, nx = 0, nys = 0, ni = 0;
     size_t smem_v = 0, smem_x = 0, smem_y = 0, smem_i = 0;
     int xi_threads = 64, xthreads = 128;
@@ -677,13 +678,15 @@ struct oqg_ensemble {
 template <class T, int NL, int E>
 static void launch_ens_step_t(oqg_ensemble *e, int par) {
     launch_pdl(vort_kernel<T, NL>(e->hb[0].vty), e->nv, VTHREADS, e->smem_v, e->st, e->d_bas, e->d_wv, par, 0.0);
-    launch_pdl(k_xfwd<T, E>, e->nx, e->xthreads, e->smem_x, e->st, e->d_bas, e->d_wx, (const void *)nullptr);
+    // members of one transform length take that length's instance
+    launch_pdl(xfwd_kernel<T, E>(e->Mu), e->nx, e->xthreads, e->smem_x, e->st, e->d_bas, e->d_wx,
+               (const void *)nullptr);
     launch_ysolve<T>(e->cyclic, e->yW, e->nys, e->smem_y, e->st, e->d_bas, e->d_wy, true);
     if (e->sep) {
         // per-member transform groups (G = 0) and one scalar CTA per member
         const int nm = (int)e->m.size();
-        launch_pdl(k_xinv_rows<T, NL, E>, e->nx + nm, e->xthreads, e->smem_x, e->st, e->d_bas, e->d_wx, 0, nm, par,
-                   0.0, (T *)nullptr);
+        launch_pdl(xinv_rows_kernel<T, NL, E>(e->Mu), e->nx + nm, e->xthreads, e->smem_x, e->st, e->d_bas, e->d_wx,
+                   0, nm, par, 0.0, (T *)nullptr);
         launch_pdl(k_xinv_asm<T, NL>, e->na, 256, 0, e->st, e->d_bas, (const Work *)e->d_wa, par);
     } else {
         launch_pdl(k_xinv<T, NL>, e->ni, e->xi_threads, e->smem_i, e->st, e->d_bas, e->d_wi, par, 0.0,
@@ -1761,6 +1764,9 @@ int oqg_ensemble_create(const oqg_params *members, int nmembers, oqg_ensemble **
     // boxes invert as a transform launch and a one-pass assembly, as single
     // handles do
     e->sep = !e->cyclic;
+    e->Mu = e->m[0]->hb.M;
+    for (oqg_handle *h : e->m)
+        if (h->hb.M != e->Mu) e->Mu = 0;
     int nfft_e = 32;
     for (oqg_handle *h : e->m) nfft_e = std::max(nfft_e, xinv_fft_threads(h->hb.M, h->hb.nl));
     e->xi_threads = nfft_e + 32;

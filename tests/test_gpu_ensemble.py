@@ -73,6 +73,16 @@ def test_box_ensemble_equals_single_handles():
     _assert_same(e, singles)
 
 
+def test_uniform_box_ensemble_equals_single_handles():
+    """Members of one transform length take that length's transform
+    instances, as a single handle of the same size does."""
+    members = [ocean_double_gyre(129) for _ in range(3)]
+    for i, b in enumerate(members):
+        b.ah4 = [(1.0 + i) * 1e10] * 3
+    e, singles = _run_pair(members, 3600.0, 4)
+    _assert_same(e, singles)
+
+
 def test_box_ensemble_member_matches_oracle():
     members = [ocean_double_gyre(97), ocean_double_gyre(65)]
     e = Ensemble(members)
